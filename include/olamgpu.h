@@ -1,0 +1,238 @@
+/*
+ * olamgpu.h -- C-ABI of the B200 implementation of OLAM's dynamical-core hot
+ * path: the acoustic RK short step (prog_wrtv_rk) and the flux-form tracer
+ * transport (scalar_transport_rk).
+ *
+ * The caller is OLAM's Fortran model through ISO_C_BINDING, so every array is
+ * passed exactly as OLAM holds it: Fortran column-major (mza, n) with the
+ * vertical index fastest, neighbour tables with OLAM's 1-based indices, and
+ * point 1 of every horizontal dimension as OLAM's dummy point.  No argument
+ * is a C++ or PyTorch type.  Every function returns an int status
+ * (OLAMGPU_OK = 0); olamgpu_strerror() turns it into text.  There is no CPU
+ * fallback: a missing or unusable GPU is an error.
+ *
+ * Reference interfaces replaced (martinjotte/OLAM v7.0):
+ *   olamgpu_init                 -> wrtv_rk::init_wrtv_rk  (omodel/prog_wrtv_rk.f90:36-54),
+ *                                   called at omodel/olam_run.f90:566 after
+ *                                   alloc_adv (:342) and the state initialisation
+ *   olamgpu_prog_wrtv_rk         -> wrtv_rk::prog_wrtv_rk  (omodel/prog_wrtv_rk.f90:58-488),
+ *                                   called at omodel/timestep.f90:205
+ *   olamgpu_scalar_transport_rk  -> scalar_transport::scalar_transport_rk(rho_old)
+ *                                   (omodel/scalar_transport_rk.F90:30-385),
+ *                                   called at omodel/timestep.f90:254
+ *   olamgpu_tend0                -> tend0 (omodel/timestep.f90:430-496)
+ *   olamgpu_timeavg_momsc        -> timeavg_momsc (omodel/timestep.f90:563-612)
+ */
+#ifndef OLAMGPU_H
+#define OLAMGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  OLAMGPU_OK = 0,
+  OLAMGPU_E_ARG = 1,          /* null pointer, bad size or inconsistent table  */
+  OLAMGPU_E_STATE = 2,        /* call out of order (not initialised, ...)      */
+  OLAMGPU_E_UNSUPPORTED = 3,  /* option combination this build does not run    */
+  OLAMGPU_E_CUDA = 4,         /* CUDA runtime error (message via strerror)     */
+  OLAMGPU_E_NOMEM = 5,        /* device allocation failed                      */
+  OLAMGPU_E_NODEVICE = 6,     /* no usable sm_100 device                       */
+  OLAMGPU_E_NUMERIC = 7       /* device status word reported a failure         */
+};
+
+/* ---- grid (modules mem_grid, mem_ijtabs, mem_adv) ----------------------- */
+/* Sizes are OLAM's: mza levels, mwa/mva/mma points INCLUDING dummy point 1.
+ * Per-point tables of OLAM derived types are passed packed, e.g. itab_w%iv
+ * as an int array (7, mwa) (member index fastest). */
+typedef struct olamgpu_grid {
+  int mza, mwa, mva, mma;
+
+  /* loop tables jtab_w(jtw_prog)%iw(1:jend) etc. (1-based point indices) */
+  int nw_prog;  const int* jtw_prog;
+  int nw_wadj;  const int* jtw_wadj;
+  int nv_prog;  const int* jtv_prog;
+  int nv_wadj;  const int* jtv_wadj;
+  int nm_prog;  const int* jtm_prog;
+
+  /* itab_w (mem_ijtabs.f90:74-110): (7, mwa) unless noted */
+  const int*   npoly;        /* (mwa) */
+  const int*   itab_w_iv;
+  const int*   itab_w_iw;
+  const int*   itab_w_im;
+  const float* itab_w_dirv;
+  const float* ecvec_vx;
+  const float* ecvec_vy;
+  const float* ecvec_vz;
+  const int*   iwglobe;      /* (mwa) */
+
+  /* itab_v (mem_ijtabs.f90:60-72): (2, mva) */
+  const int*   itab_v_iw;
+  const int*   itab_v_im;
+  const float* dxps;
+  const float* dyps;
+
+  /* itab_m (mem_ijtabs.f90:46-58): (3, mma) */
+  const int*   itab_m_iv;
+  const int*   itab_m_iw;
+  const int*   itab_m_im;
+
+  /* lowest prognosed levels (mem_grid.f90:20-24) */
+  const int* lpw;  const int* lpv;  const int* lpm;  const int* lve2;
+
+  /* 1-D vertical arrays (mza) */
+  const float*  zm;  const float* zt;  const float* dzm;  const float* dzt;
+  const float*  dzim; const float* dzit; const float* dzt_top; const float* dzt_bot;
+  const float*  zfacit;
+  const double* zwgt_top8; const double* zwgt_bot8;
+  const double* gdz_wgtm8; const double* gdz_wgtp8;
+  const float*  gdz_wgtm;  const float*  gdz_wgtp;
+
+  /* horizontal metrics */
+  const float* wnx;  const float* wny;  const float* wnz;     /* (mwa) */
+  const float* wnxo2; const float* wnyo2; const float* wnzo2; /* (mwa) */
+  const float* vnx;  const float* vny;  const float* vnz;     /* (mva) */
+  const float* dnu;  const float* dniu; const float* dnv; const float* dniv; /* (mva) */
+  const float* arw0; const float* arm0;                        /* (mwa), (mma) */
+
+  /* 3-D control volumes */
+  const float*  arv;    /* (mza, mva) */
+  const float*  arw;    /* (mza, mwa) */
+  const double* volt;   /* (mza, mwa) */
+  const float*  volti;  /* (mza, mwa) */
+  const float*  volwi;  /* (mza, mwa) */
+  const float*  volvi;  /* (mza, mva) */
+
+  /* reconstruction coefficients */
+  const float* gxps_coef; const float* gyps_coef;   /* (7, mwa) */
+  const float* a_w;  const float* a_wu;              /* (mza, 2, 2) */
+  const float* xy_h; const float* xy_hu;             /* (5, 7, mwa) */
+  const float* xx0_v;  const float* xy0_v;  const float* yy0_v;   /* (2, mva) */
+  const float* xx0_vu; const float* xy0_vu; const float* yy0_vu;  /* (2, mva) */
+  const float* xx_yy;   /* (7, mwa) */
+  const float* xx_yy_m; /* (3, mma) */
+} olamgpu_grid;
+
+/* ---- namelist options (oname_coms.f90:189-236, misc_coms) ----------------- */
+typedef struct olamgpu_opts {
+  double dtlm, dtsm;            /* long and acoustic timesteps [s]            */
+  int    nacoust;
+  int    nrk_wrtv, nrk_scal;    /* acoust_ / scalar_timestep_level (2 or 3)    */
+  int    thil_horiz_adv_order, wind_horiz_adv_order, scal_horiz_adv_order;
+  int    ithil_monot, iwind_monot, iscal_monot;
+  float  divh_damp_fact;  int divh_damp_level;  int divh_damp_short;
+  float  vort_damp_fact;  int vort_damp_level;  int vort_damp_short;
+  float  fcoriol;               /* 2*omega for a global domain                 */
+  int    mdomain;               /* 0 = global (the only domain this build runs)*/
+  /* Rayleigh friction (modules/mem_rayf.f90); all off when the pointers are NULL */
+  int          krayf_bot;       /* first level of rayf_cof, > mza when off      */
+  const float* rayf_cof;        /* (mza) or NULL                                */
+  const float* dn01d;           /* (mza) reference density   (initial == 1)     */
+  const float* th01d;           /* (mza) reference theta     (initial == 1)     */
+  const float* vc03d;           /* (mza, mva) reference VC                      */
+  int          krayfw_bot;
+  const float* rayf_cofw;       /* (mza) or NULL: W damping via b20             */
+  int          initial;
+} olamgpu_opts;
+
+/* ---- prognostic state (mem_basic, mem_tend) ------------------------------ */
+/* Host arrays the library reads and writes at the sync points. */
+typedef struct olamgpu_state {
+  double* rho;   double* press;                          /* (mza, mwa) r8 */
+  float*  thil;  float* wc; float* wmc;                  /* (mza, mwa)    */
+  float*  vxe;   float* vye; float* vze;                 /* (mza, mwa)    */
+  float*  vmc;   float* vc;                              /* (mza, mva)    */
+  float*  vmasc;                                         /* (mza, mva)    */
+  float*  wmasc;                                         /* (mza, mwa)    */
+  float*  alpha_press; float* pwfac;                     /* (mza, mwa)    */
+  float*  pvfac;                                         /* (mza, mva)    */
+  float*  thilt; float* vmxet; float* vmyet; float* vmzet; /* (mza, mwa)  */
+  float*  vmt;                                           /* (mza, mva)    */
+} olamgpu_state;
+
+/* field masks for olamgpu_sync_* */
+enum {
+  OLAMGPU_F_RHO = 1u << 0,   OLAMGPU_F_PRESS = 1u << 1, OLAMGPU_F_THIL = 1u << 2,
+  OLAMGPU_F_WC = 1u << 3,    OLAMGPU_F_WMC = 1u << 4,   OLAMGPU_F_VXE = 1u << 5,
+  OLAMGPU_F_VMC = 1u << 6,   OLAMGPU_F_VC = 1u << 7,    OLAMGPU_F_VMASC = 1u << 8,
+  OLAMGPU_F_WMASC = 1u << 9, OLAMGPU_F_TEND = 1u << 10, OLAMGPU_F_FACS = 1u << 11,
+  OLAMGPU_F_SCALARS = 1u << 12, OLAMGPU_F_SCALAR_TEND = 1u << 13,
+  OLAMGPU_F_ALL = 0xffffu
+};
+
+/* diagnostics written by check_cfls (scalar_transport_rk.F90:1476-1712) */
+typedef struct olamgpu_cfl_diag {
+  float cfl_max;  int cfl_k;  int cfl_iwglobe;     /* max total CFL  */
+  float cflh_max; int cflh_k; int cflh_iwglobe;    /* max horiz CFL  */
+  float w_max;    int w_k;    int w_iwglobe;       /* max |W| (signed) */
+} olamgpu_cfl_diag;
+
+/* ---- lifecycle ------------------------------------------------------------ */
+
+/* Replaces init_wrtv_rk (prog_wrtv_rk.f90:36-54).  Uploads the grid, packs
+ * the device neighbour tables (0-based), builds the transport tiles, and
+ * allocates device mirrors.  Must be called once, after alloc_adv. */
+int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts,
+                 const olamgpu_state* state);
+
+/* Registers the tracer table (var_tables.f90:53-69): num_scalar arrays
+ * var_p(mza,mwa) and tendencies var_t(mza,mwa), pdef and do_sgsmix flags.
+ * The host arrays are page-locked in place for fast transfers. */
+int olamgpu_register_scalars(int num_scalar, float* const* var_p,
+                             float* const* var_t, const int* pdef,
+                             const int* do_sgsmix);
+
+/* Optional turbulence inputs of the horizontal-diffusion hook
+ * (scalar_transport_rk.F90:244-274): akhodx (mza, mva), khtopv (mva).
+ * Without them diffusion is inactive, as with OLAM's idiffk = 0. */
+int olamgpu_set_turb(const float* akhodx, const int* khtopv);
+
+int olamgpu_finalize(void);
+const char* olamgpu_strerror(int status);
+
+/* ---- hot path ------------------------------------------------------------- */
+
+/* Coherence of host and device copies.
+ * OLAMGPU_SYNC_EACH_CALL (default): every hot-path call uploads its inputs
+ *   from the registered host arrays and downloads its outputs, so the call
+ *   is a drop-in for the Fortran routine.
+ * OLAMGPU_RESIDENT: state stays on the device between calls; the caller
+ *   moves fields with olamgpu_sync_to_device / olamgpu_sync_to_host where CPU
+ *   physics reads or writes them. */
+enum { OLAMGPU_SYNC_EACH_CALL = 0, OLAMGPU_RESIDENT = 1 };
+int olamgpu_set_coherence(int mode);
+int olamgpu_sync_to_device(unsigned fieldmask);
+int olamgpu_sync_to_host(unsigned fieldmask);
+
+/* Transport form: fused batched kernels (default) or one set of kernels per
+ * tracer mirroring the reference's passes (kept for comparison). */
+enum { OLAMGPU_TRANSPORT_FUSED = 0, OLAMGPU_TRANSPORT_PLAIN = 1 };
+int olamgpu_set_transport_form(int form);
+
+/* Replaces scalar_transport_rk(rho_old) (scalar_transport_rk.F90:30-385).
+ * rho_old(mza,mwa) is the host array OLAM passes; in RESIDENT mode it may
+ * be NULL, and the device copy saved by olamgpu_tend0 is used.
+ * diag (optional) receives the check_cfls maxima. */
+int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag);
+
+/* Replaces prog_wrtv_rk() (prog_wrtv_rk.f90:58-488); istp is mem_ijtabs%istp. */
+int olamgpu_prog_wrtv_rk(int istp);
+
+/* Glue of timestep (timestep.f90:430-496, 563-612). */
+int olamgpu_tend0(float* rho_old);
+int olamgpu_timeavg_momsc(void);
+
+/* Device-side CUDA stream the library launches on (cudaStream_t as void*),
+ * so a caller can order its own work against the library's. */
+void* olamgpu_stream(void);
+
+/* Number of library kernel launches issued since the last reset. */
+unsigned long long olamgpu_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OLAMGPU_H */

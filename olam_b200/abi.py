@@ -1,0 +1,216 @@
+"""ctypes mirror of include/olamgpu.h and Fortran-layout packing of a grid.
+
+OLAM hands the library its module arrays through ISO_C_BINDING; this module
+does the same from Python so tests and benchmarks drive the library exactly
+as the Fortran shim would: column-major (mza, n) arrays, OLAM's 1-based
+neighbour indices, and packed derived-type members.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+c_int_p = C.POINTER(C.c_int)
+c_float_p = C.POINTER(C.c_float)
+c_double_p = C.POINTER(C.c_double)
+
+OK = 0
+E_ARG, E_STATE, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_NODEVICE, E_NUMERIC = range(1, 8)
+
+SYNC_EACH_CALL, RESIDENT = 0, 1
+TRANSPORT_FUSED, TRANSPORT_PLAIN = 0, 1
+
+F_RHO, F_PRESS, F_THIL, F_WC, F_WMC, F_VXE, F_VMC, F_VC = (1 << i for i in range(8))
+F_VMASC, F_WMASC, F_TEND, F_FACS, F_SCALARS, F_SCALAR_TEND = (1 << i for i in range(8, 14))
+F_ALL = 0xFFFF
+
+
+class Grid(C.Structure):
+    _fields_ = [
+        ("mza", C.c_int), ("mwa", C.c_int), ("mva", C.c_int), ("mma", C.c_int),
+        ("nw_prog", C.c_int), ("jtw_prog", c_int_p),
+        ("nw_wadj", C.c_int), ("jtw_wadj", c_int_p),
+        ("nv_prog", C.c_int), ("jtv_prog", c_int_p),
+        ("nv_wadj", C.c_int), ("jtv_wadj", c_int_p),
+        ("nm_prog", C.c_int), ("jtm_prog", c_int_p),
+        ("npoly", c_int_p), ("itab_w_iv", c_int_p), ("itab_w_iw", c_int_p),
+        ("itab_w_im", c_int_p), ("itab_w_dirv", c_float_p),
+        ("ecvec_vx", c_float_p), ("ecvec_vy", c_float_p), ("ecvec_vz", c_float_p),
+        ("iwglobe", c_int_p),
+        ("itab_v_iw", c_int_p), ("itab_v_im", c_int_p), ("dxps", c_float_p), ("dyps", c_float_p),
+        ("itab_m_iv", c_int_p), ("itab_m_iw", c_int_p), ("itab_m_im", c_int_p),
+        ("lpw", c_int_p), ("lpv", c_int_p), ("lpm", c_int_p), ("lve2", c_int_p),
+        ("zm", c_float_p), ("zt", c_float_p), ("dzm", c_float_p), ("dzt", c_float_p),
+        ("dzim", c_float_p), ("dzit", c_float_p), ("dzt_top", c_float_p), ("dzt_bot", c_float_p),
+        ("zfacit", c_float_p),
+        ("zwgt_top8", c_double_p), ("zwgt_bot8", c_double_p),
+        ("gdz_wgtm8", c_double_p), ("gdz_wgtp8", c_double_p),
+        ("gdz_wgtm", c_float_p), ("gdz_wgtp", c_float_p),
+        ("wnx", c_float_p), ("wny", c_float_p), ("wnz", c_float_p),
+        ("wnxo2", c_float_p), ("wnyo2", c_float_p), ("wnzo2", c_float_p),
+        ("vnx", c_float_p), ("vny", c_float_p), ("vnz", c_float_p),
+        ("dnu", c_float_p), ("dniu", c_float_p), ("dnv", c_float_p), ("dniv", c_float_p),
+        ("arw0", c_float_p), ("arm0", c_float_p),
+        ("arv", c_float_p), ("arw", c_float_p), ("volt", c_double_p), ("volti", c_float_p),
+        ("volwi", c_float_p), ("volvi", c_float_p),
+        ("gxps_coef", c_float_p), ("gyps_coef", c_float_p),
+        ("a_w", c_float_p), ("a_wu", c_float_p), ("xy_h", c_float_p), ("xy_hu", c_float_p),
+        ("xx0_v", c_float_p), ("xy0_v", c_float_p), ("yy0_v", c_float_p),
+        ("xx0_vu", c_float_p), ("xy0_vu", c_float_p), ("yy0_vu", c_float_p),
+        ("xx_yy", c_float_p), ("xx_yy_m", c_float_p),
+    ]
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("dtlm", C.c_double), ("dtsm", C.c_double), ("nacoust", C.c_int),
+        ("nrk_wrtv", C.c_int), ("nrk_scal", C.c_int),
+        ("thil_horiz_adv_order", C.c_int), ("wind_horiz_adv_order", C.c_int),
+        ("scal_horiz_adv_order", C.c_int),
+        ("ithil_monot", C.c_int), ("iwind_monot", C.c_int), ("iscal_monot", C.c_int),
+        ("divh_damp_fact", C.c_float), ("divh_damp_level", C.c_int), ("divh_damp_short", C.c_int),
+        ("vort_damp_fact", C.c_float), ("vort_damp_level", C.c_int), ("vort_damp_short", C.c_int),
+        ("fcoriol", C.c_float), ("mdomain", C.c_int),
+        ("krayf_bot", C.c_int), ("rayf_cof", c_float_p), ("dn01d", c_float_p),
+        ("th01d", c_float_p), ("vc03d", c_float_p),
+        ("krayfw_bot", C.c_int), ("rayf_cofw", c_float_p), ("initial", C.c_int),
+    ]
+
+
+class State(C.Structure):
+    _fields_ = [
+        ("rho", c_double_p), ("press", c_double_p),
+        ("thil", c_float_p), ("wc", c_float_p), ("wmc", c_float_p),
+        ("vxe", c_float_p), ("vye", c_float_p), ("vze", c_float_p),
+        ("vmc", c_float_p), ("vc", c_float_p), ("vmasc", c_float_p), ("wmasc", c_float_p),
+        ("alpha_press", c_float_p), ("pwfac", c_float_p), ("pvfac", c_float_p),
+        ("thilt", c_float_p), ("vmxet", c_float_p), ("vmyet", c_float_p), ("vmzet", c_float_p),
+        ("vmt", c_float_p),
+    ]
+
+
+class CflDiag(C.Structure):
+    _fields_ = [
+        ("cfl_max", C.c_float), ("cfl_k", C.c_int), ("cfl_iwglobe", C.c_int),
+        ("cflh_max", C.c_float), ("cflh_k", C.c_int), ("cflh_iwglobe", C.c_int),
+        ("w_max", C.c_float), ("w_k", C.c_int), ("w_iwglobe", C.c_int),
+    ]
+
+
+def ptr(a, ctype):
+    """Pointer to a contiguous numpy array (None stays NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be contiguous"
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class FortranGrid:
+    """Fortran-layout copy of a synth Grid plus the ctypes struct over it.
+
+    Keeps every array alive for as long as the struct is used.
+    """
+
+    def __init__(self, g):
+        self.g = g
+        keep = {}
+
+        def i32(a, plus1=False):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            if plus1:
+                a = a + 1          # 0-based array index -> OLAM's 1-based index
+            keep[id(a)] = a
+            return a
+
+        def f32(a):
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            keep[id(a)] = a
+            return a
+
+        def f64(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep[id(a)] = a
+            return a
+
+        s = Grid()
+        s.mza, s.mwa, s.mva, s.mma = g.mza, g.mwa, g.mva, g.mma
+        # global domain: every real point is prognostic and adjacent
+        self.jtw = i32(np.arange(2, g.mwa + 1))
+        self.jtv = i32(np.arange(2, g.mva + 1))
+        self.jtm = i32(np.arange(2, g.mma + 1))
+        s.nw_prog = s.nw_wadj = g.mwa - 1
+        s.nv_prog = s.nv_wadj = g.mva - 1
+        s.nm_prog = g.mma - 1
+        s.jtw_prog = s.jtw_wadj = ptr(self.jtw, C.c_int)
+        s.jtv_prog = s.jtv_wadj = ptr(self.jtv, C.c_int)
+        s.jtm_prog = ptr(self.jtm, C.c_int)
+
+        def tab(a):
+            # tables hold 0-based array indices where 0 = dummy; entries past
+            # npoly are 0 -> OLAM's 1 (the dummy point), as Fortran leaves them
+            return i32(a, plus1=True)
+
+        s.npoly = ptr(i32(g.npoly), C.c_int)
+        s.itab_w_iv = ptr(tab(g.itab_w_iv), C.c_int)
+        s.itab_w_iw = ptr(tab(g.itab_w_iw), C.c_int)
+        s.itab_w_im = ptr(tab(g.itab_w_im), C.c_int)
+        s.itab_w_dirv = ptr(f32(g.dirv), C.c_float)
+        s.ecvec_vx = ptr(f32(g.ecvec_vx), C.c_float)
+        s.ecvec_vy = ptr(f32(g.ecvec_vy), C.c_float)
+        s.ecvec_vz = ptr(f32(g.ecvec_vz), C.c_float)
+        s.iwglobe = ptr(i32(g.iwglobe), C.c_int)
+        s.itab_v_iw = ptr(tab(g.itab_v_iw), C.c_int)
+        s.itab_v_im = ptr(tab(g.itab_v_im), C.c_int)
+        s.dxps = ptr(f32(g.dxps), C.c_float)
+        s.dyps = ptr(f32(g.dyps), C.c_float)
+        s.itab_m_iv = ptr(tab(g.itab_m_iv), C.c_int)
+        s.itab_m_iw = ptr(tab(g.itab_m_iw), C.c_int)
+        s.itab_m_im = ptr(tab(g.itab_m_im), C.c_int)
+        s.lpw = ptr(i32(g.lpw), C.c_int)
+        s.lpv = ptr(i32(g.lpv), C.c_int)
+        s.lpm = ptr(i32(g.lpm), C.c_int)
+        s.lve2 = ptr(i32(g.lve2), C.c_int)
+        for name in ("zm", "zt", "dzm", "dzt", "dzim", "dzit", "dzt_top", "dzt_bot", "zfacit",
+                     "gdz_wgtm", "gdz_wgtp", "wnx", "wny", "wnz", "wnxo2", "wnyo2", "wnzo2",
+                     "vnx", "vny", "vnz", "dnu", "dniu", "dnv", "dniv", "arw0", "arm0",
+                     "arv", "arw", "volti", "volwi", "volvi", "gxps_coef", "gyps_coef",
+                     "xy_h", "xy_hu", "xx0_v", "xy0_v", "yy0_v", "xx0_vu", "xy0_vu", "yy0_vu",
+                     "xx_yy", "xx_yy_m"):
+            setattr(s, name, ptr(f32(getattr(g, name)), C.c_float))
+        for name in ("zwgt_top8", "zwgt_bot8", "gdz_wgtm8", "gdz_wgtp8", "volt"):
+            setattr(s, name, ptr(f64(getattr(g, name)), C.c_double))
+        # a_w is Fortran (mza,2,2); the synth array is [i][j][k] -> [j][i][k]
+        s.a_w = ptr(f32(np.transpose(g.a_w, (1, 0, 2))), C.c_float)
+        s.a_wu = ptr(f32(np.transpose(g.a_wu, (1, 0, 2))), C.c_float)
+        self.struct = s
+        self._keep = keep
+
+
+def make_opts(dtlm, nacoust=1, nrk_scal=2, nrk_wrtv=3, scal_order=2, thil_order=2,
+              wind_order=2, iscal_monot=0, ithil_monot=0, iwind_monot=0,
+              divh_damp_fact=0.1, divh_damp_level=3, divh_damp_short=1,
+              vort_damp_fact=0.075, vort_damp_level=3, vort_damp_short=1,
+              omega=7.29212e-5):
+    o = Opts()
+    o.dtlm = float(dtlm)
+    o.nacoust = int(nacoust)
+    o.dtsm = float(dtlm) / float(np.float32(nacoust))
+    o.nrk_wrtv, o.nrk_scal = nrk_wrtv, nrk_scal
+    o.thil_horiz_adv_order, o.wind_horiz_adv_order = thil_order, wind_order
+    o.scal_horiz_adv_order = scal_order
+    o.ithil_monot, o.iwind_monot, o.iscal_monot = ithil_monot, iwind_monot, iscal_monot
+    o.divh_damp_fact, o.divh_damp_level, o.divh_damp_short = divh_damp_fact, divh_damp_level, divh_damp_short
+    o.vort_damp_fact, o.vort_damp_level, o.vort_damp_short = vort_damp_fact, vort_damp_level, vort_damp_short
+    o.fcoriol = np.float32(2.0 * omega)
+    o.mdomain = 0
+    o.krayf_bot = 10 ** 6
+    o.krayfw_bot = 10 ** 6
+    o.initial = 1
+    return o
+
+
+def ptr_array(arrays, ctype):
+    """C array of pointers to the given numpy arrays."""
+    arr_t = C.POINTER(ctype) * len(arrays)
+    return arr_t(*[ptr(a, ctype) for a in arrays])
