@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark of OLAM's scalar_transport_rk hot path on B200.
+
+Workload (the batched-tracer configuration): global icosahedral hexagonal
+grid NXP=200 (400,002 columns), 60 levels (mza = 61), 128 FP32 tracers with
+seeded lognormal mixing ratios clipped to [1e-12, 1e-6] (10 % of them zero
+above 15 km), winds and density of a balanced 35 m/s mid-latitude jet, 120 s
+long step, RK2 (OLAM's default scalar_timestep_level), second-order
+horizontal / third-order vertical reconstruction.  Data are synthetic: seeded
+fields with the shapes and value ranges of that configuration.
+
+One step = one scalar_transport_rk(rho_old) call (CFL check, RK densities,
+implicit factorisation, both RK stages for every tracer).  Metric: tracer
+cell-updates/s = tracers x prognostic (k, iw) cells / step time.
+
+  value  device-resident: inputs already in HBM, CUDA events on the
+         library stream around K steps (inputs, 12.5 GB of tracers, exceed L2)
+  e2e    through the C-ABI with OLAM-style host arrays: every step uploads
+         tracers, tendencies, winds and densities and downloads the tracers
+  plain  the one-kernel-per-pass-per-tracer GPU form on the same data
+  cpu_baseline  the C++ oracle (restatement of the reference loops), OpenMP on
+         all host cores, on a bounded sample of the same workload
+
+--impl reference runs the CPU restatement as the reference arm (the
+reference itself is Fortran and cannot be built here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nxp", type=int, default=200)
+    p.add_argument("--nlev", type=int, default=60)
+    p.add_argument("--ntr", type=int, default=128)
+    p.add_argument("--dt", type=float, default=120.0)
+    p.add_argument("--nrk", type=int, default=2)
+    p.add_argument("--order", type=int, default=2)
+    p.add_argument("--monot", type=int, default=0)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_case(a):
+    from olam_b200.synth.grid import build_grid, stretched_levels
+    from olam_b200.synth.state import fast_lognormal_tracers, transport_state
+    g = build_grid(a.nxp, stretched_levels(a.nlev, 100.0, 30000.0), seed=2)
+    st = transport_state(g, a.dt, 0, seed=2)
+    tr = fast_lognormal_tracers(g, a.ntr, seed=2024, as_list=True)
+    return g, st, tr
+
+
+def cell_updates(g, ntr):
+    # prognostic cells: levels lpw..mza of every W column (lpw = 2 here)
+    return ntr * (g.mwa - 1) * (g.mza - 1)
+
+
+def bytes_per_launch(g, ntr, stage):
+    """Algorithmic HBM bytes of one fused stage launch: per tracer and cell
+    12 B on stage 1 (read scp0 and sct, write) and 16 B on later stages (read
+    scp, scp0, sct, write), plus 32 B per cell of shared winds, densities and
+    volumes (vmasc 3 faces x 4, wmasc 4, rho 8, rho_old 4, volti 4)."""
+    cells = (g.mwa - 1) * (g.mza - 1)
+    per_tr = 12 if stage == 1 else 16
+    return cells * (ntr * per_tr + 32)
+
+
+def cpu_sample(g, st, tr, a, target_s, ntr_fixed=None):
+    """Time the oracle on a bounded tracer sample of the same workload.
+
+    The sample is the first n tracers for one long step, n chosen from a
+    one-tracer calibration so the timed run takes about ``target_s``."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    from olam_b200 import abi
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
+
+    class S:
+        pass
+    s = S()
+    s.__dict__.update(st.__dict__)
+
+    def run(n):
+        sct = [np.zeros_like(tr[0]) for _ in range(n)]
+        t0 = time.perf_counter()
+        oracle_lib.scalar_transport(fg, opts, tr[:n], sct, s)
+        return time.perf_counter() - t0
+
+    if ntr_fixed is None:
+        t1 = run(1)
+        n = int(max(1, min(a.ntr, round(target_s / max(t1, 1e-3)))))
+        t = run(n) if n > 1 else t1
+    else:
+        n = ntr_fixed
+        t = run(n)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": cell_updates(g, n) / t, "unit": "cell-updates/s", "cores": cores,
+            "kind": "port", "seconds": t, "ntr": n,
+            "sample": f"{n} of {a.ntr} tracers, one long step, NXP={a.nxp}, {a.nlev} levels"}
+
+
+def dist_init(a):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return ws, rank, local, dist
+    return 1, 0, 0, None
+
+
+def run_reference(a):
+    ws, rank, local, dist = 1, int(os.environ.get("RANK", "0")), 0, None
+    if rank != 0:
+        return 0
+    g, st, tr = make_case(a)
+    # each step is a bounded sample; the whole run stays within a few minutes
+    per_step = max(2.0, min(a.cpu_seconds, 150.0 / max(1, a.warmup + a.steps)))
+    res = cpu_sample(g, st, tr, a, per_step)
+    times = []
+    for i in range(a.warmup + a.steps):
+        r = cpu_sample(g, st, tr, a, per_step, ntr_fixed=res["ntr"])
+        if i >= a.warmup:
+            times.append(r["value"])
+    v = float(np.median(times)) if times else res["value"]
+    line = {"metric": "tracer cell-updates/s", "value": v, "unit": "cell-updates/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "impl": "reference",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"scalar_transport_rk NXP={a.nxp} {a.nlev} levels {a.ntr} "
+                                   f"tracers RK{a.nrk} order {a.order}"},
+            "cpu_baseline": {"kind": res["kind"], "cores": res["cores"], "sample": res["sample"],
+                             "value": v, "unit": "cell-updates/s"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    ws, rank, local, dist = dist_init(a)
+    import torch
+    from olam_b200 import abi
+    from olam_b200.lib import HostState, OlamGpu
+
+    torch.cuda.set_device(local)
+    g, st, tr = make_case(a)
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
+    hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)
+    dev = OlamGpu(fg, opts, hs)
+    var_p = tr                     # separately allocated, as OLAM's var_p
+    var_t = [np.zeros_like(tr[0]) for _ in range(a.ntr)]
+    dev.register_scalars(var_p, var_t)
+    stream = torch.cuda.ExternalStream(dev.stream())
+    nupd = cell_updates(g, a.ntr)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident fused form
+    dev.set_transport_form(abi.TRANSPORT_FUSED)
+    dev.set_coherence(abi.RESIDENT)
+    dev.sync_to_device(abi.F_ALL)
+    dev.scalar_transport_rk(st.rho_old)          # uploads rho_old once
+    for _ in range(a.warmup):
+        dev.scalar_transport_rk(None)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    dev.profile(True, reset=True)
+    dev.launch_count(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        dev.scalar_transport_rk(None)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = dev.launch_count()
+    prof = dev.profile_read()
+    dev.profile(False, reset=True)
+    clk = clocks.stop()
+    barrier()
+    torch.cuda.synchronize()
+    ms_step = max_over_ranks(ms / a.steps)
+    value = ws * nupd / (ms_step * 1e-3)
+
+    # roofline of the dominant kernel (fused stage launches)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = float(peak or 6650.0)
+    tot_bytes, tot_ms = 0.0, 0.0
+    for name, stage in (("fused_stage1", 1), ("fused_stage", 2)):
+        if name in prof:
+            m, c = prof[name]
+            tot_ms += m
+            tot_bytes += c * bytes_per_launch(g, a.ntr, stage)
+    nl = sum(c for nm, (m, c) in prof.items() if nm.startswith("fused"))
+    achieved = (tot_bytes / nl) / ((tot_ms / nl) * 1e-3) / 1e9 if nl else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "fused_stage_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get("dram_bytes_per_launch_full_size")
+        except (OSError, ValueError):
+            traffic = None
+
+    # ---- plain one-kernel-per-tracer form on the same device data
+    plain = None
+    if not a.no_plain:
+        dev.set_transport_form(abi.TRANSPORT_PLAIN)
+        dev.scalar_transport_rk(None)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        ksteps = max(1, min(a.steps, 3))
+        p0.record(stream)
+        for _ in range(ksteps):
+            dev.scalar_transport_rk(None)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = max_over_ranks(p0.elapsed_time(p1) / ksteps)
+        plain = ws * nupd / (pms * 1e-3)
+        dev.set_transport_form(abi.TRANSPORT_FUSED)
+
+    # ---- end to end through the C-ABI with host arrays
+    dev.sync_to_host(abi.F_SCALARS)
+    dev.set_coherence(abi.SYNC_EACH_CALL)
+    dev.scalar_transport_rk(st.rho_old)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(a.e2e_steps):
+        dev.scalar_transport_rk(st.rho_old)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / a.e2e_steps)
+    plane = g.mwa * g.mza * 4
+    h2d = a.ntr * 2 * plane + g.mva * g.mza * 4 + plane * 2 + g.mwa * g.mza * 8 + plane
+    d2h = a.ntr * plane
+    e2e = {"value": ws * nupd / e2e_s, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_s}
+    dev.close()
+
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        cpu = cpu_sample(g, st, tr, a, a.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"scalar_transport_rk NXP={a.nxp} ({g.mwa - 1} columns), "
+                                   f"{a.nlev} levels, {a.ntr} tracers, RK{a.nrk}, "
+                                   f"horiz order {a.order}, iscal_monot {a.monot}, dt {a.dt} s",
+                       "form": "fused batched", "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (12.5 GB of tracers per array)"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "peak_source": peak_src, "kernel": "k_fused (fused_stage)",
+                         "kernel_ms_per_launch": (tot_ms / nl) if nl else None},
+            "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+            "plain_gpu_value": plain,
+            "fused_over_plain": (value / plain) if plain else None,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

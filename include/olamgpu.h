@@ -232,6 +232,16 @@ void* olamgpu_stream(void);
 /* Number of library kernel launches issued since the last reset. */
 unsigned long long olamgpu_launch_count(int reset);
 
+/* Per-kernel device timing (the tracing facility; OLAM itself only prints
+ * per-step wall time, omodel/olam_run.f90:990-1032).  While enabled, every
+ * library launch is bracketed by CUDA events on the library stream.
+ * olamgpu_profile_read synchronises the stream, then fills up to max entries:
+ * names (32 bytes each, NUL-terminated), accumulated milliseconds and launch
+ * counts; it returns the number of kernels seen, or a negative status. */
+int olamgpu_profile(int enable, int reset);
+int olamgpu_profile_read(int max, char* names, double* total_ms,
+                         unsigned long long* counts);
+
 #ifdef __cplusplus
 }
 #endif

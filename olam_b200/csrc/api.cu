@@ -1,0 +1,368 @@
+// api.cu -- the extern "C" entry points declared in include/olamgpu.h.
+//
+// One library context per process (OLAM calls from its master thread,
+// outside OpenMP regions, omodel/timestep.f90:205,254); every call returns a
+// status code and never falls back to the CPU.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "transport_kernels.cuh"
+
+namespace olamgpu {
+
+unsigned long long g_launches = 0;
+
+// ---- per-kernel event timing ----------------------------------------------
+struct ProfRec { std::string name; cudaEvent_t a, b; };
+static bool g_prof_on = false;
+static std::vector<ProfRec> g_prof_pending;
+static std::vector<cudaEvent_t> g_prof_pool;
+static std::vector<std::string> g_prof_names;
+static std::vector<double> g_prof_ms;
+static std::vector<unsigned long long> g_prof_cnt;
+static std::string g_prof_open;
+static cudaEvent_t g_prof_open_ev = nullptr;
+
+static cudaEvent_t prof_event() {
+  if (!g_prof_pool.empty()) { cudaEvent_t e = g_prof_pool.back(); g_prof_pool.pop_back(); return e; }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_begin(const char* name, cudaStream_t s) {
+  if (!g_prof_on) return;
+  g_prof_open = name;
+  g_prof_open_ev = prof_event();
+  cudaEventRecord(g_prof_open_ev, s);
+}
+
+void prof_end(cudaStream_t s) {
+  if (!g_prof_on || !g_prof_open_ev) return;
+  cudaEvent_t b = prof_event();
+  cudaEventRecord(b, s);
+  g_prof_pending.push_back({g_prof_open, g_prof_open_ev, b});
+  g_prof_open_ev = nullptr;
+}
+
+static void prof_resolve() {
+  for (auto& r : g_prof_pending) {
+    float ms = 0.f;
+    cudaEventSynchronize(r.b);
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    size_t i = 0;
+    while (i < g_prof_names.size() && g_prof_names[i] != r.name) ++i;
+    if (i == g_prof_names.size()) { g_prof_names.push_back(r.name); g_prof_ms.push_back(0); g_prof_cnt.push_back(0); }
+    g_prof_ms[i] += ms;
+    g_prof_cnt[i] += 1;
+    g_prof_pool.push_back(r.a);
+    g_prof_pool.push_back(r.b);
+  }
+  g_prof_pending.clear();
+}
+
+static std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+const std::string& last_error() { return g_err; }
+
+Context& ctx() {
+  static Context c;
+  return c;
+}
+
+static int require_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error(std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count 0"));
+    return OLAMGPU_E_NODEVICE;
+  }
+  int dev = 0;
+  OG_CUDA(cudaGetDevice(&dev));
+  cudaDeviceProp p;
+  OG_CUDA(cudaGetDeviceProperties(&p, dev));
+  if (p.major < 10) {
+    set_error(std::string("device ") + p.name + " is not sm_100 class; this library is built for sm_100a");
+    return OLAMGPU_E_NODEVICE;
+  }
+  ctx().device = dev;
+  return OLAMGPU_OK;
+}
+
+static void release_all() {
+  Context& C = ctx();
+  DevGrid& d = C.g;
+  DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
+                       &d.w_nb, &d.w_ev, &d.w_im, &d.v_iw, &d.v_im, &d.m_iv, &d.m_iw, &d.m_im,
+                       &d.lpw, &d.lpv, &d.lpm, &d.iwglobe};
+  for (auto* b : ib) b->release();
+  DevBuf<float>* fb[] = {&d.w_dirv, &d.gxc, &d.gyc, &d.xy_h, &d.xy_hu, &d.dxps, &d.dyps, &d.xx0_v,
+                         &d.xy0_v, &d.yy0_v, &d.xx0_vu, &d.xy0_vu, &d.yy0_vu, &d.a_w, &d.a_wu,
+                         &d.volti, &d.ew_b, &d.ew_u};
+  for (auto* b : fb) b->release();
+  d.ew_order = 0;
+  Tracers& tr = C.tr;
+  for (size_t i = 0; i < tr.p.size(); ++i) {
+    tr.p[i].release();
+    tr.t[i].release();
+    if (i < tr.pinned.size() && tr.pinned[i]) {
+      cudaHostUnregister(tr.h_p[i]);
+      cudaHostUnregister(tr.h_t[i]);
+    }
+  }
+  for (auto& b : tr.q) b.release();
+  tr.qt.release();
+  tr.d_pdef.release();
+  tr = Tracers();
+  Transport& tp = C.tp;
+  DevBuf<float>* tb[] = {&tp.vmasc, &tp.wmasc, &tp.rho_old, &tp.wc, &tp.rhos, &tp.ff, &tp.imp_b,
+                         &tp.cfl_red, &tp.gx, &tp.upv, &tp.hiv, &tp.sfv, &tp.scale, &tp.upw,
+                         &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx};
+  for (auto* b : tb) b->release();
+  tp.rho.release();
+  tp.imp_list.release();
+  tp.imp_count.release();
+  tp.cfl_loc.release();
+  tp.d_mode.release();
+  tp.khtopv.release();
+  tp.have_turb = false;
+  C.status.release();
+}
+
+}  // namespace olamgpu
+
+using namespace olamgpu;
+
+extern "C" {
+
+const char* olamgpu_strerror(int status) {
+  static std::string msg;
+  const char* base = "unknown status";
+  switch (status) {
+    case OLAMGPU_OK: return "ok";
+    case OLAMGPU_E_ARG: base = "invalid argument"; break;
+    case OLAMGPU_E_STATE: base = "call out of order"; break;
+    case OLAMGPU_E_UNSUPPORTED: base = "unsupported option"; break;
+    case OLAMGPU_E_CUDA: base = "CUDA error"; break;
+    case OLAMGPU_E_NOMEM: base = "device out of memory"; break;
+    case OLAMGPU_E_NODEVICE: base = "no usable GPU"; break;
+    case OLAMGPU_E_NUMERIC: base = "device status reported a failure"; break;
+  }
+  msg = std::string(base) + (last_error().empty() ? "" : ": " + last_error());
+  return msg.c_str();
+}
+
+int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts, const olamgpu_state* state) {
+  if (!grid || !opts) { set_error("grid or opts is NULL"); return OLAMGPU_E_ARG; }
+  Context& C = ctx();
+  if (C.initialised) { set_error("olamgpu_init called twice without olamgpu_finalize"); return OLAMGPU_E_STATE; }
+  if (opts->mdomain != 0) { set_error("only the global domain (mdomain = 0) is supported"); return OLAMGPU_E_UNSUPPORTED; }
+  if (grid->mza > 512) { set_error("mza > 512 is not supported"); return OLAMGPU_E_UNSUPPORTED; }
+  OG_CHECK(require_device());
+  if (!C.stream) OG_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+  int rc = upload_grid(grid, C.g, C.stream);
+  if (rc != OLAMGPU_OK) { release_all(); return rc; }
+  C.hgrid = *grid;
+  C.opts = *opts;
+  C.tp.flat = true;
+  for (int i = 1; i < grid->mwa; ++i) if (grid->lpw[i] != 2) C.tp.flat = false;
+  for (int i = 1; i < grid->mva; ++i) if (grid->lpv[i] != 2) C.tp.flat = false;
+  int order = opts->scal_horiz_adv_order;
+  if (order == 2 || order == 3) {
+    rc = build_fused_weights(grid, C.g, order, C.stream);
+    if (rc != OLAMGPU_OK) { release_all(); return rc; }
+  }
+  if (state) { C.hstate = *state; C.have_state = true; } else C.have_state = false;
+  rc = C.status.alloc(16);
+  if (rc != OLAMGPU_OK) { release_all(); return rc; }
+  cudaMemsetAsync(C.status.p, 0, 16 * sizeof(int), C.stream);
+  OG_CUDA(cudaStreamSynchronize(C.stream));
+  C.initialised = true;
+  return OLAMGPU_OK;
+}
+
+int olamgpu_register_scalars(int num_scalar, float* const* var_p, float* const* var_t, const int* pdef,
+                             const int* do_sgsmix) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (num_scalar < 0 || (num_scalar > 0 && (!var_p || !var_t))) { set_error("bad scalar table"); return OLAMGPU_E_ARG; }
+  for (int n = 0; n < num_scalar; ++n)
+    if (!var_p[n] || !var_t[n]) { set_error("NULL var_p/var_t for scalar " + std::to_string(n + 1)); return OLAMGPU_E_ARG; }
+  Tracers& tr = C.tr;
+  // drop a previous registration
+  for (size_t i = 0; i < tr.p.size(); ++i) {
+    tr.p[i].release(); tr.t[i].release();
+    if (i < tr.pinned.size() && tr.pinned[i]) { cudaHostUnregister(tr.h_p[i]); cudaHostUnregister(tr.h_t[i]); }
+  }
+  for (auto& b : tr.q) b.release();
+  tr.qt.release();
+  tr = Tracers();
+  tr.n = num_scalar;
+  tr.ntp = ((num_scalar + 3) / 4) * 4;
+  const size_t plane = (size_t)C.g.mza * C.g.mwa;
+  tr.h_p.assign(var_p, var_p + num_scalar);
+  tr.h_t.assign(var_t, var_t + num_scalar);
+  tr.pdef.resize(num_scalar);
+  tr.sgsmix.resize(num_scalar);
+  tr.pinned.assign(num_scalar, 0);
+  tr.p.resize(num_scalar);
+  tr.t.resize(num_scalar);
+  for (int n = 0; n < num_scalar; ++n) {
+    tr.pdef[n] = pdef ? (pdef[n] != 0) : 0;
+    tr.sgsmix[n] = do_sgsmix ? (do_sgsmix[n] != 0) : 0;
+    OG_CHECK(tr.p[n].alloc(plane));
+    OG_CHECK(tr.t[n].alloc(plane));
+    // page-lock OLAM's arrays in place; failure only costs transfer speed
+    if (cudaHostRegister(tr.h_p[n], plane * sizeof(float), cudaHostRegisterDefault) == cudaSuccess) {
+      if (cudaHostRegister(tr.h_t[n], plane * sizeof(float), cudaHostRegisterDefault) == cudaSuccess)
+        tr.pinned[n] = 1;
+      else
+        cudaHostUnregister(tr.h_p[n]);
+    }
+    cudaGetLastError();
+  }
+  // initial device copy
+  OG_CHECK(tracers_to_device(C.stream));
+  OG_CUDA(cudaStreamSynchronize(C.stream));
+  return OLAMGPU_OK;
+}
+
+int olamgpu_set_turb(const float* akhodx, const int* khtopv) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (!akhodx || !khtopv) { C.tp.have_turb = false; return OLAMGPU_OK; }
+  OG_CHECK(upload(C.tp.akhodx, akhodx, (size_t)C.g.mza * C.g.mva, C.stream));
+  OG_CHECK(upload(C.tp.khtopv, khtopv, (size_t)C.g.mva, C.stream));
+  OG_CUDA(cudaStreamSynchronize(C.stream));
+  C.tp.have_turb = true;
+  return OLAMGPU_OK;
+}
+
+int olamgpu_finalize(void) {
+  Context& C = ctx();
+  if (C.stream) cudaStreamSynchronize(C.stream);
+  release_all();
+  C.initialised = false;
+  C.have_state = false;
+  if (C.stream) { cudaStreamDestroy(C.stream); C.stream = nullptr; }
+  return OLAMGPU_OK;
+}
+
+int olamgpu_set_coherence(int mode) {
+  if (mode != OLAMGPU_SYNC_EACH_CALL && mode != OLAMGPU_RESIDENT) { set_error("unknown coherence mode"); return OLAMGPU_E_ARG; }
+  ctx().coherence = mode;
+  return OLAMGPU_OK;
+}
+
+int olamgpu_set_transport_form(int form) {
+  if (form != OLAMGPU_TRANSPORT_FUSED && form != OLAMGPU_TRANSPORT_PLAIN) { set_error("unknown transport form"); return OLAMGPU_E_ARG; }
+  Context& C = ctx();
+  if (C.initialised && C.form != form) {
+    // keep the newest tracer values in the per-tracer mirrors across a switch
+    OG_CHECK(ensure_plain(C.stream));
+  }
+  C.form = form;
+  return OLAMGPU_OK;
+}
+
+int olamgpu_sync_to_device(unsigned fieldmask) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  cudaStream_t s = C.stream;
+  const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva;
+  if (fieldmask & (OLAMGPU_F_SCALARS | OLAMGPU_F_SCALAR_TEND)) {
+    OG_CHECK(ensure_plain(s));
+    for (int n = 0; n < C.tr.n; ++n) {
+      if (fieldmask & OLAMGPU_F_SCALARS)
+        OG_CUDA(cudaMemcpyAsync(C.tr.p[n].p, C.tr.h_p[n], wz * 4, cudaMemcpyHostToDevice, s));
+      if (fieldmask & OLAMGPU_F_SCALAR_TEND)
+        OG_CUDA(cudaMemcpyAsync(C.tr.t[n].p, C.tr.h_t[n], wz * 4, cudaMemcpyHostToDevice, s));
+    }
+  }
+  if (C.have_state) {
+    if ((fieldmask & OLAMGPU_F_VMASC) && C.hstate.vmasc) OG_CHECK(upload(C.tp.vmasc, C.hstate.vmasc, vz, s));
+    if ((fieldmask & OLAMGPU_F_WMASC) && C.hstate.wmasc) OG_CHECK(upload(C.tp.wmasc, C.hstate.wmasc, wz, s));
+    if ((fieldmask & OLAMGPU_F_RHO) && C.hstate.rho) OG_CHECK(upload(C.tp.rho, C.hstate.rho, wz, s));
+    if ((fieldmask & OLAMGPU_F_WC) && C.hstate.wc) OG_CHECK(upload(C.tp.wc, C.hstate.wc, wz, s));
+  }
+  OG_CUDA(cudaStreamSynchronize(s));
+  return OLAMGPU_OK;
+}
+
+int olamgpu_sync_to_host(unsigned fieldmask) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  cudaStream_t s = C.stream;
+  if (fieldmask & (OLAMGPU_F_SCALARS | OLAMGPU_F_SCALAR_TEND)) {
+    OG_CHECK(ensure_plain(s));
+    const size_t wz = (size_t)C.g.mza * C.g.mwa;
+    for (int n = 0; n < C.tr.n; ++n) {
+      if (fieldmask & OLAMGPU_F_SCALARS)
+        OG_CUDA(cudaMemcpyAsync(C.tr.h_p[n], C.tr.p[n].p, wz * 4, cudaMemcpyDeviceToHost, s));
+      if (fieldmask & OLAMGPU_F_SCALAR_TEND)
+        OG_CUDA(cudaMemcpyAsync(C.tr.h_t[n], C.tr.t[n].p, wz * 4, cudaMemcpyDeviceToHost, s));
+    }
+  }
+  OG_CUDA(cudaStreamSynchronize(s));
+  return OLAMGPU_OK;
+}
+
+int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag) {
+  int rc = transport_run(rho_old, diag);
+  if (rc == OLAMGPU_OK) {
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) { set_error(std::string("kernel launch: ") + cudaGetErrorString(e)); return OLAMGPU_E_CUDA; }
+  }
+  return rc;
+}
+
+int olamgpu_prog_wrtv_rk(int istp) {
+  (void)istp;
+  set_error("prog_wrtv_rk is not available in this build");
+  return OLAMGPU_E_UNSUPPORTED;
+}
+
+int olamgpu_tend0(float* rho_old) {
+  (void)rho_old;
+  set_error("tend0 is not available in this build");
+  return OLAMGPU_E_UNSUPPORTED;
+}
+
+int olamgpu_timeavg_momsc(void) {
+  set_error("timeavg_momsc is not available in this build");
+  return OLAMGPU_E_UNSUPPORTED;
+}
+
+void* olamgpu_stream(void) { return (void*)ctx().stream; }
+
+int olamgpu_profile(int enable, int reset) {
+  prof_resolve();
+  if (reset) { g_prof_names.clear(); g_prof_ms.clear(); g_prof_cnt.clear(); }
+  g_prof_on = enable != 0;
+  return OLAMGPU_OK;
+}
+
+int olamgpu_profile_read(int max, char* names, double* total_ms, unsigned long long* counts) {
+  Context& C = ctx();
+  if (C.stream) cudaStreamSynchronize(C.stream);
+  prof_resolve();
+  int n = (int)g_prof_names.size();
+  for (int i = 0; i < n && i < max; ++i) {
+    if (names) {
+      std::memset(names + 32 * i, 0, 32);
+      std::strncpy(names + 32 * i, g_prof_names[i].c_str(), 31);
+    }
+    if (total_ms) total_ms[i] = g_prof_ms[i];
+    if (counts) counts[i] = g_prof_cnt[i];
+  }
+  return n;
+}
+
+unsigned long long olamgpu_launch_count(int reset) {
+  unsigned long long v = g_launches;
+  if (reset) g_launches = 0;
+  return v;
+}
+
+}  // extern "C"

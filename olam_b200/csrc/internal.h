@@ -1,0 +1,197 @@
+// internal.h -- device data structures and helpers of libolamgpu.so.
+//
+// Device layout.  Grid and state arrays keep OLAM's Fortran layout
+// (mza, n) with k contiguous and OLAM's dummy point 1 at index 0, so a host
+// array is uploaded with one copy.  Neighbour tables are converted once to
+// 0-based indices and padded to 8 entries per W point.  Tracers have two
+// device layouts:
+//   * per-tracer (mza, mwa) arrays, the reference layout, used by the plain
+//     one-kernel-per-pass form and as the staging mirror of host arrays;
+//   * the batched layout Q[mwa][mza][ntp] (tracer index fastest, ntp = number
+//     of tracers padded to a multiple of 4), used by the fused kernels: the
+//     tracers of one (k, iw) cell form one contiguous row, so a warp gathers
+//     a neighbour cell for every tracer with one coalesced 16-byte-per-lane
+//     load, and every wind, density and table value loaded for that cell is
+//     reused across all tracers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/olamgpu.h"
+
+#define OLAMGPU_MAXNB 8  // padded neighbour count per W point (OLAM allows 7)
+
+namespace olamgpu {
+
+// ---- error handling ---------------------------------------------------------
+
+void set_error(const std::string& msg);
+const std::string& last_error();
+
+#define OG_CUDA(call)                                                        \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) {                                                 \
+      ::olamgpu::set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+      return (e_ == cudaErrorMemoryAllocation) ? OLAMGPU_E_NOMEM : OLAMGPU_E_CUDA; \
+    }                                                                        \
+  } while (0)
+
+#define OG_CHECK(rc_expr)             \
+  do {                                \
+    int rc_ = (rc_expr);              \
+    if (rc_ != OLAMGPU_OK) return rc_; \
+  } while (0)
+
+// counts kernel launches issued by the library (olamgpu_launch_count)
+extern unsigned long long g_launches;
+#define OG_LAUNCHED() (++::olamgpu::g_launches)
+
+// per-kernel event timing (olamgpu_profile); no-ops while disabled
+void prof_begin(const char* name, cudaStream_t s);
+void prof_end(cudaStream_t s);
+struct ProfScope {
+  cudaStream_t s;
+  ProfScope(const char* name, cudaStream_t st) : s(st) { prof_begin(name, st); }
+  ~ProfScope() { prof_end(s); }
+};
+#define OG_PROF(name, s) ::olamgpu::ProfScope og_prof_scope_(name, s)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (p && n == count) return OLAMGPU_OK;
+    release();
+    if (count == 0) return OLAMGPU_OK;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return OLAMGPU_E_NOMEM;
+    }
+    n = count;
+    return OLAMGPU_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---- device grid ------------------------------------------------------------
+
+struct DevGrid {
+  int mza = 0, mwa = 0, mva = 0, mma = 0;
+  int nw_prog = 0, nv_wadj = 0, nv_prog = 0, nw_wadj = 0, nm_prog = 0;
+  DevBuf<int> jtw_prog, jtv_wadj, jtv_prog, jtw_wadj, jtm_prog;  // 0-based
+  DevBuf<int> npoly;     // (mwa)
+  DevBuf<int> w_nb;      // (mwa, 8) 0-based W neighbours, padded with self
+  DevBuf<int> w_ev;      // (mwa, 8) 0-based V neighbours, padded with 0
+  DevBuf<int> w_im;      // (mwa, 8) 0-based M neighbours
+  DevBuf<float> w_dirv;  // (mwa, 8)
+  DevBuf<int> v_iw;      // (mva, 2) 0-based
+  DevBuf<int> v_im;      // (mva, 2) 0-based
+  DevBuf<int> m_iv, m_iw, m_im;  // (mma, 3) 0-based
+  DevBuf<int> lpw, lpv, lpm;     // 0-based lowest prognosed level
+  DevBuf<int> iwglobe;
+  // reconstruction coefficients (float, OLAM layouts)
+  DevBuf<float> gxc, gyc;        // (mwa, 7)
+  DevBuf<float> xy_h, xy_hu;     // (mwa, 7, 5)
+  DevBuf<float> dxps, dyps;      // (mva, 2)
+  DevBuf<float> xx0_v, xy0_v, yy0_v, xx0_vu, xy0_vu, yy0_vu;  // (mva, 2)
+  DevBuf<float> a_w, a_wu;       // Fortran (mza, 2, 2)
+  DevBuf<float> volti;           // (mwa, mza)
+  // fused-kernel stencil weights: for V face iv and side s the value
+  // reconstructed from cell c = iw(s) is
+  //   S(c) + sum_n ew[iv][s][n] * (S(w_nb[c][n]) - S(c))
+  // (order 2: dxps*gxps_coef + dyps*gyps_coef; order 3 folds the quadratic
+  //  terms xx0_v.. with xy_h the same way).  Bounded and unbounded sets.
+  DevBuf<float> ew_b, ew_u;      // (mva, 2, 8)
+  int ew_order = 0;
+  std::vector<int> h_lpw;        // host copies used at set-up
+};
+
+struct Tracers {
+  int n = 0, ntp = 0;            // count and padded count (multiple of 4)
+  std::vector<float*> h_p, h_t;  // registered host arrays
+  std::vector<int> pdef, sgsmix;
+  std::vector<int> pinned;       // 1 where cudaHostRegister succeeded
+  // per-tracer device mirrors (reference layout)
+  std::vector<DevBuf<float>> p, t, p_alt;
+  // batched layout and rotation buffers
+  DevBuf<float> q[3];            // Q layouts: q[cur] holds the tracers
+  DevBuf<float> qt;              // tendencies in Q layout
+  int qcur = 0;
+  bool q_valid = false;          // Q holds the newest values (else per-tracer p)
+  DevBuf<int> d_pdef;
+};
+
+struct Transport {
+  DevBuf<float> vmasc, wmasc, rho_old, wc;  // (mva|mwa, mza)
+  DevBuf<double> rho;
+  DevBuf<float> rhos;        // (nrk, mwa, mza)
+  DevBuf<float> ff;          // (mwa, nrk)
+  DevBuf<int> imp_list;      // (nrk, mwa): implicit columns per stage
+  DevBuf<int> imp_count;     // (nrk)
+  DevBuf<float> imp_b;       // (nrk, mwa, 3, mza): b1, scr1, cji per column slot
+  DevBuf<float> cfl_red;     // reduction scratch
+  DevBuf<unsigned long long> cfl_loc;
+  // scratch for the reference-mirroring passes
+  DevBuf<float> gx;          // gradient planes
+  DevBuf<float> upv, hiv, sfv;   // V-face arrays
+  DevBuf<float> scale, upw;      // W arrays for monot/pd
+  DevBuf<float> plain_out[2];    // per-tracer stage outputs of the plain form
+  DevBuf<int> d_mode;            // per-tracer last-stage mode
+  bool flat = true;              // lpw == lpv == 2 everywhere (fused form requirement)
+  DevBuf<float> akhodx;
+  DevBuf<int> khtopv;
+  bool have_turb = false;
+};
+
+struct Context {
+  bool initialised = false;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  olamgpu_opts opts{};
+  olamgpu_grid hgrid{};      // host pointers as given (valid while OLAM runs)
+  olamgpu_state hstate{};
+  bool have_state = false;
+  int coherence = OLAMGPU_SYNC_EACH_CALL;
+  int form = OLAMGPU_TRANSPORT_FUSED;
+  DevGrid g;
+  Tracers tr;
+  Transport tp;
+  DevBuf<int> status;        // device status word (bounds/NaN flags)
+};
+
+Context& ctx();
+
+// set-up helpers (setup.cu)
+int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s);
+int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
+
+// transport entry points (transport.cu)
+int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);
+int tracers_to_device(cudaStream_t s);   // host -> per-tracer mirrors (-> Q)
+int tracers_to_host(cudaStream_t s);     // (Q ->) per-tracer mirrors -> host
+int ensure_q(cudaStream_t s);            // per-tracer mirrors -> Q if needed
+int ensure_plain(cudaStream_t s);        // Q -> per-tracer mirrors if needed
+
+template <class T>
+int upload(DevBuf<T>& b, const T* h, size_t n, cudaStream_t s) {
+  OG_CHECK(b.alloc(n));
+  if (n) OG_CUDA(cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  return OLAMGPU_OK;
+}
+
+inline unsigned int cdiv(size_t a, size_t b) { return (unsigned int)((a + b - 1) / b); }
+
+}  // namespace olamgpu

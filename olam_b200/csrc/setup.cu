@@ -1,0 +1,209 @@
+// setup.cu -- grid upload and table packing (host side of init_wrtv_rk's
+// replacement).  OLAM's tables (mem_ijtabs.f90:60-144) arrive 1-based with
+// packed derived-type members; the device keeps 0-based, padded copies.
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+
+namespace olamgpu {
+
+static int check_index(const int* a, size_t n, int lo, int hi, const char* what) {
+  for (size_t i = 0; i < n; ++i)
+    if (a[i] < lo || a[i] > hi) {
+      set_error(std::string("grid table ") + what + " holds an index outside [" +
+                std::to_string(lo) + "," + std::to_string(hi) + "] at " + std::to_string(i));
+      return OLAMGPU_E_ARG;
+    }
+  return OLAMGPU_OK;
+}
+
+static int upload_list(DevBuf<int>& b, const int* h, int n, int maxv, const char* what,
+                       cudaStream_t s) {
+  if (n < 0 || (n > 0 && !h)) {
+    set_error(std::string("loop table ") + what + " missing");
+    return OLAMGPU_E_ARG;
+  }
+  OG_CHECK(check_index(h, (size_t)n, 2, maxv, what));
+  std::vector<int> v(n > 0 ? n : 1, 0);
+  for (int i = 0; i < n; ++i) v[i] = h[i] - 1;
+  OG_CHECK(b.alloc(v.size()));
+  OG_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  OG_CUDA(cudaStreamSynchronize(s));
+  return OLAMGPU_OK;
+}
+
+int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
+  const int mza = g->mza, mwa = g->mwa, mva = g->mva, mma = g->mma;
+  if (mza < 3 || mwa < 2 || mva < 2 || mma < 2) {
+    set_error("grid sizes mza/mwa/mva/mma out of range");
+    return OLAMGPU_E_ARG;
+  }
+  const void* need[] = {g->npoly, g->itab_w_iv, g->itab_w_iw, g->itab_w_dirv, g->itab_v_iw,
+                        g->lpw, g->lpv, g->volti, g->a_w, g->a_wu, g->dxps, g->dyps,
+                        g->gxps_coef, g->gyps_coef, g->xy_h, g->xy_hu, g->xx0_v, g->xy0_v,
+                        g->yy0_v, g->xx0_vu, g->xy0_vu, g->yy0_vu, g->dzt_top, g->dzt_bot,
+                        g->dzim};
+  for (const void* p : need)
+    if (!p) {
+      set_error("olamgpu_grid has a NULL array the transport path needs");
+      return OLAMGPU_E_ARG;
+    }
+  d.mza = mza; d.mwa = mwa; d.mva = mva; d.mma = mma;
+  d.nw_prog = g->nw_prog; d.nw_wadj = g->nw_wadj;
+  d.nv_prog = g->nv_prog; d.nv_wadj = g->nv_wadj; d.nm_prog = g->nm_prog;
+  OG_CHECK(upload_list(d.jtw_prog, g->jtw_prog, g->nw_prog, mwa, "jtw_prog", s));
+  OG_CHECK(upload_list(d.jtw_wadj, g->jtw_wadj, g->nw_wadj, mwa, "jtw_wadj", s));
+  OG_CHECK(upload_list(d.jtv_prog, g->jtv_prog, g->nv_prog, mva, "jtv_prog", s));
+  OG_CHECK(upload_list(d.jtv_wadj, g->jtv_wadj, g->nv_wadj, mva, "jtv_wadj", s));
+  if (g->jtm_prog && g->nm_prog > 0)
+    OG_CHECK(upload_list(d.jtm_prog, g->jtm_prog, g->nm_prog, mma, "jtm_prog", s));
+
+  // itab_w: npoly in [3,7]; indices checked for the first npoly entries
+  std::vector<int> npoly(mwa), nb((size_t)mwa * 8), ev((size_t)mwa * 8), im((size_t)mwa * 8, 0);
+  std::vector<float> dirv((size_t)mwa * 8, 0.f);
+  for (int iw = 0; iw < mwa; ++iw) {
+    int np = g->npoly[iw];
+    if (iw == 0) np = 0;  // dummy point
+    if (np < 0 || np > 7 || (iw > 0 && np < 3)) {
+      set_error("npoly out of range at W point " + std::to_string(iw + 1));
+      return OLAMGPU_E_ARG;
+    }
+    npoly[iw] = np;
+    for (int j = 0; j < 8; ++j) {
+      nb[(size_t)iw * 8 + j] = iw;
+      ev[(size_t)iw * 8 + j] = 0;
+    }
+    for (int j = 0; j < np; ++j) {
+      int wv = g->itab_w_iv[(size_t)iw * 7 + j], ww = g->itab_w_iw[(size_t)iw * 7 + j];
+      if (wv < 2 || wv > mva || ww < 2 || ww > mwa) {
+        set_error("itab_w neighbour index out of range at W point " + std::to_string(iw + 1));
+        return OLAMGPU_E_ARG;
+      }
+      ev[(size_t)iw * 8 + j] = wv - 1;
+      nb[(size_t)iw * 8 + j] = ww - 1;
+      dirv[(size_t)iw * 8 + j] = g->itab_w_dirv[(size_t)iw * 7 + j];
+      if (g->itab_w_im) im[(size_t)iw * 8 + j] = g->itab_w_im[(size_t)iw * 7 + j] - 1;
+    }
+  }
+  OG_CHECK(upload(d.npoly, npoly.data(), npoly.size(), s));
+  OG_CHECK(upload(d.w_nb, nb.data(), nb.size(), s));
+  OG_CHECK(upload(d.w_ev, ev.data(), ev.size(), s));
+  OG_CHECK(upload(d.w_im, im.data(), im.size(), s));
+  OG_CHECK(upload(d.w_dirv, dirv.data(), dirv.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));
+
+  std::vector<int> viw((size_t)mva * 2), vim((size_t)mva * 2, 0);
+  for (int iv = 0; iv < mva; ++iv)
+    for (int k = 0; k < 2; ++k) {
+      int w = g->itab_v_iw[(size_t)iv * 2 + k];
+      if (iv > 0 && (w < 1 || w > mwa)) {
+        set_error("itab_v%iw index out of range at V point " + std::to_string(iv + 1));
+        return OLAMGPU_E_ARG;
+      }
+      viw[(size_t)iv * 2 + k] = iv > 0 ? w - 1 : 0;
+      if (g->itab_v_im) vim[(size_t)iv * 2 + k] = iv > 0 ? g->itab_v_im[(size_t)iv * 2 + k] - 1 : 0;
+    }
+  OG_CHECK(upload(d.v_iw, viw.data(), viw.size(), s));
+  OG_CHECK(upload(d.v_im, vim.data(), vim.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));
+
+  if (g->itab_m_iv && g->itab_m_iw && g->itab_m_im) {
+    std::vector<int> miv((size_t)mma * 3), miw((size_t)mma * 3), mim((size_t)mma * 3);
+    for (size_t i = 0; i < (size_t)mma * 3; ++i) {
+      miv[i] = std::max(g->itab_m_iv[i] - 1, 0);
+      miw[i] = std::max(g->itab_m_iw[i] - 1, 0);
+      mim[i] = std::max(g->itab_m_im[i] - 1, 0);
+    }
+    OG_CHECK(upload(d.m_iv, miv.data(), miv.size(), s));
+    OG_CHECK(upload(d.m_iw, miw.data(), miw.size(), s));
+    OG_CHECK(upload(d.m_im, mim.data(), mim.size(), s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+
+  std::vector<int> lpw(mwa), lpv(mva);
+  for (int i = 0; i < mwa; ++i) {
+    int l = g->lpw[i];
+    if (i > 0 && (l < 2 || l > mza)) {
+      set_error("lpw out of range [2,mza] at W point " + std::to_string(i + 1));
+      return OLAMGPU_E_ARG;
+    }
+    lpw[i] = (i > 0 ? l : 2) - 1;
+  }
+  for (int i = 0; i < mva; ++i) {
+    int l = g->lpv[i];
+    if (i > 0 && (l < 2 || l > mza)) {
+      set_error("lpv out of range [2,mza] at V point " + std::to_string(i + 1));
+      return OLAMGPU_E_ARG;
+    }
+    lpv[i] = (i > 0 ? l : 2) - 1;
+  }
+  d.h_lpw = lpw;
+  OG_CHECK(upload(d.lpw, lpw.data(), lpw.size(), s));
+  OG_CHECK(upload(d.lpv, lpv.data(), lpv.size(), s));
+  if (g->lpm) {
+    std::vector<int> lpm(mma);
+    for (int i = 0; i < mma; ++i) lpm[i] = std::max(g->lpm[i] - 1, 1);
+    OG_CHECK(upload(d.lpm, lpm.data(), lpm.size(), s));
+  }
+  if (g->iwglobe) OG_CHECK(upload(d.iwglobe, g->iwglobe, (size_t)mwa, s));
+  OG_CUDA(cudaStreamSynchronize(s));
+
+  OG_CHECK(upload(d.gxc, g->gxps_coef, (size_t)mwa * 7, s));
+  OG_CHECK(upload(d.gyc, g->gyps_coef, (size_t)mwa * 7, s));
+  OG_CHECK(upload(d.xy_h, g->xy_h, (size_t)mwa * 35, s));
+  OG_CHECK(upload(d.xy_hu, g->xy_hu, (size_t)mwa * 35, s));
+  OG_CHECK(upload(d.dxps, g->dxps, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.dyps, g->dyps, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.xx0_v, g->xx0_v, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.xy0_v, g->xy0_v, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.yy0_v, g->yy0_v, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.xx0_vu, g->xx0_vu, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.xy0_vu, g->xy0_vu, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.yy0_vu, g->yy0_vu, (size_t)mva * 2, s));
+  OG_CHECK(upload(d.a_w, g->a_w, (size_t)mza * 4, s));
+  OG_CHECK(upload(d.a_wu, g->a_wu, (size_t)mza * 4, s));
+  OG_CHECK(upload(d.volti, g->volti, (size_t)mza * mwa, s));
+  OG_CUDA(cudaStreamSynchronize(s));
+  return OLAMGPU_OK;
+}
+
+// Per V face and side, the reconstruction folded into one weight per
+// neighbour of the upwind cell: value = S(c) + sum_n w_n (S(nb_n) - S(c)).
+// Restates scalar_v_column (scalar_transport_rk.F90:497-525) composed with
+// grad_t2d (grad_lib.f90:236-269) / grad_t2d_quadratic (:278-341).
+int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
+  const int mva = g->mva;
+  std::vector<float> wb((size_t)mva * 16, 0.f), wu((size_t)mva * 16, 0.f);
+  for (int iv = 1; iv < mva; ++iv) {
+    for (int sd = 0; sd < 2; ++sd) {
+      int c = g->itab_v_iw[(size_t)iv * 2 + sd] - 1;
+      int np = g->npoly[c];
+      double dx = g->dxps[(size_t)iv * 2 + sd], dy = g->dyps[(size_t)iv * 2 + sd];
+      for (int n = 0; n < np; ++n) {
+        double vb, vu;
+        if (order == 2) {
+          vb = dx * (double)g->gxps_coef[(size_t)c * 7 + n] + dy * (double)g->gyps_coef[(size_t)c * 7 + n];
+          vu = vb;
+        } else {
+          const float* xb = g->xy_h + ((size_t)c * 7 + n) * 5;
+          const float* xu = g->xy_hu + ((size_t)c * 7 + n) * 5;
+          size_t e = (size_t)iv * 2 + sd;
+          vb = dx * xb[0] + dy * xb[1] + (double)g->xx0_v[e] * xb[2] + (double)g->xy0_v[e] * xb[3] +
+               (double)g->yy0_v[e] * xb[4];
+          vu = dx * xu[0] + dy * xu[1] + (double)g->xx0_vu[e] * xu[2] + (double)g->xy0_vu[e] * xu[3] +
+               (double)g->yy0_vu[e] * xu[4];
+        }
+        wb[((size_t)iv * 2 + sd) * 8 + n] = (float)vb;
+        wu[((size_t)iv * 2 + sd) * 8 + n] = (float)vu;
+      }
+    }
+  }
+  OG_CHECK(upload(d.ew_b, wb.data(), wb.size(), s));
+  OG_CHECK(upload(d.ew_u, wu.data(), wu.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));
+  d.ew_order = order;
+  return OLAMGPU_OK;
+}
+
+}  // namespace olamgpu

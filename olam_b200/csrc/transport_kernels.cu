@@ -1,0 +1,830 @@
+// transport_kernels.cu -- CFL diagnosis, RK densities, implicit vertical
+// solve, and the reference-mirroring transport passes (gradient, V face,
+// W column, flux renormalisation, tendency) for any tracer count.
+//
+// The passes follow omodel/scalar_transport_rk.F90 one routine per kernel:
+//   launch_grad     grad_t2d / grad_t2d_quadratic (grad_lib.f90:236-341)
+//   launch_vflux    scalar_v_column (474-534), scalar_vflux_monot (749-832),
+//                   scalar_vflux_pd (1215-1285)
+//   launch_wcol     scalar_w_column (537-612), scalar_wflux_and_scales_monot
+//                   (835-1022), scalar_wflux_and_scale_pd (1288-1414)
+//   launch_vapply   the horizontal renormalisation loops (711-724, 1177-1190)
+//   launch_tend     scalar_tend_monot (1025-1078), scalar_tend_pd (1417-1469)
+// With one tracer in OLAM's (mza, mwa) layout they are the plain
+// one-kernel-per-pass form; with a tracer group of the batched layout they
+// run the last RK stage of the monotonic / positive-definite options.
+//
+// Device level index kd = Fortran k - 1.
+#include <cfloat>
+
+#include "transport_kernels.cuh"
+
+namespace olamgpu {
+
+static const float kEps0 = 1.e-32f;
+static const float kEps1 = 3.e-07f;
+
+GridK gridk(const DevGrid& d) {
+  GridK g;
+  g.mza = d.mza; g.mwa = d.mwa; g.mva = d.mva;
+  g.npoly = d.npoly.p; g.w_nb = d.w_nb.p; g.w_ev = d.w_ev.p; g.w_dirv = d.w_dirv.p;
+  g.v_iw = d.v_iw.p; g.lpw = d.lpw.p; g.lpv = d.lpv.p; g.volti = d.volti.p;
+  g.a_w = d.a_w.p; g.a_wu = d.a_wu.p;
+  return g;
+}
+
+__device__ __forceinline__ float AW(const float* a, int mza, int kd, int i, int j) {
+  return __ldg(a + kd + mza * ((i - 1) + 2 * (j - 1)));
+}
+
+// grad_z_quadratic (grad_lib.f90:166-229) at device level kd, from the three
+// column values around it.  Boundary flags as itopbc/ibotbc.
+__device__ __forceinline__ void zrec(const float* a, int mza, int kd, int kb, float sm1, float s0,
+                                     float sp1, float sp2_unused, bool ibot, bool itop,
+                                     float& sb, float& st) {
+  (void)sp2_unused;
+  float ds_k, ds_km1;
+  if (kd <= mza - 2) ds_k = sp1 - s0;
+  else ds_k = itop ? (s0 - sm1) : 0.f;
+  if (kd >= kb + 1) ds_km1 = s0 - sm1;
+  else ds_km1 = ibot ? ((kb <= mza - 2) ? sp1 - s0 : 0.f) : 0.f;
+  sb = s0 + ds_k * AW(a, mza, kd, 1, 1) + ds_km1 * AW(a, mza, kd, 2, 1);
+  st = s0 + ds_k * AW(a, mza, kd, 1, 2) + ds_km1 * AW(a, mza, kd, 2, 2);
+}
+
+// ---------------------------------------------------------------------------
+// check_cfls (scalar_transport_rk.F90:1476-1712)
+// red[0..5]: (cfl key, cfl nan), (cflh key, cflh nan), (|w| key, w nan)
+// key = float bits << 32 | (0xffffffff - order) so atomicMax keeps the largest
+// value and, on ties, the first point in loop order; nan = order + 1 of the
+// last NaN in loop order (OLAM's serial loop keeps the last NaN it meets).
+// ---------------------------------------------------------------------------
+__global__ void k_check_cfls(GridK g, const int* __restrict__ prog, int nprog,
+                             const float* __restrict__ vmasc, const float* __restrict__ wmasc,
+                             const float* __restrict__ rho, const float* __restrict__ wc, int nrk,
+                             float dt, float* __restrict__ ff, unsigned long long* red) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nprog) return;
+  const int mza = g.mza;
+  int iw = prog[j];
+  int np = g.npoly[iw];
+  float fimp[3] = {0.f, 0.f, 0.f};
+  unsigned long long kc = 0, kh = 0, kw = 0, nc = 0, nh = 0, nwn = 0;
+  for (int kd = g.lpw[iw]; kd < mza; ++kd) {
+    float cflh = 0.f;
+    for (int n = 0; n < np; ++n) {
+      int iv = g.w_ev[iw * 8 + n];
+      if (kd >= g.lpv[iv]) cflh = cflh - fminf(g.w_dirv[iw * 8 + n] * vmasc[(size_t)iv * mza + kd], 0.0f);
+    }
+    float dovr = dt * g.volti[(size_t)iw * mza + kd] / rho[(size_t)iw * mza + kd];
+    cflh = cflh * dovr;
+    float cflw = (fmaxf(wmasc[(size_t)iw * mza + kd], 0.f) - fminf(wmasc[(size_t)iw * mza + kd - 1], 0.f)) * dovr;
+    float cfl = cflh + cflw;
+    cflw = fmaxf(cflw, .1f);
+    fimp[nrk - 1] = fmaxf(fimp[nrk - 1], (cfl - 0.98f) / cflw);
+    fimp[nrk - 2] = fmaxf(fimp[nrk - 2], (cfl - 1.98f) / cflw);
+    if (nrk == 3) fimp[0] = fmaxf(fimp[0], (cfl - 2.98f) / cflw);
+    unsigned int order = (unsigned int)j * (unsigned int)mza + (unsigned int)kd;
+    unsigned long long low = 0xffffffffull - order;
+    if (cfl != cfl) nc = order + 1ull;
+    else if (cfl > 0.f) {
+      unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | low;
+      if (key > kc) kc = key;
+    }
+    if (cflh != cflh) nh = order + 1ull;
+    else if (cflh > 0.f) {
+      unsigned long long key = ((unsigned long long)__float_as_uint(cflh) << 32) | low;
+      if (key > kh) kh = key;
+    }
+    if (wc) {
+      float w = wc[(size_t)iw * mza + kd];
+      if (w != w) nwn = order + 1ull;
+      else if (fabsf(w) > 0.f) {
+        unsigned long long key = ((unsigned long long)__float_as_uint(fabsf(w)) << 32) | low;
+        if (key > kw) kw = key;
+      }
+    }
+  }
+  for (int n = 0; n < nrk; ++n) {
+    float f = fminf(1.0f, fimp[n]);
+    // NaN-propagating min: OLAM's min(1.0, NaN) is compiler-dependent; a NaN
+    // CFL already makes the run invalid and is reported through the keys.
+    if (f < .02f) f = 0.f;
+    ff[(size_t)iw * nrk + n] = f;
+  }
+  if (red) {
+    if (kc) atomicMax(&red[0], kc);
+    if (nc) atomicMax(&red[1], nc);
+    if (kh) atomicMax(&red[2], kh);
+    if (nh) atomicMax(&red[3], nh);
+    if (kw) atomicMax(&red[4], kw);
+    if (nwn) atomicMax(&red[5], nwn);
+  }
+}
+
+void launch_check_cfls(const DevGrid& d, const Transport& tp, int nrk, float dtl,
+                       unsigned long long* red, cudaStream_t s) {
+  if (red) cudaMemsetAsync(red, 0, 6 * sizeof(unsigned long long), s);
+  int nb = 128;
+  k_check_cfls<<<cdiv(d.nw_prog, nb), nb, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, tp.vmasc.p,
+                                                  tp.wmasc.p, tp.rho_old.p, tp.wc.p, nrk, dtl,
+                                                  tp.ff.p, red);
+  OG_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// rhos (scalar_transport_rk.F90:117-152), nudging off
+// ---------------------------------------------------------------------------
+__global__ void k_rhos(GridK g, const int* __restrict__ prog, int nprog, const double* __restrict__ rho,
+                       const float* __restrict__ rho_old, float* __restrict__ rhos, int nrk) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mza = g.mza;
+  if (i >= (size_t)nprog * mza) return;
+  int j = (int)(i / mza), kd = (int)(i % mza);
+  int iw = prog[j];
+  if (kd < g.lpw[iw]) return;
+  size_t ix = (size_t)iw * mza + kd;
+  size_t plane = (size_t)g.mwa * mza;
+  float rhof = (float)rho[ix];
+  float ro = rho_old[ix];
+  if (nrk == 3) {
+    rhos[ix] = (2.f / 3.f) * ro + (1.f / 3.f) * rhof;
+    rhos[plane + ix] = 0.5f * (ro + rhof);
+    rhos[2 * plane + ix] = rhof;
+  } else {
+    rhos[ix] = 0.5f * (ro + rhof);
+    rhos[plane + ix] = rhof;
+  }
+}
+
+void launch_rhos(const DevGrid& d, Transport& tp, int nrk, cudaStream_t s) {
+  size_t n = (size_t)d.nw_prog * d.mza;
+  k_rhos<<<cdiv(n, 256), 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, tp.rho.p, tp.rho_old.p,
+                                      tp.rhos.p, nrk);
+  OG_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// implicit-column factorisation (scalar_transport_rk.F90:164-217) with
+// tridif_prep (tridiag_lib.f90:321-338).  Column slots are handed out by an
+// atomic counter; each column's result does not depend on its slot.
+// imp_b[(n*mwa + slot)*3*mza + {0,1,2}*mza + kd] = b1, scr1, cji.
+// ---------------------------------------------------------------------------
+struct Dtlr { float v[3]; };
+
+__global__ void k_implicit_prep(GridK g, const int* __restrict__ prog, int nprog,
+                                const float* __restrict__ ff, const float* __restrict__ wmasc,
+                                const float* __restrict__ rhos, int nrk, Dtlr dtlr,
+                                int* __restrict__ list, int* __restrict__ count, float* __restrict__ b) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nprog) return;
+  const int mza = g.mza;
+  int iw = prog[j];
+  int kb = g.lpw[iw];
+  size_t plane = (size_t)g.mwa * mza;
+  for (int n = 0; n < nrk; ++n) {
+    float f = ff[(size_t)iw * nrk + n];
+    if (!(f > 0.001f)) continue;
+    int slot = atomicAdd(&count[n], 1);
+    list[(size_t)n * g.mwa + slot] = iw;
+    float* b1 = b + ((size_t)n * g.mwa + slot) * 3 * mza;
+    float* scr1 = b1 + mza;
+    float* cji = b1 + 2 * mza;
+    float c1 = f * dtlr.v[n];
+    const float* wm = wmasc + (size_t)iw * mza;
+    // wup(kd) = max(wmasc,0), wdn(kd) = min(wmasc,0) for kd in [kb, mza-2];
+    // zero at kb-1 and mza-1
+    float cji_prev = 0.f, cip1_prev = 0.f;
+    for (int kd = kb; kd < mza; ++kd) {
+      float wup_m1 = (kd - 1 >= kb) ? fmaxf(wm[kd - 1], 0.f) : 0.f;
+      float wdn_m1 = (kd - 1 >= kb) ? fminf(wm[kd - 1], 0.f) : 0.f;
+      float wup = (kd <= mza - 2) ? fmaxf(wm[kd], 0.f) : 0.f;
+      float wdn = (kd <= mza - 2) ? fminf(wm[kd], 0.f) : 0.f;
+      float c2 = c1 * g.volti[(size_t)iw * mza + kd] / rhos[(size_t)n * plane + (size_t)iw * mza + kd];
+      float cim1 = -c2 * wup_m1;
+      float ci = 1.0f + c2 * (wup - wdn_m1);
+      float cip1 = c2 * wdn;
+      b1[kd] = cim1;
+      if (kd == kb) {
+        cji_prev = 1.0f / ci;
+        cji[kd] = cji_prev;
+        scr1[kd] = 0.f;
+      } else {
+        float sc = cji_prev * cip1_prev;
+        scr1[kd] = sc;
+        cji_prev = 1.0f / (ci - cim1 * sc);
+        cji[kd] = cji_prev;
+      }
+      cip1_prev = cip1;
+    }
+  }
+}
+
+void launch_implicit_prep(const DevGrid& d, Transport& tp, int nrk, const float* dtlr, cudaStream_t s) {
+  cudaMemsetAsync(tp.imp_count.p, 0, sizeof(int) * 3, s);
+  Dtlr v{{dtlr[0], dtlr[1], nrk > 2 ? dtlr[2] : 0.f}};
+  k_implicit_prep<<<cdiv(d.nw_prog, 128), 128, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, tp.ff.p,
+                                                       tp.wmasc.p, tp.rhos.p, nrk, v, tp.imp_list.p,
+                                                       tp.imp_count.p, tp.imp_b.p);
+  OG_LAUNCHED();
+}
+
+// implicit vertical transport (scalar_transport_rk.F90:347-375) with
+// tridif_fini (tridiag_lib.f90:344-364); one thread per (column, tracer).
+__global__ void k_implicit_solve(GridK g, const int* __restrict__ list, const int* __restrict__ count,
+                                 const float* __restrict__ b, const float* __restrict__ ff,
+                                 const float* __restrict__ wmasc, const float* __restrict__ rhos_st,
+                                 int nrk, int istage, float dtr, CTView scp0, TView scp, int nt) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int n = *count;
+  if (i >= (size_t)n * nt) return;
+  int slot = (int)(i / nt), t = (int)(i % nt);
+  const int mza = g.mza;
+  int iw = list[slot];
+  int kb = g.lpw[iw];
+  const float* b1 = b + (size_t)slot * 3 * mza;
+  const float* scr1 = b1 + mza;
+  const float* cji = b1 + 2 * mza;
+  const float* wm = wmasc + (size_t)iw * mza;
+  float ffv = ff[(size_t)iw * nrk + istage - 1];
+  auto S0 = [&](int kd) { return scp0.base[((size_t)iw * mza + kd) * scp0.ld + scp0.t0 + t]; };
+  float* sp = scp.base + (size_t)iw * mza * scp.ld + scp.t0 + t;
+  // forward elimination into soln (kept in the output column), then back
+  // substitution; delex is formed on the fly from scp and scp0
+  float prev = 0.f;
+  for (int kd = kb; kd < mza; ++kd) {
+    float s0 = S0(kd);
+    float dk = (kd <= mza - 2) ? S0(kd + 1) - s0 : 0.f;
+    float dkm1 = (kd - 1 >= kb) ? s0 - S0(kd - 1) : 0.f;
+    float c1 = ffv * dtr * g.volti[(size_t)iw * mza + kd] / rhos_st[(size_t)iw * mza + kd];
+    float delex = sp[(size_t)kd * scp.ld] - s0 - c1 * (fminf(wm[kd], 0.f) * dk + fmaxf(wm[kd - 1], 0.f) * dkm1);
+    float sol = (kd == kb) ? delex * cji[kd] : cji[kd] * (delex - b1[kd] * prev);
+    sp[(size_t)kd * scp.ld] = sol;
+    prev = sol;
+  }
+  for (int kd = mza - 2; kd >= kb; --kd) {
+    float v = sp[(size_t)kd * scp.ld] - scr1[kd + 1] * sp[(size_t)(kd + 1) * scp.ld];
+    sp[(size_t)kd * scp.ld] = v;
+  }
+  for (int kd = kb; kd < mza; ++kd) sp[(size_t)kd * scp.ld] = S0(kd) + sp[(size_t)kd * scp.ld];
+  for (int kd = 1; kd < kb; ++kd) sp[(size_t)kd * scp.ld] = sp[(size_t)kb * scp.ld];
+}
+
+void launch_implicit_solve(const DevGrid& d, const Transport& tp, int nrk, int istage, float dtr,
+                           CTView scp0, TView scp, int nt, cudaStream_t s) {
+  // an upper bound on the launch size; threads past the device count exit
+  size_t n = (size_t)d.nw_prog * nt;
+  size_t plane = (size_t)d.mwa * d.mza;
+  const float* b = tp.imp_b.p + (size_t)(istage - 1) * d.mwa * 3 * d.mza;
+  k_implicit_solve<<<cdiv(n, 128), 128, 0, s>>>(gridk(d), tp.imp_list.p + (size_t)(istage - 1) * d.mwa,
+                                                tp.imp_count.p + (istage - 1), b, tp.ff.p, tp.wmasc.p,
+                                                tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage,
+                                                dtr, scp0, scp, nt);
+  OG_LAUNCHED();
+}
+
+// horizontal diffusion hook (scalar_transport_rk.F90:244-274)
+__global__ void k_diffusion(GridK g, const int* __restrict__ prog, int nprog,
+                            const float* __restrict__ akhodx, const int* __restrict__ khtopv,
+                            CTView scp, TView sct, int nt) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nprog * nt) return;
+  int j = (int)(i / nt), t = (int)(i % nt);
+  const int mza = g.mza;
+  int iw = prog[j];
+  int np = g.npoly[iw];
+  int kwtop = 0;
+  for (int n = 0; n < np; ++n) kwtop = max(kwtop, khtopv[g.w_ev[iw * 8 + n]]);
+  int kb = g.lpw[iw];
+  // khtopv holds OLAM's 1-based top level; device level = khtopv - 1
+  if (kwtop - 1 < kb) return;
+  for (int kd = kb; kd <= kwtop - 1; ++kd) {
+    float fd = 0.f;
+    for (int n = 0; n < np; ++n) {
+      int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
+      if (kd >= g.lpv[iv] && kd <= khtopv[iv] - 1)
+        fd = fd + akhodx[(size_t)iv * mza + kd] *
+                      (scp.base[((size_t)iwn * mza + kd) * scp.ld + scp.t0 + t] -
+                       scp.base[((size_t)iw * mza + kd) * scp.ld + scp.t0 + t]);
+    }
+    float* p = sct.base + ((size_t)iw * mza + kd) * sct.ld + sct.t0 + t;
+    *p = *p + fd * g.volti[(size_t)iw * mza + kd];
+  }
+}
+
+void launch_diffusion(const DevGrid& d, const Transport& tp, CTView scp, TView sct, int nt,
+                      cudaStream_t s) {
+  size_t n = (size_t)d.nw_prog * nt;
+  k_diffusion<<<cdiv(n, 128), 128, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, tp.akhodx.p,
+                                           tp.khtopv.p, scp, sct, nt);
+  OG_LAUNCHED();
+}
+
+// last-stage low-order pre-update of scp0 for monotonic / positive-definite
+// tracers (scalar_transport_rk.F90:297-314)
+__global__ void k_scp0_pd(GridK g, const int* __restrict__ wadj, int nwadj, TView scp0, CTView sct,
+                          const float* __restrict__ rho_old, const int* __restrict__ mode, int nt,
+                          float dtr) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nwadj * nt) return;
+  int j = (int)(i / nt), t = (int)(i % nt);
+  if (!mode[t]) return;
+  const int mza = g.mza;
+  int iw = wadj[j];
+  int kb = g.lpw[iw];
+  for (int kd = kb; kd < mza; ++kd) {
+    float* p = scp0.base + ((size_t)iw * mza + kd) * scp0.ld + scp0.t0 + t;
+    *p = *p + dtr * sct.base[((size_t)iw * mza + kd) * sct.ld + sct.t0 + t] /
+                  rho_old[(size_t)iw * mza + kd];
+  }
+  float v = scp0.base[((size_t)iw * mza + kb) * scp0.ld + scp0.t0 + t];
+  for (int kd = 1; kd < kb; ++kd) scp0.base[((size_t)iw * mza + kd) * scp0.ld + scp0.t0 + t] = v;
+}
+
+void launch_scp0_pd_update(const DevGrid& d, const Transport& tp, TView scp0, CTView sct,
+                           const int* mode, int nt, float dtr, cudaStream_t s) {
+  size_t n = (size_t)d.nw_wadj * nt;
+  k_scp0_pd<<<cdiv(n, 128), 128, 0, s>>>(gridk(d), d.jtw_wadj.p, d.nw_wadj, scp0, sct, tp.rho_old.p,
+                                         mode, nt, dtr);
+  OG_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// pass 1: horizontal gradient planes gx[m][iw][kd][t] (compact, ld = nt)
+// ---------------------------------------------------------------------------
+__global__ void k_grad(GridK g, const int* __restrict__ prog, int nprog, CTView scp,
+                       float* __restrict__ gx, int nt, int order, const float* __restrict__ cx,
+                       const float* __restrict__ cy, const float* __restrict__ xy) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mza = g.mza;
+  size_t tot = (size_t)nprog * mza * nt;
+  if (i >= tot) return;
+  int t = (int)(i % nt);
+  size_t r = i / nt;
+  int kd = (int)(r % mza);
+  int j = (int)(r / mza);
+  int iw = prog[j];
+  int np = g.npoly[iw];
+  size_t plane = (size_t)g.mwa * mza * nt;
+  size_t o = ((size_t)iw * mza + kd) * nt + t;
+  float sc0 = scp.base[((size_t)iw * mza + kd) * scp.ld + scp.t0 + t];
+  if (order == 2) {
+    float gxv = 0.f, gyv = 0.f;
+    for (int n = 0; n < np; ++n) {
+      int iv = g.w_ev[iw * 8 + n];
+      if (kd < g.lpv[iv]) continue;
+      int iwn = g.w_nb[iw * 8 + n];
+      float d = scp.base[((size_t)iwn * mza + kd) * scp.ld + scp.t0 + t] - sc0;
+      gxv = gxv + __ldg(cx + iw * 7 + n) * d;
+      gyv = gyv + __ldg(cy + iw * 7 + n) * d;
+    }
+    gx[o] = gxv;
+    gx[plane + o] = gyv;
+  } else {
+    float a[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int n = 0; n < np; ++n) {
+      int iv = g.w_ev[iw * 8 + n];
+      if (kd < g.lpv[iv]) continue;
+      int iwn = g.w_nb[iw * 8 + n];
+      float d = scp.base[((size_t)iwn * mza + kd) * scp.ld + scp.t0 + t] - sc0;
+      const float* c = xy + ((size_t)iw * 7 + n) * 5;
+#pragma unroll
+      for (int m = 0; m < 5; ++m) a[m] = a[m] + d * __ldg(c + m);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) gx[m * plane + o] = a[m];
+  }
+}
+
+void launch_grad(const DevGrid& d, CTView scp, float* gx, int nt, int order, bool bounded,
+                 cudaStream_t s) {
+  size_t n = (size_t)d.nw_prog * d.mza * nt;
+  k_grad<<<cdiv(n, 256), 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp, gx, nt, order, d.gxc.p,
+                                      d.gyc.p, bounded ? d.xy_h.p : d.xy_hu.p);
+  OG_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// pass 2: V-face values.  mode[t] == PLAIN: upv = upwind reconstruction.
+// MONOT/PD: upv = low-order value from scp0, hiv = high-order correction,
+// sfv = vmasc*hiv.
+// ---------------------------------------------------------------------------
+struct VCoef {
+  const float* dxps; const float* dyps;
+  const float* xx; const float* xy; const float* yy;
+};
+
+__device__ __forceinline__ float side_val(const CTView& scp, const float* __restrict__ gx, size_t plane,
+                                          int mza, int nt, int order, const VCoef& vc, int iv, int sd,
+                                          int iws, int kd, int t) {
+  size_t o = ((size_t)iws * mza + kd) * nt + t;
+  float v = scp.base[((size_t)iws * mza + kd) * scp.ld + scp.t0 + t];
+  int e = iv * 2 + sd;
+  v = v + __ldg(vc.dxps + e) * gx[o] + __ldg(vc.dyps + e) * gx[plane + o];
+  if (order == 3)
+    v = v + __ldg(vc.xx + e) * gx[2 * plane + o] + __ldg(vc.xy + e) * gx[3 * plane + o] +
+        __ldg(vc.yy + e) * gx[4 * plane + o];
+  return v;
+}
+
+__global__ void k_vflux(GridK g, const int* __restrict__ vlist, int nv, CTView scp, CTView scp0,
+                        const float* __restrict__ gx, const float* __restrict__ vmasc, int nt, int order,
+                        VCoef vc, const int* __restrict__ mode, float* __restrict__ upv,
+                        float* __restrict__ hiv, float* __restrict__ sfv) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mza = g.mza;
+  if (i >= (size_t)nv * mza * nt) return;
+  int t = (int)(i % nt);
+  size_t r = i / nt;
+  int kd = (int)(r % mza);
+  int iv = vlist[r / mza];
+  if (kd < g.lpv[iv]) return;
+  int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  size_t plane = (size_t)g.mwa * mza * nt;
+  float s1 = side_val(scp, gx, plane, mza, nt, order, vc, iv, 0, iw1, kd, t);
+  float s2 = side_val(scp, gx, plane, mza, nt, order, vc, iv, 1, iw2, kd, t);
+  float vm = vmasc[(size_t)iv * mza + kd];
+  size_t o = ((size_t)iv * mza + kd) * nt + t;
+  int md = mode ? mode[t] : MODE_PLAIN;
+  if (md == MODE_PLAIN) {
+    float up = s1;
+    if (vm < 0.f) up = s2;
+    upv[o] = up;
+  } else {
+    float lo = scp0.base[((size_t)iw1 * mza + kd) * scp0.ld + scp0.t0 + t];
+    if (vm < 0.f) lo = scp0.base[((size_t)iw2 * mza + kd) * scp0.ld + scp0.t0 + t];
+    float hi = s1;
+    if (vm < 0.f) hi = s2;
+    hi = hi - lo;
+    upv[o] = lo;
+    hiv[o] = hi;
+    sfv[o] = vm * hi;
+  }
+}
+
+void launch_vflux(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, const float* gx,
+                  int nt, int order, bool unbounded, const int* mode, bool anylim, cudaStream_t s) {
+  VCoef vc{d.dxps.p, d.dyps.p, unbounded ? d.xx0_vu.p : d.xx0_v.p, unbounded ? d.xy0_vu.p : d.xy0_v.p,
+           unbounded ? d.yy0_vu.p : d.yy0_v.p};
+  size_t n = (size_t)d.nv_wadj * d.mza * nt;
+  k_vflux<<<cdiv(n, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp, scp0, gx, tp.vmasc.p, nt,
+                                       order, vc, anylim ? mode : nullptr, tp.upv.p, tp.hiv.p, tp.sfv.p);
+  OG_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// pass 3: one thread per (column, tracer), sequential in k.
+// ---------------------------------------------------------------------------
+struct WcolArgs {
+  GridK g;
+  const int* prog; int nprog;
+  CTView scp, scp0, sct;
+  const float* rhos;        // stage density rhos(:,:,nrk)
+  const float* vmasc; const float* wmasc; const float* ff;
+  const float* upv; const float* sfv;   // compact (mva, mza, nt)
+  float* scale;             // compact (2, mwa, mza, nt)
+  float* upw;               // compact (mwa, mza, nt)
+  TView out;
+  int nt, istage, nrk; float dtr;
+  const int* mode;
+};
+
+__global__ void k_wcol(WcolArgs A) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)A.nprog * A.nt) return;
+  const GridK& g = A.g;
+  const int mza = g.mza;
+  int t = (int)(i % A.nt);
+  int iw = A.prog[i / A.nt];
+  int kb = g.lpw[iw];
+  int np = g.npoly[iw];
+  int md = A.mode ? A.mode[t] : MODE_PLAIN;
+  float fimpl = A.ff[(size_t)iw * A.nrk + A.istage - 1];
+  float fexpl = 1.0f - fimpl;
+  const float* wm = A.wmasc + (size_t)iw * mza;
+  auto S = [&](int kd) { return A.scp.base[((size_t)iw * mza + kd) * A.scp.ld + A.scp.t0 + t]; };
+  auto S0 = [&](int kd) { return A.scp0.base[((size_t)iw * mza + kd) * A.scp0.ld + A.scp0.t0 + t]; };
+  auto OUTP = [&](int kd) { return A.out.base + ((size_t)iw * mza + kd) * A.out.ld + A.out.t0 + t; };
+  const size_t ntz = (size_t)A.nt;
+
+  if (md == MODE_PLAIN) {
+    // scalar_w_column (scalar_transport_rk.F90:537-612)
+    float up_prev = S(kb);  // scp_upw(kb-1) = scp(kb)
+    float sm1 = 0.f, s0 = S(kb), sp1 = (kb + 1 < mza) ? S(kb + 1) : 0.f;
+    float sp2 = (kb + 2 < mza) ? S(kb + 2) : 0.f;
+    for (int kd = kb; kd < mza; ++kd) {
+      float up;
+      if (kd <= mza - 2) {
+        if (wm[kd] < 0.f) {
+          // scpb(kd+1): level kd+1 with neighbours kd, kd+2
+          float sb, st;
+          zrec(g.a_w, mza, kd + 1, kb, s0, sp1, sp2, 0.f, false, false, sb, st);
+          up = sb;
+        } else {
+          float sb, st;
+          zrec(g.a_w, mza, kd, kb, sm1, s0, sp1, 0.f, false, false, sb, st);
+          up = st;
+        }
+      } else {
+        up = s0;  // scp_upw(mza) = scp(mza)
+      }
+      float s00 = S0(kd);
+      float fd = 0.f;
+      for (int n = 0; n < np; ++n) {
+        int iv = g.w_ev[iw * 8 + n];
+        if (kd < g.lpv[iv]) continue;
+        fd = fd + g.w_dirv[iw * 8 + n] * A.vmasc[(size_t)iv * mza + kd] *
+                      (A.upv[((size_t)iv * mza + kd) * ntz + t] - s00);
+      }
+      fd = fd + fexpl * (wm[kd - 1] * (up_prev - s00) - wm[kd] * (up - s00));
+      float sctv = A.sct.base[((size_t)iw * mza + kd) * A.sct.ld + A.sct.t0 + t];
+      *OUTP(kd) = s00 + A.dtr * (sctv + g.volti[(size_t)iw * mza + kd] * fd) / A.rhos[(size_t)iw * mza + kd];
+      up_prev = up;
+      sm1 = s0; s0 = sp1; sp1 = sp2;
+      sp2 = (kd + 3 < mza) ? S(kd + 3) : 0.f;
+    }
+    float v = *OUTP(kb);
+    for (int kd = 0; kd < kb; ++kd) *OUTP(kd) = v;
+    return;
+  }
+
+  // monotonic (md == 1) / positive-definite (md == 2) scale factors
+  const bool monot = (md == MODE_MONOT);
+  const float eps0 = kEps0, eps1 = kEps1, onep = 1.0f + kEps1, onem = 1.0f - kEps1;
+  const float* awu = g.a_wu;
+  float* upwp = A.upw + (size_t)iw * mza * ntz + t;
+  float* sc1 = A.scale + (size_t)iw * mza * ntz + t;
+  float* sc2 = A.scale + ((size_t)g.mwa + iw) * mza * ntz + t;
+  // low-order vertical upwind value scp_upw(k) at device face kd (between kd, kd+1)
+  auto lo_face = [&](int kd) -> float {
+    if (kd == kb - 1) return monot ? S0(kb) : S(kb);
+    if (kd == mza - 1) return monot ? S0(mza - 1) : S(mza - 1);
+    float v = S0(kd);
+    if (wm[kd] < 0.f) v = S0(kd + 1);
+    return v;
+  };
+  // high-order face correction hiw(kd) for kd in [kb, mza-2]
+  auto hi_face = [&](int kd) -> float {
+    float sb, st;
+    if (wm[kd] < 0.f) {
+      float a0 = S(kd), a1 = S(kd + 1), a2 = (kd + 2 < mza) ? S(kd + 2) : 0.f;
+      zrec(monot ? awu : g.a_w, mza, kd + 1, kb, a0, a1, a2, 0.f, monot, monot, sb, st);
+      return sb - lo_face(kd);
+    } else {
+      float am = (kd - 1 >= kb) ? S(kd - 1) : 0.f, a0 = S(kd), a1 = S(kd + 1);
+      zrec(monot ? awu : g.a_w, mza, kd, kb, am, a0, a1, 0.f, monot, monot, sb, st);
+      return st - lo_face(kd);
+    }
+  };
+  float dtrp = onep * A.dtr;
+  float mdtrp = -onep * A.dtr;
+  float sfw_prev = 0.f;  // sfluxwh(kb-1) = 0
+  for (int kd = kb; kd < mza; ++kd) {
+    float sfw = 0.f;
+    if (kd <= mza - 2) sfw = fexpl * wm[kd] * hi_face(kd);
+    float s00 = S0(kd);
+    float fl = 0.f, fin = 0.f, fout = 0.f;
+    float smax = s00, smin = s00;
+    if (monot) {
+      if (kd >= kb + 1 && wm[kd - 1] > 0.f) { smax = fmaxf(smax, S0(kd - 1)); smin = fminf(smin, S0(kd - 1)); }
+      if (kd <= mza - 2 && wm[kd] < 0.f) { smax = fmaxf(smax, S0(kd + 1)); smin = fminf(smin, S0(kd + 1)); }
+    }
+    for (int n = 0; n < np; ++n) {
+      int iv = g.w_ev[iw * 8 + n];
+      if (kd < g.lpv[iv]) continue;
+      float dv = g.w_dirv[iw * 8 + n];
+      float vm = A.vmasc[(size_t)iv * mza + kd];
+      size_t o = ((size_t)iv * mza + kd) * ntz + t;
+      fl = fl + dv * vm * (A.upv[o] - s00);
+      if (monot) fin = fin + fmaxf(dv * A.sfv[o], 0.f);
+      fout = fout + fminf(dv * A.sfv[o], 0.f);
+      if (monot && dv * vm > 0.f) {
+        int iwn = g.w_nb[iw * 8 + n];
+        float sn = A.scp0.base[((size_t)iwn * mza + kd) * A.scp0.ld + A.scp0.t0 + t];
+        smax = fmaxf(smax, sn);
+        smin = fminf(smin, sn);
+      }
+    }
+    float lo_m1 = lo_face(kd - 1), lo_k = lo_face(kd);
+    float rh = A.rhos[(size_t)iw * mza + kd];
+    float vt = g.volti[(size_t)iw * mza + kd];
+    if (fimpl > .001f) {
+      float dwi = fimpl * (wm[kd] - wm[kd - 1]);
+      if (monot) {
+        fl = fl + fexpl * (wm[kd - 1] * (lo_m1 - s00) - wm[kd] * (lo_k - s00)) + s00 * dwi;
+        fin = fin + fmaxf(sfw_prev, 0.f) - fminf(sfw, 0.f);
+        fout = fout + fminf(sfw_prev, 0.f) - fmaxf(sfw, 0.f);
+        float imp = rh + A.dtr * vt * dwi;
+        smax = imp * smax;
+        smin = imp * smin;
+      } else {
+        fl = fl + fexpl * (wm[kd - 1] * (lo_m1 - s00) - wm[kd] * (lo_k - s00)) +
+             fimpl * s00 * (wm[kd] - wm[kd - 1]);
+        fout = fout + fminf(sfw_prev, 0.f) - fmaxf(sfw, 0.f);
+      }
+    } else {
+      fl = fl + wm[kd - 1] * (lo_m1 - s00) - wm[kd] * (lo_k - s00);
+      if (monot) {
+        fin = fin + fmaxf(sfw_prev, 0.f) - fminf(sfw, 0.f);
+        smax = rh * smax;
+        smin = rh * smin;
+      }
+      fout = fout + fminf(sfw_prev, 0.f) - fmaxf(sfw, 0.f);
+    }
+    float rscp_low = s00 * rh + A.dtr * vt * fl;
+    if (monot) {
+      float flux_in = fmaxf(dtrp * vt * fin, eps0);
+      float flux_out = fminf(dtrp * vt * fout, -eps0);
+      float epsr = eps1 * fabsf(rscp_low);
+      float sc_in = fmaxf(smax - (rscp_low + epsr) - eps0, 0.f);
+      float sc_out = fminf(smin - (rscp_low - epsr) + eps0, 0.f);
+      sc1[(size_t)kd * ntz] = fminf(1.f, sc_in / fmaxf(flux_in, 0.01f * sc_in));
+      sc2[(size_t)kd * ntz] = fminf(1.f, sc_out / fminf(flux_out, 0.01f * sc_out));
+    } else {
+      float flux_out = fmaxf(mdtrp * vt * fout, eps0);
+      float sc_out = fmaxf(onem * rscp_low - eps0, 0.f);
+      sc1[(size_t)kd * ntz] = fminf(1.f, sc_out / fmaxf(flux_out, 0.01f * sc_out));
+    }
+    sfw_prev = sfw;
+  }
+  // renormalised vertical face values (scp_upw) for the tendency pass
+  upwp[(size_t)(kb - 1) * ntz] = lo_face(kb - 1);
+  upwp[(size_t)(mza - 1) * ntz] = lo_face(mza - 1);
+  for (int kd = kb; kd <= mza - 2; ++kd) {
+    float hi = hi_face(kd);
+    float sfw = fexpl * wm[kd] * hi;
+    float scale;
+    if (monot) {
+      scale = fminf(sc1[(size_t)(kd + 1) * ntz], sc2[(size_t)kd * ntz]);
+      if (sfw < 0.f) scale = fminf(sc1[(size_t)kd * ntz], sc2[(size_t)(kd + 1) * ntz]);
+    } else {
+      scale = sc1[(size_t)kd * ntz];
+      if (sfw < 0.f) scale = sc1[(size_t)(kd + 1) * ntz];
+    }
+    upwp[(size_t)kd * ntz] = lo_face(kd) + hi * scale;
+  }
+}
+
+void launch_wcol(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct,
+                 const float* rhos, TView out, int nt, int istage, int nrk, float dtr,
+                 const int* mode, bool anylim, cudaStream_t s) {
+  WcolArgs A;
+  A.g = gridk(d);
+  A.prog = d.jtw_prog.p; A.nprog = d.nw_prog;
+  A.scp = scp; A.scp0 = scp0; A.sct = sct; A.rhos = rhos;
+  A.vmasc = tp.vmasc.p; A.wmasc = tp.wmasc.p; A.ff = tp.ff.p;
+  A.upv = tp.upv.p; A.sfv = tp.sfv.p; A.scale = tp.scale.p; A.upw = tp.upw.p;
+  A.out = out; A.nt = nt; A.istage = istage; A.nrk = nrk; A.dtr = dtr;
+  A.mode = anylim ? mode : nullptr;
+  size_t n = (size_t)d.nw_prog * nt;
+  k_wcol<<<cdiv(n, 128), 128, 0, s>>>(A);
+  OG_LAUNCHED();
+}
+
+// pass 4: horizontal flux renormalisation (711-724 monot, 1177-1190 pd)
+__global__ void k_vapply(GridK g, const int* __restrict__ vlist, int nv, int nt,
+                         const int* __restrict__ mode, float* __restrict__ upv,
+                         const float* __restrict__ hiv, const float* __restrict__ sfv,
+                         const float* __restrict__ scale) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int mza = g.mza;
+  if (i >= (size_t)nv * mza * nt) return;
+  int t = (int)(i % nt);
+  size_t r = i / nt;
+  int kd = (int)(r % mza);
+  int iv = vlist[r / mza];
+  int md = mode[t];
+  if (md == MODE_PLAIN || kd < g.lpv[iv]) return;
+  int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  size_t o = ((size_t)iv * mza + kd) * nt + t;
+  const size_t s2 = (size_t)g.mwa * mza * nt;
+  size_t a1 = ((size_t)iw1 * mza + kd) * nt + t, a2 = ((size_t)iw2 * mza + kd) * nt + t;
+  float sc;
+  if (md == MODE_MONOT) {
+    sc = fminf(scale[a2], scale[s2 + a1]);
+    if (sfv[o] < 0.f) sc = fminf(scale[a1], scale[s2 + a2]);
+  } else {
+    sc = scale[a1];
+    if (sfv[o] < 0.f) sc = scale[a2];
+  }
+  upv[o] = upv[o] + hiv[o] * sc;
+}
+
+void launch_vapply(const DevGrid& d, const Transport& tp, int nt, const int* mode, cudaStream_t s) {
+  size_t n = (size_t)d.nv_wadj * d.mza * nt;
+  k_vapply<<<cdiv(n, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, nt, mode, tp.upv.p, tp.hiv.p,
+                                        tp.sfv.p, tp.scale.p);
+  OG_LAUNCHED();
+}
+
+// pass 5: tendency and update for limited tracers (scalar_tend_monot/_pd)
+__global__ void k_tend(GridK g, const int* __restrict__ prog, int nprog, CTView scp0,
+                       const float* __restrict__ rhos, const float* __restrict__ vmasc,
+                       const float* __restrict__ wmasc, const float* __restrict__ ff,
+                       const float* __restrict__ upv, const float* __restrict__ upw, TView out, int nt,
+                       int istage, int nrk, float dtr, const int* __restrict__ mode) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nprog * nt) return;
+  const int mza = g.mza;
+  int t = (int)(i % nt);
+  if (mode[t] == MODE_PLAIN) return;
+  int iw = prog[i / nt];
+  int kb = g.lpw[iw];
+  int np = g.npoly[iw];
+  float fimpl = ff[(size_t)iw * nrk + istage - 1];
+  const float* wm = wmasc + (size_t)iw * mza;
+  const float* up = upw + (size_t)iw * mza * nt + t;
+  for (int kd = kb; kd < mza; ++kd) {
+    float s0 = scp0.base[((size_t)iw * mza + kd) * scp0.ld + scp0.t0 + t];
+    float fd = 0.f;
+    for (int n = 0; n < np; ++n) {
+      int iv = g.w_ev[iw * 8 + n];
+      if (kd < g.lpv[iv]) continue;
+      fd = fd + g.w_dirv[iw * 8 + n] * vmasc[(size_t)iv * mza + kd] *
+                    (upv[((size_t)iv * mza + kd) * nt + t] - s0);
+    }
+    float a = up[(size_t)(kd - 1) * nt], b = up[(size_t)kd * nt];
+    if (fimpl > .001f) {
+      float fexpl = 1.f - fimpl;
+      fd = fd + fexpl * (wm[kd - 1] * (a - s0) - wm[kd] * (b - s0));
+    } else {
+      fd = fd + wm[kd - 1] * (a - s0) - wm[kd] * (b - s0);
+    }
+    out.base[((size_t)iw * mza + kd) * out.ld + out.t0 + t] =
+        s0 + dtr * g.volti[(size_t)iw * mza + kd] * fd / rhos[(size_t)iw * mza + kd];
+  }
+  // scp(2:kb-1) = scp(kb) only in the explicit branch; level 1 keeps its value
+  if (!(fimpl > .001f)) {
+    float v = out.base[((size_t)iw * mza + kb) * out.ld + out.t0 + t];
+    for (int kd = 1; kd < kb; ++kd) out.base[((size_t)iw * mza + kd) * out.ld + out.t0 + t] = v;
+  }
+}
+
+void launch_tend(const DevGrid& d, const Transport& tp, CTView scp0, const float* rhos, TView out,
+                 int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s) {
+  size_t n = (size_t)d.nw_prog * nt;
+  k_tend<<<cdiv(n, 128), 128, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp0, rhos, tp.vmasc.p,
+                                      tp.wmasc.p, tp.ff.p, tp.upv.p, tp.upw.p, out, nt, istage, nrk, dtr,
+                                      mode);
+  OG_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// layout transposes.  q[(pk) * ntp + n] <-> src[n][pk], pk = point*mza + k.
+// 32x32 tiles through shared memory; both sides coalesced.
+// ---------------------------------------------------------------------------
+__global__ void k_gather_q(float* __restrict__ q, const float* const* __restrict__ src, int n, int ntp,
+                           size_t npk) {
+  __shared__ float tile[32][33];
+  size_t pk0 = (size_t)blockIdx.x * 32;
+  int n0 = blockIdx.y * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    int tr = n0 + r;
+    size_t pk = pk0 + tx;
+    float v = 0.f;
+    if (tr < n && pk < npk) v = src[tr][pk];
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    size_t pk = pk0 + r;
+    int tr = n0 + tx;
+    if (pk < npk && tr < ntp) q[pk * ntp + tr] = tile[tx][r];
+  }
+}
+
+__global__ void k_scatter_q(const float* __restrict__ q, float* const* __restrict__ dst, int n, int ntp,
+                            size_t npk) {
+  __shared__ float tile[32][33];
+  size_t pk0 = (size_t)blockIdx.x * 32;
+  int n0 = blockIdx.y * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;
+  for (int r = ty; r < 32; r += 8) {
+    size_t pk = pk0 + r;
+    int tr = n0 + tx;
+    float v = 0.f;
+    if (pk < npk && tr < ntp) v = q[pk * ntp + tr];
+    tile[tx][r] = v;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    int tr = n0 + r;
+    size_t pk = pk0 + tx;
+    if (tr < n && pk < npk) dst[tr][pk] = tile[r][tx];
+  }
+}
+
+void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npk, cudaStream_t s) {
+  dim3 grid(cdiv(npk, 32), cdiv(ntp, 32));
+  k_gather_q<<<grid, dim3(32, 8), 0, s>>>(q, src, n, ntp, npk);
+  OG_LAUNCHED();
+}
+
+void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npk, cudaStream_t s) {
+  dim3 grid(cdiv(npk, 32), cdiv(n, 32));
+  k_scatter_q<<<grid, dim3(32, 8), 0, s>>>(q, dst, n, ntp, npk);
+  OG_LAUNCHED();
+}
+
+}  // namespace olamgpu

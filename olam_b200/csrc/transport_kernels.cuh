@@ -1,0 +1,80 @@
+// transport_kernels.cuh -- kernel declarations and device helpers shared by
+// the transport translation units.
+#pragma once
+
+#include "internal.h"
+
+namespace olamgpu {
+
+// A tracer field: element (point p, level k, tracer t) lives at
+// base[((size_t)p * mza + k) * ld + t0 + t].  ld = 1, t0 = 0 is OLAM's own
+// (mza, n) layout of one tracer; ld = ntp is the batched layout.
+struct TView {
+  float* base;
+  int ld;
+  int t0;
+};
+
+struct CTView {
+  const float* base;
+  int ld;
+  int t0;
+};
+
+// Device-side grid pointers passed by value to kernels.
+struct GridK {
+  int mza, mwa, mva;
+  const int* __restrict__ npoly;
+  const int* __restrict__ w_nb;
+  const int* __restrict__ w_ev;
+  const float* __restrict__ w_dirv;
+  const int* __restrict__ v_iw;
+  const int* __restrict__ lpw;
+  const int* __restrict__ lpv;
+  const float* __restrict__ volti;
+  const float* __restrict__ a_w;   // Fortran (mza,2,2)
+  const float* __restrict__ a_wu;
+};
+
+GridK gridk(const DevGrid& d);
+
+// Per-tracer update mode on the last RK stage.
+enum { MODE_PLAIN = 0, MODE_MONOT = 1, MODE_PD = 2 };
+
+// ---- launchers (transport_kernels.cu) ------------------------------------
+void launch_check_cfls(const DevGrid& d, const Transport& tp, int nrk, float dtl,
+                       unsigned long long* red, cudaStream_t s);
+void launch_rhos(const DevGrid& d, Transport& tp, int nrk, cudaStream_t s);
+void launch_implicit_prep(const DevGrid& d, Transport& tp, int nrk, const float* dtlr,
+                          cudaStream_t s);
+void launch_implicit_solve(const DevGrid& d, const Transport& tp, int nrk, int istage, float dtr,
+                           CTView scp0, TView scp, int nt, cudaStream_t s);
+void launch_diffusion(const DevGrid& d, const Transport& tp, CTView scp, TView sct, int nt,
+                      cudaStream_t s);
+void launch_scp0_pd_update(const DevGrid& d, const Transport& tp, TView scp0, CTView sct,
+                           const int* mode, int nt, float dtr, cudaStream_t s);
+
+// reference-mirroring passes, generic tracer count nt
+void launch_grad(const DevGrid& d, CTView scp, float* gx, int nt, int order, bool bounded,
+                 cudaStream_t s);
+void launch_vflux(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, const float* gx,
+                  int nt, int order, bool unbounded, const int* mode, bool anylim, cudaStream_t s);
+void launch_wcol(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct,
+                 const float* rhos, TView out, int nt, int istage, int nrk, float dtr,
+                 const int* mode, bool anylim, cudaStream_t s);
+void launch_vapply(const DevGrid& d, const Transport& tp, int nt, const int* mode, cudaStream_t s);
+void launch_tend(const DevGrid& d, const Transport& tp, CTView scp0, const float* rhos, TView out,
+                 int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s);
+
+// fused batched update (plain mode), all tracers of the batched layout
+void launch_fused_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
+                        const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr,
+                        const float* rhos, cudaStream_t s);
+
+// layout transposes: per-tracer arrays <-> batched layout
+void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npts_k,
+                     cudaStream_t s);
+void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npts_k,
+                      cudaStream_t s);
+
+}  // namespace olamgpu

@@ -1,0 +1,178 @@
+"""Loader of libolamgpu.so and thin Python mirror of OLAM's hot-path interface.
+
+The product is the C-ABI library; this module is the host-side mirror of the
+reference interface (``init_wrtv_rk``, ``prog_wrtv_rk``,
+``scalar_transport_rk(rho_old)``) used by tests and benchmarks.  It loads the
+in-tree library and raises if it is missing or fails: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libolamgpu.so")
+_LIB = None
+
+# every entry point declared in include/olamgpu.h
+EXPORTS = [
+    "olamgpu_init", "olamgpu_register_scalars", "olamgpu_set_turb", "olamgpu_finalize",
+    "olamgpu_strerror", "olamgpu_set_coherence", "olamgpu_sync_to_device", "olamgpu_sync_to_host",
+    "olamgpu_set_transport_form", "olamgpu_scalar_transport_rk", "olamgpu_prog_wrtv_rk",
+    "olamgpu_tend0", "olamgpu_timeavg_momsc", "olamgpu_stream", "olamgpu_launch_count",
+    "olamgpu_profile", "olamgpu_profile_read",
+]
+
+
+class OlamGpuError(RuntimeError):
+    def __init__(self, rc, msg):
+        super().__init__(f"olamgpu status {rc}: {msg}")
+        self.rc = rc
+
+
+def load():
+    """Load the in-tree library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise OlamGpuError(-1, f"{LIB_PATH} not built; run __graft_entry__.build()")
+    lib = C.CDLL(LIB_PATH)
+    lib.olamgpu_init.argtypes = [C.POINTER(abi.Grid), C.POINTER(abi.Opts), C.POINTER(abi.State)]
+    lib.olamgpu_register_scalars.argtypes = [C.c_int, C.POINTER(abi.c_float_p),
+                                             C.POINTER(abi.c_float_p), abi.c_int_p, abi.c_int_p]
+    lib.olamgpu_set_turb.argtypes = [abi.c_float_p, abi.c_int_p]
+    lib.olamgpu_finalize.argtypes = []
+    lib.olamgpu_strerror.argtypes = [C.c_int]
+    lib.olamgpu_strerror.restype = C.c_char_p
+    lib.olamgpu_set_coherence.argtypes = [C.c_int]
+    lib.olamgpu_sync_to_device.argtypes = [C.c_uint]
+    lib.olamgpu_sync_to_host.argtypes = [C.c_uint]
+    lib.olamgpu_set_transport_form.argtypes = [C.c_int]
+    lib.olamgpu_scalar_transport_rk.argtypes = [abi.c_float_p, C.POINTER(abi.CflDiag)]
+    lib.olamgpu_prog_wrtv_rk.argtypes = [C.c_int]
+    lib.olamgpu_tend0.argtypes = [abi.c_float_p]
+    lib.olamgpu_timeavg_momsc.argtypes = []
+    lib.olamgpu_stream.restype = C.c_void_p
+    lib.olamgpu_launch_count.argtypes = [C.c_int]
+    lib.olamgpu_launch_count.restype = C.c_ulonglong
+    lib.olamgpu_profile.argtypes = [C.c_int, C.c_int]
+    lib.olamgpu_profile_read.argtypes = [C.c_int, C.c_char_p, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_ulonglong)]
+    for name in EXPORTS:
+        if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
+            getattr(lib, name).restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+def check(rc):
+    if rc != 0:
+        msg = load().olamgpu_strerror(rc).decode()
+        raise OlamGpuError(rc, msg)
+
+
+class HostState:
+    """OLAM module arrays (mem_basic / mem_tend) in Fortran layout."""
+
+    FIELDS32 = ("thil", "wc", "wmc", "vxe", "vye", "vze", "vmc", "vc", "vmasc", "wmasc",
+                "alpha_press", "pwfac", "pvfac", "thilt", "vmxet", "vmyet", "vmzet", "vmt")
+    FIELDS64 = ("rho", "press")
+
+    def __init__(self, **arrays):
+        self.arrays = {}
+        for k, v in arrays.items():
+            if v is None:
+                continue
+            dt = np.float64 if k in self.FIELDS64 else np.float32
+            self.arrays[k] = np.ascontiguousarray(v, dtype=dt)
+        s = abi.State()
+        for k in self.FIELDS32:
+            setattr(s, k, abi.ptr(self.arrays.get(k), C.c_float))
+        for k in self.FIELDS64:
+            setattr(s, k, abi.ptr(self.arrays.get(k), C.c_double))
+        self.struct = s
+
+    def __getitem__(self, k):
+        return self.arrays[k]
+
+
+class OlamGpu:
+    """Process-wide handle on the library context (one per process, as in OLAM)."""
+
+    def __init__(self, fgrid, opts, state: HostState | None = None):
+        self.lib = load()
+        self.fgrid, self.opts, self.state = fgrid, opts, state
+        check(self.lib.olamgpu_init(C.byref(fgrid.struct), C.byref(opts),
+                                    C.byref(state.struct) if state is not None else None))
+        self._scalars = None
+
+    # -- reference interface ----------------------------------------------------
+    def register_scalars(self, var_p, var_t, pdef=None, sgsmix=None):
+        """var_p / var_t: lists of (mwa, mza) float32 arrays OLAM owns."""
+        n = len(var_p)
+        self._scalars = (var_p, var_t)
+        pd = np.ascontiguousarray(pdef if pdef is not None else np.ones(n), dtype=np.int32)
+        sg = np.ascontiguousarray(sgsmix if sgsmix is not None else np.zeros(n), dtype=np.int32)
+        self._flags = (pd, sg)
+        check(self.lib.olamgpu_register_scalars(n, abi.ptr_array(var_p, C.c_float),
+                                                abi.ptr_array(var_t, C.c_float),
+                                                abi.ptr(pd, C.c_int), abi.ptr(sg, C.c_int)))
+
+    def scalar_transport_rk(self, rho_old=None, want_diag=False):
+        diag = abi.CflDiag()
+        rp = None if rho_old is None else np.ascontiguousarray(rho_old, dtype=np.float32)
+        check(self.lib.olamgpu_scalar_transport_rk(abi.ptr(rp, C.c_float), C.byref(diag)
+                                                   if want_diag else None))
+        return diag if want_diag else None
+
+    def prog_wrtv_rk(self, istp=1):
+        check(self.lib.olamgpu_prog_wrtv_rk(int(istp)))
+
+    def tend0(self, rho_old):
+        check(self.lib.olamgpu_tend0(abi.ptr(rho_old, C.c_float)))
+
+    def timeavg_momsc(self):
+        check(self.lib.olamgpu_timeavg_momsc())
+
+    # -- library controls --------------------------------------------------------
+    def set_coherence(self, mode):
+        check(self.lib.olamgpu_set_coherence(mode))
+
+    def set_transport_form(self, form):
+        check(self.lib.olamgpu_set_transport_form(form))
+
+    def sync_to_device(self, mask=abi.F_ALL):
+        check(self.lib.olamgpu_sync_to_device(mask))
+
+    def sync_to_host(self, mask=abi.F_ALL):
+        check(self.lib.olamgpu_sync_to_host(mask))
+
+    def stream(self):
+        return self.lib.olamgpu_stream()
+
+    def launch_count(self, reset=False):
+        return int(self.lib.olamgpu_launch_count(1 if reset else 0))
+
+    def profile(self, enable=True, reset=False):
+        check(self.lib.olamgpu_profile(1 if enable else 0, 1 if reset else 0))
+
+    def profile_read(self, maxn=64):
+        names = C.create_string_buffer(32 * maxn)
+        ms = (C.c_double * maxn)()
+        cnt = (C.c_ulonglong * maxn)()
+        n = self.lib.olamgpu_profile_read(maxn, names, ms, cnt)
+        if n < 0:
+            check(-n)
+        out = {}
+        for i in range(min(n, maxn)):
+            nm = names.raw[32 * i:32 * (i + 1)].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[i]), int(cnt[i]))
+        return out
+
+    def close(self):
+        check(self.lib.olamgpu_finalize())

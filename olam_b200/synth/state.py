@@ -227,3 +227,40 @@ def dynamics_state(g, jet_amp=35.0, kind="jet", t_sfc=300.0, lapse=6.5e-3,
     s.pwfac = np.broadcast_to(g.dzim, (g.mwa, g.mza)).astype(F32).copy()
     s.pvfac = (g.zfacit[None, :] * g.dniv[:, None]).astype(F32)
     return s
+
+
+def fast_lognormal_tracers(g, ntr, seed=2024, median=1.0e-8, sigma_ln=1.5,
+                           clip=(1.0e-12, 1.0e-6), zero_frac=0.1, zero_above=15000.0,
+                           dtype=np.float32, as_list=False):
+    """Large-case tracer fields: seeded lognormal mixing ratios, separable in
+    horizontal and vertical so that 100+ full-size fields generate quickly.
+
+    q_n(iw, k) = median * exp(sigma * (h_n(iw) + v_n(k))) clipped to ``clip``;
+    ``zero_frac`` of the tracers are zero above ``zero_above`` metres.
+    Returns (ntr, mwa, mza) in ``dtype``, or with ``as_list`` a list of
+    separately allocated (mwa, mza) arrays (one allocation per tracer, as
+    OLAM allocates each scalar_tab(n)%var_p).
+    """
+    rng = np.random.default_rng(seed)
+    lat, lon = _latlon(g)
+    zt = g.zt.astype(np.float64)
+    out = ([np.empty((g.mwa, g.mza), dtype=dtype) for _ in range(ntr)] if as_list
+           else np.empty((ntr, g.mwa, g.mza), dtype=dtype))
+    nz = int(round(zero_frac * ntr))
+    zsel = set(rng.choice(ntr, nz, replace=False).tolist()) if nz else set()
+    above = zt > zero_above
+    for n in range(ntr):
+        a = rng.uniform(0, 2 * np.pi, 3)
+        m1, m2 = rng.integers(1, 6, 2)
+        h = np.sin(m1 * lon + a[0]) * np.cos(m2 * lat + a[1]) + 0.3 * rng.standard_normal(g.mwa)
+        v = 0.5 * np.sin(2 * np.pi * zt / rng.uniform(5e3, 3e4) + a[2])
+        eh = (median * np.exp(sigma_ln * h / 1.2)).astype(np.float32)
+        ev = np.exp(sigma_ln * v / 1.2).astype(np.float32)
+        q = out[n]
+        np.multiply(eh[:, None], ev[None, :], out=q)
+        np.clip(q, clip[0], clip[1], out=q)
+        if n in zsel:
+            q[:, above] = 0.0
+        q[0] = 0.0
+        q[:, 0] = q[:, 1]
+    return out

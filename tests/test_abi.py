@@ -1,0 +1,49 @@
+"""CPU checks of the C-ABI library: it loads, exports every entry point the
+header declares, and reports errors without a GPU (no compute calls)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from olam_b200 import abi, lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "olamgpu.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(olamgpu_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_header_symbols():
+    L = lib.load()
+    names = _declared()
+    assert names, "header parse found no entry points"
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(names) == set(lib.EXPORTS)
+
+
+def test_struct_sizes_match_header():
+    # field counts of the ctypes mirror follow the header's declarations
+    txt = open(os.path.join(ROOT, "include", "olamgpu.h")).read()
+    assert "typedef struct olamgpu_grid" in txt
+    assert C.sizeof(abi.CflDiag) == 36
+
+
+def test_strerror_and_state_errors():
+    L = lib.load()
+    assert L.olamgpu_strerror(0) == b"ok"
+    assert b"unsupported" in L.olamgpu_strerror(3)
+    # hot-path calls before init are state errors, not crashes
+    rc = L.olamgpu_scalar_transport_rk(None, None)
+    assert rc == abi.E_STATE
+    assert L.olamgpu_sync_to_host(abi.F_ALL) == abi.E_STATE
+    assert L.olamgpu_set_coherence(7) == abi.E_ARG
+
+
+def test_null_arguments_rejected():
+    L = lib.load()
+    assert L.olamgpu_init(None, None, None) == abi.E_ARG
