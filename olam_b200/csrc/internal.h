@@ -25,6 +25,23 @@
 
 #define OLAMGPU_MAXNB 8  // padded neighbour count per W point (OLAM allows 7)
 
+// Column record of the fused transport kernel (32-bit words; floats stored
+// by bit pattern).  Built once at set-up for every prognostic column.
+#define COLREC_IW 0     // 0-based W index
+#define COLREC_NP 1     // npoly
+#define COLREC_KB 2     // lowest prognosed level (0-based)
+#define COLREC_FAST 3   // 1: hexagon whose neighbours share the usual 3 cells
+#define COLREC_NB 4     // [7] neighbour W points
+#define COLREC_EV 11    // [7] faces
+#define COLREC_OWN 18   // [7] side index (0/1) of this column on each face
+#define COLREC_LPV 25   // [7] lowest level of each face (0-based)
+#define COLREC_DV 32    // [7] dirv (float)
+#define COLREC_WOWN 39  // [7][7] own-side folded weights over nb (float)
+#define COLREC_WU 88    // [6][7] far-side weights: c, nb[n-1], nb[n+1], new0..3 (float)
+#define COLREC_NEW 130  // [6][3] far-side further neighbours
+#define COLREC_NNEW 148 // [6] count of further neighbours
+#define COLREC_WORDS 160
+
 namespace olamgpu {
 
 // ---- error handling ---------------------------------------------------------
@@ -102,6 +119,8 @@ struct DevGrid {
   DevBuf<int> m_iv, m_iw, m_im;  // (mma, 3) 0-based
   DevBuf<int> lpw, lpv, lpm;     // 0-based lowest prognosed level
   DevBuf<int> iwglobe;
+  DevBuf<int> w_nonprog;         // W points outside jtw_prog (0-based)
+  int n_nonprog = 0;
   // reconstruction coefficients (float, OLAM layouts)
   DevBuf<float> gxc, gyc;        // (mwa, 7)
   DevBuf<float> xy_h, xy_hu;     // (mwa, 7, 5)
@@ -116,6 +135,7 @@ struct DevGrid {
   //  terms xx0_v.. with xy_h the same way).  Bounded and unbounded sets.
   DevBuf<float> ew_b, ew_u;      // (mva, 2, 8)
   int ew_order = 0;
+  DevBuf<int> colrec;            // (nw_prog, COLREC_WORDS) fused-kernel column records
   std::vector<int> h_lpw;        // host copies used at set-up
 };
 

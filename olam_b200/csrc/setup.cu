@@ -59,6 +59,16 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
   if (g->jtm_prog && g->nm_prog > 0)
     OG_CHECK(upload_list(d.jtm_prog, g->jtm_prog, g->nm_prog, mma, "jtm_prog", s));
 
+  {
+    std::vector<char> isprog(mwa, 0);
+    for (int j = 0; j < g->nw_prog; ++j) isprog[g->jtw_prog[j] - 1] = 1;
+    std::vector<int> np_list;
+    for (int i = 0; i < mwa; ++i) if (!isprog[i]) np_list.push_back(i);
+    d.n_nonprog = (int)np_list.size();
+    if (!np_list.empty()) OG_CHECK(upload(d.w_nonprog, np_list.data(), np_list.size(), s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+
   // itab_w: npoly in [3,7]; indices checked for the first npoly entries
   std::vector<int> npoly(mwa), nb((size_t)mwa * 8), ev((size_t)mwa * 8), im((size_t)mwa * 8, 0);
   std::vector<float> dirv((size_t)mwa * 8, 0.f);
@@ -203,6 +213,69 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
   OG_CHECK(upload(d.ew_u, wu.data(), wu.size(), s));
   OG_CUDA(cudaStreamSynchronize(s));
   d.ew_order = order;
+
+  // Per-column records of the fused kernel (layout in internal.h, COLREC_*).
+  // For a hexagonal column c the cell u across face n shares c and the two
+  // faces' neighbours nb[n-1], nb[n+1] with c's own list, so the upwind
+  // reconstruction on u's side needs only npoly(u) - 3 further rows; their
+  // indices and all folded weights are stored here.
+  const int nprog = g->nw_prog;
+  std::vector<int> rec((size_t)nprog * COLREC_WORDS, 0);
+  auto fbits = [](float f) { int i; std::memcpy(&i, &f, 4); return i; };
+  for (int j = 0; j < nprog; ++j) {
+    int* r = &rec[(size_t)j * COLREC_WORDS];
+    const int c = g->jtw_prog[j] - 1;
+    const int np = g->npoly[c];
+    r[COLREC_IW] = c;
+    r[COLREC_NP] = np;
+    r[COLREC_KB] = g->lpw[c] - 1;
+    bool fast = (np == 6);
+    int nbc[7], evc[7];
+    for (int n = 0; n < np; ++n) {
+      nbc[n] = g->itab_w_iw[(size_t)c * 7 + n] - 1;
+      evc[n] = g->itab_w_iv[(size_t)c * 7 + n] - 1;
+    }
+    for (int n = 0; n < 7; ++n) {
+      const bool v = n < np;
+      const int iv = v ? evc[n] : 0;
+      const int own = v ? ((g->itab_v_iw[(size_t)iv * 2] - 1 == c) ? 0 : 1) : 0;
+      r[COLREC_NB + n] = v ? nbc[n] : c;
+      r[COLREC_EV + n] = iv;
+      r[COLREC_OWN + n] = own;
+      r[COLREC_LPV + n] = v ? g->lpv[iv] - 1 : 0;
+      r[COLREC_DV + n] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + n] : 0.f);
+      for (int m = 0; m < 7; ++m)
+        r[COLREC_WOWN + n * 7 + m] = fbits(v && m < np ? wb[((size_t)iv * 2 + own) * 8 + m] : 0.f);
+    }
+    for (int n = 0; n < 6 && fast; ++n) {
+      const int u = nbc[n], iv = evc[n];
+      const int own = r[COLREC_OWN + n];
+      const int su = 1 - own;  // u's side of face n
+      const int prev = nbc[(n + np - 1) % np], next = nbc[(n + 1) % np];
+      float wc = 0.f, wp = 0.f, wn = 0.f, wnew[4] = {0.f, 0.f, 0.f, 0.f};
+      int nidx[4] = {c, c, c, c}, nn = 0, hits = 0;
+      const int npu = g->npoly[u];
+      for (int m = 0; m < npu; ++m) {
+        const int x = g->itab_w_iw[(size_t)u * 7 + m] - 1;
+        const float w = wb[((size_t)iv * 2 + su) * 8 + m];
+        if (x == c) { wc = w; ++hits; }
+        else if (x == prev) { wp = w; ++hits; }
+        else if (x == next) { wn = w; ++hits; }
+        else if (nn < 3) { wnew[nn] = w; nidx[nn] = x; ++nn; }
+        else { fast = false; }
+      }
+      if (hits != 3) fast = false;
+      r[COLREC_WU + n * 7 + 0] = fbits(wc);
+      r[COLREC_WU + n * 7 + 1] = fbits(wp);
+      r[COLREC_WU + n * 7 + 2] = fbits(wn);
+      for (int q = 0; q < 4; ++q) r[COLREC_WU + n * 7 + 3 + q] = fbits(q < 3 ? wnew[q] : 0.f);
+      for (int q = 0; q < 3; ++q) r[COLREC_NEW + n * 3 + q] = nidx[q];
+      r[COLREC_NNEW + n] = nn;
+    }
+    r[COLREC_FAST] = fast ? 1 : 0;
+  }
+  OG_CHECK(upload(d.colrec, rec.data(), rec.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));
   return OLAMGPU_OK;
 }
 

@@ -121,7 +121,7 @@ static void passes_stage(Context& C, CTView in, CTView scp0, CTView sct, TView o
   { OG_PROF("pass_wcol", s); launch_wcol(d, C.tp, in, scp0, sct, rhos, out, nt, istage, nrk, dtr, mode, limited_stage, s); }
   if (limited_stage) {
     { OG_PROF("pass_vapply", s); launch_vapply(d, C.tp, nt, mode, s); }
-    { OG_PROF("pass_tend", s); launch_tend(d, C.tp, scp0, rhos, out, nt, istage, nrk, dtr, mode, s); }
+    { OG_PROF("pass_tend", s); launch_tend(d, C.tp, in, scp0, rhos, out, nt, istage, nrk, dtr, mode, s); }
   }
 }
 
@@ -160,8 +160,22 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     if (C.hstate.wc) OG_CHECK(upload(tp.wc, C.hstate.wc, wz, s));
     OG_CHECK(upload(tp.rho_old, rho_old_host, wz, s));
     OG_CHECK(tracers_to_device(s));
-  } else if (rho_old_host) {
-    OG_CHECK(upload(tp.rho_old, rho_old_host, wz, s));
+  } else {
+    // RESIDENT: device copies persist; a field never uploaded is taken from
+    // the registered host array on first use
+    if (!tp.vmasc.p) OG_CHECK(upload(tp.vmasc, C.hstate.vmasc, vz, s));
+    if (!tp.wmasc.p) OG_CHECK(upload(tp.wmasc, C.hstate.wmasc, wz, s));
+    if (!tp.rho.p) OG_CHECK(upload(tp.rho, C.hstate.rho, wz, s));
+    if (!tp.wc.p && C.hstate.wc) OG_CHECK(upload(tp.wc, C.hstate.wc, wz, s));
+    if (rho_old_host) OG_CHECK(upload(tp.rho_old, rho_old_host, wz, s));
+    if (!tp.rho_old.p) {
+      set_error("rho_old is NULL and no device copy exists (pass it once or call olamgpu_tend0)");
+      return OLAMGPU_E_STATE;
+    }
+  }
+  if (!tp.vmasc.p || !tp.wmasc.p || !tp.rho.p || !tp.rho_old.p) {
+    set_error("transport inputs missing on the device");
+    return OLAMGPU_E_STATE;
   }
   OG_CHECK(tp.rhos.alloc((size_t)nrk * wz));
   OG_CHECK(tp.ff.alloc((size_t)nrk * mwa));
@@ -229,6 +243,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
       out_b = (out_b + 1) % 3;
       if (out_b == a) out_b = (out_b + 1) % 3;
     }
+    launch_copy_cols(d.w_nonprog.p, d.n_nonprog, A, tr.q[in_b].p, (size_t)mza * ntp, s);
     tr.qcur = in_b;
     tr.q_valid = true;
   } else {
@@ -257,6 +272,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
         ob ^= 1;
       }
       // the final stage output becomes the tracer's device array
+      launch_copy_cols(d.w_nonprog.p, d.n_nonprog, A, tp.plain_out[ob ^ 1].p, (size_t)mza, s);
       std::swap(tr.p[n], tp.plain_out[ob ^ 1]);
     }
   }

@@ -4,28 +4,33 @@
 // Restates, fused into one pass, omodel/scalar_transport_rk.F90:
 //   grad_t2d / grad_t2d_quadratic (grad_lib.f90:236-341)   horizontal reconstruction
 //   scalar_v_column (474-534)                              upwind V-face value
+//   grad_z_quadratic (grad_lib.f90:166-229),
 //   scalar_w_column (537-612)                              vertical reconstruction,
 //                                                          flux divergence, update
-// Work mapping: one warp per prognostic column, lane = 4 consecutive tracers
-// (one float4), loop over levels bottom to top.  The upwind side of a V face
-// depends only on sign(vmasc(k,iv)), which is the same for every tracer, so
-// a warp evaluates only the side it needs.  The reconstruction on side s of
-// face iv is S(c) + sum_n ew[iv][s][n] * (S(nb_n(c)) - S(c)), the gradient
-// (or quadratic) coefficients pre-multiplied by the face offsets at set-up;
-// the intermediate gradient planes and face values of the reference never
-// touch memory.  The column's own values k-1..k+2 stay in registers as a
-// sliding window for the vertical quadratic reconstruction.  Winds, density,
-// volumes and tables are loaded once per (column, level) and applied to all
-// tracers held by the warp.
+// Work mapping.  A block owns one prognostic column and a chunk of KC levels;
+// LPI lanes compute one (column, level) cell for every tracer, a lane
+// holding 2 consecutive tracers (one float2) per pass.  Cells are independent, so
+// there is no sequential chain over levels: latency is hidden by the many
+// warps in flight.  The column's tables (neighbours, faces, directions, the
+// folded reconstruction weights of both sides of each face and the
+// neighbour lists of the upwind neighbours) are staged once per block in
+// shared memory.
+//
+// The upwind side of a V face depends only on sign(vmasc(k,iv)), the same
+// for every tracer, so a warp evaluates only the side it needs.  The value
+// on side s of face iv is S(c) + sum_n ew[iv][s][n] * (S(nb_n(c)) - S(c)):
+// the gradient (order 2) or quadratic (order 3) coefficients pre-multiplied
+// by the face offsets at set-up, so the reference's gradient planes and
+// face arrays never touch memory.
 //
 // HBM traffic per tracer and cell (ideal): read S, S0, SCT, write OUT = 16 B;
-// neighbour rows are re-read from L1/L2.
+// neighbour and vertical rows are re-read from L1/L2.
 #include "transport_kernels.cuh"
 
 namespace olamgpu {
 
 struct FusedArgs {
-  int mza, nprog, nq, nrk, istage;
+  int mza, nprog, nq, nrk, istage, nchunk;
   float dtr;
   const int* __restrict__ prog;
   const int* __restrict__ npoly;
@@ -42,149 +47,190 @@ struct FusedArgs {
   const float* __restrict__ wmasc;
   const float* __restrict__ rhos;   // rhos(:,:,nrk)
   const float* __restrict__ ff;     // (mwa, nrk)
+  const int* __restrict__ colrec;   // (nprog, COLREC_WORDS)
   const float4* __restrict__ S;
   const float4* __restrict__ S0;
   const float4* __restrict__ SCT;
   float4* __restrict__ OUT;
 };
 
-__device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); }
-__device__ __forceinline__ float4 operator-(float4 a, float4 b) {
-  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// a + w * b
+__device__ __forceinline__ float2 axpy2(float2 a, float w, float2 b) {
+  return make_float2(a.x + w * b.x, a.y + w * b.y);
 }
-__device__ __forceinline__ float4 operator+(float4 a, float4 b) {
-  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
-}
-__device__ __forceinline__ float4 operator*(float a, float4 b) {
-  return make_float4(a * b.x, a * b.y, a * b.z, a * b.w);
-}
-// a + w * b, evaluated as the Fortran writes it (the compiler may fuse)
-__device__ __forceinline__ float4 axpy(float4 a, float w, float4 b) {
-  return make_float4(a.x + w * b.x, a.y + w * b.y, a.z + w * b.z, a.w + w * b.w);
+__device__ __forceinline__ float2 ld2(const float2* p) { return __ldg(p); }
+
+#define FUSED_NB 7
+#define FUSED_KC 16
+#define FUSED_THREADS 256
+#ifndef FUSED_MINB
+#define FUSED_MINB 2  // 2 blocks of 256 threads per SM: up to 128 registers
+#endif
+
+
+// grad_z_quadratic (bounded, zero-gradient BCs) at level lev from rows
+// a = S(lev-1), b = S(lev), c = S(lev+1); returns the bottom (want_bot) or
+// top face value of level lev.
+__device__ __forceinline__ float2 zface(const float* __restrict__ a_w, int mza, int kb, int lev,
+                                        bool want_bot, float2 a, float2 b, float2 c) {
+  const bool top = (lev > mza - 2), bot = (lev < kb + 1);
+  const float c1 = __ldg(a_w + lev + (want_bot ? 0 : 2 * mza));       // a_w(k,1,1|2)
+  const float c2 = __ldg(a_w + lev + (want_bot ? mza : 3 * mza));     // a_w(k,2,1|2)
+  float2 r;
+  float dsk = top ? 0.f : (c.x - b.x), dskm1 = bot ? 0.f : (b.x - a.x);
+  r.x = b.x + dsk * c1 + dskm1 * c2;
+  dsk = top ? 0.f : (c.y - b.y); dskm1 = bot ? 0.f : (b.y - a.y);
+  r.y = b.y + dsk * c1 + dskm1 * c2;
+  return r;
 }
 
-__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
-
-#define FUSED_MAXNB 7
-
-template <int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_fused(FusedArgs A) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int j = blockIdx.x * WPB + warp;
-  if (j >= A.nprog) return;
+// LPI lanes cooperate on one (column, level) cell, each lane holding one
+// float2 (2 tracers) per pass; a block covers KC levels of one column.
+// Loads of a cell are issued in two rounds: everything whose address is
+// known (own column, neighbours, scp0, tendency, winds), then the far-side
+// rows of the inflow faces, whose choice depends on sign(vmasc).
+template <int LPI>
+__global__ void __launch_bounds__(FUSED_THREADS, FUSED_MINB) k_fused(FusedArgs A) {
+  __shared__ int R[COLREC_WORDS];
+  const int j = blockIdx.x / A.nchunk;
+  const int chunk = blockIdx.x - j * A.nchunk;
   const int mza = A.mza;
-  const int iw = A.prog[j];
-  const int np = A.npoly[iw];
-  const int kb = A.lpw[iw];
-  int nb[FUSED_MAXNB], ev[FUSED_MAXNB], own[FUSED_MAXNB];
-  float dv[FUSED_MAXNB];
-#pragma unroll
-  for (int n = 0; n < FUSED_MAXNB; ++n) {
-    nb[n] = A.w_nb[iw * 8 + n];
-    ev[n] = A.w_ev[iw * 8 + n];
-    dv[n] = A.w_dirv[iw * 8 + n];
-    own[n] = (n < np) ? (A.v_iw[ev[n] * 2] == iw ? 0 : 1) : 0;
-  }
-  const float fexpl = 1.0f - A.ff[(size_t)iw * A.nrk + A.istage - 1];
-  const float* wm = A.wmasc + (size_t)iw * mza;
-  const int nq = A.nq;
-  const size_t rowstride = (size_t)nq;  // float4 per (point, level) row
+  for (int i = threadIdx.x; i < COLREC_WORDS; i += FUSED_THREADS)
+    R[i] = __ldg(A.colrec + (size_t)j * COLREC_WORDS + i);
+  __syncthreads();
+  const int iw = R[COLREC_IW], np = R[COLREC_NP], kb = R[COLREC_KB];
+  const bool fast = R[COLREC_FAST] != 0;
+  const float fexpl = 1.0f - __ldg(A.ff + (size_t)iw * A.nrk + A.istage - 1);
+  const float* __restrict__ wm = A.wmasc + (size_t)iw * mza;
+  const int nq2 = A.nq * 2;                  // float2 per (point, level) row
+  const float2* __restrict__ S = reinterpret_cast<const float2*>(A.S);
+  const float2* __restrict__ S0 = reinterpret_cast<const float2*>(A.S0);
+  const float2* __restrict__ SCT = reinterpret_cast<const float2*>(A.SCT);
+  float2* __restrict__ OUT = reinterpret_cast<float2*>(A.OUT);
+  const size_t colsz = (size_t)mza * nq2;
+  const size_t cbase = (size_t)iw * colsz;
+  constexpr int IPP = FUSED_THREADS / LPI;   // cells per pass
+  const int sub = threadIdx.x / LPI, lane = threadIdx.x % LPI;
+  // weights are re-read from shared memory at each use (a broadcast LDS)
+  // instead of being hoisted into registers across the level loop
+  const volatile int* RV = R;
+  auto RF = [&](int i) { return __int_as_float(RV[i]); };
 
-  for (int q0 = 0; q0 < nq; q0 += 32) {
-    const int q = q0 + lane;
-    if (q >= nq) break;
-    auto row = [&](int p, int kd) { return ((size_t)p * mza + kd) * rowstride + q; };
-    float4 sm1 = f4(0.f);
-    float4 s0 = ld4(A.S + row(iw, kb));
-    float4 sp1 = (kb + 1 < mza) ? ld4(A.S + row(iw, kb + 1)) : f4(0.f);
-    float4 sp2 = (kb + 2 < mza) ? ld4(A.S + row(iw, kb + 2)) : f4(0.f);
-    float4 up_prev = s0;  // scp_upw(kb-1) = scp(kb)
-    float4 out_kb = f4(0.f);
-    for (int kd = kb; kd < mza; ++kd) {
-      // ---- vertical upwind face value at the top of level kd
-      float4 up;
-      if (kd <= mza - 2) {
-        const float wk = __ldg(wm + kd);
-        int lev;
-        float4 a, b, c;
-        if (wk < 0.f) { lev = kd + 1; a = s0; b = sp1; c = sp2; }   // scpb(k+1)
-        else          { lev = kd;     a = sm1; b = s0; c = sp1; }   // scpt(k)
-        float dsk, dskm1;
-        const bool top = (lev > mza - 2), bot = (lev < kb + 1);
-        const float a11 = __ldg(A.a_w + lev), a21 = __ldg(A.a_w + lev + mza);
-        const float a12 = __ldg(A.a_w + lev + 2 * mza), a22 = __ldg(A.a_w + lev + 3 * mza);
-        const float c1 = (wk < 0.f) ? a11 : a12;
-        const float c2 = (wk < 0.f) ? a21 : a22;
-        float4 r;
-#define ZC(comp)                                              \
-  dsk = top ? 0.f : (c.comp - b.comp);                        \
-  dskm1 = bot ? 0.f : (b.comp - a.comp);                      \
-  r.comp = b.comp + dsk * c1 + dskm1 * c2;
-        ZC(x) ZC(y) ZC(z) ZC(w)
-#undef ZC
-        up = r;
-      } else {
-        up = s0;  // scp_upw(mza) = scp(mza)
-      }
-      // ---- horizontal flux divergence over the V faces of this column
-      float4 sn[FUSED_MAXNB];
+  for (int kk = sub; kk < FUSED_KC; kk += IPP) {
+    const int kd = chunk * FUSED_KC + kk;
+    if (kd < kb || kd >= mza) continue;
+    const float wkm1 = __ldg(wm + kd - 1), wk0 = __ldg(wm + kd);
+    const float vt = __ldg(A.volti + (size_t)iw * mza + kd);
+    const float rh = __ldg(A.rhos + (size_t)iw * mza + kd);
+    float vm[FUSED_NB];
+    bool inflow[FUSED_NB];
 #pragma unroll
-      for (int n = 0; n < FUSED_MAXNB; ++n)
-        if (n < np) sn[n] = ld4(A.S + row(nb[n], kd));
-      const float4 s00 = ld4(A.S0 + row(iw, kd));
-      float4 fd = f4(0.f);
-#pragma unroll
-      for (int n = 0; n < FUSED_MAXNB; ++n) {
-        if (n >= np) break;
-        const int iv = ev[n];
-        if (kd < __ldg(A.lpv + iv)) continue;
-        const float vm = __ldg(A.vmasc + (size_t)iv * mza + kd);
-        const int sd = (vm < 0.f) ? 1 : 0;
-        const float* w = A.ew + ((size_t)iv * 2 + sd) * 8;
-        float4 val;
-        if (sd == own[n]) {
-          val = s0;
-#pragma unroll
-          for (int m = 0; m < FUSED_MAXNB; ++m)
-            if (m < np) val = axpy(val, __ldg(w + m), sn[m] - s0);
-        } else {
-          const int u = nb[n];
-          const int npu = __ldg(A.npoly + u);
-          const float4 su = sn[n];
-          val = su;
-          for (int m = 0; m < npu; ++m) {
-            const int um = __ldg(A.w_nb + u * 8 + m);
-            float4 sx = (um == iw) ? s0 : ld4(A.S + row(um, kd));
-            val = axpy(val, __ldg(w + m), sx - su);
-          }
-        }
-        const float f = dv[n] * vm;
-        fd = axpy(fd, f, val - s00);
-      }
-      // ---- vertical flux divergence and update
-      const float wkm1 = __ldg(wm + kd - 1), wk0 = __ldg(wm + kd);
-      float4 vz;
-      vz.x = fexpl * (wkm1 * (up_prev.x - s00.x) - wk0 * (up.x - s00.x));
-      vz.y = fexpl * (wkm1 * (up_prev.y - s00.y) - wk0 * (up.y - s00.y));
-      vz.z = fexpl * (wkm1 * (up_prev.z - s00.z) - wk0 * (up.z - s00.z));
-      vz.w = fexpl * (wkm1 * (up_prev.w - s00.w) - wk0 * (up.w - s00.w));
-      fd = fd + vz;
-      const float4 st = ld4(A.SCT + row(iw, kd));
-      const float vt = __ldg(A.volti + (size_t)iw * mza + kd);
-      const float rh = __ldg(A.rhos + (size_t)iw * mza + kd);
-      const float dtr = A.dtr;
-      float4 o;
-      o.x = s00.x + dtr * (st.x + vt * fd.x) / rh;
-      o.y = s00.y + dtr * (st.y + vt * fd.y) / rh;
-      o.z = s00.z + dtr * (st.z + vt * fd.z) / rh;
-      o.w = s00.w + dtr * (st.w + vt * fd.w) / rh;
-      A.OUT[row(iw, kd)] = o;
-      if (kd == kb) out_kb = o;
-      up_prev = up;
-      sm1 = s0; s0 = sp1; sp1 = sp2;
-      sp2 = (kd + 3 < mza) ? ld4(A.S + row(iw, kd + 3)) : f4(0.f);
+    for (int n = 0; n < FUSED_NB; ++n) {
+      vm[n] = (n < np) ? __ldg(A.vmasc + (size_t)R[COLREC_EV + n] * mza + kd) : 0.f;
+      // the upwind side of face n is not this column's side
+      inflow[n] = (n < np) && (kd >= R[COLREC_LPV + n]) && (((vm[n] < 0.f) ? 1 : 0) != R[COLREC_OWN + n]);
     }
-    for (int kd = 0; kd < kb; ++kd) A.OUT[row(iw, kd)] = out_kb;
+    const size_t lvl = (size_t)kd * nq2;
+
+    for (int q = lane; q < nq2; q += LPI) {
+      const float2* Sc = S + cbase + lvl + q;            // S(iw, kd, q)
+      // ---- round 1: rows with known addresses
+      const float2 s0 = ld2(Sc);
+      const float2 sm1 = (kd - 1 >= kb) ? ld2(Sc - nq2) : s0;
+      const float2 sp1 = (kd + 1 < mza) ? ld2(Sc + nq2) : s0;
+      const float2 sm2 = (kd - 2 >= kb) ? ld2(Sc - 2 * nq2) : sm1;
+      const float2 sp2 = (kd + 2 < mza) ? ld2(Sc + 2 * nq2) : sp1;
+      float2 sn[FUSED_NB];
+#pragma unroll
+      for (int n = 0; n < FUSED_NB; ++n)
+        if (n < np) sn[n] = ld2(S + (size_t)R[COLREC_NB + n] * colsz + lvl + q);
+      const float2 s00 = ld2(S0 + cbase + lvl + q);
+      const float2 st = ld2(SCT + cbase + lvl + q);
+      float2 fd = make_float2(0.f, 0.f);
+      if (fast) {
+        // ---- round 2: far-side rows of the inflow faces
+        float2 nw[6][3];
+#pragma unroll
+        for (int n = 0; n < 6; ++n)
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+            if (inflow[n] && m < R[COLREC_NNEW + n])
+              nw[n][m] = ld2(S + (size_t)R[COLREC_NEW + n * 3 + m] * colsz + lvl + q);
+        float2 dn[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) dn[m] = sub2(sn[m], s0);
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+          if (kd < R[COLREC_LPV + n]) continue;
+          float2 val;
+          if (!inflow[n]) {
+            val = s0;
+#pragma unroll
+            for (int m = 0; m < 6; ++m) val = axpy2(val, RF(COLREC_WOWN + n * 7 + m), dn[m]);
+          } else {
+            const float2 su = sn[n];
+            val = su;
+            val = axpy2(val, RF(COLREC_WU + n * 7 + 0), sub2(s0, su));
+            val = axpy2(val, RF(COLREC_WU + n * 7 + 1), sub2(sn[(n + 5) % 6], su));
+            val = axpy2(val, RF(COLREC_WU + n * 7 + 2), sub2(sn[(n + 1) % 6], su));
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+              if (m < R[COLREC_NNEW + n]) val = axpy2(val, RF(COLREC_WU + n * 7 + 3 + m), sub2(nw[n][m], su));
+          }
+          fd = axpy2(fd, RF(COLREC_DV + n) * vm[n], sub2(val, s00));
+        }
+      } else {
+        // general polygons (the 12 pentagons of the icosahedral grid)
+        float2 dn[FUSED_NB];
+#pragma unroll
+        for (int m = 0; m < FUSED_NB; ++m)
+          if (m < np) dn[m] = sub2(sn[m], s0);
+#pragma unroll
+        for (int n = 0; n < FUSED_NB; ++n) {
+          if (n >= np || kd < R[COLREC_LPV + n]) continue;
+          float2 val;
+          if (!inflow[n]) {
+            val = s0;
+#pragma unroll
+            for (int m = 0; m < FUSED_NB; ++m)
+              if (m < np) val = axpy2(val, RF(COLREC_WOWN + n * 7 + m), dn[m]);
+          } else {
+            const int u = R[COLREC_NB + n];
+            const int iv = R[COLREC_EV + n];
+            const float* w = A.ew + ((size_t)iv * 2 + (1 - R[COLREC_OWN + n])) * 8;
+            const float2 su = sn[n];
+            val = su;
+            const int npu = __ldg(A.npoly + u);
+            for (int m = 0; m < npu; ++m) {
+              const int um = __ldg(A.w_nb + u * 8 + m);
+              const float2 sx = (um == iw) ? s0 : ld2(S + (size_t)um * colsz + lvl + q);
+              val = axpy2(val, __ldg(w + m), sub2(sx, su));
+            }
+          }
+          fd = axpy2(fd, RF(COLREC_DV + n) * vm[n], sub2(val, s00));
+        }
+      }
+      // ---- vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded)
+      float2 up_lo, up_hi;
+      if (kd == kb) up_lo = s0;                                                   // scp_upw(kb-1) = scp(kb)
+      else if (wkm1 < 0.f) up_lo = zface(A.a_w, mza, kb, kd, true, sm1, s0, sp1);        // scpb(kd)
+      else up_lo = zface(A.a_w, mza, kb, kd - 1, false, sm2, sm1, s0);                   // scpt(kd-1)
+      if (kd == mza - 1) up_hi = s0;                                              // scp_upw(mza) = scp(mza)
+      else if (wk0 < 0.f) up_hi = zface(A.a_w, mza, kb, kd + 1, true, s0, sp1, sp2);     // scpb(kd+1)
+      else up_hi = zface(A.a_w, mza, kb, kd, false, sm1, s0, sp1);                       // scpt(kd)
+      // ---- vertical flux divergence and update
+      float2 o;
+      {
+        float v = fexpl * (wkm1 * (up_lo.x - s00.x) - wk0 * (up_hi.x - s00.x));
+        o.x = s00.x + A.dtr * (st.x + vt * (fd.x + v)) / rh;
+        v = fexpl * (wkm1 * (up_lo.y - s00.y) - wk0 * (up_hi.y - s00.y));
+        o.y = s00.y + A.dtr * (st.y + vt * (fd.y + v)) / rh;
+      }
+      OUT[cbase + lvl + q] = o;
+      if (kd == kb)
+        for (int k2 = 0; k2 < kb; ++k2) OUT[cbase + (size_t)k2 * nq2 + q] = o;
+    }
   }
 }
 
@@ -193,16 +239,30 @@ void launch_fused_stage(const DevGrid& d, const Transport& tp, const float* S, c
                         const float* rhos, cudaStream_t s) {
   FusedArgs A;
   A.mza = d.mza; A.nprog = d.nw_prog; A.nq = ntp / 4; A.nrk = nrk; A.istage = istage; A.dtr = dtr;
+  A.nchunk = (d.mza + FUSED_KC - 1) / FUSED_KC;
   A.prog = d.jtw_prog.p; A.npoly = d.npoly.p; A.w_nb = d.w_nb.p; A.w_ev = d.w_ev.p;
   A.w_dirv = d.w_dirv.p; A.v_iw = d.v_iw.p; A.lpw = d.lpw.p; A.lpv = d.lpv.p;
   A.ew = d.ew_b.p; A.a_w = d.a_w.p; A.volti = d.volti.p;
   A.vmasc = tp.vmasc.p; A.wmasc = tp.wmasc.p; A.rhos = rhos; A.ff = tp.ff.p;
+  A.colrec = d.colrec.p;
   A.S = reinterpret_cast<const float4*>(S);
   A.S0 = reinterpret_cast<const float4*>(S0);
   A.SCT = reinterpret_cast<const float4*>(SCT);
   A.OUT = reinterpret_cast<float4*>(OUT);
-  constexpr int WPB = 8;
-  k_fused<WPB><<<cdiv(d.nw_prog, WPB), WPB * 32, 0, s>>>(A);
+  const unsigned nblk = (unsigned)((size_t)d.nw_prog * A.nchunk);
+  const int nq2 = ntp / 2;
+  // lanes per cell: the power of two covering the tracer pairs, 4..256
+  int lpi = 4;
+  while (lpi < nq2 && lpi < FUSED_THREADS) lpi *= 2;
+  switch (lpi) {
+    case 4: k_fused<4><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+    case 8: k_fused<8><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+    case 16: k_fused<16><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+    case 32: k_fused<32><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+    case 64: k_fused<64><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+    case 128: k_fused<128><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+    default: k_fused<256><<<nblk, FUSED_THREADS, 0, s>>>(A); break;
+  }
   OG_LAUNCHED();
 }
 

@@ -59,76 +59,92 @@ __device__ __forceinline__ void zrec(const float* a, int mza, int kd, int kb, fl
 // value and, on ties, the first point in loop order; nan = order + 1 of the
 // last NaN in loop order (OLAM's serial loop keeps the last NaN it meets).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+// one warp per prognostic column, lanes over levels (coalesced in k)
 __global__ void k_check_cfls(GridK g, const int* __restrict__ prog, int nprog,
                              const float* __restrict__ vmasc, const float* __restrict__ wmasc,
                              const float* __restrict__ rho, const float* __restrict__ wc, int nrk,
                              float dt, float* __restrict__ ff, unsigned long long* red) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (j >= nprog) return;
   const int mza = g.mza;
-  int iw = prog[j];
-  int np = g.npoly[iw];
+  const int iw = prog[j];
+  const int np = g.npoly[iw];
+  int ev[7];
+  float dv[7];
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    ev[n] = g.w_ev[iw * 8 + n];
+    dv[n] = g.w_dirv[iw * 8 + n];
+  }
   float fimp[3] = {0.f, 0.f, 0.f};
   unsigned long long kc = 0, kh = 0, kw = 0, nc = 0, nh = 0, nwn = 0;
-  for (int kd = g.lpw[iw]; kd < mza; ++kd) {
+  for (int kd = g.lpw[iw] + lane; kd < mza; kd += 32) {
     float cflh = 0.f;
-    for (int n = 0; n < np; ++n) {
-      int iv = g.w_ev[iw * 8 + n];
-      if (kd >= g.lpv[iv]) cflh = cflh - fminf(g.w_dirv[iw * 8 + n] * vmasc[(size_t)iv * mza + kd], 0.0f);
-    }
-    float dovr = dt * g.volti[(size_t)iw * mza + kd] / rho[(size_t)iw * mza + kd];
+#pragma unroll
+    for (int n = 0; n < 7; ++n)
+      if (n < np && kd >= g.lpv[ev[n]])
+        cflh = cflh - fminf(dv[n] * __ldg(vmasc + (size_t)ev[n] * mza + kd), 0.0f);
+    const float dovr = dt * g.volti[(size_t)iw * mza + kd] / rho[(size_t)iw * mza + kd];
     cflh = cflh * dovr;
     float cflw = (fmaxf(wmasc[(size_t)iw * mza + kd], 0.f) - fminf(wmasc[(size_t)iw * mza + kd - 1], 0.f)) * dovr;
-    float cfl = cflh + cflw;
+    const float cfl = cflh + cflw;
     cflw = fmaxf(cflw, .1f);
     fimp[nrk - 1] = fmaxf(fimp[nrk - 1], (cfl - 0.98f) / cflw);
     fimp[nrk - 2] = fmaxf(fimp[nrk - 2], (cfl - 1.98f) / cflw);
     if (nrk == 3) fimp[0] = fmaxf(fimp[0], (cfl - 2.98f) / cflw);
-    unsigned int order = (unsigned int)j * (unsigned int)mza + (unsigned int)kd;
-    unsigned long long low = 0xffffffffull - order;
-    if (cfl != cfl) nc = order + 1ull;
-    else if (cfl > 0.f) {
-      unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | low;
-      if (key > kc) kc = key;
-    }
-    if (cflh != cflh) nh = order + 1ull;
-    else if (cflh > 0.f) {
-      unsigned long long key = ((unsigned long long)__float_as_uint(cflh) << 32) | low;
-      if (key > kh) kh = key;
-    }
+    const unsigned int order = (unsigned int)j * (unsigned int)mza + (unsigned int)kd;
+    const unsigned long long low = 0xffffffffull - order;
+    if (cfl != cfl) nc = max(nc, order + 1ull);
+    else if (cfl > 0.f) kc = max(kc, ((unsigned long long)__float_as_uint(cfl) << 32) | low);
+    if (cflh != cflh) nh = max(nh, order + 1ull);
+    else if (cflh > 0.f) kh = max(kh, ((unsigned long long)__float_as_uint(cflh) << 32) | low);
     if (wc) {
-      float w = wc[(size_t)iw * mza + kd];
-      if (w != w) nwn = order + 1ull;
-      else if (fabsf(w) > 0.f) {
-        unsigned long long key = ((unsigned long long)__float_as_uint(fabsf(w)) << 32) | low;
-        if (key > kw) kw = key;
-      }
+      const float w = wc[(size_t)iw * mza + kd];
+      if (w != w) nwn = max(nwn, order + 1ull);
+      else if (fabsf(w) > 0.f) kw = max(kw, ((unsigned long long)__float_as_uint(fabsf(w)) << 32) | low);
     }
   }
-  for (int n = 0; n < nrk; ++n) {
-    float f = fminf(1.0f, fimp[n]);
-    // NaN-propagating min: OLAM's min(1.0, NaN) is compiler-dependent; a NaN
-    // CFL already makes the run invalid and is reported through the keys.
-    if (f < .02f) f = 0.f;
-    ff[(size_t)iw * nrk + n] = f;
-  }
-  if (red) {
-    if (kc) atomicMax(&red[0], kc);
-    if (nc) atomicMax(&red[1], nc);
-    if (kh) atomicMax(&red[2], kh);
-    if (nh) atomicMax(&red[3], nh);
-    if (kw) atomicMax(&red[4], kw);
-    if (nwn) atomicMax(&red[5], nwn);
+#pragma unroll
+  for (int n = 0; n < 3; ++n)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) fimp[n] = fmaxf(fimp[n], __shfl_xor_sync(0xffffffffu, fimp[n], o));
+  kc = warp_max_u64(kc); nc = warp_max_u64(nc);
+  kh = warp_max_u64(kh); nh = warp_max_u64(nh);
+  kw = warp_max_u64(kw); nwn = warp_max_u64(nwn);
+  if (lane == 0) {
+    for (int n = 0; n < nrk; ++n) {
+      float f = fminf(1.0f, fimp[n]);
+      if (f < .02f) f = 0.f;
+      ff[(size_t)iw * nrk + n] = f;
+    }
+    if (red) {
+      if (kc) atomicMax(&red[0], kc);
+      if (nc) atomicMax(&red[1], nc);
+      if (kh) atomicMax(&red[2], kh);
+      if (nh) atomicMax(&red[3], nh);
+      if (kw) atomicMax(&red[4], kw);
+      if (nwn) atomicMax(&red[5], nwn);
+    }
   }
 }
 
 void launch_check_cfls(const DevGrid& d, const Transport& tp, int nrk, float dtl,
                        unsigned long long* red, cudaStream_t s) {
   if (red) cudaMemsetAsync(red, 0, 6 * sizeof(unsigned long long), s);
-  int nb = 128;
-  k_check_cfls<<<cdiv(d.nw_prog, nb), nb, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, tp.vmasc.p,
-                                                  tp.wmasc.p, tp.rho_old.p, tp.wc.p, nrk, dtl,
-                                                  tp.ff.p, red);
+  const int nb = 256;  // 8 columns per block
+  k_check_cfls<<<cdiv((size_t)d.nw_prog * 32, nb), nb, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog,
+                                                              tp.vmasc.p, tp.wmasc.p, tp.rho_old.p,
+                                                              tp.wc.p, nrk, dtl, tp.ff.p, red);
   OG_LAUNCHED();
 }
 
@@ -718,7 +734,7 @@ void launch_vapply(const DevGrid& d, const Transport& tp, int nt, const int* mod
 }
 
 // pass 5: tendency and update for limited tracers (scalar_tend_monot/_pd)
-__global__ void k_tend(GridK g, const int* __restrict__ prog, int nprog, CTView scp0,
+__global__ void k_tend(GridK g, const int* __restrict__ prog, int nprog, CTView scp_in, CTView scp0,
                        const float* __restrict__ rhos, const float* __restrict__ vmasc,
                        const float* __restrict__ wmasc, const float* __restrict__ ff,
                        const float* __restrict__ upv, const float* __restrict__ upw, TView out, int nt,
@@ -753,19 +769,43 @@ __global__ void k_tend(GridK g, const int* __restrict__ prog, int nprog, CTView 
     out.base[((size_t)iw * mza + kd) * out.ld + out.t0 + t] =
         s0 + dtr * g.volti[(size_t)iw * mza + kd] * fd / rhos[(size_t)iw * mza + kd];
   }
-  // scp(2:kb-1) = scp(kb) only in the explicit branch; level 1 keeps its value
-  if (!(fimpl > .001f)) {
-    float v = out.base[((size_t)iw * mza + kb) * out.ld + out.t0 + t];
-    for (int kd = 1; kd < kb; ++kd) out.base[((size_t)iw * mza + kd) * out.ld + out.t0 + t] = v;
+  // The reference updates scp in place: scp(2:kb-1) = scp(kb) only in the
+  // explicit branch, and levels it does not write keep the stage input.
+  const float vkb = out.base[((size_t)iw * mza + kb) * out.ld + out.t0 + t];
+  for (int kd = 0; kd < kb; ++kd) {
+    const bool copy_kb = !(fimpl > .001f) && kd >= 1;
+    out.base[((size_t)iw * mza + kd) * out.ld + out.t0 + t] =
+        copy_kb ? vkb : scp_in.base[((size_t)iw * mza + kd) * scp_in.ld + scp_in.t0 + t];
   }
 }
 
-void launch_tend(const DevGrid& d, const Transport& tp, CTView scp0, const float* rhos, TView out,
-                 int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s) {
+void launch_tend(const DevGrid& d, const Transport& tp, CTView scp_in, CTView scp0, const float* rhos,
+                 TView out, int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s) {
   size_t n = (size_t)d.nw_prog * nt;
-  k_tend<<<cdiv(n, 128), 128, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp0, rhos, tp.vmasc.p,
+  k_tend<<<cdiv(n, 128), 128, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp_in, scp0, rhos, tp.vmasc.p,
                                       tp.wmasc.p, tp.ff.p, tp.upv.p, tp.upw.p, out, nt, istage, nrk, dtr,
                                       mode);
+  OG_LAUNCHED();
+}
+
+// Points outside jtw_prog (OLAM's dummy point 1, and lateral-boundary or
+// halo columns in other domains) are never updated; the reference keeps
+// their values in place.  Stage outputs live in rotating buffers, so those
+// columns are copied from the input into the final buffer.
+__global__ void k_copy_cols(const int* __restrict__ cols, int ncol, const float* __restrict__ src,
+                            float* __restrict__ dst, size_t colsize) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)ncol * colsize) return;
+  size_t c = i / colsize, r = i % colsize;
+  size_t off = (size_t)cols[c] * colsize + r;
+  dst[off] = src[off];
+}
+
+void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, size_t colsize,
+                      cudaStream_t s) {
+  if (ncol <= 0) return;
+  size_t n = (size_t)ncol * colsize;
+  k_copy_cols<<<cdiv(n, 256), 256, 0, s>>>(cols, ncol, src, dst, colsize);
   OG_LAUNCHED();
 }
 

@@ -63,13 +63,17 @@ void launch_wcol(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0,
                  const float* rhos, TView out, int nt, int istage, int nrk, float dtr,
                  const int* mode, bool anylim, cudaStream_t s);
 void launch_vapply(const DevGrid& d, const Transport& tp, int nt, const int* mode, cudaStream_t s);
-void launch_tend(const DevGrid& d, const Transport& tp, CTView scp0, const float* rhos, TView out,
-                 int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s);
+void launch_tend(const DevGrid& d, const Transport& tp, CTView scp_in, CTView scp0, const float* rhos,
+                 TView out, int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s);
 
 // fused batched update (plain mode), all tracers of the batched layout
 void launch_fused_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
                         const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr,
                         const float* rhos, cudaStream_t s);
+
+// copy the columns outside jtw_prog (colsize floats each) from src to dst
+void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, size_t colsize,
+                      cudaStream_t s);
 
 // layout transposes: per-tracer arrays <-> batched layout
 void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npts_k,

@@ -23,8 +23,9 @@
 
 namespace oracle {
 
-static const float kEps0 = 1.e-32f;  // scalar_transport_rk.F90:14-17
-static const float kEps1 = 3.e-07f;
+// scalar_transport_rk.F90:14-17 (real parameters: in precision T)
+#define kEps0 1.e-32
+#define kEps1 3.e-07
 
 static const int kIorderv = 3;  // scalar_transport_rk.F90:20
 
@@ -279,7 +280,7 @@ static void update_scalar_monot(const TransportCtx<T>& C, T* scp, const T* scp0,
   std::vector<T> scale_inout((size_t)mza * mwa * 2, (T)0), scp_upw((size_t)mza * mwa + 1);
   const T* vmasc = C.vmasc.data();
   const T* wmasc = C.wmasc.data();
-  const T onep = (T)(1.0f + kEps1), eps0 = (T)kEps0, eps1 = (T)kEps1;
+  const T eps0 = (T)kEps0, eps1 = (T)kEps1, onep = (T)1.0 + eps1;
   if (iorderh > 1) gradients(G, scp, iorderh, false, gxyps);
   vflux_hilo(C, scp, scp0, gxyps, iorderh, true, false, scp_upv, scp_hiv, sfluxvh);
   const size_t plane = (size_t)mza * mwa;
@@ -447,7 +448,7 @@ static void update_scalar_pd(const TransportCtx<T>& C, T* scp, const T* scp0, co
   std::vector<T> scale_out((size_t)mza * mwa, (T)0), scp_upw((size_t)mza * mwa + 1);
   const T* vmasc = C.vmasc.data();
   const T* wmasc = C.wmasc.data();
-  const T onep = (T)(1.0f + kEps1), onem = (T)(1.0f - kEps1), eps0 = (T)kEps0;
+  const T eps0 = (T)kEps0, onep = (T)1.0 + (T)kEps1, onem = (T)1.0 - (T)kEps1;
   if (iorderh > 1) gradients(G, scp, iorderh, true, gxyps);
   vflux_hilo(C, scp, scp0, gxyps, iorderh, false, true, scp_upv, scp_hiv, sfluxvh);
   const int nw = G.g->nw_prog;

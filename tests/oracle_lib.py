@@ -73,3 +73,88 @@ def scalar_transport(fg, opts, tracers, sct, st, fp64=False, pdef=None, sgsmix=N
     if want_ff:
         return out, ff, diag
     return out
+
+
+class State64(C.Structure):
+    _fields_ = [(n, abi.c_double_p) for n in (
+        "rho", "press", "thil", "wc", "wmc", "vxe", "vye", "vze", "vmc", "vc", "vmasc", "wmasc",
+        "alpha_press", "pwfac", "pvfac", "thilt", "vmxet", "vmyet", "vmzet", "vmt")]
+
+
+DYN_FIELDS = ("rho", "press", "thil", "wc", "wmc", "vxe", "vye", "vze", "vmc", "vc", "vmasc",
+              "wmasc", "alpha_press", "pwfac", "pvfac", "thilt", "vmxet", "vmyet", "vmzet", "vmt")
+
+
+def _dyn_lib():
+    L = lib()
+    if not hasattr(L, "_dyn_ready"):
+        for sfx in ("f32", "f64"):
+            getattr(L, f"oracle_dyn_new_{sfx}").restype = C.c_void_p
+            getattr(L, f"oracle_dyn_new_{sfx}").argtypes = [C.POINTER(abi.Grid), C.POINTER(abi.Opts)]
+            getattr(L, f"oracle_dyn_free_{sfx}").argtypes = [C.c_void_p]
+        L.oracle_prog_wrtv_rk_f32.argtypes = [C.c_void_p, C.POINTER(abi.State), C.c_int]
+        L.oracle_prog_wrtv_rk_f64.argtypes = [C.c_void_p, C.POINTER(State64), C.c_int]
+        L.oracle_tend0_f32.argtypes = [C.c_void_p, C.POINTER(abi.State), abi.c_float_p]
+        L.oracle_tend0_f64.argtypes = [C.c_void_p, C.POINTER(State64), abi.c_double_p]
+        L.oracle_timeavg_momsc_f32.argtypes = [C.c_void_p, C.POINTER(abi.State)]
+        L.oracle_timeavg_momsc_f64.argtypes = [C.c_void_p, C.POINTER(State64)]
+        L._dyn_ready = True
+    return L
+
+
+class DynOracle:
+    """The oracle's prog_wrtv_rk with its saved damping state, on copies of
+    the given arrays (dict name -> array in OLAM layout)."""
+
+    def __init__(self, fg, opts, arrays, fp64=False):
+        self.L = _dyn_lib()
+        self.fp64 = fp64
+        self.fg, self.opts = fg, opts
+        sfx = "f64" if fp64 else "f32"
+        self.h = getattr(self.L, f"oracle_dyn_new_{sfx}")(C.byref(fg.struct), C.byref(opts))
+        self.a = {}
+        for n in DYN_FIELDS:
+            dt = np.float64 if (fp64 or n in ("rho", "press")) else np.float32
+            self.a[n] = np.ascontiguousarray(arrays[n], dtype=dt).copy()
+        if fp64:
+            s = State64()
+            for n in DYN_FIELDS:
+                setattr(s, n, abi.ptr(self.a[n], C.c_double))
+        else:
+            s = abi.State()
+            for n in DYN_FIELDS:
+                setattr(s, n, abi.ptr(self.a[n], C.c_double if n in ("rho", "press") else C.c_float))
+        self.s = s
+
+    def prog_wrtv_rk(self, istp=1):
+        f = self.L.oracle_prog_wrtv_rk_f64 if self.fp64 else self.L.oracle_prog_wrtv_rk_f32
+        rc = f(self.h, C.byref(self.s), istp)
+        assert rc == 0, rc
+
+    def tend0(self):
+        ro = np.zeros_like(self.a["thil"])
+        if self.fp64:
+            self.L.oracle_tend0_f64(self.h, C.byref(self.s), abi.ptr(ro, C.c_double))
+        else:
+            self.L.oracle_tend0_f32(self.h, C.byref(self.s), abi.ptr(ro, C.c_float))
+        return ro
+
+    def timeavg_momsc(self):
+        f = self.L.oracle_timeavg_momsc_f64 if self.fp64 else self.L.oracle_timeavg_momsc_f32
+        f(self.h, C.byref(self.s))
+
+    def __del__(self):
+        try:
+            sfx = "f64" if self.fp64 else "f32"
+            getattr(self.L, f"oracle_dyn_free_{sfx}")(self.h)
+        except Exception:
+            pass
+
+
+def dyn_arrays(g, ds):
+    """OLAM module arrays for prog_wrtv_rk from a synth dynamics state."""
+    z = lambda n: np.zeros((n, g.mza), dtype=np.float32)  # noqa: E731
+    return dict(rho=ds.rho, press=ds.press, thil=ds.thil, wc=ds.wc, wmc=ds.wmc, vxe=ds.vxe,
+                vye=ds.vye, vze=ds.vze, vmc=ds.vmc, vc=ds.vc, vmasc=z(g.mva), wmasc=z(g.mwa),
+                alpha_press=ds.alpha_press, pwfac=ds.pwfac, pvfac=ds.pvfac, thilt=z(g.mwa),
+                vmxet=z(g.mwa), vmyet=z(g.mwa), vmzet=z(g.mwa), vmt=z(g.mva))

@@ -116,3 +116,23 @@ def test_golden_fixture():
     for nrk, key in ((2, "out_rk2"), (3, "out_rk3")):
         out64, _, _ = _run(g, st, float(z["dtlm"]), fp64=True, nrk_scal=nrk)
         assert relerr(out64, z[key]) < 1e-12
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("order", [2, 3])
+def test_oracle_limiters_vs_numpy(case_small, mode, order):
+    # RK2: numpy plain stage 1, then the monotonic / positive-definite stage
+    from numpy_ref import limited_last_stage, plain_stage
+    g, st = case_small
+    dt = 1800.0
+    out64, ff, _ = _run(g, st, dt, fp64=True, iscal_monot=mode, scal_order=order,
+                        pdef=np.ones(st.ntr))
+    assert ff.max() == 0.0
+    rho = st.rho.astype(np.float64)
+    for n in range(st.ntr):
+        q0 = st.tracers[n].astype(np.float64)
+        t0 = st.sct[n].astype(np.float64)
+        s1 = plain_stage(g, st.vmasc, st.wmasc, rho, q0.copy(), q0, t0, dt * 0.5, order)
+        q0b = q0 + dt * t0 / np.where(st.rho_old == 0, 1, st.rho_old)
+        ref = limited_last_stage(g, s1, q0b, rho, st.vmasc, st.wmasc, dt, mode, order)
+        assert relerr(out64[n][1:], ref[1:]) < 1e-12

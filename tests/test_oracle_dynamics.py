@@ -1,0 +1,71 @@
+"""CPU tests of the oracle's acoustic RK step (properties and precision)."""
+import numpy as np
+import pytest
+
+import oracle_lib
+from conftest import relerr
+from olam_b200 import abi
+
+_C = {}
+
+
+def dyn_case(nxp=6, nlev=12):
+    from olam_b200.synth.grid import build_grid, stretched_levels
+    from olam_b200.synth.state import dynamics_state
+    if (nxp, nlev) not in _C:
+        g = build_grid(nxp, stretched_levels(nlev, 100.0, 30000.0), seed=4)
+        ds = dynamics_state(g, seed=4)
+        _C[(nxp, nlev)] = (g, ds)
+    return _C[(nxp, nlev)]
+
+
+def _long_step(o, nacoust):
+    o.tend0()
+    for jstp in range(1, nacoust + 1):
+        o.prog_wrtv_rk(jstp)
+    o.timeavg_momsc()
+
+
+def test_dynamics_mass_conserved_and_finite():
+    g, ds = dyn_case()
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(600.0, nacoust=4)
+    o = oracle_lib.DynOracle(fg, opts, oracle_lib.dyn_arrays(g, ds), fp64=True)
+    m0 = (o.a["rho"][1:, 1:] * g.volt[1:, 1:]).sum()
+    _long_step(o, 4)
+    m1 = (o.a["rho"][1:, 1:] * g.volt[1:, 1:]).sum()
+    # volti is real(4) even in the FP64 run, so volt*volti = 1 to float round-off
+    assert abs(m1 - m0) / m0 < 1e-10
+    for n in ("rho", "thil", "vmc", "wmc", "press"):
+        assert np.isfinite(o.a[n]).all(), n
+    # winds stay physical
+    assert np.abs(o.a["vc"]).max() < 150.0
+    assert np.abs(o.a["wc"]).max() < 20.0
+
+
+def test_dynamics_fp32_close_to_fp64():
+    g, ds = dyn_case()
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(600.0, nacoust=4)
+    a32 = oracle_lib.DynOracle(fg, opts, oracle_lib.dyn_arrays(g, ds), fp64=False)
+    a64 = oracle_lib.DynOracle(fg, opts, oracle_lib.dyn_arrays(g, ds), fp64=True)
+    _long_step(a32, 4)
+    _long_step(a64, 4)
+    assert relerr(a32.a["rho"], a64.a["rho"]) < 1e-6
+    assert relerr(a32.a["thil"], a64.a["thil"]) < 1e-6
+    assert relerr(a32.a["vmc"], a64.a["vmc"]) < 1e-4
+    assert relerr(a32.a["vmasc"], a64.a["vmasc"]) < 1e-4
+
+
+def test_dynamics_vmasc_consistent_with_rho():
+    # the long-step mean mass fluxes reproduce the density change exactly
+    from olam_b200.synth.state import flux_divergence
+    g, ds = dyn_case()
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(600.0, nacoust=4)
+    o = oracle_lib.DynOracle(fg, opts, oracle_lib.dyn_arrays(g, ds), fp64=True)
+    rho0 = o.a["rho"].copy()
+    _long_step(o, 4)
+    div = flux_divergence(g, o.a["vmasc"], o.a["wmasc"])
+    rho_pred = rho0 + 600.0 * g.volti.astype(np.float64) * div
+    assert relerr(o.a["rho"][1:, 1:], rho_pred[1:, 1:]) < 1e-6
