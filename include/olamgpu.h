@@ -201,7 +201,8 @@ const char* olamgpu_strerror(int status);
  *   is a drop-in for the Fortran routine.
  * OLAMGPU_RESIDENT: state stays on the device between calls; the caller
  *   moves fields with olamgpu_sync_to_device / olamgpu_sync_to_host where CPU
- *   physics reads or writes them. */
+ *   physics reads or writes them.
+ * olamgpu_init restores the defaults (SYNC_EACH_CALL, fused transport). */
 enum { OLAMGPU_SYNC_EACH_CALL = 0, OLAMGPU_RESIDENT = 1 };
 int olamgpu_set_coherence(int mode);
 int olamgpu_sync_to_device(unsigned fieldmask);

@@ -127,6 +127,7 @@ static void release_all() {
   tp.d_mode.release();
   tp.khtopv.release();
   tp.have_turb = false;
+  dyn_release();
   C.status.release();
 }
 
@@ -165,6 +166,8 @@ int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts, const olamg
   if (rc != OLAMGPU_OK) { release_all(); return rc; }
   C.hgrid = *grid;
   C.opts = *opts;
+  C.coherence = OLAMGPU_SYNC_EACH_CALL;
+  C.form = OLAMGPU_TRANSPORT_FUSED;
   C.tp.flat = true;
   for (int i = 1; i < grid->mwa; ++i) if (grid->lpw[i] != 2) C.tp.flat = false;
   for (int i = 1; i < grid->mva; ++i) if (grid->lpv[i] != 2) C.tp.flat = false;
@@ -174,6 +177,12 @@ int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts, const olamg
     if (rc != OLAMGPU_OK) { release_all(); return rc; }
   }
   if (state) { C.hstate = *state; C.have_state = true; } else C.have_state = false;
+  // prog_wrtv_rk needs the dynamics state and the M-point tables; without
+  // them only scalar_transport_rk is available
+  if (state && state->thil && state->vmc && state->press && grid->itab_m_iv && grid->jtm_prog) {
+    rc = dyn_setup(grid, opts, C.stream);
+    if (rc != OLAMGPU_OK) { release_all(); return rc; }
+  }
   rc = C.status.alloc(16);
   if (rc != OLAMGPU_OK) { release_all(); return rc; }
   cudaMemsetAsync(C.status.p, 0, 16 * sizeof(int), C.stream);
@@ -281,10 +290,14 @@ int olamgpu_sync_to_device(unsigned fieldmask) {
     }
   }
   if (C.have_state) {
-    if ((fieldmask & OLAMGPU_F_VMASC) && C.hstate.vmasc) OG_CHECK(upload(C.tp.vmasc, C.hstate.vmasc, vz, s));
-    if ((fieldmask & OLAMGPU_F_WMASC) && C.hstate.wmasc) OG_CHECK(upload(C.tp.wmasc, C.hstate.wmasc, wz, s));
-    if ((fieldmask & OLAMGPU_F_RHO) && C.hstate.rho) OG_CHECK(upload(C.tp.rho, C.hstate.rho, wz, s));
-    if ((fieldmask & OLAMGPU_F_WC) && C.hstate.wc) OG_CHECK(upload(C.tp.wc, C.hstate.wc, wz, s));
+    if (C.dy.ready) {
+      OG_CHECK(dyn_state_to_device(fieldmask, s));
+    } else {
+      if ((fieldmask & OLAMGPU_F_VMASC) && C.hstate.vmasc) OG_CHECK(upload(C.tp.vmasc, C.hstate.vmasc, vz, s));
+      if ((fieldmask & OLAMGPU_F_WMASC) && C.hstate.wmasc) OG_CHECK(upload(C.tp.wmasc, C.hstate.wmasc, wz, s));
+      if ((fieldmask & OLAMGPU_F_RHO) && C.hstate.rho) OG_CHECK(upload(C.tp.rho, C.hstate.rho, wz, s));
+      if ((fieldmask & OLAMGPU_F_WC) && C.hstate.wc) OG_CHECK(upload(C.tp.wc, C.hstate.wc, wz, s));
+    }
   }
   OG_CUDA(cudaStreamSynchronize(s));
   return OLAMGPU_OK;
@@ -304,6 +317,20 @@ int olamgpu_sync_to_host(unsigned fieldmask) {
         OG_CUDA(cudaMemcpyAsync(C.tr.h_t[n], C.tr.t[n].p, wz * 4, cudaMemcpyDeviceToHost, s));
     }
   }
+  if (C.have_state) {
+    if (C.dy.ready) {
+      OG_CHECK(dyn_state_to_host(fieldmask, s));
+    } else {
+      const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva;
+      auto cp = [&](void* h, const void* dv, size_t b) -> int {
+        if (h && dv) OG_CUDA(cudaMemcpyAsync(h, dv, b, cudaMemcpyDeviceToHost, s));
+        return OLAMGPU_OK;
+      };
+      if (fieldmask & OLAMGPU_F_VMASC) OG_CHECK(cp(C.hstate.vmasc, C.tp.vmasc.p, vz * 4));
+      if (fieldmask & OLAMGPU_F_WMASC) OG_CHECK(cp(C.hstate.wmasc, C.tp.wmasc.p, wz * 4));
+      if (fieldmask & OLAMGPU_F_RHO) OG_CHECK(cp(C.hstate.rho, C.tp.rho.p, wz * 8));
+    }
+  }
   OG_CUDA(cudaStreamSynchronize(s));
   return OLAMGPU_OK;
 }
@@ -317,22 +344,11 @@ int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag) {
   return rc;
 }
 
-int olamgpu_prog_wrtv_rk(int istp) {
-  (void)istp;
-  set_error("prog_wrtv_rk is not available in this build");
-  return OLAMGPU_E_UNSUPPORTED;
-}
+int olamgpu_prog_wrtv_rk(int istp) { return dyn_prog_wrtv_rk(istp); }
 
-int olamgpu_tend0(float* rho_old) {
-  (void)rho_old;
-  set_error("tend0 is not available in this build");
-  return OLAMGPU_E_UNSUPPORTED;
-}
+int olamgpu_tend0(float* rho_old) { return dyn_tend0(rho_old); }
 
-int olamgpu_timeavg_momsc(void) {
-  set_error("timeavg_momsc is not available in this build");
-  return OLAMGPU_E_UNSUPPORTED;
-}
+int olamgpu_timeavg_momsc(void) { return dyn_timeavg_momsc(); }
 
 void* olamgpu_stream(void) { return (void*)ctx().stream; }
 

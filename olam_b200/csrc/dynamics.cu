@@ -1,0 +1,1039 @@
+// dynamics.cu -- the acoustic RK short step prog_wrtv_rk and its glue on the
+// device (omodel/prog_wrtv_rk.f90:36-488, omodel/timestep.f90:430-612).
+//
+// Kernel per reference routine, each over the reference's loop table:
+//   k_setup_w / k_setup_v   column set-up and Rayleigh terms   (prog_wrtv_rk.f90:166-303)
+//   k_div_* / k_lap_w       divh_damp                          (vort_div_damp.f90:1-230)
+//   k_vort_* / k_lap_m      vort_damp                          (vort_div_damp.f90:234-445)
+//   k_rk_copy, k_vmca       stage copies, vmca and vmasc       (prog_wrtv_rk.f90:320-368)
+//   k_grad4, k_upw4, k_upv4 fluxes_wrtv for thil, vxe, vye, vze (:950-1129), the four
+//                           fields of one stage in one launch each
+//   k_wrt_begs              prog_wrt_begs (:494-884): one warp per column, lanes over
+//                           levels for the explicit terms, one lane for the serial
+//                           tridiagonal solve (tridiffo, tridiag_lib.f90:10-36)
+//   k_prog_v                prog_v_begs (:888-946)
+//   k_vel_t3d               vel_t3d_hex (vel_t3d.f90:39-108)
+// Precision as declared by OLAM: rho, press and the implicit weights are
+// double; every other field is float.  Device level kd = Fortran k - 1.
+#include <cmath>
+#include <cstring>
+
+#include "transport_kernels.cuh"
+
+namespace olamgpu {
+
+struct DynK {
+  int mza, mwa, mva, mma;
+  const int* __restrict__ npoly;
+  const int* __restrict__ w_nb;
+  const int* __restrict__ w_ev;
+  const float* __restrict__ w_dirv;
+  const int* __restrict__ v_iw;
+  const int* __restrict__ v_im;
+  const int* __restrict__ m_iv;
+  const int* __restrict__ m_im;
+  const int* __restrict__ lpw;
+  const int* __restrict__ lpv;
+  const int* __restrict__ lpm;
+  const float* __restrict__ volti;
+  const float* __restrict__ a_w;
+};
+
+static DynK dynk(const DevGrid& d) {
+  DynK k;
+  k.mza = d.mza; k.mwa = d.mwa; k.mva = d.mva; k.mma = d.mma;
+  k.npoly = d.npoly.p; k.w_nb = d.w_nb.p; k.w_ev = d.w_ev.p; k.w_dirv = d.w_dirv.p;
+  k.v_iw = d.v_iw.p; k.v_im = d.v_im.p; k.m_iv = d.m_iv.p; k.m_im = d.m_im.p;
+  k.lpw = d.lpw.p; k.lpv = d.lpv.p; k.lpm = d.lpm.p; k.volti = d.volti.p; k.a_w = d.a_w.p;
+  return k;
+}
+
+#define PK(j, kd, n)                                               \
+  size_t i_ = (size_t)blockIdx.x * blockDim.x + threadIdx.x;       \
+  if (i_ >= (size_t)(n) * g.mza) return;                           \
+  const int j = (int)(i_ / g.mza), kd = (int)(i_ % g.mza);
+
+// ---- column set-up (prog_wrtv_rk.f90:166-253) --------------------------------
+struct SetupW {
+  const double* rho; const float* thil; const float* wmc;
+  const float* thilt; const float* vmxet; const float* vmyet; const float* vmzet;
+  const double* volt;
+  double* rho0; double* rth0; float* wmc0;
+  float* sh_th; float* sh_vx; float* sh_vy; float* sh_vz;
+  const float* rayf_cof; const float* dn01d; const float* th01d; int krayf_bot;
+};
+
+__global__ void k_setup_w(DynK g, const int* __restrict__ prog, int nprog, SetupW a) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  if (kd < g.lpw[iw]) return;
+  const size_t x = (size_t)iw * g.mza + kd;
+  const float v4 = (float)a.volt[x];
+  a.rth0[x] = (double)a.thil[x] * a.rho[x];
+  a.rho0[x] = a.rho[x];
+  a.wmc0[x] = a.wmc[x];
+  float th = a.thilt[x] * v4;
+  if (a.rayf_cof && kd >= a.krayf_bot - 1)
+    th = th + a.rayf_cof[kd] * a.dn01d[kd] * (a.th01d[kd] - a.thil[x]) * v4;
+  a.sh_th[x] = th;
+  a.sh_vx[x] = a.vmxet[x] * v4;
+  a.sh_vy[x] = a.vmyet[x] * v4;
+  a.sh_vz[x] = a.vmzet[x] * v4;
+}
+
+__global__ void k_setup_v(DynK g, const int* __restrict__ vprog, int nv, const float* __restrict__ vmc,
+                          const float* __restrict__ vmt, float* __restrict__ vmc0, float* __restrict__ sh_vmt,
+                          const float* __restrict__ rayf_cof, const float* __restrict__ vc03d,
+                          const float* __restrict__ vc, const double* __restrict__ rho, int krayf_bot) {
+  PK(j, kd, nv);
+  const int iv = vprog[j];
+  const size_t x = (size_t)iv * g.mza + kd;
+  vmc0[x] = vmc[x];
+  float v = vmt[x];
+  if (rayf_cof && kd >= krayf_bot - 1) {
+    const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+    const double t = (double)(rayf_cof[kd] * 0.5f) * (rho[(size_t)iw1 * g.mza + kd] + rho[(size_t)iw2 * g.mza + kd]) *
+                     (double)(vc03d[x] - vc[x]);
+    v = (float)((double)v + t);
+  }
+  sh_vmt[x] = v;
+}
+
+// ---- divh_damp ----------------------------------------------------------------
+__global__ void k_div_fdivh(DynK g, const int* __restrict__ vprog, int nv, const float* __restrict__ arw0,
+                            const float* __restrict__ dniv, const float* __restrict__ zfacit,
+                            const float* __restrict__ dzit, const double* __restrict__ volt, double facth,
+                            int level, float fact2, float* __restrict__ fdivh) {
+  PK(j, kd, nv);
+  const int iv = vprog[j];
+  if (kd < g.lpv[iv]) return;
+  const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  const double vmin = fmin(volt[(size_t)iw1 * g.mza + kd], volt[(size_t)iw2 * g.mza + kd]);
+  double v;
+  if (level > 1) {
+    const float amin = fminf(arw0[iw1], arw0[iw2]);
+    float pw = 1.f;
+    for (int i = 0; i < level - 1; ++i) pw = pw * amin;
+    const double factb = facth * (double)pw;
+    v = factb * (double)dniv[iv] * (double)zfacit[kd] * (double)dzit[kd] * vmin * 1.0;
+  } else {
+    v = (double)fact2 * (double)dniv[iv] * (double)zfacit[kd] * (double)dzit[kd] * vmin;
+  }
+  fdivh[(size_t)iv * g.mza + kd] = (float)v;
+}
+
+// The saved div2d is not cleared: plane 1 accumulates onto what the previous
+// call left there, as the Fortran does (vort_div_damp.f90:136-148).
+__global__ void k_div_accum(DynK g, const int* __restrict__ prog, int nprog, const float* __restrict__ arv,
+                            const float* __restrict__ vmc, float* __restrict__ div1) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  const size_t x = (size_t)iw * g.mza + kd;
+  float d = div1[x];
+  const int np = g.npoly[iw];
+  for (int n = 0; n < np; ++n) {
+    const int iv = g.w_ev[iw * 8 + n];
+    if (kd >= g.lpv[iv])
+      d = d - arv[(size_t)iv * g.mza + kd] * g.w_dirv[iw * 8 + n] * vmc[(size_t)iv * g.mza + kd];
+  }
+  if (kd >= g.lpw[iw]) d = d * g.volti[x];
+  div1[x] = d;
+}
+
+// laplacian2d (grad_lib.f90:494-524)
+__global__ void k_lap_w(DynK g, const int* __restrict__ prog, int nprog, const float* __restrict__ xx_yy,
+                        const float* __restrict__ src, float* __restrict__ dst) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  const size_t x = (size_t)iw * g.mza + kd;
+  float d = 0.f;
+  const int np = g.npoly[iw];
+  for (int n = 0; n < np; ++n) {
+    const int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
+    if (kd >= g.lpv[iv]) d = d + (src[(size_t)iwn * g.mza + kd] - src[x]) * xx_yy[iw * 7 + n];
+  }
+  dst[x] = d;
+}
+
+__global__ void k_div_apply(DynK g, const int* __restrict__ vprog, int nv, const float* __restrict__ fdivh,
+                            const float* __restrict__ dh, float* __restrict__ vmt) {
+  PK(j, kd, nv);
+  const int iv = vprog[j];
+  if (kd < g.lpv[iv]) return;
+  const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  const size_t x = (size_t)iv * g.mza + kd;
+  vmt[x] = vmt[x] + fdivh[x] * (dh[(size_t)iw2 * g.mza + kd] - dh[(size_t)iw1 * g.mza + kd]);
+}
+
+// ---- vort_damp ----------------------------------------------------------------
+__global__ void k_vort_first_m(DynK g, const int* __restrict__ mprog, int nm, const float* __restrict__ dnv,
+                               const float* __restrict__ arm0, float* __restrict__ vfact,
+                               int* __restrict__ lpmmin) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nm) return;
+  const int im = mprog[j];
+  int lm = 1 << 30;
+  for (int jv = 0; jv < 3; ++jv) lm = min(lm, g.lpv[g.m_iv[im * 3 + jv]]);
+  lpmmin[im] = lm;
+  for (int jv = 0; jv < 3; ++jv) {
+    const int iv = g.m_iv[im * 3 + jv];
+    const float v = dnv[iv] / arm0[im];
+    vfact[im * 3 + jv] = (g.v_im[iv * 2 + 1] == im) ? v : -v;
+  }
+}
+
+__global__ void k_vort_first_v(DynK g, const int* __restrict__ vprog, int nv, const float* __restrict__ dniu,
+                               const float* __restrict__ arm0, float dtm_f, float fact, int level,
+                               float* __restrict__ fvorth, float* __restrict__ fvortl) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nv) return;
+  const int iv = vprog[j];
+  const int im1 = g.v_im[iv * 2], im2 = g.v_im[iv * 2 + 1];
+  const float a = -fact * fminf(arm0[im1], arm0[im2]);
+  float ph = 1.f, pl = 1.f;
+  for (int i = 0; i < level; ++i) ph = ph * a;
+  for (int i = 0; i < level - 1; ++i) pl = pl * a;
+  fvorth[iv] = 0.50f * dniu[iv] / dtm_f * ph;
+  fvortl[iv] = (level > 2) ? 0.50f * dniu[iv] / dtm_f * pl : 0.f;
+}
+
+__global__ void k_vort(DynK g, const int* __restrict__ mprog, int nm, const float* __restrict__ vfact,
+                       const float* __restrict__ vc, float* __restrict__ v1) {
+  PK(j, kd, nm);
+  const int im = mprog[j];
+  float v = 0.f;
+  for (int jv = 0; jv < 3; ++jv) {
+    const int iv = g.m_iv[im * 3 + jv];
+    if (kd >= g.lpv[iv]) v = v + vc[(size_t)iv * g.mza + kd] * vfact[im * 3 + jv];
+  }
+  v1[(size_t)im * g.mza + kd] = v;
+}
+
+// laplacian_m (grad_lib.f90:531-559)
+__global__ void k_lap_m(DynK g, const int* __restrict__ mprog, int nm, const float* __restrict__ xx_yy_m,
+                        const float* __restrict__ src, float* __restrict__ dst) {
+  PK(j, kd, nm);
+  const int im = mprog[j];
+  const size_t x = (size_t)im * g.mza + kd;
+  float d = 0.f;
+  for (int jj = 0; jj < 3; ++jj) {
+    const int imn = g.m_im[im * 3 + jj];
+    if (kd >= g.lpv[g.m_iv[im * 3 + jj]]) d = d + (src[(size_t)imn * g.mza + kd] - src[x]) * xx_yy_m[im * 3 + jj];
+  }
+  dst[x] = d;
+}
+
+__global__ void k_vort_apply(DynK g, const int* __restrict__ vprog, int nv, int level,
+                             const float* __restrict__ fvorth, const float* __restrict__ fvortl,
+                             const float* __restrict__ dl, const float* __restrict__ dh,
+                             const double* __restrict__ rho, float* __restrict__ vmt) {
+  PK(j, kd, nv);
+  const int iv = vprog[j];
+  if (kd < g.lpv[iv]) return;
+  const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  const int im1 = g.v_im[iv * 2], im2 = g.v_im[iv * 2 + 1];
+  const float rr = (float)(rho[(size_t)iw1 * g.mza + kd] + rho[(size_t)iw2 * g.mza + kd]);
+  const size_t x = (size_t)iv * g.mza + kd;
+  if (level == 1) {
+    vmt[x] = vmt[x] + fvorth[iv] * (dh[(size_t)im2 * g.mza + kd] - dh[(size_t)im1 * g.mza + kd]) * rr;
+    return;
+  }
+  const int ka = (level == 3) ? max(g.lpm[im1], g.lpm[im2]) : g.lpv[iv];
+  if (kd < ka)
+    vmt[x] = vmt[x] + fvortl[iv] * (dl[(size_t)im2 * g.mza + kd] - dl[(size_t)im1 * g.mza + kd]) * rr;
+  else
+    vmt[x] = vmt[x] + fvorth[iv] * (dh[(size_t)im2 * g.mza + kd] - dh[(size_t)im1 * g.mza + kd]) * rr;
+}
+
+// ---- stage kernels ----------------------------------------------------------------
+__global__ void k_rk_copy(DynK g, const int* __restrict__ prog, int nprog, const float* sth, const float* svx,
+                          const float* svy, const float* svz, float* rth, float* rvx, float* rvy, float* rvz) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  if (kd < g.lpw[iw]) return;
+  const size_t x = (size_t)iw * g.mza + kd;
+  rth[x] = sth[x]; rvx[x] = svx[x]; rvy[x] = svy[x]; rvz[x] = svz[x];
+}
+
+__global__ void k_vmca(DynK g, const int* __restrict__ vadj, int nv, const float* __restrict__ vmc,
+                       const float* __restrict__ arv, float* __restrict__ vmca, float* __restrict__ vmasc,
+                       int last) {
+  PK(j, kd, nv);
+  const int iv = vadj[j];
+  if (kd < g.lpv[iv]) return;
+  const size_t x = (size_t)iv * g.mza + kd;
+  const float v = vmc[x] * arv[x];
+  vmca[x] = v;
+  if (last) vmasc[x] = vmasc[x] + v;
+}
+
+struct Four { const float* f[4]; };
+
+// gradient planes of the four fields (grad_t2d, or grad_t2d_quadratic with
+// bounded=.false. as fluxes_wrtv calls it).  gx layout: [field][plane][iw][kd]
+__global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s, int ord_th, int ord_v,
+                        const float* __restrict__ cx, const float* __restrict__ cy,
+                        const float* __restrict__ xy_hu, float* __restrict__ gx) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  const size_t plane = (size_t)g.mwa * g.mza;
+  const size_t x = (size_t)iw * g.mza + kd;
+  const int np = g.npoly[iw];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const int ord = f == 0 ? ord_th : ord_v;
+    if (ord < 2) continue;
+    const float* S = s.f[f];
+    const float c0 = S[x];
+    float a[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int n = 0; n < np; ++n) {
+      const int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
+      if (kd < g.lpv[iv]) continue;
+      const float d = S[(size_t)iwn * g.mza + kd] - c0;
+      if (ord == 2) {
+        a[0] = a[0] + cx[iw * 7 + n] * d;
+        a[1] = a[1] + cy[iw * 7 + n] * d;
+      } else {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) a[m] = a[m] + d * xy_hu[((size_t)iw * 7 + n) * 5 + m];
+      }
+    }
+    float* G = gx + (size_t)f * 5 * plane;
+    const int nplanes = ord == 2 ? 2 : 5;
+    for (int m = 0; m < nplanes; ++m) G[m * plane + x] = a[m];
+  }
+}
+
+// vertical upwind face values of the four fields (scalar_w_column of
+// fluxes_wrtv, prog_wrtv_rk.f90:1085-1126): thread per (column, face kd)
+__global__ void k_upw4(DynK g, const int* __restrict__ prog, int nprog, Four s, const float* __restrict__ wmc,
+                       float* __restrict__ upw) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  const int kb = g.lpw[iw];
+  const int mza = g.mza;
+  if (kd < kb - 1) return;
+  const size_t plane = (size_t)g.mwa * mza;
+  const size_t cb = (size_t)iw * mza;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const float* S = s.f[f] + cb;
+    float v;
+    if (kd == kb - 1) v = S[kb];
+    else if (kd == mza - 1) v = S[mza - 1];
+    else {
+      const bool down = wmc[cb + kd] < 0.f;
+      const int lev = down ? kd + 1 : kd;
+      const float b = S[lev];
+      const float dsk = (lev <= mza - 2) ? S[lev + 1] - b : 0.f;
+      const float dskm1 = (lev >= kb + 1) ? b - S[lev - 1] : 0.f;
+      const float c1 = g.a_w[lev + (down ? 0 : 2 * mza)];
+      const float c2 = g.a_w[lev + (down ? mza : 3 * mza)];
+      v = b + dsk * c1 + dskm1 * c2;
+    }
+    upw[(size_t)f * plane + cb + kd] = v;
+  }
+}
+
+struct VSide { const float* dxps; const float* dyps; const float* xx0_v; const float* xy0_v; const float* yy0_v; };
+
+__global__ void k_upv4(DynK g, const int* __restrict__ vadj, int nv, Four s, int ord_th, int ord_v,
+                       const float* __restrict__ gx, VSide c, const float* __restrict__ vmc,
+                       float* __restrict__ upv) {
+  PK(j, kd, nv);
+  const int iv = vadj[j];
+  if (kd < g.lpv[iv]) return;
+  const int mza = g.mza;
+  const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  const size_t plane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
+  const size_t x1 = (size_t)iw1 * mza + kd, x2 = (size_t)iw2 * mza + kd;
+  const bool neg = vmc[(size_t)iv * mza + kd] < 0.f;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const int ord = f == 0 ? ord_th : ord_v;
+    const float* S = s.f[f];
+    float s1 = S[x1], s2 = S[x2];
+    if (ord >= 2) {
+      const float* G = gx + (size_t)f * 5 * plane;
+      s1 = s1 + c.dxps[iv * 2] * G[x1] + c.dyps[iv * 2] * G[plane + x1];
+      s2 = s2 + c.dxps[iv * 2 + 1] * G[x2] + c.dyps[iv * 2 + 1] * G[plane + x2];
+      if (ord == 3) {
+        s1 = s1 + c.xx0_v[iv * 2] * G[2 * plane + x1] + c.xy0_v[iv * 2] * G[3 * plane + x1] +
+             c.yy0_v[iv * 2] * G[4 * plane + x1];
+        s2 = s2 + c.xx0_v[iv * 2 + 1] * G[2 * plane + x2] + c.xy0_v[iv * 2 + 1] * G[3 * plane + x2] +
+             c.yy0_v[iv * 2 + 1] * G[4 * plane + x2];
+      }
+    }
+    upv[(size_t)f * vplane + (size_t)iv * mza + kd] = neg ? s2 : s1;
+  }
+}
+
+// ---- prog_wrt_begs: one warp per column ------------------------------------------
+struct WrtArgs {
+  int istage, nrk;
+  double dt8;
+  float dts, fcoriol, c8, c9, rocv;
+  double pc2, pc3, fr;
+  const int* prog; int nprog;
+  const float* vmca; const float* upv; const float* upw;   // 4-field arrays
+  float* rk_th; float* rk_vx; float* rk_vy; float* rk_vz;
+  double* rho; double* press; const double* rho0; const double* rth0;
+  float* thil; float* wc; float* wmc; const float* wmc0; const float* vxe; const float* vye;
+  float* wmasc;
+  const float* alpha_press; const float* pwfac;
+  const double* volt; const float* volwi; const float* arw; const float* wn;
+  const double* gdz_wgtm8; const double* gdz_wgtp8; const float* gdz_wgtm; const float* gdz_wgtp;
+  const double* zwgt_bot8; const double* zwgt_top8; const float* b20;
+};
+
+#define WRT_WARPS 4
+// per-warp shared scratch, arrays of mza entries
+struct WrtSmem {
+  double *hflx, *rt, *b10, *b5, *drt, *pex, *rex, *rhon;
+  float *b15, *rkx, *rky, *rkz, *b31, *b32, *b33, *dwm, *wmf;
+};
+
+__global__ void __launch_bounds__(WRT_WARPS * 32) k_wrt_begs(DynK g, WrtArgs A) {
+  extern __shared__ double wsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.x * WRT_WARPS + warp;
+  if (j >= A.nprog) return;
+  const int mza = g.mza;
+  double* base = wsm + (size_t)warp * mza * 13;  // 8 double + 9 float arrays (9 floats <= 5 doubles)
+  WrtSmem m;
+  m.hflx = base; m.rt = base + mza; m.b10 = base + 2 * mza; m.b5 = base + 3 * mza; m.drt = base + 4 * mza;
+  m.pex = base + 5 * mza; m.rex = base + 6 * mza; m.rhon = base + 7 * mza;
+  float* fb = reinterpret_cast<float*>(base + 8 * mza);
+  m.b15 = fb; m.rkx = fb + mza; m.rky = fb + 2 * mza; m.rkz = fb + 3 * mza; m.b31 = fb + 4 * mza;
+  m.b32 = fb + 5 * mza; m.b33 = fb + 6 * mza; m.dwm = fb + 7 * mza; m.wmf = fb + 8 * mza;
+
+  const int iw = A.prog[j];
+  const int kb = g.lpw[iw];
+  const int np = g.npoly[iw];
+  const size_t cb = (size_t)iw * mza;
+  const size_t wplane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
+  const float* thil_upw = A.upw;
+  const float* vxe_upw = A.upw + wplane;
+  const float* vye_upw = A.upw + 2 * wplane;
+  const float* vze_upw = A.upw + 3 * wplane;
+  const float wnx = A.wn[iw * 3], wny = A.wn[iw * 3 + 1], wnz = A.wn[iw * 3 + 2];
+
+  // phase 1: horizontal sums, Coriolis and explicit density / rho*thil terms
+  for (int kd = kb + lane; kd < mza; kd += 32) {
+    double hf = 0.0;
+    float th = A.rk_th[cb + kd], vx = A.rk_vx[cb + kd], vy = A.rk_vy[cb + kd], vz = A.rk_vz[cb + kd];
+    for (int n = 0; n < np; ++n) {
+      const int iv = g.w_ev[iw * 8 + n];
+      if (kd < g.lpv[iv]) continue;
+      const size_t xv = (size_t)iv * mza + kd;
+      const float vm = A.vmca[xv];
+      if (g.w_dirv[iw * 8 + n] > 0.f) {
+        hf = hf + (double)vm;
+        th = th + vm * A.upv[xv];
+        vx = vx + vm * A.upv[vplane + xv];
+        vy = vy + vm * A.upv[2 * vplane + xv];
+        vz = vz + vm * A.upv[3 * vplane + xv];
+      } else {
+        hf = hf - (double)vm;
+        th = th - vm * A.upv[xv];
+        vx = vx - vm * A.upv[vplane + xv];
+        vy = vy - vm * A.upv[2 * vplane + xv];
+        vz = vz - vm * A.upv[3 * vplane + xv];
+      }
+    }
+    const double rho = A.rho[cb + kd];
+    const float mass = (float)(rho * A.volt[cb + kd]);
+    vx = vx + mass * A.fcoriol * A.vye[cb + kd];
+    vy = vy - mass * A.fcoriol * A.vxe[cb + kd];
+    const double rt = rho * (double)A.thil[cb + kd];
+    const double b10 = A.dt8 * (double)g.volti[cb + kd];
+    const double b5 = (double)(A.alpha_press[cb + kd] * powf((float)rt, A.rocv));
+    double drho = b10 * hf;
+    double drt = b10 * (double)th;
+    if (A.istage > 1) {
+      drho = drho + A.rho0[cb + kd] - rho;
+      drt = drt + A.rth0[cb + kd] - rt;
+    }
+    m.hflx[kd] = hf; m.rt[kd] = rt; m.b10[kd] = b10; m.b5[kd] = b5; m.drt[kd] = drt;
+    m.pex[kd] = b5 * (rt + A.pc2 * drt);
+    m.rex[kd] = rho + A.fr * drho;
+    m.b15[kd] = (float)(b10 * b5);
+    m.rkx[kd] = vx; m.rky[kd] = vy; m.rkz[kd] = vz;
+  }
+  __syncwarp();
+  // phase 2: explicit W momentum and the tridiagonal coefficients (faces kb..mza-2)
+  for (int kd = kb + lane; kd <= mza - 2; kd += 32) {
+    const size_t x = cb + kd;
+    const float a = (float)(m.pex[kd] - m.pex[kd + 1]) * A.pwfac[x];
+    const float b = (float)(A.gdz_wgtm8[kd] * m.rex[kd] + A.gdz_wgtp8[kd] * m.rex[kd + 1]);
+    const float c = (wnx * (m.rkx[kd] + m.rkx[kd + 1]) + wny * (m.rky[kd] + m.rky[kd + 1]) +
+                     wnz * (m.rkz[kd] + m.rkz[kd + 1])) * A.volwi[x];
+    m.dwm[kd] = A.wmc0[x] + A.dts * (a - b + c);
+    const float b7 = A.dts * A.volwi[x];
+    const float b8 = A.c8 * A.pwfac[x];
+    const float b21 = b7 * A.wc[x - 1];
+    const float b22 = b7 * A.wc[x + 1];
+    const float b23 = b8 * m.b15[kd];
+    const float b24 = b8 * m.b15[kd + 1];
+    const float b25 = A.c9 * g.volti[x] * A.gdz_wgtm[kd];
+    const float b26 = A.c9 * g.volti[x + 1] * A.gdz_wgtp[kd];
+    m.b31[kd] = -A.arw[x - 1] * (b21 + b25 + b23 * thil_upw[x - 1]);
+    m.b32[kd] = A.b20[kd] + A.arw[x] * (b25 - b26 + (b23 + b24) * thil_upw[x]);
+    m.b33[kd] = A.arw[x + 1] * (b22 + b26 - b24 * thil_upw[x + 1]);
+  }
+  __syncwarp();
+  // phase 3: tridiffo (ka..mza-1) on one lane
+  if (lane == 0 && kb <= mza - 2) {
+    float cji = 1.0f / m.b32[kb];
+    m.wmf[kb] = m.dwm[kb] * cji;
+    for (int kd = kb + 1; kd <= mza - 2; ++kd) {
+      const float scr = cji * m.b33[kd - 1];
+      m.b33[kd - 1] = scr;  // keep scr1(k) for the back substitution
+      cji = 1.0f / (m.b32[kd] - m.b31[kd] * scr);
+      m.wmf[kd] = cji * (m.dwm[kd] - m.b31[kd] * m.wmf[kd - 1]);
+    }
+    for (int kd = mza - 3; kd >= kb; --kd) m.wmf[kd] = m.wmf[kd] - m.b33[kd] * m.wmf[kd + 1];
+  }
+  __syncwarp();
+  // phase 4: implicit fluxes and the updates of rho, press, thil and vm*et_rk
+  for (int kd = kb + lane; kd < mza; kd += 32) {
+    const size_t x = cb + kd;
+    const float wma = (kd <= mza - 2) ? m.wmf[kd] * A.arw[x] : 0.f;
+    const float wmam = (kd - 1 >= kb) ? m.wmf[kd - 1] * A.arw[x - 1] : 0.f;
+    const double vft = (kd <= mza - 2) ? (double)(wma * thil_upw[x]) : 0.0;
+    const double vftm = (kd - 1 >= kb) ? (double)(wmam * thil_upw[x - 1]) : 0.0;
+    const float vfx = (kd <= mza - 2) ? wma * vxe_upw[x] : 0.f;
+    const float vfxm = (kd - 1 >= kb) ? wmam * vxe_upw[x - 1] : 0.f;
+    const float vfy = (kd <= mza - 2) ? wma * vye_upw[x] : 0.f;
+    const float vfym = (kd - 1 >= kb) ? wmam * vye_upw[x - 1] : 0.f;
+    const float vfz = (kd <= mza - 2) ? wma * vze_upw[x] : 0.f;
+    const float vfzm = (kd - 1 >= kb) ? wmam * vze_upw[x - 1] : 0.f;
+    if (A.istage == A.nrk && kd <= mza - 2) A.wmasc[x] = A.wmasc[x] + wma;
+    const double rhon = A.rho0[x] + A.dt8 * (double)g.volti[x] * (m.hflx[kd] + (double)wmam - (double)wma);
+    A.rho[x] = rhon;
+    m.rhon[kd] = rhon;
+    const double drt = m.drt[kd] + m.b10[kd] * (vftm - vft);
+    A.press[x] = m.b5[kd] * (m.rt[kd] + A.pc3 * drt);
+    A.thil[x] = (float)((m.rt[kd] + drt) / rhon);
+    A.rk_vx[x] = m.rkx[kd] + vfxm - vfx;
+    A.rk_vy[x] = m.rky[kd] + vfym - vfy;
+    A.rk_vz[x] = m.rkz[kd] + vfzm - vfz;
+  }
+  __syncwarp();
+  // phase 5: W momentum and velocity, bottom values
+  for (int kd = kb + lane; kd <= mza - 2; kd += 32) {
+    const size_t x = cb + kd;
+    const float wf = m.wmf[kd];
+    A.wmc[x] = wf;
+    A.wc[x] = wf / (float)(A.zwgt_bot8[kd] * m.rhon[kd] + A.zwgt_top8[kd] * m.rhon[kd + 1]);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    A.wc[cb + kb - 1] = A.wc[cb + kb];
+    const float t = A.thil[cb + kb];
+    for (int kd = 0; kd < kb; ++kd) A.thil[cb + kd] = t;
+  }
+}
+
+// prog_v_begs (prog_wrtv_rk.f90:888-946)
+__global__ void k_prog_v(DynK g, const int* __restrict__ vprog, int nv, float dts, const float* __restrict__ vmc0,
+                         const float* __restrict__ vmt_short, const double* __restrict__ press,
+                         const float* __restrict__ pvfac, const float* __restrict__ vn,
+                         const float* __restrict__ rkx, const float* __restrict__ rky,
+                         const float* __restrict__ rkz, const float* __restrict__ volvi,
+                         const double* __restrict__ rho, float* __restrict__ vmc, float* __restrict__ vc) {
+  PK(j, kd, nv);
+  const int iv = vprog[j];
+  if (kd < g.lpv[iv]) return;
+  const int mza = g.mza;
+  const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  const size_t x = (size_t)iv * mza + kd, x1 = (size_t)iw1 * mza + kd, x2 = (size_t)iw2 * mza + kd;
+  const float pgf = (float)(press[x1] - press[x2]) * pvfac[x];
+  const float v = vmc0[x] + dts * (vmt_short[x] + pgf +
+                                   (vn[iv * 3] * (rkx[x1] + rkx[x2]) + vn[iv * 3 + 1] * (rky[x1] + rky[x2]) +
+                                    vn[iv * 3 + 2] * (rkz[x1] + rkz[x2])) * volvi[x]);
+  vmc[x] = v;
+  vc[x] = 2.0f * v / (float)(rho[x1] + rho[x2]);
+}
+
+// vel_t3d_hex (vel_t3d.f90:39-108), no shaved cells
+__global__ void k_vel_t3d(DynK g, const int* __restrict__ prog, int nprog, const float* __restrict__ wc,
+                          const float* __restrict__ vc, const float* __restrict__ wno2,
+                          const float* __restrict__ ecv, float* __restrict__ vxe, float* __restrict__ vye,
+                          float* __restrict__ vze) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  const int kb = g.lpw[iw];
+  if (kd < kb) return;
+  const int mza = g.mza;
+  const size_t cb = (size_t)iw * mza;
+  const float wst = wc[cb + kd - 1] + wc[cb + kd];
+  float x = wst * wno2[iw * 3], y = wst * wno2[iw * 3 + 1], z = wst * wno2[iw * 3 + 2];
+  const int np = g.npoly[iw];
+  for (int n = 0; n < np; ++n) {
+    const int iv = g.w_ev[iw * 8 + n];
+    if (kd < g.lpv[iv]) continue;
+    const float v = vc[(size_t)iv * mza + kd];
+    x = x + ecv[(iw * 7 + n) * 3] * v;
+    y = y + ecv[(iw * 7 + n) * 3 + 1] * v;
+    z = z + ecv[(iw * 7 + n) * 3 + 2] * v;
+  }
+  vxe[cb + kd] = x; vye[cb + kd] = y; vze[cb + kd] = z;
+  if (kd == kb)
+    for (int k2 = 0; k2 < kb; ++k2) { vxe[cb + k2] = x; vye[cb + k2] = y; vze[cb + k2] = z; }
+}
+
+// tend0 (timestep.f90:430-496) for the hot-path arrays
+__global__ void k_tend0_w(DynK g, float* thilt, float* vmxet, float* vmyet, float* vmzet,
+                          const double* rho, float* rho_old, float* wmasc) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)(g.mwa - 1) * g.mza) return;
+  const int iw = 1 + (int)(i / g.mza), kd = (int)(i % g.mza);
+  if (kd < g.lpw[iw]) return;
+  const size_t x = (size_t)iw * g.mza + kd;
+  thilt[x] = 0.f; vmxet[x] = 0.f; vmyet[x] = 0.f; vmzet[x] = 0.f;
+  rho_old[x] = (float)rho[x];
+  wmasc[x] = 0.f;
+}
+
+__global__ void k_tend0_v(DynK g, float* vmt, float* vmasc) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)(g.mva - 1) * g.mza) return;
+  const int iv = 1 + (int)(i / g.mza), kd = (int)(i % g.mza);
+  if (kd < g.lpv[iv]) return;
+  const size_t x = (size_t)iv * g.mza + kd;
+  vmt[x] = 0.f;
+  vmasc[x] = 0.f;
+}
+
+// timeavg_momsc (timestep.f90:563-612)
+__global__ void k_timeavg_v(DynK g, const int* __restrict__ vadj, int nv, float a, float* vmasc) {
+  PK(j, kd, nv);
+  const int iv = vadj[j];
+  if (kd < g.lpv[iv]) return;
+  vmasc[(size_t)iv * g.mza + kd] = vmasc[(size_t)iv * g.mza + kd] / a;
+}
+
+__global__ void k_timeavg_w(DynK g, const int* __restrict__ prog, int nprog, float a, float* wmasc) {
+  PK(j, kd, nprog);
+  const int iw = prog[j];
+  if (kd < g.lpw[iw] || kd > g.mza - 2) return;
+  wmasc[(size_t)iw * g.mza + kd] = wmasc[(size_t)iw * g.mza + kd] / a;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <class T>
+static int up(DevBuf<T>& b, const T* h, size_t n, cudaStream_t s, const char* name) {
+  if (!h) {
+    set_error(std::string("olamgpu_grid/opts: ") + name + " is NULL (needed by prog_wrtv_rk)");
+    return OLAMGPU_E_ARG;
+  }
+  return upload(b, h, n, s);
+}
+
+int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s) {
+  Context& C = ctx();
+  Dyn& y = C.dy;
+  const int mza = g->mza, mwa = g->mwa, mva = g->mva, mma = g->mma;
+  if (!g->itab_m_iv || !g->jtm_prog || g->nm_prog <= 0 || !g->lpm) {
+    set_error("prog_wrtv_rk needs the M-point tables (itab_m, jtm_prog, lpm)");
+    return OLAMGPU_E_ARG;
+  }
+  for (int i = 1; i < mma; ++i)
+    if (g->lpm[i] != 2) { set_error("prog_wrtv_rk on this build needs flat terrain (lpm = 2)"); return OLAMGPU_E_UNSUPPORTED; }
+  if (!C.tp.flat) { set_error("prog_wrtv_rk on this build needs flat terrain (lpw = lpv = 2)"); return OLAMGPU_E_UNSUPPORTED; }
+  for (int i = 1; i < mwa; ++i)
+    if (g->lve2 && g->lve2[i] != 0) { set_error("shaved cells (lve2 > 0) are not supported"); return OLAMGPU_E_UNSUPPORTED; }
+  if (mza > 128) { set_error("prog_wrtv_rk supports mza <= 128"); return OLAMGPU_E_UNSUPPORTED; }
+  OG_CHECK(up(y.arv, g->arv, (size_t)mza * mva, s, "arv"));
+  OG_CHECK(up(y.arw, g->arw, (size_t)mza * mwa, s, "arw"));
+  OG_CHECK(up(y.volwi, g->volwi, (size_t)mza * mwa, s, "volwi"));
+  OG_CHECK(up(y.volvi, g->volvi, (size_t)mza * mva, s, "volvi"));
+  OG_CHECK(up(y.volt, g->volt, (size_t)mza * mwa, s, "volt"));
+  {
+    if (!g->wnx || !g->wnxo2 || !g->vnx || !g->ecvec_vx) { set_error("normals/ecvec missing"); return OLAMGPU_E_ARG; }
+    std::vector<float> wn((size_t)mwa * 3), wno2((size_t)mwa * 3), vn((size_t)mva * 3), ec((size_t)mwa * 21);
+    for (int i = 0; i < mwa; ++i) {
+      wn[i * 3] = g->wnx[i]; wn[i * 3 + 1] = g->wny[i]; wn[i * 3 + 2] = g->wnz[i];
+      wno2[i * 3] = g->wnxo2[i]; wno2[i * 3 + 1] = g->wnyo2[i]; wno2[i * 3 + 2] = g->wnzo2[i];
+      for (int n = 0; n < 7; ++n) {
+        ec[(i * 7 + n) * 3] = g->ecvec_vx[i * 7 + n];
+        ec[(i * 7 + n) * 3 + 1] = g->ecvec_vy[i * 7 + n];
+        ec[(i * 7 + n) * 3 + 2] = g->ecvec_vz[i * 7 + n];
+      }
+    }
+    for (int i = 0; i < mva; ++i) { vn[i * 3] = g->vnx[i]; vn[i * 3 + 1] = g->vny[i]; vn[i * 3 + 2] = g->vnz[i]; }
+    OG_CHECK(upload(y.wn, wn.data(), wn.size(), s));
+    OG_CHECK(upload(y.wno2, wno2.data(), wno2.size(), s));
+    OG_CHECK(upload(y.vn, vn.data(), vn.size(), s));
+    OG_CHECK(upload(y.ecv, ec.data(), ec.size(), s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+  OG_CHECK(up(y.gdz_wgtm, g->gdz_wgtm, mza, s, "gdz_wgtm"));
+  OG_CHECK(up(y.gdz_wgtp, g->gdz_wgtp, mza, s, "gdz_wgtp"));
+  OG_CHECK(up(y.gdz_wgtm8, g->gdz_wgtm8, mza, s, "gdz_wgtm8"));
+  OG_CHECK(up(y.gdz_wgtp8, g->gdz_wgtp8, mza, s, "gdz_wgtp8"));
+  OG_CHECK(up(y.zwgt_top8, g->zwgt_top8, mza, s, "zwgt_top8"));
+  OG_CHECK(up(y.zwgt_bot8, g->zwgt_bot8, mza, s, "zwgt_bot8"));
+  OG_CHECK(up(y.dniv, g->dniv, mva, s, "dniv"));
+  OG_CHECK(up(y.dniu, g->dniu, mva, s, "dniu"));
+  OG_CHECK(up(y.dnv, g->dnv, mva, s, "dnv"));
+  OG_CHECK(up(y.arw0, g->arw0, mwa, s, "arw0"));
+  OG_CHECK(up(y.arm0, g->arm0, mma, s, "arm0"));
+  OG_CHECK(up(y.zfacit, g->zfacit, mza, s, "zfacit"));
+  OG_CHECK(up(y.dzit, g->dzit, mza, s, "dzit"));
+  OG_CHECK(up(y.xx_yy, g->xx_yy, (size_t)mwa * 7, s, "xx_yy"));
+  OG_CHECK(up(y.xx_yy_m, g->xx_yy_m, (size_t)mma * 3, s, "xx_yy_m"));
+  // init_wrtv_rk (prog_wrtv_rk.f90:36-54): b20 = 1 + dtsm * rayf_cofw
+  std::vector<float> b20(mza, 1.0f);
+  if (o->rayf_cofw)
+    for (int k = o->krayfw_bot; k <= mza - 1; ++k) b20[k - 1] = 1.0f + (float)o->dtsm * o->rayf_cofw[k - 1];
+  OG_CHECK(upload(y.b20, b20.data(), b20.size(), s));
+  if (o->rayf_cof) {
+    OG_CHECK(up(y.rayf_cof, o->rayf_cof, mza, s, "rayf_cof"));
+    if (o->initial == 1) {
+      OG_CHECK(up(y.dn01d, o->dn01d, mza, s, "dn01d"));
+      OG_CHECK(up(y.th01d, o->th01d, mza, s, "th01d"));
+    }
+    OG_CHECK(up(y.vc03d, o->vc03d, (size_t)mza * mva, s, "vc03d"));
+  }
+  OG_CUDA(cudaStreamSynchronize(s));
+  y.div_first = y.vort_first = true;
+  y.uploaded = false;
+  y.ready = true;
+  return OLAMGPU_OK;
+}
+
+static int ensure_dyn_buffers(Context& C) {
+  Dyn& y = C.dy;
+  Transport& tp = C.tp;
+  const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva, mz = (size_t)C.g.mza * C.g.mma;
+  auto A = [](auto& b, size_t n) { return b.p ? OLAMGPU_OK : b.alloc(n); };
+  OG_CHECK(A(tp.rho, wz)); OG_CHECK(A(tp.vmasc, vz)); OG_CHECK(A(tp.wmasc, wz)); OG_CHECK(A(tp.wc, wz));
+  OG_CHECK(A(tp.rho_old, wz));
+  OG_CHECK(A(y.press, wz)); OG_CHECK(A(y.rho0, wz)); OG_CHECK(A(y.rth0, wz));
+  DevBuf<float>* w[] = {&y.thil, &y.wmc, &y.vxe, &y.vye, &y.vze, &y.alpha_press, &y.pwfac, &y.thilt,
+                        &y.vmxet, &y.vmyet, &y.vmzet, &y.wmc0, &y.sh_th, &y.sh_vx, &y.sh_vy, &y.sh_vz,
+                        &y.rk_th, &y.rk_vx, &y.rk_vy, &y.rk_vz};
+  for (auto* b : w) OG_CHECK(A(*b, wz));
+  DevBuf<float>* v[] = {&y.vmc, &y.vc, &y.pvfac, &y.vmt, &y.vmc0, &y.vmca, &y.sh_vmt, &y.fdivh};
+  for (auto* b : v) OG_CHECK(A(*b, vz));
+  OG_CHECK(A(y.upw, 4 * wz));
+  OG_CHECK(A(y.upv, 4 * vz));
+  OG_CHECK(A(y.gx, 20 * wz));
+  OG_CHECK(A(y.div2d, 2 * wz));
+  OG_CHECK(A(y.vort2d, 2 * mz));
+  OG_CHECK(A(y.fvorth, C.g.mva)); OG_CHECK(A(y.fvortl, C.g.mva));
+  OG_CHECK(A(y.vfact, 3 * (size_t)C.g.mma)); OG_CHECK(A(y.lpmmin, C.g.mma));
+  return OLAMGPU_OK;
+}
+
+// host <-> device copies of the registered mem_basic / mem_tend arrays
+int dyn_state_to_device(unsigned mask, cudaStream_t s) {
+  Context& C = ctx();
+  if (!C.have_state) return OLAMGPU_OK;
+  OG_CHECK(ensure_dyn_buffers(C));
+  const olamgpu_state& h = C.hstate;
+  Dyn& y = C.dy;
+  Transport& tp = C.tp;
+  const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva;
+  auto cp = [&](void* d, const void* hp, size_t bytes) -> int {
+    if (!hp) return OLAMGPU_OK;
+    OG_CUDA(cudaMemcpyAsync(d, hp, bytes, cudaMemcpyHostToDevice, s));
+    return OLAMGPU_OK;
+  };
+  if (mask & OLAMGPU_F_RHO) OG_CHECK(cp(tp.rho.p, h.rho, wz * 8));
+  if (mask & OLAMGPU_F_PRESS) OG_CHECK(cp(y.press.p, h.press, wz * 8));
+  if (mask & OLAMGPU_F_THIL) OG_CHECK(cp(y.thil.p, h.thil, wz * 4));
+  if (mask & OLAMGPU_F_WC) OG_CHECK(cp(tp.wc.p, h.wc, wz * 4));
+  if (mask & OLAMGPU_F_WMC) OG_CHECK(cp(y.wmc.p, h.wmc, wz * 4));
+  if (mask & OLAMGPU_F_VXE) {
+    OG_CHECK(cp(y.vxe.p, h.vxe, wz * 4)); OG_CHECK(cp(y.vye.p, h.vye, wz * 4)); OG_CHECK(cp(y.vze.p, h.vze, wz * 4));
+  }
+  if (mask & OLAMGPU_F_VMC) OG_CHECK(cp(y.vmc.p, h.vmc, vz * 4));
+  if (mask & OLAMGPU_F_VC) OG_CHECK(cp(y.vc.p, h.vc, vz * 4));
+  if (mask & OLAMGPU_F_VMASC) OG_CHECK(cp(tp.vmasc.p, h.vmasc, vz * 4));
+  if (mask & OLAMGPU_F_WMASC) OG_CHECK(cp(tp.wmasc.p, h.wmasc, wz * 4));
+  if (mask & OLAMGPU_F_FACS) {
+    OG_CHECK(cp(y.alpha_press.p, h.alpha_press, wz * 4)); OG_CHECK(cp(y.pwfac.p, h.pwfac, wz * 4));
+    OG_CHECK(cp(y.pvfac.p, h.pvfac, vz * 4));
+  }
+  if (mask & OLAMGPU_F_TEND) {
+    OG_CHECK(cp(y.thilt.p, h.thilt, wz * 4)); OG_CHECK(cp(y.vmxet.p, h.vmxet, wz * 4));
+    OG_CHECK(cp(y.vmyet.p, h.vmyet, wz * 4)); OG_CHECK(cp(y.vmzet.p, h.vmzet, wz * 4));
+    OG_CHECK(cp(y.vmt.p, h.vmt, vz * 4));
+  }
+  return OLAMGPU_OK;
+}
+
+int dyn_state_to_host(unsigned mask, cudaStream_t s) {
+  Context& C = ctx();
+  if (!C.have_state || !C.dy.thil.p) return OLAMGPU_OK;
+  const olamgpu_state& h = C.hstate;
+  Dyn& y = C.dy;
+  Transport& tp = C.tp;
+  const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva;
+  auto cp = [&](void* hp, const void* d, size_t bytes) -> int {
+    if (!hp || !d) return OLAMGPU_OK;
+    OG_CUDA(cudaMemcpyAsync(hp, d, bytes, cudaMemcpyDeviceToHost, s));
+    return OLAMGPU_OK;
+  };
+  if (mask & OLAMGPU_F_RHO) OG_CHECK(cp(h.rho, tp.rho.p, wz * 8));
+  if (mask & OLAMGPU_F_PRESS) OG_CHECK(cp(h.press, y.press.p, wz * 8));
+  if (mask & OLAMGPU_F_THIL) OG_CHECK(cp(h.thil, y.thil.p, wz * 4));
+  if (mask & OLAMGPU_F_WC) OG_CHECK(cp(h.wc, tp.wc.p, wz * 4));
+  if (mask & OLAMGPU_F_WMC) OG_CHECK(cp(h.wmc, y.wmc.p, wz * 4));
+  if (mask & OLAMGPU_F_VXE) {
+    OG_CHECK(cp(h.vxe, y.vxe.p, wz * 4)); OG_CHECK(cp(h.vye, y.vye.p, wz * 4)); OG_CHECK(cp(h.vze, y.vze.p, wz * 4));
+  }
+  if (mask & OLAMGPU_F_VMC) OG_CHECK(cp(h.vmc, y.vmc.p, vz * 4));
+  if (mask & OLAMGPU_F_VC) OG_CHECK(cp(h.vc, y.vc.p, vz * 4));
+  if (mask & OLAMGPU_F_VMASC) OG_CHECK(cp(h.vmasc, tp.vmasc.p, vz * 4));
+  if (mask & OLAMGPU_F_WMASC) OG_CHECK(cp(h.wmasc, tp.wmasc.p, wz * 4));
+  if (mask & OLAMGPU_F_TEND) {
+    OG_CHECK(cp(h.thilt, y.thilt.p, wz * 4)); OG_CHECK(cp(h.vmxet, y.vmxet.p, wz * 4));
+    OG_CHECK(cp(h.vmyet, y.vmyet.p, wz * 4)); OG_CHECK(cp(h.vmzet, y.vmzet.p, wz * 4));
+    OG_CHECK(cp(h.vmt, y.vmt.p, vz * 4));
+  }
+  return OLAMGPU_OK;
+}
+
+#define DYN_IN_MASK (OLAMGPU_F_RHO | OLAMGPU_F_PRESS | OLAMGPU_F_THIL | OLAMGPU_F_WC | OLAMGPU_F_WMC | \
+                     OLAMGPU_F_VXE | OLAMGPU_F_VMC | OLAMGPU_F_VC | OLAMGPU_F_VMASC | OLAMGPU_F_WMASC | \
+                     OLAMGPU_F_FACS | OLAMGPU_F_TEND)
+#define DYN_OUT_MASK (OLAMGPU_F_RHO | OLAMGPU_F_PRESS | OLAMGPU_F_THIL | OLAMGPU_F_WC | OLAMGPU_F_WMC | \
+                      OLAMGPU_F_VXE | OLAMGPU_F_VMC | OLAMGPU_F_VC | OLAMGPU_F_VMASC | OLAMGPU_F_WMASC | \
+                      OLAMGPU_F_TEND)
+
+static void divh_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
+  const olamgpu_opts& o = C.opts;
+  const DevGrid& d = C.g;
+  Dyn& y = C.dy;
+  if (!(o.divh_damp_fact > 1.e-7f) || o.divh_damp_level <= 0) return;
+  const int level = o.divh_damp_level;
+  const DynK g = dynk(d);
+  const size_t wz = (size_t)d.mza * d.mwa;
+  const unsigned nbv = cdiv((size_t)d.nv_prog * d.mza, 256), nbw = cdiv((size_t)d.nw_prog * d.mza, 256);
+  if (y.div_first) {
+    y.div_first = false;
+    cudaMemsetAsync(y.div2d.p, 0, 2 * wz * sizeof(float), s);
+    float p = 1.f;
+    for (int i = 0; i < level; ++i) p = p * (-o.divh_damp_fact);
+    const double facth = -((double)p / dtm);
+    const float fact2 = o.divh_damp_fact / (float)dtm;
+    k_div_fdivh<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.arw0.p, y.dniv.p, y.zfacit.p, y.dzit.p,
+                                    y.volt.p, facth, level, fact2, y.fdivh.p);
+    OG_LAUNCHED();
+  }
+  float* d1 = y.div2d.p;
+  k_div_accum<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.arv.p, y.vmc.p, d1);
+  OG_LAUNCHED();
+  const float* dh = d1;
+  if (level > 1) {
+    int ih = 2;
+    for (int nn = 1; nn <= level - 1; ++nn) {
+      const int il = (nn - 1) % 2 + 1;
+      ih = nn % 2 + 1;
+      k_lap_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.xx_yy.p, y.div2d.p + (il - 1) * wz,
+                                  y.div2d.p + (ih - 1) * wz);
+      OG_LAUNCHED();
+    }
+    dh = y.div2d.p + (ih - 1) * wz;
+  }
+  k_div_apply<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.fdivh.p, dh, vmt);
+  OG_LAUNCHED();
+}
+
+static void vort_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
+  const olamgpu_opts& o = C.opts;
+  const DevGrid& d = C.g;
+  Dyn& y = C.dy;
+  if (o.vort_damp_fact < 1.e-7f || o.vort_damp_level <= 0) return;
+  const int level = o.vort_damp_level;
+  const DynK g = dynk(d);
+  const size_t mz = (size_t)d.mza * d.mma;
+  if (y.vort_first) {
+    y.vort_first = false;
+    k_vort_first_m<<<cdiv(d.nm_prog, 128), 128, 0, s>>>(g, d.jtm_prog.p, d.nm_prog, y.dnv.p, y.arm0.p, y.vfact.p,
+                                                        y.lpmmin.p);
+    k_vort_first_v<<<cdiv(d.nv_prog, 128), 128, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.dniu.p, y.arm0.p, (float)dtm,
+                                                        o.vort_damp_fact, level, y.fvorth.p, y.fvortl.p);
+    OG_LAUNCHED(); OG_LAUNCHED();
+  }
+  const unsigned nbm = cdiv((size_t)d.nm_prog * d.mza, 256), nbv = cdiv((size_t)d.nv_prog * d.mza, 256);
+  k_vort<<<nbm, 256, 0, s>>>(g, d.jtm_prog.p, d.nm_prog, y.vfact.p, y.vc.p, y.vort2d.p);
+  OG_LAUNCHED();
+  int il = 1, ih = 1;
+  if (level > 1) {
+    for (int nn = 1; nn <= level - 1; ++nn) {
+      il = (nn - 1) % 2 + 1;
+      ih = nn % 2 + 1;
+      k_lap_m<<<nbm, 256, 0, s>>>(g, d.jtm_prog.p, d.nm_prog, y.xx_yy_m.p, y.vort2d.p + (il - 1) * mz,
+                                  y.vort2d.p + (ih - 1) * mz);
+      OG_LAUNCHED();
+    }
+  }
+  k_vort_apply<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, level, y.fvorth.p, y.fvortl.p,
+                                   y.vort2d.p + (il - 1) * mz, y.vort2d.p + (ih - 1) * mz, C.tp.rho.p, vmt);
+  OG_LAUNCHED();
+}
+
+int dyn_prog_wrtv_rk(int istp) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (!C.dy.ready) { set_error("prog_wrtv_rk was not set up (see olamgpu_init's status)"); return OLAMGPU_E_STATE; }
+  if (!C.have_state) { set_error("prog_wrtv_rk needs the state arrays registered at init"); return OLAMGPU_E_STATE; }
+  const olamgpu_opts& o = C.opts;
+  if (o.ithil_monot > 0 || o.iwind_monot > 0) {
+    set_error("ithil_monot / iwind_monot > 0 (fluxes_wrtv_monot) is not available in this build");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  if (o.nrk_wrtv != 2 && o.nrk_wrtv != 3) { set_error("acoust_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  cudaStream_t s = C.stream;
+  OG_CHECK(ensure_dyn_buffers(C));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL || !C.dy.uploaded) OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s));
+  C.dy.uploaded = true;
+  const DevGrid& d = C.g;
+  Dyn& y = C.dy;
+  Transport& tp = C.tp;
+  const DynK g = dynk(d);
+  const int mza = d.mza;
+  const unsigned nbw = cdiv((size_t)d.nw_prog * mza, 256), nbv = cdiv((size_t)d.nv_prog * mza, 256),
+                 nbva = cdiv((size_t)d.nv_wadj * mza, 256);
+  OG_PROF("dyn_setup", s);
+  if (!o.divh_damp_short && istp == 1) divh_damp(C, y.vmt.p, o.dtlm, s);
+  if (!o.vort_damp_short && istp == 1) vort_damp(C, y.vmt.p, o.dtlm, s);
+  SetupW sw{tp.rho.p, y.thil.p, y.wmc.p, y.thilt.p, y.vmxet.p, y.vmyet.p, y.vmzet.p, y.volt.p, y.rho0.p,
+            y.rth0.p, y.wmc0.p, y.sh_th.p, y.sh_vx.p, y.sh_vy.p, y.sh_vz.p, y.rayf_cof.p, y.dn01d.p, y.th01d.p,
+            o.krayf_bot};
+  if (!(o.rayf_cof && o.initial == 1)) sw.rayf_cof = nullptr;
+  k_setup_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, sw);
+  k_setup_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.vmc.p, y.vmt.p, y.vmc0.p, y.sh_vmt.p,
+                                (o.rayf_cof && o.vc03d) ? y.rayf_cof.p : nullptr, y.vc03d.p, y.vc.p, tp.rho.p,
+                                o.krayf_bot);
+  OG_LAUNCHED(); OG_LAUNCHED();
+  if (o.divh_damp_short) divh_damp(C, y.sh_vmt.p, o.dtsm, s);
+  if (o.vort_damp_short) vort_damp(C, y.sh_vmt.p, o.dtsm, s);
+
+  const int nrk = o.nrk_wrtv;
+  const double third = 1.0 / 3.0;
+  const double xstg3[3] = {third, 0.5, 1.0}, xstg2[2] = {0.5, 1.0};
+  const size_t wz = (size_t)mza * d.mwa;
+  for (int istage = 1; istage <= nrk; ++istage) {
+    const double dt8 = (nrk <= 2 ? xstg2[istage - 1] : xstg3[istage - 1]) * o.dtsm;
+    const float dts = (float)dt8;
+    const int last = istage == nrk;
+    k_rk_copy<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.sh_th.p, y.sh_vx.p, y.sh_vy.p, y.sh_vz.p,
+                                  y.rk_th.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p);
+    k_vmca<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, y.vmc.p, y.arv.p, y.vmca.p, tp.vmasc.p, last);
+    Four f{{y.thil.p, y.vxe.p, y.vye.p, y.vze.p}};
+    k_grad4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, o.thil_horiz_adv_order, o.wind_horiz_adv_order,
+                                d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p);
+    k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p);
+    VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
+    k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, o.thil_horiz_adv_order, o.wind_horiz_adv_order,
+                                y.gx.p, vs, y.vmc.p, y.upv.p);
+    OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+    WrtArgs A;
+    A.istage = istage; A.nrk = nrk; A.dt8 = dt8; A.dts = dts; A.fcoriol = o.fcoriol;
+    A.fr = (double)0.70f;
+    const float cpocv = 1004.f / 717.f;
+    A.pc2 = A.fr * (double)cpocv;
+    A.pc3 = A.fr * (double)cpocv;
+    A.rocv = (1004.f - 717.f) / 717.f;
+    A.c8 = dts * (float)A.pc2;
+    A.c9 = -dts * dts * (float)A.fr;
+    A.prog = d.jtw_prog.p; A.nprog = d.nw_prog;
+    A.vmca = y.vmca.p; A.upv = y.upv.p; A.upw = y.upw.p;
+    A.rk_th = y.rk_th.p; A.rk_vx = y.rk_vx.p; A.rk_vy = y.rk_vy.p; A.rk_vz = y.rk_vz.p;
+    A.rho = tp.rho.p; A.press = y.press.p; A.rho0 = y.rho0.p; A.rth0 = y.rth0.p;
+    A.thil = y.thil.p; A.wc = tp.wc.p; A.wmc = y.wmc.p; A.wmc0 = y.wmc0.p; A.vxe = y.vxe.p; A.vye = y.vye.p;
+    A.wmasc = tp.wmasc.p; A.alpha_press = y.alpha_press.p; A.pwfac = y.pwfac.p;
+    A.volt = y.volt.p; A.volwi = y.volwi.p; A.arw = y.arw.p; A.wn = y.wn.p;
+    A.gdz_wgtm8 = y.gdz_wgtm8.p; A.gdz_wgtp8 = y.gdz_wgtp8.p; A.gdz_wgtm = y.gdz_wgtm.p; A.gdz_wgtp = y.gdz_wgtp.p;
+    A.zwgt_bot8 = y.zwgt_bot8.p; A.zwgt_top8 = y.zwgt_top8.p; A.b20 = y.b20.p;
+    const size_t smem = (size_t)WRT_WARPS * mza * 13 * sizeof(double);
+    k_wrt_begs<<<cdiv(d.nw_prog, WRT_WARPS), WRT_WARPS * 32, smem, s>>>(g, A);
+    k_prog_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, dts, y.vmc0.p, y.sh_vmt.p, y.press.p, y.pvfac.p,
+                                 y.vn.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p, y.volvi.p, tp.rho.p, y.vmc.p, y.vc.p);
+    k_vel_t3d<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, tp.wc.p, y.vc.p, y.wno2.p, y.ecv.p, y.vxe.p,
+                                  y.vye.p, y.vze.p);
+    OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+  }
+  (void)wz;
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
+    OG_CHECK(dyn_state_to_host(DYN_OUT_MASK, s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+  OG_CUDA(cudaGetLastError());
+  return OLAMGPU_OK;
+}
+
+int dyn_tend0(float* rho_old_host) {
+  Context& C = ctx();
+  if (!C.initialised || !C.dy.ready || !C.have_state) { set_error("tend0 before init"); return OLAMGPU_E_STATE; }
+  cudaStream_t s = C.stream;
+  OG_CHECK(ensure_dyn_buffers(C));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(dyn_state_to_device(OLAMGPU_F_RHO, s));
+  else if (!C.dy.uploaded) { OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s)); C.dy.uploaded = true; }
+  const DynK g = dynk(C.g);
+  Dyn& y = C.dy;
+  Transport& tp = C.tp;
+  k_tend0_w<<<cdiv((size_t)(C.g.mwa - 1) * C.g.mza, 256), 256, 0, s>>>(g, y.thilt.p, y.vmxet.p, y.vmyet.p,
+                                                                      y.vmzet.p, tp.rho.p, tp.rho_old.p,
+                                                                      tp.wmasc.p);
+  k_tend0_v<<<cdiv((size_t)(C.g.mva - 1) * C.g.mza, 256), 256, 0, s>>>(g, y.vmt.p, tp.vmasc.p);
+  OG_LAUNCHED(); OG_LAUNCHED();
+  // scalar tendencies var_t = 0 for k >= lpw (the device copies)
+  for (int n = 0; n < C.tr.n; ++n) OG_CUDA(cudaMemsetAsync(C.tr.t[n].p, 0, (size_t)C.g.mza * C.g.mwa * 4, s));
+  if (C.tr.q_valid && C.tr.qt.p) OG_CUDA(cudaMemsetAsync(C.tr.qt.p, 0, C.tr.qt.bytes(), s));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
+    OG_CHECK(dyn_state_to_host(OLAMGPU_F_TEND | OLAMGPU_F_VMASC | OLAMGPU_F_WMASC, s));
+    if (rho_old_host)
+      OG_CUDA(cudaMemcpyAsync(rho_old_host, tp.rho_old.p, (size_t)C.g.mza * C.g.mwa * 4, cudaMemcpyDeviceToHost, s));
+    for (int n = 0; n < C.tr.n; ++n)
+      OG_CUDA(cudaMemcpyAsync(C.tr.h_t[n], C.tr.t[n].p, (size_t)C.g.mza * C.g.mwa * 4, cudaMemcpyDeviceToHost, s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+  return OLAMGPU_OK;
+}
+
+int dyn_timeavg_momsc() {
+  Context& C = ctx();
+  if (!C.initialised || !C.dy.ready) { set_error("timeavg_momsc before init"); return OLAMGPU_E_STATE; }
+  if (C.opts.nacoust <= 1) return OLAMGPU_OK;
+  cudaStream_t s = C.stream;
+  OG_CHECK(ensure_dyn_buffers(C));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(dyn_state_to_device(OLAMGPU_F_VMASC | OLAMGPU_F_WMASC, s));
+  else if (!C.dy.uploaded) { OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s)); C.dy.uploaded = true; }
+  const DynK g = dynk(C.g);
+  const float a = (float)C.opts.nacoust;
+  k_timeavg_v<<<cdiv((size_t)C.g.nv_wadj * C.g.mza, 256), 256, 0, s>>>(g, C.g.jtv_wadj.p, C.g.nv_wadj, a, C.tp.vmasc.p);
+  k_timeavg_w<<<cdiv((size_t)C.g.nw_prog * C.g.mza, 256), 256, 0, s>>>(g, C.g.jtw_prog.p, C.g.nw_prog, a, C.tp.wmasc.p);
+  OG_LAUNCHED(); OG_LAUNCHED();
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
+    OG_CHECK(dyn_state_to_host(OLAMGPU_F_VMASC | OLAMGPU_F_WMASC, s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+  return OLAMGPU_OK;
+}
+
+void dyn_release() {
+  Dyn& y = ctx().dy;
+  DevBuf<double>* d8[] = {&y.press, &y.rho0, &y.rth0, &y.volt, &y.zwgt_top8, &y.zwgt_bot8, &y.gdz_wgtm8, &y.gdz_wgtp8};
+  for (auto* b : d8) b->release();
+  DevBuf<float>* f[] = {&y.thil, &y.wmc, &y.vxe, &y.vye, &y.vze, &y.vmc, &y.vc, &y.alpha_press, &y.pwfac,
+                        &y.pvfac, &y.thilt, &y.vmxet, &y.vmyet, &y.vmzet, &y.vmt, &y.wmc0, &y.vmc0, &y.vmca,
+                        &y.sh_th, &y.sh_vx, &y.sh_vy, &y.sh_vz, &y.sh_vmt, &y.rk_th, &y.rk_vx, &y.rk_vy,
+                        &y.rk_vz, &y.upw, &y.upv, &y.gx, &y.div2d, &y.fdivh, &y.vort2d, &y.fvorth, &y.fvortl,
+                        &y.vfact, &y.arv, &y.arw, &y.volwi, &y.volvi, &y.wn, &y.wno2, &y.vn, &y.ecv,
+                        &y.gdz_wgtm, &y.gdz_wgtp, &y.dniv, &y.dniu, &y.dnv, &y.arw0, &y.arm0, &y.zfacit,
+                        &y.dzit, &y.xx_yy, &y.xx_yy_m, &y.b20, &y.rayf_cof, &y.dn01d, &y.th01d, &y.vc03d};
+  for (auto* b : f) b->release();
+  y.lpmmin.release();
+  y = Dyn();
+}
+
+}  // namespace olamgpu

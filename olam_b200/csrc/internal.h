@@ -176,6 +176,30 @@ struct Transport {
   bool have_turb = false;
 };
 
+// Device state and scratch of prog_wrtv_rk (omodel/prog_wrtv_rk.f90).  The
+// fields it shares with scalar_transport_rk (rho, vmasc, wmasc, wc, rho_old)
+// live in Transport so one device copy serves both.
+struct Dyn {
+  bool ready = false;            // grid metrics uploaded
+  bool uploaded = false;         // RESIDENT mode: host state copied once
+  DevBuf<double> press, rho0, rth0;
+  DevBuf<float> thil, wmc, vxe, vye, vze, vmc, vc, alpha_press, pwfac, pvfac;
+  DevBuf<float> thilt, vmxet, vmyet, vmzet, vmt;       // long-step tendencies
+  DevBuf<float> wmc0, vmc0, vmca;
+  DevBuf<float> sh_th, sh_vx, sh_vy, sh_vz, sh_vmt;    // *_short
+  DevBuf<float> rk_th, rk_vx, rk_vy, rk_vz;            // *_rk
+  DevBuf<float> upw, upv;        // 4 fields: thil, vxe, vye, vze
+  DevBuf<float> gx;              // gradient planes of the 4 fields
+  DevBuf<float> div2d, fdivh, vort2d, fvorth, fvortl, vfact;
+  DevBuf<int> lpmmin;
+  bool div_first = true, vort_first = true;
+  // grid metrics of the dynamics
+  DevBuf<float> arv, arw, volwi, volvi, wn, wno2, vn, ecv, gdz_wgtm, gdz_wgtp;
+  DevBuf<float> dniv, dniu, dnv, arw0, arm0, zfacit, dzit, xx_yy, xx_yy_m, b20;
+  DevBuf<double> volt, zwgt_top8, zwgt_bot8, gdz_wgtm8, gdz_wgtp8;
+  DevBuf<float> rayf_cof, dn01d, th01d, vc03d;
+};
+
 struct Context {
   bool initialised = false;
   int device = -1;
@@ -189,6 +213,7 @@ struct Context {
   DevGrid g;
   Tracers tr;
   Transport tp;
+  Dyn dy;
   DevBuf<int> status;        // device status word (bounds/NaN flags)
 };
 
@@ -197,6 +222,15 @@ Context& ctx();
 // set-up helpers (setup.cu)
 int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s);
 int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
+
+// dynamics entry points (dynamics.cu)
+int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s);
+int dyn_prog_wrtv_rk(int istp);
+int dyn_tend0(float* rho_old_host);
+int dyn_timeavg_momsc();
+int dyn_state_to_device(unsigned mask, cudaStream_t s);
+int dyn_state_to_host(unsigned mask, cudaStream_t s);
+void dyn_release();
 
 // transport entry points (transport.cu)
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);

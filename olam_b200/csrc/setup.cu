@@ -229,7 +229,7 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
     r[COLREC_IW] = c;
     r[COLREC_NP] = np;
     r[COLREC_KB] = g->lpw[c] - 1;
-    bool fast = (np == 6);
+    bool fast = (np == 6) && (g->lpw[c] == 2);
     int nbc[7], evc[7];
     for (int n = 0; n < np; ++n) {
       nbc[n] = g->itab_w_iw[(size_t)c * 7 + n] - 1;
@@ -243,6 +243,7 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
       r[COLREC_EV + n] = iv;
       r[COLREC_OWN + n] = own;
       r[COLREC_LPV + n] = v ? g->lpv[iv] - 1 : 0;
+      if (v && g->lpv[iv] != 2) fast = false;
       r[COLREC_DV + n] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + n] : 0.f);
       for (int m = 0; m < 7; ++m)
         r[COLREC_WOWN + n * 7 + m] = fbits(v && m < np ? wb[((size_t)iv * 2 + own) * 8 + m] : 0.f);

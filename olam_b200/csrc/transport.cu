@@ -148,6 +148,11 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     set_error("the fused transport form needs lpw = lpv = 2 (no terrain); use the plain form");
     return OLAMGPU_E_UNSUPPORTED;
   }
+  if (C.form == OLAMGPU_TRANSPORT_FUSED &&
+      (double)mwa * mza * (double)((tr.ntp + 3) / 4 * 2) >= 4294967296.0) {
+    set_error("the fused transport form needs mwa * mza * ntp / 2 < 2^32; use the plain form");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
   if (C.form == OLAMGPU_TRANSPORT_FUSED && d.ew_order != order)
     OG_CHECK(build_fused_weights(&C.hgrid, C.g, order, s));
 
@@ -162,7 +167,12 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     OG_CHECK(tracers_to_device(s));
   } else {
     // RESIDENT: device copies persist; a field never uploaded is taken from
-    // the registered host array on first use
+    // the registered host array on first use (the dynamics keeps them when
+    // it runs on the device)
+    if (C.dy.ready && !C.dy.uploaded) {
+      OG_CHECK(dyn_state_to_device(OLAMGPU_F_ALL, s));
+      C.dy.uploaded = true;
+    }
     if (!tp.vmasc.p) OG_CHECK(upload(tp.vmasc, C.hstate.vmasc, vz, s));
     if (!tp.wmasc.p) OG_CHECK(upload(tp.wmasc, C.hstate.wmasc, wz, s));
     if (!tp.rho.p) OG_CHECK(upload(tp.rho, C.hstate.rho, wz, s));

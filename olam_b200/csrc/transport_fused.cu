@@ -85,6 +85,18 @@ __device__ __forceinline__ float2 zface(const float* __restrict__ a_w, int mza, 
   return r;
 }
 
+// Per-block staging of a column record into the form the inner loop reads:
+// 32-bit row bases of the cells it gathers, per-face weights as float4
+// vectors (one broadcast LDS.128 per 4 weights) and a face-flag word.
+struct FusedSmem {
+  unsigned base[25];     // (point * mza) * nq2 for c, nb[0..5], new[6][3]
+  float4 wown[6][2];     // own-side weights of face n over nb[0..5] (+2 pad)
+  float4 wfar[6][2];     // far side: c, nb[n-1], nb[n+1], new0..2 (+1 pad)
+  float dv[6];
+  int own, nnew;         // bit n: this column is side 1 of face n; nnew(n) in 2 bits
+  int rec[COLREC_WORDS]; // raw record (general path)
+};
+
 // LPI lanes cooperate on one (column, level) cell, each lane holding one
 // float2 (2 tracers) per pass; a block covers KC levels of one column.
 // Loads of a cell are issued in two rounds: everything whose address is
@@ -92,30 +104,58 @@ __device__ __forceinline__ float2 zface(const float* __restrict__ a_w, int mza, 
 // rows of the inflow faces, whose choice depends on sign(vmasc).
 template <int LPI>
 __global__ void __launch_bounds__(FUSED_THREADS, FUSED_MINB) k_fused(FusedArgs A) {
-  __shared__ int R[COLREC_WORDS];
+  __shared__ FusedSmem T;
   const int j = blockIdx.x / A.nchunk;
   const int chunk = blockIdx.x - j * A.nchunk;
   const int mza = A.mza;
+  const int nq2 = A.nq * 2;                  // float2 per (point, level) row
+  int* R = T.rec;
   for (int i = threadIdx.x; i < COLREC_WORDS; i += FUSED_THREADS)
     R[i] = __ldg(A.colrec + (size_t)j * COLREC_WORDS + i);
   __syncthreads();
   const int iw = R[COLREC_IW], np = R[COLREC_NP], kb = R[COLREC_KB];
   const bool fast = R[COLREC_FAST] != 0;
+  const unsigned colsz = (unsigned)mza * (unsigned)nq2;
+  if (fast) {
+    const int t = threadIdx.x;
+    if (t < 25) {
+      int p;
+      if (t == 0) p = iw;
+      else if (t < 7) p = R[COLREC_NB + t - 1];
+      else {
+        const int n = (t - 7) / 3, m = (t - 7) % 3;
+        p = (m < R[COLREC_NNEW + n]) ? R[COLREC_NEW + n * 3 + m] : iw;
+      }
+      T.base[t] = (unsigned)p * colsz;
+    } else if (t >= 32 && t < 32 + 48) {
+      const int i = t - 32, n = i >> 3, m = i & 7;
+      reinterpret_cast<float*>(&T.wown[n][0])[m] = (m < 6) ? __int_as_float(R[COLREC_WOWN + n * 7 + m]) : 0.f;
+    } else if (t >= 96 && t < 96 + 48) {
+      const int i = t - 96, n = i >> 3, m = i & 7;
+      reinterpret_cast<float*>(&T.wfar[n][0])[m] = (m < 6) ? __int_as_float(R[COLREC_WU + n * 7 + m]) : 0.f;
+    } else if (t >= 160 && t < 166) {
+      T.dv[t - 160] = __int_as_float(R[COLREC_DV + t - 160]);
+    } else if (t == 192) {
+      int own = 0, nn = 0;
+      for (int n = 0; n < 6; ++n) {
+        own |= (R[COLREC_OWN + n] & 1) << n;
+        nn |= (R[COLREC_NNEW + n] & 3) << (2 * n);
+      }
+      T.own = own;
+      T.nnew = nn;
+    }
+    __syncthreads();
+  }
   const float fexpl = 1.0f - __ldg(A.ff + (size_t)iw * A.nrk + A.istage - 1);
   const float* __restrict__ wm = A.wmasc + (size_t)iw * mza;
-  const int nq2 = A.nq * 2;                  // float2 per (point, level) row
   const float2* __restrict__ S = reinterpret_cast<const float2*>(A.S);
   const float2* __restrict__ S0 = reinterpret_cast<const float2*>(A.S0);
   const float2* __restrict__ SCT = reinterpret_cast<const float2*>(A.SCT);
   float2* __restrict__ OUT = reinterpret_cast<float2*>(A.OUT);
-  const size_t colsz = (size_t)mza * nq2;
   const size_t cbase = (size_t)iw * colsz;
   constexpr int IPP = FUSED_THREADS / LPI;   // cells per pass
   const int sub = threadIdx.x / LPI, lane = threadIdx.x % LPI;
-  // weights are re-read from shared memory at each use (a broadcast LDS)
-  // instead of being hoisted into registers across the level loop
-  const volatile int* RV = R;
-  auto RF = [&](int i) { return __int_as_float(RV[i]); };
+  auto RF = [&](int i) { return __int_as_float(R[i]); };
 
   for (int kk = sub; kk < FUSED_KC; kk += IPP) {
     const int kd = chunk * FUSED_KC + kk;
@@ -123,19 +163,99 @@ __global__ void __launch_bounds__(FUSED_THREADS, FUSED_MINB) k_fused(FusedArgs A
     const float wkm1 = __ldg(wm + kd - 1), wk0 = __ldg(wm + kd);
     const float vt = __ldg(A.volti + (size_t)iw * mza + kd);
     const float rh = __ldg(A.rhos + (size_t)iw * mza + kd);
+    const unsigned lvl = (unsigned)kd * (unsigned)nq2;
+    if (fast) {
+      // ---- flat hexagonal column
+      float vm[6];
+      unsigned inflow = 0;
+#pragma unroll
+      for (int n = 0; n < 6; ++n) {
+        vm[n] = __ldg(A.vmasc + (size_t)R[COLREC_EV + n] * mza + kd);
+        const unsigned up1 = vm[n] < 0.f ? 1u : 0u;          // upwind side of face n
+        inflow |= (up1 ^ ((T.own >> n) & 1u)) << n;
+      }
+      const int nnew = T.nnew;
+      for (int q = lane; q < nq2; q += LPI) {
+        const unsigned lq = lvl + (unsigned)q;
+        const float2 s0 = ld2(S + cbase + lq);
+        const float2 sm1 = (kd - 1 >= kb) ? ld2(S + cbase + lq - nq2) : s0;
+        const float2 sp1 = (kd + 1 < mza) ? ld2(S + cbase + lq + nq2) : s0;
+        const float2 sm2 = (kd - 2 >= kb) ? ld2(S + cbase + lq - 2 * nq2) : sm1;
+        const float2 sp2 = (kd + 2 < mza) ? ld2(S + cbase + lq + 2 * nq2) : sp1;
+        float2 sn[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) sn[n] = ld2(S + (T.base[1 + n] + lq));
+        const float2 s00 = ld2(S0 + cbase + lq);
+        const float2 st = ld2(SCT + cbase + lq);
+        float2 nw[6][3];
+#pragma unroll
+        for (int n = 0; n < 6; ++n)
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+            if (((inflow >> n) & 1u) && m < ((nnew >> (2 * n)) & 3))
+              nw[n][m] = ld2(S + (T.base[7 + n * 3 + m] + lq));
+        float2 dn[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) dn[m] = sub2(sn[m], s0);
+        float2 fd = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+          float2 val;
+          if (!((inflow >> n) & 1u)) {
+            const float4 w0 = T.wown[n][0], w1 = T.wown[n][1];
+            val = s0;
+            val = axpy2(val, w0.x, dn[0]);
+            val = axpy2(val, w0.y, dn[1]);
+            val = axpy2(val, w0.z, dn[2]);
+            val = axpy2(val, w0.w, dn[3]);
+            val = axpy2(val, w1.x, dn[4]);
+            val = axpy2(val, w1.y, dn[5]);
+          } else {
+            const float4 w0 = T.wfar[n][0], w1 = T.wfar[n][1];
+            const float2 su = sn[n];
+            const int nn = (nnew >> (2 * n)) & 3;
+            val = su;
+            val = axpy2(val, w0.x, sub2(s0, su));
+            val = axpy2(val, w0.y, sub2(sn[(n + 5) % 6], su));
+            val = axpy2(val, w0.z, sub2(sn[(n + 1) % 6], su));
+            if (nn > 0) val = axpy2(val, w0.w, sub2(nw[n][0], su));
+            if (nn > 1) val = axpy2(val, w1.x, sub2(nw[n][1], su));
+            if (nn > 2) val = axpy2(val, w1.y, sub2(nw[n][2], su));
+          }
+          fd = axpy2(fd, T.dv[n] * vm[n], sub2(val, s00));
+        }
+        // ---- vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded)
+        float2 up_lo, up_hi;
+        if (kd == kb) up_lo = s0;                                                   // scp_upw(kb-1) = scp(kb)
+        else if (wkm1 < 0.f) up_lo = zface(A.a_w, mza, kb, kd, true, sm1, s0, sp1);        // scpb(kd)
+        else up_lo = zface(A.a_w, mza, kb, kd - 1, false, sm2, sm1, s0);                   // scpt(kd-1)
+        if (kd == mza - 1) up_hi = s0;                                              // scp_upw(mza) = scp(mza)
+        else if (wk0 < 0.f) up_hi = zface(A.a_w, mza, kb, kd + 1, true, s0, sp1, sp2);     // scpb(kd+1)
+        else up_hi = zface(A.a_w, mza, kb, kd, false, sm1, s0, sp1);                       // scpt(kd)
+        float2 o;
+        {
+          float v = fexpl * (wkm1 * (up_lo.x - s00.x) - wk0 * (up_hi.x - s00.x));
+          o.x = s00.x + A.dtr * (st.x + vt * (fd.x + v)) / rh;
+          v = fexpl * (wkm1 * (up_lo.y - s00.y) - wk0 * (up_hi.y - s00.y));
+          o.y = s00.y + A.dtr * (st.y + vt * (fd.y + v)) / rh;
+        }
+        OUT[cbase + lq] = o;
+        if (kd == kb)
+          for (int k2 = 0; k2 < kb; ++k2) OUT[cbase + (size_t)k2 * nq2 + q] = o;
+      }
+      continue;
+    }
+    // ---- general columns (the 12 pentagons, or terrain)
     float vm[FUSED_NB];
     bool inflow[FUSED_NB];
 #pragma unroll
     for (int n = 0; n < FUSED_NB; ++n) {
       vm[n] = (n < np) ? __ldg(A.vmasc + (size_t)R[COLREC_EV + n] * mza + kd) : 0.f;
-      // the upwind side of face n is not this column's side
       inflow[n] = (n < np) && (kd >= R[COLREC_LPV + n]) && (((vm[n] < 0.f) ? 1 : 0) != R[COLREC_OWN + n]);
     }
-    const size_t lvl = (size_t)kd * nq2;
-
     for (int q = lane; q < nq2; q += LPI) {
-      const float2* Sc = S + cbase + lvl + q;            // S(iw, kd, q)
-      // ---- round 1: rows with known addresses
+      const size_t lq = (size_t)lvl + q;
+      const float2* Sc = S + cbase + lq;
       const float2 s0 = ld2(Sc);
       const float2 sm1 = (kd - 1 >= kb) ? ld2(Sc - nq2) : s0;
       const float2 sp1 = (kd + 1 < mza) ? ld2(Sc + nq2) : s0;
@@ -144,82 +264,45 @@ __global__ void __launch_bounds__(FUSED_THREADS, FUSED_MINB) k_fused(FusedArgs A
       float2 sn[FUSED_NB];
 #pragma unroll
       for (int n = 0; n < FUSED_NB; ++n)
-        if (n < np) sn[n] = ld2(S + (size_t)R[COLREC_NB + n] * colsz + lvl + q);
-      const float2 s00 = ld2(S0 + cbase + lvl + q);
-      const float2 st = ld2(SCT + cbase + lvl + q);
+        if (n < np) sn[n] = ld2(S + (size_t)R[COLREC_NB + n] * colsz + lq);
+      const float2 s00 = ld2(S0 + cbase + lq);
+      const float2 st = ld2(SCT + cbase + lq);
+      float2 dn[FUSED_NB];
+#pragma unroll
+      for (int m = 0; m < FUSED_NB; ++m)
+        if (m < np) dn[m] = sub2(sn[m], s0);
       float2 fd = make_float2(0.f, 0.f);
-      if (fast) {
-        // ---- round 2: far-side rows of the inflow faces
-        float2 nw[6][3];
 #pragma unroll
-        for (int n = 0; n < 6; ++n)
+      for (int n = 0; n < FUSED_NB; ++n) {
+        if (n >= np || kd < R[COLREC_LPV + n]) continue;
+        float2 val;
+        if (!inflow[n]) {
+          val = s0;
 #pragma unroll
-          for (int m = 0; m < 3; ++m)
-            if (inflow[n] && m < R[COLREC_NNEW + n])
-              nw[n][m] = ld2(S + (size_t)R[COLREC_NEW + n * 3 + m] * colsz + lvl + q);
-        float2 dn[6];
-#pragma unroll
-        for (int m = 0; m < 6; ++m) dn[m] = sub2(sn[m], s0);
-#pragma unroll
-        for (int n = 0; n < 6; ++n) {
-          if (kd < R[COLREC_LPV + n]) continue;
-          float2 val;
-          if (!inflow[n]) {
-            val = s0;
-#pragma unroll
-            for (int m = 0; m < 6; ++m) val = axpy2(val, RF(COLREC_WOWN + n * 7 + m), dn[m]);
-          } else {
-            const float2 su = sn[n];
-            val = su;
-            val = axpy2(val, RF(COLREC_WU + n * 7 + 0), sub2(s0, su));
-            val = axpy2(val, RF(COLREC_WU + n * 7 + 1), sub2(sn[(n + 5) % 6], su));
-            val = axpy2(val, RF(COLREC_WU + n * 7 + 2), sub2(sn[(n + 1) % 6], su));
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-              if (m < R[COLREC_NNEW + n]) val = axpy2(val, RF(COLREC_WU + n * 7 + 3 + m), sub2(nw[n][m], su));
+          for (int m = 0; m < FUSED_NB; ++m)
+            if (m < np) val = axpy2(val, RF(COLREC_WOWN + n * 7 + m), dn[m]);
+        } else {
+          const int u = R[COLREC_NB + n];
+          const int iv = R[COLREC_EV + n];
+          const float* w = A.ew + ((size_t)iv * 2 + (1 - R[COLREC_OWN + n])) * 8;
+          const float2 su = sn[n];
+          val = su;
+          const int npu = __ldg(A.npoly + u);
+          for (int m = 0; m < npu; ++m) {
+            const int um = __ldg(A.w_nb + u * 8 + m);
+            const float2 sx = (um == iw) ? s0 : ld2(S + (size_t)um * colsz + lq);
+            val = axpy2(val, __ldg(w + m), sub2(sx, su));
           }
-          fd = axpy2(fd, RF(COLREC_DV + n) * vm[n], sub2(val, s00));
         }
-      } else {
-        // general polygons (the 12 pentagons of the icosahedral grid)
-        float2 dn[FUSED_NB];
-#pragma unroll
-        for (int m = 0; m < FUSED_NB; ++m)
-          if (m < np) dn[m] = sub2(sn[m], s0);
-#pragma unroll
-        for (int n = 0; n < FUSED_NB; ++n) {
-          if (n >= np || kd < R[COLREC_LPV + n]) continue;
-          float2 val;
-          if (!inflow[n]) {
-            val = s0;
-#pragma unroll
-            for (int m = 0; m < FUSED_NB; ++m)
-              if (m < np) val = axpy2(val, RF(COLREC_WOWN + n * 7 + m), dn[m]);
-          } else {
-            const int u = R[COLREC_NB + n];
-            const int iv = R[COLREC_EV + n];
-            const float* w = A.ew + ((size_t)iv * 2 + (1 - R[COLREC_OWN + n])) * 8;
-            const float2 su = sn[n];
-            val = su;
-            const int npu = __ldg(A.npoly + u);
-            for (int m = 0; m < npu; ++m) {
-              const int um = __ldg(A.w_nb + u * 8 + m);
-              const float2 sx = (um == iw) ? s0 : ld2(S + (size_t)um * colsz + lvl + q);
-              val = axpy2(val, __ldg(w + m), sub2(sx, su));
-            }
-          }
-          fd = axpy2(fd, RF(COLREC_DV + n) * vm[n], sub2(val, s00));
-        }
+        fd = axpy2(fd, RF(COLREC_DV + n) * vm[n], sub2(val, s00));
       }
-      // ---- vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded)
       float2 up_lo, up_hi;
-      if (kd == kb) up_lo = s0;                                                   // scp_upw(kb-1) = scp(kb)
-      else if (wkm1 < 0.f) up_lo = zface(A.a_w, mza, kb, kd, true, sm1, s0, sp1);        // scpb(kd)
-      else up_lo = zface(A.a_w, mza, kb, kd - 1, false, sm2, sm1, s0);                   // scpt(kd-1)
-      if (kd == mza - 1) up_hi = s0;                                              // scp_upw(mza) = scp(mza)
-      else if (wk0 < 0.f) up_hi = zface(A.a_w, mza, kb, kd + 1, true, s0, sp1, sp2);     // scpb(kd+1)
-      else up_hi = zface(A.a_w, mza, kb, kd, false, sm1, s0, sp1);                       // scpt(kd)
-      // ---- vertical flux divergence and update
+      if (kd == kb) up_lo = s0;
+      else if (wkm1 < 0.f) up_lo = zface(A.a_w, mza, kb, kd, true, sm1, s0, sp1);
+      else up_lo = zface(A.a_w, mza, kb, kd - 1, false, sm2, sm1, s0);
+      if (kd == mza - 1) up_hi = s0;
+      else if (wk0 < 0.f) up_hi = zface(A.a_w, mza, kb, kd + 1, true, s0, sp1, sp2);
+      else up_hi = zface(A.a_w, mza, kb, kd, false, sm1, s0, sp1);
       float2 o;
       {
         float v = fexpl * (wkm1 * (up_lo.x - s00.x) - wk0 * (up_hi.x - s00.x));
@@ -227,7 +310,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, FUSED_MINB) k_fused(FusedArgs A
         v = fexpl * (wkm1 * (up_lo.y - s00.y) - wk0 * (up_hi.y - s00.y));
         o.y = s00.y + A.dtr * (st.y + vt * (fd.y + v)) / rh;
       }
-      OUT[cbase + lvl + q] = o;
+      OUT[cbase + lq] = o;
       if (kd == kb)
         for (int k2 = 0; k2 < kb; ++k2) OUT[cbase + (size_t)k2 * nq2 + q] = o;
     }
