@@ -208,9 +208,16 @@ int olamgpu_set_coherence(int mode);
 int olamgpu_sync_to_device(unsigned fieldmask);
 int olamgpu_sync_to_host(unsigned fieldmask);
 
-/* Transport form: fused batched kernels (default) or one set of kernels per
- * tracer mirroring the reference's passes (kept for comparison). */
-enum { OLAMGPU_TRANSPORT_FUSED = 0, OLAMGPU_TRANSPORT_PLAIN = 1 };
+/* Transport form.
+ * OLAMGPU_TRANSPORT_FUSED (default): all tracers of an RK stage in one
+ *   launch over the batched layout, in tiles of neighbouring columns whose
+ *   neighbourhood is staged in shared memory (one column per block where
+ *   the tile tables do not fit).
+ * OLAMGPU_TRANSPORT_PLAIN: one set of kernels per tracer mirroring the
+ *   reference's passes (kept for comparison).
+ * OLAMGPU_TRANSPORT_FUSED_COLUMN: the batched form with one column per
+ *   block (kept for comparison). */
+enum { OLAMGPU_TRANSPORT_FUSED = 0, OLAMGPU_TRANSPORT_PLAIN = 1, OLAMGPU_TRANSPORT_FUSED_COLUMN = 2 };
 int olamgpu_set_transport_form(int form);
 
 /* Replaces scalar_transport_rk(rho_old) (scalar_transport_rk.F90:30-385).

@@ -19,7 +19,7 @@ OK = 0
 E_ARG, E_STATE, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_NODEVICE, E_NUMERIC = range(1, 8)
 
 SYNC_EACH_CALL, RESIDENT = 0, 1
-TRANSPORT_FUSED, TRANSPORT_PLAIN = 0, 1
+TRANSPORT_FUSED, TRANSPORT_PLAIN, TRANSPORT_FUSED_COLUMN = 0, 1, 2
 
 F_RHO, F_PRESS, F_THIL, F_WC, F_WMC, F_VXE, F_VMC, F_VC = (1 << i for i in range(8))
 F_VMASC, F_WMASC, F_TEND, F_FACS, F_SCALARS, F_SCALAR_TEND = (1 << i for i in range(8, 14))

@@ -13,6 +13,32 @@ namespace olamgpu {
 
 unsigned long long g_launches = 0;
 
+int check_device_status() {
+  Context& C = ctx();
+  if (!C.status.p) return OLAMGPU_OK;
+  int h[4];
+  OG_CUDA(cudaMemcpyAsync(h, C.status.p, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+  OG_CUDA(cudaStreamSynchronize(C.stream));
+  if (h[0]) {
+    set_error("a device bounds check failed (code " + std::to_string(h[0]) + ", value " + std::to_string(h[1]) +
+              ", block " + std::to_string(h[2]) + ", thread " + std::to_string(h[3]) + ")");
+    return OLAMGPU_E_NUMERIC;
+  }
+  return OLAMGPU_OK;
+}
+
+#ifdef OLAMGPU_DEBUG_SYNC
+void debug_sync(const char* file, int line) {
+  ++g_launches;
+  static bool reported = false;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess && !reported) {
+    reported = true;
+    std::fprintf(stderr, "olamgpu: launch at %s:%d failed: %s\n", file, line, cudaGetErrorString(e));
+  }
+}
+#endif
+
 // ---- per-kernel event timing ----------------------------------------------
 struct ProfRec { std::string name; cudaEvent_t a, b; };
 static bool g_prof_on = false;
@@ -95,13 +121,15 @@ static void release_all() {
   DevGrid& d = C.g;
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
                        &d.w_nb, &d.w_ev, &d.w_im, &d.v_iw, &d.v_im, &d.m_iv, &d.m_iw, &d.m_im,
-                       &d.lpw, &d.lpv, &d.lpm, &d.iwglobe, &d.w_nonprog, &d.colrec};
+                       &d.lpw, &d.lpv, &d.lpm, &d.iwglobe, &d.w_nonprog, &d.colrec,
+                       &d.tile_hdr, &d.tile_u, &d.tile_r1, &d.tile_tc};
   for (auto* b : ib) b->release();
   DevBuf<float>* fb[] = {&d.w_dirv, &d.gxc, &d.gyc, &d.xy_h, &d.xy_hu, &d.dxps, &d.dyps, &d.xx0_v,
                          &d.xy0_v, &d.yy0_v, &d.xx0_vu, &d.xy0_vu, &d.yy0_vu, &d.a_w, &d.a_wu,
                          &d.volti, &d.ew_b, &d.ew_u};
   for (auto* b : fb) b->release();
   d.ew_order = 0;
+  d.tile_T = d.ntiles = d.tile_nu_max = d.tile_nr1_max = d.tile_order = 0;
   Tracers& tr = C.tr;
   for (size_t i = 0; i < tr.p.size(); ++i) {
     tr.p[i].release();
@@ -175,6 +203,10 @@ int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts, const olamg
   if (order == 2 || order == 3) {
     rc = build_fused_weights(grid, C.g, order, C.stream);
     if (rc != OLAMGPU_OK) { release_all(); return rc; }
+    if (C.tp.flat) {
+      rc = build_tiles(grid, C.g, order, C.stream);
+      if (rc != OLAMGPU_OK) { release_all(); return rc; }
+    }
   }
   if (state) { C.hstate = *state; C.have_state = true; } else C.have_state = false;
   // prog_wrtv_rk needs the dynamics state and the M-point tables; without
@@ -265,9 +297,12 @@ int olamgpu_set_coherence(int mode) {
 }
 
 int olamgpu_set_transport_form(int form) {
-  if (form != OLAMGPU_TRANSPORT_FUSED && form != OLAMGPU_TRANSPORT_PLAIN) { set_error("unknown transport form"); return OLAMGPU_E_ARG; }
+  if (form != OLAMGPU_TRANSPORT_FUSED && form != OLAMGPU_TRANSPORT_PLAIN && form != OLAMGPU_TRANSPORT_FUSED_COLUMN) {
+    set_error("unknown transport form");
+    return OLAMGPU_E_ARG;
+  }
   Context& C = ctx();
-  if (C.initialised && C.form != form) {
+  if (C.initialised && (C.form == OLAMGPU_TRANSPORT_PLAIN) != (form == OLAMGPU_TRANSPORT_PLAIN)) {
     // keep the newest tracer values in the per-tracer mirrors across a switch
     OG_CHECK(ensure_plain(C.stream));
   }
@@ -332,7 +367,7 @@ int olamgpu_sync_to_host(unsigned fieldmask) {
     }
   }
   OG_CUDA(cudaStreamSynchronize(s));
-  return OLAMGPU_OK;
+  return check_device_status();
 }
 
 int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag) {

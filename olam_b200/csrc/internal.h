@@ -66,7 +66,13 @@ const std::string& last_error();
 
 // counts kernel launches issued by the library (olamgpu_launch_count)
 extern unsigned long long g_launches;
+#ifdef OLAMGPU_DEBUG_SYNC
+// diagnostic builds: wait for every launch and name the first one that failed
+void debug_sync(const char* file, int line);
+#define OG_LAUNCHED() ::olamgpu::debug_sync(__FILE__, __LINE__)
+#else
 #define OG_LAUNCHED() (++::olamgpu::g_launches)
+#endif
 
 // per-kernel event timing (olamgpu_profile); no-ops while disabled
 void prof_begin(const char* name, cudaStream_t s);
@@ -136,8 +142,42 @@ struct DevGrid {
   DevBuf<float> ew_b, ew_u;      // (mva, 2, 8)
   int ew_order = 0;
   DevBuf<int> colrec;            // (nw_prog, COLREC_WORDS) fused-kernel column records
+  // Tile tables of the tiled fused kernel (flat grids).  Tile t owns TILE_T
+  // consecutive prognostic columns; its neighbourhood U lists those columns,
+  // then the rest of their neighbours (U[0, nr1) = ring 1), then the rest of
+  // the ring-1 cells' neighbours.  hdr[t] = {u_off, nU, nR1, nT}.
+  DevBuf<int> tile_hdr;          // (ntiles, 4)
+  DevBuf<int> tile_u;            // (sum nU) column of each U entry
+  DevBuf<int> tile_r1;           // (sum nU, TILE_R1W) ring-1 records, indexed u_off + r
+  DevBuf<int> tile_tc;           // (ntiles * tile_T, TILE_TCW) tile-cell records
+  int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_nr1_max = 0, tile_order = 0;
   std::vector<int> h_lpw;        // host copies used at set-up
 };
+
+// Records are laid out in 16-byte groups so the kernel reads them with
+// vector loads.  Pentagons are padded to six faces: the sixth neighbour is
+// the cell itself with zero weights, offsets, dirv and vmasc, which leaves
+// every sum unchanged.
+// Ring-1 record (words): U-local index of the 6 neighbours, np, pad, then
+// the gradient coefficients by plane, c[m][n] at 8 + 6 m + n: order 2
+// gxps_coef, gyps_coef; order 3 xy_h(1..5, n).
+#define TILE_R1_NB 0
+#define TILE_R1_NP 6
+#define TILE_R1_C 8
+#define TILE_R1W(order) ((order) == 2 ? 20 : 40)
+// Tile-cell record (words): column, side bits (bit n: the cell is side 2,
+// itab_v%iw(2), of face n), np, pad; ring-1 index of the neighbour across
+// each face; V index of each face; dirv of each face; pad; the face offsets
+// of the cell's own side (NOFF per face: dxps, dyps [, xx0_v, xy0_v,
+// yy0_v]); then those of the neighbour's side.
+#define TILE_TC_IW 0
+#define TILE_TC_SIDE 1
+#define TILE_TC_NP 2
+#define TILE_TC_NB 4
+#define TILE_TC_EV 10
+#define TILE_TC_DV 16
+#define TILE_TC_OFF 24
+#define TILE_TCW(order) ((order) == 2 ? 48 : 84)
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)
@@ -222,6 +262,14 @@ Context& ctx();
 // set-up helpers (setup.cu)
 int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s);
 int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
+// host tile tables (layouts above); T == 0 when the grid is left to the column kernel
+struct TileHost {
+  int T = 0, ntiles = 0, nu_max = 0, nr1_max = 0, order = 0;
+  std::vector<int> hdr, ulist, r1, tc;
+};
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th);
+int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
+size_t tile_smem_bytes(int order, int T, int nu_max, int nr1_max);
 
 // dynamics entry points (dynamics.cu)
 int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s);
@@ -231,6 +279,10 @@ int dyn_timeavg_momsc();
 int dyn_state_to_device(unsigned mask, cudaStream_t s);
 int dyn_state_to_host(unsigned mask, cudaStream_t s);
 void dyn_release();
+
+// reads the device status record (call with the library stream idle); a
+// kernel that found an inconsistent table reports it here
+int check_device_status();
 
 // transport entry points (transport.cu)
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);

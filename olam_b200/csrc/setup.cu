@@ -1,8 +1,10 @@
 // setup.cu -- grid upload and table packing (host side of init_wrtv_rk's
 // replacement).  OLAM's tables (mem_ijtabs.f90:60-144) arrive 1-based with
 // packed derived-type members; the device keeps 0-based, padded copies.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "internal.h"
 
@@ -277,6 +279,153 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
   }
   OG_CHECK(upload(d.colrec, rec.data(), rec.size(), s));
   OG_CUDA(cudaStreamSynchronize(s));
+  return OLAMGPU_OK;
+}
+
+
+// ---- tiles of the tiled fused kernel ------------------------------------------
+
+size_t tile_smem_bytes(int order, int T, int nu, int nr1) {
+  const int npl = order == 2 ? 2 : 5;
+  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+  return al((size_t)nu * 256) + al((size_t)nr1 * npl * 256) + al((size_t)nr1 * TILE_R1W(order) * 4) +
+         al((size_t)T * TILE_TCW(order) * 4) + al((size_t)T * 12 * 4) + al((size_t)nu * 4) + 64;
+}
+
+// Two blocks per SM: 228 KB of shared memory less 1 KB reserved per block.
+#define TILE_SMEM_MAX (113 * 1024)
+
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
+  th = TileHost();
+  if (order != 2 && order != 3) return;
+  const int nprog = g->nw_prog, mwa = g->mwa;
+  if (nprog <= 0) return;
+  for (int j = 0; j < nprog; ++j) {
+    const int c = g->jtw_prog[j] - 1;
+    if (g->npoly[c] < 3 || g->npoly[c] > 6) return;  // left to the column kernel
+  }
+  auto nbr = [&](int c, int n) { return g->itab_w_iw[(size_t)c * 7 + n] - 1; };
+  std::vector<int> stamp(mwa, -1), loc(mwa, 0);
+  std::vector<int> U;
+  // neighbourhood of tile t in U (local index of column x: loc[x] while stamp[x] == t)
+  auto gather = [&](int t, int T, int& nr1) {
+    U.clear();
+    const int j0 = t * T, j1 = std::min(nprog, j0 + T);
+    auto add = [&](int x) {
+      if (stamp[x] != t) { stamp[x] = t; loc[x] = (int)U.size(); U.push_back(x); }
+    };
+    for (int j = j0; j < j1; ++j) add(g->jtw_prog[j] - 1);
+    const int nt = (int)U.size();
+    for (int i = 0; i < nt; ++i)
+      for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
+    nr1 = (int)U.size();
+    for (int i = nt; i < nr1; ++i)
+      for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
+  };
+  int T = 0, numax = 0, nr1max = 0;
+  const int cand[] = {64, 48, 32, 24, 16, 8};
+  for (int Tc : cand) {
+    std::fill(stamp.begin(), stamp.end(), -1);
+    const int nt = (nprog + Tc - 1) / Tc;
+    int nu = 0, nr = 0;
+    for (int t = 0; t < nt; ++t) {
+      int nr1;
+      gather(t, Tc, nr1);
+      nu = std::max(nu, (int)U.size());
+      nr = std::max(nr, nr1);
+    }
+    if (nu <= 65535 && tile_smem_bytes(order, Tc, nu, nr) <= TILE_SMEM_MAX) {
+      T = Tc; numax = nu; nr1max = nr;
+      break;
+    }
+  }
+  if (!T) return;  // neighbourhoods too large: the column kernel runs
+  const int ntiles = (nprog + T - 1) / T;
+  const int R1W = TILE_R1W(order), TCW = TILE_TCW(order), noff = order == 2 ? 2 : 5;
+  std::vector<int>& hdr = th.hdr;
+  std::vector<int>& ulist = th.ulist;
+  std::vector<int>& r1 = th.r1;
+  std::vector<int>& tc = th.tc;
+  hdr.assign((size_t)ntiles * 4, 0);
+  tc.assign((size_t)ntiles * T * TCW, 0);
+  auto fbits = [](float f) { int i; std::memcpy(&i, &f, 4); return i; };
+  std::fill(stamp.begin(), stamp.end(), -1);
+  for (int t = 0; t < ntiles; ++t) {
+    int nr1;
+    gather(t, T, nr1);
+    const int u_off = (int)ulist.size();
+    const int nT = std::min(T, nprog - t * T);
+    hdr[(size_t)t * 4 + 0] = u_off;
+    hdr[(size_t)t * 4 + 1] = (int)U.size();
+    hdr[(size_t)t * 4 + 2] = nr1;
+    hdr[(size_t)t * 4 + 3] = nT;
+    ulist.insert(ulist.end(), U.begin(), U.end());
+    r1.resize(ulist.size() * R1W, 0);
+    for (int r = 0; r < nr1; ++r) {
+      const int c = U[r];
+      int* w = &r1[((size_t)u_off + r) * R1W];
+      const int np = g->npoly[c];
+      w[TILE_R1_NP] = np;
+      for (int n = 0; n < 6; ++n) w[TILE_R1_NB + n] = n < np ? loc[nbr(c, n)] : r;
+      for (int n = 0; n < np; ++n) {
+        if (order == 2) {
+          w[TILE_R1_C + n] = fbits(g->gxps_coef[(size_t)c * 7 + n]);
+          w[TILE_R1_C + 6 + n] = fbits(g->gyps_coef[(size_t)c * 7 + n]);
+        } else {
+          for (int m = 0; m < 5; ++m) w[TILE_R1_C + m * 6 + n] = fbits(g->xy_h[((size_t)c * 7 + n) * 5 + m]);
+        }
+      }
+    }
+    for (int i = 0; i < nT; ++i) {
+      const int c = U[i];
+      int* w = &tc[((size_t)t * T + i) * TCW];
+      const int np = g->npoly[c];
+      w[TILE_TC_IW] = c;
+      w[TILE_TC_NP] = np;
+      int side = 0;
+      for (int n = 0; n < 6; ++n) {
+        const bool v = n < np;
+        const int iv = v ? g->itab_w_iv[(size_t)c * 7 + n] - 1 : 0;
+        const int sd = v ? ((g->itab_v_iw[(size_t)iv * 2] - 1 == c) ? 0 : 1) : 0;
+        side |= sd << n;
+        w[TILE_TC_NB + n] = v ? loc[nbr(c, n)] : i;
+        w[TILE_TC_EV + n] = iv;
+        w[TILE_TC_DV + n] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + n] : 0.f);
+        if (!v) continue;
+        for (int k = 0; k < 2; ++k) {
+          const size_t e = (size_t)iv * 2 + (k == 0 ? sd : 1 - sd);
+          float* o = reinterpret_cast<float*>(w + TILE_TC_OFF + (k * 6 + n) * noff);
+          o[0] = g->dxps[e];
+          o[1] = g->dyps[e];
+          if (order == 3) { o[2] = g->xx0_v[e]; o[3] = g->xy0_v[e]; o[4] = g->yy0_v[e]; }
+        }
+      }
+      w[TILE_TC_SIDE] = side;
+    }
+  }
+  th.T = T;
+  th.ntiles = ntiles;
+  th.nu_max = numax;
+  th.nr1_max = nr1max;
+  th.order = order;
+}
+
+int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
+  d.tile_T = d.ntiles = d.tile_nu_max = d.tile_nr1_max = 0;
+  d.tile_order = 0;
+  TileHost th;
+  make_tiles(g, order, th);
+  if (!th.T) return OLAMGPU_OK;
+  OG_CHECK(upload(d.tile_hdr, th.hdr.data(), th.hdr.size(), s));
+  OG_CHECK(upload(d.tile_u, th.ulist.data(), th.ulist.size(), s));
+  OG_CHECK(upload(d.tile_r1, th.r1.data(), th.r1.size(), s));
+  OG_CHECK(upload(d.tile_tc, th.tc.data(), th.tc.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));
+  d.tile_T = th.T;
+  d.ntiles = th.ntiles;
+  d.tile_nu_max = th.nu_max;
+  d.tile_nr1_max = th.nr1_max;
+  d.tile_order = order;
   return OLAMGPU_OK;
 }
 

@@ -144,16 +144,17 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   if (nrk != 2 && nrk != 3) { set_error("scalar_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
   if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
   if (C.opts.iscal_monot < 0 || C.opts.iscal_monot > 2) { set_error("iscal_monot must be 0, 1 or 2"); return OLAMGPU_E_UNSUPPORTED; }
-  if (C.form == OLAMGPU_TRANSPORT_FUSED && !tp.flat) {
+  const bool batched = C.form != OLAMGPU_TRANSPORT_PLAIN;
+  const bool tiled = C.form == OLAMGPU_TRANSPORT_FUSED && tile_stage_available(d, tp, order);
+  if (batched && !tp.flat) {
     set_error("the fused transport form needs lpw = lpv = 2 (no terrain); use the plain form");
     return OLAMGPU_E_UNSUPPORTED;
   }
-  if (C.form == OLAMGPU_TRANSPORT_FUSED &&
-      (double)mwa * mza * (double)((tr.ntp + 3) / 4 * 2) >= 4294967296.0) {
+  if (batched && !tiled && (double)mwa * mza * (double)((tr.ntp + 3) / 4 * 2) >= 4294967296.0) {
     set_error("the fused transport form needs mwa * mza * ntp / 2 < 2^32; use the plain form");
     return OLAMGPU_E_UNSUPPORTED;
   }
-  if (C.form == OLAMGPU_TRANSPORT_FUSED && d.ew_order != order)
+  if (batched && !tiled && d.ew_order != order)
     OG_CHECK(build_fused_weights(&C.hgrid, C.g, order, s));
 
   // ---- inputs
@@ -215,7 +216,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   OG_CUDA(cudaMemcpyAsync(tp.d_mode.p + tr.n, pdm.data(), tr.n * sizeof(int), cudaMemcpyHostToDevice, s));
   const bool any_pdm = std::any_of(pdm.begin(), pdm.end(), [](int v) { return v != 0; });
 
-  if (C.form == OLAMGPU_TRANSPORT_FUSED) {
+  if (batched) {
     OG_CHECK(ensure_q(s));
     const int ntp = tr.ntp;
     const int a = tr.qcur;
@@ -246,7 +247,8 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
         }
       } else {
         OG_PROF(istage == 1 ? "fused_stage1" : "fused_stage", s);
-        launch_fused_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, s);
+        if (tiled) OG_CHECK(launch_tile_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, C.status.p, s));
+        else launch_fused_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, s);
       }
       { OG_PROF("implicit_solve", s); launch_implicit_solve(d, tp, nrk, istage, dtr, CTView{A, ntp, 0}, TView{OUT, ntp, 0}, ntp, s); }
       in_b = out_b;
@@ -319,7 +321,10 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   }
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(tracers_to_host(s));
   OG_CUDA(cudaGetLastError());
-  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CUDA(cudaStreamSynchronize(s));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
+    OG_CUDA(cudaStreamSynchronize(s));
+    OG_CHECK(check_device_status());
+  }
   return OLAMGPU_OK;
 }
 

@@ -15,7 +15,8 @@ import numpy as np
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libolamgpu.so")
+# OLAMGPU_LIBRARY selects another build of the library (e.g. a diagnostic one)
+LIB_PATH = os.environ.get("OLAMGPU_LIBRARY") or os.path.join(HERE, "libolamgpu.so")
 _LIB = None
 
 # every entry point declared in include/olamgpu.h

@@ -44,7 +44,10 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("form", [abi.TRANSPORT_FUSED, abi.TRANSPORT_PLAIN])
+FORMS = [abi.TRANSPORT_FUSED, abi.TRANSPORT_PLAIN, abi.TRANSPORT_FUSED_COLUMN]
+
+
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("kw", CASES)
 def test_transport_parity_small(form, kw):
     g, st = small_case(nxp=6, nlev=12, ntr=6)
@@ -62,7 +65,7 @@ def test_transport_parity_small(form, kw):
     assert (diag.cfl_k, diag.cfl_iwglobe) == (d32.cfl_k, d32.cfl_iwglobe)
 
 
-@pytest.mark.parametrize("form", [abi.TRANSPORT_FUSED, abi.TRANSPORT_PLAIN])
+@pytest.mark.parametrize("form", FORMS)
 def test_transport_parity_implicit(form):
     # vertical CFL > 1: implicit columns in every stage
     g, st = small_case(nxp=5, nlev=12, ntr=4, dtlm=3600.0, seed=7, w_amp=3.0)
@@ -104,11 +107,15 @@ def test_resident_multistep_matches_oracle():
         assert relerr(out[n], tr[n]) < 3 * TOL64
 
 
-def test_fused_equals_plain_many_tracers():
-    # 40 tracers: exercises the tracer padding and more than one float4 lane group
-    g, st = small_case(nxp=8, nlev=16, ntr=40, seed=21)
-    opts = abi.make_opts(1800.0)
+@pytest.mark.parametrize("ntr,order", [(40, 2), (130, 2), (130, 3), (64, 3)])
+def test_fused_forms_agree_many_tracers(ntr, order):
+    # 40 tracers: one ragged 64-tracer group; 130: two full groups and a
+    # ragged one; the tiled, per-column and plain forms agree
+    g, st = small_case(nxp=8, nlev=16, ntr=ntr, seed=21)
+    opts = abi.make_opts(1800.0, scal_order=order)
     a, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED)
     b, _ = run_gpu(g, st, opts, abi.TRANSPORT_PLAIN)
+    c, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED_COLUMN)
     for n in range(st.ntr):
-        assert relerr(a[n], b[n]) < 1e-6
+        assert relerr(a[n], b[n]) < 1e-6, (n, relerr(a[n], b[n]))
+        assert relerr(c[n], b[n]) < 1e-6, (n, relerr(c[n], b[n]))
