@@ -158,26 +158,29 @@ struct DevGrid {
 // vector loads.  Pentagons are padded to six faces: the sixth neighbour is
 // the cell itself with zero weights, offsets, dirv and vmasc, which leaves
 // every sum unchanged.
-// Ring-1 record (words): U-local index of the 6 neighbours, np, pad, then
-// the gradient coefficients by plane, c[m][n] at 8 + 6 m + n: order 2
-// gxps_coef, gyps_coef; order 3 xy_h(1..5, n).
+// Ring-1 record (words): byte offset in the U rows (U-local index * 256) of
+// the 6 neighbours, np, pad, then the gradient coefficients by plane,
+// c[m][n] at 8 + 6 m + n: order 2 gxps_coef, gyps_coef; order 3
+// xy_h(1..5, n).
 #define TILE_R1_NB 0
 #define TILE_R1_NP 6
 #define TILE_R1_C 8
 #define TILE_R1W(order) ((order) == 2 ? 20 : 40)
 // Tile-cell record (words): column, side bits (bit n: the cell is side 2,
-// itab_v%iw(2), of face n), np, pad; ring-1 index of the neighbour across
-// each face; V index of each face; dirv of each face; pad; the face offsets
-// of the cell's own side (NOFF per face: dxps, dyps [, xx0_v, xy0_v,
-// yy0_v]); then those of the neighbour's side.
+// itab_v%iw(2), of face n), np, pad; for the neighbour across each face its
+// byte offset in the U rows (index * 256) and in the gradient planes (index
+// * NOFF * 256); V index of each face; dirv of each face; pad; the face
+// offsets of the cell's own side (NOFF per face: dxps, dyps [, xx0_v,
+// xy0_v, yy0_v]); then those of the neighbour's side.
 #define TILE_TC_IW 0
 #define TILE_TC_SIDE 1
 #define TILE_TC_NP 2
-#define TILE_TC_NB 4
-#define TILE_TC_EV 10
-#define TILE_TC_DV 16
-#define TILE_TC_OFF 24
-#define TILE_TCW(order) ((order) == 2 ? 48 : 84)
+#define TILE_TC_NBU 4
+#define TILE_TC_NBG 10
+#define TILE_TC_EV 16
+#define TILE_TC_DV 22
+#define TILE_TC_OFF 32
+#define TILE_TCW(order) ((order) == 2 ? 56 : 92)
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)

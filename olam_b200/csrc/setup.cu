@@ -288,8 +288,10 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 size_t tile_smem_bytes(int order, int T, int nu, int nr1) {
   const int npl = order == 2 ? 2 : 5;
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  return al((size_t)nu * 256) + al((size_t)nr1 * npl * 256) + al((size_t)nr1 * TILE_R1W(order) * 4) +
-         al((size_t)T * TILE_TCW(order) * 4) + al((size_t)T * 12 * 4) + al((size_t)nu * 4) + 64;
+  // U rows, gradient planes, scp0/sct rows, records, LV, U columns, a_w
+  return al((size_t)nu * 256) + al((size_t)nr1 * npl * 256) + al((size_t)T * 2 * 256) +
+         al((size_t)nr1 * TILE_R1W(order) * 4) + al((size_t)T * TILE_TCW(order) * 4) + al((size_t)T * 12 * 4) +
+         al((size_t)nu * 4) + 64;
 }
 
 // Two blocks per SM: 228 KB of shared memory less 1 KB reserved per block.
@@ -366,7 +368,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       int* w = &r1[((size_t)u_off + r) * R1W];
       const int np = g->npoly[c];
       w[TILE_R1_NP] = np;
-      for (int n = 0; n < 6; ++n) w[TILE_R1_NB + n] = n < np ? loc[nbr(c, n)] : r;
+      for (int n = 0; n < 6; ++n) w[TILE_R1_NB + n] = (n < np ? loc[nbr(c, n)] : r) * 256;
       for (int n = 0; n < np; ++n) {
         if (order == 2) {
           w[TILE_R1_C + n] = fbits(g->gxps_coef[(size_t)c * 7 + n]);
@@ -388,7 +390,9 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
         const int iv = v ? g->itab_w_iv[(size_t)c * 7 + n] - 1 : 0;
         const int sd = v ? ((g->itab_v_iw[(size_t)iv * 2] - 1 == c) ? 0 : 1) : 0;
         side |= sd << n;
-        w[TILE_TC_NB + n] = v ? loc[nbr(c, n)] : i;
+        const int u = v ? loc[nbr(c, n)] : i;
+        w[TILE_TC_NBU + n] = u * 256;
+        w[TILE_TC_NBG + n] = u * noff * 256;
         w[TILE_TC_EV + n] = iv;
         w[TILE_TC_DV + n] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + n] : 0.f);
         if (!v) continue;

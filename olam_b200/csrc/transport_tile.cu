@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   unsigned char* p = smraw;
   float2* U = reinterpret_cast<float2*>(p);  p += al((size_t)A.nu_max * 256);
   float2* G = reinterpret_cast<float2*>(p);  p += al((size_t)A.nr1_max * NPL * 256);
+  float2* Q0 = reinterpret_cast<float2*>(p); p += al((size_t)A.T * 2 * 256);   // scp0, sct rows of the tile
   int* R1 = reinterpret_cast<int*>(p);       p += al((size_t)A.nr1_max * R1W * 4);
   int* TC = reinterpret_cast<int*>(p);       p += al((size_t)A.T * TCW * 4);
   float* LV = reinterpret_cast<float*>(p);   p += al((size_t)A.T * TILE_LV * 4);
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   if (!bad) {
     for (int i = tid; i < nR1 * R1W; i += TILE_THREADS) {
       const int v = __ldg(A.r1 + (size_t)u_off * R1W + i), f = i % R1W;
-      if (f < 6 && (unsigned)v >= (unsigned)nU) bad = 2;
+      if (f < 6 && ((unsigned)v >= (unsigned)nU * 256u || (v & 255))) bad = 2;
       if (f == TILE_R1_NP && (v < 3 || v > 6)) bad = 3;
       R1[i] = v;
     }
@@ -113,7 +114,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       const int v = __ldg(A.tc + (size_t)tile * A.T * TCW + i), f = i % TCW;
       if (f == TILE_TC_IW && (v < 1 || v >= A.mwa)) bad = 4;
       if (f == TILE_TC_NP && (v < 3 || v > 6)) bad = 5;
-      if (f >= TILE_TC_NB && f < TILE_TC_NB + 6 && (unsigned)v >= (unsigned)nR1) bad = 6;
+      if (f >= TILE_TC_NBU && f < TILE_TC_NBU + 6 && ((unsigned)v >= (unsigned)nR1 * 256u || (v & 255))) bad = 6;
+      if (f >= TILE_TC_NBG && f < TILE_TC_NBG + 6 && ((unsigned)v >= (unsigned)nR1 * NPL * 256u || (v & 255)))
+        bad = 9;
       if (f >= TILE_TC_EV && f < TILE_TC_EV + 6 && (unsigned)v >= (unsigned)A.mva) bad = 7;
       TC[i] = v;
     }
@@ -140,6 +143,12 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       if (ch < nch)
         cp_async16(reinterpret_cast<char*>(U) + row * 256 + ch * 16,
                    A.S + ((size_t)UIW[row] * mza + kd) * ntp + t0 + ch * 4);
+    }
+    for (int i = tid; i < nT * 32; i += TILE_THREADS) {
+      const int row = i >> 4, ch = i & 15;   // row = 2 * cell + (0: scp0, 1: sct)
+      if (ch < nch)
+        cp_async16(reinterpret_cast<char*>(Q0) + row * 256 + ch * 16,
+                   ((row & 1) ? A.SCT : A.S0) + ((size_t)UIW[row >> 1] * mza + kd) * ntp + t0 + ch * 4);
     }
     cp_async_commit();
     for (int i = tid; i < nT * TILE_LV; i += TILE_THREADS) {
@@ -171,7 +180,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
     for (int r = warp; r < nR1; r += TILE_NW) {
       const int4* w4 = reinterpret_cast<const int4*>(R1 + r * R1W);
       const int4 na = w4[0], nb = w4[1];
-      const int nbi[6] = {na.x, na.y, na.z, na.w, nb.x, nb.y};
+      const int nbo[6] = {na.x, na.y, na.z, na.w, nb.x, nb.y};   // byte offsets of the U rows
       float cf[6 * NPL];
       const float4* c4 = reinterpret_cast<const float4*>(R1 + r * R1W + TILE_R1_C);
 #pragma unroll
@@ -183,13 +192,14 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
         const float2 v = reinterpret_cast<const float2*>(c4 + (6 * NPL) / 4)[0];
         cf[6 * NPL - 2] = v.x; cf[6 * NPL - 1] = v.y;
       }
+      const char* Ul = reinterpret_cast<const char*>(U + lane);
       const float2 nsc = neg2(U[r * 32 + lane]);
       float2 g[NPL];
 #pragma unroll
       for (int m = 0; m < NPL; ++m) g[m] = make_float2(0.f, 0.f);
 #pragma unroll
       for (int n = 0; n < 6; ++n) {
-        const float2 d = add2(U[nbi[n] * 32 + lane], nsc);
+        const float2 d = add2(*reinterpret_cast<const float2*>(Ul + nbo[n]), nsc);
 #pragma unroll
         for (int m = 0; m < NPL; ++m) g[m] = fma2s(cf[m * 6 + n], d, g[m]);
       }
@@ -203,12 +213,14 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       const int* w = TC + c * TCW;
       const int4 h4 = reinterpret_cast<const int4*>(w)[0];
       const int iw = h4.x, side = h4.y;
-      const int4 nba = reinterpret_cast<const int4*>(w)[1];   // nb0..3
-      const int4 nbb = reinterpret_cast<const int4*>(w)[2];   // nb4, nb5, ev0, ev1
-      const float4 dva = reinterpret_cast<const float4*>(w)[4];  // dv0..3
-      const float4 dvb = reinterpret_cast<const float4*>(w)[5];  // dv4, dv5, pad
-      const int nbi[6] = {nba.x, nba.y, nba.z, nba.w, nbb.x, nbb.y};
-      const float dvv[6] = {dva.x, dva.y, dva.z, dva.w, dvb.x, dvb.y};
+      const int4 q1 = reinterpret_cast<const int4*>(w)[1];      // U offsets 0..3
+      const int4 q2 = reinterpret_cast<const int4*>(w)[2];      // U offsets 4, 5, G offsets 0, 1
+      const int4 q3 = reinterpret_cast<const int4*>(w)[3];      // G offsets 2..5
+      const float4 dva = reinterpret_cast<const float4*>(w)[5];  // ev 4, 5, dv 0, 1
+      const float4 dvb = reinterpret_cast<const float4*>(w)[6];  // dv 2..5
+      const int nbu[6] = {q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
+      const int nbg[6] = {q2.z, q2.w, q3.x, q3.y, q3.z, q3.w};
+      const float dvv[6] = {dva.z, dva.w, dvb.x, dvb.y, dvb.z, dvb.w};
       const float4 l0 = reinterpret_cast<const float4*>(LV + c * TILE_LV)[0];
       const float4 l1 = reinterpret_cast<const float4*>(LV + c * TILE_LV)[1];
       const float4 l2 = reinterpret_cast<const float4*>(LV + c * TILE_LV)[2];
@@ -217,12 +229,11 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       const size_t row = ((size_t)iw * mza + kd) * ntp + t0 + 2 * lane;
       const size_t lvl = (size_t)ntp;
       const float2 s0 = U[c * 32 + lane];
-      float2 s00 = make_float2(0.f, 0.f), st = s00, sm1 = s0, sp1 = s0;
+      const float2 s00 = Q0[(2 * c) * 32 + lane], st = Q0[(2 * c + 1) * 32 + lane];
+      float2 sm1 = s0, sp1 = s0;
       const bool need_m2 = kd != kb && !(wkm1 < 0.f);
       const bool need_p2 = kd != mza - 1 && wk0 < 0.f;
       if (act) {
-        s00 = __ldg(reinterpret_cast<const float2*>(A.S0 + row));
-        st = __ldg(reinterpret_cast<const float2*>(A.SCT + row));
         if (kd - 1 >= kb) sm1 = __ldg(reinterpret_cast<const float2*>(A.S + row - lvl));
         if (kd + 1 < mza) sp1 = __ldg(reinterpret_cast<const float2*>(A.S + row + lvl));
       }
@@ -231,20 +242,23 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       if (act && need_p2 && kd + 2 < mza) sp2 = __ldg(reinterpret_cast<const float2*>(A.S + row + 2 * lvl));
       const float2 ns00 = neg2(s00);
       float2 fd = make_float2(0.f, 0.f);
+      const char* Ul = reinterpret_cast<const char*>(U + lane);
+      const char* Gl = reinterpret_cast<const char*>(G + lane);
+      const int cu = c * 256, cg = c * NPL * 256;
 #pragma unroll
       for (int n = 0; n < 6; ++n) {
         // upwind side of face n: the neighbour (inflow) or the cell itself
         const bool inflow = (vmv[n] < 0.f ? 1 : 0) != ((side >> n) & 1);
-        const int src = inflow ? nbi[n] : c;
+        const int su = inflow ? nbu[n] : cu, sg = inflow ? nbg[n] : cg;
         const float* off = reinterpret_cast<const float*>(w + TILE_TC_OFF + ((inflow ? 6 : 0) + n) * NPL);
-        float2 val = U[src * 32 + lane];
+        float2 val = *reinterpret_cast<const float2*>(Ul + su);
         if (NPL == 2) {
           const float2 o2 = *reinterpret_cast<const float2*>(off);
-          val = fma2s(o2.x, G[(src * NPL) * 32 + lane], val);
-          val = fma2s(o2.y, G[(src * NPL + 1) * 32 + lane], val);
+          val = fma2s(o2.x, *reinterpret_cast<const float2*>(Gl + sg), val);
+          val = fma2s(o2.y, *reinterpret_cast<const float2*>(Gl + sg + 256), val);
         } else {
 #pragma unroll
-          for (int m = 0; m < NPL; ++m) val = fma2s(off[m], G[(src * NPL + m) * 32 + lane], val);
+          for (int m = 0; m < NPL; ++m) val = fma2s(off[m], *reinterpret_cast<const float2*>(Gl + sg + m * 256), val);
         }
         fd = fma2s(dvv[n] * vmv[n], add2(val, ns00), fd);
       }
