@@ -55,6 +55,7 @@ def parse():
     p.add_argument("--monot", type=int, default=0)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-column", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     return p.parse_args()
@@ -286,20 +287,27 @@ def main():
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = float(peak or 6650.0)
-    tot_bytes, tot_ms = 0.0, 0.0
-    for name, stage in (("fused_stage1", 1), ("fused_stage", 2)):
+    # the stage kernel: k_tile (tiled form) or k_fused (one column per block)
+    tiled = "tile_stage1" in prof
+    pre = "tile_stage" if tiled else "fused_stage"
+    kname = "k_tile" if tiled else "k_fused"
+    tot_bytes, tot_ms, nl = 0.0, 0.0, 0
+    for name, stage in ((pre + "1", 1), (pre, 2)):
         if name in prof:
             m, c = prof[name]
             tot_ms += m
+            nl += c
             tot_bytes += c * bytes_per_launch(g, a.ntr, stage)
-    nl = sum(c for nm, (m, c) in prof.items() if nm.startswith("fused"))
     achieved = (tot_bytes / nl) / ((tot_ms / nl) * 1e-3) / 1e9 if nl else None
+    # DRAM traffic per launch: the ratio of measured (ncu, smaller grid of the
+    # same kernel) to algorithmic bytes, applied to this launch's algorithmic bytes
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "fused_stage_traffic.json")
-    if os.path.exists(tfile):
+    tfile = os.path.join(ROOT, "profiles", f"{kname}_traffic.json")
+    if nl and os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile)).get("dram_bytes_per_launch_full_size")
-        except (OSError, ValueError):
+            ratio = float(json.load(open(tfile))["dram_over_algorithmic"])
+            traffic = ratio * tot_bytes / nl
+        except (OSError, ValueError, KeyError):
             traffic = None
 
     # ---- plain one-kernel-per-tracer form on the same device data
@@ -318,6 +326,23 @@ def main():
         torch.cuda.synchronize()
         pms = max_over_ranks(p0.elapsed_time(p1) / ksteps)
         plain = ws * nupd / (pms * 1e-3)
+        dev.set_transport_form(abi.TRANSPORT_FUSED)
+
+    # ---- the batched form with one column per block, for comparison
+    column = None
+    if not a.no_column:
+        dev.set_transport_form(abi.TRANSPORT_FUSED_COLUMN)
+        dev.scalar_transport_rk(None)
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        ksteps = max(1, min(a.steps, 3))
+        c0.record(stream)
+        for _ in range(ksteps):
+            dev.scalar_transport_rk(None)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        column = ws * nupd / (max_over_ranks(c0.elapsed_time(c1) / ksteps) * 1e-3)
         dev.set_transport_form(abi.TRANSPORT_FUSED)
 
     # ---- end to end through the C-ABI with host arrays
@@ -351,16 +376,18 @@ def main():
             "config": {"workload": f"scalar_transport_rk NXP={a.nxp} ({g.mwa - 1} columns), "
                                    f"{a.nlev} levels, {a.ntr} tracers, RK{a.nrk}, "
                                    f"horiz order {a.order}, iscal_monot {a.monot}, dt {a.dt} s",
-                       "form": "fused batched", "parallelism": f"replicas x{ws}",
+                       "form": "fused batched, tiled" if tiled else "fused batched",
+                       "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (12.5 GB of tracers per array)"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "peak_source": peak_src, "kernel": "k_fused (fused_stage)",
+                         "peak_source": peak_src, "kernel": f"{kname} ({pre})",
                          "kernel_ms_per_launch": (tot_ms / nl) if nl else None},
             "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
             "plain_gpu_value": plain,
             "fused_over_plain": (value / plain) if plain else None,
+            "fused_column_value": column,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": clk,

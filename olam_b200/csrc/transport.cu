@@ -246,7 +246,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
                        TView{OUT, ntp, g0}, nt, istage, nrk, dtr, rhos_nrk, tp.d_mode.p + g0, true, s);
         }
       } else {
-        OG_PROF(istage == 1 ? "fused_stage1" : "fused_stage", s);
+        OG_PROF(tiled ? (istage == 1 ? "tile_stage1" : "tile_stage") : (istage == 1 ? "fused_stage1" : "fused_stage"), s);
         if (tiled) OG_CHECK(launch_tile_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, C.status.p, s));
         else launch_fused_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, s);
       }
