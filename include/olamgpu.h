@@ -233,6 +233,26 @@ int olamgpu_prog_wrtv_rk(int istp);
 int olamgpu_tend0(float* rho_old);
 int olamgpu_timeavg_momsc(void);
 
+/* One explicit RK stage of update_scalar (scalar_transport_rk.F90:389-615:
+ * grad_t2d[_quadratic], scalar_v_column, scalar_w_column; every column
+ * explicit, no limiter) for ONE tracer, on device arrays the caller owns, in
+ * OLAM's (mza, mwa) / (mza, mva) layout: out = the stage's update of scp
+ * from scp0, sct, rhos (the stage density, real(4)), vmasc, wmasc with
+ * timestep dtr, using the grid and scal_horiz_adv_order given to
+ * olamgpu_init.  Columns outside jtw_prog are not written.  No counterpart
+ * in the reference: it serves callers that must not allocate device memory
+ * during the call (a caller whose memory is fixed up front, or that records
+ * its work into a CUDA graph).  The call allocates nothing: its scratch is
+ * a fixed 64 MiB device array (gradient planes, V-face values, a zeroed
+ * implicit fraction), so grids needing more (about NXP > 66 at 61 levels,
+ * order 2) get OLAMGPU_E_ARG.  The first call on a device looks the scratch
+ * up (make it before any stream capture); calls that overlap in time share
+ * the scratch and race, so serialise them.  stream: a cudaStream_t, or NULL
+ * for the library's stream. */
+int olamgpu_update_scalar_noalloc(const float* scp, const float* scp0, const float* sct,
+                                  const float* rhos, const float* vmasc, const float* wmasc,
+                                  float dtr, float* out, void* stream);
+
 /* Device-side CUDA stream the library launches on (cudaStream_t as void*),
  * so a caller can order its own work against the library's. */
 void* olamgpu_stream(void);

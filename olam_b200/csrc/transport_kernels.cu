@@ -16,6 +16,7 @@
 //
 // Device level index kd = Fortran k - 1.
 #include <cfloat>
+#include <string>
 
 #include "transport_kernels.cuh"
 
@@ -867,4 +868,91 @@ void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t 
   OG_LAUNCHED();
 }
 
+// ---------------------------------------------------------------------------
+// Stage without allocation (olamgpu_update_scalar_noalloc): one explicit,
+// unlimited RK stage of update_scalar for one tracer on device arrays the
+// caller owns, through the plain passes above.  Its scratch -- the gradient
+// planes (2 or 5 per cell), the V-face values and a zero implicit fraction
+// per column -- lives in a fixed device array, so the call itself never
+// allocates device memory.
+// ---------------------------------------------------------------------------
+#define NOALLOC_SCRATCH_FLOATS (16u << 20)   // 64 MiB: about NXP <= 66 at 61 levels, order 2
+static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_SCRATCH_FLOATS];
+
+// address of g_noalloc_scratch on the current device, looked up on the first
+// call made with that device current
+static int noalloc_scratch(float** out) {
+  static float* ptrs[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e)); return OLAMGPU_E_CUDA; }
+  if (dev < 0 || dev >= 64) { set_error("device ordinal above 63"); return OLAMGPU_E_UNSUPPORTED; }
+  if (!ptrs[dev]) {
+    float* p = nullptr;
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return OLAMGPU_E_CUDA;
+    }
+    ptrs[dev] = p;
+  }
+  *out = ptrs[dev];
+  return OLAMGPU_OK;
+}
+
+static int update_scalar_noalloc(const float* scp, const float* scp0, const float* sct, const float* rhos,
+                                 const float* vmasc, const float* wmasc, float dtr, float* out, void* stream) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (!scp || !scp0 || !sct || !rhos || !vmasc || !wmasc || !out) {
+    set_error("update_scalar_noalloc: NULL array");
+    return OLAMGPU_E_ARG;
+  }
+  const DevGrid& d = C.g;
+  const int order = C.opts.scal_horiz_adv_order;
+  if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  const size_t i2d = order == 3 ? 5 : 2;
+  const size_t n_gx = i2d * d.mwa * d.mza, n_upv = (size_t)d.mva * d.mza, n_ff = d.mwa;
+  const size_t need = n_gx + n_upv + n_ff;
+  if (need > NOALLOC_SCRATCH_FLOATS) {
+    set_error("update_scalar_noalloc: this grid needs " + std::to_string(need) +
+              " floats of scratch; the fixed scratch holds " + std::to_string(NOALLOC_SCRATCH_FLOATS));
+    return OLAMGPU_E_ARG;
+  }
+  float* scr = nullptr;
+  OG_CHECK(noalloc_scratch(&scr));
+  float* gx = scr;
+  float* upv = scr + n_gx;
+  float* ff = upv + n_upv;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : C.stream;
+  // every column explicit: the implicit fraction must read zero
+  OG_CUDA(cudaMemsetAsync(ff, 0, n_ff * sizeof(float), s));
+  const CTView in{scp, 1, 0}, in0{scp0, 1, 0}, tend{sct, 1, 0};
+  const GridK g = gridk(d);
+  const size_t ng = (size_t)d.nw_prog * d.mza;
+  k_grad<<<cdiv(ng, 256), 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, in, gx, 1, order, d.gxc.p, d.gyc.p, d.xy_h.p);
+  const VCoef vc{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
+  const size_t nv = (size_t)d.nv_wadj * d.mza;
+  k_vflux<<<cdiv(nv, 256), 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, in, in0, gx, vmasc, 1, order, vc, nullptr,
+                                        upv, nullptr, nullptr);
+  WcolArgs A;
+  A.g = g;
+  A.prog = d.jtw_prog.p; A.nprog = d.nw_prog;
+  A.scp = in; A.scp0 = in0; A.sct = tend; A.rhos = rhos;
+  A.vmasc = vmasc; A.wmasc = wmasc; A.ff = ff;
+  A.upv = upv; A.sfv = nullptr; A.scale = nullptr; A.upw = nullptr;
+  A.out = TView{out, 1, 0}; A.nt = 1; A.istage = 1; A.nrk = 1; A.dtr = dtr;
+  A.mode = nullptr;
+  k_wcol<<<cdiv((size_t)d.nw_prog, 128), 128, 0, s>>>(A);
+  OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+  OG_CUDA(cudaGetLastError());
+  return OLAMGPU_OK;
+}
+
 }  // namespace olamgpu
+
+extern "C" int olamgpu_update_scalar_noalloc(const float* scp, const float* scp0, const float* sct,
+                                             const float* rhos, const float* vmasc, const float* wmasc,
+                                             float dtr, float* out, void* stream) {
+  return olamgpu::update_scalar_noalloc(scp, scp0, sct, rhos, vmasc, wmasc, dtr, out, stream);
+}

@@ -25,7 +25,7 @@ EXPORTS = [
     "olamgpu_strerror", "olamgpu_set_coherence", "olamgpu_sync_to_device", "olamgpu_sync_to_host",
     "olamgpu_set_transport_form", "olamgpu_scalar_transport_rk", "olamgpu_prog_wrtv_rk",
     "olamgpu_tend0", "olamgpu_timeavg_momsc", "olamgpu_stream", "olamgpu_launch_count",
-    "olamgpu_profile", "olamgpu_profile_read",
+    "olamgpu_profile", "olamgpu_profile_read", "olamgpu_update_scalar_noalloc",
 ]
 
 
@@ -64,6 +64,7 @@ def load():
     lib.olamgpu_profile.argtypes = [C.c_int, C.c_int]
     lib.olamgpu_profile_read.argtypes = [C.c_int, C.c_char_p, C.POINTER(C.c_double),
                                          C.POINTER(C.c_ulonglong)]
+    lib.olamgpu_update_scalar_noalloc.argtypes = [C.c_void_p] * 6 + [C.c_float, C.c_void_p, C.c_void_p]
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
             getattr(lib, name).restype = C.c_int

@@ -42,6 +42,8 @@ def test_strerror_and_state_errors():
     assert rc == abi.E_STATE
     assert L.olamgpu_sync_to_host(abi.F_ALL) == abi.E_STATE
     assert L.olamgpu_set_coherence(7) == abi.E_ARG
+    assert L.olamgpu_update_scalar_noalloc(None, None, None, None, None, None, C.c_float(1.0),
+                                           None, None) == abi.E_STATE
 
 
 def test_null_arguments_rejected():
