@@ -288,8 +288,9 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 size_t tile_smem_bytes(int order, int T, int nu, int nr1) {
   const int npl = order == 2 ? 2 : 5;
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  // U rows, gradient planes, scp0/sct rows, records, LV, U columns, a_w
-  return al((size_t)nu * 256) + al((size_t)nr1 * npl * 256) + al((size_t)T * 2 * 256) +
+  // mbarrier, U rows, gradient planes, scp0/sct rows, records, per-level
+  // values, U columns, a_w
+  return 16 + al((size_t)nu * 256) + al((size_t)nr1 * npl * 256) + al((size_t)T * 2 * 256) +
          al((size_t)nr1 * TILE_R1W(order) * 4) + al((size_t)T * TILE_TCW(order) * 4) + al((size_t)T * 12 * 4) +
          al((size_t)nu * 4) + 64;
 }

@@ -52,12 +52,36 @@ struct TileArgs {
 // volti, dtr / rhos, 1 - ff, pad
 #define TILE_LV 12
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+// ---- bulk copies into shared memory, completed on an mbarrier -------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// the single arrival of a phase, announcing the bytes its copies will deliver
+__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// waits for the phase with the given parity to complete; gives up after
+// about a second of clock (returns false)
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  const long long t_start = clock64();
+  while (true) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t_start > (1ll << 31)) return false;
+  }
+}
 
 // acc + w * a on both tracers of a lane (one packed FFMA2)
 __device__ __forceinline__ float2 fma2s(float w, float2 a, float2 acc) {
@@ -80,6 +104,43 @@ __device__ __forceinline__ float2 zface_t(const float* aw, int mza, int kb, int 
   return r;
 }
 
+// four tracers of a lane as two packed pairs
+struct F4 {
+  float2 a, b;
+};
+__device__ __forceinline__ F4 zero4() { return F4{make_float2(0.f, 0.f), make_float2(0.f, 0.f)}; }
+__device__ __forceinline__ F4 lds4(const char* base, int off) {
+  const float4 v = *reinterpret_cast<const float4*>(base + off);
+  return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+__device__ __forceinline__ void sts4(const char* base, int off, F4 v) {
+  *reinterpret_cast<float4*>(const_cast<char*>(base) + off) = make_float4(v.a.x, v.a.y, v.b.x, v.b.y);
+}
+__device__ __forceinline__ F4 ldg4(const float* p) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+__device__ __forceinline__ void stg4(float* p, F4 v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v.a.x, v.a.y, v.b.x, v.b.y);
+}
+__device__ __forceinline__ F4 add4(F4 x, F4 y) { return F4{__fadd2_rn(x.a, y.a), __fadd2_rn(x.b, y.b)}; }
+__device__ __forceinline__ F4 neg4(F4 x) { return F4{make_float2(-x.a.x, -x.a.y), make_float2(-x.b.x, -x.b.y)}; }
+// acc + w * x
+__device__ __forceinline__ F4 fma4s(float w, F4 x, F4 acc) {
+  const float2 w2 = make_float2(w, w);
+  return F4{__ffma2_rn(w2, x.a, acc.a), __ffma2_rn(w2, x.b, acc.b)};
+}
+// x * w + acc (acc a vector)
+__device__ __forceinline__ F4 fma4v(F4 x, float w, F4 acc) { return fma4s(w, x, acc); }
+__device__ __forceinline__ F4 scale4(float w, F4 x) {
+  const float2 w2 = make_float2(w, w);
+  return F4{__fmul2_rn(w2, x.a), __fmul2_rn(w2, x.b)};
+}
+// grad_z_quadratic on four tracers (zface_t per pair)
+__device__ __forceinline__ F4 zface4(const float* aw, int mza, int kb, int lev, bool want_bot, F4 a, F4 b, F4 c) {
+  return F4{zface_t(aw, mza, kb, lev, want_bot, a.a, b.a, c.a), zface_t(aw, mza, kb, lev, want_bot, a.b, b.b, c.b)};
+}
+
 template <int ORDER>
 __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   constexpr int NPL = ORDER == 2 ? 2 : 5;     // gradient planes (and face offsets)
@@ -90,6 +151,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   const int u_off = h.x, nU = h.y, nR1 = h.z, nT = h.w;
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
   unsigned char* p = smraw;
+  unsigned long long* MB = reinterpret_cast<unsigned long long*>(p);  p += 16;
   float2* U = reinterpret_cast<float2*>(p);  p += al((size_t)A.nu_max * 256);
   float2* G = reinterpret_cast<float2*>(p);  p += al((size_t)A.nr1_max * NPL * 256);
   float2* Q0 = reinterpret_cast<float2*>(p); p += al((size_t)A.T * 2 * 256);   // scp0, sct rows of the tile
@@ -99,6 +161,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   int* UIW = reinterpret_cast<int*>(p);      p += al((size_t)A.nu_max * 4);
   float* AW = reinterpret_cast<float*>(p);   // a_w at levels kd-1, kd, kd+1 (4 each)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned bar = smem_addr(MB);
 
   // tables of this tile, checked once: every index must address the arrays
   // it is used on (a failure is recorded and the block does nothing)
@@ -126,6 +189,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       UIW[i] = v;
     }
   }
+  if (tid == 0) mbar_init(bar, 1);
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
     return;
@@ -134,23 +198,29 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;
   const int t0 = grp * 64;
   const int seg = min(64, ntp - t0);  // tracers of this group (a multiple of 4)
-  const int nch = seg >> 2;           // 16-byte chunks per row
-  const bool act = 2 * lane < seg;
+  // a half warp per column: lane hl of half h holds tracers 4 hl .. 4 hl + 3
+  const int half = lane >> 4, hl = lane & 15;
+  const bool act = 4 * hl < seg;
+  const int nrow = nU + 2 * nT;
+  const unsigned rowbytes = (unsigned)seg * 4u;
 
+  // staging of level kd: one bulk copy per row (the U rows, then the
+  // tile's scp0 / sct rows) completing on the mbarrier, whose arrival with
+  // the byte count thread 0 has made beforehand; raw LV values; a_w
   auto stage = [&](int kd) {
-    for (int i = tid; i < nU * 16; i += TILE_THREADS) {
-      const int row = i >> 4, ch = i & 15;
-      if (ch < nch)
-        cp_async16(reinterpret_cast<char*>(U) + row * 256 + ch * 16,
-                   A.S + ((size_t)UIW[row] * mza + kd) * ntp + t0 + ch * 4);
+    for (int i = tid; i < nrow; i += TILE_THREADS) {
+      const float* src;
+      unsigned dst;
+      if (i < nU) {
+        src = A.S + ((size_t)UIW[i] * mza + kd) * ntp + t0;
+        dst = smem_addr(reinterpret_cast<char*>(U) + i * 256);
+      } else {
+        const int j = i - nU;   // 2 * cell + (0: scp0, 1: sct)
+        src = ((j & 1) ? A.SCT : A.S0) + ((size_t)UIW[j >> 1] * mza + kd) * ntp + t0;
+        dst = smem_addr(reinterpret_cast<char*>(Q0) + j * 256);
+      }
+      bulk_g2s(dst, src, rowbytes, bar);
     }
-    for (int i = tid; i < nT * 32; i += TILE_THREADS) {
-      const int row = i >> 4, ch = i & 15;   // row = 2 * cell + (0: scp0, 1: sct)
-      if (ch < nch)
-        cp_async16(reinterpret_cast<char*>(Q0) + row * 256 + ch * 16,
-                   ((row & 1) ? A.SCT : A.S0) + ((size_t)UIW[row >> 1] * mza + kd) * ntp + t0 + ch * 4);
-    }
-    cp_async_commit();
     for (int i = tid; i < nT * TILE_LV; i += TILE_THREADS) {
       const int c = i / TILE_LV, f = i - c * TILE_LV;
       const int* w = TC + c * TCW;
@@ -171,13 +241,24 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
     }
   };
 
+  const char* Ul = reinterpret_cast<const char*>(U) + hl * 16;
+  const char* Gl = reinterpret_cast<const char*>(G) + hl * 16;
+  if (tid == 0) mbar_expect(bar, (unsigned)nrow * rowbytes);
+  __syncthreads();
   stage(kb);
   for (int kd = kb; kd < mza; ++kd) {
-    cp_async_wait_all();
-    __syncthreads();
+    const bool arrived = mbar_wait(bar, (unsigned)((kd - kb) & 1));
+    if (__syncthreads_or(!arrived)) {
+      // the copies did not complete: record it, give them a second bound, leave
+      if (tid == 0 && atomicCAS(A.err, 0, 200) == 0) { A.err[1] = kd; A.err[2] = blockIdx.x; A.err[3] = tile; }
+      mbar_wait(bar, (unsigned)((kd - kb) & 1));
+      return;
+    }
+    // the next level's arrival; its copies start after phase B
+    if (tid == 0 && kd + 1 < mza) mbar_expect(bar, (unsigned)nrow * rowbytes);
     // ---- phase A: gradient planes of the ring-1 cells (grad_t2d order:
     // differences to the cell, summed over the neighbours in table order)
-    for (int r = warp; r < nR1; r += TILE_NW) {
+    for (int r = 2 * warp + half; r < nR1; r += 2 * TILE_NW) {
       const int4* w4 = reinterpret_cast<const int4*>(R1 + r * R1W);
       const int4 na = w4[0], nb = w4[1];
       const int nbo[6] = {na.x, na.y, na.z, na.w, nb.x, nb.y};   // byte offsets of the U rows
@@ -192,96 +273,98 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
         const float2 v = reinterpret_cast<const float2*>(c4 + (6 * NPL) / 4)[0];
         cf[6 * NPL - 2] = v.x; cf[6 * NPL - 1] = v.y;
       }
-      const char* Ul = reinterpret_cast<const char*>(U + lane);
-      const float2 nsc = neg2(U[r * 32 + lane]);
-      float2 g[NPL];
+      const F4 nsc = neg4(lds4(Ul, r * 256));
+      F4 g[NPL];
 #pragma unroll
-      for (int m = 0; m < NPL; ++m) g[m] = make_float2(0.f, 0.f);
+      for (int m = 0; m < NPL; ++m) g[m] = zero4();
 #pragma unroll
       for (int n = 0; n < 6; ++n) {
-        const float2 d = add2(*reinterpret_cast<const float2*>(Ul + nbo[n]), nsc);
+        const F4 d = add4(lds4(Ul, nbo[n]), nsc);
 #pragma unroll
-        for (int m = 0; m < NPL; ++m) g[m] = fma2s(cf[m * 6 + n], d, g[m]);
+        for (int m = 0; m < NPL; ++m) g[m] = fma4s(cf[m * 6 + n], d, g[m]);
       }
 #pragma unroll
-      for (int m = 0; m < NPL; ++m) G[(r * NPL + m) * 32 + lane] = g[m];
+      for (int m = 0; m < NPL; ++m) sts4(Gl, (r * NPL + m) * 256, g[m]);
     }
     __syncthreads();
     // ---- phase B: faces, vertical fluxes and the update of the tile columns
     const float* aw = AW;
-    for (int c = warp; c < nT; c += TILE_NW) {
+    for (int c = 2 * warp + half; c < nT; c += 2 * TILE_NW) {
+      const float* lv = LV + c * TILE_LV;
       const int* w = TC + c * TCW;
-      const int4 h4 = reinterpret_cast<const int4*>(w)[0];
-      const int iw = h4.x, side = h4.y;
-      const int4 q1 = reinterpret_cast<const int4*>(w)[1];      // U offsets 0..3
-      const int4 q2 = reinterpret_cast<const int4*>(w)[2];      // U offsets 4, 5, G offsets 0, 1
-      const int4 q3 = reinterpret_cast<const int4*>(w)[3];      // G offsets 2..5
-      const float4 dva = reinterpret_cast<const float4*>(w)[5];  // ev 4, 5, dv 0, 1
-      const float4 dvb = reinterpret_cast<const float4*>(w)[6];  // dv 2..5
-      const int nbu[6] = {q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
-      const int nbg[6] = {q2.z, q2.w, q3.x, q3.y, q3.z, q3.w};
-      const float dvv[6] = {dva.z, dva.w, dvb.x, dvb.y, dvb.z, dvb.w};
-      const float4 l0 = reinterpret_cast<const float4*>(LV + c * TILE_LV)[0];
-      const float4 l1 = reinterpret_cast<const float4*>(LV + c * TILE_LV)[1];
-      const float4 l2 = reinterpret_cast<const float4*>(LV + c * TILE_LV)[2];
-      const float vmv[6] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y};
+      const int iw = w[TILE_TC_IW], side = w[TILE_TC_SIDE];
+      const float4 l1 = reinterpret_cast<const float4*>(lv)[1];
+      const float4 l2 = reinterpret_cast<const float4*>(lv)[2];
       const float wkm1 = l1.z, wk0 = l1.w, vt = l2.x, rinv = l2.y, fexpl = l2.z;
-      const size_t row = ((size_t)iw * mza + kd) * ntp + t0 + 2 * lane;
+      const size_t row = ((size_t)iw * mza + kd) * ntp + t0 + 4 * hl;
       const size_t lvl = (size_t)ntp;
-      const float2 s0 = U[c * 32 + lane];
-      const float2 s00 = Q0[(2 * c) * 32 + lane], st = Q0[(2 * c + 1) * 32 + lane];
-      float2 sm1 = s0, sp1 = s0;
+      const F4 s0 = lds4(Ul, c * 256);
+      const F4 s00 = lds4(reinterpret_cast<const char*>(Q0) + hl * 16, (2 * c) * 256);
+      const F4 st = lds4(reinterpret_cast<const char*>(Q0) + hl * 16, (2 * c + 1) * 256);
+      F4 sm1 = s0, sp1 = s0;
       const bool need_m2 = kd != kb && !(wkm1 < 0.f);
       const bool need_p2 = kd != mza - 1 && wk0 < 0.f;
       if (act) {
-        if (kd - 1 >= kb) sm1 = __ldg(reinterpret_cast<const float2*>(A.S + row - lvl));
-        if (kd + 1 < mza) sp1 = __ldg(reinterpret_cast<const float2*>(A.S + row + lvl));
+        if (kd - 1 >= kb) sm1 = ldg4(A.S + row - lvl);
+        if (kd + 1 < mza) sp1 = ldg4(A.S + row + lvl);
       }
-      float2 sm2 = sm1, sp2 = sp1;
-      if (act && need_m2 && kd - 2 >= kb) sm2 = __ldg(reinterpret_cast<const float2*>(A.S + row - 2 * lvl));
-      if (act && need_p2 && kd + 2 < mza) sp2 = __ldg(reinterpret_cast<const float2*>(A.S + row + 2 * lvl));
-      const float2 ns00 = neg2(s00);
-      float2 fd = make_float2(0.f, 0.f);
-      const char* Ul = reinterpret_cast<const char*>(U + lane);
-      const char* Gl = reinterpret_cast<const char*>(G + lane);
-      const int cu = c * 256, cg = c * NPL * 256;
+      F4 sm2 = sm1, sp2 = sp1;
+      if (act && need_m2 && kd - 2 >= kb) sm2 = ldg4(A.S + row - 2 * lvl);
+      if (act && need_p2 && kd + 2 < mza) sp2 = ldg4(A.S + row + 2 * lvl);
+      const F4 ns00 = neg4(s00);
+      // the six faces across lanes 0..5 of the half warp: dirv*vmasc, upwind
+      // side, and the outflow faces' sums (their share of the flux divergence
+      // is so * (S - S0) + sum_m sm[m] * grad_m(cell))
+      const int nf = hl < 6 ? hl : 0;
+      const float vmf = hl < 6 ? lv[nf] : 0.f;
+      const float dvvm = __int_as_float(w[TILE_TC_DV + nf]) * vmf;
+      const bool inflow = hl < 6 && ((vmf < 0.f ? 1 : 0) != ((side >> nf) & 1));
+      float so = inflow ? 0.f : dvvm, sm[NPL];
+      {
+        const float* oo = reinterpret_cast<const float*>(w + TILE_TC_OFF + nf * NPL);
 #pragma unroll
-      for (int n = 0; n < 6; ++n) {
-        // upwind side of face n: the neighbour (inflow) or the cell itself
-        const bool inflow = (vmv[n] < 0.f ? 1 : 0) != ((side >> n) & 1);
-        const int su = inflow ? nbu[n] : cu, sg = inflow ? nbg[n] : cg;
-        const float* off = reinterpret_cast<const float*>(w + TILE_TC_OFF + ((inflow ? 6 : 0) + n) * NPL);
-        float2 val = *reinterpret_cast<const float2*>(Ul + su);
-        if (NPL == 2) {
-          const float2 o2 = *reinterpret_cast<const float2*>(off);
-          val = fma2s(o2.x, *reinterpret_cast<const float2*>(Gl + sg), val);
-          val = fma2s(o2.y, *reinterpret_cast<const float2*>(Gl + sg + 256), val);
-        } else {
+        for (int m = 0; m < NPL; ++m) sm[m] = so * oo[m];
+      }
 #pragma unroll
-          for (int m = 0; m < NPL; ++m) val = fma2s(off[m], *reinterpret_cast<const float2*>(Gl + sg + m * 256), val);
+      for (int o = 8; o > 0; o >>= 1) {
+        so += __shfl_xor_sync(0xffffffffu, so, o, 16);
+#pragma unroll
+        for (int m = 0; m < NPL; ++m) sm[m] += __shfl_xor_sync(0xffffffffu, sm[m], o, 16);
+      }
+      unsigned inmask = (__ballot_sync(0xffffffffu, inflow) >> (16 * half)) & 0x3fu;
+      F4 fd = scale4(so, add4(s0, ns00));
+#pragma unroll
+      for (int m = 0; m < NPL; ++m) fd = fma4s(sm[m], lds4(Gl, (c * NPL + m) * 256), fd);
+      // inflow faces: the upwind neighbour's reconstruction
+      const float dvsrc = dvvm;
+      while (__any_sync(0xffffffffu, inmask != 0)) {
+        const int f = inmask ? __ffs(inmask) - 1 : 0;
+        const float coef = __shfl_sync(0xffffffffu, dvsrc, f, 16);
+        if (inmask) {
+          inmask &= inmask - 1;
+          const int su = w[TILE_TC_NBU + f], sg = w[TILE_TC_NBG + f];
+          const float* of = reinterpret_cast<const float*>(w + TILE_TC_OFF + (6 + f) * NPL);
+          F4 val = lds4(Ul, su);
+#pragma unroll
+          for (int m = 0; m < NPL; ++m) val = fma4s(of[m], lds4(Gl, sg + m * 256), val);
+          fd = fma4s(coef, add4(val, ns00), fd);
         }
-        fd = fma2s(dvv[n] * vmv[n], add2(val, ns00), fd);
       }
       // vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded)
-      float2 up_lo, up_hi;
+      F4 up_lo, up_hi;
       if (kd == kb) up_lo = s0;                                                    // scp_upw(kb-1) = scp(kb)
-      else if (wkm1 < 0.f) up_lo = zface_t(aw + 4, mza, kb, kd, true, sm1, s0, sp1);      // scpb(kd)
-      else up_lo = zface_t(aw, mza, kb, kd - 1, false, sm2, sm1, s0);                     // scpt(kd-1)
+      else if (wkm1 < 0.f) up_lo = zface4(aw + 4, mza, kb, kd, true, sm1, s0, sp1);       // scpb(kd)
+      else up_lo = zface4(aw, mza, kb, kd - 1, false, sm2, sm1, s0);                      // scpt(kd-1)
       if (kd == mza - 1) up_hi = s0;                                               // scp_upw(mza) = scp(mza)
-      else if (wk0 < 0.f) up_hi = zface_t(aw + 8, mza, kb, kd + 1, true, s0, sp1, sp2);   // scpb(kd+1)
-      else up_hi = zface_t(aw + 4, mza, kb, kd, false, sm1, s0, sp1);                     // scpt(kd)
-      float2 o;
-      {
-        float v = fexpl * (wkm1 * (up_lo.x - s00.x) - wk0 * (up_hi.x - s00.x));
-        o.x = s00.x + (st.x + vt * (fd.x + v)) * rinv;
-        v = fexpl * (wkm1 * (up_lo.y - s00.y) - wk0 * (up_hi.y - s00.y));
-        o.y = s00.y + (st.y + vt * (fd.y + v)) * rinv;
-      }
+      else if (wk0 < 0.f) up_hi = zface4(aw + 8, mza, kb, kd + 1, true, s0, sp1, sp2);    // scpb(kd+1)
+      else up_hi = zface4(aw + 4, mza, kb, kd, false, sm1, s0, sp1);                      // scpt(kd)
+      // scp = scp0 + dtr * (sct + volti * (fluxdiv + fexpl * vertical)) / rhos
+      const F4 v = scale4(fexpl, add4(scale4(wkm1, add4(up_lo, ns00)), scale4(-wk0, add4(up_hi, ns00))));
+      const F4 o = fma4v(add4(st, scale4(vt, add4(fd, v))), rinv, s00);
       if (act) {
-        *reinterpret_cast<float2*>(A.OUT + row) = o;
+        stg4(A.OUT + row, o);
         if (kd == kb)
-          for (int k2 = 0; k2 < kb; ++k2)
-            *reinterpret_cast<float2*>(A.OUT + ((size_t)iw * mza + k2) * ntp + t0 + 2 * lane) = o;
+          for (int k2 = 0; k2 < kb; ++k2) stg4(A.OUT + ((size_t)iw * mza + k2) * ntp + t0 + 4 * hl, o);
       }
     }
     __syncthreads();
