@@ -122,14 +122,14 @@ static void release_all() {
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
                        &d.w_nb, &d.w_ev, &d.w_im, &d.v_iw, &d.v_im, &d.m_iv, &d.m_iw, &d.m_im,
                        &d.lpw, &d.lpv, &d.lpm, &d.iwglobe, &d.w_nonprog, &d.colrec,
-                       &d.tile_hdr, &d.tile_u, &d.tile_r1, &d.tile_tc};
+                       &d.tile_hdr, &d.tile_u, &d.tile_tc};
   for (auto* b : ib) b->release();
   DevBuf<float>* fb[] = {&d.w_dirv, &d.gxc, &d.gyc, &d.xy_h, &d.xy_hu, &d.dxps, &d.dyps, &d.xx0_v,
                          &d.xy0_v, &d.yy0_v, &d.xx0_vu, &d.xy0_vu, &d.yy0_vu, &d.a_w, &d.a_wu,
-                         &d.volti, &d.ew_b, &d.ew_u};
+                         &d.volti, &d.ew_b, &d.ew_u, &d.tile_a};
   for (auto* b : fb) b->release();
   d.ew_order = 0;
-  d.tile_T = d.ntiles = d.tile_nu_max = d.tile_nr1_max = d.tile_order = 0;
+  d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
   Tracers& tr = C.tr;
   for (size_t i = 0; i < tr.p.size(); ++i) {
     tr.p[i].release();

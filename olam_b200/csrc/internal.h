@@ -142,45 +142,39 @@ struct DevGrid {
   DevBuf<float> ew_b, ew_u;      // (mva, 2, 8)
   int ew_order = 0;
   DevBuf<int> colrec;            // (nw_prog, COLREC_WORDS) fused-kernel column records
-  // Tile tables of the tiled fused kernel (flat grids).  Tile t owns TILE_T
+  // Tile tables of the tiled fused kernel (flat grids).  Tile t owns tile_T
   // consecutive prognostic columns; its neighbourhood U lists those columns,
-  // then the rest of their neighbours (U[0, nr1) = ring 1), then the rest of
-  // the ring-1 cells' neighbours.  hdr[t] = {u_off, nU, nR1, nT}.
+  // then the rest of their neighbours, then the rest of those cells'
+  // neighbours.  hdr[t] = {u_off, nU, 0, nT}.
   DevBuf<int> tile_hdr;          // (ntiles, 4)
   DevBuf<int> tile_u;            // (sum nU) column of each U entry
-  DevBuf<int> tile_r1;           // (sum nU, TILE_R1W) ring-1 records, indexed u_off + r
   DevBuf<int> tile_tc;           // (ntiles * tile_T, TILE_TCW) tile-cell records
-  int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_nr1_max = 0, tile_order = 0;
+  DevBuf<float> tile_a;          // (ntiles * tile_T, TILE_AW) slot weights
+  int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_order = 0;
   std::vector<int> h_lpw;        // host copies used at set-up
 };
 
-// Records are laid out in 16-byte groups so the kernel reads them with
-// vector loads.  Pentagons are padded to six faces: the sixth neighbour is
-// the cell itself with zero weights, offsets, dirv and vmasc, which leaves
-// every sum unchanged.
-// Ring-1 record (words): byte offset in the U rows (U-local index * 256) of
-// the 6 neighbours, np, pad, then the gradient coefficients by plane,
-// c[m][n] at 8 + 6 m + n: order 2 gxps_coef, gyps_coef; order 3
-// xy_h(1..5, n).
-#define TILE_R1_NB 0
-#define TILE_R1_NP 6
-#define TILE_R1_C 8
-#define TILE_R1W(order) ((order) == 2 ? 20 : 40)
-// Tile-cell record (words): column, side bits (bit n: the cell is side 2,
-// itab_v%iw(2), of face n), np, pad; for the neighbour across each face its
-// byte offset in the U rows (index * 256) and in the gradient planes (index
-// * NOFF * 256); V index of each face; dirv of each face; pad; the face
-// offsets of the cell's own side (NOFF per face: dxps, dyps [, xx0_v,
-// xy0_v, yy0_v]); then those of the neighbour's side.
+// Tile-cell record (TILE_TCW words, in 16-byte groups): column, side bits
+// (bit n: the cell is side 2, itab_v%iw(2), of face n), np, number of
+// slots; the U-row byte offsets (U index * 256) of the TILE_NS slot columns
+// -- the cell's neighbours, then their other neighbours; unused slots point
+// at the cell itself; V index of each face; dirv of each face (pentagons:
+// the sixth face has dirv 0); pad.
+#define TILE_NS 20
 #define TILE_TC_IW 0
 #define TILE_TC_SIDE 1
 #define TILE_TC_NP 2
-#define TILE_TC_NBU 4
-#define TILE_TC_NBG 10
-#define TILE_TC_EV 16
-#define TILE_TC_DV 22
-#define TILE_TC_OFF 32
-#define TILE_TCW(order) ((order) == 2 ? 56 : 92)
+#define TILE_TC_NS 3
+#define TILE_TC_SLOT 4
+#define TILE_TC_EV 24
+#define TILE_TC_DV 30
+#define TILE_TCW 40
+// Slot weights (TILE_AW floats per tile cell): A[f][k][j] for face f < 6,
+// k = 0 when the cell is the upwind side of face f and 1 when the
+// neighbour across it is, slot j < TILE_NS: the weight of S(slot j) - S(cell)
+// in (upwind face value) - S(cell).  The order-2 or order-3 reconstruction
+// (gradient coefficients times face offsets) is folded into A at set-up.
+#define TILE_AW (6 * 2 * TILE_NS)
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)
@@ -267,12 +261,13 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s);
 int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
 // host tile tables (layouts above); T == 0 when the grid is left to the column kernel
 struct TileHost {
-  int T = 0, ntiles = 0, nu_max = 0, nr1_max = 0, order = 0;
-  std::vector<int> hdr, ulist, r1, tc;
+  int T = 0, ntiles = 0, nu_max = 0, order = 0;
+  std::vector<int> hdr, ulist, tc;
+  std::vector<float> a;
 };
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th);
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
-size_t tile_smem_bytes(int order, int T, int nu_max, int nr1_max);
+size_t tile_smem_bytes(int T, int nu_max);
 
 // dynamics entry points (dynamics.cu)
 int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s);

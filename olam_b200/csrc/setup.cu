@@ -285,18 +285,29 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 
 // ---- tiles of the tiled fused kernel ------------------------------------------
 
-size_t tile_smem_bytes(int order, int T, int nu, int nr1) {
-  const int npl = order == 2 ? 2 : 5;
+size_t tile_smem_bytes(int T, int nu) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  // mbarrier, U rows, gradient planes, scp0/sct rows, records, per-level
-  // values, U columns, a_w
-  return 16 + al((size_t)nu * 256) + al((size_t)nr1 * npl * 256) + al((size_t)T * 2 * 256) +
-         al((size_t)nr1 * TILE_R1W(order) * 4) + al((size_t)T * TILE_TCW(order) * 4) + al((size_t)T * 12 * 4) +
-         al((size_t)nu * 4) + 64;
+  // reserved, U rows, scp0/sct rows, tile-cell records, slot weights A, the
+  // level's slot weights W, per-level values, U columns, a_w
+  return 16 + al((size_t)nu * 256) + al((size_t)T * 2 * 256) + al((size_t)T * TILE_TCW * 4) +
+         al((size_t)T * TILE_AW * 4) + al((size_t)T * 24 * 4) + al((size_t)T * 12 * 4) + al((size_t)nu * 4) + 64;
 }
 
 // Two blocks per SM: 228 KB of shared memory less 1 KB reserved per block.
 #define TILE_SMEM_MAX (113 * 1024)
+
+// weight of the n-th neighbour of the cell on side sd of face iv in that
+// side's reconstructed face value: S(cell) + sum_n w_n (S(nb_n) - S(cell))
+// (grad_t2d: dxps*gxps_coef + dyps*gyps_coef; grad_t2d_quadratic folds the
+// quadratic terms xx0_v.. with xy_h the same way; bounded coefficients)
+static double face_weight(const olamgpu_grid* g, int order, int iv, int sd, int n) {
+  const int c = g->itab_v_iw[(size_t)iv * 2 + sd] - 1;
+  const size_t e = (size_t)iv * 2 + sd;
+  const double dx = g->dxps[e], dy = g->dyps[e];
+  if (order == 2) return dx * (double)g->gxps_coef[(size_t)c * 7 + n] + dy * (double)g->gyps_coef[(size_t)c * 7 + n];
+  const float* x = g->xy_h + ((size_t)c * 7 + n) * 5;
+  return dx * x[0] + dy * x[1] + (double)g->xx0_v[e] * x[2] + (double)g->xy0_v[e] * x[3] + (double)g->yy0_v[e] * x[4];
+}
 
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
   th = TileHost();
@@ -308,10 +319,28 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
     if (g->npoly[c] < 3 || g->npoly[c] > 6) return;  // left to the column kernel
   }
   auto nbr = [&](int c, int n) { return g->itab_w_iw[(size_t)c * 7 + n] - 1; };
+  // slot columns of cell c: its neighbours, then their other neighbours
+  std::vector<int> slots;
+  auto cell_slots = [&](int c) {
+    slots.clear();
+    auto add = [&](int x) {
+      if (x == c) return;
+      for (int y : slots) if (y == x) return;
+      slots.push_back(x);
+    };
+    for (int n = 0; n < g->npoly[c]; ++n) add(nbr(c, n));
+    const int n1 = (int)slots.size();
+    for (int i = 0; i < n1; ++i)
+      for (int n = 0; n < g->npoly[slots[i]]; ++n) add(nbr(slots[i], n));
+  };
+  for (int j = 0; j < nprog; ++j) {
+    cell_slots(g->jtw_prog[j] - 1);
+    if ((int)slots.size() > TILE_NS) return;   // left to the column kernel
+  }
   std::vector<int> stamp(mwa, -1), loc(mwa, 0);
   std::vector<int> U;
   // neighbourhood of tile t in U (local index of column x: loc[x] while stamp[x] == t)
-  auto gather = [&](int t, int T, int& nr1) {
+  auto gather = [&](int t, int T) {
     U.clear();
     const int j0 = t * T, j1 = std::min(nprog, j0 + T);
     auto add = [&](int x) {
@@ -321,115 +350,108 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
     const int nt = (int)U.size();
     for (int i = 0; i < nt; ++i)
       for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
-    nr1 = (int)U.size();
+    const int nr1 = (int)U.size();
     for (int i = nt; i < nr1; ++i)
       for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
   };
-  int T = 0, numax = 0, nr1max = 0;
-  const int cand[] = {64, 48, 32, 24, 16, 8};
+  int T = 0, numax = 0;
+  // multiples of the 16 half-warps of a block, so every warp gets the same work
+  const int cand[] = {64, 48, 32, 16};
   for (int Tc : cand) {
     std::fill(stamp.begin(), stamp.end(), -1);
     const int nt = (nprog + Tc - 1) / Tc;
-    int nu = 0, nr = 0;
+    int nu = 0;
     for (int t = 0; t < nt; ++t) {
-      int nr1;
-      gather(t, Tc, nr1);
+      gather(t, Tc);
       nu = std::max(nu, (int)U.size());
-      nr = std::max(nr, nr1);
     }
-    if (nu <= 65535 && tile_smem_bytes(order, Tc, nu, nr) <= TILE_SMEM_MAX) {
-      T = Tc; numax = nu; nr1max = nr;
+    if (nu <= 65535 && tile_smem_bytes(Tc, nu) <= TILE_SMEM_MAX) {
+      T = Tc; numax = nu;
       break;
     }
   }
   if (!T) return;  // neighbourhoods too large: the column kernel runs
   const int ntiles = (nprog + T - 1) / T;
-  const int R1W = TILE_R1W(order), TCW = TILE_TCW(order), noff = order == 2 ? 2 : 5;
   std::vector<int>& hdr = th.hdr;
   std::vector<int>& ulist = th.ulist;
-  std::vector<int>& r1 = th.r1;
   std::vector<int>& tc = th.tc;
+  std::vector<float>& am = th.a;
   hdr.assign((size_t)ntiles * 4, 0);
-  tc.assign((size_t)ntiles * T * TCW, 0);
+  tc.assign((size_t)ntiles * T * TILE_TCW, 0);
+  am.assign((size_t)ntiles * T * TILE_AW, 0.f);
   auto fbits = [](float f) { int i; std::memcpy(&i, &f, 4); return i; };
   std::fill(stamp.begin(), stamp.end(), -1);
+  std::vector<double> acc(TILE_AW);
   for (int t = 0; t < ntiles; ++t) {
-    int nr1;
-    gather(t, T, nr1);
+    gather(t, T);
     const int u_off = (int)ulist.size();
     const int nT = std::min(T, nprog - t * T);
     hdr[(size_t)t * 4 + 0] = u_off;
     hdr[(size_t)t * 4 + 1] = (int)U.size();
-    hdr[(size_t)t * 4 + 2] = nr1;
     hdr[(size_t)t * 4 + 3] = nT;
     ulist.insert(ulist.end(), U.begin(), U.end());
-    r1.resize(ulist.size() * R1W, 0);
-    for (int r = 0; r < nr1; ++r) {
-      const int c = U[r];
-      int* w = &r1[((size_t)u_off + r) * R1W];
-      const int np = g->npoly[c];
-      w[TILE_R1_NP] = np;
-      for (int n = 0; n < 6; ++n) w[TILE_R1_NB + n] = (n < np ? loc[nbr(c, n)] : r) * 256;
-      for (int n = 0; n < np; ++n) {
-        if (order == 2) {
-          w[TILE_R1_C + n] = fbits(g->gxps_coef[(size_t)c * 7 + n]);
-          w[TILE_R1_C + 6 + n] = fbits(g->gyps_coef[(size_t)c * 7 + n]);
-        } else {
-          for (int m = 0; m < 5; ++m) w[TILE_R1_C + m * 6 + n] = fbits(g->xy_h[((size_t)c * 7 + n) * 5 + m]);
-        }
-      }
-    }
     for (int i = 0; i < nT; ++i) {
       const int c = U[i];
-      int* w = &tc[((size_t)t * T + i) * TCW];
+      int* w = &tc[((size_t)t * T + i) * TILE_TCW];
+      float* a = &am[((size_t)t * T + i) * TILE_AW];
       const int np = g->npoly[c];
+      cell_slots(c);
+      const int ns = (int)slots.size();
+      auto slot_of = [&](int x) {
+        for (int j = 0; j < ns; ++j) if (slots[j] == x) return j;
+        return -1;
+      };
       w[TILE_TC_IW] = c;
       w[TILE_TC_NP] = np;
+      w[TILE_TC_NS] = ns;
+      for (int j = 0; j < TILE_NS; ++j) w[TILE_TC_SLOT + j] = (j < ns ? loc[slots[j]] : i) * 256;
+      std::fill(acc.begin(), acc.end(), 0.0);
       int side = 0;
-      for (int n = 0; n < 6; ++n) {
-        const bool v = n < np;
-        const int iv = v ? g->itab_w_iv[(size_t)c * 7 + n] - 1 : 0;
+      for (int f = 0; f < 6; ++f) {
+        const bool v = f < np;
+        const int iv = v ? g->itab_w_iv[(size_t)c * 7 + f] - 1 : 0;
         const int sd = v ? ((g->itab_v_iw[(size_t)iv * 2] - 1 == c) ? 0 : 1) : 0;
-        side |= sd << n;
-        const int u = v ? loc[nbr(c, n)] : i;
-        w[TILE_TC_NBU + n] = u * 256;
-        w[TILE_TC_NBG + n] = u * noff * 256;
-        w[TILE_TC_EV + n] = iv;
-        w[TILE_TC_DV + n] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + n] : 0.f);
+        side |= sd << f;
+        w[TILE_TC_EV + f] = iv;
+        w[TILE_TC_DV + f] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + f] : 0.f);
         if (!v) continue;
-        for (int k = 0; k < 2; ++k) {
-          const size_t e = (size_t)iv * 2 + (k == 0 ? sd : 1 - sd);
-          float* o = reinterpret_cast<float*>(w + TILE_TC_OFF + (k * 6 + n) * noff);
-          o[0] = g->dxps[e];
-          o[1] = g->dyps[e];
-          if (order == 3) { o[2] = g->xx0_v[e]; o[3] = g->xy0_v[e]; o[4] = g->yy0_v[e]; }
+        // the cell upwind: S(c) + sum_n w_n (S(nb_n(c)) - S(c))
+        for (int n = 0; n < np; ++n) acc[(f * 2 + 0) * TILE_NS + slot_of(nbr(c, n))] += face_weight(g, order, iv, sd, n);
+        // the neighbour u upwind: (1 - sum_n w_n)(S(u) - S(c)) + sum_n w_n (S(nb_n(u)) - S(c))
+        const int u = nbr(c, f), npu = g->npoly[u];
+        double sw = 0.0;
+        for (int n = 0; n < npu; ++n) {
+          const double wn = face_weight(g, order, iv, 1 - sd, n);
+          sw += wn;
+          const int x = nbr(u, n);
+          if (x != c) acc[(f * 2 + 1) * TILE_NS + slot_of(x)] += wn;
         }
+        acc[(f * 2 + 1) * TILE_NS + slot_of(u)] += 1.0 - sw;
       }
       w[TILE_TC_SIDE] = side;
+      for (int k = 0; k < TILE_AW; ++k) a[k] = (float)acc[k];
     }
   }
   th.T = T;
   th.ntiles = ntiles;
   th.nu_max = numax;
-  th.nr1_max = nr1max;
   th.order = order;
 }
 
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
-  d.tile_T = d.ntiles = d.tile_nu_max = d.tile_nr1_max = 0;
+  d.tile_T = d.ntiles = d.tile_nu_max = 0;
   d.tile_order = 0;
   TileHost th;
   make_tiles(g, order, th);
   if (!th.T) return OLAMGPU_OK;
   OG_CHECK(upload(d.tile_hdr, th.hdr.data(), th.hdr.size(), s));
   OG_CHECK(upload(d.tile_u, th.ulist.data(), th.ulist.size(), s));
-  OG_CHECK(upload(d.tile_r1, th.r1.data(), th.r1.size(), s));
+  OG_CHECK(upload(d.tile_a, th.a.data(), th.a.size(), s));
   OG_CHECK(upload(d.tile_tc, th.tc.data(), th.tc.size(), s));
   OG_CUDA(cudaStreamSynchronize(s));
   d.tile_T = th.T;
   d.ntiles = th.ntiles;
   d.tile_nu_max = th.nu_max;
-  d.tile_nr1_max = th.nr1_max;
   d.tile_order = order;
   return OLAMGPU_OK;
 }

@@ -27,11 +27,11 @@
 namespace olamgpu {
 
 struct TileArgs {
-  int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, nr1_max, mwa, mva;
+  int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa, mva;
   float dtr;
   const int4* __restrict__ hdr;
   const int* __restrict__ ulist;
-  const int* __restrict__ r1;
+  const float* __restrict__ amat;   // slot weights, TILE_AW per tile column
   const int* __restrict__ tc;
   const float* __restrict__ a_w;    // Fortran (mza, 2, 2)
   const float* __restrict__ volti;
@@ -52,36 +52,13 @@ struct TileArgs {
 // volti, dtr / rhos, 1 - ff, pad
 #define TILE_LV 12
 
-// ---- bulk copies into shared memory, completed on an mbarrier -------------------
-__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+// ---- 16-byte asynchronous copies into shared memory ------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
-// the single arrival of a phase, announcing the bytes its copies will deliver
-__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-// waits for the phase with the given parity to complete; gives up after
-// about a second of clock (returns false)
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  const long long t_start = clock64();
-  while (true) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (clock64() - t_start > (1ll << 31)) return false;
-  }
-}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // acc + w * a on both tracers of a lane (one packed FFMA2)
 __device__ __forceinline__ float2 fma2s(float w, float2 a, float2 acc) {
@@ -136,60 +113,57 @@ __device__ __forceinline__ F4 scale4(float w, F4 x) {
   const float2 w2 = make_float2(w, w);
   return F4{__fmul2_rn(w2, x.a), __fmul2_rn(w2, x.b)};
 }
+__device__ __forceinline__ F4 sel4(bool p, F4 x, F4 y) { return p ? x : y; }
 // grad_z_quadratic on four tracers (zface_t per pair)
 __device__ __forceinline__ F4 zface4(const float* aw, int mza, int kb, int lev, bool want_bot, F4 a, F4 b, F4 c) {
   return F4{zface_t(aw, mza, kb, lev, want_bot, a.a, b.a, c.a), zface_t(aw, mza, kb, lev, want_bot, a.b, b.b, c.b)};
 }
 
-template <int ORDER>
+// Work per level: phase W forms, for every tile column, the weights of its
+// slot columns in the horizontal flux divergence from the level's vmasc
+// (one thread per (column, slot), shared by all tracers); phase B computes,
+// per column and tracer,
+//   fluxdiv = SW * (S - S0) + sum_j W_j (S(slot j) - S)
+// with SW = sum_f dirv*vmasc, which is update_scalar's sum over the faces of
+// dirv*vmasc*(upwind face value - S0) with the reconstruction folded into W.
 __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
-  constexpr int NPL = ORDER == 2 ? 2 : 5;     // gradient planes (and face offsets)
-  constexpr int R1W = TILE_R1W(ORDER), TCW = TILE_TCW(ORDER);
   extern __shared__ __align__(16) unsigned char smraw[];
   const int tile = blockIdx.x % A.ntiles, grp = blockIdx.x / A.ntiles;
   const int4 h = A.hdr[tile];
-  const int u_off = h.x, nU = h.y, nR1 = h.z, nT = h.w;
+  const int u_off = h.x, nU = h.y, nT = h.w;
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
   unsigned char* p = smraw;
-  unsigned long long* MB = reinterpret_cast<unsigned long long*>(p);  p += 16;
+  p += 16;   // reserved
   float2* U = reinterpret_cast<float2*>(p);  p += al((size_t)A.nu_max * 256);
-  float2* G = reinterpret_cast<float2*>(p);  p += al((size_t)A.nr1_max * NPL * 256);
   float2* Q0 = reinterpret_cast<float2*>(p); p += al((size_t)A.T * 2 * 256);   // scp0, sct rows of the tile
-  int* R1 = reinterpret_cast<int*>(p);       p += al((size_t)A.nr1_max * R1W * 4);
-  int* TC = reinterpret_cast<int*>(p);       p += al((size_t)A.T * TCW * 4);
+  int* TC = reinterpret_cast<int*>(p);       p += al((size_t)A.T * TILE_TCW * 4);
+  float* AM = reinterpret_cast<float*>(p);   p += al((size_t)A.T * TILE_AW * 4);
+  float* WW = reinterpret_cast<float*>(p);   p += al((size_t)A.T * 24 * 4);    // W[0..20), SW at 20
   float* LV = reinterpret_cast<float*>(p);   p += al((size_t)A.T * TILE_LV * 4);
   int* UIW = reinterpret_cast<int*>(p);      p += al((size_t)A.nu_max * 4);
   float* AW = reinterpret_cast<float*>(p);   // a_w at levels kd-1, kd, kd+1 (4 each)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const unsigned bar = smem_addr(MB);
 
   // tables of this tile, checked once: every index must address the arrays
   // it is used on (a failure is recorded and the block does nothing)
-  int bad = (nU > A.nu_max || nR1 > A.nr1_max || nT > A.T || nR1 > nU || nT > nR1) ? 1 : 0;
+  int bad = (nU > A.nu_max || nT > A.T || nT > nU) ? 1 : 0;
   if (!bad) {
-    for (int i = tid; i < nR1 * R1W; i += TILE_THREADS) {
-      const int v = __ldg(A.r1 + (size_t)u_off * R1W + i), f = i % R1W;
-      if (f < 6 && ((unsigned)v >= (unsigned)nU * 256u || (v & 255))) bad = 2;
-      if (f == TILE_R1_NP && (v < 3 || v > 6)) bad = 3;
-      R1[i] = v;
-    }
-    for (int i = tid; i < nT * TCW; i += TILE_THREADS) {
-      const int v = __ldg(A.tc + (size_t)tile * A.T * TCW + i), f = i % TCW;
+    for (int i = tid; i < nT * TILE_TCW; i += TILE_THREADS) {
+      const int v = __ldg(A.tc + (size_t)tile * A.T * TILE_TCW + i), f = i % TILE_TCW;
       if (f == TILE_TC_IW && (v < 1 || v >= A.mwa)) bad = 4;
       if (f == TILE_TC_NP && (v < 3 || v > 6)) bad = 5;
-      if (f >= TILE_TC_NBU && f < TILE_TC_NBU + 6 && ((unsigned)v >= (unsigned)nR1 * 256u || (v & 255))) bad = 6;
-      if (f >= TILE_TC_NBG && f < TILE_TC_NBG + 6 && ((unsigned)v >= (unsigned)nR1 * NPL * 256u || (v & 255)))
-        bad = 9;
+      if (f >= TILE_TC_SLOT && f < TILE_TC_SLOT + TILE_NS && ((unsigned)v >= (unsigned)nU * 256u || (v & 255)))
+        bad = 6;
       if (f >= TILE_TC_EV && f < TILE_TC_EV + 6 && (unsigned)v >= (unsigned)A.mva) bad = 7;
       TC[i] = v;
     }
+    for (int i = tid; i < nT * TILE_AW; i += TILE_THREADS) AM[i] = __ldg(A.amat + (size_t)tile * A.T * TILE_AW + i);
     for (int i = tid; i < nU; i += TILE_THREADS) {
       const int v = __ldg(A.ulist + u_off + i);
       if (v < 1 || v >= A.mwa) bad = 8;
       UIW[i] = v;
     }
   }
-  if (tid == 0) mbar_init(bar, 1);
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
     return;
@@ -202,28 +176,30 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   const int half = lane >> 4, hl = lane & 15;
   const bool act = 4 * hl < seg;
   const int nrow = nU + 2 * nT;
-  const unsigned rowbytes = (unsigned)seg * 4u;
 
-  // staging of level kd: one bulk copy per row (the U rows, then the
-  // tile's scp0 / sct rows) completing on the mbarrier, whose arrival with
-  // the byte count thread 0 has made beforehand; raw LV values; a_w
+  // staging of level kd: 16-byte asynchronous copies of the U rows, then
+  // of the tile's scp0 / sct rows (a row is 16 chunks); per-level values; a_w
+  const int nch = seg >> 2;
   auto stage = [&](int kd) {
-    for (int i = tid; i < nrow; i += TILE_THREADS) {
+    for (int i = tid; i < nrow * 16; i += TILE_THREADS) {
+      const int r = i >> 4, ch = i & 15;
+      if (ch >= nch) continue;
       const float* src;
-      unsigned dst;
-      if (i < nU) {
-        src = A.S + ((size_t)UIW[i] * mza + kd) * ntp + t0;
-        dst = smem_addr(reinterpret_cast<char*>(U) + i * 256);
+      char* dst;
+      if (r < nU) {
+        src = A.S + ((size_t)UIW[r] * mza + kd) * ntp + t0;
+        dst = reinterpret_cast<char*>(U) + r * 256;
       } else {
-        const int j = i - nU;   // 2 * cell + (0: scp0, 1: sct)
+        const int j = r - nU;   // 2 * cell + (0: scp0, 1: sct)
         src = ((j & 1) ? A.SCT : A.S0) + ((size_t)UIW[j >> 1] * mza + kd) * ntp + t0;
-        dst = smem_addr(reinterpret_cast<char*>(Q0) + j * 256);
+        dst = reinterpret_cast<char*>(Q0) + j * 256;
       }
-      bulk_g2s(dst, src, rowbytes, bar);
+      cp_async16(dst + ch * 16, src + ch * 4);
     }
+    cp_async_commit();
     for (int i = tid; i < nT * TILE_LV; i += TILE_THREADS) {
       const int c = i / TILE_LV, f = i - c * TILE_LV;
-      const int* w = TC + c * TCW;
+      const int* w = TC + c * TILE_TCW;
       const int iw = w[TILE_TC_IW];
       const size_t x = (size_t)iw * mza + kd;
       float v = 0.f;
@@ -242,122 +218,81 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   };
 
   const char* Ul = reinterpret_cast<const char*>(U) + hl * 16;
-  const char* Gl = reinterpret_cast<const char*>(G) + hl * 16;
-  if (tid == 0) mbar_expect(bar, (unsigned)nrow * rowbytes);
-  __syncthreads();
   stage(kb);
   for (int kd = kb; kd < mza; ++kd) {
-    const bool arrived = mbar_wait(bar, (unsigned)((kd - kb) & 1));
-    if (__syncthreads_or(!arrived)) {
-      // the copies did not complete: record it, give them a second bound, leave
-      if (tid == 0 && atomicCAS(A.err, 0, 200) == 0) { A.err[1] = kd; A.err[2] = blockIdx.x; A.err[3] = tile; }
-      mbar_wait(bar, (unsigned)((kd - kb) & 1));
-      return;
-    }
-    // the next level's arrival; its copies start after phase B
-    if (tid == 0 && kd + 1 < mza) mbar_expect(bar, (unsigned)nrow * rowbytes);
-    // ---- phase A: gradient planes of the ring-1 cells (grad_t2d order:
-    // differences to the cell, summed over the neighbours in table order)
-    for (int r = 2 * warp + half; r < nR1; r += 2 * TILE_NW) {
-      const int4* w4 = reinterpret_cast<const int4*>(R1 + r * R1W);
-      const int4 na = w4[0], nb = w4[1];
-      const int nbo[6] = {na.x, na.y, na.z, na.w, nb.x, nb.y};   // byte offsets of the U rows
-      float cf[6 * NPL];
-      const float4* c4 = reinterpret_cast<const float4*>(R1 + r * R1W + TILE_R1_C);
+    cp_async_wait_all();
+    __syncthreads();
+    // ---- phase W: slot weights of this level, a thread per (column, slot)
+    for (int i = tid; i < nT * TILE_NS; i += TILE_THREADS) {
+      const int c = i / TILE_NS, j = i - c * TILE_NS;
+      const int* w = TC + c * TILE_TCW;
+      const float* lv = LV + c * TILE_LV;
+      const float* am = AM + c * TILE_AW;
+      const int side = w[TILE_TC_SIDE];
+      float acc = 0.f;
 #pragma unroll
-      for (int q = 0; q < (6 * NPL) / 4; ++q) {
-        const float4 v = c4[q];
-        cf[4 * q] = v.x; cf[4 * q + 1] = v.y; cf[4 * q + 2] = v.z; cf[4 * q + 3] = v.w;
+      for (int f = 0; f < 6; ++f) {
+        const float vm = lv[f];
+        const int k = ((vm < 0.f ? 1 : 0) != ((side >> f) & 1)) ? 1 : 0;   // 1: the neighbour is upwind
+        acc = fmaf(__int_as_float(w[TILE_TC_DV + f]) * vm, am[(f * 2 + k) * TILE_NS + j], acc);
       }
-      if ((6 * NPL) % 4) {
-        const float2 v = reinterpret_cast<const float2*>(c4 + (6 * NPL) / 4)[0];
-        cf[6 * NPL - 2] = v.x; cf[6 * NPL - 1] = v.y;
-      }
-      const F4 nsc = neg4(lds4(Ul, r * 256));
-      F4 g[NPL];
-#pragma unroll
-      for (int m = 0; m < NPL; ++m) g[m] = zero4();
-#pragma unroll
-      for (int n = 0; n < 6; ++n) {
-        const F4 d = add4(lds4(Ul, nbo[n]), nsc);
-#pragma unroll
-        for (int m = 0; m < NPL; ++m) g[m] = fma4s(cf[m * 6 + n], d, g[m]);
-      }
-#pragma unroll
-      for (int m = 0; m < NPL; ++m) sts4(Gl, (r * NPL + m) * 256, g[m]);
+      WW[c * 24 + j] = acc;
     }
     __syncthreads();
-    // ---- phase B: faces, vertical fluxes and the update of the tile columns
+    // ---- phase B: horizontal and vertical fluxes, the update of the tile columns
     const float* aw = AW;
     for (int c = 2 * warp + half; c < nT; c += 2 * TILE_NW) {
       const float* lv = LV + c * TILE_LV;
-      const int* w = TC + c * TCW;
-      const int iw = w[TILE_TC_IW], side = w[TILE_TC_SIDE];
+      const int* w = TC + c * TILE_TCW;
+      const int iw = w[TILE_TC_IW];
       const float4 l1 = reinterpret_cast<const float4*>(lv)[1];
       const float4 l2 = reinterpret_cast<const float4*>(lv)[2];
       const float wkm1 = l1.z, wk0 = l1.w, vt = l2.x, rinv = l2.y, fexpl = l2.z;
       const size_t row = ((size_t)iw * mza + kd) * ntp + t0 + 4 * hl;
       const size_t lvl = (size_t)ntp;
+      // the column's values two levels either side (the level's own range
+      // checks are the same for the whole block)
       const F4 s0 = lds4(Ul, c * 256);
+      F4 sm1 = s0, sp1 = s0;
+      if (act && kd - 1 >= kb) sm1 = ldg4(A.S + row - lvl);
+      if (act && kd + 1 < mza) sp1 = ldg4(A.S + row + lvl);
+      F4 sm2 = sm1, sp2 = sp1;
+      if (act && kd - 2 >= kb) sm2 = ldg4(A.S + row - 2 * lvl);
+      if (act && kd + 2 < mza) sp2 = ldg4(A.S + row + 2 * lvl);
       const F4 s00 = lds4(reinterpret_cast<const char*>(Q0) + hl * 16, (2 * c) * 256);
       const F4 st = lds4(reinterpret_cast<const char*>(Q0) + hl * 16, (2 * c + 1) * 256);
-      F4 sm1 = s0, sp1 = s0;
-      const bool need_m2 = kd != kb && !(wkm1 < 0.f);
-      const bool need_p2 = kd != mza - 1 && wk0 < 0.f;
-      if (act) {
-        if (kd - 1 >= kb) sm1 = ldg4(A.S + row - lvl);
-        if (kd + 1 < mza) sp1 = ldg4(A.S + row + lvl);
+      const F4 ns0 = neg4(s0), ns00 = neg4(s00);
+      const float* wc = WW + c * 24;
+      float sw = 0.f;   // sum over the faces of dirv * vmasc
+#pragma unroll
+      for (int f = 0; f < 6; ++f) sw = fmaf(__int_as_float(w[TILE_TC_DV + f]), lv[f], sw);
+      F4 fd = scale4(sw, add4(s0, ns00));
+#pragma unroll
+      for (int q = 0; q < TILE_NS / 4; ++q) {
+        const int4 so4 = reinterpret_cast<const int4*>(w + TILE_TC_SLOT)[q];
+        const float4 w4 = reinterpret_cast<const float4*>(wc)[q];
+        fd = fma4s(w4.x, add4(lds4(Ul, so4.x), ns0), fd);
+        fd = fma4s(w4.y, add4(lds4(Ul, so4.y), ns0), fd);
+        fd = fma4s(w4.z, add4(lds4(Ul, so4.z), ns0), fd);
+        fd = fma4s(w4.w, add4(lds4(Ul, so4.w), ns0), fd);
       }
-      F4 sm2 = sm1, sp2 = sp1;
-      if (act && need_m2 && kd - 2 >= kb) sm2 = ldg4(A.S + row - 2 * lvl);
-      if (act && need_p2 && kd + 2 < mza) sp2 = ldg4(A.S + row + 2 * lvl);
-      const F4 ns00 = neg4(s00);
-      // the six faces across lanes 0..5 of the half warp: dirv*vmasc, upwind
-      // side, and the outflow faces' sums (their share of the flux divergence
-      // is so * (S - S0) + sum_m sm[m] * grad_m(cell))
-      const int nf = hl < 6 ? hl : 0;
-      const float vmf = hl < 6 ? lv[nf] : 0.f;
-      const float dvvm = __int_as_float(w[TILE_TC_DV + nf]) * vmf;
-      const bool inflow = hl < 6 && ((vmf < 0.f ? 1 : 0) != ((side >> nf) & 1));
-      float so = inflow ? 0.f : dvvm, sm[NPL];
-      {
-        const float* oo = reinterpret_cast<const float*>(w + TILE_TC_OFF + nf * NPL);
-#pragma unroll
-        for (int m = 0; m < NPL; ++m) sm[m] = so * oo[m];
-      }
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
-        so += __shfl_xor_sync(0xffffffffu, so, o, 16);
-#pragma unroll
-        for (int m = 0; m < NPL; ++m) sm[m] += __shfl_xor_sync(0xffffffffu, sm[m], o, 16);
-      }
-      unsigned inmask = (__ballot_sync(0xffffffffu, inflow) >> (16 * half)) & 0x3fu;
-      F4 fd = scale4(so, add4(s0, ns00));
-#pragma unroll
-      for (int m = 0; m < NPL; ++m) fd = fma4s(sm[m], lds4(Gl, (c * NPL + m) * 256), fd);
-      // inflow faces: the upwind neighbour's reconstruction
-      const float dvsrc = dvvm;
-      while (__any_sync(0xffffffffu, inmask != 0)) {
-        const int f = inmask ? __ffs(inmask) - 1 : 0;
-        const float coef = __shfl_sync(0xffffffffu, dvsrc, f, 16);
-        if (inmask) {
-          inmask &= inmask - 1;
-          const int su = w[TILE_TC_NBU + f], sg = w[TILE_TC_NBG + f];
-          const float* of = reinterpret_cast<const float*>(w + TILE_TC_OFF + (6 + f) * NPL);
-          F4 val = lds4(Ul, su);
-#pragma unroll
-          for (int m = 0; m < NPL; ++m) val = fma4s(of[m], lds4(Gl, sg + m * 256), val);
-          fd = fma4s(coef, add4(val, ns00), fd);
-        }
-      }
-      // vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded)
+      // vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded): the
+      // upwind level's stencil is selected, then reconstructed once
       F4 up_lo, up_hi;
-      if (kd == kb) up_lo = s0;                                                    // scp_upw(kb-1) = scp(kb)
-      else if (wkm1 < 0.f) up_lo = zface4(aw + 4, mza, kb, kd, true, sm1, s0, sp1);       // scpb(kd)
-      else up_lo = zface4(aw, mza, kb, kd - 1, false, sm2, sm1, s0);                      // scpt(kd-1)
-      if (kd == mza - 1) up_hi = s0;                                               // scp_upw(mza) = scp(mza)
-      else if (wk0 < 0.f) up_hi = zface4(aw + 8, mza, kb, kd + 1, true, s0, sp1, sp2);    // scpb(kd+1)
-      else up_hi = zface4(aw + 4, mza, kb, kd, false, sm1, s0, sp1);                      // scpt(kd)
+      if (kd == kb) {
+        up_lo = s0;                                                   // scp_upw(kb-1) = scp(kb)
+      } else {
+        const bool dn = wkm1 < 0.f;   // scpb(kd) from (kd-1, kd, kd+1), else scpt(kd-1) from (kd-2, kd-1, kd)
+        up_lo = zface4(dn ? aw + 4 : aw, mza, kb, dn ? kd : kd - 1, dn, sel4(dn, sm1, sm2), sel4(dn, s0, sm1),
+                       sel4(dn, sp1, s0));
+      }
+      if (kd == mza - 1) {
+        up_hi = s0;                                                   // scp_upw(mza) = scp(mza)
+      } else {
+        const bool dn = wk0 < 0.f;    // scpb(kd+1) from (kd, kd+1, kd+2), else scpt(kd) from (kd-1, kd, kd+1)
+        up_hi = zface4(dn ? aw + 8 : aw + 4, mza, kb, dn ? kd + 1 : kd, dn, sel4(dn, s0, sm1), sel4(dn, sp1, s0),
+                       sel4(dn, sp2, sp1));
+      }
       // scp = scp0 + dtr * (sct + volti * (fluxdiv + fexpl * vertical)) / rhos
       const F4 v = scale4(fexpl, add4(scale4(wkm1, add4(up_lo, ns00)), scale4(-wk0, add4(up_hi, ns00))));
       const F4 o = fma4v(add4(st, scale4(vt, add4(fd, v))), rinv, s00);
@@ -381,26 +316,20 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
                       const float* rhos, int* status, cudaStream_t s) {
   TileArgs A;
   A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1;
-  A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.nr1_max = d.tile_nr1_max;
+  A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max;
   A.mwa = d.mwa; A.mva = d.mva;
   A.dtr = dtr;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
-  A.ulist = d.tile_u.p; A.r1 = d.tile_r1.p; A.tc = d.tile_tc.p;
+  A.ulist = d.tile_u.p; A.amat = d.tile_a.p; A.tc = d.tile_tc.p;
   A.a_w = d.a_w.p; A.volti = d.volti.p; A.vmasc = tp.vmasc.p; A.wmasc = tp.wmasc.p;
   A.rhos = rhos; A.ff = tp.ff.p;
   A.S = S; A.S0 = S0; A.SCT = SCT; A.OUT = OUT;
   A.err = status;
-  const int order = d.tile_order;
-  const size_t smem = tile_smem_bytes(order, d.tile_T, d.tile_nu_max, d.tile_nr1_max);
+  const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max);
   const unsigned ngrp = (unsigned)((ntp + 63) / 64);
   const unsigned nblk = (unsigned)d.ntiles * ngrp;
-  if (order == 2) {
-    OG_CUDA(cudaFuncSetAttribute(k_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile<2><<<nblk, TILE_THREADS, smem, s>>>(A);
-  } else {
-    OG_CUDA(cudaFuncSetAttribute(k_tile<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile<3><<<nblk, TILE_THREADS, smem, s>>>(A);
-  }
+  OG_CUDA(cudaFuncSetAttribute(k_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_tile<<<nblk, TILE_THREADS, smem, s>>>(A);
   OG_LAUNCHED();
   return OLAMGPU_OK;
 }
