@@ -643,6 +643,98 @@ static void tridif_fini(int ka, int kz, const T* cim1, const T* scr1, const T* c
   for (int k = kz - 1; k >= ka; --k) soln[k] = soln[k] - scr1[k + 1] * soln[k + 1];
 }
 
+/* Per-long-step coefficients of scalar_transport_rk that depend only on the
+ * winds and densities (scalar_transport_rk.F90:95-217): RK stage timesteps,
+ * the implicit fractions from check_cfls, the stage densities rhos and the
+ * implicit columns' tridiagonal factors.  Shared by the forward and adjoint. */
+template <class T>
+struct StepCoef {
+  int nrk = 0;
+  T dtlr[3] = {0, 0, 0};
+  std::vector<T> vmasc, wmasc, rho_old, ff_implic, rhos;
+  std::vector<int> kwtop;
+  struct Imp { std::vector<int> iw; std::vector<T> b1, b2, b3; };
+  std::vector<Imp> imp;
+};
+
+template <class T>
+static int prepare_step(const GridT<T>& G, const olamgpu_grid* g, const olamgpu_opts* o, const float* vmasc_f,
+                        const float* wmasc_f, const double* rho, const float* rho_old_f, const float* wc,
+                        const int* khtopv, olamgpu_cfl_diag* diag, StepCoef<T>& S) {
+  const int mza = g->mza, mwa = g->mwa, mva = g->mva;
+  const int nrk = o->nrk_scal;
+  if (nrk != 2 && nrk != 3) return OLAMGPU_E_UNSUPPORTED;
+  S.nrk = nrk;
+  const T dtl = (T)o->dtlm;  // real dtl = dtlm (r8 -> real)
+  S.vmasc = cvt<T>(vmasc_f, (size_t)mza * mva);
+  S.wmasc = cvt<T>(wmasc_f, (size_t)mza * mwa);
+  S.rho_old = cvt<T>(rho_old_f, (size_t)mza * mwa);
+  const T one3 = (T)1. / (T)3.;
+  const T frk3[3] = {one3, (T)0.5, (T)1.0};
+  const T frk2[2] = {(T)0.5, (T)1.0};
+  for (int n = 0; n < nrk; ++n) S.dtlr[n] = dtl * (nrk == 3 ? frk3[n] : frk2[n]);
+
+  S.ff_implic.assign((size_t)nrk * mwa, (T)0);
+  check_cfls(G, S.vmasc, S.wmasc, S.rho_old, wc, nrk, dtl, S.ff_implic, diag);
+
+  // rhos (117-162); nudging off
+  S.rhos.assign((size_t)mza * mwa * nrk, (T)0);
+  S.kwtop.assign(mwa + 1, 0);
+  const size_t plane = (size_t)mza * mwa;
+  for (int j = 0; j < g->nw_prog; ++j) {
+    int iw = g->jtw_prog[j];
+    int kb = G.lpw(iw);
+    for (int k = kb; k <= mza; ++k) {
+      T rhof = (T)F2(rho, k, iw);
+      T ro = F2(S.rho_old.data(), k, iw);
+      size_t ix = (size_t)(iw - 1) * mza + k - 1;
+      if (nrk == 3) {
+        S.rhos[ix] = (T)(2. / 3.) * ro + (T)(1. / 3.) * rhof;
+        S.rhos[plane + ix] = (T)0.5 * (ro + rhof);
+        S.rhos[2 * plane + ix] = rhof;
+      } else {
+        S.rhos[ix] = (T)0.5 * (ro + rhof);
+        S.rhos[plane + ix] = rhof;
+      }
+    }
+    if (khtopv) {
+      int m = 0;
+      for (int n = 1; n <= G.npoly(iw); ++n) m = std::max(m, khtopv[G.w_iv(iw, n) - 1]);
+      S.kwtop[iw] = m;
+    }
+  }
+  // implicit factorisation per stage (164-217); columns kept in jtw_prog order
+  S.imp.assign(nrk, typename StepCoef<T>::Imp());
+  for (int n = 1; n <= nrk; ++n) {
+    auto& I = S.imp[n - 1];
+    for (int j = 0; j < g->nw_prog; ++j) {
+      int iw = g->jtw_prog[j];
+      if (S.ff_implic[(size_t)(iw - 1) * nrk + n - 1] > (T)0.001) I.iw.push_back(iw);
+    }
+    size_t nn = I.iw.size();
+    I.b1.assign(nn * (mza + 1), 0); I.b2.assign(nn * (mza + 1), 0); I.b3.assign(nn * (mza + 1), 0);
+    for (size_t jj = 0; jj < nn; ++jj) {
+      int iw = I.iw[jj];
+      int kb = G.lpw(iw);
+      std::vector<T> wup(mza + 1, 0), wdn(mza + 1, 0), b2a(mza + 1, 0), b3a(mza + 1, 0);
+      for (int k = kb; k <= mza - 1; ++k) {
+        wup[k] = fmax_(F2(S.wmasc.data(), k, iw), (T)0.);
+        wdn[k] = fmin_(F2(S.wmasc.data(), k, iw), (T)0.);
+      }
+      T c1 = S.ff_implic[(size_t)(iw - 1) * nrk + n - 1] * S.dtlr[n - 1];
+      T* b1 = &I.b1[jj * (mza + 1)];
+      for (int k = kb; k <= mza; ++k) {
+        T c2 = c1 * G.volti_(k, iw) / S.rhos[(size_t)(n - 1) * plane + (size_t)(iw - 1) * mza + k - 1];
+        b1[k] = -c2 * wup[k - 1];
+        b2a[k] = (T)1.0 + c2 * (wup[k] - wdn[k - 1]);
+        b3a[k] = c2 * wdn[k];
+      }
+      tridif_prep(kb, mza, b1, b2a.data(), b3a.data(), &I.b2[jj * (mza + 1)], &I.b3[jj * (mza + 1)]);
+    }
+  }
+  return OLAMGPU_OK;
+}
+
 /* scalar_transport_rk (scalar_transport_rk.F90:30-385) */
 template <class T>
 static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
@@ -653,82 +745,24 @@ static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int
                                olamgpu_cfl_diag* diag) {
   GridT<T> G(g);
   const int mza = g->mza, mwa = g->mwa, mva = g->mva;
-  const int nrk = o->nrk_scal;
-  if (nrk != 2 && nrk != 3) return OLAMGPU_E_UNSUPPORTED;
   const int iorder = o->scal_horiz_adv_order;
   const int imonot = o->iscal_monot;
-  const T dtl = (T)o->dtlm;  // real dtl = dtlm (r8 -> real)
-  std::vector<T> vmasc = cvt<T>(vmasc_f, (size_t)mza * mva);
-  std::vector<T> wmasc = cvt<T>(wmasc_f, (size_t)mza * mwa);
-  std::vector<T> rho_old = cvt<T>(rho_old_f, (size_t)mza * mwa);
-  const T one3 = (T)1. / (T)3.;
-  const T frk3[3] = {one3, (T)0.5, (T)1.0};
-  const T frk2[2] = {(T)0.5, (T)1.0};
-  T dtlr[3];
-  for (int n = 0; n < nrk; ++n) dtlr[n] = dtl * (nrk == 3 ? frk3[n] : frk2[n]);
-
-  std::vector<T> ff_implic((size_t)nrk * mwa, (T)0);
-  check_cfls(G, vmasc, wmasc, rho_old, wc, nrk, dtl, ff_implic, diag);
+  StepCoef<T> SC;
+  int rc = prepare_step(G, g, o, vmasc_f, wmasc_f, rho, rho_old_f, wc, khtopv, diag, SC);
+  if (rc != OLAMGPU_OK) return rc;
+  const int nrk = SC.nrk;
+  const T* dtlr = SC.dtlr;
+  const std::vector<T>& vmasc = SC.vmasc;
+  const std::vector<T>& wmasc = SC.wmasc;
+  const std::vector<T>& rho_old = SC.rho_old;
+  const std::vector<T>& ff_implic = SC.ff_implic;
+  const std::vector<T>& rhos = SC.rhos;
+  const std::vector<int>& kwtop = SC.kwtop;
+  auto& imp = SC.imp;
+  const size_t plane = (size_t)mza * mwa;
   if (ff_out)
     for (size_t i = 0; i < ff_implic.size(); ++i) ff_out[i] = (float)ff_implic[i];
 
-  // rhos (117-162); nudging off
-  std::vector<T> rhos((size_t)mza * mwa * nrk, (T)0);
-  std::vector<int> kwtop(mwa + 1, 0);
-  const size_t plane = (size_t)mza * mwa;
-  for (int j = 0; j < g->nw_prog; ++j) {
-    int iw = g->jtw_prog[j];
-    int kb = G.lpw(iw);
-    for (int k = kb; k <= mza; ++k) {
-      T rhof = (T)F2(rho, k, iw);
-      T ro = F2(rho_old.data(), k, iw);
-      size_t ix = (size_t)(iw - 1) * mza + k - 1;
-      if (nrk == 3) {
-        rhos[ix] = (T)(2. / 3.) * ro + (T)(1. / 3.) * rhof;
-        rhos[plane + ix] = (T)0.5 * (ro + rhof);
-        rhos[2 * plane + ix] = rhof;
-      } else {
-        rhos[ix] = (T)0.5 * (ro + rhof);
-        rhos[plane + ix] = rhof;
-      }
-    }
-    if (khtopv) {
-      int m = 0;
-      for (int n = 1; n <= G.npoly(iw); ++n) m = std::max(m, khtopv[G.w_iv(iw, n) - 1]);
-      kwtop[iw] = m;
-    }
-  }
-  // implicit factorisation per stage (164-217); columns kept in jtw_prog order
-  struct Imp { std::vector<int> iw; std::vector<T> b1, b2, b3; };
-  std::vector<Imp> imp(nrk);
-  for (int n = 1; n <= nrk; ++n) {
-    Imp& I = imp[n - 1];
-    for (int j = 0; j < g->nw_prog; ++j) {
-      int iw = g->jtw_prog[j];
-      if (ff_implic[(size_t)(iw - 1) * nrk + n - 1] > (T)0.001) I.iw.push_back(iw);
-    }
-    size_t nn = I.iw.size();
-    I.b1.assign(nn * (mza + 1), 0); I.b2.assign(nn * (mza + 1), 0); I.b3.assign(nn * (mza + 1), 0);
-    for (size_t jj = 0; jj < nn; ++jj) {
-      int iw = I.iw[jj];
-      int kb = G.lpw(iw);
-      std::vector<T> wup(mza + 1, 0), wdn(mza + 1, 0), b2a(mza + 1, 0), b3a(mza + 1, 0);
-      wup[mza] = 0; wdn[mza] = 0; wup[kb - 1] = 0; wdn[kb - 1] = 0;
-      for (int k = kb; k <= mza - 1; ++k) {
-        wup[k] = fmax_(F2(wmasc.data(), k, iw), (T)0.);
-        wdn[k] = fmin_(F2(wmasc.data(), k, iw), (T)0.);
-      }
-      T c1 = ff_implic[(size_t)(iw - 1) * nrk + n - 1] * dtlr[n - 1];
-      T* b1 = &I.b1[jj * (mza + 1)];
-      for (int k = kb; k <= mza; ++k) {
-        T c2 = c1 * G.volti_(k, iw) / rhos[(size_t)(n - 1) * plane + (size_t)(iw - 1) * mza + k - 1];
-        b1[k] = -c2 * wup[k - 1];
-        b2a[k] = (T)1.0 + c2 * (wup[k] - wdn[k - 1]);
-        b3a[k] = c2 * wdn[k];
-      }
-      tridif_prep(kb, mza, b1, b2a.data(), b3a.data(), &I.b2[jj * (mza + 1)], &I.b3[jj * (mza + 1)]);
-    }
-  }
   TransportCtx<T> C{G, mza, mwa, mva, vmasc, wmasc, ff_implic, nrk};
   std::vector<T> scp0(plane);
   const T* rhos_nrk = rhos.data() + (size_t)(nrk - 1) * plane;
@@ -776,7 +810,7 @@ static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int
         update_scalar(C, scp, scp0.data(), sct, rhos_nrk, dtr, iorder, istage);
       }
       // implicit vertical transport (347-375)
-      Imp& I = imp[istage - 1];
+      auto& I = imp[istage - 1];
       const int nn = (int)I.iw.size();
 #pragma omp parallel for schedule(static)
       for (int jj = 0; jj < nn; ++jj) {
@@ -804,6 +838,171 @@ static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int
   return OLAMGPU_OK;
 }
 
+/* Adjoint of scalar_transport_rk for one long step with the winds and
+ * densities fixed and no limiter (iscal_monot = 0, no horizontal diffusion):
+ * the step maps (scp, sct) linearly to the new scp, and this applies the
+ * transpose.  lam holds dJ/d(new scp) on entry and dJ/d(old scp) on exit;
+ * lsct receives dJ/d(sct).  Each forward pass -- grad_t2d[_quadratic],
+ * scalar_v_column, grad_z_quadratic, scalar_w_column, tridif_fini -- is
+ * transposed in reverse order, stage by stage. */
+template <class T>
+static int scalar_transport_rk_adjoint(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
+                                       T* const* lam_list, T* const* lsct_list, const float* vmasc_f,
+                                       const float* wmasc_f, const double* rho, const float* rho_old_f,
+                                       const float* wc) {
+  if (o->iscal_monot != 0) return OLAMGPU_E_UNSUPPORTED;
+  GridT<T> G(g);
+  const int mza = g->mza, mwa = g->mwa, mva = g->mva;
+  const int iorder = o->scal_horiz_adv_order;
+  if (iorder != 2 && iorder != 3) return OLAMGPU_E_UNSUPPORTED;
+  StepCoef<T> SC;
+  int rc = prepare_step(G, g, o, vmasc_f, wmasc_f, rho, rho_old_f, wc, nullptr, nullptr, SC);
+  if (rc != OLAMGPU_OK) return rc;
+  const int nrk = SC.nrk;
+  const size_t plane = (size_t)mza * mwa;
+  const int np2d = iorder == 2 ? 2 : 5;
+  const T* vm = SC.vmasc.data();
+  const T* wm = SC.wmasc.data();
+  const T* rhos_nrk = SC.rhos.data() + (size_t)(nrk - 1) * plane;
+  std::vector<char> prog(mwa + 1, 0);
+  for (int j = 0; j < g->nw_prog; ++j) prog[g->jtw_prog[j]] = 1;
+
+  for (int n = 0; n < nscal; ++n) {
+    T* lam = lam_list[n];
+    T* ls = lsct_list[n];
+    std::fill(ls, ls + plane, (T)0);
+    std::vector<T> L(lam, lam + plane), L0(plane, (T)0), Lin(plane), Lupv((size_t)mza * mva),
+        Lg(plane * np2d);
+    // columns outside jtw_prog keep their values through the step
+    for (int iw = 1; iw <= mwa; ++iw)
+      if (!prog[iw])
+        for (int k = 1; k <= mza; ++k) { F2(L0.data(), k, iw) += F2(L.data(), k, iw); F2(L.data(), k, iw) = 0; }
+
+    for (int istage = nrk; istage >= 1; --istage) {
+      const T dtr = SC.dtlr[istage - 1];
+      // ---- implicit columns: out' = s0 + T^-1 (out - s0 - G s0)
+      auto& I = SC.imp[istage - 1];
+      for (size_t jj = 0; jj < I.iw.size(); ++jj) {
+        const int iw = I.iw[jj], kb = G.lpw(iw);
+        const T* cim1 = &I.b1[jj * (mza + 1)];
+        const T* scr1 = &I.b2[jj * (mza + 1)];
+        const T* cji = &I.b3[jj * (mza + 1)];
+        for (int k = 2; k <= kb - 1; ++k) { F2(L.data(), kb, iw) += F2(L.data(), k, iw); F2(L.data(), k, iw) = 0; }
+        // T = L U with L(k,k) = 1/cji(k), L(k,k-1) = cim1(k), U(k,k+1) = scr1(k+1):
+        // nu = T^-T lam: U^T z = lam (forward), then L^T nu = z (backward)
+        std::vector<T> z(mza + 2, (T)0), nu(mza + 2, (T)0);
+        for (int k = kb; k <= mza; ++k) z[k] = F2(L.data(), k, iw) - (k > kb ? scr1[k] * z[k - 1] : (T)0);
+        for (int k = mza; k >= kb; --k) nu[k] = cji[k] * (z[k] - (k < mza ? cim1[k + 1] * nu[k + 1] : (T)0));
+        const T ffv = SC.ff_implic[(size_t)(iw - 1) * nrk + istage - 1];
+        for (int k = kb; k <= mza; ++k) {
+          F2(L0.data(), k, iw) += F2(L.data(), k, iw) - nu[k];
+          const T c1 = ffv * dtr * G.volti_(k, iw) / SC.rhos[(size_t)(istage - 1) * plane + (size_t)(iw - 1) * mza + k - 1];
+          const T gk = -c1 * nu[k];
+          if (k <= mza - 1) {   // min(wmasc(k),0) * (s0(k+1) - s0(k))
+            const T a = fmin_(F2(wm, k, iw), (T)0.) * gk;
+            F2(L0.data(), k + 1, iw) += a; F2(L0.data(), k, iw) -= a;
+          }
+          if (k - 1 >= kb) {    // max(wmasc(k-1),0) * (s0(k) - s0(k-1))
+            const T a = fmax_(F2(wm, k - 1, iw), (T)0.) * gk;
+            F2(L0.data(), k, iw) += a; F2(L0.data(), k - 1, iw) -= a;
+          }
+          F2(L.data(), k, iw) = nu[k];
+        }
+      }
+      // ---- explicit update_scalar: out = s0 + dtr (sct + volti fluxdiv(s_in, s0)) / rhos
+      std::fill(Lin.begin(), Lin.end(), (T)0);
+      std::fill(Lupv.begin(), Lupv.end(), (T)0);
+      std::fill(Lg.begin(), Lg.end(), (T)0);
+      for (int j = 0; j < g->nw_prog; ++j) {
+        const int iw = g->jtw_prog[j], kb = G.lpw(iw);
+        const T fexpl = (T)1.0 - SC.ff_implic[(size_t)(iw - 1) * nrk + istage - 1];
+        for (int k = 1; k <= kb - 1; ++k) { F2(L.data(), kb, iw) += F2(L.data(), k, iw); F2(L.data(), k, iw) = 0; }
+        std::vector<T> mu(mza + 1, (T)0), Lupw(mza + 1, (T)0), Lb(mza + 1, (T)0), Lt(mza + 1, (T)0), Lds(mza + 1, (T)0);
+        for (int k = kb; k <= mza; ++k) {
+          const T lk = F2(L.data(), k, iw);
+          const T r = dtr / F2(rhos_nrk, k, iw);
+          F2(ls, k, iw) += lk * r;
+          F2(L0.data(), k, iw) += lk;
+          mu[k] = lk * r * G.volti_(k, iw);
+          // the vertical flux: fexpl (wm(k-1) (upw(k-1) - s0) - wm(k) (upw(k) - s0))
+          F2(L0.data(), k, iw) -= mu[k] * fexpl * (F2(wm, k - 1, iw) - F2(wm, k, iw));
+          Lupw[k - 1] += mu[k] * fexpl * F2(wm, k - 1, iw);
+          Lupw[k] -= mu[k] * fexpl * F2(wm, k, iw);
+        }
+        // the horizontal flux: sum_v dirv vmasc (upv - s0)
+        for (int jv = 1; jv <= G.npoly(iw); ++jv) {
+          const int iv = G.w_iv(iw, jv);
+          const T d = G.w_dirv(iw, jv);
+          for (int k = G.lpv(iv); k <= mza; ++k) {
+            const T a = mu[k] * d * F2(vm, k, iv);
+            F2(Lupv.data(), k, iv) += a;
+            F2(L0.data(), k, iw) -= a;
+          }
+        }
+        // scp_upw: boundary faces take the column's end values, the others the
+        // upwind level's quadratic face value (grad_z_quadratic, bounded)
+        F2(Lin.data(), kb, iw) += Lupw[kb - 1];
+        F2(Lin.data(), mza, iw) += Lupw[mza];
+        for (int k = kb; k <= mza - 1; ++k) {
+          if (F2(wm, k, iw) < (T)0) Lb[k + 1] += Lupw[k];
+          else Lt[k] += Lupw[k];
+        }
+        for (int k = kb; k <= mza; ++k) {
+          F2(Lin.data(), k, iw) += Lb[k] + Lt[k];
+          Lds[k] += Lb[k] * G.aw(G.a_w, k, 1, 1) + Lt[k] * G.aw(G.a_w, k, 1, 2);
+          Lds[k - 1] += Lb[k] * G.aw(G.a_w, k, 2, 1) + Lt[k] * G.aw(G.a_w, k, 2, 2);
+        }
+        for (int k = kb; k <= mza - 1; ++k) {   // ds(k) = s(k+1) - s(k)
+          F2(Lin.data(), k + 1, iw) += Lds[k];
+          F2(Lin.data(), k, iw) -= Lds[k];
+        }
+      }
+      // scalar_v_column: upv = side value of the upwind side
+      const std::vector<T>& xx = G.xx0_v;
+      const std::vector<T>& xy = G.xy0_v;
+      const std::vector<T>& yy = G.yy0_v;
+      for (int j = 0; j < g->nv_wadj; ++j) {
+        const int iv = g->jtv_wadj[j];
+        for (int k = G.lpv(iv); k <= mza; ++k) {
+          const T a = F2(Lupv.data(), k, iv);
+          if (a == (T)0) continue;
+          const int s = F2(vm, k, iv) < (T)0 ? 2 : 1;
+          const int iws = G.v_iw(iv, s);
+          const size_t x = (size_t)(iws - 1) * mza + k - 1;
+          Lin[x] += a;
+          Lg[x] += G.v2(G.dxps, s, iv) * a;
+          Lg[plane + x] += G.v2(G.dyps, s, iv) * a;
+          if (iorder == 3) {
+            Lg[2 * plane + x] += G.v2(xx, s, iv) * a;
+            Lg[3 * plane + x] += G.v2(xy, s, iv) * a;
+            Lg[4 * plane + x] += G.v2(yy, s, iv) * a;
+          }
+        }
+      }
+      // grad_t2d[_quadratic]: g_m(iw) = sum_n c_m(n) (s(iwn) - s(iw))
+      for (int j = 0; j < g->nw_prog; ++j) {
+        const int iw = g->jtw_prog[j];
+        for (int nn = 1; nn <= G.npoly(iw); ++nn) {
+          const int iwn = G.w_iw(iw, nn), ivn = G.w_iv(iw, nn);
+          T c[5];
+          if (iorder == 2) { c[0] = G.gxps_coef(nn, iw); c[1] = G.gyps_coef(nn, iw); }
+          else for (int m = 0; m < 5; ++m) c[m] = G.xyh(G.xy_h, m + 1, nn, iw);
+          for (int k = G.lpv(ivn); k <= mza; ++k) {
+            const size_t x = (size_t)(iw - 1) * mza + k - 1;
+            T t = 0;
+            for (int m = 0; m < np2d; ++m) t += c[m] * Lg[m * plane + x];
+            F2(Lin.data(), k, iwn) += t;
+            Lin[x] -= t;
+          }
+        }
+      }
+      L.swap(Lin);   // the adjoint of this stage's input, the previous stage's output
+    }
+    for (size_t i = 0; i < plane; ++i) lam[i] = L[i] + L0[i];
+  }
+  return OLAMGPU_OK;
+}
+
 }  // namespace oracle
 
 extern "C" {
@@ -826,6 +1025,24 @@ int oracle_scalar_transport_rk_f64(const olamgpu_grid* g, const olamgpu_opts* o,
                                    olamgpu_cfl_diag* diag) {
   return oracle::scalar_transport_rk<double>(g, o, nscal, scp, sct, pdef, sgsmix, vmasc, wmasc, rho,
                                              rho_old, wc, akhodx, khtopv, ff_out, diag);
+}
+
+}
+
+extern "C" {
+
+int oracle_scalar_transport_rk_adjoint_f32(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
+                                           float* const* lam, float* const* lsct, const float* vmasc,
+                                           const float* wmasc, const double* rho, const float* rho_old,
+                                           const float* wc) {
+  return oracle::scalar_transport_rk_adjoint<float>(g, o, nscal, lam, lsct, vmasc, wmasc, rho, rho_old, wc);
+}
+
+int oracle_scalar_transport_rk_adjoint_f64(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
+                                           double* const* lam, double* const* lsct, const float* vmasc,
+                                           const float* wmasc, const double* rho, const float* rho_old,
+                                           const float* wc) {
+  return oracle::scalar_transport_rk_adjoint<double>(g, o, nscal, lam, lsct, vmasc, wmasc, rho, rho_old, wc);
 }
 
 }

@@ -158,3 +158,38 @@ def dyn_arrays(g, ds):
                 vye=ds.vye, vze=ds.vze, vmc=ds.vmc, vc=ds.vc, vmasc=z(g.mva), wmasc=z(g.mwa),
                 alpha_press=ds.alpha_press, pwfac=ds.pwfac, pvfac=ds.pvfac, thilt=z(g.mwa),
                 vmxet=z(g.mwa), vmyet=z(g.mwa), vmzet=z(g.mwa), vmt=z(g.mva))
+
+
+def _adj_lib():
+    L = lib()
+    if not hasattr(L, "_adj_ready"):
+        for name, t in (("oracle_scalar_transport_rk_adjoint_f32", C.c_float),
+                        ("oracle_scalar_transport_rk_adjoint_f64", C.c_double)):
+            f = getattr(L, name)
+            f.restype = C.c_int
+            f.argtypes = [C.POINTER(abi.Grid), C.POINTER(abi.Opts), C.c_int,
+                          C.POINTER(C.POINTER(t)), C.POINTER(C.POINTER(t)),
+                          abi.c_float_p, abi.c_float_p, abi.c_double_p, abi.c_float_p, abi.c_float_p]
+        L._adj_ready = True
+    return L
+
+
+def scalar_transport_adjoint(fg, opts, lam, st, fp64=False):
+    """The oracle's adjoint of one unlimited scalar_transport_rk step.
+
+    lam: (ntr, mwa, mza) adjoint of the new tracers.  Returns (adjoint of the
+    old tracers, adjoint of the tendencies sct), same shape."""
+    dt = np.float64 if fp64 else np.float32
+    ct = C.c_double if fp64 else C.c_float
+    la = [np.ascontiguousarray(x, dtype=dt).copy() for x in lam]
+    ls = [np.zeros_like(x) for x in la]
+    L = _adj_lib()
+    f = L.oracle_scalar_transport_rk_adjoint_f64 if fp64 else L.oracle_scalar_transport_rk_adjoint_f32
+    rc = f(C.byref(fg.struct), C.byref(opts), len(la), abi.ptr_array(la, ct), abi.ptr_array(ls, ct),
+           abi.ptr(np.ascontiguousarray(st.vmasc, np.float32), C.c_float),
+           abi.ptr(np.ascontiguousarray(st.wmasc, np.float32), C.c_float),
+           abi.ptr(np.ascontiguousarray(st.rho, np.float64), C.c_double),
+           abi.ptr(np.ascontiguousarray(st.rho_old, np.float32), C.c_float),
+           abi.ptr(np.ascontiguousarray(st.wc, np.float32), C.c_float))
+    assert rc == 0, f"oracle adjoint returned {rc}"
+    return np.stack(la), np.stack(ls)
