@@ -18,6 +18,9 @@ cell-updates/s = tracers x prognostic (k, iw) cells / step time.
   e2e    through the C-ABI with OLAM-style host arrays: every step uploads
          tracers, tendencies, winds and densities and downloads the tracers
   plain  the one-kernel-per-pass-per-tracer GPU form on the same data
+  adjoint  device time of one adjoint call (scalar_transport_rk_adjoint:
+         per-step records, layout transposes, reverse stages) over the
+         forward step's, the adjoint/forward time ratio of the metric
   cpu_baseline  the C++ oracle (restatement of the reference loops), OpenMP on
          all host cores, on a bounded sample of the same workload
 
@@ -57,6 +60,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-column", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     return p.parse_args()
 
@@ -345,6 +349,31 @@ def main():
         column = ws * nupd / (max_over_ranks(c0.elapsed_time(c1) / ksteps) * 1e-3)
         dev.set_transport_form(abi.TRANSPORT_FUSED)
 
+    # ---- adjoint of the step: device time of the adjoint call (its
+    # preparation, layout transposes and reverse stages; RESIDENT, so no
+    # inputs are uploaded inside it) against the forward step above
+    adjoint = None
+    if not a.no_adjoint and a.monot == 0:
+        dev.scalar_transport_rk_adjoint(var_p)          # allocates, builds records
+        torch.cuda.synchronize()
+        dev.profile(True, reset=True)
+        kadj = max(1, min(a.steps, 2))
+        for _ in range(kadj):
+            dev.scalar_transport_rk_adjoint(var_p)
+        aprof = dev.profile_read()
+        dev.profile(False, reset=True)
+        adj_ms = max_over_ranks(aprof["adjoint"][0] / aprof["adjoint"][1])
+        st_ms, st_n = aprof.get("adj_stage", (0.0, 0))
+        stage_bytes = (a.ntr * 24 + 96) * (g.mwa - 1) * (g.mza - 1)
+        adjoint = {
+            "ms_per_step": adj_ms, "forward_ms_per_step": ms_step,
+            "adjoint_over_forward": adj_ms / ms_step,
+            "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in aprof.items()},
+            "stage_kernel": "k_tile_adj",
+            "stage_algorithmic_bytes": stage_bytes,
+            "stage_achieved_gbs": (stage_bytes / ((st_ms / st_n) * 1e-3) / 1e9) if st_n else None,
+        }
+
     # ---- end to end through the C-ABI with host arrays
     dev.sync_to_host(abi.F_SCALARS)
     dev.set_coherence(abi.SYNC_EACH_CALL)
@@ -389,6 +418,7 @@ def main():
             "fused_over_plain": (value / plain) if plain else None,
             "fused_column_value": column,
             "e2e": e2e,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -226,6 +226,17 @@ int olamgpu_set_transport_form(int form);
  * diag (optional) receives the check_cfls maxima. */
 int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag);
 
+/* Adjoint of one scalar_transport_rk step (scalar_transport_rk.F90:30-615)
+ * for every registered tracer, with the winds, densities and implicit
+ * fractions of the step fixed: the unlimited step (iscal_monot = 0, no
+ * horizontal diffusion) maps (scp, sct) linearly to the new scp, and this
+ * applies its transpose.  lam[n] (mza,mwa) holds dJ/d(new scp) of tracer n
+ * on entry and dJ/d(old scp) on return; lam_sct[n] receives dJ/d(sct).
+ * rho_old and the registered vmasc / wmasc / rho are those of the forward
+ * step.  No counterpart in the reference (OLAM has no adjoint); grids with
+ * terrain, iscal_monot > 0 and tracer diffusion get OLAMGPU_E_UNSUPPORTED. */
+int olamgpu_scalar_transport_rk_adjoint(const float* rho_old, float* const* lam, float* const* lam_sct);
+
 /* Replaces prog_wrtv_rk() (prog_wrtv_rk.f90:58-488); istp is mem_ijtabs%istp. */
 int olamgpu_prog_wrtv_rk(int istp);
 

@@ -47,8 +47,8 @@ static std::vector<cudaEvent_t> g_prof_pool;
 static std::vector<std::string> g_prof_names;
 static std::vector<double> g_prof_ms;
 static std::vector<unsigned long long> g_prof_cnt;
-static std::string g_prof_open;
-static cudaEvent_t g_prof_open_ev = nullptr;
+// open scopes, innermost last (scopes nest: a step's scope holds its kernels')
+static std::vector<std::pair<std::string, cudaEvent_t>> g_prof_open;
 
 static cudaEvent_t prof_event() {
   if (!g_prof_pool.empty()) { cudaEvent_t e = g_prof_pool.back(); g_prof_pool.pop_back(); return e; }
@@ -59,17 +59,17 @@ static cudaEvent_t prof_event() {
 
 void prof_begin(const char* name, cudaStream_t s) {
   if (!g_prof_on) return;
-  g_prof_open = name;
-  g_prof_open_ev = prof_event();
-  cudaEventRecord(g_prof_open_ev, s);
+  cudaEvent_t a = prof_event();
+  cudaEventRecord(a, s);
+  g_prof_open.push_back({name, a});
 }
 
 void prof_end(cudaStream_t s) {
-  if (!g_prof_on || !g_prof_open_ev) return;
+  if (!g_prof_on || g_prof_open.empty()) return;
   cudaEvent_t b = prof_event();
   cudaEventRecord(b, s);
-  g_prof_pending.push_back({g_prof_open, g_prof_open_ev, b});
-  g_prof_open_ev = nullptr;
+  g_prof_pending.push_back({g_prof_open.back().first, g_prof_open.back().second, b});
+  g_prof_open.pop_back();
 }
 
 static void prof_resolve() {
@@ -122,7 +122,7 @@ static void release_all() {
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
                        &d.w_nb, &d.w_ev, &d.w_im, &d.v_iw, &d.v_im, &d.m_iv, &d.m_iw, &d.m_im,
                        &d.lpw, &d.lpv, &d.lpm, &d.iwglobe, &d.w_nonprog, &d.colrec,
-                       &d.tile_hdr, &d.tile_u, &d.tile_tc};
+                       &d.tile_hdr, &d.tile_u, &d.tile_tc, &d.tile_rev};
   for (auto* b : ib) b->release();
   DevBuf<float>* fb[] = {&d.w_dirv, &d.gxc, &d.gyc, &d.xy_h, &d.xy_hu, &d.dxps, &d.dyps, &d.xx0_v,
                          &d.xy0_v, &d.yy0_v, &d.xx0_vu, &d.xy0_vu, &d.yy0_vu, &d.a_w, &d.a_wu,
@@ -146,7 +146,9 @@ static void release_all() {
   Transport& tp = C.tp;
   DevBuf<float>* tb[] = {&tp.vmasc, &tp.wmasc, &tp.rho_old, &tp.wc, &tp.rhos, &tp.ff, &tp.imp_b,
                          &tp.cfl_red, &tp.gx, &tp.upv, &tp.hiv, &tp.sfv, &tp.scale, &tp.upw,
-                         &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx};
+                         &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx,
+                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.adj_wrec,
+                         &tp.adj_planes};
   for (auto* b : tb) b->release();
   tp.rho.release();
   tp.imp_list.release();
@@ -154,6 +156,7 @@ static void release_all() {
   tp.cfl_loc.release();
   tp.d_mode.release();
   tp.khtopv.release();
+  tp.adj_ptab.release();
   tp.have_turb = false;
   dyn_release();
   C.status.release();
@@ -372,6 +375,15 @@ int olamgpu_sync_to_host(unsigned fieldmask) {
 
 int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag) {
   int rc = transport_run(rho_old, diag);
+  if (rc == OLAMGPU_OK) {
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) { set_error(std::string("kernel launch: ") + cudaGetErrorString(e)); return OLAMGPU_E_CUDA; }
+  }
+  return rc;
+}
+
+int olamgpu_scalar_transport_rk_adjoint(const float* rho_old, float* const* lam, float* const* lam_sct) {
+  int rc = transport_adjoint_run(rho_old, lam, lam_sct);
   if (rc == OLAMGPU_OK) {
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) { set_error(std::string("kernel launch: ") + cudaGetErrorString(e)); return OLAMGPU_E_CUDA; }

@@ -976,8 +976,13 @@ int dyn_tend0(float* rho_old_host) {
   if (!C.initialised || !C.dy.ready || !C.have_state) { set_error("tend0 before init"); return OLAMGPU_E_STATE; }
   cudaStream_t s = C.stream;
   OG_CHECK(ensure_dyn_buffers(C));
-  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(dyn_state_to_device(OLAMGPU_F_RHO, s));
-  else if (!C.dy.uploaded) { OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s)); C.dy.uploaded = true; }
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
+    // the kernels write levels k >= lpw only: the rest of each array it
+    // returns keeps the caller's values
+    OG_CHECK(dyn_state_to_device(OLAMGPU_F_RHO | OLAMGPU_F_TEND | OLAMGPU_F_VMASC | OLAMGPU_F_WMASC, s));
+    if (rho_old_host)
+      OG_CUDA(cudaMemcpyAsync(C.tp.rho_old.p, rho_old_host, (size_t)C.g.mza * C.g.mwa * 4, cudaMemcpyHostToDevice, s));
+  } else if (!C.dy.uploaded) { OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s)); C.dy.uploaded = true; }
   const DynK g = dynk(C.g);
   Dyn& y = C.dy;
   Transport& tp = C.tp;

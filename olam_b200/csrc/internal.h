@@ -150,6 +150,7 @@ struct DevGrid {
   DevBuf<int> tile_u;            // (sum nU) column of each U entry
   DevBuf<int> tile_tc;           // (ntiles * tile_T, TILE_TCW) tile-cell records
   DevBuf<float> tile_a;          // (ntiles * tile_T, TILE_AW) slot weights
+  DevBuf<int> tile_rev;          // (ntiles * tile_T, TILE_NS) transposed slots
   int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_order = 0;
   std::vector<int> h_lpw;        // host copies used at set-up
 };
@@ -175,6 +176,12 @@ struct DevGrid {
 // in (upwind face value) - S(cell).  The order-2 or order-3 reconstruction
 // (gradient coefficients times face offsets) is folded into A at set-up.
 #define TILE_AW (6 * 2 * TILE_NS)
+// Transposed slots (TILE_NS ints per tile cell), for the adjoint: for each
+// column c that has this cell as its slot j, c's U-row byte offset | j;
+// unused entries hold the cell's own offset | TILE_NS.
+// Per-(column, level) weight record of the adjoint (TILE_WR floats): the
+// slot weights W[0..TILE_NS), SW, volti / rhos, 1 / rhos, SW - sum W.
+#define TILE_WR 24
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)
@@ -207,6 +214,10 @@ struct Transport {
   DevBuf<float> scale, upw;      // W arrays for monot/pd
   DevBuf<float> plain_out[2];    // per-tracer stage outputs of the plain form
   DevBuf<int> d_mode;            // per-tracer last-stage mode
+  // adjoint (transport_adjoint.cu): lam rotation, lam0, lams in the batched
+  // layout, per-(column, level) weight records, per-tracer planes
+  DevBuf<float> adj_l[2], adj_l0, adj_ls, adj_wrec, adj_planes;
+  DevBuf<float*> adj_ptab;
   bool flat = true;              // lpw == lpv == 2 everywhere (fused form requirement)
   DevBuf<float> akhodx;
   DevBuf<int> khtopv;
@@ -262,7 +273,7 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 // host tile tables (layouts above); T == 0 when the grid is left to the column kernel
 struct TileHost {
   int T = 0, ntiles = 0, nu_max = 0, order = 0;
-  std::vector<int> hdr, ulist, tc;
+  std::vector<int> hdr, ulist, tc, rev;
   std::vector<float> a;
 };
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th);
@@ -284,6 +295,8 @@ int check_device_status();
 
 // transport entry points (transport.cu)
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);
+// adjoint of one unlimited step (transport_adjoint.cu)
+int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* const* lam_sct);
 int tracers_to_device(cudaStream_t s);   // host -> per-tracer mirrors (-> Q)
 int tracers_to_host(cudaStream_t s);     // (Q ->) per-tracer mirrors -> host
 int ensure_q(cudaStream_t s);            // per-tracer mirrors -> Q if needed

@@ -379,6 +379,8 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
   hdr.assign((size_t)ntiles * 4, 0);
   tc.assign((size_t)ntiles * T * TILE_TCW, 0);
   am.assign((size_t)ntiles * T * TILE_AW, 0.f);
+  std::vector<int>& rv = th.rev;
+  rv.assign((size_t)ntiles * T * TILE_NS, 0);
   auto fbits = [](float f) { int i; std::memcpy(&i, &f, 4); return i; };
   std::fill(stamp.begin(), stamp.end(), -1);
   std::vector<double> acc(TILE_AW);
@@ -430,6 +432,20 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       }
       w[TILE_TC_SIDE] = side;
       for (int k = 0; k < TILE_AW; ++k) a[k] = (float)acc[k];
+      // transposed slots: the cells that have c as a slot are c's own slot
+      // cells (the relation "within two rings" is symmetric)
+      int* r = &rv[((size_t)t * T + i) * TILE_NS];
+      const std::vector<int> mine = slots;
+      for (int e = 0; e < TILE_NS; ++e) r[e] = i * 256 + TILE_NS;
+      for (int e = 0; e < (int)mine.size(); ++e) {
+        const int x = mine[e];
+        cell_slots(x);
+        int jx = -1;
+        for (int j = 0; j < (int)slots.size(); ++j) if (slots[j] == c) jx = j;
+        if (jx < 0) { th = TileHost(); return; }   // not symmetric: leave the grid to the column kernel
+        r[e] = loc[x] * 256 + jx;
+      }
+      slots = mine;
     }
   }
   th.T = T;
@@ -447,6 +463,7 @@ int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
   OG_CHECK(upload(d.tile_hdr, th.hdr.data(), th.hdr.size(), s));
   OG_CHECK(upload(d.tile_u, th.ulist.data(), th.ulist.size(), s));
   OG_CHECK(upload(d.tile_a, th.a.data(), th.a.size(), s));
+  OG_CHECK(upload(d.tile_rev, th.rev.data(), th.rev.size(), s));
   OG_CHECK(upload(d.tile_tc, th.tc.data(), th.tc.size(), s));
   OG_CUDA(cudaStreamSynchronize(s));
   d.tile_T = th.T;

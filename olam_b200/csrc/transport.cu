@@ -125,38 +125,17 @@ static void passes_stage(Context& C, CTView in, CTView scp0, CTView sct, TView o
   }
 }
 
-int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
-  Context& C = ctx();
-  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
-  if (!C.have_state || !C.hstate.vmasc || !C.hstate.wmasc || !C.hstate.rho) {
-    set_error("state arrays vmasc/wmasc/rho were not registered at init");
-    return OLAMGPU_E_STATE;
-  }
-  if (C.tr.n <= 0) return OLAMGPU_OK;  // num_scalar = 0: the loop body never runs
+// Inputs and per-step coefficients shared by the transport and its adjoint:
+// winds and densities on the device (uploaded in SYNC_EACH_CALL mode, or on
+// first use in RESIDENT mode), then check_cfls (ff_implic and the CFL
+// maxima), the stage densities rhos and the implicit columns' factors.
+int transport_prepare(Context& C, const float* rho_old_host, bool upload_tracers, float dtlr[3]) {
   const DevGrid& d = C.g;
   Transport& tp = C.tp;
-  Tracers& tr = C.tr;
   cudaStream_t s = C.stream;
   const int mza = d.mza, mwa = d.mwa, mva = d.mva;
   const int nrk = C.opts.nrk_scal;
-  const int order = C.opts.scal_horiz_adv_order;
   const size_t wz = (size_t)mza * mwa, vz = (size_t)mza * mva;
-  if (nrk != 2 && nrk != 3) { set_error("scalar_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
-  if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
-  if (C.opts.iscal_monot < 0 || C.opts.iscal_monot > 2) { set_error("iscal_monot must be 0, 1 or 2"); return OLAMGPU_E_UNSUPPORTED; }
-  const bool batched = C.form != OLAMGPU_TRANSPORT_PLAIN;
-  const bool tiled = C.form == OLAMGPU_TRANSPORT_FUSED && tile_stage_available(d, tp, order);
-  if (batched && !tp.flat) {
-    set_error("the fused transport form needs lpw = lpv = 2 (no terrain); use the plain form");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
-  if (batched && !tiled && (double)mwa * mza * (double)((tr.ntp + 3) / 4 * 2) >= 4294967296.0) {
-    set_error("the fused transport form needs mwa * mza * ntp / 2 < 2^32; use the plain form");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
-  if (batched && !tiled && d.ew_order != order)
-    OG_CHECK(build_fused_weights(&C.hgrid, C.g, order, s));
-
   // ---- inputs
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
     if (!rho_old_host) { set_error("rho_old is NULL"); return OLAMGPU_E_ARG; }
@@ -165,7 +144,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     OG_CHECK(upload(tp.rho, C.hstate.rho, wz, s));
     if (C.hstate.wc) OG_CHECK(upload(tp.wc, C.hstate.wc, wz, s));
     OG_CHECK(upload(tp.rho_old, rho_old_host, wz, s));
-    OG_CHECK(tracers_to_device(s));
+    if (upload_tracers) OG_CHECK(tracers_to_device(s));
   } else {
     // RESIDENT: device copies persist; a field never uploaded is taken from
     // the registered host array on first use (the dynamics keeps them when
@@ -197,12 +176,48 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
 
   const float dtl = (float)C.opts.dtlm;
   const float one3 = 1.f / 3.f;
-  float dtlr[3];
   for (int n = 0; n < nrk; ++n) dtlr[n] = dtl * (nrk == 3 ? (n == 0 ? one3 : (n == 1 ? 0.5f : 1.0f))
                                                           : (n == 0 ? 0.5f : 1.0f));
   { OG_PROF("check_cfls", s); launch_check_cfls(d, tp, nrk, dtl, tp.cfl_loc.p, s); }
   { OG_PROF("rhos", s); launch_rhos(d, tp, nrk, s); }
   { OG_PROF("implicit_prep", s); launch_implicit_prep(d, tp, nrk, dtlr, s); }
+  return OLAMGPU_OK;
+}
+
+int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (!C.have_state || !C.hstate.vmasc || !C.hstate.wmasc || !C.hstate.rho) {
+    set_error("state arrays vmasc/wmasc/rho were not registered at init");
+    return OLAMGPU_E_STATE;
+  }
+  if (C.tr.n <= 0) return OLAMGPU_OK;  // num_scalar = 0: the loop body never runs
+  const DevGrid& d = C.g;
+  Transport& tp = C.tp;
+  Tracers& tr = C.tr;
+  cudaStream_t s = C.stream;
+  const int mza = d.mza, mwa = d.mwa, mva = d.mva;
+  const int nrk = C.opts.nrk_scal;
+  const int order = C.opts.scal_horiz_adv_order;
+  const size_t wz = (size_t)mza * mwa;
+  if (nrk != 2 && nrk != 3) { set_error("scalar_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  if (C.opts.iscal_monot < 0 || C.opts.iscal_monot > 2) { set_error("iscal_monot must be 0, 1 or 2"); return OLAMGPU_E_UNSUPPORTED; }
+  const bool batched = C.form != OLAMGPU_TRANSPORT_PLAIN;
+  const bool tiled = C.form == OLAMGPU_TRANSPORT_FUSED && tile_stage_available(d, tp, order);
+  if (batched && !tp.flat) {
+    set_error("the fused transport form needs lpw = lpv = 2 (no terrain); use the plain form");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  if (batched && !tiled && (double)mwa * mza * (double)((tr.ntp + 3) / 4 * 2) >= 4294967296.0) {
+    set_error("the fused transport form needs mwa * mza * ntp / 2 < 2^32; use the plain form");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  if (batched && !tiled && d.ew_order != order)
+    OG_CHECK(build_fused_weights(&C.hgrid, C.g, order, s));
+
+  float dtlr[3];
+  OG_CHECK(transport_prepare(C, rho_old_host, true, dtlr));
   const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * wz;
 
   // last-stage mode per tracer

@@ -87,4 +87,8 @@ void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t n
 void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npts_k,
                       cudaStream_t s);
 
+// inputs and per-step coefficients shared by the transport and its adjoint
+// (transport.cu): uploads, check_cfls, rhos, implicit factors; dtlr per stage
+int transport_prepare(Context& C, const float* rho_old_host, bool upload_tracers, float dtlr[3]);
+
 }  // namespace olamgpu

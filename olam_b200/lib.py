@@ -26,6 +26,7 @@ EXPORTS = [
     "olamgpu_set_transport_form", "olamgpu_scalar_transport_rk", "olamgpu_prog_wrtv_rk",
     "olamgpu_tend0", "olamgpu_timeavg_momsc", "olamgpu_stream", "olamgpu_launch_count",
     "olamgpu_profile", "olamgpu_profile_read", "olamgpu_update_scalar_noalloc",
+    "olamgpu_scalar_transport_rk_adjoint",
 ]
 
 
@@ -65,6 +66,8 @@ def load():
     lib.olamgpu_profile_read.argtypes = [C.c_int, C.c_char_p, C.POINTER(C.c_double),
                                          C.POINTER(C.c_ulonglong)]
     lib.olamgpu_update_scalar_noalloc.argtypes = [C.c_void_p] * 6 + [C.c_float, C.c_void_p, C.c_void_p]
+    lib.olamgpu_scalar_transport_rk_adjoint.argtypes = [abi.c_float_p, C.POINTER(abi.c_float_p),
+                                                        C.POINTER(abi.c_float_p)]
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
             getattr(lib, name).restype = C.c_int
@@ -131,6 +134,18 @@ class OlamGpu:
         check(self.lib.olamgpu_scalar_transport_rk(abi.ptr(rp, C.c_float), C.byref(diag)
                                                    if want_diag else None))
         return diag if want_diag else None
+
+    def scalar_transport_rk_adjoint(self, lam, rho_old=None):
+        """Adjoint of one unlimited step: lam is a list of (mwa, mza)
+        float32 arrays of dJ/d(new scp) per registered tracer; returns
+        (dJ/d(old scp), dJ/d(sct)) as lists of new arrays of that shape."""
+        lam_io = [np.array(x, dtype=np.float32, order="C", copy=True) for x in lam]
+        lsct = [np.zeros_like(x) for x in lam_io]
+        lp = abi.ptr_array(lam_io, C.c_float)
+        sp = abi.ptr_array(lsct, C.c_float)
+        rp = None if rho_old is None else np.ascontiguousarray(rho_old, dtype=np.float32)
+        check(self.lib.olamgpu_scalar_transport_rk_adjoint(abi.ptr(rp, C.c_float), lp, sp))
+        return lam_io, lsct
 
     def prog_wrtv_rk(self, istp=1):
         check(self.lib.olamgpu_prog_wrtv_rk(int(istp)))

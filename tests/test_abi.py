@@ -44,6 +44,7 @@ def test_strerror_and_state_errors():
     assert L.olamgpu_set_coherence(7) == abi.E_ARG
     assert L.olamgpu_update_scalar_noalloc(None, None, None, None, None, None, C.c_float(1.0),
                                            None, None) == abi.E_STATE
+    assert L.olamgpu_scalar_transport_rk_adjoint(None, None, None) == abi.E_STATE
 
 
 def test_null_arguments_rejected():
