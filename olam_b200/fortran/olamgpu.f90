@@ -102,6 +102,14 @@ module olamgpu_c
        real(c_float), intent(in) :: rho_old(*)
        type(c_ptr), value :: diag
      end function
+     ! lam(n) / lam_sct(n): c_loc of tracer n's (mza,mwa) adjoint arrays
+     integer(c_int) function olamgpu_scalar_transport_rk_adjoint(rho_old, lam, lam_sct) &
+          bind(C, name="olamgpu_scalar_transport_rk_adjoint")
+       import :: c_int, c_float, c_ptr
+       real(c_float), intent(in) :: rho_old(*)
+       type(c_ptr), intent(in) :: lam(*)
+       type(c_ptr), intent(in) :: lam_sct(*)
+     end function
      integer(c_int) function olamgpu_prog_wrtv_rk(istp) bind(C, name="olamgpu_prog_wrtv_rk")
        import :: c_int
        integer(c_int), value :: istp
