@@ -179,9 +179,10 @@ struct DevGrid {
 // Transposed slots (TILE_NS ints per tile cell), for the adjoint: for each
 // column c that has this cell as its slot j, c's U-row byte offset | j;
 // unused entries hold the cell's own offset | TILE_NS.
-// Per-(column, level) weight record of the adjoint (TILE_WR floats): the
-// slot weights W[0..TILE_NS), SW, volti / rhos, 1 / rhos, SW - sum W.
-#define TILE_WR 24
+// Per-(column, level) weight record of a long step (TILE_WR floats, read by
+// the stage kernel and the adjoint): the slot weights W[0..TILE_NS), SW,
+// volti / rhos, 1 / rhos, SW - sum W, wmasc(kd-1), wmasc(kd), 0, 0.
+#define TILE_WR 28
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)
@@ -214,9 +215,10 @@ struct Transport {
   DevBuf<float> scale, upw;      // W arrays for monot/pd
   DevBuf<float> plain_out[2];    // per-tracer stage outputs of the plain form
   DevBuf<int> d_mode;            // per-tracer last-stage mode
+  DevBuf<float> wrec;            // (mwa, mza, TILE_WR) weight records of the step
   // adjoint (transport_adjoint.cu): lam rotation, lam0, lams in the batched
-  // layout, per-(column, level) weight records, per-tracer planes
-  DevBuf<float> adj_l[2], adj_l0, adj_ls, adj_wrec, adj_planes;
+  // layout, per-tracer planes
+  DevBuf<float> adj_l[2], adj_l0, adj_ls, adj_planes;
   DevBuf<float*> adj_ptab;
   bool flat = true;              // lpw == lpv == 2 everywhere (fused form requirement)
   DevBuf<float> akhodx;
@@ -278,7 +280,7 @@ struct TileHost {
 };
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th);
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
-size_t tile_smem_bytes(int T, int nu_max);
+size_t tile_smem_bytes(int T, int nu_max, int mza);
 
 // dynamics entry points (dynamics.cu)
 int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s);

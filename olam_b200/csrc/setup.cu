@@ -285,12 +285,13 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 
 // ---- tiles of the tiled fused kernel ------------------------------------------
 
-size_t tile_smem_bytes(int T, int nu) {
+size_t tile_smem_bytes(int T, int nu, int mza) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  // reserved, U rows, scp0/sct rows, tile-cell records, slot weights A, the
-  // level's slot weights W, per-level values, U columns, a_w
-  return 16 + al((size_t)nu * 256) + al((size_t)T * 2 * 256) + al((size_t)T * TILE_TCW * 4) +
-         al((size_t)T * TILE_AW * 4) + al((size_t)T * 24 * 4) + al((size_t)T * 12 * 4) + al((size_t)nu * 4) + 64;
+  // k_tile's layout: two level buffers of U rows and of the tile columns'
+  // weight records, the U rows' global offsets, slot offsets, tile columns,
+  // explicit fractions, a_w of every level
+  return 2 * al((size_t)nu * 256) + 2 * al((size_t)T * TILE_WR * 4) + al((size_t)nu * 8) +
+         al((size_t)T * TILE_NS * 4) + 2 * al((size_t)T * 4) + (size_t)4 * mza * 4;
 }
 
 // Two blocks per SM: 228 KB of shared memory less 1 KB reserved per block.
@@ -355,8 +356,8 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
   };
   int T = 0, numax = 0;
-  // multiples of the 16 half-warps of a block, so every warp gets the same work
-  const int cand[] = {64, 48, 32, 16};
+  // one or two columns for each of the 16 half-warps of a block
+  const int cand[] = {32, 16};
   for (int Tc : cand) {
     std::fill(stamp.begin(), stamp.end(), -1);
     const int nt = (nprog + Tc - 1) / Tc;
@@ -365,7 +366,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       gather(t, Tc);
       nu = std::max(nu, (int)U.size());
     }
-    if (nu <= 65535 && tile_smem_bytes(Tc, nu) <= TILE_SMEM_MAX) {
+    if (nu <= 65535 && tile_smem_bytes(Tc, nu, g->mza) <= TILE_SMEM_MAX) {
       T = Tc; numax = nu;
       break;
     }

@@ -241,6 +241,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     if (tp.have_turb)
       for (int n = 0; n < tr.n; ++n)
         if (tr.sgsmix[n]) launch_diffusion(d, tp, CTView{A, ntp, n}, TView{T, ntp, n}, 1, s);
+    if (tiled) { OG_PROF("tile_weights", s); OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s)); }
     int in_b = a, out_b = (a + 1) % 3;
     for (int istage = 1; istage <= nrk; ++istage) {
       const float dtr = dtlr[istage - 1];
@@ -262,7 +263,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
         }
       } else {
         OG_PROF(tiled ? (istage == 1 ? "tile_stage1" : "tile_stage") : (istage == 1 ? "fused_stage1" : "fused_stage"), s);
-        if (tiled) OG_CHECK(launch_tile_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, C.status.p, s));
+        if (tiled) OG_CHECK(launch_tile_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, C.status.p, s));
         else launch_fused_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, s);
       }
       { OG_PROF("implicit_solve", s); launch_implicit_solve(d, tp, nrk, istage, dtr, CTView{A, ntp, 0}, TView{OUT, ntp, 0}, ntp, s); }

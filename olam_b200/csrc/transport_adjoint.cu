@@ -4,9 +4,9 @@
 //
 // With the winds and densities fixed the step maps (scp, sct) linearly to
 // the new scp; the adjoint applies the transpose, stage by stage in reverse:
-//   k_adj_weights   the per-(column, level) record of the forward's slot
-//                   weights W (the same folded reconstruction as k_tile),
-//                   SW, volti / rhos, 1 / rhos and SW - sum W, once per step
+//   k_weights       (transport_tile.cu) the per-(column, level) records of
+//                   the forward's slot weights W, SW, volti / rhos, 1 / rhos
+//                   and SW - sum W, once per step
 //   k_adj_fold0     the forward copies level kb to the levels below it
 //   k_adj_implicit  transpose of the implicit columns' tridif_fini solve
 //   k_tile_adj      transpose of update_scalar per tile: for each column x,
@@ -18,58 +18,6 @@
 #include "transport_kernels.cuh"
 
 namespace olamgpu {
-
-// ---- per-(column, level) weight records -------------------------------------
-struct AdjW {
-  int mza, T, nrk;
-  const int4* __restrict__ hdr;
-  const int* __restrict__ tc;
-  const float* __restrict__ amat;
-  const float* __restrict__ vmasc;
-  const float* __restrict__ volti;
-  const float* __restrict__ rhos;   // rhos(:,:,nrk)
-  float* __restrict__ wrec;         // (mwa, mza, TILE_WR)
-};
-
-// one block per tile column, a thread per level
-__global__ void k_adj_weights(AdjW A) {
-  __shared__ int w[TILE_TCW];
-  __shared__ float am[TILE_AW];
-  const int t = blockIdx.x / A.T, i = blockIdx.x - t * A.T;
-  if (i >= A.hdr[t].w) return;   // padding of the last tile (uniform per block)
-  const size_t r = (size_t)blockIdx.x;
-  for (int q = threadIdx.x; q < TILE_TCW; q += blockDim.x) w[q] = __ldg(A.tc + r * TILE_TCW + q);
-  for (int q = threadIdx.x; q < TILE_AW; q += blockDim.x) am[q] = __ldg(A.amat + r * TILE_AW + q);
-  __syncthreads();
-  const int iw = w[TILE_TC_IW], np = w[TILE_TC_NP], side = w[TILE_TC_SIDE];
-  for (int kd = 1 + threadIdx.x; kd < A.mza; kd += blockDim.x) {
-    float dvvm[6];
-    int up[6];
-    float sw = 0.f;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      const float vm = f < np ? __ldg(A.vmasc + (size_t)w[TILE_TC_EV + f] * A.mza + kd) : 0.f;
-      dvvm[f] = __int_as_float(w[TILE_TC_DV + f]) * vm;
-      up[f] = ((vm < 0.f ? 1 : 0) != ((side >> f) & 1)) ? 1 : 0;
-      sw = fmaf(__int_as_float(w[TILE_TC_DV + f]), vm, sw);
-    }
-    float* o = A.wrec + ((size_t)iw * A.mza + kd) * TILE_WR;
-    float sumw = 0.f;
-    for (int j = 0; j < TILE_NS; ++j) {
-      float acc = 0.f;
-#pragma unroll
-      for (int f = 0; f < 6; ++f) acc = fmaf(dvvm[f], am[(f * 2 + up[f]) * TILE_NS + j], acc);
-      o[j] = acc;
-      sumw += acc;
-    }
-    const size_t x = (size_t)iw * A.mza + kd;
-    const float rh = __ldg(A.rhos + x);
-    o[TILE_NS] = sw;
-    o[TILE_NS + 1] = __ldg(A.volti + x) / rh;
-    o[TILE_NS + 2] = 1.0f / rh;
-    o[TILE_NS + 3] = sw - sumw;
-  }
-}
 
 // columns outside jtw_prog keep their values through the step: their
 // adjoint passes straight to lam0; lam0 and lams start at zero elsewhere
@@ -367,7 +315,7 @@ static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L
   A.dtr = dtr;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   A.ulist = d.tile_u.p; A.tc = d.tile_tc.p; A.rev = d.tile_rev.p;
-  A.a_w = d.a_w.p; A.wmasc = tp.wmasc.p; A.ff = tp.ff.p; A.wrec = tp.adj_wrec.p;
+  A.a_w = d.a_w.p; A.wmasc = tp.wmasc.p; A.ff = tp.ff.p; A.wrec = tp.wrec.p;
   A.L = L; A.LIN = LIN; A.L0 = L0; A.LS = LS;
   A.err = status;
   const size_t smem = tile_adj_smem_bytes(d.tile_T, d.tile_nu_max);
@@ -434,10 +382,6 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   OG_CHECK(tp.adj_l0.alloc(qn));
   OG_CHECK(tp.adj_ls.alloc(qn));
   OG_CHECK(tp.adj_planes.alloc(plane * n));
-  if (tp.adj_wrec.n != plane * TILE_WR) {
-    OG_CHECK(tp.adj_wrec.alloc(plane * TILE_WR));
-    OG_CUDA(cudaMemsetAsync(tp.adj_wrec.p, 0, tp.adj_wrec.bytes(), s));
-  }
   OG_CHECK(planes_table(tp, n, plane, s));
   for (int i = 0; i < n; ++i)
     OG_CUDA(cudaMemcpyAsync(tp.adj_planes.p + (size_t)i * plane, lam[i], plane * sizeof(float),
@@ -453,16 +397,7 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
     OG_CHECK(transport_prepare(C, rho_old_host, false, dtlr));
     const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * plane;
     { OG_PROF("adj_gather", s); launch_gather_q(tp.adj_l[0].p, (const float* const*)tp.adj_ptab.p, n, ntp, plane, s); }
-    {
-      OG_PROF("adj_weights", s);
-      AdjW W;
-      W.mza = mza; W.T = d.tile_T; W.nrk = nrk;
-      W.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
-      W.tc = d.tile_tc.p; W.amat = d.tile_a.p;
-      W.vmasc = tp.vmasc.p; W.volti = d.volti.p; W.rhos = rhos_nrk; W.wrec = tp.adj_wrec.p;
-      k_adj_weights<<<(unsigned)d.ntiles * d.tile_T, 64, 0, s>>>(W);
-      OG_LAUNCHED();
-    }
+    { OG_PROF("adj_weights", s); OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s)); }
     float* L = tp.adj_l[0].p;
     float* LIN = tp.adj_l[1].p;
     const size_t colsize = (size_t)mza * ntp;

@@ -71,11 +71,13 @@ void launch_fused_stage(const DevGrid& d, const Transport& tp, const float* S, c
                         const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr,
                         const float* rhos, cudaStream_t s);
 
-// the same update in tiles of columns (grids without terrain; transport_tile.cu)
+// the same update in tiles of columns (grids without terrain; transport_tile.cu):
+// the step's per-(column, level) weight records (into tp.wrec), then a stage
 bool tile_stage_available(const DevGrid& d, const Transport& tp, int order);
+int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cudaStream_t s);
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
-                      const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr,
-                      const float* rhos, int* status, cudaStream_t s);
+                      const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr, int* status,
+                      cudaStream_t s);
 
 // copy the columns outside jtw_prog (colsize floats each) from src to dst
 void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, size_t colsize,
