@@ -364,7 +364,7 @@ def main():
         dev.profile(False, reset=True)
         adj_ms = max_over_ranks(aprof["adjoint"][0] / aprof["adjoint"][1])
         st_ms, st_n = aprof.get("adj_stage", (0.0, 0))
-        stage_bytes = (a.ntr * 24 + 96) * (g.mwa - 1) * (g.mza - 1)
+        stage_bytes = (a.ntr * 24 + 128) * (g.mwa - 1) * (g.mza - 1)
         adjoint = {
             "ms_per_step": adj_ms, "forward_ms_per_step": ms_step,
             "adjoint_over_forward": adj_ms / ms_step,

@@ -147,7 +147,7 @@ static void release_all() {
   DevBuf<float>* tb[] = {&tp.vmasc, &tp.wmasc, &tp.rho_old, &tp.wc, &tp.rhos, &tp.ff, &tp.imp_b,
                          &tp.cfl_red, &tp.gx, &tp.upv, &tp.hiv, &tp.sfv, &tp.scale, &tp.upw,
                          &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx,
-                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec,
+                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec, &tp.adj_trec,
                          &tp.adj_planes};
   for (auto* b : tb) b->release();
   tp.rho.release();
@@ -157,6 +157,7 @@ static void release_all() {
   tp.d_mode.release();
   tp.khtopv.release();
   tp.adj_ptab.release();
+  tp.adj_ptab2.release();
   tp.have_turb = false;
   dyn_release();
   C.status.release();

@@ -152,6 +152,7 @@ struct DevGrid {
   DevBuf<float> tile_a;          // (ntiles * tile_T, TILE_AW) slot weights
   DevBuf<int> tile_rev;          // (ntiles * tile_T, TILE_NS) transposed slots
   int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_order = 0;
+  bool tile_closed = false;      // every neighbourhood column is prognosed
   std::vector<int> h_lpw;        // host copies used at set-up
 };
 
@@ -219,7 +220,8 @@ struct Transport {
   // adjoint (transport_adjoint.cu): lam rotation, lam0, lams in the batched
   // layout, per-tracer planes
   DevBuf<float> adj_l[2], adj_l0, adj_ls, adj_planes;
-  DevBuf<float*> adj_ptab;
+  DevBuf<float> adj_trec;        // (mwa, mza, 32) transposed records of the step
+  DevBuf<float*> adj_ptab, adj_ptab2;
   bool flat = true;              // lpw == lpv == 2 everywhere (fused form requirement)
   DevBuf<float> akhodx;
   DevBuf<int> khtopv;

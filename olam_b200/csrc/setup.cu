@@ -458,6 +458,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
   d.tile_T = d.ntiles = d.tile_nu_max = 0;
   d.tile_order = 0;
+  d.tile_closed = false;
   TileHost th;
   make_tiles(g, order, th);
   if (!th.T) return OLAMGPU_OK;
@@ -467,6 +468,11 @@ int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
   OG_CHECK(upload(d.tile_rev, th.rev.data(), th.rev.size(), s));
   OG_CHECK(upload(d.tile_tc, th.tc.data(), th.tc.size(), s));
   OG_CUDA(cudaStreamSynchronize(s));
+  // closed: every column of every neighbourhood is prognosed (a global
+  // domain), so the transposed slots cover every column a stage reads
+  std::vector<char> isprog(g->mwa, 0);
+  for (int j = 0; j < g->nw_prog; ++j) isprog[g->jtw_prog[j] - 1] = 1;
+  d.tile_closed = std::all_of(th.ulist.begin(), th.ulist.end(), [&](int x) { return isprog[x] != 0; });
   d.tile_T = th.T;
   d.ntiles = th.ntiles;
   d.tile_nu_max = th.nu_max;

@@ -4,30 +4,38 @@
 //
 // With the winds and densities fixed the step maps (scp, sct) linearly to
 // the new scp; the adjoint applies the transpose, stage by stage in reverse:
-//   k_weights       (transport_tile.cu) the per-(column, level) records of
-//                   the forward's slot weights W, SW, volti / rhos, 1 / rhos
-//                   and SW - sum W, once per step
-//   k_adj_fold0     the forward copies level kb to the levels below it
+//   k_weights       (transport_tile.cu) the forward's per-(column, level)
+//                   records: slot weights W, SW, volti / rhos, 1 / rhos,
+//                   SW - sum W, once per step
+//   k_adj_records   their transpose per (column x, level): for every column
+//                   c that has x as its slot j (the transposed slot table),
+//                   W_{c,j} volti_c / rhos_c; the vertical quadratic faces
+//                   transposed into coefficients on lam(kd-2 .. kd+2); the
+//                   own-column factors of lam(scp0) and lam(sct)
 //   k_adj_implicit  transpose of the implicit columns' tridif_fini solve
-//   k_tile_adj      transpose of update_scalar per tile: for each column x,
-//                   the slot weights of the columns that have x as a slot
-//                   (the transposed slot table), the vertical quadratic
-//                   faces transposed per face, and the scp0 / sct terms
-// lam0 collects the adjoint of scp0 (the stage input of every stage's s00
-// terms and the columns outside jtw_prog), lams the adjoint of sct.
+//   k_adj_fold0     the forward copies level kb to the levels below it
+//   k_tile_adj      transpose of update_scalar per tile: a gather over the
+//                   transposed slots and the column's own levels
+// lam0 collects the adjoint of scp0 (the s00 terms of every stage and the
+// columns outside jtw_prog), lams the adjoint of sct.  Neither is cleared
+// first: the first reverse stage writes them, later stages accumulate.
 #include "transport_kernels.cuh"
+#include "tile_common.cuh"
 
 namespace olamgpu {
 
-// columns outside jtw_prog keep their values through the step: their
-// adjoint passes straight to lam0; lam0 and lams start at zero elsewhere
+// Columns outside jtw_prog keep their values through the step, so their
+// adjoint passes through: the buffer the last reverse stage writes holds lam
+// there, the other lam buffer and lams hold zero.
 __global__ void k_adj_nonprog(const int* __restrict__ cols, int ncol, size_t colsize, float* __restrict__ lam,
-                              float* __restrict__ lam0) {
+                              float* __restrict__ other, float* __restrict__ lams, int final_is_other) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (size_t)ncol * colsize) return;
   const size_t x = (size_t)cols[i / colsize] * colsize + i % colsize;
-  lam0[x] = lam[x];
-  lam[x] = 0.f;
+  const float v = lam[x];
+  lams[x] = 0.f;
+  if (final_is_other) { other[x] = v; lam[x] = 0.f; }
+  else other[x] = 0.f;
 }
 
 // the forward stage copies level kb to the levels below: their adjoint folds into kb
@@ -47,11 +55,13 @@ __global__ void k_adj_fold0(const int* __restrict__ prog, int nprog, const int* 
 // tridif_fini): out' = s0 + T^-1 (out - s0 - G s0) with T = L U,
 // L(k,k) = 1/cji(k), L(k,k-1) = b1(k), U(k,k+1) = scr1(k+1).  For lam' the
 // adjoint of out': nu = T^-T lam', lam(out) = nu, lam0 += lam' - nu - G^T nu.
-// One thread per (implicit column, tracer), sequential in k.
+// One thread per (implicit column, tracer), sequential in k.  On the first
+// reverse stage (first != 0) lam0 of the column starts from zero.
 __global__ void k_adj_implicit(GridK g, const int* __restrict__ list, const int* __restrict__ count,
                                const float* __restrict__ b, const float* __restrict__ ff,
                                const float* __restrict__ wmasc, const float* __restrict__ rhos_st, int nrk,
-                               int istage, float dtr, int ntp, float* __restrict__ lam, float* __restrict__ lam0) {
+                               int istage, float dtr, int ntp, int first, float* __restrict__ lam,
+                               float* __restrict__ lam0) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = *count;
   if (i >= (size_t)n * ntp) return;
@@ -67,6 +77,8 @@ __global__ void k_adj_implicit(GridK g, const int* __restrict__ list, const int*
   float* L = lam + (size_t)iw * mza * ntp + t;
   float* L0 = lam0 + (size_t)iw * mza * ntp + t;
   auto at = [&](float* p, int kd) -> float& { return p[(size_t)kd * ntp]; };
+  if (first)
+    for (int kd = kb; kd < mza; ++kd) at(L0, kd) = 0.f;
   for (int kd = 1; kd < kb; ++kd) { at(L, kb) += at(L, kd); at(L, kd) = 0.f; }
   // U^T z = lam' (forward sweep), kept in lam
   float prev = 0.f;
@@ -98,246 +110,338 @@ __global__ void k_adj_implicit(GridK g, const int* __restrict__ list, const int*
   }
 }
 
-// ---- transpose of update_scalar over a tile -----------------------------------
-struct TileAdjArgs {
-  int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa;
-  float dtr;
+// ---- transposed records, once per step -----------------------------------------
+// Per (tile column x, level kd), TADJ_RW floats:
+//   [0, TILE_NS)   W_{c,j} volti_c / rhos_c for the e-th (c, j) with x in
+//                  c's slot j (0 for unused entries)
+//   [20, 25)       the vertical faces transposed: coefficient of
+//                  lam(kd-2+q) is dtr (fexpl a_q + (q == 2) d)
+//   25 d           volti / rhos (SW - sum W), the diagonal of the horizontal part
+//   26, 27         volti / rhos SW and volti / rhos (wmasc(kd-1) - wmasc(kd)):
+//                  lam(scp0) gains lam (1 - dtr (b26 + fexpl b27))
+//   28             1 / rhos: lam(sct) gains lam dtr / rhos
+#define TADJ_RW 32
+
+struct AdjRecArgs {
+  int mza, T, kb, mwa;
   const int4* __restrict__ hdr;
   const int* __restrict__ ulist;
   const int* __restrict__ tc;
   const int* __restrict__ rev;
-  const float* __restrict__ a_w;
-  const float* __restrict__ wmasc;
-  const float* __restrict__ ff;
   const float* __restrict__ wrec;   // (mwa, mza, TILE_WR)
+  const float* __restrict__ wmasc;
+  const float* __restrict__ a_w;    // Fortran (mza, 2, 2)
+  float* __restrict__ trec;         // (mwa, mza, TADJ_RW)
+  int* err;
+};
+
+// one block per tile column, a thread per level
+__global__ void k_adj_records(AdjRecArgs A) {
+  __shared__ int cols[TILE_NS], js[TILE_NS];
+  __shared__ int xs;
+  const int t = blockIdx.x / A.T, i = blockIdx.x - t * A.T;
+  const int4 h = A.hdr[t];
+  if (i >= h.w) return;   // padding of the last tile (uniform per block)
+  if (threadIdx.x < TILE_NS) {
+    const int v = __ldg(A.rev + (size_t)blockIdx.x * TILE_NS + threadIdx.x);
+    int uu = v >> 8, j = v & 255;
+    if ((unsigned)uu >= (unsigned)h.y || j > TILE_NS) {   // inconsistent table: record, contribute nothing
+      if (atomicCAS(A.err, 0, 121) == 0) { A.err[1] = t; A.err[2] = blockIdx.x; A.err[3] = threadIdx.x; }
+      uu = 0; j = TILE_NS;
+    }
+    int c = __ldg(A.ulist + h.x + uu);
+    if (c < 1 || c >= A.mwa) { c = 1; j = TILE_NS; }
+    cols[threadIdx.x] = c;
+    js[threadIdx.x] = j;
+  }
+  if (threadIdx.x == 0) {
+    int x = __ldg(A.tc + (size_t)blockIdx.x * TILE_TCW + TILE_TC_IW);
+    xs = (x >= 1 && x < A.mwa) ? x : 0;
+  }
+  __syncthreads();
+  const int x = xs, mza = A.mza, kb = A.kb;
+  if (x == 0) return;
+  const float* wm = A.wmasc + (size_t)x * mza;
+  auto rec = [&](int col, int k) { return A.wrec + ((size_t)col * mza + k) * TILE_WR; };
+  for (int kd = kb + threadIdx.x; kd < mza; kd += blockDim.x) {
+    float* o = A.trec + ((size_t)x * mza + kd) * TADJ_RW;
+    float v4[4];
+#pragma unroll
+    for (int e = 0; e < TILE_NS; ++e) {
+      const int j = js[e];
+      const float* rc = rec(cols[e], kd);
+      v4[e & 3] = j < TILE_NS ? __ldg(rc + j) * __ldg(rc + TILE_NS + 1) : 0.f;
+      if ((e & 3) == 3) reinterpret_cast<float4*>(o)[e >> 2] = make_float4(v4[0], v4[1], v4[2], v4[3]);
+    }
+    // faces f = kd-2 .. kd+1 (the ones whose upwind stencil can hold level
+    // kd): lam_F(f) = fexpl wm(f) (mu(f+1) - mu(f)) times dF/dS(kd)
+    float V[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int f = kd - 2 + q;
+      if (f < kb || f > mza - 2) continue;
+      const float w = __ldg(wm + f);
+      const bool neg = w < 0.f;                 // upwind level f+1 (its bottom face), else f (top)
+      const int lev = neg ? f + 1 : f;
+      const int pos = kd - (neg ? f : f - 1);   // kd's place in the stencil (lev-1, lev, lev+1)
+      const float c1 = __ldg(A.a_w + lev + (neg ? 0 : 2) * mza), c2 = __ldg(A.a_w + lev + (neg ? 1 : 3) * mza);
+      const float it = lev <= mza - 2 ? 1.f : 0.f, ib = lev >= kb + 1 ? 1.f : 0.f;
+      const float dF = pos == 0 ? -c2 * ib : (pos == 1 ? 1.f - c1 * it + c2 * ib : (pos == 2 ? c1 * it : 0.f));
+      V[q + 1] += w * dF;
+      V[q] -= w * dF;
+    }
+    if (kd == kb) V[2] += __ldg(wm + kb - 1);
+    if (kd == mza - 1) V[2] -= __ldg(wm + mza - 1);
+    const float* rx = rec(x, kd);
+    const float rv = __ldg(rx + TILE_NS + 1);
+    float a[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int k2 = kd - 2 + q;
+      a[q] = (k2 >= kb && k2 < mza) ? (q == 2 ? rv : __ldg(rec(x, k2) + TILE_NS + 1)) * V[q] : 0.f;
+    }
+    reinterpret_cast<float4*>(o)[5] = make_float4(a[0], a[1], a[2], a[3]);
+    reinterpret_cast<float4*>(o)[6] = make_float4(a[4], rv * __ldg(rx + TILE_NS + 3), rv * __ldg(rx + TILE_NS),
+                                                  rv * (__ldg(wm + kd - 1) - __ldg(wm + kd)));
+    reinterpret_cast<float4*>(o)[7] = make_float4(__ldg(rx + TILE_NS + 2), 0.f, 0.f, 0.f);
+  }
+}
+
+// ---- transpose of update_scalar over a tile -----------------------------------
+struct TileAdjArgs {
+  int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa;
+  float dtr;
+  int first, last;                  // first / last reverse stage of the step
+  const int4* __restrict__ hdr;
+  const int* __restrict__ ulist;
+  const int* __restrict__ tc;
+  const int* __restrict__ rev;
+  const float* __restrict__ ff;     // (mwa, nrk)
+  const float* __restrict__ trec;   // (mwa, mza, TADJ_RW)
   const float* __restrict__ L;      // adjoint of the stage output (batched layout)
-  float* __restrict__ LIN;          // adjoint of the stage input
-  float* __restrict__ L0;           // adjoint of scp0, accumulated
-  float* __restrict__ LS;           // adjoint of sct, accumulated
+  float* __restrict__ LIN;          // adjoint of the stage input (last stage: of the old scp)
+  float* __restrict__ L0;           // adjoint of scp0
+  float* __restrict__ LS;           // adjoint of sct
   int* err;
 };
 
 #define TADJ_THREADS 256
-#define TADJ_NW (TADJ_THREADS / 32)
-#define TADJ_CF 28   // per column and level: TILE_NS slot coefficients, 5 vertical, lam0 and sct factors
 
-__device__ __forceinline__ void cpa16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-
-struct G4 { float2 a, b; };
-__device__ __forceinline__ G4 lds_g4(const char* p) {
-  const float4 v = *reinterpret_cast<const float4*>(p);
-  return G4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
-}
-__device__ __forceinline__ G4 ldg_g4(const float* p) {
-  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-  return G4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
-}
-__device__ __forceinline__ G4 fma_g4(float w, G4 x, G4 acc) {
-  const float2 w2 = make_float2(w, w);
-  return G4{__ffma2_rn(w2, x.a, acc.a), __ffma2_rn(w2, x.b, acc.b)};
-}
-__device__ __forceinline__ void st_g4(float* p, G4 v) {
-  *reinterpret_cast<float4*>(p) = make_float4(v.a.x, v.a.y, v.b.x, v.b.y);
+size_t tile_adj_smem_bytes(int T, int nu) {
+  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+  return 2 * al((size_t)nu * 256) + 2 * al((size_t)T * TADJ_RW * 4) + al((size_t)nu * 8) +
+         al((size_t)T * TILE_NS * 4) + 2 * al((size_t)T * 4);
 }
 
+// The same sweep as k_tile: level kd+1 is copied into one buffer while kd is
+// computed from the other; a half warp owns NC columns with lam of the
+// column's levels kd-2 .. kd+3 and its lam0 / lams rows in registers.
+//   lam_in(x) = dtr (sum_e T_e lam(c_e) + sum_q (fexpl a_q + [q == 2] d) lam(kd-2+q))
+//   lam0 += lam (1 - dtr (b26 + fexpl b27)),  lams += lam dtr / rhos
+// On the first reverse stage lam0 is read only in implicit columns (the
+// implicit transpose wrote it there) and lams is not read; on the last the
+// result lam_in + lam0 is the adjoint of the old scp, written to LIN.
+template <int NC>
 __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int T = 16 * NC;
   const int tile = blockIdx.x % A.ntiles, grp = blockIdx.x / A.ntiles;
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
+  const int mza = A.mza, ntp = A.ntp, kb = A.kb;
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+  const size_t ubuf = al((size_t)A.nu_max * 256), rbuf = al((size_t)T * TADJ_RW * 4);
   unsigned char* p = smraw;
-  char* U = reinterpret_cast<char*>(p);   p += al((size_t)A.nu_max * 256);              // lam rows
-  float* WS = reinterpret_cast<float*>(p); p += al((size_t)A.nu_max * TILE_WR * 4 + 16); // weight records (+ zeros)
-  float* CF = reinterpret_cast<float*>(p); p += al((size_t)A.T * TADJ_CF * 4);
-  int* REV = reinterpret_cast<int*>(p);    p += al((size_t)A.T * TILE_NS * 4);
-  int* IWT = reinterpret_cast<int*>(p);    p += al((size_t)A.T * 4);
-  int* UIW = reinterpret_cast<int*>(p);    p += al((size_t)A.nu_max * 4);
-  float* AW = reinterpret_cast<float*>(p);  // a_w at levels kd-2 .. kd+2 (4 each)
+  char* UB = reinterpret_cast<char*>(p);              p += 2 * ubuf;
+  unsigned char* RBB = p;                             p += 2 * rbuf;
+  long long* ROW = reinterpret_cast<long long*>(p);   p += al((size_t)A.nu_max * 8);
+  int* REVO = reinterpret_cast<int*>(p);              p += al((size_t)T * TILE_NS * 4);
+  int* IWT = reinterpret_cast<int*>(p);               p += al((size_t)T * 4);
+  float* FEX = reinterpret_cast<float*>(p);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int t0 = grp * 64;
 
-  int bad = (nU > A.nu_max || nT > A.T || nT > nU) ? 1 : 0;
+  int bad = (nU > A.nu_max || nT > T || nT > nU || A.T != T) ? 1 : 0;
   if (!bad) {
     for (int i = tid; i < nT * TILE_NS; i += TADJ_THREADS) {
-      const int v = __ldg(A.rev + (size_t)tile * A.T * TILE_NS + i);
+      const int v = __ldg(A.rev + (size_t)tile * T * TILE_NS + i);
       if ((unsigned)(v >> 8) >= (unsigned)nU || (v & 255) > TILE_NS) bad = 11;
-      REV[i] = v;
+      REVO[i] = (v >> 8) * 256;
     }
     for (int i = tid; i < nT; i += TADJ_THREADS) {
-      const int v = __ldg(A.tc + ((size_t)tile * A.T + i) * TILE_TCW + TILE_TC_IW);
+      const int v = __ldg(A.tc + ((size_t)tile * T + i) * TILE_TCW + TILE_TC_IW);
       if (v < 1 || v >= A.mwa) bad = 12;
       IWT[i] = v;
     }
     for (int i = tid; i < nU; i += TADJ_THREADS) {
       const int v = __ldg(A.ulist + u_off + i);
       if (v < 1 || v >= A.mwa) bad = 13;
-      UIW[i] = v;
+      ROW[i] = (long long)v * mza * ntp + t0;
     }
-    if (tid < 4) WS[(size_t)nU * TILE_WR + tid] = 0.f;
   }
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
     return;
   }
+  for (int i = tid; i < nT; i += TADJ_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
-  const int mza = A.mza, ntp = A.ntp, kb = A.kb;
-  const int t0 = grp * 64;
   const int seg = min(64, ntp - t0);
   const int nch = seg >> 2;
-  const int half = lane >> 4, hl = lane & 15;
-  const bool act = 4 * hl < seg;
-  const float dtr = A.dtr;
-
-  auto stage = [&](int kd) {
-    for (int i = tid; i < nU * 16; i += TADJ_THREADS) {
-      const int r = i >> 4, ch = i & 15;
-      if (ch < nch) cpa16(U + r * 256 + ch * 16, A.L + ((size_t)UIW[r] * mza + kd) * ntp + t0 + ch * 4);
+  const int ch = tid & 15;
+  auto stage = [&](int k, int b) {
+    char* Ub = UB + b * ubuf;
+    float* Rb = reinterpret_cast<float*>(RBB + b * rbuf);
+    const long long koff = (long long)k * ntp + ch * 4;
+    if (ch < nch)
+      for (int r = tid >> 4; r < nU; r += TADJ_THREADS / 16) cp_async16(Ub + r * 256 + ch * 16, A.L + ROW[r] + koff);
+    for (int i = tid; i < nT * (TADJ_RW / 4); i += TADJ_THREADS) {
+      const int c = i / (TADJ_RW / 4), q = i - c * (TADJ_RW / 4);
+      cp_async16(Rb + c * TADJ_RW + q * 4, A.trec + ((size_t)IWT[c] * mza + k) * TADJ_RW + q * 4);
     }
-    for (int i = tid; i < nU * (TILE_WR / 4); i += TADJ_THREADS) {
-      const int r = i / (TILE_WR / 4), ch = i - r * (TILE_WR / 4);
-      cpa16(WS + r * TILE_WR + ch * 4, A.wrec + ((size_t)UIW[r] * mza + kd) * TILE_WR + ch * 4);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    if (tid < 20) {
-      const int lev = kd - 2 + tid / 4, m = tid & 3;
-      AW[tid] = (lev >= 0 && lev < mza) ? __ldg(A.a_w + lev + m * mza) : 0.f;
-    }
+    cp_async_commit();
   };
 
-  stage(kb);
-  for (int kd = kb; kd < mza; ++kd) {
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
-    // ---- phase C: coefficients of this level, a thread per (column, entry)
-    for (int i = tid; i < nT * (TILE_NS + 1); i += TADJ_THREADS) {
-      const int c = i / (TILE_NS + 1), e = i - c * (TILE_NS + 1);
-      float* cf = CF + c * TADJ_CF;
-      if (e < TILE_NS) {
-        // the column across this transposed slot: its weight of our column, times
-        // dtr * volti / rhos of that column
-        const int v = REV[c * TILE_NS + e];
-        const int uu = v >> 8, j = v & 255;
-        cf[e] = j < TILE_NS ? dtr * WS[uu * TILE_WR + j] * WS[uu * TILE_WR + TILE_NS + 1] : 0.f;
-        continue;
-      }
-      // the vertical faces kd-2 .. kd+1 transposed, and the own-column terms
-      const int iw = IWT[c];
-      const float* wm = A.wmasc + (size_t)iw * mza;
-      const float fexpl = 1.0f - __ldg(A.ff + (size_t)iw * A.nrk + A.istage - 1);
-      float cm[5] = {0.f, 0.f, 0.f, 0.f, 0.f};   // coefficients of mu(kd-2 .. kd+2)
+  const int half = lane >> 4, hl = lane & 15;
+  const bool act = 4 * hl < seg;
+  const int cb = 2 * warp + half;
+  const bool first = A.first != 0, last = A.last != 0;
+  const float dtr = A.dtr;
+  F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], l0[NC], ls[NC];
+  long long cbase[NC];
+  bool need0[NC];
+  stage(kb, 0);
+  __syncthreads();   // FEX
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int f = kd - 2 + q;
-        if (f < kb || f > mza - 2) continue;
-        const float w = __ldg(wm + f);
-        const bool neg = w < 0.f;                 // upwind level f+1 (its bottom face), else f (top)
-        const int lev = neg ? f + 1 : f;
-        const int pos = kd - (neg ? f : f - 1);   // kd's place in the stencil (lev-1, lev, lev+1)
-        const float* a = AW + (lev - (kd - 2)) * 4;
-        const float c1 = a[neg ? 0 : 2], c2 = a[neg ? 1 : 3];
-        const float it = lev <= mza - 2 ? 1.f : 0.f, ib = lev >= kb + 1 ? 1.f : 0.f;
-        const float dF = pos == 0 ? -c2 * ib : (pos == 1 ? 1.f - c1 * it + c2 * ib : (pos == 2 ? c1 * it : 0.f));
-        const float a2 = fexpl * w * dF;   // lam_F(f) = fexpl wm(f) (mu(f+1) - mu(f))
-        cm[q + 1] += a2;
-        cm[q] -= a2;
-      }
-      if (kd == kb) cm[2] += fexpl * __ldg(wm + kb - 1);
-      if (kd == mza - 1) cm[2] -= fexpl * __ldg(wm + mza - 1);
-      const float* ws = WS + c * TILE_WR;   // the tile columns are the first U rows
-      cm[2] += ws[TILE_NS + 3];              // mu(x) (SW - sum W)
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        const int k2 = kd - 2 + q;
-        const float rv = (k2 >= kb && k2 < mza)
-                             ? (q == 2 ? ws[TILE_NS + 1] : __ldg(A.wrec + ((size_t)iw * mza + k2) * TILE_WR + TILE_NS + 1))
-                             : 0.f;
-        cf[TILE_NS + q] = dtr * rv * cm[q];
-      }
-      cf[TILE_NS + 5] = 1.0f - dtr * ws[TILE_NS + 1] * (ws[TILE_NS] + fexpl * (__ldg(wm + kd - 1) - __ldg(wm + kd)));
-      cf[TILE_NS + 6] = dtr * ws[TILE_NS + 2];
+  for (int n = 0; n < NC; ++n) {
+    const int c = cb + 16 * n;
+    m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = l0[n] = ls[n] = zero4();
+    cbase[n] = 0;
+    need0[n] = false;
+    if (c < nT && act) {
+      need0[n] = !first || FEX[c] < 1.0f;
+      cbase[n] = (long long)IWT[c] * mza * ntp + t0 + 4 * hl;
+      const float* q = A.L + cbase[n];
+      if (kb + 1 < mza) p1[n] = ldg4(q + (long long)(kb + 1) * ntp);
+      if (kb + 2 < mza) p2[n] = ldg4(q + (long long)(kb + 2) * ntp);
+      if (kb + 3 < mza) p3[n] = ldg4(q + (long long)(kb + 3) * ntp);
+      if (need0[n]) l0[n] = ldg4(A.L0 + cbase[n] + (long long)kb * ntp);
+      if (!first) ls[n] = ldg4(A.LS + cbase[n] + (long long)kb * ntp);
     }
-    __syncthreads();
-    // ---- phase B: the adjoint of the stage input, lam0 and lams, a half warp per column
-    for (int c = 2 * warp + half; c < nT; c += 2 * TADJ_NW) {
-      const int iw = IWT[c];
-      const float* cf = CF + c * TADJ_CF;
-      const size_t row = ((size_t)iw * mza + kd) * ntp + t0 + 4 * hl;
-      const size_t lvl = (size_t)ntp;
-      const char* Ul = U + hl * 16;
-      const G4 lx = lds_g4(Ul + c * 256);
-      G4 acc = G4{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      acc = fma_g4(cf[TILE_NS + 2], lx, acc);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  for (int kd = kb; kd < mza; ++kd) {
+    const int cur = (kd - kb) & 1;
+    if (kd + 1 < mza) stage(kd + 1, cur ^ 1);
+    const char* Ul = UB + cur * ubuf + hl * 16;
+    const float* Rc = reinterpret_cast<const float*>(RBB + cur * rbuf);
+#pragma unroll
+    for (int n = 0; n < NC; ++n) {
+      const int c = cb + 16 * n;
+      if (c >= nT) continue;
+      const float* rc = Rc + c * TADJ_RW;
+      const F4 lx = lds4(Ul, c * 256);
+      F4 acc = zero4();
+      const int* ro = REVO + c * TILE_NS;
 #pragma unroll
       for (int q = 0; q < TILE_NS / 4; ++q) {
-        const int4 r4 = reinterpret_cast<const int4*>(REV + c * TILE_NS)[q];
-        const float4 c4 = reinterpret_cast<const float4*>(cf)[q];
-        acc = fma_g4(c4.x, lds_g4(Ul + (r4.x & ~255)), acc);
-        acc = fma_g4(c4.y, lds_g4(Ul + (r4.y & ~255)), acc);
-        acc = fma_g4(c4.z, lds_g4(Ul + (r4.z & ~255)), acc);
-        acc = fma_g4(c4.w, lds_g4(Ul + (r4.w & ~255)), acc);
+        const int4 so = reinterpret_cast<const int4*>(ro)[q];
+        const float4 w4 = reinterpret_cast<const float4*>(rc)[q];
+        acc = fma4s(w4.x, lds4(Ul, so.x), acc);
+        acc = fma4s(w4.y, lds4(Ul, so.y), acc);
+        acc = fma4s(w4.z, lds4(Ul, so.z), acc);
+        acc = fma4s(w4.w, lds4(Ul, so.w), acc);
       }
+      const float fx = FEX[c];
+      const float4 r5 = reinterpret_cast<const float4*>(rc)[5];   // a0 .. a3
+      const float4 r6 = reinterpret_cast<const float4*>(rc)[6];   // a4, d, b26, b27
+      const float ri = rc[TILE_NS + 8];
+      acc = fma4s(fx * r5.x, m2[n], acc);
+      acc = fma4s(fx * r5.y, m1[n], acc);
+      acc = fma4s(fmaf(fx, r5.z, r6.y), lx, acc);
+      acc = fma4s(fx * r5.w, p1[n], acc);
+      acc = fma4s(fx * r6.x, p2[n], acc);
+      const F4 lin = scale4(dtr, acc);
+      const F4 l0n = fma4s(1.0f - dtr * fmaf(fx, r6.w, r6.z), lx, l0[n]);
+      const F4 lsn = fma4s(dtr * ri, lx, ls[n]);
       if (act) {
-        if (kd - 2 >= kb) acc = fma_g4(cf[TILE_NS + 0], ldg_g4(A.L + row - 2 * lvl), acc);
-        if (kd - 1 >= kb) acc = fma_g4(cf[TILE_NS + 1], ldg_g4(A.L + row - lvl), acc);
-        if (kd + 1 < mza) acc = fma_g4(cf[TILE_NS + 3], ldg_g4(A.L + row + lvl), acc);
-        if (kd + 2 < mza) acc = fma_g4(cf[TILE_NS + 4], ldg_g4(A.L + row + 2 * lvl), acc);
-        st_g4(A.LIN + row, acc);
-        G4 l0 = ldg_g4(A.L0 + row), ls = ldg_g4(A.LS + row);
-        l0 = fma_g4(cf[TILE_NS + 5], lx, l0);
-        ls = fma_g4(cf[TILE_NS + 6], lx, ls);
-        st_g4(A.L0 + row, l0);
-        st_g4(A.LS + row, ls);
+        const long long row = cbase[n] + (long long)kd * ntp;
+        if (last) {
+          stg4(A.LIN + row, add4(lin, l0n));
+        } else {
+          stg4(A.LIN + row, lin);
+          stg4(A.L0 + row, l0n);
+        }
+        stg4(A.LS + row, lsn);
         if (kd == kb)
-          for (int k2 = 0; k2 < kb; ++k2)
-            st_g4(A.LIN + ((size_t)iw * mza + k2) * ntp + t0 + 4 * hl, G4{make_float2(0.f, 0.f), make_float2(0.f, 0.f)});
+          for (int k2 = 0; k2 < kb; ++k2) {
+            const long long r2 = cbase[n] + (long long)k2 * ntp;
+            stg4(A.LIN + r2, zero4());
+            if (first) { stg4(A.L0 + r2, zero4()); stg4(A.LS + r2, zero4()); }
+          }
+        // slide the column's window up one level and read ahead
+        m2[n] = m1[n]; m1[n] = lx; p1[n] = p2[n]; p2[n] = p3[n];
+        if (kd + 4 < mza) p3[n] = ldg4(A.L + cbase[n] + (long long)(kd + 4) * ntp);
+        if (kd + 1 < mza) {
+          if (need0[n]) l0[n] = ldg4(A.L0 + cbase[n] + (long long)(kd + 1) * ntp);
+          if (!first) ls[n] = ldg4(A.LS + cbase[n] + (long long)(kd + 1) * ntp);
+        }
       }
     }
+    cp_async_wait_all();
     __syncthreads();
-    if (kd + 1 < mza) stage(kd + 1);
   }
 }
 
-
-static size_t tile_adj_smem_bytes(int T, int nu) {
-  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  return al((size_t)nu * 256) + al((size_t)nu * TILE_WR * 4 + 16) + al((size_t)T * TADJ_CF * 4) +
-         al((size_t)T * TILE_NS * 4) + al((size_t)T * 4) + al((size_t)nu * 4) + 20 * 4;
-}
-
-static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L, float* LIN, float* L0,
-                           float* LS, int ntp, int istage, int nrk, float dtr, int* status, cudaStream_t s) {
+static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L, float* LIN, float* L0, float* LS,
+                           int ntp, int istage, int nrk, float dtr, int first, int last, int* status,
+                           cudaStream_t s) {
   TileAdjArgs A;
   A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1;
   A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.mwa = d.mwa;
-  A.dtr = dtr;
+  A.dtr = dtr; A.first = first; A.last = last;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   A.ulist = d.tile_u.p; A.tc = d.tile_tc.p; A.rev = d.tile_rev.p;
-  A.a_w = d.a_w.p; A.wmasc = tp.wmasc.p; A.ff = tp.ff.p; A.wrec = tp.wrec.p;
+  A.ff = tp.ff.p; A.trec = tp.adj_trec.p;
   A.L = L; A.LIN = LIN; A.L0 = L0; A.LS = LS;
   A.err = status;
   const size_t smem = tile_adj_smem_bytes(d.tile_T, d.tile_nu_max);
-  if (smem > 227 * 1024) { set_error("adjoint tile neighbourhood exceeds shared memory"); return OLAMGPU_E_UNSUPPORTED; }
-  const unsigned ngrp = (unsigned)((ntp + 63) / 64);
-  OG_CUDA(cudaFuncSetAttribute(k_tile_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_tile_adj<<<(unsigned)d.ntiles * ngrp, TADJ_THREADS, smem, s>>>(A);
+  const unsigned nblk = (unsigned)d.ntiles * (unsigned)((ntp + 63) / 64);
+  if (d.tile_T == 32) {
+    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tile_adj<2><<<nblk, TADJ_THREADS, smem, s>>>(A);
+  } else {
+    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tile_adj<1><<<nblk, TADJ_THREADS, smem, s>>>(A);
+  }
   OG_LAUNCHED();
   return OLAMGPU_OK;
 }
 
-__global__ void k_adj_finish(size_t n, float* __restrict__ lam, const float* __restrict__ lam0) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) lam[i] += lam0[i];
+static int launch_adj_records(const DevGrid& d, Transport& tp, int* status, cudaStream_t s) {
+  const size_t n = (size_t)d.mza * d.mwa * TADJ_RW;
+  if (tp.adj_trec.n != n) {
+    OG_CHECK(tp.adj_trec.alloc(n));
+    OG_CUDA(cudaMemsetAsync(tp.adj_trec.p, 0, tp.adj_trec.bytes(), s));
+  }
+  AdjRecArgs R;
+  R.mza = d.mza; R.T = d.tile_T; R.kb = 1; R.mwa = d.mwa;
+  R.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
+  R.ulist = d.tile_u.p; R.tc = d.tile_tc.p; R.rev = d.tile_rev.p;
+  R.wrec = tp.wrec.p; R.wmasc = tp.wmasc.p; R.a_w = d.a_w.p; R.trec = tp.adj_trec.p;
+  R.err = status;
+  k_adj_records<<<(unsigned)d.ntiles * d.tile_T, 64, 0, s>>>(R);
+  OG_LAUNCHED();
+  return OLAMGPU_OK;
 }
 
-// per-tracer planes of the caller's arrays <-> the batched layout
-static int planes_table(Transport& tp, int n, size_t plane, cudaStream_t s) {
+// device pointer table of n planes of `plane` floats starting at base
+static int planes_table(DevBuf<float*>& tab, float* base, int n, size_t plane, cudaStream_t s) {
   std::vector<float*> h(n);
-  for (int i = 0; i < n; ++i) h[i] = tp.adj_planes.p + (size_t)i * plane;
-  OG_CHECK(tp.adj_ptab.alloc(n));
-  OG_CUDA(cudaMemcpyAsync(tp.adj_ptab.p, h.data(), n * sizeof(float*), cudaMemcpyHostToDevice, s));
+  for (int i = 0; i < n; ++i) h[i] = base + (size_t)i * plane;
+  OG_CHECK(tab.alloc(n));
+  OG_CUDA(cudaMemcpyAsync(tab.p, h.data(), n * sizeof(float*), cudaMemcpyHostToDevice, s));
   OG_CUDA(cudaStreamSynchronize(s));   // h dies here
   return OLAMGPU_OK;
 }
@@ -374,6 +478,10 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
     set_error("the adjoint needs the tiled transport tables (grids without terrain, lpw = lpv = 2)");
     return OLAMGPU_E_UNSUPPORTED;
   }
+  if (!d.tile_closed) {
+    set_error("the adjoint needs every neighbour of a prognosed column to be prognosed (a global domain)");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
   const int ntp = C.tr.ntp;
   const size_t plane = (size_t)mza * mwa, qn = plane * ntp;
 
@@ -382,7 +490,9 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   OG_CHECK(tp.adj_l0.alloc(qn));
   OG_CHECK(tp.adj_ls.alloc(qn));
   OG_CHECK(tp.adj_planes.alloc(plane * n));
-  OG_CHECK(planes_table(tp, n, plane, s));
+  OG_CHECK(planes_table(tp.adj_ptab, tp.adj_planes.p, n, plane, s));
+  // lams leaves through lam0's memory, which is free after the last stage
+  OG_CHECK(planes_table(tp.adj_ptab2, tp.adj_l0.p, n, plane, s));
   for (int i = 0; i < n; ++i)
     OG_CUDA(cudaMemcpyAsync(tp.adj_planes.p + (size_t)i * plane, lam[i], plane * sizeof(float),
                             cudaMemcpyHostToDevice, s));
@@ -390,51 +500,58 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   {
     // device work of the step (in RESIDENT mode the preparation uploads nothing)
     OG_PROF("adjoint", s);
-    OG_CUDA(cudaMemsetAsync(tp.adj_l[1].p, 0, qn * sizeof(float), s));
-    OG_CUDA(cudaMemsetAsync(tp.adj_l0.p, 0, qn * sizeof(float), s));
-    OG_CUDA(cudaMemsetAsync(tp.adj_ls.p, 0, qn * sizeof(float), s));
     float dtlr[3];
     OG_CHECK(transport_prepare(C, rho_old_host, false, dtlr));
     const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * plane;
     { OG_PROF("adj_gather", s); launch_gather_q(tp.adj_l[0].p, (const float* const*)tp.adj_ptab.p, n, ntp, plane, s); }
-    { OG_PROF("adj_weights", s); OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s)); }
+    {
+      OG_PROF("adj_records", s);
+      OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s));
+      OG_CHECK(launch_adj_records(d, tp, C.status.p, s));
+    }
+    // the reverse stages alternate between the two lam buffers; the last
+    // one writes into adj_l[fin]
+    const int fin = nrk & 1;
     float* L = tp.adj_l[0].p;
     float* LIN = tp.adj_l[1].p;
     const size_t colsize = (size_t)mza * ntp;
     if (d.n_nonprog > 0) {
-      k_adj_nonprog<<<cdiv((size_t)d.n_nonprog * colsize, 256), 256, 0, s>>>(d.w_nonprog.p, d.n_nonprog, colsize,
-                                                                            L, tp.adj_l0.p);
+      k_adj_nonprog<<<cdiv((size_t)d.n_nonprog * colsize, 256), 256, 0, s>>>(d.w_nonprog.p, d.n_nonprog, colsize, L,
+                                                                            LIN, tp.adj_ls.p, fin);
       OG_LAUNCHED();
     }
     for (int istage = nrk; istage >= 1; --istage) {
       const float dtr = dtlr[istage - 1];
+      const int first = istage == nrk, last = istage == 1;
       {
         OG_PROF("adj_implicit", s);
         k_adj_implicit<<<cdiv((size_t)d.nw_prog * ntp, 128), 128, 0, s>>>(
             gridk(d), tp.imp_list.p + (size_t)(istage - 1) * mwa, tp.imp_count.p + (istage - 1),
             tp.imp_b.p + (size_t)(istage - 1) * mwa * 3 * mza, tp.ff.p, tp.wmasc.p,
-            tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage, dtr, ntp, L, tp.adj_l0.p);
+            tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage, dtr, ntp, first, L, tp.adj_l0.p);
         OG_LAUNCHED();
         k_adj_fold0<<<cdiv((size_t)d.nw_prog * ntp, 256), 256, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p, mza, ntp, L);
         OG_LAUNCHED();
       }
       {
         OG_PROF("adj_stage", s);
-        OG_CHECK(launch_tile_adj(d, tp, L, LIN, tp.adj_l0.p, tp.adj_ls.p, ntp, istage, nrk, dtr, C.status.p, s));
+        OG_CHECK(launch_tile_adj(d, tp, L, LIN, tp.adj_l0.p, tp.adj_ls.p, ntp, istage, nrk, dtr, first, last,
+                                 C.status.p, s));
       }
       std::swap(L, LIN);
     }
-    k_adj_finish<<<cdiv(qn, 256), 256, 0, s>>>(qn, L, tp.adj_l0.p);
-    OG_LAUNCHED();
-    launch_scatter_q(L, tp.adj_ptab.p, n, ntp, plane, s);
+    {
+      OG_PROF("adj_scatter", s);
+      launch_scatter_q(tp.adj_l[fin].p, tp.adj_ptab.p, n, ntp, plane, s);
+      launch_scatter_q(tp.adj_ls.p, tp.adj_ptab2.p, n, ntp, plane, s);
+    }
   }
-  for (int i = 0; i < n; ++i)
+  for (int i = 0; i < n; ++i) {
     OG_CUDA(cudaMemcpyAsync(lam[i], tp.adj_planes.p + (size_t)i * plane, plane * sizeof(float),
                             cudaMemcpyDeviceToHost, s));
-  launch_scatter_q(tp.adj_ls.p, tp.adj_ptab.p, n, ntp, plane, s);
-  for (int i = 0; i < n; ++i)
-    OG_CUDA(cudaMemcpyAsync(lam_sct[i], tp.adj_planes.p + (size_t)i * plane, plane * sizeof(float),
+    OG_CUDA(cudaMemcpyAsync(lam_sct[i], tp.adj_l0.p + (size_t)i * plane, plane * sizeof(float),
                             cudaMemcpyDeviceToHost, s));
+  }
   OG_CUDA(cudaGetLastError());
   OG_CUDA(cudaStreamSynchronize(s));
   return check_device_status();
