@@ -181,9 +181,10 @@ struct DevGrid {
 // column c that has this cell as its slot j, c's U-row byte offset | j;
 // unused entries hold the cell's own offset | TILE_NS.
 // Per-(column, level) weight record of a long step (TILE_WR floats, read by
-// the stage kernel and the adjoint): the slot weights W[0..TILE_NS), SW,
-// volti / rhos, 1 / rhos, SW - sum W, wmasc(kd-1), wmasc(kd), 0, 0.
-#define TILE_WR 28
+// the stage kernel and the adjoint; layout at k_weights): the slot weights
+// W[0..TILE_NS), SW, volti / rhos, 1 / rhos, SW - sum W, the vertical flux's
+// coefficients on S(kd-2 .. kd+2) and on S0, wmasc(kd-1), wmasc(kd).
+#define TILE_WR 32
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)

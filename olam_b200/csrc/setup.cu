@@ -289,9 +289,10 @@ size_t tile_smem_bytes(int T, int nu, int mza) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
   // k_tile's layout: two level buffers of U rows and of the tile columns'
   // weight records, the U rows' global offsets, slot offsets, tile columns,
-  // explicit fractions, a_w of every level
+  // explicit fractions
+  (void)mza;
   return 2 * al((size_t)nu * 256) + 2 * al((size_t)T * TILE_WR * 4) + al((size_t)nu * 8) +
-         al((size_t)T * TILE_NS * 4) + 2 * al((size_t)T * 4) + (size_t)4 * mza * 4;
+         al((size_t)T * TILE_NS * 4) + 2 * al((size_t)T * 4);
 }
 
 // Two blocks per SM: 228 KB of shared memory less 1 KB reserved per block.

@@ -1,7 +1,7 @@
 // tile_common.cuh -- device helpers shared by the tiled stage kernel
 // (transport_tile.cu) and its transpose (transport_adjoint.cu): 16-byte
 // asynchronous copies into shared memory, four tracers per lane as two
-// packed float2 pairs (FFMA2 / FADD2 / FMUL2), grad_z_quadratic faces.
+// packed float2 pairs (FFMA2 / FADD2 / FMUL2).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -43,25 +43,6 @@ __device__ __forceinline__ F4 fma4s(float w, F4 x, F4 acc) {
 __device__ __forceinline__ F4 scale4(float w, F4 x) {
   const float2 w2 = make_float2(w, w);
   return F4{__fmul2_rn(w2, x.a), __fmul2_rn(w2, x.b)};
-}
-__device__ __forceinline__ F4 sel4(bool p, F4 x, F4 y) { return p ? x : y; }
-
-// grad_z_quadratic (bounded, zero-gradient BCs) at level lev from rows
-// a = S(lev-1), b = S(lev), c = S(lev+1); aw holds a_w(lev,1:2,1:2).
-// Rows outside the column are never used (the select drops them).
-__device__ __forceinline__ float2 zface_t(const float* aw, int mza, int kb, int lev, bool want_bot, float2 a,
-                                          float2 b, float2 c) {
-  const bool top = (lev > mza - 2), bot = (lev < kb + 1);
-  const float c1 = aw[want_bot ? 0 : 2], c2 = aw[want_bot ? 1 : 3];
-  float2 r;
-  float dsk = top ? 0.f : (c.x - b.x), dskm1 = bot ? 0.f : (b.x - a.x);
-  r.x = b.x + dsk * c1 + dskm1 * c2;
-  dsk = top ? 0.f : (c.y - b.y); dskm1 = bot ? 0.f : (b.y - a.y);
-  r.y = b.y + dsk * c1 + dskm1 * c2;
-  return r;
-}
-__device__ __forceinline__ F4 zface4(const float* aw, int mza, int kb, int lev, bool want_bot, F4 a, F4 b, F4 c) {
-  return F4{zface_t(aw, mza, kb, lev, want_bot, a.a, b.a, c.a), zface_t(aw, mza, kb, lev, want_bot, a.b, b.b, c.b)};
 }
 
 }  // namespace olamgpu

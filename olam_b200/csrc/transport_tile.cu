@@ -29,14 +29,15 @@
 // columns, four tracers per lane (packed FFMA2); the column's own values at
 // kd-2 .. kd+3 and its scp0 / sct rows stay in registers across levels (one
 // row per level is read ahead from global memory), so the vertical quadratic
-// faces need no staging.
+// faces -- linear in those rows with the records' coefficients -- need no
+// staging.
 #include "transport_kernels.cuh"
 #include "tile_common.cuh"
 
 namespace olamgpu {
 
 struct WeightArgs {
-  int mza, T;
+  int mza, T, kb;
   const int4* __restrict__ hdr;
   const int* __restrict__ tc;
   const float* __restrict__ amat;
@@ -44,6 +45,7 @@ struct WeightArgs {
   const float* __restrict__ wmasc;
   const float* __restrict__ volti;
   const float* __restrict__ rhos;   // rhos(:,:,nrk)
+  const float* __restrict__ a_w;    // Fortran (mza, 2, 2)
   float* __restrict__ wrec;         // (mwa, mza, TILE_WR)
 };
 
@@ -53,7 +55,6 @@ struct TileArgs {
   const int4* __restrict__ hdr;
   const int* __restrict__ ulist;
   const int* __restrict__ tc;
-  const float* __restrict__ a_w;    // Fortran (mza, 2, 2)
   const float* __restrict__ ff;     // (mwa, nrk)
   const float* __restrict__ wrec;   // (mwa, mza, TILE_WR)
   const float* __restrict__ S;
@@ -67,9 +68,19 @@ struct TileArgs {
 #define TILE_NW (TILE_THREADS / 32)
 
 // ---- per-(column, level) weight records, once per long step -------------------
-// Record (TILE_WR floats): W[0..TILE_NS), SW, volti / rhos, 1 / rhos,
-// SW - sum W, wmasc(kd-1), wmasc(kd), 0, 0.  One block per tile column, a
-// thread per level.
+// Record (TILE_WR floats):
+//   [0, TILE_NS)  W_j, the slot weights
+//   20 SW, 21 volti / rhos, 22 1 / rhos, 23 D = SW - sum W
+//   24 .. 28      beta_q: the vertical flux wmasc(kd-1) upw(kd-1) - wmasc(kd) upw(kd)
+//                 as sum_q beta_q S(kd-2+q), the upwind face values upw being
+//                 grad_z_quadratic of the upwind level (bounded) or, at the
+//                 bottom and top faces, S(kd) itself
+//   29            omega = wmasc(kd) - wmasc(kd-1), the vertical flux's S0 term
+//   30, 31        wmasc(kd-1), wmasc(kd)
+// so that a stage is
+//   scp = S0 + dtr / rhos sct + dtr volti / rhos (sum_j W_j S(slot j) + D S
+//         - SW S0 + fexpl (sum_q beta_q S(kd-2+q) + omega S0)).
+// One block per tile column, a thread per level.
 __global__ void k_weights(WeightArgs A) {
   __shared__ int w[TILE_TCW];
   __shared__ float am[TILE_AW];
@@ -80,36 +91,54 @@ __global__ void k_weights(WeightArgs A) {
   for (int q = threadIdx.x; q < TILE_AW; q += blockDim.x) am[q] = __ldg(A.amat + r * TILE_AW + q);
   __syncthreads();
   const int iw = w[TILE_TC_IW], np = w[TILE_TC_NP], side = w[TILE_TC_SIDE];
-  for (int kd = 1 + threadIdx.x; kd < A.mza; kd += blockDim.x) {
+  const int mza = A.mza, kb = A.kb;
+  for (int kd = kb + threadIdx.x; kd < mza; kd += blockDim.x) {
     float dvvm[6];
     int up[6];
     float sw = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      const float vm = f < np ? __ldg(A.vmasc + (size_t)w[TILE_TC_EV + f] * A.mza + kd) : 0.f;
+      const float vm = f < np ? __ldg(A.vmasc + (size_t)w[TILE_TC_EV + f] * mza + kd) : 0.f;
       dvvm[f] = __int_as_float(w[TILE_TC_DV + f]) * vm;
       // 1: the neighbour across face f is upwind
       up[f] = ((vm < 0.f ? 1 : 0) != ((side >> f) & 1)) ? 1 : 0;
       sw = fmaf(__int_as_float(w[TILE_TC_DV + f]), vm, sw);
     }
-    const size_t x = (size_t)iw * A.mza + kd;
+    const size_t x = (size_t)iw * mza + kd;
     float* o = A.wrec + x * TILE_WR;
     float sumw = 0.f;
-    float4 v4;
+    float v4[4];
 #pragma unroll
     for (int j = 0; j < TILE_NS; ++j) {
       float acc = 0.f;
 #pragma unroll
       for (int f = 0; f < 6; ++f) acc = fmaf(dvvm[f], am[(f * 2 + up[f]) * TILE_NS + j], acc);
       sumw += acc;
-      if ((j & 3) == 0) v4.x = acc;
-      else if ((j & 3) == 1) v4.y = acc;
-      else if ((j & 3) == 2) v4.z = acc;
-      else { v4.w = acc; reinterpret_cast<float4*>(o)[j >> 2] = v4; }
+      v4[j & 3] = acc;
+      if ((j & 3) == 3) reinterpret_cast<float4*>(o)[j >> 2] = make_float4(v4[0], v4[1], v4[2], v4[3]);
     }
+    // vertical faces: grad_z_quadratic at level lev from (lev-1, lev, lev+1),
+    // S(lev) + c1' (S(lev+1) - S(lev)) + c2' (S(lev) - S(lev-1)), the primes
+    // zeroing the differences across the column's ends
+    float beta[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    auto face = [&](float wf, int lev, bool bot, int q0) {   // q0: beta index of S(lev-1)
+      const float c1 = lev <= mza - 2 ? __ldg(A.a_w + lev + (bot ? 0 : 2) * mza) : 0.f;
+      const float c2 = lev >= kb + 1 ? __ldg(A.a_w + lev + (bot ? 1 : 3) * mza) : 0.f;
+      beta[q0] -= wf * c2;
+      beta[q0 + 1] += wf * (1.f - c1 + c2);
+      beta[q0 + 2] += wf * c1;
+    };
+    const float wkm1 = __ldg(A.wmasc + x - 1), wk0 = __ldg(A.wmasc + x);
+    if (kd == kb) beta[2] += wkm1;                   // scp_upw(kb-1) = scp(kb)
+    else if (wkm1 < 0.f) face(wkm1, kd, true, 1);    // scpb(kd) from (kd-1, kd, kd+1)
+    else face(wkm1, kd - 1, false, 0);               // scpt(kd-1) from (kd-2, kd-1, kd)
+    if (kd == mza - 1) beta[2] -= wk0;               // scp_upw(mza) = scp(mza)
+    else if (wk0 < 0.f) face(-wk0, kd + 1, true, 2); // scpb(kd+1) from (kd, kd+1, kd+2)
+    else face(-wk0, kd, false, 1);                   // scpt(kd) from (kd-1, kd, kd+1)
     const float rh = __ldg(A.rhos + x);
     reinterpret_cast<float4*>(o)[5] = make_float4(sw, __ldg(A.volti + x) / rh, 1.0f / rh, sw - sumw);
-    reinterpret_cast<float4*>(o)[6] = make_float4(__ldg(A.wmasc + x - 1), __ldg(A.wmasc + x), 0.f, 0.f);
+    reinterpret_cast<float4*>(o)[6] = make_float4(beta[0], beta[1], beta[2], beta[3]);
+    reinterpret_cast<float4*>(o)[7] = make_float4(beta[4], wk0 - wkm1, wkm1, wk0);
   }
 }
 
@@ -121,10 +150,11 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
     OG_CUDA(cudaMemsetAsync(tp.wrec.p, 0, tp.wrec.bytes(), s));
   }
   WeightArgs W;
-  W.mza = d.mza; W.T = d.tile_T;
+  W.mza = d.mza; W.T = d.tile_T; W.kb = 1;
   W.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   W.tc = d.tile_tc.p; W.amat = d.tile_a.p;
-  W.vmasc = tp.vmasc.p; W.wmasc = tp.wmasc.p; W.volti = d.volti.p; W.rhos = rhos; W.wrec = tp.wrec.p;
+  W.vmasc = tp.vmasc.p; W.wmasc = tp.wmasc.p; W.volti = d.volti.p; W.rhos = rhos; W.a_w = d.a_w.p;
+  W.wrec = tp.wrec.p;
   k_weights<<<(unsigned)d.ntiles * d.tile_T, 64, 0, s>>>(W);
   OG_LAUNCHED();
   return OLAMGPU_OK;
@@ -134,7 +164,7 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
 // Shared memory (in this order; tile_smem_bytes in setup.cu sizes it the
 // same way): two level buffers of U rows (256 B each), two of the tile
 // columns' records, the U rows' global row offsets, the slot byte offsets,
-// the tile columns, their explicit fractions, a_w of every level.
+// the tile columns, their explicit fractions.
 template <int NC>
 __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -151,8 +181,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   long long* ROW = reinterpret_cast<long long*>(p);   p += al((size_t)A.nu_max * 8);
   int* SLOT = reinterpret_cast<int*>(p);              p += al((size_t)T * TILE_NS * 4);
   int* IWT = reinterpret_cast<int*>(p);               p += al((size_t)T * 4);
-  float* FEX = reinterpret_cast<float*>(p);           p += al((size_t)T * 4);
-  float* AWS = reinterpret_cast<float*>(p);           // a_w(lev, 1:2, 1:2) at 4 lev
+  float* FEX = reinterpret_cast<float*>(p);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int t0 = grp * 64;
 
@@ -176,7 +205,6 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       if (v < 1 || v >= A.mwa) bad = 8;
       ROW[i] = (long long)v * mza * ntp + t0;
     }
-    for (int i = tid; i < 4 * mza; i += TILE_THREADS) AWS[i] = __ldg(A.a_w + (i >> 2) + (i & 3) * mza);
   }
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
@@ -238,11 +266,13 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       const int c = cb + 16 * n;
       if (c >= nT) continue;
       const float* rc = Rc + c * TILE_WR;
-      const float4 r5 = *reinterpret_cast<const float4*>(rc + TILE_NS);       // SW, volti/rhos, 1/rhos, D
-      const float2 r6 = *reinterpret_cast<const float2*>(rc + TILE_NS + 4);   // wmasc(kd-1), wmasc(kd)
+      const float4 r5 = reinterpret_cast<const float4*>(rc)[5];   // SW, volti/rhos, 1/rhos, D
+      const float4 r6 = reinterpret_cast<const float4*>(rc)[6];   // beta0 .. beta3
+      const float2 r7 = reinterpret_cast<const float2*>(rc)[14];  // beta4, omega
+      const float fx = FEX[c];
       const F4 s0 = lds4(Ul, c * 256);
-      // horizontal: D S - SW S0 + sum_j W_j S(slot j)
-      F4 fd = fma4s(r5.w, s0, scale4(-r5.x, s00[n]));
+      // horizontal: sum_j W_j S(slot j) + D S - SW S0
+      F4 fd = zero4();
       const int* sl = SLOT + c * TILE_NS;
 #pragma unroll
       for (int q = 0; q < TILE_NS / 4; ++q) {
@@ -253,29 +283,15 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
         fd = fma4s(w4.z, lds4(Ul, so.z), fd);
         fd = fma4s(w4.w, lds4(Ul, so.w), fd);
       }
-      // vertical upwind faces kd-1 and kd (grad_z_quadratic, bounded): the
-      // upwind level's stencil is selected, then reconstructed once
-      const float wkm1 = r6.x, wk0 = r6.y;
-      F4 up_lo, up_hi;
-      if (kd == kb) {
-        up_lo = s0;   // scp_upw(kb-1) = scp(kb)
-      } else {
-        const bool dn = wkm1 < 0.f;   // scpb(kd) from (kd-1, kd, kd+1), else scpt(kd-1) from (kd-2, kd-1, kd)
-        const int lev = dn ? kd : kd - 1;
-        up_lo = zface4(AWS + 4 * lev, mza, kb, lev, dn, sel4(dn, m1[n], m2[n]), sel4(dn, s0, m1[n]),
-                       sel4(dn, p1[n], s0));
-      }
-      if (kd == mza - 1) {
-        up_hi = s0;   // scp_upw(mza) = scp(mza)
-      } else {
-        const bool dn = wk0 < 0.f;    // scpb(kd+1) from (kd, kd+1, kd+2), else scpt(kd) from (kd-1, kd, kd+1)
-        const int lev = dn ? kd + 1 : kd;
-        up_hi = zface4(AWS + 4 * lev, mza, kb, lev, dn, sel4(dn, s0, m1[n]), sel4(dn, p1[n], s0),
-                       sel4(dn, p2[n], p1[n]));
-      }
-      const F4 v = scale4(FEX[c], sub4(scale4(wkm1, sub4(up_lo, s00[n])), scale4(wk0, sub4(up_hi, s00[n]))));
+      // vertical quadratic upwind faces, fexpl times sum_q beta_q S(kd-2+q) + omega S0
+      fd = fma4s(fx * r6.x, m2[n], fd);
+      fd = fma4s(fx * r6.y, m1[n], fd);
+      fd = fma4s(fmaf(fx, r6.z, r5.w), s0, fd);
+      fd = fma4s(fx * r6.w, p1[n], fd);
+      fd = fma4s(fx * r7.x, p2[n], fd);
+      fd = fma4s(fmaf(fx, r7.y, -r5.x), s00[n], fd);
       // scp = scp0 + dtr * (sct + volti * (fluxdiv + fexpl * vflux)) / rhos
-      const F4 o = fma4s(A.dtr * r5.y, add4(fd, v), fma4s(A.dtr * r5.z, st[n], s00[n]));
+      const F4 o = fma4s(A.dtr * r5.y, fd, fma4s(A.dtr * r5.z, st[n], s00[n]));
       if (act) {
         stg4(A.OUT + cbase[n] + (long long)kd * ntp, o);
         if (kd == kb)
@@ -311,7 +327,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   A.dtr = dtr;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   A.ulist = d.tile_u.p; A.tc = d.tile_tc.p;
-  A.a_w = d.a_w.p; A.ff = tp.ff.p; A.wrec = tp.wrec.p;
+  A.ff = tp.ff.p; A.wrec = tp.wrec.p;
   A.S = S; A.S0 = S0; A.SCT = SCT; A.OUT = OUT;
   A.err = status;
   const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, d.mza);
