@@ -19,6 +19,8 @@
 // lam0 collects the adjoint of scp0 (the s00 terms of every stage and the
 // columns outside jtw_prog), lams the adjoint of sct.  Neither is cleared
 // first: the first reverse stage writes them, later stages accumulate.
+#include <algorithm>
+
 #include "transport_kernels.cuh"
 #include "tile_common.cuh"
 
@@ -38,17 +40,20 @@ __global__ void k_adj_nonprog(const int* __restrict__ cols, int ncol, size_t col
   else other[x] = 0.f;
 }
 
-// the forward stage copies level kb to the levels below: their adjoint folds into kb
+// the forward stage copies level kb to the levels below: their adjoint folds
+// into kb.  Blocks stride over the prognostic columns, threads over the tracers.
 __global__ void k_adj_fold0(const int* __restrict__ prog, int nprog, const int* __restrict__ lpw, int mza, int ntp,
                             float* __restrict__ lam) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (size_t)nprog * ntp) return;
-  const int iw = prog[i / ntp], t = (int)(i % ntp);
-  const int kb = lpw[iw];
-  float* c = lam + (size_t)iw * mza * ntp + t;
-  float a = c[(size_t)kb * ntp];
-  for (int k = 0; k < kb; ++k) { a += c[(size_t)k * ntp]; c[(size_t)k * ntp] = 0.f; }
-  c[(size_t)kb * ntp] = a;
+  for (int j = blockIdx.x; j < nprog; j += gridDim.x) {
+    const int iw = prog[j];
+    const int kb = lpw[iw];
+    for (int t = threadIdx.x; t < ntp; t += blockDim.x) {
+      float* c = lam + (size_t)iw * mza * ntp + t;
+      float a = c[(size_t)kb * ntp];
+      for (int k = 0; k < kb; ++k) { a += c[(size_t)k * ntp]; c[(size_t)k * ntp] = 0.f; }
+      c[(size_t)kb * ntp] = a;
+    }
+  }
 }
 
 // transpose of the implicit vertical step (scalar_transport_rk.F90:347-375,
@@ -245,7 +250,8 @@ template <int NC>
 __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int T = 16 * NC;
-  const int tile = blockIdx.x % A.ntiles, grp = blockIdx.x / A.ntiles;
+  const int ngrp = (A.ntp + 63) >> 6;   // the tracer groups of a tile side by side
+  const int tile = blockIdx.x / ngrp, grp = blockIdx.x - tile * ngrp;
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;
@@ -530,7 +536,9 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
             tp.imp_b.p + (size_t)(istage - 1) * mwa * 3 * mza, tp.ff.p, tp.wmasc.p,
             tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage, dtr, ntp, first, L, tp.adj_l0.p);
         OG_LAUNCHED();
-        k_adj_fold0<<<cdiv((size_t)d.nw_prog * ntp, 256), 256, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p, mza, ntp, L);
+        if (d.nw_prog > 0)
+          k_adj_fold0<<<(unsigned)std::min(d.nw_prog, 148 * 16), 128, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p, mza,
+                                                                              ntp, L);
         OG_LAUNCHED();
       }
       {

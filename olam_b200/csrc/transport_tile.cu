@@ -37,7 +37,7 @@
 namespace olamgpu {
 
 struct WeightArgs {
-  int mza, T, kb;
+  int mza, T, kb, ntiles;
   const int4* __restrict__ hdr;
   const int* __restrict__ tc;
   const float* __restrict__ amat;
@@ -80,19 +80,25 @@ struct TileArgs {
 // so that a stage is
 //   scp = S0 + dtr / rhos sct + dtr volti / rhos (sum_j W_j S(slot j) + D S
 //         - SW S0 + fexpl (sum_q beta_q S(kd-2+q) + omega S0)).
-// One block per tile column, a thread per level.
-__global__ void k_weights(WeightArgs A) {
-  __shared__ int w[TILE_TCW];
-  __shared__ float am[TILE_AW];
-  const int t = blockIdx.x / A.T, i = blockIdx.x - t * A.T;
-  if (i >= A.hdr[t].w) return;   // padding of the last tile (uniform per block)
-  const size_t r = (size_t)blockIdx.x;
-  for (int q = threadIdx.x; q < TILE_TCW; q += blockDim.x) w[q] = __ldg(A.tc + r * TILE_TCW + q);
-  for (int q = threadIdx.x; q < TILE_AW; q += blockDim.x) am[q] = __ldg(A.amat + r * TILE_AW + q);
+// Four tile columns per block of 256 threads, a thread per level.
+__global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
+  __shared__ int wall[4][TILE_TCW];
+  __shared__ float amall[4][TILE_AW];
+  const int sub = threadIdx.x >> 6, lt = threadIdx.x & 63;
+  const size_t r = (size_t)blockIdx.x * 4 + sub;   // tile-column record
+  const int t = (int)(r / A.T), i = (int)(r - (size_t)t * A.T);
+  const bool live = t < A.ntiles && i < A.hdr[t].w;   // not padding of the last tile
+  int* w = wall[sub];
+  float* am = amall[sub];
+  if (live) {
+    for (int q = lt; q < TILE_TCW; q += 64) w[q] = __ldg(A.tc + r * TILE_TCW + q);
+    for (int q = lt; q < TILE_AW; q += 64) am[q] = __ldg(A.amat + r * TILE_AW + q);
+  }
   __syncthreads();
+  if (!live) return;
   const int iw = w[TILE_TC_IW], np = w[TILE_TC_NP], side = w[TILE_TC_SIDE];
   const int mza = A.mza, kb = A.kb;
-  for (int kd = kb + threadIdx.x; kd < mza; kd += blockDim.x) {
+  for (int kd = kb + lt; kd < mza; kd += 64) {
     float dvvm[6];
     int up[6];
     float sw = 0.f;
@@ -150,12 +156,12 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
     OG_CUDA(cudaMemsetAsync(tp.wrec.p, 0, tp.wrec.bytes(), s));
   }
   WeightArgs W;
-  W.mza = d.mza; W.T = d.tile_T; W.kb = 1;
+  W.mza = d.mza; W.T = d.tile_T; W.kb = 1; W.ntiles = d.ntiles;
   W.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   W.tc = d.tile_tc.p; W.amat = d.tile_a.p;
   W.vmasc = tp.vmasc.p; W.wmasc = tp.wmasc.p; W.volti = d.volti.p; W.rhos = rhos; W.a_w = d.a_w.p;
   W.wrec = tp.wrec.p;
-  k_weights<<<(unsigned)d.ntiles * d.tile_T, 64, 0, s>>>(W);
+  k_weights<<<cdiv((size_t)d.ntiles * d.tile_T, 4), 256, 0, s>>>(W);
   OG_LAUNCHED();
   return OLAMGPU_OK;
 }
@@ -169,7 +175,9 @@ template <int NC>
 __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int T = 16 * NC;
-  const int tile = blockIdx.x % A.ntiles, grp = blockIdx.x / A.ntiles;
+  // the tracer groups of a tile run side by side (its records are read once from HBM)
+  const int ngrp = (A.ntp + 63) >> 6;
+  const int tile = blockIdx.x / ngrp, grp = blockIdx.x - tile * ngrp;
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;
