@@ -7,7 +7,9 @@
 //   k_vort_* / k_lap_m      vort_damp                          (vort_div_damp.f90:234-445)
 //   k_rk_copy, k_vmca       stage copies, vmca and vmasc       (prog_wrtv_rk.f90:320-368)
 //   k_grad4, k_upw4, k_upv4 fluxes_wrtv for thil, vxe, vye, vze (:950-1129), the four
-//                           fields of one stage in one launch each
+//                           fields of one stage in one launch each; on the
+//                           last stage the fields with ithil_monot /
+//                           iwind_monot > 0 take dynamics_monot.cu's values
 //   k_wrt_begs              prog_wrt_begs (:494-884): one warp per column, lanes over
 //                           levels for the explicit terms, one lane for the serial
 //                           tridiagonal solve (tridiffo, tridiag_lib.f90:10-36)
@@ -886,10 +888,6 @@ int dyn_prog_wrtv_rk(int istp) {
   if (!C.dy.ready) { set_error("prog_wrtv_rk was not set up (see olamgpu_init's status)"); return OLAMGPU_E_STATE; }
   if (!C.have_state) { set_error("prog_wrtv_rk needs the state arrays registered at init"); return OLAMGPU_E_STATE; }
   const olamgpu_opts& o = C.opts;
-  if (o.ithil_monot > 0 || o.iwind_monot > 0) {
-    set_error("ithil_monot / iwind_monot > 0 (fluxes_wrtv_monot) is not available in this build");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
   if (o.nrk_wrtv != 2 && o.nrk_wrtv != 3) { set_error("acoust_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
   cudaStream_t s = C.stream;
   OG_CHECK(ensure_dyn_buffers(C));
@@ -916,6 +914,21 @@ int dyn_prog_wrtv_rk(int istp) {
   OG_LAUNCHED(); OG_LAUNCHED();
   if (o.divh_damp_short) divh_damp(C, y.sh_vmt.p, o.dtsm, s);
   if (o.vort_damp_short) vort_damp(C, y.sh_vmt.p, o.dtsm, s);
+  // start values of the fields fluxes_wrtv_monot limits (prog_wrtv_rk.f90:186-198)
+  const bool thil_monot = o.ithil_monot > 0, wind_monot = o.iwind_monot > 0;
+  const size_t wzb = (size_t)mza * d.mwa * sizeof(float);
+  if (thil_monot) {
+    OG_CHECK(y.th0.alloc((size_t)mza * d.mwa));
+    OG_CUDA(cudaMemcpyAsync(y.th0.p, y.thil.p, wzb, cudaMemcpyDeviceToDevice, s));
+  }
+  if (wind_monot) {
+    DevBuf<float>* b0[3] = {&y.vx0, &y.vy0, &y.vz0};
+    const float* src[3] = {y.vxe.p, y.vye.p, y.vze.p};
+    for (int i = 0; i < 3; ++i) {
+      OG_CHECK(b0[i]->alloc((size_t)mza * d.mwa));
+      OG_CUDA(cudaMemcpyAsync(b0[i]->p, src[i], wzb, cudaMemcpyDeviceToDevice, s));
+    }
+  }
 
   const int nrk = o.nrk_wrtv;
   const double third = 1.0 / 3.0;
@@ -936,6 +949,17 @@ int dyn_prog_wrtv_rk(int istp) {
     k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, o.thil_horiz_adv_order, o.wind_horiz_adv_order,
                                 y.gx.p, vs, y.vmc.p, y.upv.p);
     OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+    // last stage: flux-corrected face values replace those of the limited fields (370-399)
+    if (last && thil_monot) {
+      OG_PROF("monot_faces", s);
+      OG_CHECK(dyn_monot_faces(C, 0, y.thil.p, y.th0.p, y.sh_th.p, dts, o.thil_horiz_adv_order, s));
+    }
+    if (last && wind_monot) {
+      OG_PROF("monot_faces", s);
+      OG_CHECK(dyn_monot_faces(C, 1, y.vxe.p, y.vx0.p, y.sh_vx.p, dts, o.wind_horiz_adv_order, s));
+      OG_CHECK(dyn_monot_faces(C, 2, y.vye.p, y.vy0.p, y.sh_vy.p, dts, o.wind_horiz_adv_order, s));
+      OG_CHECK(dyn_monot_faces(C, 3, y.vze.p, y.vz0.p, y.sh_vz.p, dts, o.wind_horiz_adv_order, s));
+    }
     WrtArgs A;
     A.istage = istage; A.nrk = nrk; A.dt8 = dt8; A.dts = dts; A.fcoriol = o.fcoriol;
     A.fr = (double)0.70f;
@@ -1035,7 +1059,9 @@ void dyn_release() {
                         &y.rk_vz, &y.upw, &y.upv, &y.gx, &y.div2d, &y.fdivh, &y.vort2d, &y.fvorth, &y.fvortl,
                         &y.vfact, &y.arv, &y.arw, &y.volwi, &y.volvi, &y.wn, &y.wno2, &y.vn, &y.ecv,
                         &y.gdz_wgtm, &y.gdz_wgtp, &y.dniv, &y.dniu, &y.dnv, &y.arw0, &y.arm0, &y.zfacit,
-                        &y.dzit, &y.xx_yy, &y.xx_yy_m, &y.b20, &y.rayf_cof, &y.dn01d, &y.th01d, &y.vc03d};
+                        &y.dzit, &y.xx_yy, &y.xx_yy_m, &y.b20, &y.rayf_cof, &y.dn01d, &y.th01d, &y.vc03d,
+                        &y.th0, &y.vx0, &y.vy0, &y.vz0, &y.m_scpt, &y.m_gx, &y.m_hiw, &y.m_sfw, &y.m_hiv,
+                        &y.m_sfv, &y.m_sin, &y.m_sout};
   for (auto* b : f) b->release();
   y.lpmmin.release();
   y = Dyn();

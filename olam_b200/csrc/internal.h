@@ -251,6 +251,10 @@ struct Dyn {
   DevBuf<float> dniv, dniu, dnv, arw0, arm0, zfacit, dzit, xx_yy, xx_yy_m, b20;
   DevBuf<double> volt, zwgt_top8, zwgt_bot8, gdz_wgtm8, gdz_wgtp8;
   DevBuf<float> rayf_cof, dn01d, th01d, vc03d;
+  // fluxes_wrtv_monot (dynamics_monot.cu): start values of the limited
+  // fields, and scratch shared by the fields in turn
+  DevBuf<float> th0, vx0, vy0, vz0;
+  DevBuf<float> m_scpt, m_gx, m_hiw, m_sfw, m_hiv, m_sfv, m_sin, m_sout;
 };
 
 struct Context {
@@ -293,6 +297,10 @@ int dyn_timeavg_momsc();
 int dyn_state_to_device(unsigned mask, cudaStream_t s);
 int dyn_state_to_host(unsigned mask, cudaStream_t s);
 void dyn_release();
+// the flux-corrected face values of field 0 (thil) .. 3 (vze) on the last
+// RK stage (dynamics_monot.cu): scp, its start value, its *_short tendency
+int dyn_monot_faces(Context& C, int field, const float* scp, const float* scp0, const float* sct, float dts,
+                    int ord, cudaStream_t s);
 
 // reads the device status record (call with the library stream idle); a
 // kernel that found an inconsistent table reports it here

@@ -8,6 +8,10 @@
  *   prog_wrt_begs          omodel/prog_wrtv_rk.f90:494-884
  *   prog_v_begs            omodel/prog_wrtv_rk.f90:888-946
  *   fluxes_wrtv            omodel/prog_wrtv_rk.f90:950-1129
+ *   fluxes_wrtv_monot      omodel/prog_wrtv_rk.f90:1133-1554 (with
+ *                          scalar_wflux_monot, scalar_vflux_monot and
+ *                          scalar_monot_limiter; centered_monot = .false.,
+ *                          iorderv = 3)
  *   vel_t3d_hex            omodel/vel_t3d.f90:39-108
  *   divh_damp, vort_damp   omodel/vort_div_damp.f90:1-445
  *   laplacian2d/_m         omodel/grad_lib.f90:494-559
@@ -20,8 +24,10 @@
  * their single-precision value when promoted to real(8).
  * Not restated (off in every configuration this build runs): nudging,
  * shaved cells (lve2 > 0), eddy diffusion hooks (turbulence off), Lagrangian
- * particle sums, the shallow-water test cases, fluxes_wrtv_monot.
+ * particle sums, the shallow-water test cases.
  */
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -389,13 +395,182 @@ static void fluxes_wrtv(const DynCtx<T>& X, const T* scp, T* scp_upw, T* scp_upv
   }
 }
 
+/* fluxes_wrtv_monot (prog_wrtv_rk.f90:1133-1554): on the last RK stage,
+ * flux-corrected upwinded face values of one field.  Low-order faces take
+ * the upwind cell of scpt = scp0 + dtr volti sct / rho0 (1179-1186);
+ * high-order faces (scp with bounded horizontal gradients, grad_t2d or
+ * grad_t2d_quadratic, the xx0_vu face terms, and grad_z_quadratic with
+ * constant-gradient ends and a_wu) add their difference to the low-order
+ * value scaled by the cell limiter of scalar_monot_limiter (1450-1552). */
+template <class T>
+static void fluxes_wrtv_monot(const DynCtx<T>& X, const T* scp, const T* scp0, const T* sct, T* scp_upw, T* scp_upv,
+                              const R8* rho, const R8* rho0, const T* vmca, const T* wmc, T dtr, int iorderh) {
+  const GridT<T>& G = X.G;
+  const int mza = X.mza, mwa = X.mwa, mva = X.mva;
+  const size_t plane = (size_t)mza * mwa, vplane = (size_t)mza * mva;
+  const T eps0 = (T)1.e-32, eps1 = (T)3.e-07, onep = (T)1.0 + eps1;
+  std::vector<T> scpt(plane, (T)0), sin_(plane, (T)0), sout(plane, (T)0);
+  std::vector<T> sfluxvh(vplane, (T)0), scp_hiv(vplane, (T)0);
+  std::vector<T> sfluxwh(plane + 1, (T)0), scp_hiw(plane + 1, (T)0);
+  std::vector<T> gx(plane * 5, (T)0);
+  // scpt (1179-1186)
+  for (int j = 0; j < X.g->nw_prog; ++j) {
+    const int iw = X.g->jtw_prog[j];
+    for (int k = G.lpw(iw); k <= mza; ++k)
+      F2(scpt.data(), k, iw) = F2(scp0, k, iw) + dtr * G.volti_(k, iw) * F2(sct, k, iw) / (T)F2(rho0, k, iw);
+  }
+  // bounded horizontal gradients (1192-1206)
+  if (iorderh > 1) {
+    for (int j = 0; j < X.g->nw_prog; ++j) {
+      const int iw = X.g->jtw_prog[j];
+      T* c0 = gx.data() + (size_t)(iw - 1) * mza;
+      for (int n = 1; n <= G.npoly(iw); ++n) {
+        const int iwn = G.w_iw(iw, n), ivn = G.w_iv(iw, n);
+        for (int k = G.lpv(ivn); k <= mza; ++k) {
+          const T d = F2(scp, k, iwn) - F2(scp, k, iw);
+          if (iorderh == 2) {
+            c0[k - 1] = c0[k - 1] + G.gxps_coef(n, iw) * d;
+            c0[plane + k - 1] = c0[plane + k - 1] + G.gyps_coef(n, iw) * d;
+          } else {
+            for (int m = 0; m < 5; ++m) c0[m * plane + k - 1] = c0[m * plane + k - 1] + d * G.xyh(G.xy_h, m + 1, n, iw);
+          }
+        }
+      }
+    }
+  }
+  // scalar_wflux_monot (1380-1446)
+  for (int j = 0; j < X.g->nw_prog; ++j) {
+    const int iw = X.g->jtw_prog[j];
+    const int kb = G.lpw(iw);
+    const T* col = scp + (size_t)(iw - 1) * mza;
+    F2(scp_upw, kb - 1, iw) = col[kb - 1];
+    F2(scp_upw, mza, iw) = col[mza - 1];
+    for (int k = kb; k <= mza - 1; ++k) {
+      T v = F2(scpt.data(), k, iw);
+      if (F2(wmc, k, iw) < (T)0) v = F2(scpt.data(), k + 1, iw);
+      F2(scp_upw, k, iw) = v;
+    }
+    // grad_z_quadratic(itopbc=1, ibotbc=1, bounded=.false.)
+    std::vector<T> ds(mza + 1), sb(mza + 1), st(mza + 1);
+    for (int k = kb; k <= mza - 1; ++k) ds[k] = col[k] - col[k - 1];
+    ds[kb - 1] = ds[kb];
+    ds[mza] = ds[mza - 1];
+    for (int k = kb; k <= mza; ++k) {
+      sb[k] = col[k - 1] + ds[k] * G.aw(G.a_wu, k, 1, 1) + ds[k - 1] * G.aw(G.a_wu, k, 2, 1);
+      st[k] = col[k - 1] + ds[k] * G.aw(G.a_wu, k, 1, 2) + ds[k - 1] * G.aw(G.a_wu, k, 2, 2);
+    }
+    F2(sfluxwh.data(), kb - 1, iw) = 0;
+    F2(sfluxwh.data(), mza, iw) = 0;
+    for (int k = kb; k <= mza - 1; ++k) {
+      T h = st[k];
+      if (F2(wmc, k, iw) < (T)0) h = sb[k + 1];
+      h = h - F2(scp_upw, k, iw);
+      F2(scp_hiw.data(), k, iw) = h;
+      F2(sfluxwh.data(), k, iw) = F2(X.arw.data(), k, iw) * F2(wmc, k, iw) * h;
+    }
+  }
+  // scalar_vflux_monot (1293-1376)
+  for (int j = 0; j < X.g->nv_wadj; ++j) {
+    const int iv = X.g->jtv_wadj[j];
+    const int iw1 = G.v_iw(iv, 1), iw2 = G.v_iw(iv, 2);
+    for (int k = G.lpv(iv); k <= mza; ++k) {
+      const bool neg = F2(vmca, k, iv) < (T)0;
+      const T low = neg ? F2(scpt.data(), k, iw2) : F2(scpt.data(), k, iw1);
+      F2(scp_upv, k, iv) = low;
+      T s1 = F2(scp, k, iw1), s2 = F2(scp, k, iw2);
+      if (iorderh >= 2) {
+        const size_t o1 = (size_t)(iw1 - 1) * mza + k - 1, o2 = (size_t)(iw2 - 1) * mza + k - 1;
+        s1 = s1 + G.v2(G.dxps, 1, iv) * gx[o1] + G.v2(G.dyps, 1, iv) * gx[plane + o1];
+        s2 = s2 + G.v2(G.dxps, 2, iv) * gx[o2] + G.v2(G.dyps, 2, iv) * gx[plane + o2];
+        if (iorderh == 3) {
+          s1 = s1 + G.v2(G.xx0_vu, 1, iv) * gx[2 * plane + o1] + G.v2(G.xy0_vu, 1, iv) * gx[3 * plane + o1] +
+               G.v2(G.yy0_vu, 1, iv) * gx[4 * plane + o1];
+          s2 = s2 + G.v2(G.xx0_vu, 2, iv) * gx[2 * plane + o2] + G.v2(G.xy0_vu, 2, iv) * gx[3 * plane + o2] +
+               G.v2(G.yy0_vu, 2, iv) * gx[4 * plane + o2];
+        }
+      }
+      T h = neg ? s2 : s1;
+      h = h - low;
+      F2(scp_hiv.data(), k, iv) = h;
+      F2(sfluxvh.data(), k, iv) = F2(vmca, k, iv) * h;
+    }
+  }
+  // scalar_monot_limiter (1450-1552)
+  const T dtrp = onep * dtr;
+  for (int j = 0; j < X.g->nw_prog; ++j) {
+    const int iw = X.g->jtw_prog[j];
+    const int kb = G.lpw(iw);
+    std::vector<T> wmca(mza + 1, (T)0), smax(mza + 1), smin(mza + 1), rhos(mza + 1), fl(mza + 1, (T)0),
+        fi(mza + 1, (T)0), fo(mza + 1, (T)0);
+    for (int k = kb; k <= mza - 1; ++k) wmca[k] = F2(wmc, k, iw) * F2(X.arw.data(), k, iw);
+    for (int k = kb; k <= mza; ++k) {
+      smax[k] = smin[k] = F2(scpt.data(), k, iw);
+      rhos[k] = (T)F2(rho, k, iw);
+    }
+    for (int k = kb + 1; k <= mza; ++k)
+      if (wmca[k - 1] > (T)0) {
+        smax[k] = std::max(smax[k], F2(scpt.data(), k - 1, iw));
+        smin[k] = std::min(smin[k], F2(scpt.data(), k - 1, iw));
+      }
+    for (int k = kb; k <= mza - 1; ++k)
+      if (wmca[k] < (T)0) {
+        smax[k] = std::max(smax[k], F2(scpt.data(), k + 1, iw));
+        smin[k] = std::min(smin[k], F2(scpt.data(), k + 1, iw));
+      }
+    for (int jv = 1; jv <= G.npoly(iw); ++jv) {
+      const int iv = G.w_iv(iw, jv), iwn = G.w_iw(iw, jv);
+      const T dv = G.w_dirv(iw, jv);
+      for (int k = G.lpv(iv); k <= mza; ++k) {
+        fl[k] = fl[k] + dv * F2(vmca, k, iv) * (F2(scp_upv, k, iv) - F2(scpt.data(), k, iw));
+        fi[k] = fi[k] + std::max(dv * F2(sfluxvh.data(), k, iv), (T)0);
+        fo[k] = fo[k] + std::min(dv * F2(sfluxvh.data(), k, iv), (T)0);
+        if (dv * F2(vmca, k, iv) > (T)0) {
+          smax[k] = std::max(smax[k], F2(scpt.data(), k, iwn));
+          smin[k] = std::min(smin[k], F2(scpt.data(), k, iwn));
+        }
+      }
+    }
+    for (int k = kb; k <= mza; ++k) {
+      const T s = F2(scpt.data(), k, iw);
+      fl[k] = fl[k] + wmca[k - 1] * (F2(scp_upw, k - 1, iw) - s) - wmca[k] * (F2(scp_upw, k, iw) - s);
+      fi[k] = fi[k] + std::max(F2(sfluxwh.data(), k - 1, iw), (T)0) - std::min(F2(sfluxwh.data(), k, iw), (T)0);
+      fo[k] = fo[k] + std::min(F2(sfluxwh.data(), k - 1, iw), (T)0) - std::max(F2(sfluxwh.data(), k, iw), (T)0);
+      const T rscp_low = s * rhos[k] + dtr * G.volti_(k, iw) * fl[k];
+      const T flux_in = std::max(dtrp * G.volti_(k, iw) * fi[k], eps0);
+      const T flux_out = std::min(dtrp * G.volti_(k, iw) * fo[k], -eps0);
+      const T epsr = eps1 * std::fabs(rscp_low);
+      const T sc_in = std::max(rhos[k] * smax[k] - (rscp_low + epsr) - eps0, (T)0);
+      const T sc_out = std::min(rhos[k] * smin[k] - (rscp_low - epsr) + eps0, (T)0);
+      F2(sin_.data(), k, iw) = std::min((T)1, sc_in / std::max(flux_in, (T)0.01 * sc_in));
+      F2(sout.data(), k, iw) = std::min((T)1, sc_out / std::min(flux_out, (T)0.01 * sc_out));
+    }
+  }
+  // flux renormalisation (1250-1284)
+  for (int j = 0; j < X.g->nw_prog; ++j) {
+    const int iw = X.g->jtw_prog[j];
+    for (int k = G.lpw(iw); k <= mza - 1; ++k) {
+      T sc = std::min(F2(sin_.data(), k + 1, iw), F2(sout.data(), k, iw));
+      if (F2(sfluxwh.data(), k, iw) < (T)0) sc = std::min(F2(sin_.data(), k, iw), F2(sout.data(), k + 1, iw));
+      F2(scp_upw, k, iw) = F2(scp_upw, k, iw) + F2(scp_hiw.data(), k, iw) * sc;
+    }
+  }
+  for (int j = 0; j < X.g->nv_wadj; ++j) {
+    const int iv = X.g->jtv_wadj[j];
+    const int iw1 = G.v_iw(iv, 1), iw2 = G.v_iw(iv, 2);
+    for (int k = G.lpv(iv); k <= mza; ++k) {
+      T sc = std::min(F2(sin_.data(), k, iw2), F2(sout.data(), k, iw1));
+      if (F2(sfluxvh.data(), k, iv) < (T)0) sc = std::min(F2(sin_.data(), k, iw1), F2(sout.data(), k, iw2));
+      F2(scp_upv, k, iv) = F2(scp_upv, k, iv) + F2(scp_hiv.data(), k, iv) * sc;
+    }
+  }
+}
+
 /* prog_wrtv_rk (prog_wrtv_rk.f90:58-488) */
 template <class T>
 static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
   const GridT<T>& G = X.G;
   const olamgpu_opts& o = X.o;
   const int mza = X.mza, mwa = X.mwa, mva = X.mva;
-  if (o.ithil_monot > 0 || o.iwind_monot > 0) return OLAMGPU_E_UNSUPPORTED;
   const R8 dtsm = o.dtsm, dtlm = o.dtlm;
   const size_t wz = (size_t)mza * mwa, vz = (size_t)mza * mva;
   if (!o.divh_damp_short && istp == 1) divh_damp(X, s, s.vmt, dtlm);
@@ -406,6 +581,10 @@ static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
   std::vector<R8> rho0(wz), rth0(wz);
   std::vector<T> wmc0(wz), vmc0(vz), vmca(vz, (T)0);
   std::vector<T> thilt_short(wz), vmxet_short(wz), vmyet_short(wz), vmzet_short(wz), vmt_short(vz);
+  const bool thil_monot = o.ithil_monot > 0, wind_monot = o.iwind_monot > 0;
+  std::vector<T> thl0, vxe0, vye0, vze0;   // start values of the limited fields (186-198)
+  if (thil_monot) thl0.assign(s.thil, s.thil + wz);
+  if (wind_monot) { vxe0.assign(s.vxe, s.vxe + wz); vye0.assign(s.vye, s.vye + wz); vze0.assign(s.vze, s.vze + wz); }
   // column setup (166-253)
   for (int j = 0; j < X.g->nw_prog; ++j) {
     int iw = X.g->jtw_prog[j];
@@ -481,10 +660,24 @@ static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
       if (istage == nrk)
         for (int k = G.lpv(iv); k <= mza; ++k) F2(s.vmasc, k, iv) = F2(s.vmasc, k, iv) + F2(vmca.data(), k, iv);
     }
-    fluxes_wrtv(X, s.thil, thil_upw.data(), thil_upv.data(), s.vmc, s.wmc, o.thil_horiz_adv_order);
-    fluxes_wrtv(X, s.vxe, vxe_upw.data(), vxe_upv.data(), s.vmc, s.wmc, o.wind_horiz_adv_order);
-    fluxes_wrtv(X, s.vye, vye_upw.data(), vye_upv.data(), s.vmc, s.wmc, o.wind_horiz_adv_order);
-    fluxes_wrtv(X, s.vze, vze_upw.data(), vze_upv.data(), s.vmc, s.wmc, o.wind_horiz_adv_order);
+    // (370-399)
+    if (istage == nrk && thil_monot)
+      fluxes_wrtv_monot(X, s.thil, thl0.data(), thilt_short.data(), thil_upw.data(), thil_upv.data(), s.rho,
+                        rho0.data(), vmca.data(), s.wmc, dts, o.thil_horiz_adv_order);
+    else
+      fluxes_wrtv(X, s.thil, thil_upw.data(), thil_upv.data(), s.vmc, s.wmc, o.thil_horiz_adv_order);
+    if (istage == nrk && wind_monot) {
+      fluxes_wrtv_monot(X, s.vxe, vxe0.data(), vmxet_short.data(), vxe_upw.data(), vxe_upv.data(), s.rho,
+                        rho0.data(), vmca.data(), s.wmc, dts, o.wind_horiz_adv_order);
+      fluxes_wrtv_monot(X, s.vye, vye0.data(), vmyet_short.data(), vye_upw.data(), vye_upv.data(), s.rho,
+                        rho0.data(), vmca.data(), s.wmc, dts, o.wind_horiz_adv_order);
+      fluxes_wrtv_monot(X, s.vze, vze0.data(), vmzet_short.data(), vze_upw.data(), vze_upv.data(), s.rho,
+                        rho0.data(), vmca.data(), s.wmc, dts, o.wind_horiz_adv_order);
+    } else {
+      fluxes_wrtv(X, s.vxe, vxe_upw.data(), vxe_upv.data(), s.vmc, s.wmc, o.wind_horiz_adv_order);
+      fluxes_wrtv(X, s.vye, vye_upw.data(), vye_upv.data(), s.vmc, s.wmc, o.wind_horiz_adv_order);
+      fluxes_wrtv(X, s.vze, vze_upw.data(), vze_upv.data(), s.vmc, s.wmc, o.wind_horiz_adv_order);
+    }
 
     // prog_wrt_begs (494-884) for every prognostic column
     for (int j = 0; j < X.g->nw_prog; ++j) {

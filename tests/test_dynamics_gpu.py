@@ -80,6 +80,9 @@ CASES = [
     dict(divh_damp_short=0, vort_damp_short=0),
     dict(thil_order=3, wind_order=3),
     dict(divh_damp_fact=0.0, vort_damp_fact=0.0),
+    dict(ithil_monot=1, iwind_monot=1),
+    dict(ithil_monot=1, thil_order=3, wind_order=3, nrk_wrtv=2),
+    dict(iwind_monot=1, wind_order=3),
 ]
 
 

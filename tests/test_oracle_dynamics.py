@@ -69,3 +69,30 @@ def test_dynamics_vmasc_consistent_with_rho():
     div = flux_divergence(g, o.a["vmasc"], o.a["wmasc"])
     rho_pred = rho0 + 600.0 * g.volti.astype(np.float64) * div
     assert relerr(o.a["rho"][1:, 1:], rho_pred[1:, 1:]) < 1e-6
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(thil_order=3, wind_order=3), dict(nrk_wrtv=2)])
+def test_dynamics_flux_corrected_step(kw):
+    # fluxes_wrtv_monot on the last stage for thil and the winds: mass is
+    # still conserved, the fields stay finite, FP32 tracks FP64, and the
+    # limited step differs from the unlimited one (the limiter is active)
+    g, ds = dyn_case()
+    fg = abi.FortranGrid(g)
+    res = {}
+    for mon in (0, 1):
+        for fp64 in (False, True):
+            opts = abi.make_opts(600.0, nacoust=4, ithil_monot=mon, iwind_monot=mon, **kw)
+            o = oracle_lib.DynOracle(fg, opts, oracle_lib.dyn_arrays(g, ds), fp64=fp64)
+            m0 = (o.a["rho"][1:, 1:] * g.volt[1:, 1:]).sum()
+            _long_step(o, 4)
+            m1 = (o.a["rho"][1:, 1:] * g.volt[1:, 1:]).sum()
+            assert abs(m1 - m0) / m0 < 1e-10
+            for n in ("rho", "thil", "vmc", "wmc", "press", "vxe", "vye", "vze"):
+                assert np.isfinite(o.a[n]).all(), n
+            res[(mon, fp64)] = o
+    lim32, lim64, unl64 = res[(1, False)], res[(1, True)], res[(0, True)]
+    assert relerr(lim32.a["rho"], lim64.a["rho"]) < 1e-6
+    assert relerr(lim32.a["thil"], lim64.a["thil"]) < 1e-5
+    assert relerr(lim32.a["vmc"], lim64.a["vmc"]) < 1e-4
+    assert relerr(lim64.a["thil"], unl64.a["thil"]) > 1e-5
+    assert relerr(lim64.a["vxe"], unl64.a["vxe"]) > 1e-5
