@@ -31,6 +31,8 @@
 // row per level is read ahead from global memory), so the vertical quadratic
 // faces -- linear in those rows with the records' coefficients -- need no
 // staging.
+#include <cudaTypedefs.h>
+
 #include "transport_kernels.cuh"
 #include "tile_common.cuh"
 
@@ -66,6 +68,8 @@ struct TileArgs {
 
 #define TILE_THREADS 256
 #define TILE_NW (TILE_THREADS / 32)
+// polls of a level barrier before a block gives up (seconds at the slowest)
+#define TILE_WAIT_POLLS (1u << 26)
 
 // ---- per-(column, level) weight records, once per long step -------------------
 // Record (TILE_WR floats):
@@ -171,8 +175,11 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
 // same way): two level buffers of U rows (256 B each), two of the tile
 // columns' records, the U rows' global row offsets, the slot byte offsets,
 // the tile columns, their explicit fractions.
-template <int NC>
-__global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
+// OFF: the type of element offsets into the batched arrays -- unsigned when
+// they all fit in 32 bits (fewer address instructions), else long long.
+template <int NC, typename OFF>
+__global__ void __launch_bounds__(TILE_THREADS, 2)
+    k_tile(TileArgs A, const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int T = 16 * NC;
   // the tracer groups of a tile run side by side (its records are read once from HBM)
@@ -181,12 +188,16 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;
-  auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  const size_t ubuf = al((size_t)A.nu_max * 256), rbuf = al((size_t)T * TILE_WR * 4);
-  unsigned char* p = smraw;
+  const int nu4 = (nU + 3) & ~3;      // rows gathered four at a time
+  auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
+  const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * 256), rbuf = al((size_t)T * TILE_WR * 4);
+  // 128-byte aligned start (pointer arithmetic on the shared array keeps the
+  // accesses shared-memory instructions)
+  unsigned char* p = smraw + ((128u - (smem_addr(smraw) & 127u)) & 127u);
+  unsigned long long* BAR = reinterpret_cast<unsigned long long*>(p); p += 128;   // a barrier per level buffer
   char* UB = reinterpret_cast<char*>(p);              p += 2 * ubuf;
   unsigned char* RBB = p;                             p += 2 * rbuf;
-  long long* ROW = reinterpret_cast<long long*>(p);   p += al((size_t)A.nu_max * 8);
+  int* RIDX = reinterpret_cast<int*>(p);              p += al((size_t)(A.nu_max + 3) * 4);
   int* SLOT = reinterpret_cast<int*>(p);              p += al((size_t)T * TILE_NS * 4);
   int* IWT = reinterpret_cast<int*>(p);               p += al((size_t)T * 4);
   float* FEX = reinterpret_cast<float*>(p);
@@ -208,11 +219,16 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       if (v < 1 || v >= A.mwa) bad = 4;
       IWT[i] = v;
     }
-    for (int i = tid; i < nU; i += TILE_THREADS) {
-      const int v = __ldg(A.ulist + u_off + i);
+    for (int i = tid; i < nu4; i += TILE_THREADS) {
+      const int v = __ldg(A.ulist + u_off + (i < nU ? i : 0));   // padding rows repeat row 0
       if (v < 1 || v >= A.mwa) bad = 8;
-      ROW[i] = (long long)v * mza * ntp + t0;
+      RIDX[i] = v * mza;
     }
+  }
+  if (tid == 0) {
+    mbar_init(&BAR[0], TILE_NW);
+    mbar_init(&BAR[1], TILE_NW);
+    mbar_init_fence();
   }
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
@@ -221,20 +237,27 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   for (int i = tid; i < nT; i += TILE_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
   const int seg = min(64, ntp - t0);  // tracers of this group (a multiple of 4)
-  const int nch = seg >> 2;
-  const int ch = tid & 15;            // the 16-byte chunk of every row this thread copies
-  // level k into buffer b: the U rows, then the tile columns' records
+  // level k into buffer b, completing on barrier b: warp w's lane 0 gathers
+  // the U-row quadruples w, w + 8, ... (TMA, 256 B per row) and the records
+  // of tile columns 4w .. 4w+3
   auto stage = [&](int k, int b) {
+    if (lane != 0) return;
+    const int ng = nu4 >> 2, nr = (nT + 3) >> 2;
+    const int myg = warp < ng ? (ng - warp + TILE_NW - 1) / TILE_NW : 0;
+    const int myr = warp < nr ? 1 : 0;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * 256 + myr * 4 * TILE_WR * 4));
     char* Ub = UB + b * ubuf;
-    float* Rb = reinterpret_cast<float*>(RBB + b * rbuf);
-    const long long koff = (long long)k * ntp + ch * 4;
-    if (ch < nch)
-      for (int r = tid >> 4; r < nU; r += TILE_THREADS / 16) cp_async16(Ub + r * 256 + ch * 16, A.S + ROW[r] + koff);
-    for (int i = tid; i < nT * (TILE_WR / 4); i += TILE_THREADS) {
-      const int c = i / (TILE_WR / 4), q = i - c * (TILE_WR / 4);
-      cp_async16(Rb + c * TILE_WR + q * 4, A.wrec + ((size_t)IWT[c] * mza + k) * TILE_WR + q * 4);
+    for (int g = warp; g < ng; g += TILE_NW) {
+      const int* r = RIDX + 4 * g;
+      tma_gather4(Ub + 4 * g * 256, &tmS, t0, r[0] + k, r[1] + k, r[2] + k, r[3] + k, &BAR[b]);
     }
-    cp_async_commit();
+    if (myr) {
+      const int c0 = 4 * warp;
+      const int y0 = IWT[c0] * mza, y1 = IWT[min(c0 + 1, nT - 1)] * mza;
+      const int y2 = IWT[min(c0 + 2, nT - 1)] * mza, y3 = IWT[min(c0 + 3, nT - 1)] * mza;
+      tma_gather4(RBB + b * rbuf + c0 * TILE_WR * 4, &tmR, 0, y0 + k, y1 + k, y2 + k, y3 + k, &BAR[b]);
+    }
   };
 
   // a half warp per column (columns cb, cb + 16, ...): lane hl holds tracers
@@ -244,7 +267,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
   const bool act = 4 * hl < seg;
   const int cb = 2 * warp + half;
   F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], s00[NC], st[NC];
-  long long cbase[NC];
+  OFF cbase[NC];
   stage(kb, 0);
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
@@ -252,20 +275,21 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
     m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = s00[n] = st[n] = zero4();
     cbase[n] = 0;
     if (c < nT && act) {
-      cbase[n] = (long long)IWT[c] * mza * ntp + t0 + 4 * hl;
-      const float* q = A.S + cbase[n];
-      if (kb + 1 < mza) p1[n] = ldg4(q + (long long)(kb + 1) * ntp);
-      if (kb + 2 < mza) p2[n] = ldg4(q + (long long)(kb + 2) * ntp);
-      if (kb + 3 < mza) p3[n] = ldg4(q + (long long)(kb + 3) * ntp);
-      s00[n] = ldg4(A.S0 + cbase[n] + (long long)kb * ntp);
-      st[n] = ldg4(A.SCT + cbase[n] + (long long)kb * ntp);
+      cbase[n] = (OFF)IWT[c] * (OFF)mza * (OFF)ntp + (OFF)(t0 + 4 * hl);
+      if (kb + 1 < mza) p1[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 1) * (OFF)ntp));
+      if (kb + 2 < mza) p2[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 2) * (OFF)ntp));
+      if (kb + 3 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 3) * (OFF)ntp));
+      s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)kb * (OFF)ntp));
+      st[n] = ldg4(A.SCT + (cbase[n] + (OFF)kb * (OFF)ntp));
     }
   }
-  cp_async_wait_all();
-  __syncthreads();
-
+  __syncthreads();   // the explicit fractions
+  // a level's copies are waited for at most TILE_WAIT_POLLS polls; a block
+  // whose copies never complete records it and stops at the level's end
+  int failed = 0;
   for (int kd = kb; kd < mza; ++kd) {
-    const int cur = (kd - kb) & 1;
+    const int lv = kd - kb, cur = lv & 1;
+    if (!mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS)) failed = 1;
     if (kd + 1 < mza) stage(kd + 1, cur ^ 1);
     const char* Ul = UB + cur * ubuf + hl * 16;
     const float* Rc = reinterpret_cast<const float*>(RBB + cur * rbuf);
@@ -301,21 +325,55 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A) {
       // scp = scp0 + dtr * (sct + volti * (fluxdiv + fexpl * vflux)) / rhos
       const F4 o = fma4s(A.dtr * r5.y, fd, fma4s(A.dtr * r5.z, st[n], s00[n]));
       if (act) {
-        stg4(A.OUT + cbase[n] + (long long)kd * ntp, o);
+        stg4(A.OUT + (cbase[n] + (OFF)kd * (OFF)ntp), o);
         if (kd == kb)
-          for (int k2 = 0; k2 < kb; ++k2) stg4(A.OUT + cbase[n] + (long long)k2 * ntp, o);
+          for (int k2 = 0; k2 < kb; ++k2) stg4(A.OUT + (cbase[n] + (OFF)k2 * (OFF)ntp), o);
         // slide the column's window up one level and read ahead
         m2[n] = m1[n]; m1[n] = s0; p1[n] = p2[n]; p2[n] = p3[n];
-        if (kd + 4 < mza) p3[n] = ldg4(A.S + cbase[n] + (long long)(kd + 4) * ntp);
+        if (kd + 4 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(kd + 4) * (OFF)ntp));
         if (kd + 1 < mza) {
-          s00[n] = ldg4(A.S0 + cbase[n] + (long long)(kd + 1) * ntp);
-          st[n] = ldg4(A.SCT + cbase[n] + (long long)(kd + 1) * ntp);
+          s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
+          st[n] = ldg4(A.SCT + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
         }
       }
     }
-    cp_async_wait_all();
-    __syncthreads();
+    if (__syncthreads_or(failed)) {
+      if (tid == 0 && atomicCAS(A.err, 0, 130) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = kd; }
+      return;
+    }
   }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+
+// a 2-D map over nrows rows of width floats with boxes of one row of box
+// floats, for four-row gathers
+static int row_map(CUtensorMap* m, const float* base, int width, size_t nrows, int box) {
+  auto enc = tmap_encoder();
+  if (!enc) { set_error("cuTensorMapEncodeTiled is not available"); return OLAMGPU_E_CUDA; }
+  const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)nrows};
+  const cuuint64_t strides[1] = {(cuuint64_t)width * sizeof(float)};
+  const cuuint32_t boxd[2] = {(cuuint32_t)box, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, boxd, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return OLAMGPU_E_CUDA; }
+  return OLAMGPU_OK;
 }
 
 bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
@@ -341,13 +399,18 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, d.mza);
   const unsigned ngrp = (unsigned)((ntp + 63) / 64);
   const unsigned nblk = (unsigned)d.ntiles * ngrp;
-  if (d.tile_T == 32) {
-    OG_CUDA(cudaFuncSetAttribute(k_tile<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile<2><<<nblk, TILE_THREADS, smem, s>>>(A);
-  } else {
-    OG_CUDA(cudaFuncSetAttribute(k_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile<1><<<nblk, TILE_THREADS, smem, s>>>(A);
-  }
+  // element offsets in 32 bits when every array of the batched layout fits
+  const bool off32 = (double)d.mwa * d.mza * ntp < 4294967296.0;
+  alignas(64) CUtensorMap tmS, tmR;
+  OG_CHECK(row_map(&tmS, S, ntp, (size_t)d.mwa * d.mza, 64));
+  OG_CHECK(row_map(&tmR, tp.wrec.p, TILE_WR, (size_t)d.mwa * d.mza, TILE_WR));
+  auto go = [&](auto kern) -> int {
+    OG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<nblk, TILE_THREADS, smem, s>>>(A, tmS, tmR);
+    return OLAMGPU_OK;
+  };
+  if (d.tile_T == 32) OG_CHECK(off32 ? go(k_tile<2, unsigned>) : go(k_tile<2, long long>));
+  else OG_CHECK(off32 ? go(k_tile<1, unsigned>) : go(k_tile<1, long long>));
   OG_LAUNCHED();
   return OLAMGPU_OK;
 }
