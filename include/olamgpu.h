@@ -160,6 +160,7 @@ enum {
   OLAMGPU_F_VMC = 1u << 6,   OLAMGPU_F_VC = 1u << 7,    OLAMGPU_F_VMASC = 1u << 8,
   OLAMGPU_F_WMASC = 1u << 9, OLAMGPU_F_TEND = 1u << 10, OLAMGPU_F_FACS = 1u << 11,
   OLAMGPU_F_SCALARS = 1u << 12, OLAMGPU_F_SCALAR_TEND = 1u << 13,
+  OLAMGPU_F_EDDY = 1u << 14,     /* the olamgpu_eddy arrays                     */
   OLAMGPU_F_ALL = 0xffffu
 };
 
@@ -189,6 +190,42 @@ int olamgpu_register_scalars(int num_scalar, float* const* var_p,
  * (scalar_transport_rk.F90:244-274): akhodx (mza, mva), khtopv (mva).
  * Without them diffusion is inactive, as with OLAM's idiffk = 0. */
 int olamgpu_set_turb(const float* akhodx, const int* khtopv);
+
+/* ---- eddy diffusion inside the acoustic step ------------------------------
+ * Inputs that OLAM's PBL scheme leaves in mem_turb each long step, the
+ * comp_horiz_k outputs, and the grid / option values the column solves
+ * read (convect/pbl_driver.f90:136-238, 519-742; modules/mem_rayf.f90:
+ * 177-220; omodel/prog_wrtv_rk.f90:214-251).  Host arrays in OLAM layout,
+ * read (and for comp_horiz_k written) at the sync points like the state. */
+typedef struct olamgpu_eddy {
+  float* vkm;    float* vkh;       /* (mza, mwa) eddy viscosity / heat diffusivity */
+  float* agamma;                   /* (mza, mwa) non-local heat term (idiffk = 1)  */
+  float* akm_sfc;                  /* (nsw_max, mwa) surface momentum exchange     */
+  float* sfluxt;                   /* (mwa) surface sensible heat flux [W m^-2]    */
+  int*   kmtop;  int* khtop; int* kpblh;      /* (mwa) 1-based levels             */
+  float* theta;  float* tair;      /* (mza, mwa)                                   */
+  float* akmodx; float* akhodx;    /* (mza, mva) comp_horiz_k outputs              */
+  int*   kmtopv; int* khtopv;      /* (mva)     comp_horiz_k outputs               */
+  const int* lsw; int nsw_max;     /* (mwa) levels in contact with the surface     */
+  const int* mrlw; const int* mrlv;              /* (mwa), (mva) itab_w/v%mrl*     */
+  int mrls; const int* idiffk; const float* akmin;   /* (mrls) namelist values    */
+  int test_case;                   /* DCMIP cases 110-114, 121, 122 mix elsewhere  */
+  float cp;                        /* consts_coms cp                               */
+  int krayfmix_bot;                /* first level of rayf_cofmix                   */
+  const float* rayf_cofmix;        /* (mza) or NULL: no top-level wind mixing      */
+} olamgpu_eddy;
+
+/* Registers the eddy-diffusion inputs (NULL: off, as with idiffk = 0).  From
+ * then on prog_wrtv_rk adds, in each call's column set-up, the implicit
+ * vertical heat and momentum diffusion (solve_eddy_diff_heat / _vxe), the
+ * top-level wind mixing (rayf_mix_top_vxe) and the horizontal diffusion of
+ * thil and the winds. */
+int olamgpu_set_eddy(const olamgpu_eddy* eddy);
+
+/* Replaces comp_horiz_k (pbl_driver.f90:136-238): akmodx, akhodx, kmtopv,
+ * khtopv from vkm, vkh, kmtop, khtop and rho, for every V point of
+ * jtv_wadj. */
+int olamgpu_comp_horiz_k(void);
 
 int olamgpu_finalize(void);
 const char* olamgpu_strerror(int status);

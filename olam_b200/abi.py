@@ -22,7 +22,7 @@ SYNC_EACH_CALL, RESIDENT = 0, 1
 TRANSPORT_FUSED, TRANSPORT_PLAIN, TRANSPORT_FUSED_COLUMN = 0, 1, 2
 
 F_RHO, F_PRESS, F_THIL, F_WC, F_WMC, F_VXE, F_VMC, F_VC = (1 << i for i in range(8))
-F_VMASC, F_WMASC, F_TEND, F_FACS, F_SCALARS, F_SCALAR_TEND = (1 << i for i in range(8, 14))
+F_VMASC, F_WMASC, F_TEND, F_FACS, F_SCALARS, F_SCALAR_TEND, F_EDDY = (1 << i for i in range(8, 15))
 F_ALL = 0xFFFF
 
 
@@ -88,6 +88,45 @@ class State(C.Structure):
         ("thilt", c_float_p), ("vmxet", c_float_p), ("vmyet", c_float_p), ("vmzet", c_float_p),
         ("vmt", c_float_p),
     ]
+
+
+class Eddy(C.Structure):
+    """olamgpu_eddy: the acoustic step's eddy-diffusion inputs."""
+    _fields_ = [
+        ("vkm", c_float_p), ("vkh", c_float_p), ("agamma", c_float_p), ("akm_sfc", c_float_p),
+        ("sfluxt", c_float_p), ("kmtop", c_int_p), ("khtop", c_int_p), ("kpblh", c_int_p),
+        ("theta", c_float_p), ("tair", c_float_p), ("akmodx", c_float_p), ("akhodx", c_float_p),
+        ("kmtopv", c_int_p), ("khtopv", c_int_p), ("lsw", c_int_p), ("nsw_max", C.c_int),
+        ("mrlw", c_int_p), ("mrlv", c_int_p), ("mrls", C.c_int), ("idiffk", c_int_p),
+        ("akmin", c_float_p), ("test_case", C.c_int), ("cp", C.c_float),
+        ("krayfmix_bot", C.c_int), ("rayf_cofmix", c_float_p),
+    ]
+
+
+def make_eddy(d):
+    """An Eddy struct over the arrays of dict ``d`` (kept referenced by the
+    returned struct's ``keep`` attribute)."""
+    e = Eddy()
+    keep = {}
+    for name, ct in (("vkm", C.c_float), ("vkh", C.c_float), ("agamma", C.c_float),
+                     ("akm_sfc", C.c_float), ("sfluxt", C.c_float), ("kmtop", C.c_int),
+                     ("khtop", C.c_int), ("kpblh", C.c_int), ("theta", C.c_float),
+                     ("tair", C.c_float), ("akmodx", C.c_float), ("akhodx", C.c_float),
+                     ("kmtopv", C.c_int), ("khtopv", C.c_int), ("lsw", C.c_int), ("mrlw", C.c_int),
+                     ("mrlv", C.c_int), ("idiffk", C.c_int), ("akmin", C.c_float),
+                     ("rayf_cofmix", C.c_float)):
+        a = d.get(name)
+        if a is None:
+            continue
+        dt = np.int32 if ct is C.c_int else np.float32
+        a = np.ascontiguousarray(a, dtype=dt)
+        d[name] = a
+        keep[name] = a
+        setattr(e, name, ptr(a, ct))
+    e.nsw_max, e.mrls, e.test_case = int(d["nsw_max"]), int(d["mrls"]), int(d["test_case"])
+    e.cp, e.krayfmix_bot = float(d["cp"]), int(d["krayfmix_bot"])
+    e.keep = keep
+    return e
 
 
 class CflDiag(C.Structure):

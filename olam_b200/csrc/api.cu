@@ -284,6 +284,10 @@ int olamgpu_set_turb(const float* akhodx, const int* khtopv) {
   return OLAMGPU_OK;
 }
 
+int olamgpu_set_eddy(const olamgpu_eddy* eddy) { return dyn_eddy_set(eddy); }
+
+int olamgpu_comp_horiz_k(void) { return dyn_comp_horiz_k(); }
+
 int olamgpu_finalize(void) {
   Context& C = ctx();
   if (C.stream) cudaStreamSynchronize(C.stream);
@@ -331,6 +335,7 @@ int olamgpu_sync_to_device(unsigned fieldmask) {
   if (C.have_state) {
     if (C.dy.ready) {
       OG_CHECK(dyn_state_to_device(fieldmask, s));
+      if (fieldmask & OLAMGPU_F_EDDY) OG_CHECK(dyn_eddy_to_device(s));
     } else {
       if ((fieldmask & OLAMGPU_F_VMASC) && C.hstate.vmasc) OG_CHECK(upload(C.tp.vmasc, C.hstate.vmasc, vz, s));
       if ((fieldmask & OLAMGPU_F_WMASC) && C.hstate.wmasc) OG_CHECK(upload(C.tp.wmasc, C.hstate.wmasc, wz, s));
@@ -359,6 +364,7 @@ int olamgpu_sync_to_host(unsigned fieldmask) {
   if (C.have_state) {
     if (C.dy.ready) {
       OG_CHECK(dyn_state_to_host(fieldmask, s));
+      if (fieldmask & OLAMGPU_F_EDDY) OG_CHECK(dyn_eddy_to_host(s));
     } else {
       const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva;
       auto cp = [&](void* h, const void* dv, size_t b) -> int {

@@ -15,6 +15,8 @@
 //                           tridiagonal solve (tridiffo, tridiag_lib.f90:10-36)
 //   k_prog_v                prog_v_begs (:888-946)
 //   k_vel_t3d               vel_t3d_hex (vel_t3d.f90:39-108)
+// With eddy diffusion registered, dynamics_eddy.cu's k_eddy_w follows
+// k_setup_w (the vertical and horizontal eddy terms of :214-251).
 // Precision as declared by OLAM: rho, press and the implicit weights are
 // double; every other field is float.  Device level kd = Fortran k - 1.
 #include <cmath>
@@ -891,7 +893,10 @@ int dyn_prog_wrtv_rk(int istp) {
   if (o.nrk_wrtv != 2 && o.nrk_wrtv != 3) { set_error("acoust_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
   cudaStream_t s = C.stream;
   OG_CHECK(ensure_dyn_buffers(C));
-  if (C.coherence == OLAMGPU_SYNC_EACH_CALL || !C.dy.uploaded) OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL || !C.dy.uploaded) {
+    OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s));
+    OG_CHECK(dyn_eddy_to_device(s));
+  }
   C.dy.uploaded = true;
   const DevGrid& d = C.g;
   Dyn& y = C.dy;
@@ -906,12 +911,18 @@ int dyn_prog_wrtv_rk(int istp) {
   SetupW sw{tp.rho.p, y.thil.p, y.wmc.p, y.thilt.p, y.vmxet.p, y.vmyet.p, y.vmzet.p, y.volt.p, y.rho0.p,
             y.rth0.p, y.wmc0.p, y.sh_th.p, y.sh_vx.p, y.sh_vy.p, y.sh_vz.p, y.rayf_cof.p, y.dn01d.p, y.th01d.p,
             o.krayf_bot};
-  if (!(o.rayf_cof && o.initial == 1)) sw.rayf_cof = nullptr;
+  const bool rayleigh_th = o.rayf_cof && o.initial == 1;
+  // with eddy diffusion the Rayleigh term on thil follows the eddy terms
+  if (!rayleigh_th || y.eddy_on) sw.rayf_cof = nullptr;
   k_setup_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, sw);
   k_setup_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.vmc.p, y.vmt.p, y.vmc0.p, y.sh_vmt.p,
                                 (o.rayf_cof && o.vc03d) ? y.rayf_cof.p : nullptr, y.vc03d.p, y.vc.p, tp.rho.p,
                                 o.krayf_bot);
   OG_LAUNCHED(); OG_LAUNCHED();
+  if (y.eddy_on) {
+    OG_PROF("eddy_columns", s);
+    OG_CHECK(dyn_eddy_columns(C, rayleigh_th, s));
+  }
   if (o.divh_damp_short) divh_damp(C, y.sh_vmt.p, o.dtsm, s);
   if (o.vort_damp_short) vort_damp(C, y.sh_vmt.p, o.dtsm, s);
   // start values of the fields fluxes_wrtv_monot limits (prog_wrtv_rk.f90:186-198)
@@ -1064,6 +1075,7 @@ void dyn_release() {
                         &y.m_sfv, &y.m_sin, &y.m_sout};
   for (auto* b : f) b->release();
   y.lpmmin.release();
+  dyn_eddy_release();
   y = Dyn();
 }
 

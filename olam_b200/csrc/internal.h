@@ -255,6 +255,14 @@ struct Dyn {
   // fields, and scratch shared by the fields in turn
   DevBuf<float> th0, vx0, vy0, vz0;
   DevBuf<float> m_scpt, m_gx, m_hiw, m_sfw, m_hiv, m_sfv, m_sin, m_sout;
+  // eddy diffusion (dynamics_eddy.cu): the registered host arrays and their
+  // device copies; hk_on_device: comp_horiz_k's outputs were last written
+  // on the device (host copies stale until a sync to the host)
+  bool eddy_on = false, hk_on_device = false;
+  olamgpu_eddy heddy{};
+  DevBuf<float> e_vkm, e_vkh, e_agamma, e_theta, e_tair, e_akm_sfc, e_sfluxt, e_akmodx, e_akhodx;
+  DevBuf<float> e_dzim, e_dztbi, e_akmin, e_rayf;
+  DevBuf<int> e_kmtop, e_khtop, e_kpblh, e_kmtopv, e_khtopv, e_lsw, e_mrlw, e_mrlv, e_idiffk;
 };
 
 struct Context {
@@ -299,6 +307,15 @@ int dyn_state_to_host(unsigned mask, cudaStream_t s);
 void dyn_release();
 // the flux-corrected face values of field 0 (thil) .. 3 (vze) on the last
 // RK stage (dynamics_monot.cu): scp, its start value, its *_short tendency
+int dyn_eddy_set(const olamgpu_eddy* e);
+int dyn_eddy_to_device(cudaStream_t s);
+int dyn_eddy_to_host(cudaStream_t s);
+int dyn_comp_horiz_k();
+// the eddy-diffusion column terms on sh_th / sh_vx / sh_vy / sh_vz after
+// k_setup_w; with rayleigh, also the Rayleigh term on thil (which k_setup_w
+// then leaves out, so that the terms add in the reference's order)
+int dyn_eddy_columns(Context& C, bool rayleigh, cudaStream_t s);
+void dyn_eddy_release();
 int dyn_monot_faces(Context& C, int field, const float* scp, const float* scp0, const float* sct, float dts,
                     int ord, cudaStream_t s);
 

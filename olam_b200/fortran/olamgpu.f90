@@ -26,7 +26,8 @@ module olamgpu_c
                                OLAMGPU_F_VMC = 64, OLAMGPU_F_VC = 128, OLAMGPU_F_VMASC = 256, &
                                OLAMGPU_F_WMASC = 512, OLAMGPU_F_TEND = 1024,                &
                                OLAMGPU_F_FACS = 2048, OLAMGPU_F_SCALARS = 4096,            &
-                               OLAMGPU_F_SCALAR_TEND = 8192, OLAMGPU_F_ALL = 65535
+                               OLAMGPU_F_SCALAR_TEND = 8192, OLAMGPU_F_EDDY = 16384,       &
+                               OLAMGPU_F_ALL = 65535
 
   type, bind(C) :: olamgpu_grid
      integer(c_int) :: mza, mwa, mva, mma
@@ -69,6 +70,19 @@ module olamgpu_c
      type(c_ptr) :: rho, press, thil, wc, wmc, vxe, vye, vze, vmc, vc, vmasc, wmasc
      type(c_ptr) :: alpha_press, pwfac, pvfac, thilt, vmxet, vmyet, vmzet, vmt
   end type olamgpu_state
+
+  type, bind(C) :: olamgpu_eddy
+     type(c_ptr) :: vkm, vkh, agamma, akm_sfc, sfluxt, kmtop, khtop, kpblh, theta, tair
+     type(c_ptr) :: akmodx, akhodx, kmtopv, khtopv, lsw
+     integer(c_int) :: nsw_max
+     type(c_ptr) :: mrlw, mrlv
+     integer(c_int) :: mrls
+     type(c_ptr) :: idiffk, akmin
+     integer(c_int) :: test_case
+     real(c_float) :: cp
+     integer(c_int) :: krayfmix_bot
+     type(c_ptr) :: rayf_cofmix
+  end type olamgpu_eddy
 
   interface
      integer(c_int) function olamgpu_init(grid, opts, state) bind(C, name="olamgpu_init")
@@ -119,6 +133,13 @@ module olamgpu_c
        real(c_float), intent(out) :: rho_old(*)
      end function
      integer(c_int) function olamgpu_timeavg_momsc() bind(C, name="olamgpu_timeavg_momsc")
+       import :: c_int
+     end function
+     integer(c_int) function olamgpu_set_eddy(eddy) bind(C, name="olamgpu_set_eddy")
+       import :: c_int, olamgpu_eddy
+       type(olamgpu_eddy), intent(in) :: eddy
+     end function
+     integer(c_int) function olamgpu_comp_horiz_k() bind(C, name="olamgpu_comp_horiz_k")
        import :: c_int
      end function
      integer(c_int) function olamgpu_finalize() bind(C, name="olamgpu_finalize")
@@ -179,7 +200,7 @@ module olamgpu_shim
   implicit none
 
   private
-  public :: olamgpu_shim_init, olamgpu_shim_scalars
+  public :: olamgpu_shim_init, olamgpu_shim_scalars, olamgpu_shim_eddy
 
   ! packed copies of OLAM's derived-type tables (kept for the run)
   integer(c_int), allocatable, target, save :: npoly_p(:), iwglobe_p(:)
@@ -191,6 +212,8 @@ module olamgpu_shim
   integer(c_int), allocatable, target, save :: jtw_p(:), jtw_a(:), jtv_p(:), jtv_a(:), jtm_p(:)
   type(c_ptr),    allocatable, target, save :: vp(:), vt(:)
   integer(c_int), allocatable, target, save :: pdef_p(:), sgs_p(:)
+  integer(c_int), allocatable, target, save :: mrlw_p(:), mrlv_p(:), idiffk_p(:)
+  real(c_float),  allocatable, target, save :: akmin_p(:)
 
 contains
 
@@ -320,5 +343,50 @@ contains
     call olamgpu_check(olamgpu_register_scalars(int(num_scalar, c_int), vp, vt, pdef_p, sgs_p), &
                        'register_scalars')
   end subroutine olamgpu_shim_scalars
+
+  ! eddy diffusion inside the acoustic step: mem_turb's PBL arrays and
+  ! comp_horiz_k outputs, the refinement levels of itab_w / itab_v, and the
+  ! namelist values solve_eddy_diff_heat / _vxe and rayf_mix_top_vxe read
+  ! (pbl_driver.f90:136-238, 519-742; mem_rayf.f90:177-220).  Call once
+  ! after the PBL arrays are allocated; with the RESIDENT coherence, sync
+  ! OLAMGPU_F_EDDY to the device after each PBL update.
+  subroutine olamgpu_shim_eddy()
+    use mem_turb,    only: vkm, vkh, agamma, akm_sfc, sfluxt, kmtop, khtop, kpblh, &
+                           akmodx, akhodx, kmtopv, khtopv
+    use mem_basic,   only: theta, tair
+    use mem_grid,    only: mwa, mva, lsw, nsw_max
+    use mem_ijtabs,  only: itab_w, itab_v, mrls
+    use misc_coms,   only: akmin
+    use oname_coms,  only: nl
+    use consts_coms, only: cp
+    use mem_rayf,    only: rayf_cofmix, krayfmix_bot, dorayfmix
+
+    type(olamgpu_eddy), save :: e
+    integer :: iw, iv
+
+    allocate(mrlw_p(mwa), mrlv_p(mva), idiffk_p(mrls), akmin_p(mrls))
+    do iw = 1, mwa
+       mrlw_p(iw) = max(1, itab_w(iw)%mrlw)
+    enddo
+    do iv = 1, mva
+       mrlv_p(iv) = max(1, itab_v(iv)%mrlv)
+    enddo
+    idiffk_p = nl%idiffk(1:mrls)
+    akmin_p = akmin(1:mrls)
+    e%vkm = addr_r4(vkm); e%vkh = addr_r4(vkh); e%agamma = addr_r4(agamma)
+    e%akm_sfc = addr_r4(akm_sfc); e%sfluxt = addr_r4(sfluxt)
+    e%kmtop = addr_i4(kmtop); e%khtop = addr_i4(khtop); e%kpblh = addr_i4(kpblh)
+    e%theta = addr_r4(theta); e%tair = addr_r4(tair)
+    e%akmodx = addr_r4(akmodx); e%akhodx = addr_r4(akhodx)
+    e%kmtopv = addr_i4(kmtopv); e%khtopv = addr_i4(khtopv)
+    e%lsw = addr_i4(lsw); e%nsw_max = nsw_max
+    e%mrlw = c_loc(mrlw_p); e%mrlv = c_loc(mrlv_p); e%mrls = mrls
+    e%idiffk = c_loc(idiffk_p); e%akmin = c_loc(akmin_p)
+    e%test_case = nl%test_case; e%cp = cp
+    e%krayfmix_bot = krayfmix_bot
+    e%rayf_cofmix = c_null_ptr
+    if (dorayfmix) e%rayf_cofmix = addr_r4(rayf_cofmix)
+    call olamgpu_check(olamgpu_set_eddy(e), 'set_eddy')
+  end subroutine olamgpu_shim_eddy
 
 end module olamgpu_shim

@@ -26,7 +26,7 @@ EXPORTS = [
     "olamgpu_set_transport_form", "olamgpu_scalar_transport_rk", "olamgpu_prog_wrtv_rk",
     "olamgpu_tend0", "olamgpu_timeavg_momsc", "olamgpu_stream", "olamgpu_launch_count",
     "olamgpu_profile", "olamgpu_profile_read", "olamgpu_update_scalar_noalloc",
-    "olamgpu_scalar_transport_rk_adjoint",
+    "olamgpu_scalar_transport_rk_adjoint", "olamgpu_set_eddy", "olamgpu_comp_horiz_k",
 ]
 
 
@@ -68,6 +68,8 @@ def load():
     lib.olamgpu_update_scalar_noalloc.argtypes = [C.c_void_p] * 6 + [C.c_float, C.c_void_p, C.c_void_p]
     lib.olamgpu_scalar_transport_rk_adjoint.argtypes = [abi.c_float_p, C.POINTER(abi.c_float_p),
                                                         C.POINTER(abi.c_float_p)]
+    lib.olamgpu_set_eddy.argtypes = [C.POINTER(abi.Eddy)]
+    lib.olamgpu_comp_horiz_k.argtypes = []
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
             getattr(lib, name).restype = C.c_int
@@ -155,6 +157,15 @@ class OlamGpu:
 
     def timeavg_momsc(self):
         check(self.lib.olamgpu_timeavg_momsc())
+
+    def set_eddy(self, eddy):
+        """Register the eddy-diffusion inputs (an ``abi.Eddy``; None: off).
+        The struct and its arrays must stay alive while registered."""
+        self._eddy = eddy
+        check(self.lib.olamgpu_set_eddy(C.byref(eddy) if eddy is not None else None))
+
+    def comp_horiz_k(self):
+        check(self.lib.olamgpu_comp_horiz_k())
 
     # -- library controls --------------------------------------------------------
     def set_coherence(self, mode):

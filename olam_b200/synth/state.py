@@ -264,3 +264,52 @@ def fast_lognormal_tracers(g, ntr, seed=2024, median=1.0e-8, sigma_ln=1.5,
         q[0] = 0.0
         q[:, 0] = q[:, 1]
     return out
+
+
+def eddy_inputs(g, rho, thil, press, akmin=0.0, idiffk=1, rayf_mix=False, seed=7):
+    """Seeded stand-ins for the PBL scheme's outputs that the acoustic step's
+    eddy diffusion reads (convect/mem_turb.f90 arrays, OLAM layout): a
+    boundary layer 0.8-1.6 km deep with K(z) = Kmax (z/h)(1 - z/h)^2 scaled
+    by density, a small non-local heat term, a surface heat flux and a
+    surface momentum exchange on the lowest level.  Returns a dict of
+    numpy arrays and scalars for ``abi.make_eddy``."""
+    rng = np.random.default_rng(seed)
+    mwa, mza, mva = g.mwa, g.mza, g.mva
+    zm = g.zm.astype(np.float64)                       # W-level heights, Fortran k = index + 1
+    h = rng.uniform(800.0, 1600.0, mwa)                 # boundary-layer depth per column
+    kmax_m, kmax_h = rng.uniform(20.0, 60.0, mwa), rng.uniform(25.0, 80.0, mwa)
+    z = zm[None, :] / h[:, None]
+    shape = np.where((z > 0) & (z < 1), z * (1 - z) ** 2 * 6.75, 0.0)   # peak 1 at z = h/3
+    rhow = rho.astype(np.float64)
+    vkm = (rhow * kmax_m[:, None] * shape).astype(F32)
+    vkh = (rhow * kmax_h[:, None] * shape).astype(F32)
+    # top W level (1-based) with a nonzero coefficient
+    top = np.array([int(np.max(np.nonzero(shape[i] > 0)[0])) + 1 if (shape[i] > 0).any() else 0
+                    for i in range(mwa)], np.int32)
+    kpblh = np.maximum(top - 1, 1).astype(np.int32)
+    agamma = (1.0e-3 * g.arw.astype(np.float64) * np.clip(1 - z, 0, 1) * (z > 0)).astype(F32)
+    sfluxt = rng.uniform(50.0, 200.0, mwa).astype(F32)
+    theta = thil.astype(F32).copy()
+    tair = (theta.astype(np.float64) * (np.maximum(press, 1.0) / P00) ** ROCP).astype(F32)
+    nsw_max = 1
+    akm_sfc = rng.uniform(0.01, 0.05, (mwa, nsw_max)).astype(F32)
+    for a in (vkm, vkh, agamma, theta, tair):
+        a[0] = 0
+    sfluxt[0] = 0
+    akm_sfc[0] = 0
+    top[0] = 0
+    kpblh[0] = 0
+    rayf = None
+    krayfmix_bot = mza + 1
+    if rayf_mix:
+        krayfmix_bot = mza - 2
+        rayf = np.zeros(mza, F32)
+        rayf[krayfmix_bot - 1:mza - 1] = np.array([0.02, 0.05], F32)   # m/s, like K / dz
+    return dict(vkm=vkm, vkh=vkh, agamma=agamma, akm_sfc=akm_sfc, sfluxt=sfluxt, kmtop=top.copy(),
+                khtop=top.copy(), kpblh=kpblh, theta=theta, tair=tair,
+                akmodx=np.zeros((mva, mza), F32), akhodx=np.zeros((mva, mza), F32),
+                kmtopv=np.ones(mva, np.int32), khtopv=np.ones(mva, np.int32),
+                lsw=np.ones(mwa, np.int32), nsw_max=nsw_max, mrlw=np.ones(mwa, np.int32),
+                mrlv=np.ones(mva, np.int32), mrls=1, idiffk=np.array([idiffk], np.int32),
+                akmin=np.array([akmin], F32), test_case=0, cp=CP, krayfmix_bot=krayfmix_bot,
+                rayf_cofmix=rayf)

@@ -8,6 +8,11 @@
  *   prog_wrt_begs          omodel/prog_wrtv_rk.f90:494-884
  *   prog_v_begs            omodel/prog_wrtv_rk.f90:888-946
  *   fluxes_wrtv            omodel/prog_wrtv_rk.f90:950-1129
+ *   eddy diffusion         convect/pbl_driver.f90:136-238 (comp_horiz_k),
+ *                          519-742 (solve_eddy_diff_heat / _vxe),
+ *                          modules/mem_rayf.f90:177-220 (rayf_mix_top_vxe),
+ *                          outils/tridiag_lib.f90:40-104 (tridv),
+ *                          omodel/prog_wrtv_rk.f90:214-251 (their calls)
  *   fluxes_wrtv_monot      omodel/prog_wrtv_rk.f90:1133-1554 (with
  *                          scalar_wflux_monot, scalar_vflux_monot and
  *                          scalar_monot_limiter; centered_monot = .false.,
@@ -23,7 +28,7 @@
  * Real literals that OLAM writes in default precision (e.g. fr = .70) keep
  * their single-precision value when promoted to real(8).
  * Not restated (off in every configuration this build runs): nudging,
- * shaved cells (lve2 > 0), eddy diffusion hooks (turbulence off), Lagrangian
+ * shaved cells (lve2 > 0), the supercell test's thil_init offset, Lagrangian
  * particle sums, the shallow-water test cases.
  */
 #include <algorithm>
@@ -61,6 +66,12 @@ struct DynCtx {
   bool vort_first = true;
   std::vector<T> vort2d, fvorth, fvortl, vfact;
   std::vector<int> lpmmin;
+  // eddy diffusion (olamgpu_eddy host arrays; NULL: off) and comp_horiz_k's
+  // outputs when the oracle computed them
+  const olamgpu_eddy* eddy = nullptr;
+  bool have_hk = false;
+  std::vector<T> akmodx, akhodx;
+  std::vector<int> kmtopv, khtopv;
   explicit DynCtx(const olamgpu_grid* gr, const olamgpu_opts* op) : g(gr), o(*op), G(gr) {
     mza = g->mza; mwa = g->mwa; mva = g->mva; mma = g->mma;
     arv = cvt<T>(g->arv, (size_t)mza * mva);
@@ -305,6 +316,186 @@ static void vort_damp(DynCtx<T>& X, const DynState<T>& s, T* vmt, R8 dtm) {
       F2(vmt, k, iv) = F2(vmt, k, iv) + X.fvortl[iv] * (F2(dl, k, im2) - F2(dl, k, im1)) * rr(k, iw1, iw2);
     for (int k = ka; k <= mza; ++k)
       F2(vmt, k, iv) = F2(vmt, k, iv) + X.fvorth[iv] * (F2(dh, k, im2) - F2(dh, k, im1)) * rr(k, iw1, iw2);
+  }
+}
+
+/* ---- eddy diffusion (convect/pbl_driver.f90, modules/mem_rayf.f90) ---------- */
+
+static bool dcmip_mixing_case(int tc) {
+  return tc == 110 || tc == 111 || tc == 112 || tc == 113 || tc == 114 || tc == 121 || tc == 122;
+}
+
+/* comp_horiz_k / comp_horiz_k_column (pbl_driver.f90:136-238) */
+template <class T>
+static void comp_horiz_k(DynCtx<T>& X, const DynState<T>& s) {
+  const GridT<T>& G = X.G;
+  const olamgpu_eddy& e = *X.eddy;
+  const int mza = X.mza, mva = X.mva;
+  X.akmodx.assign((size_t)mza * mva, (T)0);
+  X.akhodx.assign((size_t)mza * mva, (T)0);
+  // the arrays keep values the loops do not reach: start from OLAM's
+  for (size_t i = 0; i < X.akmodx.size(); ++i) { X.akmodx[i] = (T)e.akmodx[i]; X.akhodx[i] = (T)e.akhodx[i]; }
+  X.kmtopv.assign(e.kmtopv, e.kmtopv + mva);
+  X.khtopv.assign(e.khtopv, e.khtopv + mva);
+  const T dtl = (T)(float)X.o.dtlm;
+  std::vector<T> hk0(mza + 1), akstab(mza + 1);
+  for (int j = 0; j < X.g->nv_wadj; ++j) {
+    const int iv = X.g->jtv_wadj[j];
+    const int iw1 = G.v_iw(iv, 1), iw2 = G.v_iw(iv, 2);
+    const int mrl = e.mrlv[iv - 1];
+    const T fact1 = (T)0.95f / (dtl * (T)G.npoly(iw1));
+    const T fact2 = (T)0.95f / (dtl * (T)G.npoly(iw2));
+    const T akmin = (T)e.akmin[mrl - 1];
+    const int lpv = G.lpv(iv);
+    int& khv = X.khtopv[iv - 1];
+    int& kmv = X.kmtopv[iv - 1];
+    if (akmin > (T)1.e-7f) {
+      const T bkmin = akmin * (T).075f * std::pow(std::min(X.arw0[iw1 - 1], X.arw0[iw2 - 1]), (T).66666666f);
+      khv = mza;
+      kmv = mza;
+      for (int k = lpv; k <= mza; ++k) hk0[k] = (T)0.5f * (T)(F2(s.rho, k, iw1) + F2(s.rho, k, iw2)) * bkmin;
+    } else {
+      khv = std::max(e.khtop[iw1 - 1], e.khtop[iw2 - 1]);
+      khv = khv >= lpv ? khv + 1 : 1;
+      kmv = std::max(e.kmtop[iw1 - 1], e.kmtop[iw2 - 1]);
+      kmv = kmv >= lpv ? kmv + 1 : 1;
+    }
+    for (int k = lpv; k <= std::min(mza, std::max(kmv, khv)); ++k) {
+      const T stab1 = (T)(F2(s.rho, k, iw1) * (R8)(T)F2(X.g->volt, k, iw1) * (R8)fact1);
+      const T stab2 = (T)(F2(s.rho, k, iw2) * (R8)(T)F2(X.g->volt, k, iw2) * (R8)fact2);
+      akstab[k] = std::min(stab1, stab2);
+    }
+    auto vk = [&](const float* a, int k, int iw) { return (T)a[(size_t)(iw - 1) * mza + (k - 1)]; };
+    for (int k = lpv; k <= std::min(mza, kmv); ++k) {
+      T hkm = (T)0.25f * (vk(e.vkm, k, iw1) + vk(e.vkm, k, iw2) + vk(e.vkm, k - 1, iw1) + vk(e.vkm, k - 1, iw2));
+      if (akmin > (T)1.e-7f) hkm = std::max(hkm, hk0[k]);
+      F2(X.akmodx.data(), k, iv) = std::min(X.dniv[iv - 1] * F2(X.arv.data(), k, iv) * hkm, akstab[k]);
+    }
+    for (int k = lpv; k <= std::min(mza, khv); ++k) {
+      T hkh = (T)0.25f * (vk(e.vkh, k, iw1) + vk(e.vkh, k, iw2) + vk(e.vkh, k - 1, iw1) + vk(e.vkh, k - 1, iw2));
+      if (akmin > (T)1.e-7f) hkh = std::max(hkh, hk0[k]);
+      F2(X.akhodx.data(), k, iv) = std::min(X.dniv[iv - 1] * F2(X.arv.data(), k, iv) * hkh, akstab[k]);
+    }
+  }
+  X.have_hk = true;
+}
+
+/* tridv (tridiag_lib.f90:40-104) for nsp right-hand sides, arrays indexed by k */
+template <class T>
+static void tridv(const T* l, const T* d, const T* u, const std::vector<T>* b, std::vector<T>* x, int ka, int kz,
+                  int nsp) {
+  std::vector<T> gam(kz + 2);
+  T bet = (T)1.0 / d[ka];
+  for (int v = 0; v < nsp; ++v) x[v][ka] = bet * b[v][ka];
+  for (int k = ka + 1; k <= kz; ++k) {
+    gam[k] = bet * u[k - 1];
+    bet = (T)1.0 / (d[k] - l[k] * gam[k]);
+    for (int v = 0; v < nsp; ++v) x[v][k] = bet * (b[v][k] - l[k] * x[v][k - 1]);
+  }
+  for (int v = 0; v < nsp; ++v)
+    for (int k = kz - 1; k >= ka; --k) x[v][k] = x[v][k] - gam[k + 1] * x[v][k + 1];
+}
+
+/* solve_eddy_diff_heat (pbl_driver.f90:519-624) on one column of thilt_short */
+template <class T>
+static void solve_eddy_diff_heat(const DynCtx<T>& X, const DynState<T>& s, int iw, T* thilt) {
+  const olamgpu_eddy& e = *X.eddy;
+  const GridT<T>& G = X.G;
+  const int mza = X.mza;
+  if (dcmip_mixing_case(e.test_case)) return;
+  const int ka = G.lpw(iw), khtop = e.khtop[iw - 1];
+  if (khtop < ka) return;
+  const T dts = (T)(float)X.o.dtsm, forw_imp = (T)1.1f;
+  const int kmax = khtop + 1;
+  auto fld = [&](const float* a, int k) { return (T)a[(size_t)(iw - 1) * mza + (k - 1)]; };
+  std::vector<T> dtomass(mza + 2), varp(mza + 2), v5(mza + 2), v6(mza + 2), v7(mza + 2), rhs(mza + 2), soln(mza + 2);
+  for (int k = ka; k <= kmax; ++k) {
+    const T dtom = dts * G.volti_(k, iw) / (T)F2(s.rho, k, iw);
+    dtomass[k] = forw_imp * dtom;
+    varp[k] = F2(s.thil, k, iw) + dtom * thilt[k - 1];
+  }
+  for (int k = ka; k <= khtop; ++k) {
+    const T akodz = F2(X.arw.data(), k, iw) * fld(e.vkh, k) * (T)X.g->dzim[k - 1];
+    rhs[k] = akodz * (varp[k] - varp[k + 1]);
+    v5[k] = -akodz * dtomass[k];
+    v7[k] = -akodz * dtomass[k + 1];
+    v6[k] = (T)1. - v5[k] - v7[k];
+  }
+  // non-local PBL term
+  const int mrl = e.mrlw[iw - 1];
+  if (e.idiffk[mrl - 1] == 1 && fld(e.agamma, ka) > (T)1.e-7f * F2(X.arw.data(), ka, iw)) {
+    const T wt0 = (T)e.sfluxt[iw - 1] * fld(e.theta, ka) / ((T)F2(s.rho, ka, iw) * (T)e.cp * fld(e.tair, ka));
+    for (int k = ka; k <= e.kpblh[iw - 1]; ++k) rhs[k] = rhs[k] + wt0 * fld(e.agamma, k);
+  }
+  tridiffo(ka, khtop, v5.data(), v6.data(), v7.data(), rhs.data(), soln.data());
+  std::vector<R8> flux(mza + 2, 0.0);
+  for (int k = ka; k <= kmax - 1; ++k) flux[k] = (R8)soln[k];
+  for (int k = ka; k <= kmax; ++k) thilt[k - 1] = thilt[k - 1] + (T)(flux[k - 1] - flux[k]);
+}
+
+/* solve_eddy_diff_vxe (pbl_driver.f90:628-742) on one column */
+template <class T>
+static void solve_eddy_diff_vxe(const DynCtx<T>& X, const DynState<T>& s, int iw, T* vmxet, T* vmyet, T* vmzet) {
+  const olamgpu_eddy& e = *X.eddy;
+  const GridT<T>& G = X.G;
+  const int mza = X.mza;
+  if (dcmip_mixing_case(e.test_case)) return;
+  const int ka = G.lpw(iw), lsw = e.lsw[iw - 1], kmtop = e.kmtop[iw - 1];
+  const T dts = (T)(float)X.o.dtsm, forw_imp = (T)1.1f;
+  const int kmax = std::max(kmtop + 1, ka + lsw - 1);
+  const int n = std::max(mza, kmax) + 2;
+  std::vector<T> akodz(n, (T)0), dtomass(n), v3(n, (T)0), v5(n), v6(n), v7(n);
+  std::vector<T> rhs[3] = {std::vector<T>(n), std::vector<T>(n), std::vector<T>(n)};
+  std::vector<T> sol[3] = {std::vector<T>(n), std::vector<T>(n), std::vector<T>(n)};
+  std::vector<T> v2[3] = {std::vector<T>(n, (T)0), std::vector<T>(n, (T)0), std::vector<T>(n, (T)0)};
+  auto fld = [&](const float* a, int k) { return (T)a[(size_t)(iw - 1) * mza + (k - 1)]; };
+  const T* ve[3] = {s.vxe, s.vye, s.vze};
+  T* vt[3] = {vmxet, vmyet, vmzet};
+  akodz[ka - 1] = 0;
+  for (int k = kmtop + 1; k <= kmax; ++k) akodz[k] = 0;
+  for (int k = ka; k <= kmtop; ++k) akodz[k] = F2(X.arw.data(), k, iw) * fld(e.vkm, k) * (T)X.g->dzim[k - 1];
+  for (int k = ka; k <= kmax; ++k) {
+    const T dtom = (T)((R8)(dts * G.volti_(k, iw)) / F2(s.rho, k, iw));
+    dtomass[k] = forw_imp * dtom;
+    v5[k] = -dtomass[k] * akodz[k - 1];
+    v7[k] = -dtomass[k] * akodz[k];
+    v6[k] = (T)1. - v5[k] - v7[k];
+    for (int c = 0; c < 3; ++c) rhs[c][k] = F2(ve[c], k, iw);
+  }
+  // surface drag over the levels in contact with the surface
+  for (int k = ka; k <= ka + lsw - 1; ++k) {
+    const int ks = k - ka + 1;
+    v3[k] = (T)e.akm_sfc[(size_t)(iw - 1) * e.nsw_max + (ks - 1)] * (T)(1.0f / X.g->dzt_bot[k - 1]);
+    v6[k] = v6[k] + dtomass[k] * v3[k];
+  }
+  if (ka <= kmax) tridv(v5.data(), v6.data(), v7.data(), rhs, sol, ka, kmax, 3);
+  for (int k = ka; k <= kmax - 1; ++k)
+    for (int c = 0; c < 3; ++c) v2[c][k] = akodz[k] * (sol[c][k] - sol[c][k + 1]);
+  for (int c = 0; c < 3; ++c) { v2[c][ka - 1] = 0; v2[c][kmax] = 0; }
+  for (int k = ka; k <= ka + lsw - 1; ++k)
+    for (int c = 0; c < 3; ++c) vt[c][k - 1] = vt[c][k - 1] + (v2[c][k - 1] - v2[c][k] - v3[k] * sol[c][k]);
+  for (int k = ka + lsw; k <= kmax; ++k)
+    for (int c = 0; c < 3; ++c) vt[c][k - 1] = vt[c][k - 1] + v2[c][k - 1] - v2[c][k];
+}
+
+/* rayf_mix_top_vxe (mem_rayf.f90:177-220) */
+template <class T>
+static void rayf_mix_top_vxe(const DynCtx<T>& X, const DynState<T>& s, int iw, T* vmxet, T* vmyet, T* vmzet) {
+  const olamgpu_eddy& e = *X.eddy;
+  const int mza = X.mza;
+  if (!e.rayf_cofmix || e.krayfmix_bot >= mza) return;   // dorayfmix false
+  const int ka = std::max(e.krayfmix_bot, X.G.lpw(iw));
+  std::vector<T> fx(mza + 1, (T)0), fy(mza + 1, (T)0), fz(mza + 1, (T)0);
+  for (int k = ka; k <= mza - 1; ++k) {
+    const T fact = X.arw0[iw - 1] * (T)e.rayf_cofmix[k - 1] * (T)(F2(s.rho, k + 1, iw) + F2(s.rho, k, iw));
+    fx[k] = fact * (F2(s.vxe, k, iw) - F2(s.vxe, k + 1, iw));
+    fy[k] = fact * (F2(s.vye, k, iw) - F2(s.vye, k + 1, iw));
+    fz[k] = fact * (F2(s.vze, k, iw) - F2(s.vze, k + 1, iw));
+  }
+  for (int k = ka; k <= mza; ++k) {
+    vmxet[k - 1] = vmxet[k - 1] + fx[k - 1] - fx[k];
+    vmyet[k - 1] = vmyet[k - 1] + fy[k - 1] - fy[k];
+    vmzet[k - 1] = vmzet[k - 1] + fz[k - 1] - fz[k];
   }
 }
 
@@ -600,11 +791,40 @@ static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
       F2(vmyet_short.data(), k, iw) = F2(s.vmyet, k, iw) * v4;
       F2(vmzet_short.data(), k, iw) = F2(s.vmzet, k, iw) * v4;
     }
+    // vertical eddy diffusion of heat and momentum, top-level wind mixing (214-225)
+    T* sth = thilt_short.data() + (size_t)(iw - 1) * mza;
+    T* svx = vmxet_short.data() + (size_t)(iw - 1) * mza;
+    T* svy = vmyet_short.data() + (size_t)(iw - 1) * mza;
+    T* svz = vmzet_short.data() + (size_t)(iw - 1) * mza;
+    if (X.eddy) {
+      solve_eddy_diff_heat(X, s, iw, sth);
+      solve_eddy_diff_vxe(X, s, iw, svx, svy, svz);
+      rayf_mix_top_vxe(X, s, iw, svx, svy, svz);
+    }
     if (o.rayf_cof && o.initial == 1 && o.dn01d && o.th01d) {
       for (int k = o.krayf_bot; k <= mza; ++k) {
         T v4 = (T)F2(X.g->volt, k, iw);
         F2(thilt_short.data(), k, iw) = F2(thilt_short.data(), k, iw) +
             (T)o.rayf_cof[k - 1] * (T)o.dn01d[k - 1] * ((T)o.th01d[k - 1] - F2(s.thil, k, iw)) * v4;
+      }
+    }
+    // horizontal diffusion (238-251)
+    if (X.eddy) {
+      const olamgpu_eddy& e = *X.eddy;
+      for (int jv = 1; jv <= G.npoly(iw); ++jv) {
+        const int iv = G.w_iv(iw, jv), iwn = G.w_iw(iw, jv);
+        const int khv = X.have_hk ? X.khtopv[iv - 1] : e.khtopv[iv - 1];
+        const int kmv = X.have_hk ? X.kmtopv[iv - 1] : e.kmtopv[iv - 1];
+        auto akh = [&](int k) { return X.have_hk ? F2(X.akhodx.data(), k, iv) : (T)e.akhodx[(size_t)(iv - 1) * mza + k - 1]; };
+        auto akm = [&](int k) { return X.have_hk ? F2(X.akmodx.data(), k, iv) : (T)e.akmodx[(size_t)(iv - 1) * mza + k - 1]; };
+        for (int k = G.lpv(iv); k <= std::min(mza, khv); ++k)
+          sth[k - 1] = sth[k - 1] + akh(k) * (F2(s.thil, k, iwn) - F2(s.thil, k, iw));
+        for (int k = G.lpv(iv); k <= std::min(mza, kmv); ++k) {
+          const T a = akm(k);
+          svx[k - 1] = svx[k - 1] + a * (F2(s.vxe, k, iwn) - F2(s.vxe, k, iw));
+          svy[k - 1] = svy[k - 1] + a * (F2(s.vye, k, iwn) - F2(s.vye, k, iw));
+          svz[k - 1] = svz[k - 1] + a * (F2(s.vze, k, iwn) - F2(s.vze, k, iw));
+        }
       }
     }
   }
@@ -901,6 +1121,40 @@ static oracle::DynState<double> st64(const oracle_state64* s) {
   d.pvfac = s->pvfac; d.thilt = s->thilt; d.vmxet = s->vmxet; d.vmyet = s->vmyet;
   d.vmzet = s->vmzet; d.vmt = s->vmt;
   return d;
+}
+
+void oracle_dyn_set_eddy_f32(void* h, const olamgpu_eddy* e) {
+  auto* X = (oracle::DynCtx<float>*)h;
+  X->eddy = e;
+  X->have_hk = false;
+}
+void oracle_dyn_set_eddy_f64(void* h, const olamgpu_eddy* e) {
+  auto* X = (oracle::DynCtx<double>*)h;
+  X->eddy = e;
+  X->have_hk = false;
+}
+/* comp_horiz_k into the oracle's own arrays; copies them out as float or
+ * double (akmodx, akhodx (mza, mva)) and int (kmtopv, khtopv (mva)) */
+int oracle_comp_horiz_k_f32(void* h, const olamgpu_state* s, float* akmodx, float* akhodx, int* kmtopv, int* khtopv) {
+  auto* X = (oracle::DynCtx<float>*)h;
+  if (!X->eddy) return OLAMGPU_E_STATE;
+  oracle::comp_horiz_k(*X, st32(s));
+  std::copy(X->akmodx.begin(), X->akmodx.end(), akmodx);
+  std::copy(X->akhodx.begin(), X->akhodx.end(), akhodx);
+  std::copy(X->kmtopv.begin(), X->kmtopv.end(), kmtopv);
+  std::copy(X->khtopv.begin(), X->khtopv.end(), khtopv);
+  return OLAMGPU_OK;
+}
+int oracle_comp_horiz_k_f64(void* h, const oracle_state64* s, double* akmodx, double* akhodx, int* kmtopv,
+                            int* khtopv) {
+  auto* X = (oracle::DynCtx<double>*)h;
+  if (!X->eddy) return OLAMGPU_E_STATE;
+  oracle::comp_horiz_k(*X, st64(s));
+  std::copy(X->akmodx.begin(), X->akmodx.end(), akmodx);
+  std::copy(X->akhodx.begin(), X->akhodx.end(), akhodx);
+  std::copy(X->kmtopv.begin(), X->kmtopv.end(), kmtopv);
+  std::copy(X->khtopv.begin(), X->khtopv.end(), khtopv);
+  return OLAMGPU_OK;
 }
 
 int oracle_prog_wrtv_rk_f32(void* h, const olamgpu_state* s, int istp) {

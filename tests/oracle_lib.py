@@ -98,6 +98,12 @@ def _dyn_lib():
         L.oracle_tend0_f64.argtypes = [C.c_void_p, C.POINTER(State64), abi.c_double_p]
         L.oracle_timeavg_momsc_f32.argtypes = [C.c_void_p, C.POINTER(abi.State)]
         L.oracle_timeavg_momsc_f64.argtypes = [C.c_void_p, C.POINTER(State64)]
+        L.oracle_dyn_set_eddy_f32.argtypes = [C.c_void_p, C.POINTER(abi.Eddy)]
+        L.oracle_dyn_set_eddy_f64.argtypes = [C.c_void_p, C.POINTER(abi.Eddy)]
+        L.oracle_comp_horiz_k_f32.argtypes = [C.c_void_p, C.POINTER(abi.State), abi.c_float_p,
+                                              abi.c_float_p, abi.c_int_p, abi.c_int_p]
+        L.oracle_comp_horiz_k_f64.argtypes = [C.c_void_p, C.POINTER(State64), abi.c_double_p,
+                                              abi.c_double_p, abi.c_int_p, abi.c_int_p]
         L._dyn_ready = True
     return L
 
@@ -142,6 +148,26 @@ class DynOracle:
     def timeavg_momsc(self):
         f = self.L.oracle_timeavg_momsc_f64 if self.fp64 else self.L.oracle_timeavg_momsc_f32
         f(self.h, C.byref(self.s))
+
+    def set_eddy(self, eddy):
+        """Eddy diffusion from an ``abi.Eddy`` (kept alive here; None: off)."""
+        self.eddy = eddy
+        f = self.L.oracle_dyn_set_eddy_f64 if self.fp64 else self.L.oracle_dyn_set_eddy_f32
+        f(self.h, C.byref(eddy) if eddy is not None else None)
+
+    def comp_horiz_k(self):
+        """comp_horiz_k into the oracle's own arrays, which its later steps
+        use; returns copies (akmodx, akhodx, kmtopv, khtopv)."""
+        mza, mva = self.a["thil"].shape[1], self.a["vmc"].shape[0]
+        dt = np.float64 if self.fp64 else np.float32
+        ct = C.c_double if self.fp64 else C.c_float
+        am, ah = np.zeros((mva, mza), dt), np.zeros((mva, mza), dt)
+        km, kh = np.zeros(mva, np.int32), np.zeros(mva, np.int32)
+        f = self.L.oracle_comp_horiz_k_f64 if self.fp64 else self.L.oracle_comp_horiz_k_f32
+        rc = f(self.h, C.byref(self.s), abi.ptr(am, ct), abi.ptr(ah, ct), abi.ptr(km, C.c_int),
+               abi.ptr(kh, C.c_int))
+        assert rc == 0, rc
+        return am, ah, km, kh
 
     def __del__(self):
         try:
