@@ -281,6 +281,54 @@ int olamgpu_prog_wrtv_rk(int istp);
 int olamgpu_tend0(float* rho_old);
 int olamgpu_timeavg_momsc(void);
 
+/* ---- long-step glue on the device ------------------------------------------
+ * set_scalars_bottom (omodel/obnd.f90:7-36): below-ground levels 1..lpw-1
+ * of every registered scalar and of thil take the value at lpw, over
+ * jtw_prog.  diagvel_t3d (omodel/vel_t3d.f90:7-35): vxe, vye, vze from wc
+ * and vc over jtw_prog. */
+int olamgpu_set_scalars_bottom(void);
+int olamgpu_diagvel_t3d(void);
+
+/* tracer_maxmin (outils/check_nans.F90:164-203): smax[2n] = the largest
+ * value and smax[2n+1] = minus the smallest value of scalar n over
+ * jtw_prog, levels lpw..mza (-huge(1.) when no point is seen).  Values that
+ * are NaN are skipped.  Synchronises the stream. */
+int olamgpu_tracer_maxmin(float* smax);
+
+/* compute_mass_sums (outils/check_nans.F90:207-332) and the
+ * mass_sum_from_* helpers: sums[0] = sum of rho * volt and sums[1 + i] =
+ * sum of rho * volt * scalar[ids[i] - 1] (e.g. rr_w, rr_co2, an added
+ * scalar) over jtw_prog, levels lpw..mza, in real(8).  0 <= nsel <= 8.
+ * The device adds in a fixed order, so a sum repeats bit for bit from run
+ * to run; it differs from a serial CPU sum by round-off only.
+ * Synchronises the stream. */
+int olamgpu_mass_sums(int nsel, const int* ids, double* sums);
+
+/* One long step of the dynamical core on the device, in timestep.f90's
+ * order (:66-319) for the parts this library holds: tend0 (rho_old kept on
+ * the device), [comp_horiz_k], nacoust x prog_wrtv_rk, timeavg_momsc,
+ * scalar_transport_rk, [tracer_maxmin], set_scalars_bottom, [mass sums].
+ * Physics that OLAM runs between them stays on the host and is not called.
+ * With OLAMGPU_TS_GRAPH in RESIDENT mode, the first call runs the sequence
+ * as it is, and the first call for each of the three tracer-buffer
+ * rotations after it records the sequence as a CUDA graph; later calls
+ * replay the graph (no host work per kernel, no host round-trip).
+ * Registering scalars, eddy inputs or turbulence, or changing the
+ * coherence or transport form, drops the recorded graphs.  The plain
+ * transport form always runs without a graph.  The diagnostics of the last
+ * call are read with olamgpu_timestep_diag. */
+enum {
+  OLAMGPU_TS_GRAPH = 1u << 0,     /* record / replay the step as a CUDA graph      */
+  OLAMGPU_TS_HORIZ_K = 1u << 1,   /* comp_horiz_k first (eddy inputs registered)   */
+  OLAMGPU_TS_MAXMIN = 1u << 2,    /* tracer_maxmin after the tracer step           */
+  OLAMGPU_TS_MASS = 1u << 3       /* mass sums of rho and mass_ids at the end      */
+};
+int olamgpu_timestep(unsigned flags, int nmass, const int* mass_ids);
+/* smax as olamgpu_tracer_maxmin (2 x num_scalar), sums as olamgpu_mass_sums
+ * (1 + nmass); either may be NULL.  Synchronises the stream and returns a
+ * status the device recorded during the step, if any. */
+int olamgpu_timestep_diag(float* smax, double* sums);
+
 /* One explicit RK stage of update_scalar (scalar_transport_rk.F90:389-615:
  * grad_t2d[_quadratic], scalar_v_column, scalar_w_column; every column
  * explicit, no limiter) for ONE tracer, on device arrays the caller owns, in

@@ -90,6 +90,10 @@ class State(C.Structure):
     ]
 
 
+# olamgpu_timestep flags
+TS_GRAPH, TS_HORIZ_K, TS_MAXMIN, TS_MASS = 1, 2, 4, 8
+
+
 class Eddy(C.Structure):
     """olamgpu_eddy: the acoustic step's eddy-diffusion inputs."""
     _fields_ = [

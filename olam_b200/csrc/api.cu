@@ -57,15 +57,18 @@ static cudaEvent_t prof_event() {
   return e;
 }
 
+static bool g_prof_suspended = false;
+void prof_suspend(bool on) { g_prof_suspended = on; }
+
 void prof_begin(const char* name, cudaStream_t s) {
-  if (!g_prof_on) return;
+  if (!g_prof_on || g_prof_suspended) return;
   cudaEvent_t a = prof_event();
   cudaEventRecord(a, s);
   g_prof_open.push_back({name, a});
 }
 
 void prof_end(cudaStream_t s) {
-  if (!g_prof_on || g_prof_open.empty()) return;
+  if (!g_prof_on || g_prof_suspended || g_prof_open.empty()) return;
   cudaEvent_t b = prof_event();
   cudaEventRecord(b, s);
   g_prof_pending.push_back({g_prof_open.back().first, g_prof_open.back().second, b});
@@ -155,10 +158,12 @@ static void release_all() {
   tp.imp_count.release();
   tp.cfl_loc.release();
   tp.d_mode.release();
+  tp.h_mode.clear();
   tp.khtopv.release();
   tp.adj_ptab.release();
   tp.adj_ptab2.release();
   tp.have_turb = false;
+  glue_release();
   dyn_release();
   C.status.release();
 }
@@ -234,6 +239,7 @@ int olamgpu_register_scalars(int num_scalar, float* const* var_p, float* const* 
   if (num_scalar < 0 || (num_scalar > 0 && (!var_p || !var_t))) { set_error("bad scalar table"); return OLAMGPU_E_ARG; }
   for (int n = 0; n < num_scalar; ++n)
     if (!var_p[n] || !var_t[n]) { set_error("NULL var_p/var_t for scalar " + std::to_string(n + 1)); return OLAMGPU_E_ARG; }
+  glue_drop_graphs();
   Tracers& tr = C.tr;
   // drop a previous registration
   for (size_t i = 0; i < tr.p.size(); ++i) {
@@ -276,6 +282,7 @@ int olamgpu_register_scalars(int num_scalar, float* const* var_p, float* const* 
 int olamgpu_set_turb(const float* akhodx, const int* khtopv) {
   Context& C = ctx();
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  glue_drop_graphs();
   if (!akhodx || !khtopv) { C.tp.have_turb = false; return OLAMGPU_OK; }
   OG_CHECK(upload(C.tp.akhodx, akhodx, (size_t)C.g.mza * C.g.mva, C.stream));
   OG_CHECK(upload(C.tp.khtopv, khtopv, (size_t)C.g.mva, C.stream));
@@ -284,7 +291,10 @@ int olamgpu_set_turb(const float* akhodx, const int* khtopv) {
   return OLAMGPU_OK;
 }
 
-int olamgpu_set_eddy(const olamgpu_eddy* eddy) { return dyn_eddy_set(eddy); }
+int olamgpu_set_eddy(const olamgpu_eddy* eddy) {
+  glue_drop_graphs();
+  return dyn_eddy_set(eddy);
+}
 
 int olamgpu_comp_horiz_k(void) { return dyn_comp_horiz_k(); }
 
@@ -300,6 +310,7 @@ int olamgpu_finalize(void) {
 
 int olamgpu_set_coherence(int mode) {
   if (mode != OLAMGPU_SYNC_EACH_CALL && mode != OLAMGPU_RESIDENT) { set_error("unknown coherence mode"); return OLAMGPU_E_ARG; }
+  if (ctx().coherence != mode) glue_drop_graphs();
   ctx().coherence = mode;
   return OLAMGPU_OK;
 }
@@ -314,6 +325,7 @@ int olamgpu_set_transport_form(int form) {
     // keep the newest tracer values in the per-tracer mirrors across a switch
     OG_CHECK(ensure_plain(C.stream));
   }
+  if (C.form != form) glue_drop_graphs();
   C.form = form;
   return OLAMGPU_OK;
 }
@@ -403,6 +415,20 @@ int olamgpu_prog_wrtv_rk(int istp) { return dyn_prog_wrtv_rk(istp); }
 int olamgpu_tend0(float* rho_old) { return dyn_tend0(rho_old); }
 
 int olamgpu_timeavg_momsc(void) { return dyn_timeavg_momsc(); }
+
+int olamgpu_set_scalars_bottom(void) { return glue_set_scalars_bottom(); }
+
+int olamgpu_diagvel_t3d(void) { return dyn_diagvel_t3d(); }
+
+int olamgpu_tracer_maxmin(float* smax) { return glue_tracer_maxmin(smax); }
+
+int olamgpu_mass_sums(int nsel, const int* ids, double* sums) { return glue_mass_sums(nsel, ids, sums); }
+
+int olamgpu_timestep(unsigned flags, int nmass, const int* mass_ids) {
+  return glue_timestep(flags, nmass, mass_ids);
+}
+
+int olamgpu_timestep_diag(float* smax, double* sums) { return glue_timestep_diag(smax, sums); }
 
 void* olamgpu_stream(void) { return (void*)ctx().stream; }
 

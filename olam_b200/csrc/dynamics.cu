@@ -1060,6 +1060,29 @@ int dyn_timeavg_momsc() {
   return OLAMGPU_OK;
 }
 
+// diagvel_t3d (vel_t3d.f90:7-35): vel_t3d_hex over jtw_prog
+int dyn_diagvel_t3d() {
+  Context& C = ctx();
+  if (!C.initialised || !C.dy.ready || !C.have_state) { set_error("diagvel_t3d before init"); return OLAMGPU_E_STATE; }
+  cudaStream_t s = C.stream;
+  OG_CHECK(ensure_dyn_buffers(C));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(dyn_state_to_device(OLAMGPU_F_WC | OLAMGPU_F_VC | OLAMGPU_F_VXE, s));
+  else if (!C.dy.uploaded) { OG_CHECK(dyn_state_to_device(DYN_IN_MASK, s)); C.dy.uploaded = true; }
+  const DevGrid& d = C.g;
+  Dyn& y = C.dy;
+  if (d.nw_prog > 0) {
+    k_vel_t3d<<<cdiv((size_t)d.nw_prog * d.mza, 256), 256, 0, s>>>(dynk(d), d.jtw_prog.p, d.nw_prog, C.tp.wc.p, y.vc.p,
+                                                                    y.wno2.p, y.ecv.p, y.vxe.p, y.vye.p, y.vze.p);
+    OG_LAUNCHED();
+  }
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
+    OG_CHECK(dyn_state_to_host(OLAMGPU_F_VXE, s));
+    OG_CUDA(cudaStreamSynchronize(s));
+  }
+  OG_CUDA(cudaGetLastError());
+  return OLAMGPU_OK;
+}
+
 void dyn_release() {
   Dyn& y = ctx().dy;
   DevBuf<double>* d8[] = {&y.press, &y.rho0, &y.rth0, &y.volt, &y.zwgt_top8, &y.zwgt_bot8, &y.gdz_wgtm8, &y.gdz_wgtp8};

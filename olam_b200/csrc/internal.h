@@ -217,6 +217,7 @@ struct Transport {
   DevBuf<float> scale, upw;      // W arrays for monot/pd
   DevBuf<float> plain_out[2];    // per-tracer stage outputs of the plain form
   DevBuf<int> d_mode;            // per-tracer last-stage mode
+  std::vector<int> h_mode;       // what d_mode holds (uploaded when it changes)
   DevBuf<float> wrec;            // (mwa, mza, TILE_WR) weight records of the step
   // adjoint (transport_adjoint.cu): lam rotation, lam0, lams in the batched
   // layout, per-tracer planes
@@ -265,6 +266,27 @@ struct Dyn {
   DevBuf<int> e_kmtop, e_khtop, e_kpblh, e_kmtopv, e_khtopv, e_lsw, e_mrlw, e_mrlv, e_idiffk;
 };
 
+// one recorded long step (timestep.cu): the graph of the sequence for the
+// tracer buffer rotation it started from
+struct StepGraph {
+  cudaGraphExec_t exec = nullptr;
+  unsigned flags = 0;
+  int nmass = 0;
+  int ids[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int qcur_after = 0;
+  unsigned long long launches = 0;   // library kernels in the graph
+};
+
+struct Glue {
+  DevBuf<unsigned> keys;     // tracer_maxmin: (2, num_scalar) ordered keys
+  DevBuf<double> part;       // mass sums: per-block partial sums
+  DevBuf<double> sums;       // mass sums: (1 + nsel)
+  StepGraph g[3];            // indexed by the tracer rotation at the step's start
+  bool eager_done = false;   // a step ran without a graph since the last drop
+  unsigned last_flags = 0;
+  int last_nmass = 0, last_ntr = 0;
+};
+
 struct Context {
   bool initialised = false;
   int device = -1;
@@ -279,6 +301,7 @@ struct Context {
   Tracers tr;
   Transport tp;
   Dyn dy;
+  Glue glue;
   DevBuf<int> status;        // device status word (bounds/NaN flags)
 };
 
@@ -325,6 +348,17 @@ int check_device_status();
 
 // transport entry points (transport.cu)
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);
+// long-step glue and the recorded step (timestep.cu)
+int glue_set_scalars_bottom();
+int glue_tracer_maxmin(float* smax);
+int glue_mass_sums(int nsel, const int* ids, double* sums);
+int glue_timestep(unsigned flags, int nmass, const int* ids);
+int glue_timestep_diag(float* smax, double* sums);
+void glue_drop_graphs();
+void glue_release();
+int dyn_diagvel_t3d();
+// profiling off while a stream is being recorded into a graph
+void prof_suspend(bool on);
 // adjoint of one unlimited step (transport_adjoint.cu)
 int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* const* lam_sct);
 int tracers_to_device(cudaStream_t s);   // host -> per-tracer mirrors (-> Q)

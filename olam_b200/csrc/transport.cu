@@ -226,9 +226,20 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   for (int n = 0; n < tr.n; ++n) { modes[n] = mode_for(C, n); anylim |= modes[n] != MODE_PLAIN; }
   std::vector<int> pdm(tr.n);
   for (int n = 0; n < tr.n; ++n) pdm[n] = (C.opts.iscal_monot > 0 && tr.pdef[n]) ? 1 : 0;
-  OG_CHECK(tp.d_mode.alloc((size_t)std::max(tr.n, 1) * 2));
-  OG_CUDA(cudaMemcpyAsync(tp.d_mode.p, modes.data(), tr.n * sizeof(int), cudaMemcpyHostToDevice, s));
-  OG_CUDA(cudaMemcpyAsync(tp.d_mode.p + tr.n, pdm.data(), tr.n * sizeof(int), cudaMemcpyHostToDevice, s));
+  {
+    // uploaded when they change only (the upload reads pageable host memory,
+    // which a recorded step could not repeat)
+    std::vector<int> hm(modes);
+    hm.insert(hm.end(), pdm.begin(), pdm.end());
+    if (hm != tp.h_mode || !tp.d_mode.p) {
+      OG_CHECK(tp.d_mode.alloc((size_t)std::max(tr.n, 1) * 2));
+      if (tr.n > 0) {
+        OG_CUDA(cudaMemcpyAsync(tp.d_mode.p, hm.data(), hm.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        OG_CUDA(cudaStreamSynchronize(s));
+      }
+      tp.h_mode = hm;
+    }
+  }
   const bool any_pdm = std::any_of(pdm.begin(), pdm.end(), [](int v) { return v != 0; });
 
   if (batched) {

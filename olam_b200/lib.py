@@ -27,6 +27,8 @@ EXPORTS = [
     "olamgpu_tend0", "olamgpu_timeavg_momsc", "olamgpu_stream", "olamgpu_launch_count",
     "olamgpu_profile", "olamgpu_profile_read", "olamgpu_update_scalar_noalloc",
     "olamgpu_scalar_transport_rk_adjoint", "olamgpu_set_eddy", "olamgpu_comp_horiz_k",
+    "olamgpu_set_scalars_bottom", "olamgpu_diagvel_t3d", "olamgpu_tracer_maxmin", "olamgpu_mass_sums",
+    "olamgpu_timestep", "olamgpu_timestep_diag",
 ]
 
 
@@ -70,6 +72,12 @@ def load():
                                                         C.POINTER(abi.c_float_p)]
     lib.olamgpu_set_eddy.argtypes = [C.POINTER(abi.Eddy)]
     lib.olamgpu_comp_horiz_k.argtypes = []
+    lib.olamgpu_set_scalars_bottom.argtypes = []
+    lib.olamgpu_diagvel_t3d.argtypes = []
+    lib.olamgpu_tracer_maxmin.argtypes = [abi.c_float_p]
+    lib.olamgpu_mass_sums.argtypes = [C.c_int, abi.c_int_p, abi.c_double_p]
+    lib.olamgpu_timestep.argtypes = [C.c_uint, C.c_int, abi.c_int_p]
+    lib.olamgpu_timestep_diag.argtypes = [abi.c_float_p, abi.c_double_p]
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
             getattr(lib, name).restype = C.c_int
@@ -166,6 +174,38 @@ class OlamGpu:
 
     def comp_horiz_k(self):
         check(self.lib.olamgpu_comp_horiz_k())
+
+    # -- long-step glue ------------------------------------------------------------
+    def set_scalars_bottom(self):
+        check(self.lib.olamgpu_set_scalars_bottom())
+
+    def diagvel_t3d(self):
+        check(self.lib.olamgpu_diagvel_t3d())
+
+    def tracer_maxmin(self, ntr):
+        """(ntr, 2) array of (max, -min) per registered scalar."""
+        out = np.zeros((ntr, 2), np.float32)
+        check(self.lib.olamgpu_tracer_maxmin(abi.ptr(out, C.c_float)))
+        return out
+
+    def mass_sums(self, ids=()):
+        """[sum rho volt, sum rho volt scalar[i - 1] for i in ids]."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.zeros(1 + ids.size, np.float64)
+        check(self.lib.olamgpu_mass_sums(int(ids.size), abi.ptr(ids, C.c_int) if ids.size else None,
+                                         abi.ptr(out, C.c_double)))
+        return out
+
+    def timestep(self, flags=0, mass_ids=()):
+        ids = np.ascontiguousarray(mass_ids, dtype=np.int32)
+        self._mass_ids = ids
+        check(self.lib.olamgpu_timestep(int(flags), int(ids.size), abi.ptr(ids, C.c_int) if ids.size else None))
+
+    def timestep_diag(self, ntr, nmass=0):
+        smax = np.zeros((ntr, 2), np.float32)
+        sums = np.zeros(1 + nmass, np.float64)
+        check(self.lib.olamgpu_timestep_diag(abi.ptr(smax, C.c_float), abi.ptr(sums, C.c_double)))
+        return smax, sums
 
     # -- library controls --------------------------------------------------------
     def set_coherence(self, mode):

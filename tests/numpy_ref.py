@@ -9,6 +9,8 @@ cross-check the oracle's loop-by-loop restatement:
 * scalar_w_column                 omodel/scalar_transport_rk.F90:537-612
 * the RK loop of scalar_transport_rk without implicit columns or limiters
   (scalar_transport_rk.F90:95-111, 137-152, 223-381)
+* tracer_maxmin                   outils/check_nans.F90:164-203
+* compute_mass_sums / mass_sum_from_*   outils/check_nans.F90:207-550
 
 Arrays use the synth grid layout: (n, mza), slot 0 = dummy point.
 """
@@ -209,3 +211,33 @@ def limited_last_stage(g, scp, scp0, rhos, vm, wm, dtr, mode, order=2):
     new[:, 0] = s[:, 0]       # level 1 is not written: it keeps the stage input
     new[0] = 0.0
     return new
+
+
+def tracer_maxmin(scp, lpw):
+    """(ntr, 2): max and -min of each scalar over columns 1.. (every W point
+    is in jtw_prog on the synth grid), levels lpw..mza; NaNs skipped."""
+    ntr, mwa, mza = scp.shape
+    out = np.full((ntr, 2), -np.finfo(np.float32).max, np.float32)
+    for iw in range(1, mwa):
+        kb = int(lpw[iw]) - 1
+        col = scp[:, iw, kb:]
+        with np.errstate(invalid="ignore"):
+            hi = np.nanmax(np.where(np.isnan(col), -np.inf, col), axis=1)
+            lo = np.nanmin(np.where(np.isnan(col), np.inf, col), axis=1)
+        out[:, 0] = np.maximum(out[:, 0], hi)
+        out[:, 1] = np.maximum(out[:, 1], -lo)
+    return out
+
+
+def mass_sums(rho, volt, scalars, lpw):
+    """[sum rho volt, sum rho volt s for s in scalars] over columns 1..,
+    levels lpw..mza, in float64 (rho * volt first, as the reference)."""
+    out = np.zeros(1 + len(scalars))
+    mwa = rho.shape[0]
+    for iw in range(1, mwa):
+        kb = int(lpw[iw]) - 1
+        rv = rho[iw, kb:].astype(np.float64) * volt[iw, kb:].astype(np.float64)
+        out[0] += rv.sum()
+        for i, s in enumerate(scalars):
+            out[1 + i] += (rv * s[iw, kb:].astype(np.float64)).sum()
+    return out

@@ -45,6 +45,15 @@ def test_strerror_and_state_errors():
     assert L.olamgpu_update_scalar_noalloc(None, None, None, None, None, None, C.c_float(1.0),
                                            None, None) == abi.E_STATE
     assert L.olamgpu_scalar_transport_rk_adjoint(None, None, None) == abi.E_STATE
+    # the eddy and long-step entries too
+    assert L.olamgpu_set_eddy(None) == abi.E_STATE
+    assert L.olamgpu_comp_horiz_k() == abi.E_STATE
+    assert L.olamgpu_set_scalars_bottom() == abi.E_STATE
+    assert L.olamgpu_diagvel_t3d() == abi.E_STATE
+    assert L.olamgpu_tracer_maxmin(None) == abi.E_STATE
+    assert L.olamgpu_mass_sums(0, None, None) == abi.E_STATE
+    assert L.olamgpu_timestep(0, 0, None) == abi.E_STATE
+    assert L.olamgpu_timestep_diag(None, None) == abi.E_STATE
 
 
 def test_null_arguments_rejected():
