@@ -18,6 +18,8 @@ cell-updates/s = tracers x prognostic (k, iw) cells / step time.
   e2e    through the C-ABI with OLAM-style host arrays: every step uploads
          tracers, tendencies, winds and densities and downloads the tracers
   plain  the one-kernel-per-pass-per-tracer GPU form on the same data
+  long_step  one long step of the dynamical core (olamgpu_timestep) on the
+         same grid and tracers, unrecorded and replayed as a CUDA graph
   adjoint  device time of one adjoint call (scalar_transport_rk_adjoint:
          per-step records, layout transposes, reverse stages) over the
          forward step's, the adjoint/forward time ratio of the metric
@@ -61,6 +63,7 @@ def parse():
     p.add_argument("--no-column", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-long-step", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     return p.parse_args()
 
@@ -217,6 +220,57 @@ def run_reference(a):
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def bench_long_step(g, tr, a, max_over_ranks):
+    """One long step of the dynamical core on the device through
+    olamgpu_timestep (tend0, 4 acoustic RK3 steps, timeavg_momsc, the tracer
+    step, set_scalars_bottom), on the same grid and tracers with a balanced
+    jet: device time per long step unrecorded and replayed as a CUDA graph,
+    and the host time per call of each."""
+    import torch
+    from olam_b200 import abi
+    from olam_b200.lib import HostState, OlamGpu
+    from olam_b200.synth.state import dynamics_state
+
+    ds = dynamics_state(g, seed=4)
+    wz = lambda: np.zeros((g.mwa, g.mza), np.float32)   # noqa: E731
+    arrays = dict(rho=ds.rho, press=ds.press, thil=ds.thil, wc=ds.wc, wmc=ds.wmc, vxe=ds.vxe,
+                  vye=ds.vye, vze=ds.vze, vmc=ds.vmc, vc=ds.vc,
+                  vmasc=np.zeros((g.mva, g.mza), np.float32), wmasc=wz(),
+                  alpha_press=ds.alpha_press, pwfac=ds.pwfac, pvfac=ds.pvfac, thilt=wz(),
+                  vmxet=wz(), vmyet=wz(), vmzet=wz(), vmt=np.zeros((g.mva, g.mza), np.float32))
+    from olam_b200.abi import FortranGrid
+    fg = FortranGrid(g)
+    opts = abi.make_opts(a.dt, nacoust=4, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
+    hs = HostState(**arrays)
+    dev = OlamGpu(fg, opts, hs)
+    var_t = [np.zeros_like(tr[0]) for _ in range(len(tr))]
+    dev.register_scalars(tr, var_t)
+    dev.set_coherence(abi.RESIDENT)
+    stream = torch.cuda.ExternalStream(dev.stream())
+    out = {"workload": f"olamgpu_timestep: NXP={a.nxp}, {a.nlev} levels, {len(tr)} tracers, "
+                       f"dt {a.dt} s, nacoust 4, acoustic RK3, tracer RK{a.nrk}"}
+    k = max(2, min(a.steps, 5))
+    for mode, flags in (("eager", 0), ("graph", abi.TS_GRAPH)):
+        for _ in range(4):                     # first step, then one recording per rotation
+            dev.timestep(flags)
+        torch.cuda.synchronize()
+        dev.launch_count(reset=True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t0 = time.perf_counter()
+        for _ in range(k):
+            dev.timestep(flags)
+        host_s = time.perf_counter() - t0
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[f"{mode}_ms_per_step"] = max_over_ranks(e0.elapsed_time(e1) / k)
+        out[f"{mode}_host_ms_per_call"] = host_s * 1e3 / k
+        out["launches_per_step"] = dev.launch_count() // k
+    dev.close()
+    return out
 
 
 def main():
@@ -392,6 +446,10 @@ def main():
            "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_s}
     dev.close()
 
+    long_step = None
+    if not a.no_long_step:
+        long_step = bench_long_step(g, tr, a, max_over_ranks)
+
     cpu = None
     if rank == 0 and not a.no_cpu:
         cpu = cpu_sample(g, st, tr, a, a.cpu_seconds)
@@ -419,6 +477,7 @@ def main():
             "fused_column_value": column,
             "e2e": e2e,
             "adjoint": adjoint,
+            "long_step": long_step,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
