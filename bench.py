@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-long-step", action="store_true")
+    p.add_argument("--long-step-only", action="store_true",
+                   help="time only the long step (olamgpu_timestep) and print its object")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     return p.parse_args()
 
@@ -284,6 +286,11 @@ def main():
 
     torch.cuda.set_device(local)
     g, st, tr = make_case(a)
+    if a.long_step_only:
+        out = bench_long_step(g, tr, a, lambda x: x)
+        if rank == 0:
+            print(json.dumps({"long_step": out}), flush=True)
+        return 0
     fg = abi.FortranGrid(g)
     opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
     hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)

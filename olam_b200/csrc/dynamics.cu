@@ -19,6 +19,7 @@
 // k_setup_w (the vertical and horizontal eddy terms of :214-251).
 // Precision as declared by OLAM: rho, press and the implicit weights are
 // double; every other field is float.  Device level kd = Fortran k - 1.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -52,10 +53,11 @@ static DynK dynk(const DevGrid& d) {
   return k;
 }
 
+// thread per (table entry j, level kd); n * mza < 2^31 (dyn_setup checks)
 #define PK(j, kd, n)                                               \
-  size_t i_ = (size_t)blockIdx.x * blockDim.x + threadIdx.x;       \
-  if (i_ >= (size_t)(n) * g.mza) return;                           \
-  const int j = (int)(i_ / g.mza), kd = (int)(i_ % g.mza);
+  const unsigned i_ = blockIdx.x * blockDim.x + threadIdx.x;       \
+  if (i_ >= (unsigned)(n) * (unsigned)g.mza) return;               \
+  const int j = (int)(i_ / (unsigned)g.mza), kd = (int)(i_ - (unsigned)j * (unsigned)g.mza);
 
 // ---- column set-up (prog_wrtv_rk.f90:166-253) --------------------------------
 struct SetupW {
@@ -273,38 +275,57 @@ __global__ void k_vmca(DynK g, const int* __restrict__ vadj, int nv, const float
 
 struct Four { const float* f[4]; };
 
-// gradient planes of the four fields (grad_t2d, or grad_t2d_quadratic with
-// bounded=.false. as fluxes_wrtv calls it).  gx layout: [field][plane][iw][kd]
-__global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s, int ord_th, int ord_v,
+// gradient planes of the fields in fmask (grad_t2d for ORD 2, or
+// grad_t2d_quadratic with bounded=.false. for ORD 3, as fluxes_wrtv calls
+// them).  gx layout: [field][plane][iw][kd].  The neighbour loop is outside
+// the field loop: each neighbour's table entries and coefficients are read
+// once for the four fields, and the four gathers are independent.
+template <int ORD>
+__global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s, unsigned fmask,
                         const float* __restrict__ cx, const float* __restrict__ cy,
                         const float* __restrict__ xy_hu, float* __restrict__ gx) {
   PK(j, kd, nprog);
+  constexpr int NPL = ORD == 2 ? 2 : 5;
   const int iw = prog[j];
-  const size_t plane = (size_t)g.mwa * g.mza;
-  const size_t x = (size_t)iw * g.mza + kd;
+  const unsigned mza = g.mza;
+  const size_t plane = (size_t)g.mwa * mza;
+  const unsigned x = (unsigned)iw * mza + kd;
   const int np = g.npoly[iw];
+  float c0[4], a[4][NPL];
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
-    const int ord = f == 0 ? ord_th : ord_v;
-    if (ord < 2) continue;
-    const float* S = s.f[f];
-    const float c0 = S[x];
-    float a[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int n = 0; n < np; ++n) {
-      const int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
-      if (kd < g.lpv[iv]) continue;
-      const float d = S[(size_t)iwn * g.mza + kd] - c0;
-      if (ord == 2) {
-        a[0] = a[0] + cx[iw * 7 + n] * d;
-        a[1] = a[1] + cy[iw * 7 + n] * d;
-      } else {
+    c0[f] = ((fmask >> f) & 1u) ? s.f[f][x] : 0.f;
 #pragma unroll
-        for (int m = 0; m < 5; ++m) a[m] = a[m] + d * xy_hu[((size_t)iw * 7 + n) * 5 + m];
-      }
+    for (int m = 0; m < NPL; ++m) a[f][m] = 0.f;
+  }
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    if (n >= np) break;
+    const int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
+    if (kd < g.lpv[iv]) continue;
+    float w[NPL];
+    if (ORD == 2) {
+      w[0] = cx[iw * 7 + n];
+      w[1] = cy[iw * 7 + n];
+    } else {
+#pragma unroll
+      for (int m = 0; m < NPL; ++m) w[m] = xy_hu[((size_t)iw * 7 + n) * 5 + m];
     }
+    const unsigned xn = (unsigned)iwn * mza + kd;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      if (!((fmask >> f) & 1u)) continue;
+      const float d = s.f[f][xn] - c0[f];
+#pragma unroll
+      for (int m = 0; m < NPL; ++m) a[f][m] = a[f][m] + w[m] * d;
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    if (!((fmask >> f) & 1u)) continue;
     float* G = gx + (size_t)f * 5 * plane;
-    const int nplanes = ord == 2 ? 2 : 5;
-    for (int m = 0; m < nplanes; ++m) G[m * plane + x] = a[m];
+#pragma unroll
+    for (int m = 0; m < NPL; ++m) G[m * plane + x] = a[f][m];
   }
 }
 
@@ -341,34 +362,33 @@ __global__ void k_upw4(DynK g, const int* __restrict__ prog, int nprog, Four s, 
 
 struct VSide { const float* dxps; const float* dyps; const float* xx0_v; const float* xy0_v; const float* yy0_v; };
 
-__global__ void k_upv4(DynK g, const int* __restrict__ vadj, int nv, Four s, int ord_th, int ord_v,
+// V-face values of the four fields, from the upwind cell only (the side the
+// sign of vmc selects): fields in gmask add the linear gradient terms,
+// fields in qmask also the quadratic ones (order 3)
+__global__ void k_upv4(DynK g, const int* __restrict__ vadj, int nv, Four s, unsigned gmask, unsigned qmask,
                        const float* __restrict__ gx, VSide c, const float* __restrict__ vmc,
                        float* __restrict__ upv) {
   PK(j, kd, nv);
   const int iv = vadj[j];
   if (kd < g.lpv[iv]) return;
-  const int mza = g.mza;
-  const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
+  const unsigned mza = g.mza;
   const size_t plane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
-  const size_t x1 = (size_t)iw1 * mza + kd, x2 = (size_t)iw2 * mza + kd;
-  const bool neg = vmc[(size_t)iv * mza + kd] < 0.f;
+  const unsigned xv = (unsigned)iv * mza + kd;
+  const int side = vmc[xv] < 0.f ? 1 : 0;
+  const int iw = g.v_iw[iv * 2 + side];
+  const unsigned xw = (unsigned)iw * mza + kd;
+  const float dx = c.dxps[iv * 2 + side], dy = c.dyps[iv * 2 + side];
+  float xx = 0.f, xy = 0.f, yy = 0.f;
+  if (qmask) { xx = c.xx0_v[iv * 2 + side]; xy = c.xy0_v[iv * 2 + side]; yy = c.yy0_v[iv * 2 + side]; }
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
-    const int ord = f == 0 ? ord_th : ord_v;
-    const float* S = s.f[f];
-    float s1 = S[x1], s2 = S[x2];
-    if (ord >= 2) {
+    float v = s.f[f][xw];
+    if ((gmask >> f) & 1u) {
       const float* G = gx + (size_t)f * 5 * plane;
-      s1 = s1 + c.dxps[iv * 2] * G[x1] + c.dyps[iv * 2] * G[plane + x1];
-      s2 = s2 + c.dxps[iv * 2 + 1] * G[x2] + c.dyps[iv * 2 + 1] * G[plane + x2];
-      if (ord == 3) {
-        s1 = s1 + c.xx0_v[iv * 2] * G[2 * plane + x1] + c.xy0_v[iv * 2] * G[3 * plane + x1] +
-             c.yy0_v[iv * 2] * G[4 * plane + x1];
-        s2 = s2 + c.xx0_v[iv * 2 + 1] * G[2 * plane + x2] + c.xy0_v[iv * 2 + 1] * G[3 * plane + x2] +
-             c.yy0_v[iv * 2 + 1] * G[4 * plane + x2];
-      }
+      v = v + dx * G[xw] + dy * G[plane + xw];
+      if ((qmask >> f) & 1u) v = v + xx * G[2 * plane + xw] + xy * G[3 * plane + xw] + yy * G[4 * plane + xw];
     }
-    upv[(size_t)f * vplane + (size_t)iv * mza + kd] = neg ? s2 : s1;
+    upv[(size_t)f * vplane + xv] = v;
   }
 }
 
@@ -651,6 +671,10 @@ int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s) {
   for (int i = 1; i < mwa; ++i)
     if (g->lve2 && g->lve2[i] != 0) { set_error("shaved cells (lve2 > 0) are not supported"); return OLAMGPU_E_UNSUPPORTED; }
   if (mza > 128) { set_error("prog_wrtv_rk supports mza <= 128"); return OLAMGPU_E_UNSUPPORTED; }
+  if ((size_t)std::max(std::max(mwa, mva), mma) * mza >= (1ull << 31)) {
+    set_error("prog_wrtv_rk supports grids with max(mwa, mva, mma) * mza < 2^31");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
   OG_CHECK(up(y.arv, g->arv, (size_t)mza * mva, s, "arv"));
   OG_CHECK(up(y.arw, g->arw, (size_t)mza * mwa, s, "arw"));
   OG_CHECK(up(y.volwi, g->volwi, (size_t)mza * mwa, s, "volwi"));
@@ -953,13 +977,18 @@ int dyn_prog_wrtv_rk(int istp) {
                                   y.rk_th.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p);
     k_vmca<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, y.vmc.p, y.arv.p, y.vmca.p, tp.vmasc.p, last);
     Four f{{y.thil.p, y.vxe.p, y.vye.p, y.vze.p}};
-    k_grad4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, o.thil_horiz_adv_order, o.wind_horiz_adv_order,
-                                d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p);
+    // fields by reconstruction order: thil has thil_horiz_adv_order, the
+    // winds wind_horiz_adv_order (order 1: no gradient)
+    const int ordf[4] = {o.thil_horiz_adv_order, o.wind_horiz_adv_order, o.wind_horiz_adv_order,
+                         o.wind_horiz_adv_order};
+    unsigned m2 = 0, m3 = 0;
+    for (int q = 0; q < 4; ++q) { if (ordf[q] == 2) m2 |= 1u << q; if (ordf[q] >= 3) m3 |= 1u << q; }
+    if (m2) { k_grad4<2><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m2, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
+    if (m3) { k_grad4<3><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m3, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
     k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p);
     VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
-    k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, o.thil_horiz_adv_order, o.wind_horiz_adv_order,
-                                y.gx.p, vs, y.vmc.p, y.upv.p);
-    OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+    k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, m2 | m3, m3, y.gx.p, vs, y.vmc.p, y.upv.p);
+    OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
     // last stage: flux-corrected face values replace those of the limited fields (370-399)
     if (last && thil_monot) {
       OG_PROF("monot_faces", s);
