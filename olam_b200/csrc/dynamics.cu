@@ -5,7 +5,9 @@
 //   k_setup_w / k_setup_v   column set-up and Rayleigh terms   (prog_wrtv_rk.f90:166-303)
 //   k_div_* / k_lap_w       divh_damp                          (vort_div_damp.f90:1-230)
 //   k_vort_* / k_lap_m      vort_damp                          (vort_div_damp.f90:234-445)
-//   k_rk_copy, k_vmca       stage copies, vmca and vmasc       (prog_wrtv_rk.f90:320-368)
+//   k_vmca                  vmca and vmasc on the last stage   (prog_wrtv_rk.f90:320-368); the
+//                           stage copies *_rk = *_short and vmca of the other stages are
+//                           formed inside k_wrt_begs
 //   k_grad4, k_upw4, k_upv4 fluxes_wrtv for thil, vxe, vye, vze (:950-1129), the four
 //                           fields of one stage in one launch each; on the
 //                           last stage the fields with ithil_monot /
@@ -252,15 +254,6 @@ __global__ void k_vort_apply(DynK g, const int* __restrict__ vprog, int nv, int 
 }
 
 // ---- stage kernels ----------------------------------------------------------------
-__global__ void k_rk_copy(DynK g, const int* __restrict__ prog, int nprog, const float* sth, const float* svx,
-                          const float* svy, const float* svz, float* rth, float* rvx, float* rvy, float* rvz) {
-  PK(j, kd, nprog);
-  const int iw = prog[j];
-  if (kd < g.lpw[iw]) return;
-  const size_t x = (size_t)iw * g.mza + kd;
-  rth[x] = sth[x]; rvx[x] = svx[x]; rvy[x] = svy[x]; rvz[x] = svz[x];
-}
-
 __global__ void k_vmca(DynK g, const int* __restrict__ vadj, int nv, const float* __restrict__ vmc,
                        const float* __restrict__ arv, float* __restrict__ vmca, float* __restrict__ vmasc,
                        int last) {
@@ -399,8 +392,10 @@ struct WrtArgs {
   float dts, fcoriol, c8, c9, rocv;
   double pc2, pc3, fr;
   const int* prog; int nprog;
-  const float* vmca; const float* upv; const float* upw;   // 4-field arrays
-  float* rk_th; float* rk_vx; float* rk_vy; float* rk_vz;
+  const float* vmc; const float* arv;                       // vmca = vmc arv
+  const float* upv; const float* upw;                       // 4-field arrays
+  const float* sh_th; const float* sh_vx; const float* sh_vy; const float* sh_vz;   // *_rk at stage start
+  float* rk_vx; float* rk_vy; float* rk_vz;
   double* rho; double* press; const double* rho0; const double* rth0;
   float* thil; float* wc; float* wmc; const float* wmc0; const float* vxe; const float* vye;
   float* wmasc;
@@ -417,7 +412,7 @@ struct WrtSmem {
   float *b15, *rkx, *rky, *rkz, *b31, *b32, *b33, *dwm, *wmf;
 };
 
-__global__ void __launch_bounds__(WRT_WARPS * 32) k_wrt_begs(DynK g, WrtArgs A) {
+__global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs A) {
   extern __shared__ double wsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j = blockIdx.x * WRT_WARPS + warp;
@@ -441,28 +436,41 @@ __global__ void __launch_bounds__(WRT_WARPS * 32) k_wrt_begs(DynK g, WrtArgs A) 
   const float* vye_upw = A.upw + 2 * wplane;
   const float* vze_upw = A.upw + 3 * wplane;
   const float wnx = A.wn[iw * 3], wny = A.wn[iw * 3 + 1], wnz = A.wn[iw * 3 + 2];
+  // the column's edges, read once: V point, with the sign bit set where the
+  // edge's dirv is not positive; -1 past npoly
+  int ev[7];
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    const int iv = n < np ? g.w_ev[iw * 8 + n] : -1;
+    ev[n] = (iv >= 0 && !(g.w_dirv[iw * 8 + n] > 0.f)) ? (iv | (int)0x80000000) : iv;
+  }
 
   // phase 1: horizontal sums, Coriolis and explicit density / rho*thil terms
   for (int kd = kb + lane; kd < mza; kd += 32) {
     double hf = 0.0;
-    float th = A.rk_th[cb + kd], vx = A.rk_vx[cb + kd], vy = A.rk_vy[cb + kd], vz = A.rk_vz[cb + kd];
-    for (int n = 0; n < np; ++n) {
-      const int iv = g.w_ev[iw * 8 + n];
+    // *_rk start each stage as *_short (prog_wrtv_rk.f90:320-330)
+    float th = A.sh_th[cb + kd], vx = A.sh_vx[cb + kd], vy = A.sh_vy[cb + kd], vz = A.sh_vz[cb + kd];
+#pragma unroll
+    for (int n = 0; n < 7; ++n) {
+      if (ev[n] == -1) break;
+      const int iv = ev[n] & 0x7fffffff;
       if (kd < g.lpv[iv]) continue;
       const size_t xv = (size_t)iv * mza + kd;
-      const float vm = A.vmca[xv];
-      if (g.w_dirv[iw * 8 + n] > 0.f) {
+      const float vm = A.vmc[xv] * A.arv[xv];
+      const float u0 = A.upv[xv], u1 = A.upv[vplane + xv], u2 = A.upv[2 * vplane + xv],
+                  u3 = A.upv[3 * vplane + xv];
+      if (ev[n] >= 0) {
         hf = hf + (double)vm;
-        th = th + vm * A.upv[xv];
-        vx = vx + vm * A.upv[vplane + xv];
-        vy = vy + vm * A.upv[2 * vplane + xv];
-        vz = vz + vm * A.upv[3 * vplane + xv];
+        th = th + vm * u0;
+        vx = vx + vm * u1;
+        vy = vy + vm * u2;
+        vz = vz + vm * u3;
       } else {
         hf = hf - (double)vm;
-        th = th - vm * A.upv[xv];
-        vx = vx - vm * A.upv[vplane + xv];
-        vy = vy - vm * A.upv[2 * vplane + xv];
-        vz = vz - vm * A.upv[3 * vplane + xv];
+        th = th - vm * u0;
+        vx = vx - vm * u1;
+        vy = vy - vm * u2;
+        vz = vz - vm * u3;
       }
     }
     const double rho = A.rho[cb + kd];
@@ -594,7 +602,9 @@ __global__ void k_vel_t3d(DynK g, const int* __restrict__ prog, int nprog, const
   const float wst = wc[cb + kd - 1] + wc[cb + kd];
   float x = wst * wno2[iw * 3], y = wst * wno2[iw * 3 + 1], z = wst * wno2[iw * 3 + 2];
   const int np = g.npoly[iw];
-  for (int n = 0; n < np; ++n) {
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    if (n >= np) break;
     const int iv = g.w_ev[iw * 8 + n];
     if (kd < g.lpv[iv]) continue;
     const float v = vc[(size_t)iv * mza + kd];
@@ -744,7 +754,7 @@ static int ensure_dyn_buffers(Context& C) {
   OG_CHECK(A(y.press, wz)); OG_CHECK(A(y.rho0, wz)); OG_CHECK(A(y.rth0, wz));
   DevBuf<float>* w[] = {&y.thil, &y.wmc, &y.vxe, &y.vye, &y.vze, &y.alpha_press, &y.pwfac, &y.thilt,
                         &y.vmxet, &y.vmyet, &y.vmzet, &y.wmc0, &y.sh_th, &y.sh_vx, &y.sh_vy, &y.sh_vz,
-                        &y.rk_th, &y.rk_vx, &y.rk_vy, &y.rk_vz};
+                        &y.rk_vx, &y.rk_vy, &y.rk_vz};
   for (auto* b : w) OG_CHECK(A(*b, wz));
   DevBuf<float>* v[] = {&y.vmc, &y.vc, &y.pvfac, &y.vmt, &y.vmc0, &y.vmca, &y.sh_vmt, &y.fdivh};
   for (auto* b : v) OG_CHECK(A(*b, vz));
@@ -973,9 +983,9 @@ int dyn_prog_wrtv_rk(int istp) {
     const double dt8 = (nrk <= 2 ? xstg2[istage - 1] : xstg3[istage - 1]) * o.dtsm;
     const float dts = (float)dt8;
     const int last = istage == nrk;
-    k_rk_copy<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.sh_th.p, y.sh_vx.p, y.sh_vy.p, y.sh_vz.p,
-                                  y.rk_th.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p);
-    k_vmca<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, y.vmc.p, y.arv.p, y.vmca.p, tp.vmasc.p, last);
+    // vmca = vmc arv is formed where it is read; the last stage also keeps
+    // it (the flux-corrected faces read it) and adds it to vmasc
+    if (last) { k_vmca<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, y.vmc.p, y.arv.p, y.vmca.p, tp.vmasc.p, 1); OG_LAUNCHED(); }
     Four f{{y.thil.p, y.vxe.p, y.vye.p, y.vze.p}};
     // fields by reconstruction order: thil has thil_horiz_adv_order, the
     // winds wind_horiz_adv_order (order 1: no gradient)
@@ -988,7 +998,7 @@ int dyn_prog_wrtv_rk(int istp) {
     k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p);
     VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
     k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, m2 | m3, m3, y.gx.p, vs, y.vmc.p, y.upv.p);
-    OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+    OG_LAUNCHED(); OG_LAUNCHED();
     // last stage: flux-corrected face values replace those of the limited fields (370-399)
     if (last && thil_monot) {
       OG_PROF("monot_faces", s);
@@ -1010,8 +1020,9 @@ int dyn_prog_wrtv_rk(int istp) {
     A.c8 = dts * (float)A.pc2;
     A.c9 = -dts * dts * (float)A.fr;
     A.prog = d.jtw_prog.p; A.nprog = d.nw_prog;
-    A.vmca = y.vmca.p; A.upv = y.upv.p; A.upw = y.upw.p;
-    A.rk_th = y.rk_th.p; A.rk_vx = y.rk_vx.p; A.rk_vy = y.rk_vy.p; A.rk_vz = y.rk_vz.p;
+    A.vmc = y.vmc.p; A.arv = y.arv.p; A.upv = y.upv.p; A.upw = y.upw.p;
+    A.sh_th = y.sh_th.p; A.sh_vx = y.sh_vx.p; A.sh_vy = y.sh_vy.p; A.sh_vz = y.sh_vz.p;
+    A.rk_vx = y.rk_vx.p; A.rk_vy = y.rk_vy.p; A.rk_vz = y.rk_vz.p;
     A.rho = tp.rho.p; A.press = y.press.p; A.rho0 = y.rho0.p; A.rth0 = y.rth0.p;
     A.thil = y.thil.p; A.wc = tp.wc.p; A.wmc = y.wmc.p; A.wmc0 = y.wmc0.p; A.vxe = y.vxe.p; A.vye = y.vye.p;
     A.wmasc = tp.wmasc.p; A.alpha_press = y.alpha_press.p; A.pwfac = y.pwfac.p;
@@ -1118,7 +1129,7 @@ void dyn_release() {
   for (auto* b : d8) b->release();
   DevBuf<float>* f[] = {&y.thil, &y.wmc, &y.vxe, &y.vye, &y.vze, &y.vmc, &y.vc, &y.alpha_press, &y.pwfac,
                         &y.pvfac, &y.thilt, &y.vmxet, &y.vmyet, &y.vmzet, &y.vmt, &y.wmc0, &y.vmc0, &y.vmca,
-                        &y.sh_th, &y.sh_vx, &y.sh_vy, &y.sh_vz, &y.sh_vmt, &y.rk_th, &y.rk_vx, &y.rk_vy,
+                        &y.sh_th, &y.sh_vx, &y.sh_vy, &y.sh_vz, &y.sh_vmt, &y.rk_vx, &y.rk_vy,
                         &y.rk_vz, &y.upw, &y.upv, &y.gx, &y.div2d, &y.fdivh, &y.vort2d, &y.fvorth, &y.fvortl,
                         &y.vfact, &y.arv, &y.arw, &y.volwi, &y.volvi, &y.wn, &y.wno2, &y.vn, &y.ecv,
                         &y.gdz_wgtm, &y.gdz_wgtp, &y.dniv, &y.dniu, &y.dnv, &y.arw0, &y.arm0, &y.zfacit,

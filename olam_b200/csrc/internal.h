@@ -241,7 +241,7 @@ struct Dyn {
   DevBuf<float> thilt, vmxet, vmyet, vmzet, vmt;       // long-step tendencies
   DevBuf<float> wmc0, vmc0, vmca;
   DevBuf<float> sh_th, sh_vx, sh_vy, sh_vz, sh_vmt;    // *_short
-  DevBuf<float> rk_th, rk_vx, rk_vy, rk_vz;            // *_rk
+  DevBuf<float> rk_vx, rk_vy, rk_vz;                   // *_rk (thilt_rk stays in registers)
   DevBuf<float> upw, upv;        // 4 fields: thil, vxe, vye, vze
   DevBuf<float> gx;              // gradient planes of the 4 fields
   DevBuf<float> div2d, fdivh, vort2d, fvorth, fvortl, vfact;
