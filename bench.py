@@ -271,7 +271,37 @@ def bench_long_step(g, tr, a, max_over_ranks):
         out[f"{mode}_ms_per_step"] = max_over_ranks(e0.elapsed_time(e1) / k)
         out[f"{mode}_host_ms_per_call"] = host_s * 1e3 / k
         out["launches_per_step"] = dev.launch_count() // k
+    # per-kernel device time of the acoustic step (CUDA events around each
+    # launch, unrecorded steps) against its algorithmic bytes
+    dev.profile(True, reset=True)
+    for _ in range(2):
+        dev.timestep(0)
+    prof = dev.profile_read()
+    dev.profile(False, reset=True)
     dev.close()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs") or 6650.0)
+    cw, cv = (g.mwa - 1) * (g.mza - 1), (g.mva - 1) * (g.mza - 1)   # above-ground W and V cells
+    # bytes each launch must move at least (every array element it reads or
+    # writes once; stage-averaged for wrt_begs over the 3 RK stages)
+    algo = {
+        "setup_w": 76 * cw, "setup_v": 16 * cv, "vmca": 20 * cv, "grad4": 48 * cw, "upw4": 36 * cw,
+        "upv4": 20 * cv + 48 * cw, "wrt_begs": (136 + 16 / 3) * cw + 24 * cv, "prog_v": 24 * cv + 28 * cw,
+        "vel_t3d": 16 * cw + 4 * cv,
+    }
+    kern = {}
+    for name, b in algo.items():
+        if name in prof and prof[name][1]:
+            ms = prof[name][0] / prof[name][1]
+            kern[name] = {"ms_per_launch": ms, "algorithmic_gb": b / 1e9,
+                          "achieved_gbs": b / (ms * 1e-3) / 1e9, "frac": b / (ms * 1e-3) / 1e9 / peak}
+    out["acoustic_kernels"] = kern
+    if "prog_wrtv_rk" in prof:
+        out["prog_wrtv_rk_ms"] = prof["prog_wrtv_rk"][0] / prof["prog_wrtv_rk"][1]
     return out
 
 

@@ -367,10 +367,16 @@ __global__ void k_upv4(DynK g, const int* __restrict__ vadj, int nv, Four s, uns
   const unsigned mza = g.mza;
   const size_t plane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
   const unsigned xv = (unsigned)iv * mza + kd;
-  const int side = vmc[xv] < 0.f ? 1 : 0;
-  const int iw = g.v_iw[iv * 2 + side];
+  // both sides' table entries load alongside vmc; the sign picks one
+  const float vm = vmc[xv];
+  const int2 iwp = *reinterpret_cast<const int2*>(g.v_iw + iv * 2);
+  const float2 dxp = *reinterpret_cast<const float2*>(c.dxps + iv * 2);
+  const float2 dyp = *reinterpret_cast<const float2*>(c.dyps + iv * 2);
+  const bool neg = vm < 0.f;
+  const int side = neg ? 1 : 0;
+  const int iw = neg ? iwp.y : iwp.x;
   const unsigned xw = (unsigned)iw * mza + kd;
-  const float dx = c.dxps[iv * 2 + side], dy = c.dyps[iv * 2 + side];
+  const float dx = neg ? dxp.y : dxp.x, dy = neg ? dyp.y : dyp.x;
   float xx = 0.f, xy = 0.f, yy = 0.f;
   if (qmask) { xx = c.xx0_v[iv * 2 + side]; xy = c.xy0_v[iv * 2 + side]; yy = c.yy0_v[iv * 2 + side]; }
 #pragma unroll
@@ -939,26 +945,29 @@ int dyn_prog_wrtv_rk(int istp) {
   const int mza = d.mza;
   const unsigned nbw = cdiv((size_t)d.nw_prog * mza, 256), nbv = cdiv((size_t)d.nv_prog * mza, 256),
                  nbva = cdiv((size_t)d.nv_wadj * mza, 256);
-  OG_PROF("dyn_setup", s);
-  if (!o.divh_damp_short && istp == 1) divh_damp(C, y.vmt.p, o.dtlm, s);
-  if (!o.vort_damp_short && istp == 1) vort_damp(C, y.vmt.p, o.dtlm, s);
+  OG_PROF("prog_wrtv_rk", s);
+  if (!o.divh_damp_short && istp == 1) { OG_PROF("divh_damp", s); divh_damp(C, y.vmt.p, o.dtlm, s); }
+  if (!o.vort_damp_short && istp == 1) { OG_PROF("vort_damp", s); vort_damp(C, y.vmt.p, o.dtlm, s); }
   SetupW sw{tp.rho.p, y.thil.p, y.wmc.p, y.thilt.p, y.vmxet.p, y.vmyet.p, y.vmzet.p, y.volt.p, y.rho0.p,
             y.rth0.p, y.wmc0.p, y.sh_th.p, y.sh_vx.p, y.sh_vy.p, y.sh_vz.p, y.rayf_cof.p, y.dn01d.p, y.th01d.p,
             o.krayf_bot};
   const bool rayleigh_th = o.rayf_cof && o.initial == 1;
   // with eddy diffusion the Rayleigh term on thil follows the eddy terms
   if (!rayleigh_th || y.eddy_on) sw.rayf_cof = nullptr;
-  k_setup_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, sw);
-  k_setup_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.vmc.p, y.vmt.p, y.vmc0.p, y.sh_vmt.p,
-                                (o.rayf_cof && o.vc03d) ? y.rayf_cof.p : nullptr, y.vc03d.p, y.vc.p, tp.rho.p,
-                                o.krayf_bot);
-  OG_LAUNCHED(); OG_LAUNCHED();
+  { OG_PROF("setup_w", s); k_setup_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, sw); OG_LAUNCHED(); }
+  {
+    OG_PROF("setup_v", s);
+    k_setup_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.vmc.p, y.vmt.p, y.vmc0.p, y.sh_vmt.p,
+                                  (o.rayf_cof && o.vc03d) ? y.rayf_cof.p : nullptr, y.vc03d.p, y.vc.p, tp.rho.p,
+                                  o.krayf_bot);
+    OG_LAUNCHED();
+  }
   if (y.eddy_on) {
     OG_PROF("eddy_columns", s);
     OG_CHECK(dyn_eddy_columns(C, rayleigh_th, s));
   }
-  if (o.divh_damp_short) divh_damp(C, y.sh_vmt.p, o.dtsm, s);
-  if (o.vort_damp_short) vort_damp(C, y.sh_vmt.p, o.dtsm, s);
+  if (o.divh_damp_short) { OG_PROF("divh_damp", s); divh_damp(C, y.sh_vmt.p, o.dtsm, s); }
+  if (o.vort_damp_short) { OG_PROF("vort_damp", s); vort_damp(C, y.sh_vmt.p, o.dtsm, s); }
   // start values of the fields fluxes_wrtv_monot limits (prog_wrtv_rk.f90:186-198)
   const bool thil_monot = o.ithil_monot > 0, wind_monot = o.iwind_monot > 0;
   const size_t wzb = (size_t)mza * d.mwa * sizeof(float);
@@ -985,7 +994,11 @@ int dyn_prog_wrtv_rk(int istp) {
     const int last = istage == nrk;
     // vmca = vmc arv is formed where it is read; the last stage also keeps
     // it (the flux-corrected faces read it) and adds it to vmasc
-    if (last) { k_vmca<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, y.vmc.p, y.arv.p, y.vmca.p, tp.vmasc.p, 1); OG_LAUNCHED(); }
+    if (last) {
+      OG_PROF("vmca", s);
+      k_vmca<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, y.vmc.p, y.arv.p, y.vmca.p, tp.vmasc.p, 1);
+      OG_LAUNCHED();
+    }
     Four f{{y.thil.p, y.vxe.p, y.vye.p, y.vze.p}};
     // fields by reconstruction order: thil has thil_horiz_adv_order, the
     // winds wind_horiz_adv_order (order 1: no gradient)
@@ -993,12 +1006,18 @@ int dyn_prog_wrtv_rk(int istp) {
                          o.wind_horiz_adv_order};
     unsigned m2 = 0, m3 = 0;
     for (int q = 0; q < 4; ++q) { if (ordf[q] == 2) m2 |= 1u << q; if (ordf[q] >= 3) m3 |= 1u << q; }
-    if (m2) { k_grad4<2><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m2, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
-    if (m3) { k_grad4<3><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m3, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
-    k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p);
-    VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
-    k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, m2 | m3, m3, y.gx.p, vs, y.vmc.p, y.upv.p);
-    OG_LAUNCHED(); OG_LAUNCHED();
+    {
+      OG_PROF("grad4", s);
+      if (m2) { k_grad4<2><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m2, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
+      if (m3) { k_grad4<3><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m3, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
+    }
+    { OG_PROF("upw4", s); k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p); OG_LAUNCHED(); }
+    {
+      OG_PROF("upv4", s);
+      VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
+      k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, m2 | m3, m3, y.gx.p, vs, y.vmc.p, y.upv.p);
+      OG_LAUNCHED();
+    }
     // last stage: flux-corrected face values replace those of the limited fields (370-399)
     if (last && thil_monot) {
       OG_PROF("monot_faces", s);
@@ -1030,12 +1049,19 @@ int dyn_prog_wrtv_rk(int istp) {
     A.gdz_wgtm8 = y.gdz_wgtm8.p; A.gdz_wgtp8 = y.gdz_wgtp8.p; A.gdz_wgtm = y.gdz_wgtm.p; A.gdz_wgtp = y.gdz_wgtp.p;
     A.zwgt_bot8 = y.zwgt_bot8.p; A.zwgt_top8 = y.zwgt_top8.p; A.b20 = y.b20.p;
     const size_t smem = (size_t)WRT_WARPS * mza * 13 * sizeof(double);
-    k_wrt_begs<<<cdiv(d.nw_prog, WRT_WARPS), WRT_WARPS * 32, smem, s>>>(g, A);
-    k_prog_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, dts, y.vmc0.p, y.sh_vmt.p, y.press.p, y.pvfac.p,
-                                 y.vn.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p, y.volvi.p, tp.rho.p, y.vmc.p, y.vc.p);
-    k_vel_t3d<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, tp.wc.p, y.vc.p, y.wno2.p, y.ecv.p, y.vxe.p,
-                                  y.vye.p, y.vze.p);
-    OG_LAUNCHED(); OG_LAUNCHED(); OG_LAUNCHED();
+    { OG_PROF("wrt_begs", s); k_wrt_begs<<<cdiv(d.nw_prog, WRT_WARPS), WRT_WARPS * 32, smem, s>>>(g, A); OG_LAUNCHED(); }
+    {
+      OG_PROF("prog_v", s);
+      k_prog_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, dts, y.vmc0.p, y.sh_vmt.p, y.press.p, y.pvfac.p,
+                                   y.vn.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p, y.volvi.p, tp.rho.p, y.vmc.p, y.vc.p);
+      OG_LAUNCHED();
+    }
+    {
+      OG_PROF("vel_t3d", s);
+      k_vel_t3d<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, tp.wc.p, y.vc.p, y.wno2.p, y.ecv.p, y.vxe.p,
+                                    y.vye.p, y.vze.p);
+      OG_LAUNCHED();
+    }
   }
   (void)wz;
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
