@@ -310,10 +310,12 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
       for (int q = 0; q < TILE_NS / 4; ++q) {
         const int4 so = reinterpret_cast<const int4*>(sl)[q];
         const float4 w4 = reinterpret_cast<const float4*>(rc)[q];
-        fd = fma4s(w4.x, lds4(Ul, so.x), fd);
-        fd = fma4s(w4.y, lds4(Ul, so.y), fd);
-        fd = fma4s(w4.z, lds4(Ul, so.z), fd);
-        fd = fma4s(w4.w, lds4(Ul, so.w), fd);
+        // a slot whose weight is zero at this level (a face whose upwind
+        // side does not reach it) is not read
+        if (w4.x != 0.f) fd = fma4s(w4.x, lds4(Ul, so.x), fd);
+        if (w4.y != 0.f) fd = fma4s(w4.y, lds4(Ul, so.y), fd);
+        if (w4.z != 0.f) fd = fma4s(w4.z, lds4(Ul, so.z), fd);
+        if (w4.w != 0.f) fd = fma4s(w4.w, lds4(Ul, so.w), fd);
       }
       // vertical quadratic upwind faces, fexpl times sum_q beta_q S(kd-2+q) + omega S0
       fd = fma4s(fx * r6.x, m2[n], fd);
