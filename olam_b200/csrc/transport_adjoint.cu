@@ -354,10 +354,12 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
       for (int q = 0; q < TILE_NS / 4; ++q) {
         const int4 so = reinterpret_cast<const int4*>(ro)[q];
         const float4 w4 = reinterpret_cast<const float4*>(rc)[q];
-        acc = fma4s(w4.x, lds4(Ul, so.x), acc);
-        acc = fma4s(w4.y, lds4(Ul, so.y), acc);
-        acc = fma4s(w4.z, lds4(Ul, so.z), acc);
-        acc = fma4s(w4.w, lds4(Ul, so.w), acc);
+        // zero transposed weights (no upwind path between the two columns
+        // at this level) are not read
+        if (w4.x != 0.f) acc = fma4s(w4.x, lds4(Ul, so.x), acc);
+        if (w4.y != 0.f) acc = fma4s(w4.y, lds4(Ul, so.y), acc);
+        if (w4.z != 0.f) acc = fma4s(w4.z, lds4(Ul, so.z), acc);
+        if (w4.w != 0.f) acc = fma4s(w4.w, lds4(Ul, so.w), acc);
       }
       const float fx = FEX[c];
       const float4 r5 = reinterpret_cast<const float4*>(rc)[5];   // a0 .. a3
