@@ -492,17 +492,20 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   }
   const int ntp = C.tr.ntp;
   const size_t plane = (size_t)mza * mwa, qn = plane * ntp;
+  // per-tracer planes on the device start on 16-byte boundaries (the layout
+  // transposes move them in 16-byte pieces)
+  const size_t pstride = (plane + 3) & ~(size_t)3;
 
   OG_CHECK(tp.adj_l[0].alloc(qn));
   OG_CHECK(tp.adj_l[1].alloc(qn));
-  OG_CHECK(tp.adj_l0.alloc(qn));
+  OG_CHECK(tp.adj_l0.alloc(std::max(qn, pstride * n)));
   OG_CHECK(tp.adj_ls.alloc(qn));
-  OG_CHECK(tp.adj_planes.alloc(plane * n));
-  OG_CHECK(planes_table(tp.adj_ptab, tp.adj_planes.p, n, plane, s));
+  OG_CHECK(tp.adj_planes.alloc(pstride * n));
+  OG_CHECK(planes_table(tp.adj_ptab, tp.adj_planes.p, n, pstride, s));
   // lams leaves through lam0's memory, which is free after the last stage
-  OG_CHECK(planes_table(tp.adj_ptab2, tp.adj_l0.p, n, plane, s));
+  OG_CHECK(planes_table(tp.adj_ptab2, tp.adj_l0.p, n, pstride, s));
   for (int i = 0; i < n; ++i)
-    OG_CUDA(cudaMemcpyAsync(tp.adj_planes.p + (size_t)i * plane, lam[i], plane * sizeof(float),
+    OG_CUDA(cudaMemcpyAsync(tp.adj_planes.p + (size_t)i * pstride, lam[i], plane * sizeof(float),
                             cudaMemcpyHostToDevice, s));
 
   {
@@ -557,9 +560,9 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
     }
   }
   for (int i = 0; i < n; ++i) {
-    OG_CUDA(cudaMemcpyAsync(lam[i], tp.adj_planes.p + (size_t)i * plane, plane * sizeof(float),
+    OG_CUDA(cudaMemcpyAsync(lam[i], tp.adj_planes.p + (size_t)i * pstride, plane * sizeof(float),
                             cudaMemcpyDeviceToHost, s));
-    OG_CUDA(cudaMemcpyAsync(lam_sct[i], tp.adj_l0.p + (size_t)i * plane, plane * sizeof(float),
+    OG_CUDA(cudaMemcpyAsync(lam_sct[i], tp.adj_l0.p + (size_t)i * pstride, plane * sizeof(float),
                             cudaMemcpyDeviceToHost, s));
   }
   OG_CUDA(cudaGetLastError());

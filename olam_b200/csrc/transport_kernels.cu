@@ -15,7 +15,9 @@
 // run the last RK stage of the monotonic / positive-definite options.
 //
 // Device level index kd = Fortran k - 1.
+#include <algorithm>
 #include <cfloat>
+#include <cstdint>
 #include <string>
 
 #include "transport_kernels.cuh"
@@ -814,57 +816,89 @@ void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, s
 // layout transposes.  q[(pk) * ntp + n] <-> src[n][pk], pk = point*mza + k.
 // 32x32 tiles through shared memory; both sides coalesced.
 // ---------------------------------------------------------------------------
+// Layout transposes between the per-tracer arrays (one (mza, mwa) plane per
+// tracer, the reference layout) and the batched layout Q[cell][ntp].  A
+// thread moves a block of 4 cells x 8 tracers: eight 16-byte accesses along
+// the cells of one tracer each (a warp covers 512 contiguous bytes per
+// tracer) and four 32-byte accesses along the tracers of one cell each; the
+// warps of a block take consecutive tracer octets of the same cells, so
+// together they write (or read) whole rows of Q.  Tracers n .. ntp-1 of Q are
+// zero.  Unaligned planes or a partial last quad take the element-wise path.
 __global__ void k_gather_q(float* __restrict__ q, const float* const* __restrict__ src, int n, int ntp,
                            size_t npk) {
-  __shared__ float tile[32][33];
-  size_t pk0 = (size_t)blockIdx.x * 32;
-  int n0 = blockIdx.y * 32;
-  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  for (int r = ty; r < 32; r += 8) {
-    int tr = n0 + r;
-    size_t pk = pk0 + tx;
-    float v = 0.f;
-    if (tr < n && pk < npk) v = src[tr][pk];
-    tile[r][tx] = v;
+  const size_t pk = ((size_t)blockIdx.x * 32 + threadIdx.x) * 4;
+  const int t0 = (blockIdx.y * blockDim.y + threadIdx.y) * 8;
+  if (pk >= npk || t0 >= ntp) return;
+  const int nt = min(8, ntp - t0);   // 4 or 8: ntp is a multiple of 4
+  const bool full = pk + 4 <= npk;
+  float v[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    v[i][0] = v[i][1] = v[i][2] = v[i][3] = 0.f;
+    if (i < nt && t0 + i < n) {
+      const float* p = src[t0 + i] + pk;
+      if (full && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+        const float4 x = __ldcs(reinterpret_cast<const float4*>(p));
+        v[i][0] = x.x; v[i][1] = x.y; v[i][2] = x.z; v[i][3] = x.w;
+      } else {
+        for (int j = 0; j < 4; ++j) if (pk + j < npk) v[i][j] = p[j];
+      }
+    }
   }
-  __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    size_t pk = pk0 + r;
-    int tr = n0 + tx;
-    if (pk < npk && tr < ntp) q[pk * ntp + tr] = tile[tx][r];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (pk + j >= npk) break;
+    float4* d = reinterpret_cast<float4*>(q + (pk + j) * ntp + t0);
+    __stcs(d, make_float4(v[0][j], v[1][j], v[2][j], v[3][j]));
+    if (nt == 8) __stcs(d + 1, make_float4(v[4][j], v[5][j], v[6][j], v[7][j]));
   }
 }
 
 __global__ void k_scatter_q(const float* __restrict__ q, float* const* __restrict__ dst, int n, int ntp,
                             size_t npk) {
-  __shared__ float tile[32][33];
-  size_t pk0 = (size_t)blockIdx.x * 32;
-  int n0 = blockIdx.y * 32;
-  int tx = threadIdx.x, ty = threadIdx.y;
-  for (int r = ty; r < 32; r += 8) {
-    size_t pk = pk0 + r;
-    int tr = n0 + tx;
-    float v = 0.f;
-    if (pk < npk && tr < ntp) v = q[pk * ntp + tr];
-    tile[tx][r] = v;
+  const size_t pk = ((size_t)blockIdx.x * 32 + threadIdx.x) * 4;
+  const int t0 = (blockIdx.y * blockDim.y + threadIdx.y) * 8;
+  if (pk >= npk || t0 >= n) return;
+  const int nt = min(8, ntp - t0);
+  const bool full = pk + 4 <= npk;
+  float v[8][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+    if (pk + j < npk) {
+      const float4* sp = reinterpret_cast<const float4*>(q + (pk + j) * ntp + t0);
+      a = __ldcs(sp);
+      if (nt == 8) b = __ldcs(sp + 1);
+    }
+    v[0][j] = a.x; v[1][j] = a.y; v[2][j] = a.z; v[3][j] = a.w;
+    v[4][j] = b.x; v[5][j] = b.y; v[6][j] = b.z; v[7][j] = b.w;
   }
-  __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    int tr = n0 + r;
-    size_t pk = pk0 + tx;
-    if (tr < n && pk < npk) dst[tr][pk] = tile[r][tx];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (i >= nt || t0 + i >= n) break;
+    float* p = dst[t0 + i] + pk;
+    if (full && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+      __stcs(reinterpret_cast<float4*>(p), make_float4(v[i][0], v[i][1], v[i][2], v[i][3]));
+    } else {
+      for (int j = 0; j < 4; ++j) if (pk + j < npk) p[j] = v[i][j];
+    }
   }
 }
 
+// blocks of 32 cell quads x up to 16 tracer octets (warps)
+static dim3 transpose_block(int ntr) { return dim3(32, std::max(1, std::min(16, (ntr + 7) / 8))); }
+
 void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npk, cudaStream_t s) {
-  dim3 grid(cdiv(npk, 32), cdiv(ntp, 32));
-  k_gather_q<<<grid, dim3(32, 8), 0, s>>>(q, src, n, ntp, npk);
+  const dim3 b = transpose_block(ntp);
+  const dim3 grid(cdiv(cdiv(npk, 4), 32), cdiv(cdiv(ntp, 8), b.y));
+  k_gather_q<<<grid, b, 0, s>>>(q, src, n, ntp, npk);
   OG_LAUNCHED();
 }
 
 void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npk, cudaStream_t s) {
-  dim3 grid(cdiv(npk, 32), cdiv(n, 32));
-  k_scatter_q<<<grid, dim3(32, 8), 0, s>>>(q, dst, n, ntp, npk);
+  const dim3 b = transpose_block(n);
+  const dim3 grid(cdiv(cdiv(npk, 4), 32), cdiv(cdiv(n, 8), b.y));
+  k_scatter_q<<<grid, b, 0, s>>>(q, dst, n, ntp, npk);
   OG_LAUNCHED();
 }
 
