@@ -42,18 +42,24 @@ __global__ void k_adj_nonprog(const int* __restrict__ cols, int ncol, size_t col
 
 // the forward stage copies level kb to the levels below: their adjoint folds
 // into kb.  Blocks stride over the prognostic columns, threads over the tracers.
+// thread per (column, four tracers); ntp is a multiple of 4
 __global__ void k_adj_fold0(const int* __restrict__ prog, int nprog, const int* __restrict__ lpw, int mza, int ntp,
                             float* __restrict__ lam) {
-  for (int j = blockIdx.x; j < nprog; j += gridDim.x) {
-    const int iw = prog[j];
-    const int kb = lpw[iw];
-    for (int t = threadIdx.x; t < ntp; t += blockDim.x) {
-      float* c = lam + (size_t)iw * mza * ntp + t;
-      float a = c[(size_t)kb * ntp];
-      for (int k = 0; k < kb; ++k) { a += c[(size_t)k * ntp]; c[(size_t)k * ntp] = 0.f; }
-      c[(size_t)kb * ntp] = a;
-    }
+  const int nq = ntp >> 2;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nprog * nq) return;
+  const int j = (int)(i / nq), t = (int)(i - (size_t)j * nq) * 4;
+  const int iw = prog[j];
+  const int kb = lpw[iw];
+  float* c = lam + (size_t)iw * mza * ntp + t;
+  float4 a = *reinterpret_cast<const float4*>(c + (size_t)kb * ntp);
+  for (int k = 0; k < kb; ++k) {
+    float4* p = reinterpret_cast<float4*>(c + (size_t)k * ntp);
+    const float4 v = *p;
+    a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
+    *p = make_float4(0.f, 0.f, 0.f, 0.f);
   }
+  *reinterpret_cast<float4*>(c + (size_t)kb * ntp) = a;
 }
 
 // transpose of the implicit vertical step (scalar_transport_rk.F90:347-375,
@@ -542,8 +548,8 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
             tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage, dtr, ntp, first, L, tp.adj_l0.p);
         OG_LAUNCHED();
         if (d.nw_prog > 0)
-          k_adj_fold0<<<(unsigned)std::min(d.nw_prog, 148 * 16), 128, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p, mza,
-                                                                              ntp, L);
+          k_adj_fold0<<<cdiv((size_t)d.nw_prog * (ntp / 4), 256), 256, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p,
+                                                                               mza, ntp, L);
         OG_LAUNCHED();
       }
       {
