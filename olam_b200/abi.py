@@ -178,16 +178,28 @@ class FortranGrid:
 
         s = Grid()
         s.mza, s.mwa, s.mva, s.mma = g.mza, g.mwa, g.mva, g.mma
-        # global domain: every real point is prognostic and adjacent
-        self.jtw = i32(np.arange(2, g.mwa + 1))
-        self.jtv = i32(np.arange(2, g.mva + 1))
-        self.jtm = i32(np.arange(2, g.mma + 1))
-        s.nw_prog = s.nw_wadj = g.mwa - 1
-        s.nv_prog = s.nv_wadj = g.mva - 1
-        s.nm_prog = g.mma - 1
-        s.jtw_prog = s.jtw_wadj = ptr(self.jtw, C.c_int)
-        s.jtv_prog = s.jtv_wadj = ptr(self.jtv, C.c_int)
-        s.jtm_prog = ptr(self.jtm, C.c_int)
+        if hasattr(g, "jtw_prog"):
+            # a rank's part of a decomposed grid (olam_b200.decomp): its own
+            # loop tables, 1-based
+            lists = {n: i32(getattr(g, n)) for n in ("jtw_prog", "jtw_wadj", "jtv_prog", "jtv_wadj",
+                                                      "jtm_prog")}
+            self.lists = lists
+            s.nw_prog, s.jtw_prog = lists["jtw_prog"].size, ptr(lists["jtw_prog"], C.c_int)
+            s.nw_wadj, s.jtw_wadj = lists["jtw_wadj"].size, ptr(lists["jtw_wadj"], C.c_int)
+            s.nv_prog, s.jtv_prog = lists["jtv_prog"].size, ptr(lists["jtv_prog"], C.c_int)
+            s.nv_wadj, s.jtv_wadj = lists["jtv_wadj"].size, ptr(lists["jtv_wadj"], C.c_int)
+            s.nm_prog, s.jtm_prog = lists["jtm_prog"].size, ptr(lists["jtm_prog"], C.c_int)
+        else:
+            # global domain: every real point is prognostic and adjacent
+            self.jtw = i32(np.arange(2, g.mwa + 1))
+            self.jtv = i32(np.arange(2, g.mva + 1))
+            self.jtm = i32(np.arange(2, g.mma + 1))
+            s.nw_prog = s.nw_wadj = g.mwa - 1
+            s.nv_prog = s.nv_wadj = g.mva - 1
+            s.nm_prog = g.mma - 1
+            s.jtw_prog = s.jtw_wadj = ptr(self.jtw, C.c_int)
+            s.jtv_prog = s.jtv_wadj = ptr(self.jtv, C.c_int)
+            s.jtm_prog = ptr(self.jtm, C.c_int)
 
         def tab(a):
             # tables hold 0-based array indices where 0 = dummy; entries past
