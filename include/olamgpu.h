@@ -281,6 +281,37 @@ int olamgpu_prog_wrtv_rk(int istp);
 int olamgpu_tend0(float* rho_old);
 int olamgpu_timeavg_momsc(void);
 
+/* ---- halo exchange of the tracer step over ranks ---------------------------
+ * When a rank's grid is one part of a decomposed domain (its own columns
+ * prognosed, two rings of neighbours held as a halo), scalar_transport_rk
+ * exchanges the tracers of the border columns after every RK stage but the
+ * last, as omodel/scalar_transport_rk.F90:315-322, 343, 379 does with
+ * mpi_post_direct_send/recv_w.  The halo is two rings deep, so the
+ * reconstruction planes that OLAM also exchanges (:416-440) are recomputed
+ * locally.  The library packs, per neighbour, the columns to send (all
+ * levels, all tracers) and calls the exchange hook, which moves them (MPI,
+ * NCCL) and fills the receive buffers; the library then writes them into
+ * the halo columns.  The step must be the unlimited one (iscal_monot = 0)
+ * in a batched transport form; otherwise OLAMGPU_E_UNSUPPORTED. */
+typedef struct olamgpu_halo {
+  int nnb;                         /* neighbour ranks                           */
+  const int* rank;                 /* (nnb) their ranks                          */
+  const int* nsend; const int* send_cols;   /* (nnb), concatenated 1-based W    */
+  const int* nrecv; const int* recv_cols;   /* indices of this rank's grid      */
+  int host_staged;                 /* 1: the hook gets host buffers (the library
+                                      copies through pinned memory around it);
+                                      0: device buffers, and the hook orders its
+                                      transfers on the stream it is given      */
+  /* moves sendbuf[i] (sendcount[i] floats) to rank[i] and receives recvbuf[i]
+   * (recvcount[i] floats) from it; returns 0 on success */
+  int (*exchange)(void* user, int nnb, const int* rank, float* const* sendbuf, const size_t* sendcount,
+                  float* const* recvbuf, const size_t* recvcount, void* stream);
+  void* user;
+} olamgpu_halo;
+
+/* Registers the halo plan (NULL: one domain, no exchange). */
+int olamgpu_set_halo(const olamgpu_halo* halo);
+
 /* ---- long-step glue on the device ------------------------------------------
  * set_scalars_bottom (omodel/obnd.f90:7-36): below-ground levels 1..lpw-1
  * of every registered scalar and of thil take the value at lpw, over

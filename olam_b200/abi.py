@@ -90,6 +90,50 @@ class State(C.Structure):
     ]
 
 
+# olamgpu_halo's exchange hook
+HALO_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_float)),
+                      C.POINTER(C.c_size_t), C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_size_t), C.c_void_p)
+
+
+class Halo(C.Structure):
+    """olamgpu_halo: the halo plan of a rank and its exchange hook."""
+    _fields_ = [("nnb", C.c_int), ("rank", c_int_p), ("nsend", c_int_p), ("send_cols", c_int_p),
+                ("nrecv", c_int_p), ("recv_cols", c_int_p), ("host_staged", C.c_int),
+                ("exchange", HALO_FN), ("user", C.c_void_p)]
+
+
+def make_halo(send, recv, fn, host_staged=True):
+    """A Halo over a plan {rank: local 0-based column indices} (olam_b200.decomp)
+    and a Python hook fn(ranks, sendbufs, recvbufs) -> int on numpy views of
+    the buffers (host-staged).  The returned struct keeps its arrays."""
+    ranks = sorted(set(send) | set(recv))
+    rk = np.array(ranks, np.int32)
+    ns = np.array([len(send.get(r, ())) for r in ranks], np.int32)
+    nr = np.array([len(recv.get(r, ())) for r in ranks], np.int32)
+    sc = np.concatenate([np.asarray(send.get(r, []), np.int64) for r in ranks] + [np.zeros(0, np.int64)]) + 1
+    rc = np.concatenate([np.asarray(recv.get(r, []), np.int64) for r in ranks] + [np.zeros(0, np.int64)]) + 1
+    sc = np.ascontiguousarray(sc, np.int32)
+    rc = np.ascontiguousarray(rc, np.int32)
+
+    def hook(user, nnb, rank, sbuf, scount, rbuf, rcount, stream):
+        try:
+            sv = [np.ctypeslib.as_array(sbuf[i], shape=(scount[i],)) for i in range(nnb)]
+            rv = [np.ctypeslib.as_array(rbuf[i], shape=(rcount[i],)) for i in range(nnb)]
+            return int(fn([rank[i] for i in range(nnb)], sv, rv))
+        except Exception:   # an exception must not cross the C frame
+            return 1
+
+    h = Halo()
+    h.nnb = len(ranks)
+    h.rank, h.nsend, h.nrecv = ptr(rk, C.c_int), ptr(ns, C.c_int), ptr(nr, C.c_int)
+    h.send_cols, h.recv_cols = ptr(sc, C.c_int), ptr(rc, C.c_int)
+    h.host_staged = 1 if host_staged else 0
+    h.exchange = HALO_FN(hook)
+    h.user = None
+    h.keep = (rk, ns, nr, sc, rc, h.exchange)
+    return h
+
+
 # olamgpu_timestep flags
 TS_GRAPH, TS_HORIZ_K, TS_MAXMIN, TS_MASS = 1, 2, 4, 8
 

@@ -163,6 +163,7 @@ static void release_all() {
   tp.adj_ptab.release();
   tp.adj_ptab2.release();
   tp.have_turb = false;
+  halo_release();
   glue_release();
   dyn_release();
   C.status.release();
@@ -415,6 +416,11 @@ int olamgpu_prog_wrtv_rk(int istp) { return dyn_prog_wrtv_rk(istp); }
 int olamgpu_tend0(float* rho_old) { return dyn_tend0(rho_old); }
 
 int olamgpu_timeavg_momsc(void) { return dyn_timeavg_momsc(); }
+
+int olamgpu_set_halo(const olamgpu_halo* halo) {
+  glue_drop_graphs();
+  return halo_set(halo);
+}
 
 int olamgpu_set_scalars_bottom(void) { return glue_set_scalars_bottom(); }
 

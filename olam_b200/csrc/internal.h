@@ -287,6 +287,20 @@ struct Glue {
   int last_nmass = 0, last_ntr = 0;
 };
 
+// halo exchange of the tracer step (halo.cu)
+struct Halo {
+  bool on = false, host_staged = false;
+  std::vector<int> rank, nsend, nrecv;
+  size_t ns = 0, nr = 0;             // columns sent / received in all
+  DevBuf<int> send_cols, recv_cols;  // 0-based W indices, neighbour after neighbour
+  DevBuf<float> sendbuf, recvbuf;    // packed columns (all levels and tracers)
+  float* hsend = nullptr;            // pinned host copies (host-staged hook)
+  float* hrecv = nullptr;
+  size_t hcap = 0;
+  int (*fn)(void*, int, const int*, float* const*, const size_t*, float* const*, const size_t*, void*) = nullptr;
+  void* user = nullptr;
+};
+
 struct Context {
   bool initialised = false;
   int device = -1;
@@ -302,6 +316,7 @@ struct Context {
   Transport tp;
   Dyn dy;
   Glue glue;
+  Halo halo;
   DevBuf<int> status;        // device status word (bounds/NaN flags)
 };
 
@@ -348,6 +363,10 @@ int check_device_status();
 
 // transport entry points (transport.cu)
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);
+// halo exchange (halo.cu)
+int halo_set(const olamgpu_halo* h);
+int halo_exchange(Context& C, float* Q, int ntp, cudaStream_t s);
+void halo_release();
 // long-step glue and the recorded step (timestep.cu)
 int glue_set_scalars_bottom();
 int glue_tracer_maxmin(float* smax);

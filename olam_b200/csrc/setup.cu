@@ -61,9 +61,9 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
   if (g->jtm_prog && g->nm_prog > 0)
     OG_CHECK(upload_list(d.jtm_prog, g->jtm_prog, g->nm_prog, mma, "jtm_prog", s));
 
+  std::vector<char> isprog(mwa, 0);
+  for (int j = 0; j < g->nw_prog; ++j) isprog[g->jtw_prog[j] - 1] = 1;
   {
-    std::vector<char> isprog(mwa, 0);
-    for (int j = 0; j < g->nw_prog; ++j) isprog[g->jtw_prog[j] - 1] = 1;
     std::vector<int> np_list;
     for (int i = 0; i < mwa; ++i) if (!isprog[i]) np_list.push_back(i);
     d.n_nonprog = (int)np_list.size();
@@ -71,7 +71,10 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
     OG_CUDA(cudaStreamSynchronize(s));
   }
 
-  // itab_w: npoly in [3,7]; indices checked for the first npoly entries
+  // itab_w: npoly in [3,7]; indices checked for the first npoly entries.  A
+  // column that is not prognosed (the outer halo of a rank's part of a
+  // decomposed domain) may name the dummy point 1 for a neighbour or edge
+  // the rank does not hold; the stages never read past such a column.
   std::vector<int> npoly(mwa), nb((size_t)mwa * 8), ev((size_t)mwa * 8), im((size_t)mwa * 8, 0);
   std::vector<float> dirv((size_t)mwa * 8, 0.f);
   for (int iw = 0; iw < mwa; ++iw) {
@@ -88,7 +91,8 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
     }
     for (int j = 0; j < np; ++j) {
       int wv = g->itab_w_iv[(size_t)iw * 7 + j], ww = g->itab_w_iw[(size_t)iw * 7 + j];
-      if (wv < 2 || wv > mva || ww < 2 || ww > mwa) {
+      const int lo = isprog[iw] ? 2 : 1;
+      if (wv < lo || wv > mva || ww < lo || ww > mwa) {
         set_error("itab_w neighbour index out of range at W point " + std::to_string(iw + 1));
         return OLAMGPU_E_ARG;
       }

@@ -205,6 +205,10 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   if (C.opts.iscal_monot < 0 || C.opts.iscal_monot > 2) { set_error("iscal_monot must be 0, 1 or 2"); return OLAMGPU_E_UNSUPPORTED; }
   const bool batched = C.form != OLAMGPU_TRANSPORT_PLAIN;
   const bool tiled = C.form == OLAMGPU_TRANSPORT_FUSED && tile_stage_available(d, tp, order);
+  if (C.halo.on && (!batched || C.opts.iscal_monot != 0)) {
+    set_error("a halo exchange needs the unlimited step (iscal_monot = 0) in a batched transport form");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
   if (batched && !tp.flat) {
     set_error("the fused transport form needs lpw = lpv = 2 (no terrain); use the plain form");
     return OLAMGPU_E_UNSUPPORTED;
@@ -278,6 +282,8 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
         else launch_fused_stage(d, tp, IN, A, T, OUT, ntp, istage, nrk, dtr, rhos_nrk, s);
       }
       { OG_PROF("implicit_solve", s); launch_implicit_solve(d, tp, nrk, istage, dtr, CTView{A, ntp, 0}, TView{OUT, ntp, 0}, ntp, s); }
+      // border columns for the next stage (scalar_transport_rk.F90:343, 379)
+      if (istage < nrk && C.halo.on) { OG_PROF("halo_exchange", s); OG_CHECK(halo_exchange(C, OUT, ntp, s)); }
       in_b = out_b;
       out_b = (out_b + 1) % 3;
       if (out_b == a) out_b = (out_b + 1) % 3;

@@ -28,7 +28,7 @@ EXPORTS = [
     "olamgpu_profile", "olamgpu_profile_read", "olamgpu_update_scalar_noalloc",
     "olamgpu_scalar_transport_rk_adjoint", "olamgpu_set_eddy", "olamgpu_comp_horiz_k",
     "olamgpu_set_scalars_bottom", "olamgpu_diagvel_t3d", "olamgpu_tracer_maxmin", "olamgpu_mass_sums",
-    "olamgpu_timestep", "olamgpu_timestep_diag",
+    "olamgpu_timestep", "olamgpu_timestep_diag", "olamgpu_set_halo",
 ]
 
 
@@ -72,6 +72,7 @@ def load():
                                                         C.POINTER(abi.c_float_p)]
     lib.olamgpu_set_eddy.argtypes = [C.POINTER(abi.Eddy)]
     lib.olamgpu_comp_horiz_k.argtypes = []
+    lib.olamgpu_set_halo.argtypes = [C.POINTER(abi.Halo)]
     lib.olamgpu_set_scalars_bottom.argtypes = []
     lib.olamgpu_diagvel_t3d.argtypes = []
     lib.olamgpu_tracer_maxmin.argtypes = [abi.c_float_p]
@@ -174,6 +175,12 @@ class OlamGpu:
 
     def comp_horiz_k(self):
         check(self.lib.olamgpu_comp_horiz_k())
+
+    def set_halo(self, halo):
+        """Register a halo plan (an ``abi.Halo``; None: one domain).  The
+        struct and its hook must stay alive while registered."""
+        self._halo = halo
+        check(self.lib.olamgpu_set_halo(C.byref(halo) if halo is not None else None))
 
     # -- long-step glue ------------------------------------------------------------
     def set_scalars_bottom(self):

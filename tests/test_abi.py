@@ -54,6 +54,7 @@ def test_strerror_and_state_errors():
     assert L.olamgpu_mass_sums(0, None, None) == abi.E_STATE
     assert L.olamgpu_timestep(0, 0, None) == abi.E_STATE
     assert L.olamgpu_timestep_diag(None, None) == abi.E_STATE
+    assert L.olamgpu_set_halo(None) == abi.E_STATE
 
 
 def test_null_arguments_rejected():

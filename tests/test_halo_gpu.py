@@ -1,0 +1,105 @@
+"""GPU test of the halo exchange of the tracer step (olamgpu_set_halo;
+omodel/scalar_transport_rk.F90:315-322, 343, 379): each rank of a two-way
+decomposition (olam_b200/decomp.py) runs its part through the library, and
+the exchange hook hands it, after every RK stage but the last, the border
+values its neighbour computes (taken from the single-domain stages of the
+numpy restatement).  Together the ranks' owned columns reproduce the
+single-domain GPU step; the columns each rank sends are its own stage
+values."""
+import numpy as np
+import pytest
+
+import numpy_ref
+import oracle_lib
+from conftest import relerr, small_case
+from olam_b200 import abi, decomp
+from olam_b200.lib import HostState, OlamGpu, OlamGpuError
+from test_transport_gpu import run_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _stages(g, st, dtlm, nrk):
+    """Single-domain stage outputs (float64), [stage][tracer](mwa, mza)."""
+    dt = dtlm * (np.array([1 / 3, 0.5, 1.0]) if nrk == 3 else np.array([0.5, 1.0]))
+    vm, wm, rho = (st.vmasc.astype(np.float64), st.wmasc.astype(np.float64), st.rho.astype(np.float64))
+    out = [[] for _ in range(nrk)]
+    for q0, t0 in zip(st.tracers, st.sct):
+        q0 = q0.astype(np.float64)
+        t0 = t0.astype(np.float64)
+        s = q0.copy()
+        for k in range(nrk):
+            s = numpy_ref.plain_stage(g, vm, wm, rho, s, q0, t0, dt[k])
+            out[k].append(s)
+    return [np.stack(o) for o in out]
+
+
+def _rank(g, st, opts, loc, stages, form, nrk):
+    ntr = len(st.tracers)
+    ntp = (ntr + 3) // 4 * 4
+    mza = g.mza
+    calls = {"n": 0, "send_err": 0.0}
+
+    def hook(ranks, sbuf, rbuf):
+        k = calls["n"]
+        calls["n"] += 1
+        for r, sv, rv in zip(ranks, sbuf, rbuf):
+            if r in loc.send:
+                got = sv.reshape(len(loc.send[r]), mza, ntp)[:, :, :ntr]
+                want = stages[k][:, loc.wmap[loc.send[r]], :].transpose(1, 2, 0)
+                calls["send_err"] = max(calls["send_err"], relerr(got, want))
+            if r in loc.recv:
+                cols = loc.wmap[loc.recv[r]]
+                blk = np.zeros((len(cols), mza, ntp), np.float32)
+                blk[:, :, :ntr] = stages[k][:, cols, :].transpose(1, 2, 0)
+                rv[:] = blk.ravel()
+        return 0
+
+    lg = loc.grid
+    fg = abi.FortranGrid(lg)
+    hs = HostState(vmasc=loc.v(st.vmasc), wmasc=loc.w(st.wmasc), rho=loc.w(st.rho), wc=loc.w(st.wc))
+    dev = OlamGpu(fg, opts, hs)
+    try:
+        dev.set_transport_form(form)
+        var_p = [loc.w(t).copy() for t in st.tracers]
+        var_t = [loc.w(t).copy() for t in st.sct]
+        dev.register_scalars(var_p, var_t)
+        halo = abi.make_halo(loc.send, loc.recv, hook)
+        dev.set_halo(halo)
+        dev.scalar_transport_rk(loc.w(st.rho_old))
+        return np.stack(var_p), calls
+    finally:
+        dev.close()
+
+
+@pytest.mark.parametrize("form", [abi.TRANSPORT_FUSED, abi.TRANSPORT_FUSED_COLUMN])
+@pytest.mark.parametrize("nrk", [2, 3])
+def test_two_ranks_match_one_domain(form, nrk):
+    g, st = small_case(nxp=8, nlev=12, ntr=6)
+    opts = abi.make_opts(1800.0, nrk_scal=nrk)
+    # the restatement has no implicit columns: the case must have none
+    _, ff, _ = oracle_lib.scalar_transport(abi.FortranGrid(g), opts, st.tracers, st.sct, st, want_ff=True)
+    assert not (ff > 0).any()
+    ref, _ = run_gpu(g, st, opts, form)
+    stages = _stages(g, st, 1800.0, nrk)
+    owner = decomp.bisect(g, 2)
+    covered = np.zeros(g.mwa, bool)
+    for r in range(2):
+        loc = decomp.local_grid(g, owner, r)
+        out, calls = _rank(g, st, opts, loc, stages, form, nrk)
+        assert calls["n"] == nrk - 1                 # after every stage but the last
+        assert calls["send_err"] < 1e-5, calls
+        own = loc.owned
+        for n in range(len(st.tracers)):
+            e = relerr(out[n][own], ref[n][loc.wmap[own]])
+            assert e < 1e-5, (r, n, e)
+        covered[loc.wmap[own]] = True
+    assert covered[1:].all()
+
+
+def test_halo_needs_the_unlimited_batched_step():
+    g, st = small_case(nxp=6, nlev=8, ntr=2)
+    loc = decomp.local_grid(g, decomp.bisect(g, 2), 0)
+    opts = abi.make_opts(1800.0)
+    with pytest.raises(OlamGpuError):
+        _rank(g, st, opts, loc, _stages(g, st, 1800.0, 2), abi.TRANSPORT_PLAIN, 2)
