@@ -71,6 +71,14 @@ module olamgpu_c
      type(c_ptr) :: alpha_press, pwfac, pvfac, thilt, vmxet, vmyet, vmzet, vmt
   end type olamgpu_state
 
+  type, bind(C) :: olamgpu_halo
+     integer(c_int) :: nnb
+     type(c_ptr)    :: rank, nsend, send_cols, nrecv, recv_cols
+     integer(c_int) :: host_staged
+     type(c_funptr) :: exchange     ! int f(user, nnb, rank, sendbuf, sendcount, recvbuf, recvcount, stream)
+     type(c_ptr)    :: user
+  end type olamgpu_halo
+
   type, bind(C) :: olamgpu_eddy
      type(c_ptr) :: vkm, vkh, agamma, akm_sfc, sfluxt, kmtop, khtop, kpblh, theta, tair
      type(c_ptr) :: akmodx, akhodx, kmtopv, khtopv, lsw
@@ -141,6 +149,10 @@ module olamgpu_c
      end function
      integer(c_int) function olamgpu_comp_horiz_k() bind(C, name="olamgpu_comp_horiz_k")
        import :: c_int
+     end function
+     integer(c_int) function olamgpu_set_halo(halo) bind(C, name="olamgpu_set_halo")
+       import :: c_int, olamgpu_halo
+       type(olamgpu_halo), intent(in) :: halo
      end function
      integer(c_int) function olamgpu_finalize() bind(C, name="olamgpu_finalize")
        import :: c_int
