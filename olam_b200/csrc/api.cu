@@ -163,6 +163,7 @@ static void release_all() {
   tp.adj_ptab.release();
   tp.adj_ptab2.release();
   tp.have_turb = false;
+  transport_release_pipeline();
   halo_release();
   glue_release();
   dyn_release();

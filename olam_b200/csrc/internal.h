@@ -216,6 +216,11 @@ struct Transport {
   DevBuf<float> upv, hiv, sfv;   // V-face arrays
   DevBuf<float> scale, upw;      // W arrays for monot/pd
   DevBuf<float> plain_out[2];    // per-tracer stage outputs of the plain form
+  // the pipelined per-call step (transport.cu): copy streams, events of
+  // its tracer groups, device tables of the per-tracer arrays
+  cudaStream_t s_up = nullptr, s_dn = nullptr;
+  std::vector<cudaEvent_t> ev;
+  DevBuf<float*> ptab_p, ptab_t;
   DevBuf<int> d_mode;            // per-tracer last-stage mode
   std::vector<int> h_mode;       // what d_mode holds (uploaded when it changes)
   DevBuf<float> wrec;            // (mwa, mza, TILE_WR) weight records of the step
@@ -363,6 +368,7 @@ int check_device_status();
 
 // transport entry points (transport.cu)
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag);
+void transport_release_pipeline();
 // halo exchange (halo.cu)
 int halo_set(const olamgpu_halo* h);
 int halo_exchange(Context& C, float* Q, int ntp, cudaStream_t s);

@@ -184,6 +184,105 @@ int transport_prepare(Context& C, const float* rho_old_host, bool upload_tracers
   return OLAMGPU_OK;
 }
 
+void transport_release_pipeline() {
+  Transport& tp = ctx().tp;
+  for (cudaEvent_t e : tp.ev) cudaEventDestroy(e);
+  tp.ev.clear();
+  if (tp.s_up) cudaStreamDestroy(tp.s_up);
+  if (tp.s_dn) cudaStreamDestroy(tp.s_dn);
+  tp.s_up = tp.s_dn = nullptr;
+  tp.ptab_p.release();
+  tp.ptab_t.release();
+}
+
+// The per-call step in tracer groups of 64 (one tile group each): the
+// host->device copies of a group's scp and sct (stream s_up), its gather
+// into the batched layout, its RK stages and its scatter back (the library
+// stream), and the device->host copies of its result (stream s_dn) are
+// ordered by events, so group g's step overlaps group g+1's copies in and
+// group g-1's copies out on the two copy engines.  The state and the
+// step's records are on the device already (transport_prepare, k_weights).
+static int pipelined_step(Context& C, const float* dtlr, const float* rhos_nrk) {
+  const DevGrid& d = C.g;
+  Transport& tp = C.tp;
+  Tracers& tr = C.tr;
+  cudaStream_t s = C.stream;
+  const int nrk = C.opts.nrk_scal, ntp = tr.ntp, n = tr.n;
+  const size_t npk = (size_t)d.mza * d.mwa, plane = npk * sizeof(float);
+  const int ngrp = (ntp + 63) / 64;
+  if (!tp.s_up) OG_CUDA(cudaStreamCreateWithFlags(&tp.s_up, cudaStreamNonBlocking));
+  if (!tp.s_dn) OG_CUDA(cudaStreamCreateWithFlags(&tp.s_dn, cudaStreamNonBlocking));
+  while ((int)tp.ev.size() < 2 * ngrp + 1) {
+    cudaEvent_t e;
+    OG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    tp.ev.push_back(e);
+  }
+  for (int b = 0; b < 3; ++b) OG_CHECK(tr.q[b].alloc(npk * ntp));
+  OG_CHECK(tr.qt.alloc(npk * ntp));
+  {
+    std::vector<float*> hp(n), ht(n);
+    for (int i = 0; i < n; ++i) { hp[i] = tr.p[i].p; ht[i] = tr.t[i].p; }
+    OG_CHECK(tp.ptab_p.alloc(n));
+    OG_CHECK(tp.ptab_t.alloc(n));
+    OG_CUDA(cudaMemcpyAsync(tp.ptab_p.p, hp.data(), n * sizeof(float*), cudaMemcpyHostToDevice, s));
+    OG_CUDA(cudaMemcpyAsync(tp.ptab_t.p, ht.data(), n * sizeof(float*), cudaMemcpyHostToDevice, s));
+    OG_CUDA(cudaStreamSynchronize(s));   // the host vectors die here
+  }
+  { OG_PROF("tile_weights", s); OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s)); }
+  // the RK buffer sequence of the batched step
+  const int a = tr.qcur;
+  int bin[3], bout[3];
+  {
+    int in_b = a, out_b = (a + 1) % 3;
+    for (int k = 0; k < nrk; ++k) {
+      bin[k] = in_b;
+      bout[k] = out_b;
+      in_b = out_b;
+      out_b = (out_b + 1) % 3;
+      if (out_b == a) out_b = (out_b + 1) % 3;
+    }
+  }
+  const int fin = bout[nrk - 1];
+  // copies in may start at once: the previous call has ended
+  for (int g = 0; g < ngrp; ++g) {
+    const int tb = 64 * g, tc = std::min(64, n - tb), width = std::min(64, ntp - tb);
+    if (tc <= 0) break;
+    for (int i = tb; i < tb + tc; ++i) {
+      OG_CUDA(cudaMemcpyAsync(tr.p[i].p, tr.h_p[i], plane, cudaMemcpyHostToDevice, tp.s_up));
+      OG_CUDA(cudaMemcpyAsync(tr.t[i].p, tr.h_t[i], plane, cudaMemcpyHostToDevice, tp.s_up));
+    }
+    OG_CUDA(cudaEventRecord(tp.ev[2 * g], tp.s_up));
+    OG_CUDA(cudaStreamWaitEvent(s, tp.ev[2 * g], 0));
+    float* A = tr.q[a].p;
+    launch_gather_q_range(A + tb, (const float* const*)tp.ptab_p.p + tb, tc, width, ntp, npk, s);
+    launch_gather_q_range(tr.qt.p + tb, (const float* const*)tp.ptab_t.p + tb, tc, width, ntp, npk, s);
+    for (int istage = 1; istage <= nrk; ++istage) {
+      const float dtr = dtlr[istage - 1];
+      float* IN = tr.q[bin[istage - 1]].p;
+      float* OUT = tr.q[bout[istage - 1]].p;
+      {
+        OG_PROF(istage == 1 ? "tile_stage1" : "tile_stage", s);
+        OG_CHECK(launch_tile_stage(d, tp, IN, A, tr.qt.p, OUT, ntp, istage, nrk, dtr, C.status.p, s, g, 1));
+      }
+      {
+        OG_PROF("implicit_solve", s);
+        launch_implicit_solve(d, tp, nrk, istage, dtr, CTView{A, ntp, tb}, TView{OUT, ntp, tb}, width, s);
+      }
+    }
+    launch_scatter_q_range(tr.q[fin].p + tb, tp.ptab_p.p + tb, tc, width, ntp, npk, s);
+    OG_CUDA(cudaEventRecord(tp.ev[2 * g + 1], s));
+    OG_CUDA(cudaStreamWaitEvent(tp.s_dn, tp.ev[2 * g + 1], 0));
+    for (int i = tb; i < tb + tc; ++i)
+      OG_CUDA(cudaMemcpyAsync(tr.h_p[i], tr.p[i].p, plane, cudaMemcpyDeviceToHost, tp.s_dn));
+  }
+  // the library stream ends after the last copy out
+  OG_CUDA(cudaEventRecord(tp.ev[2 * ngrp], tp.s_dn));
+  OG_CUDA(cudaStreamWaitEvent(s, tp.ev[2 * ngrp], 0));
+  tr.qcur = fin;
+  tr.q_valid = false;   // the per-tracer arrays hold the result too
+  return OLAMGPU_OK;
+}
+
 int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   Context& C = ctx();
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
@@ -220,8 +319,13 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   if (batched && !tiled && d.ew_order != order)
     OG_CHECK(build_fused_weights(&C.hgrid, C.g, order, s));
 
+  // per-call step (SYNC_EACH_CALL) of the tiled, unlimited step on a global
+  // domain: the tracers go through in groups of 64 so that the copies in,
+  // the step and the copies out of different groups overlap
+  const bool pipelined = C.coherence == OLAMGPU_SYNC_EACH_CALL && tiled && C.opts.iscal_monot == 0 &&
+                         !tp.have_turb && !C.halo.on && d.n_nonprog == 0 && tr.n > 64;
   float dtlr[3];
-  OG_CHECK(transport_prepare(C, rho_old_host, true, dtlr));
+  OG_CHECK(transport_prepare(C, rho_old_host, !pipelined, dtlr));
   const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * wz;
 
   // last-stage mode per tracer
@@ -246,7 +350,9 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   }
   const bool any_pdm = std::any_of(pdm.begin(), pdm.end(), [](int v) { return v != 0; });
 
-  if (batched) {
+  if (pipelined) {
+    OG_CHECK(pipelined_step(C, dtlr, rhos_nrk));
+  } else if (batched) {
     OG_CHECK(ensure_q(s));
     const int ntp = tr.ntp;
     const int a = tr.qcur;
@@ -352,7 +458,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     OG_CHECK(decode(red[2], red[3], diag->cflh_max, diag->cflh_k, diag->cflh_iwglobe, false));
     OG_CHECK(decode(red[4], red[5], diag->w_max, diag->w_k, diag->w_iwglobe, true));
   }
-  if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(tracers_to_host(s));
+  if (C.coherence == OLAMGPU_SYNC_EACH_CALL && !pipelined) OG_CHECK(tracers_to_host(s));
   OG_CUDA(cudaGetLastError());
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
     OG_CUDA(cudaStreamSynchronize(s));

@@ -824,12 +824,14 @@ void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, s
 // warps of a block take consecutive tracer octets of the same cells, so
 // together they write (or read) whole rows of Q.  Tracers n .. ntp-1 of Q are
 // zero.  Unaligned planes or a partial last quad take the element-wise path.
-__global__ void k_gather_q(float* __restrict__ q, const float* const* __restrict__ src, int n, int ntp,
-                           size_t npk) {
+// width: tracer slots of a Q row written (a multiple of 4), stride: Q's row
+// length; n <= width of them come from src, the rest are zero
+__global__ void k_gather_q(float* __restrict__ q, const float* const* __restrict__ src, int n, int width,
+                           int stride, size_t npk) {
   const size_t pk = ((size_t)blockIdx.x * 32 + threadIdx.x) * 4;
   const int t0 = (blockIdx.y * blockDim.y + threadIdx.y) * 8;
-  if (pk >= npk || t0 >= ntp) return;
-  const int nt = min(8, ntp - t0);   // 4 or 8: ntp is a multiple of 4
+  if (pk >= npk || t0 >= width) return;
+  const int nt = min(8, width - t0);   // 4 or 8
   const bool full = pk + 4 <= npk;
   float v[8][4];
 #pragma unroll
@@ -848,25 +850,25 @@ __global__ void k_gather_q(float* __restrict__ q, const float* const* __restrict
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     if (pk + j >= npk) break;
-    float4* d = reinterpret_cast<float4*>(q + (pk + j) * ntp + t0);
+    float4* d = reinterpret_cast<float4*>(q + (pk + j) * stride + t0);
     __stcs(d, make_float4(v[0][j], v[1][j], v[2][j], v[3][j]));
     if (nt == 8) __stcs(d + 1, make_float4(v[4][j], v[5][j], v[6][j], v[7][j]));
   }
 }
 
-__global__ void k_scatter_q(const float* __restrict__ q, float* const* __restrict__ dst, int n, int ntp,
-                            size_t npk) {
+__global__ void k_scatter_q(const float* __restrict__ q, float* const* __restrict__ dst, int n, int width,
+                            int stride, size_t npk) {
   const size_t pk = ((size_t)blockIdx.x * 32 + threadIdx.x) * 4;
   const int t0 = (blockIdx.y * blockDim.y + threadIdx.y) * 8;
   if (pk >= npk || t0 >= n) return;
-  const int nt = min(8, ntp - t0);
+  const int nt = min(8, width - t0);
   const bool full = pk + 4 <= npk;
   float v[8][4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
     if (pk + j < npk) {
-      const float4* sp = reinterpret_cast<const float4*>(q + (pk + j) * ntp + t0);
+      const float4* sp = reinterpret_cast<const float4*>(q + (pk + j) * stride + t0);
       a = __ldcs(sp);
       if (nt == 8) b = __ldcs(sp + 1);
     }
@@ -888,18 +890,28 @@ __global__ void k_scatter_q(const float* __restrict__ q, float* const* __restric
 // blocks of 32 cell quads x up to 16 tracer octets (warps)
 static dim3 transpose_block(int ntr) { return dim3(32, std::max(1, std::min(16, (ntr + 7) / 8))); }
 
-void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npk, cudaStream_t s) {
-  const dim3 b = transpose_block(ntp);
-  const dim3 grid(cdiv(cdiv(npk, 4), 32), cdiv(cdiv(ntp, 8), b.y));
-  k_gather_q<<<grid, b, 0, s>>>(q, src, n, ntp, npk);
+void launch_gather_q_range(float* q, const float* const* src, int n, int width, int stride, size_t npk,
+                           cudaStream_t s) {
+  const dim3 b = transpose_block(width);
+  const dim3 grid(cdiv(cdiv(npk, 4), 32), cdiv(cdiv(width, 8), b.y));
+  k_gather_q<<<grid, b, 0, s>>>(q, src, n, width, stride, npk);
   OG_LAUNCHED();
 }
 
-void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npk, cudaStream_t s) {
+void launch_scatter_q_range(const float* q, float* const* dst, int n, int width, int stride, size_t npk,
+                            cudaStream_t s) {
   const dim3 b = transpose_block(n);
   const dim3 grid(cdiv(cdiv(npk, 4), 32), cdiv(cdiv(n, 8), b.y));
-  k_scatter_q<<<grid, b, 0, s>>>(q, dst, n, ntp, npk);
+  k_scatter_q<<<grid, b, 0, s>>>(q, dst, n, width, stride, npk);
   OG_LAUNCHED();
+}
+
+void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npk, cudaStream_t s) {
+  launch_gather_q_range(q, src, n, ntp, ntp, npk, s);
+}
+
+void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npk, cudaStream_t s) {
+  launch_scatter_q_range(q, dst, n, ntp, ntp, npk, s);
 }
 
 // ---------------------------------------------------------------------------

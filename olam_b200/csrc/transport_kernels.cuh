@@ -77,13 +77,19 @@ bool tile_stage_available(const DevGrid& d, const Transport& tp, int order);
 int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cudaStream_t s);
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
                       const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr, int* status,
-                      cudaStream_t s);
+                      cudaStream_t s, int grp0 = 0, int ngrp_run = 0);
 
 // copy the columns outside jtw_prog (colsize floats each) from src to dst
 void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, size_t colsize,
                       cudaStream_t s);
 
 // layout transposes: per-tracer arrays <-> batched layout
+// tracers [0, n) of src / dst into slots [0, width) of Q rows of length
+// stride (q and src / dst offset by the caller to a tracer range)
+void launch_gather_q_range(float* q, const float* const* src, int n, int width, int stride, size_t npk,
+                           cudaStream_t s);
+void launch_scatter_q_range(const float* q, float* const* dst, int n, int width, int stride, size_t npk,
+                            cudaStream_t s);
 void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t npts_k,
                      cudaStream_t s);
 void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npts_k,

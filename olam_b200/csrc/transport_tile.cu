@@ -53,6 +53,7 @@ struct WeightArgs {
 
 struct TileArgs {
   int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa;
+  int grp0, ngrp;                   // the tracer groups of 64 this launch runs
   float dtr;
   const int4* __restrict__ hdr;
   const int* __restrict__ ulist;
@@ -183,8 +184,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int T = 16 * NC;
   // the tracer groups of a tile run side by side (its records are read once from HBM)
-  const int ngrp = (A.ntp + 63) >> 6;
-  const int tile = blockIdx.x / ngrp, grp = blockIdx.x - tile * ngrp;
+  const int ngrp = A.ngrp;
+  const int tile = blockIdx.x / ngrp, grp = A.grp0 + (blockIdx.x - tile * ngrp);
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;
@@ -384,7 +385,7 @@ bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
 
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
                       const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr, int* status,
-                      cudaStream_t s) {
+                      cudaStream_t s, int grp0, int ngrp_run) {
   if (tp.wrec.n != (size_t)d.mza * d.mwa * TILE_WR) {
     set_error("tile stage: the weight records of the step were not formed");
     return OLAMGPU_E_STATE;
@@ -399,8 +400,11 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   A.S = S; A.S0 = S0; A.SCT = SCT; A.OUT = OUT;
   A.err = status;
   const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, d.mza);
-  const unsigned ngrp = (unsigned)((ntp + 63) / 64);
-  const unsigned nblk = (unsigned)d.ntiles * ngrp;
+  const int ngrp_all = (ntp + 63) / 64;
+  if (ngrp_run <= 0) { grp0 = 0; ngrp_run = ngrp_all; }
+  if (grp0 < 0 || grp0 + ngrp_run > ngrp_all) { set_error("tile stage: tracer groups out of range"); return OLAMGPU_E_ARG; }
+  A.grp0 = grp0; A.ngrp = ngrp_run;
+  const unsigned nblk = (unsigned)d.ntiles * (unsigned)ngrp_run;
   // element offsets in 32 bits when every array of the batched layout fits
   const bool off32 = (double)d.mwa * d.mza * ntp < 4294967296.0;
   alignas(64) CUtensorMap tmS, tmR;

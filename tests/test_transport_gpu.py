@@ -119,3 +119,21 @@ def test_fused_forms_agree_many_tracers(ntr, order):
     for n in range(st.ntr):
         assert relerr(a[n], b[n]) < 1e-6, (n, relerr(a[n], b[n]))
         assert relerr(c[n], b[n]) < 1e-6, (n, relerr(c[n], b[n]))
+
+
+def test_per_call_step_in_tracer_groups():
+    # more than 64 tracers in the per-call (SYNC_EACH_CALL) mode: the tiled
+    # step runs group by group with the copies in and out overlapped; the
+    # result is the device-resident step's, bit for bit, and the oracle's
+    g, st = small_case(nxp=5, nlev=10, ntr=70)
+    opts = abi.make_opts(1800.0)
+    sync, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED, coherence=abi.SYNC_EACH_CALL, steps=2)
+    res, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED, coherence=abi.RESIDENT, steps=2)
+    assert np.array_equal(sync[:, 1:], res[:, 1:])
+    fg = abi.FortranGrid(g)
+    sel = [0, 63, 64, 69]
+    ref64 = oracle_lib.scalar_transport(fg, opts, [st.tracers[i] for i in sel], [st.sct[i] for i in sel], st,
+                                        fp64=True)
+    one, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED, coherence=abi.SYNC_EACH_CALL, steps=1)
+    for j, i in enumerate(sel):
+        assert relerr(one[i], ref64[j]) < TOL64, (i, relerr(one[i], ref64[j]))
