@@ -119,7 +119,34 @@ static int require_device() {
   return OLAMGPU_OK;
 }
 
+// page-lock OLAM's state arrays in place so that the per-call copies run at
+// full speed and asynchronously; a failure only costs transfer speed
+static std::vector<void*> g_pinned_state;
+
+static void register_state_arrays(Context& C) {
+  if (!C.have_state) return;
+  const size_t wz = (size_t)C.g.mza * C.g.mwa, vz = (size_t)C.g.mza * C.g.mva;
+  const olamgpu_state& h = C.hstate;
+  const std::pair<void*, size_t> arr[] = {
+      {h.rho, wz * 8}, {h.press, wz * 8}, {h.thil, wz * 4}, {h.wc, wz * 4}, {h.wmc, wz * 4}, {h.vxe, wz * 4},
+      {h.vye, wz * 4}, {h.vze, wz * 4}, {h.vmc, vz * 4}, {h.vc, vz * 4}, {h.vmasc, vz * 4}, {h.wmasc, wz * 4},
+      {h.alpha_press, wz * 4}, {h.pwfac, wz * 4}, {h.pvfac, vz * 4}, {h.thilt, wz * 4}, {h.vmxet, wz * 4},
+      {h.vmyet, wz * 4}, {h.vmzet, wz * 4}, {h.vmt, vz * 4}};
+  for (const auto& a : arr) {
+    if (!a.first) continue;
+    if (cudaHostRegister(a.first, a.second, cudaHostRegisterDefault) == cudaSuccess) g_pinned_state.push_back(a.first);
+    cudaGetLastError();
+  }
+}
+
+static void unregister_state_arrays() {
+  for (void* p : g_pinned_state) cudaHostUnregister(p);
+  g_pinned_state.clear();
+  cudaGetLastError();
+}
+
 static void release_all() {
+  unregister_state_arrays();
   Context& C = ctx();
   DevGrid& d = C.g;
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
@@ -220,6 +247,7 @@ int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts, const olamg
     }
   }
   if (state) { C.hstate = *state; C.have_state = true; } else C.have_state = false;
+  register_state_arrays(C);
   // prog_wrtv_rk needs the dynamics state and the M-point tables; without
   // them only scalar_transport_rk is available
   if (state && state->thil && state->vmc && state->press && grid->itab_m_iv && grid->jtm_prog) {

@@ -809,6 +809,9 @@ int dyn_state_to_device(unsigned mask, cudaStream_t s) {
     OG_CHECK(cp(y.vmyet.p, h.vmyet, wz * 4)); OG_CHECK(cp(y.vmzet.p, h.vmzet, wz * 4));
     OG_CHECK(cp(y.vmt.p, h.vmt, vz * 4));
   }
+  // the registered arrays are page-locked: the copies read them when they
+  // run, so they must end before the caller may write them again
+  OG_CUDA(cudaStreamSynchronize(s));
   return OLAMGPU_OK;
 }
 

@@ -153,11 +153,14 @@ int transport_prepare(Context& C, const float* rho_old_host, bool upload_tracers
       OG_CHECK(dyn_state_to_device(OLAMGPU_F_ALL, s));
       C.dy.uploaded = true;
     }
-    if (!tp.vmasc.p) OG_CHECK(upload(tp.vmasc, C.hstate.vmasc, vz, s));
-    if (!tp.wmasc.p) OG_CHECK(upload(tp.wmasc, C.hstate.wmasc, wz, s));
-    if (!tp.rho.p) OG_CHECK(upload(tp.rho, C.hstate.rho, wz, s));
-    if (!tp.wc.p && C.hstate.wc) OG_CHECK(upload(tp.wc, C.hstate.wc, wz, s));
-    if (rho_old_host) OG_CHECK(upload(tp.rho_old, rho_old_host, wz, s));
+    bool copied = false;
+    if (!tp.vmasc.p) { OG_CHECK(upload(tp.vmasc, C.hstate.vmasc, vz, s)); copied = true; }
+    if (!tp.wmasc.p) { OG_CHECK(upload(tp.wmasc, C.hstate.wmasc, wz, s)); copied = true; }
+    if (!tp.rho.p) { OG_CHECK(upload(tp.rho, C.hstate.rho, wz, s)); copied = true; }
+    if (!tp.wc.p && C.hstate.wc) { OG_CHECK(upload(tp.wc, C.hstate.wc, wz, s)); copied = true; }
+    if (rho_old_host) { OG_CHECK(upload(tp.rho_old, rho_old_host, wz, s)); copied = true; }
+    // page-locked sources are read when the copies run
+    if (copied) OG_CUDA(cudaStreamSynchronize(s));
     if (!tp.rho_old.p) {
       set_error("rho_old is NULL and no device copy exists (pass it once or call olamgpu_tend0)");
       return OLAMGPU_E_STATE;
