@@ -44,7 +44,18 @@ struct DynK {
   const int* __restrict__ lpm;
   const float* __restrict__ volti;
   const float* __restrict__ a_w;
+  // flat: lpw = lpv = 2 everywhere (device level 1), no table read needed;
+  // off_*: the loop table is the contiguous run off, off + 1, ... (a
+  // global domain), no table read needed; -1 otherwise
+  int flat, off_w, off_vp, off_va;
 };
+
+// lowest device level of a W / V point; a loop table's j-th entry
+#define LPW(i) (g.flat ? 1 : g.lpw[i])
+#define LPV(i) (g.flat ? 1 : g.lpv[i])
+#define WTAB(j) (g.off_w >= 0 ? g.off_w + (j) : prog[j])
+#define VPTAB(j) (g.off_vp >= 0 ? g.off_vp + (j) : vprog[j])
+#define VATAB(j) (g.off_va >= 0 ? g.off_va + (j) : vadj[j])
 
 static DynK dynk(const DevGrid& d) {
   DynK k;
@@ -52,6 +63,8 @@ static DynK dynk(const DevGrid& d) {
   k.npoly = d.npoly.p; k.w_nb = d.w_nb.p; k.w_ev = d.w_ev.p; k.w_dirv = d.w_dirv.p;
   k.v_iw = d.v_iw.p; k.v_im = d.v_im.p; k.m_iv = d.m_iv.p; k.m_im = d.m_im.p;
   k.lpw = d.lpw.p; k.lpv = d.lpv.p; k.lpm = d.lpm.p; k.volti = d.volti.p; k.a_w = d.a_w.p;
+  k.flat = ctx().tp.flat ? 1 : 0;
+  k.off_w = d.off_wprog; k.off_vp = d.off_vprog; k.off_va = d.off_vwadj;
   return k;
 }
 
@@ -73,8 +86,8 @@ struct SetupW {
 
 __global__ void k_setup_w(DynK g, const int* __restrict__ prog, int nprog, SetupW a) {
   PK(j, kd, nprog);
-  const int iw = prog[j];
-  if (kd < g.lpw[iw]) return;
+  const int iw = WTAB(j);
+  if (kd < LPW(iw)) return;
   const size_t x = (size_t)iw * g.mza + kd;
   const float v4 = (float)a.volt[x];
   a.rth0[x] = (double)a.thil[x] * a.rho[x];
@@ -94,7 +107,7 @@ __global__ void k_setup_v(DynK g, const int* __restrict__ vprog, int nv, const f
                           const float* __restrict__ rayf_cof, const float* __restrict__ vc03d,
                           const float* __restrict__ vc, const double* __restrict__ rho, int krayf_bot) {
   PK(j, kd, nv);
-  const int iv = vprog[j];
+  const int iv = VPTAB(j);
   const size_t x = (size_t)iv * g.mza + kd;
   vmc0[x] = vmc[x];
   float v = vmt[x];
@@ -113,8 +126,8 @@ __global__ void k_div_fdivh(DynK g, const int* __restrict__ vprog, int nv, const
                             const float* __restrict__ dzit, const double* __restrict__ volt, double facth,
                             int level, float fact2, float* __restrict__ fdivh) {
   PK(j, kd, nv);
-  const int iv = vprog[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VPTAB(j);
+  if (kd < LPV(iv)) return;
   const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
   const double vmin = fmin(volt[(size_t)iw1 * g.mza + kd], volt[(size_t)iw2 * g.mza + kd]);
   double v;
@@ -135,16 +148,16 @@ __global__ void k_div_fdivh(DynK g, const int* __restrict__ vprog, int nv, const
 __global__ void k_div_accum(DynK g, const int* __restrict__ prog, int nprog, const float* __restrict__ arv,
                             const float* __restrict__ vmc, float* __restrict__ div1) {
   PK(j, kd, nprog);
-  const int iw = prog[j];
+  const int iw = WTAB(j);
   const size_t x = (size_t)iw * g.mza + kd;
   float d = div1[x];
   const int np = g.npoly[iw];
   for (int n = 0; n < np; ++n) {
     const int iv = g.w_ev[iw * 8 + n];
-    if (kd >= g.lpv[iv])
+    if (kd >= LPV(iv))
       d = d - arv[(size_t)iv * g.mza + kd] * g.w_dirv[iw * 8 + n] * vmc[(size_t)iv * g.mza + kd];
   }
-  if (kd >= g.lpw[iw]) d = d * g.volti[x];
+  if (kd >= LPW(iw)) d = d * g.volti[x];
   div1[x] = d;
 }
 
@@ -152,13 +165,13 @@ __global__ void k_div_accum(DynK g, const int* __restrict__ prog, int nprog, con
 __global__ void k_lap_w(DynK g, const int* __restrict__ prog, int nprog, const float* __restrict__ xx_yy,
                         const float* __restrict__ src, float* __restrict__ dst) {
   PK(j, kd, nprog);
-  const int iw = prog[j];
+  const int iw = WTAB(j);
   const size_t x = (size_t)iw * g.mza + kd;
   float d = 0.f;
   const int np = g.npoly[iw];
   for (int n = 0; n < np; ++n) {
     const int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
-    if (kd >= g.lpv[iv]) d = d + (src[(size_t)iwn * g.mza + kd] - src[x]) * xx_yy[iw * 7 + n];
+    if (kd >= LPV(iv)) d = d + (src[(size_t)iwn * g.mza + kd] - src[x]) * xx_yy[iw * 7 + n];
   }
   dst[x] = d;
 }
@@ -166,8 +179,8 @@ __global__ void k_lap_w(DynK g, const int* __restrict__ prog, int nprog, const f
 __global__ void k_div_apply(DynK g, const int* __restrict__ vprog, int nv, const float* __restrict__ fdivh,
                             const float* __restrict__ dh, float* __restrict__ vmt) {
   PK(j, kd, nv);
-  const int iv = vprog[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VPTAB(j);
+  if (kd < LPV(iv)) return;
   const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
   const size_t x = (size_t)iv * g.mza + kd;
   vmt[x] = vmt[x] + fdivh[x] * (dh[(size_t)iw2 * g.mza + kd] - dh[(size_t)iw1 * g.mza + kd]);
@@ -181,7 +194,7 @@ __global__ void k_vort_first_m(DynK g, const int* __restrict__ mprog, int nm, co
   if (j >= nm) return;
   const int im = mprog[j];
   int lm = 1 << 30;
-  for (int jv = 0; jv < 3; ++jv) lm = min(lm, g.lpv[g.m_iv[im * 3 + jv]]);
+  for (int jv = 0; jv < 3; ++jv) lm = min(lm, LPV(g.m_iv[im * 3 + jv]));
   lpmmin[im] = lm;
   for (int jv = 0; jv < 3; ++jv) {
     const int iv = g.m_iv[im * 3 + jv];
@@ -195,7 +208,7 @@ __global__ void k_vort_first_v(DynK g, const int* __restrict__ vprog, int nv, co
                                float* __restrict__ fvorth, float* __restrict__ fvortl) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nv) return;
-  const int iv = vprog[j];
+  const int iv = VPTAB(j);
   const int im1 = g.v_im[iv * 2], im2 = g.v_im[iv * 2 + 1];
   const float a = -fact * fminf(arm0[im1], arm0[im2]);
   float ph = 1.f, pl = 1.f;
@@ -212,7 +225,7 @@ __global__ void k_vort(DynK g, const int* __restrict__ mprog, int nm, const floa
   float v = 0.f;
   for (int jv = 0; jv < 3; ++jv) {
     const int iv = g.m_iv[im * 3 + jv];
-    if (kd >= g.lpv[iv]) v = v + vc[(size_t)iv * g.mza + kd] * vfact[im * 3 + jv];
+    if (kd >= LPV(iv)) v = v + vc[(size_t)iv * g.mza + kd] * vfact[im * 3 + jv];
   }
   v1[(size_t)im * g.mza + kd] = v;
 }
@@ -226,7 +239,7 @@ __global__ void k_lap_m(DynK g, const int* __restrict__ mprog, int nm, const flo
   float d = 0.f;
   for (int jj = 0; jj < 3; ++jj) {
     const int imn = g.m_im[im * 3 + jj];
-    if (kd >= g.lpv[g.m_iv[im * 3 + jj]]) d = d + (src[(size_t)imn * g.mza + kd] - src[x]) * xx_yy_m[im * 3 + jj];
+    if (kd >= LPV(g.m_iv[im * 3 + jj])) d = d + (src[(size_t)imn * g.mza + kd] - src[x]) * xx_yy_m[im * 3 + jj];
   }
   dst[x] = d;
 }
@@ -236,8 +249,8 @@ __global__ void k_vort_apply(DynK g, const int* __restrict__ vprog, int nv, int 
                              const float* __restrict__ dl, const float* __restrict__ dh,
                              const double* __restrict__ rho, float* __restrict__ vmt) {
   PK(j, kd, nv);
-  const int iv = vprog[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VPTAB(j);
+  if (kd < LPV(iv)) return;
   const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
   const int im1 = g.v_im[iv * 2], im2 = g.v_im[iv * 2 + 1];
   const float rr = (float)(rho[(size_t)iw1 * g.mza + kd] + rho[(size_t)iw2 * g.mza + kd]);
@@ -246,7 +259,7 @@ __global__ void k_vort_apply(DynK g, const int* __restrict__ vprog, int nv, int 
     vmt[x] = vmt[x] + fvorth[iv] * (dh[(size_t)im2 * g.mza + kd] - dh[(size_t)im1 * g.mza + kd]) * rr;
     return;
   }
-  const int ka = (level == 3) ? max(g.lpm[im1], g.lpm[im2]) : g.lpv[iv];
+  const int ka = (level == 3) ? max(g.lpm[im1], g.lpm[im2]) : LPV(iv);
   if (kd < ka)
     vmt[x] = vmt[x] + fvortl[iv] * (dl[(size_t)im2 * g.mza + kd] - dl[(size_t)im1 * g.mza + kd]) * rr;
   else
@@ -258,8 +271,8 @@ __global__ void k_vmca(DynK g, const int* __restrict__ vadj, int nv, const float
                        const float* __restrict__ arv, float* __restrict__ vmca, float* __restrict__ vmasc,
                        int last) {
   PK(j, kd, nv);
-  const int iv = vadj[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VATAB(j);
+  if (kd < LPV(iv)) return;
   const size_t x = (size_t)iv * g.mza + kd;
   const float v = vmc[x] * arv[x];
   vmca[x] = v;
@@ -279,7 +292,7 @@ __global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s,
                         const float* __restrict__ xy_hu, float* __restrict__ gx) {
   PK(j, kd, nprog);
   constexpr int NPL = ORD == 2 ? 2 : 5;
-  const int iw = prog[j];
+  const int iw = WTAB(j);
   const unsigned mza = g.mza;
   const size_t plane = (size_t)g.mwa * mza;
   const unsigned x = (unsigned)iw * mza + kd;
@@ -295,7 +308,7 @@ __global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s,
   for (int n = 0; n < 7; ++n) {
     if (n >= np) break;
     const int iv = g.w_ev[iw * 8 + n], iwn = g.w_nb[iw * 8 + n];
-    if (kd < g.lpv[iv]) continue;
+    if (kd < LPV(iv)) continue;
     float w[NPL];
     if (ORD == 2) {
       w[0] = cx[iw * 7 + n];
@@ -327,8 +340,8 @@ __global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s,
 __global__ void k_upw4(DynK g, const int* __restrict__ prog, int nprog, Four s, const float* __restrict__ wmc,
                        float* __restrict__ upw) {
   PK(j, kd, nprog);
-  const int iw = prog[j];
-  const int kb = g.lpw[iw];
+  const int iw = WTAB(j);
+  const int kb = LPW(iw);
   const int mza = g.mza;
   if (kd < kb - 1) return;
   const size_t plane = (size_t)g.mwa * mza;
@@ -362,8 +375,8 @@ __global__ void k_upv4(DynK g, const int* __restrict__ vadj, int nv, Four s, uns
                        const float* __restrict__ gx, VSide c, const float* __restrict__ vmc,
                        float* __restrict__ upv) {
   PK(j, kd, nv);
-  const int iv = vadj[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VATAB(j);
+  if (kd < LPV(iv)) return;
   const unsigned mza = g.mza;
   const size_t plane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
   const unsigned xv = (unsigned)iv * mza + kd;
@@ -433,7 +446,7 @@ __global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs 
   m.b32 = fb + 5 * mza; m.b33 = fb + 6 * mza; m.dwm = fb + 7 * mza; m.wmf = fb + 8 * mza;
 
   const int iw = A.prog[j];
-  const int kb = g.lpw[iw];
+  const int kb = LPW(iw);
   const int np = g.npoly[iw];
   const size_t cb = (size_t)iw * mza;
   const size_t wplane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
@@ -460,7 +473,7 @@ __global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs 
     for (int n = 0; n < 7; ++n) {
       if (ev[n] == -1) break;
       const int iv = ev[n] & 0x7fffffff;
-      if (kd < g.lpv[iv]) continue;
+      if (kd < LPV(iv)) continue;
       const size_t xv = (size_t)iv * mza + kd;
       const float vm = A.vmc[xv] * A.arv[xv];
       const float u0 = A.upv[xv], u1 = A.upv[vplane + xv], u2 = A.upv[2 * vplane + xv],
@@ -581,8 +594,8 @@ __global__ void k_prog_v(DynK g, const int* __restrict__ vprog, int nv, float dt
                          const float* __restrict__ rkz, const float* __restrict__ volvi,
                          const double* __restrict__ rho, float* __restrict__ vmc, float* __restrict__ vc) {
   PK(j, kd, nv);
-  const int iv = vprog[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VPTAB(j);
+  if (kd < LPV(iv)) return;
   const int mza = g.mza;
   const int iw1 = g.v_iw[iv * 2], iw2 = g.v_iw[iv * 2 + 1];
   const size_t x = (size_t)iv * mza + kd, x1 = (size_t)iw1 * mza + kd, x2 = (size_t)iw2 * mza + kd;
@@ -600,8 +613,8 @@ __global__ void k_vel_t3d(DynK g, const int* __restrict__ prog, int nprog, const
                           const float* __restrict__ ecv, float* __restrict__ vxe, float* __restrict__ vye,
                           float* __restrict__ vze) {
   PK(j, kd, nprog);
-  const int iw = prog[j];
-  const int kb = g.lpw[iw];
+  const int iw = WTAB(j);
+  const int kb = LPW(iw);
   if (kd < kb) return;
   const int mza = g.mza;
   const size_t cb = (size_t)iw * mza;
@@ -612,7 +625,7 @@ __global__ void k_vel_t3d(DynK g, const int* __restrict__ prog, int nprog, const
   for (int n = 0; n < 7; ++n) {
     if (n >= np) break;
     const int iv = g.w_ev[iw * 8 + n];
-    if (kd < g.lpv[iv]) continue;
+    if (kd < LPV(iv)) continue;
     const float v = vc[(size_t)iv * mza + kd];
     x = x + ecv[(iw * 7 + n) * 3] * v;
     y = y + ecv[(iw * 7 + n) * 3 + 1] * v;
@@ -629,7 +642,7 @@ __global__ void k_tend0_w(DynK g, float* thilt, float* vmxet, float* vmyet, floa
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (size_t)(g.mwa - 1) * g.mza) return;
   const int iw = 1 + (int)(i / g.mza), kd = (int)(i % g.mza);
-  if (kd < g.lpw[iw]) return;
+  if (kd < LPW(iw)) return;
   const size_t x = (size_t)iw * g.mza + kd;
   thilt[x] = 0.f; vmxet[x] = 0.f; vmyet[x] = 0.f; vmzet[x] = 0.f;
   rho_old[x] = (float)rho[x];
@@ -640,7 +653,7 @@ __global__ void k_tend0_v(DynK g, float* vmt, float* vmasc) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (size_t)(g.mva - 1) * g.mza) return;
   const int iv = 1 + (int)(i / g.mza), kd = (int)(i % g.mza);
-  if (kd < g.lpv[iv]) return;
+  if (kd < LPV(iv)) return;
   const size_t x = (size_t)iv * g.mza + kd;
   vmt[x] = 0.f;
   vmasc[x] = 0.f;
@@ -649,15 +662,15 @@ __global__ void k_tend0_v(DynK g, float* vmt, float* vmasc) {
 // timeavg_momsc (timestep.f90:563-612)
 __global__ void k_timeavg_v(DynK g, const int* __restrict__ vadj, int nv, float a, float* vmasc) {
   PK(j, kd, nv);
-  const int iv = vadj[j];
-  if (kd < g.lpv[iv]) return;
+  const int iv = VATAB(j);
+  if (kd < LPV(iv)) return;
   vmasc[(size_t)iv * g.mza + kd] = vmasc[(size_t)iv * g.mza + kd] / a;
 }
 
 __global__ void k_timeavg_w(DynK g, const int* __restrict__ prog, int nprog, float a, float* wmasc) {
   PK(j, kd, nprog);
-  const int iw = prog[j];
-  if (kd < g.lpw[iw] || kd > g.mza - 2) return;
+  const int iw = WTAB(j);
+  if (kd < LPW(iw) || kd > g.mza - 2) return;
   wmasc[(size_t)iw * g.mza + kd] = wmasc[(size_t)iw * g.mza + kd] / a;
 }
 

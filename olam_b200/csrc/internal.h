@@ -115,6 +115,7 @@ struct DevGrid {
   int mza = 0, mwa = 0, mva = 0, mma = 0;
   int nw_prog = 0, nv_wadj = 0, nv_prog = 0, nw_wadj = 0, nm_prog = 0;
   DevBuf<int> jtw_prog, jtv_wadj, jtv_prog, jtw_wadj, jtm_prog;  // 0-based
+  int off_wprog = -1, off_vwadj = -1, off_vprog = -1;   // contiguous tables: first entry (0-based), else -1
   DevBuf<int> npoly;     // (mwa)
   DevBuf<int> w_nb;      // (mwa, 8) 0-based W neighbours, padded with self
   DevBuf<int> w_ev;      // (mwa, 8) 0-based V neighbours, padded with 0

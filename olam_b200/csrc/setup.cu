@@ -58,6 +58,15 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
   OG_CHECK(upload_list(d.jtw_wadj, g->jtw_wadj, g->nw_wadj, mwa, "jtw_wadj", s));
   OG_CHECK(upload_list(d.jtv_prog, g->jtv_prog, g->nv_prog, mva, "jtv_prog", s));
   OG_CHECK(upload_list(d.jtv_wadj, g->jtv_wadj, g->nv_wadj, mva, "jtv_wadj", s));
+  // a table that is a contiguous ascending run needs no reads on the device
+  auto run_start = [](const int* t, int n) -> int {
+    if (n <= 0 || !t) return -1;
+    for (int j = 1; j < n; ++j) if (t[j] != t[0] + j) return -1;
+    return t[0] - 1;
+  };
+  d.off_wprog = run_start(g->jtw_prog, g->nw_prog);
+  d.off_vwadj = run_start(g->jtv_wadj, g->nv_wadj);
+  d.off_vprog = run_start(g->jtv_prog, g->nv_prog);
   if (g->jtm_prog && g->nm_prog > 0)
     OG_CHECK(upload_list(d.jtm_prog, g->jtm_prog, g->nm_prog, mma, "jtm_prog", s));
 
