@@ -98,7 +98,9 @@ def _case():
 def _rank_main(rank, world, port, q):
     try:
         import torch.distributed as dist
-        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+        from datetime import timedelta
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                                timeout=timedelta(seconds=120))
         g, st, tr, sct = _case()
         ref = numpy_ref.transport_plain(g, st, tr, sct, 600.0, nrk=2)
         loc = decomp.local_grid(g, decomp.bisect(g, world), rank)

@@ -5,7 +5,8 @@ the exchange hook hands it, after every RK stage but the last, the border
 values its neighbour computes (taken from the single-domain stages of the
 numpy restatement).  Together the ranks' owned columns reproduce the
 single-domain GPU step; the columns each rank sends are its own stage
-values."""
+values.  The last test runs the two ranks as two processes on the one GPU,
+the hook moving the border columns over gloo."""
 import numpy as np
 import pytest
 
@@ -103,3 +104,86 @@ def test_halo_needs_the_unlimited_batched_step():
     opts = abi.make_opts(1800.0)
     with pytest.raises(OlamGpuError):
         _rank(g, st, opts, loc, _stages(g, st, 1800.0, 2), abi.TRANSPORT_PLAIN, 2)
+
+
+def _proc_main(rank, world, port, q):
+    """One rank of a decomposed tracer step as its own process: its part of
+    the grid through the library, the exchange hook moving the packed border
+    columns over gloo (host-staged)."""
+    try:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                                timeout=timedelta(seconds=120))
+        g, st = small_case(nxp=8, nlev=12, ntr=6)
+        opts = abi.make_opts(1800.0, nrk_scal=3)
+        loc = decomp.local_grid(g, decomp.bisect(g, world), rank)
+        calls = {"n": 0}
+
+        def hook(ranks, sbuf, rbuf):
+            calls["n"] += 1
+            ops, got = [], []
+            for r, sv, rv in zip(ranks, sbuf, rbuf):
+                if sv.size:
+                    ops.append(dist.P2POp(dist.isend, torch.from_numpy(sv.copy()), r))
+                if rv.size:
+                    t = torch.empty(rv.size, dtype=torch.float32)
+                    got.append((rv, t))
+                    ops.append(dist.P2POp(dist.irecv, t, r))
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+            for rv, t in got:
+                rv[:] = t.numpy()
+            return 0
+
+        fg = abi.FortranGrid(loc.grid)
+        hs = HostState(vmasc=loc.v(st.vmasc), wmasc=loc.w(st.wmasc), rho=loc.w(st.rho), wc=loc.w(st.wc))
+        dev = OlamGpu(fg, opts, hs)
+        try:
+            var_p = [loc.w(t).copy() for t in st.tracers]
+            var_t = [loc.w(t).copy() for t in st.sct]
+            dev.register_scalars(var_p, var_t)
+            dev.set_halo(abi.make_halo(loc.send, loc.recv, hook))
+            dev.scalar_transport_rk(loc.w(st.rho_old))
+        finally:
+            dev.close()
+        own = loc.owned
+        q.put((rank, loc.wmap[own], np.stack([p[own] for p in var_p]), calls["n"]))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:   # report to the parent instead of hanging it
+        q.put((rank, repr(e), None, None))
+
+
+def test_two_processes_over_gloo():
+    # two ranks as two processes sharing the GPU: no kernel waits on the
+    # other rank (each hook call follows a finished stage on the host), the
+    # border columns move over gloo; together the ranks reproduce the
+    # one-domain step
+    import socket
+    import torch.multiprocessing as mp
+    g, st = small_case(nxp=8, nlev=12, ntr=6)
+    opts = abi.make_opts(1800.0, nrk_scal=3)
+    ref, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_proc_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=600) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    covered = np.zeros(g.mwa, bool)
+    for rank, cols, vals, n in res:
+        assert not isinstance(cols, str), cols
+        assert n == 2                                  # RK3: after stages 1 and 2
+        for t in range(len(st.tracers)):
+            e = relerr(vals[t], ref[t][cols])
+            assert e < 1e-5, (rank, t, e)
+        covered[cols] = True
+    assert covered[1:].all()
