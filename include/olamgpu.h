@@ -344,9 +344,10 @@ int olamgpu_mass_sums(int nsel, const int* ids, double* sums);
  * as it is, and the first call for each of the three tracer-buffer
  * rotations after it records the sequence as a CUDA graph; later calls
  * replay the graph (no host work per kernel, no host round-trip).
- * Registering scalars, eddy inputs or turbulence, or changing the
+ * Registering scalars, eddy inputs, turbulence or a halo, or changing the
  * coherence or transport form, drops the recorded graphs.  The plain
- * transport form always runs without a graph.  The diagnostics of the last
+ * transport form, and a rank with a halo exchange (its hook runs on the
+ * host between stages), always run without a graph.  The diagnostics of the last
  * call are read with olamgpu_timestep_diag. */
 enum {
   OLAMGPU_TS_GRAPH = 1u << 0,     /* record / replay the step as a CUDA graph      */

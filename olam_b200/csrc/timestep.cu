@@ -327,7 +327,8 @@ int glue_timestep(unsigned flags, int nmass, const int* ids) {
   G.last_flags = flags;
   G.last_nmass = nmass;
   G.last_ntr = C.tr.n;
-  const bool graph = (flags & OLAMGPU_TS_GRAPH) && C.form != OLAMGPU_TRANSPORT_PLAIN && C.tr.n > 0;
+  // a halo exchange calls back into the host between stages: no graph
+  const bool graph = (flags & OLAMGPU_TS_GRAPH) && C.form != OLAMGPU_TRANSPORT_PLAIN && C.tr.n > 0 && !C.halo.on;
   if (!graph) return run_sequence(C, flags, nmass, ids);
   // the graph reads the tracers from Q[qcur]; a sync to the device may have
   // refreshed the per-tracer arrays instead
