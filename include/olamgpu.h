@@ -307,9 +307,21 @@ typedef struct olamgpu_halo {
   int (*exchange)(void* user, int nnb, const int* rank, float* const* sendbuf, const size_t* sendcount,
                   float* const* recvbuf, const size_t* recvcount, void* stream);
   void* user;
+  /* the acoustic step's V- and M-point plans, (nnb) counts and concatenated
+   * 1-based indices as for the columns; NULL counts: no V / M points move
+   * (then prog_wrtv_rk on this rank returns OLAMGPU_E_UNSUPPORTED) */
+  const int* nsend_v; const int* send_v; const int* nrecv_v; const int* recv_v;
+  const int* nsend_m; const int* send_m; const int* nrecv_m; const int* recv_m;
 } olamgpu_halo;
 
-/* Registers the halo plan (NULL: one domain, no exchange). */
+/* Registers the halo plan (NULL: one domain, no exchange).  With the V and
+ * M plans, prog_wrtv_rk exchanges as omodel/prog_wrtv_rk.f90:418-472 does
+ * after prog_wrt_begs (press, rho, vm*et_rk), prog_v_begs (vmc, vc) and
+ * vel_t3d (vxe, vye, vze, wmc, wc, thil), and the damping exchanges its
+ * divergence and vorticity planes (omodel/vort_div_damp.f90:150, 208 and
+ * the M-point ones); the gradients of ring-1 columns are computed locally
+ * instead of exchanged.  olamgpu_timestep also exchanges the tracers and
+ * thil after set_scalars_bottom (omodel/timestep.f90:310-314). */
 int olamgpu_set_halo(const olamgpu_halo* halo);
 
 /* ---- long-step glue on the device ------------------------------------------

@@ -99,14 +99,17 @@ class Halo(C.Structure):
     """olamgpu_halo: the halo plan of a rank and its exchange hook."""
     _fields_ = [("nnb", C.c_int), ("rank", c_int_p), ("nsend", c_int_p), ("send_cols", c_int_p),
                 ("nrecv", c_int_p), ("recv_cols", c_int_p), ("host_staged", C.c_int),
-                ("exchange", HALO_FN), ("user", C.c_void_p)]
+                ("exchange", HALO_FN), ("user", C.c_void_p),
+                ("nsend_v", c_int_p), ("send_v", c_int_p), ("nrecv_v", c_int_p), ("recv_v", c_int_p),
+                ("nsend_m", c_int_p), ("send_m", c_int_p), ("nrecv_m", c_int_p), ("recv_m", c_int_p)]
 
 
-def make_halo(send, recv, fn, host_staged=True):
+def make_halo(send, recv, fn, host_staged=True, vm=None):
     """A Halo over a plan {rank: local 0-based column indices} (olam_b200.decomp)
     and a Python hook fn(ranks, sendbufs, recvbufs) -> int on numpy views of
-    the buffers (host-staged).  The returned struct keeps its arrays."""
-    ranks = sorted(set(send) | set(recv))
+    the buffers (host-staged).  vm: (send_v, recv_v, send_m, recv_m) plans of
+    the acoustic step, or None.  The returned struct keeps its arrays."""
+    ranks = sorted(set(send) | set(recv) | (set().union(*[set(d) for d in vm]) if vm else set()))
     rk = np.array(ranks, np.int32)
     ns = np.array([len(send.get(r, ())) for r in ranks], np.int32)
     nr = np.array([len(recv.get(r, ())) for r in ranks], np.int32)
@@ -130,7 +133,17 @@ def make_halo(send, recv, fn, host_staged=True):
     h.host_staged = 1 if host_staged else 0
     h.exchange = HALO_FN(hook)
     h.user = None
-    h.keep = (rk, ns, nr, sc, rc, h.exchange)
+    keep = [rk, ns, nr, sc, rc, h.exchange]
+    if vm:
+        names = (("nsend_v", "send_v"), ("nrecv_v", "recv_v"), ("nsend_m", "send_m"), ("nrecv_m", "recv_m"))
+        for plan, (cname, lname) in zip(vm, names):
+            cnt = np.array([len(plan.get(r, ())) for r in ranks], np.int32)
+            idx = np.ascontiguousarray(np.concatenate([np.asarray(plan.get(r, []), np.int64) for r in ranks]
+                                                      + [np.zeros(0, np.int64)]) + 1, np.int32)
+            setattr(h, cname, ptr(cnt, C.c_int))
+            setattr(h, lname, ptr(idx, C.c_int))
+            keep += [cnt, idx]
+    h.keep = tuple(keep)
     return h
 
 

@@ -867,11 +867,11 @@ int dyn_state_to_host(unsigned mask, cudaStream_t s) {
                       OLAMGPU_F_VXE | OLAMGPU_F_VMC | OLAMGPU_F_VC | OLAMGPU_F_VMASC | OLAMGPU_F_WMASC | \
                       OLAMGPU_F_TEND)
 
-static void divh_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
+static int divh_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
   const olamgpu_opts& o = C.opts;
   const DevGrid& d = C.g;
   Dyn& y = C.dy;
-  if (!(o.divh_damp_fact > 1.e-7f) || o.divh_damp_level <= 0) return;
+  if (!(o.divh_damp_fact > 1.e-7f) || o.divh_damp_level <= 0) return OLAMGPU_OK;
   const int level = o.divh_damp_level;
   const DynK g = dynk(d);
   const size_t wz = (size_t)d.mza * d.mwa;
@@ -890,6 +890,8 @@ static void divh_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
   float* d1 = y.div2d.p;
   k_div_accum<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.arv.p, y.vmc.p, d1);
   OG_LAUNCHED();
+  // border divergence for the Laplacian and the apply (vort_div_damp.f90:150)
+  { HField f[1] = {{d1, 4}}; OG_CHECK(halo_exchange_fields(C, HALO_W, f, 1, s)); }
   const float* dh = d1;
   if (level > 1) {
     int ih = 2;
@@ -899,18 +901,20 @@ static void divh_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
       k_lap_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.xx_yy.p, y.div2d.p + (il - 1) * wz,
                                   y.div2d.p + (ih - 1) * wz);
       OG_LAUNCHED();
+      { HField f[1] = {{y.div2d.p + (ih - 1) * wz, 4}}; OG_CHECK(halo_exchange_fields(C, HALO_W, f, 1, s)); }
     }
     dh = y.div2d.p + (ih - 1) * wz;
   }
   k_div_apply<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, y.fdivh.p, dh, vmt);
   OG_LAUNCHED();
+  return OLAMGPU_OK;
 }
 
-static void vort_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
+static int vort_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
   const olamgpu_opts& o = C.opts;
   const DevGrid& d = C.g;
   Dyn& y = C.dy;
-  if (o.vort_damp_fact < 1.e-7f || o.vort_damp_level <= 0) return;
+  if (o.vort_damp_fact < 1.e-7f || o.vort_damp_level <= 0) return OLAMGPU_OK;
   const int level = o.vort_damp_level;
   const DynK g = dynk(d);
   const size_t mz = (size_t)d.mza * d.mma;
@@ -925,6 +929,7 @@ static void vort_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
   const unsigned nbm = cdiv((size_t)d.nm_prog * d.mza, 256), nbv = cdiv((size_t)d.nv_prog * d.mza, 256);
   k_vort<<<nbm, 256, 0, s>>>(g, d.jtm_prog.p, d.nm_prog, y.vfact.p, y.vc.p, y.vort2d.p);
   OG_LAUNCHED();
+  { HField f[1] = {{y.vort2d.p, 4}}; OG_CHECK(halo_exchange_fields(C, HALO_M, f, 1, s)); }
   int il = 1, ih = 1;
   if (level > 1) {
     for (int nn = 1; nn <= level - 1; ++nn) {
@@ -933,11 +938,13 @@ static void vort_damp(Context& C, float* vmt, double dtm, cudaStream_t s) {
       k_lap_m<<<nbm, 256, 0, s>>>(g, d.jtm_prog.p, d.nm_prog, y.xx_yy_m.p, y.vort2d.p + (il - 1) * mz,
                                   y.vort2d.p + (ih - 1) * mz);
       OG_LAUNCHED();
+      { HField f[1] = {{y.vort2d.p + (ih - 1) * mz, 4}}; OG_CHECK(halo_exchange_fields(C, HALO_M, f, 1, s)); }
     }
   }
   k_vort_apply<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, level, y.fvorth.p, y.fvortl.p,
                                    y.vort2d.p + (il - 1) * mz, y.vort2d.p + (ih - 1) * mz, C.tp.rho.p, vmt);
   OG_LAUNCHED();
+  return OLAMGPU_OK;
 }
 
 int dyn_prog_wrtv_rk(int istp) {
@@ -947,6 +954,10 @@ int dyn_prog_wrtv_rk(int istp) {
   if (!C.have_state) { set_error("prog_wrtv_rk needs the state arrays registered at init"); return OLAMGPU_E_STATE; }
   const olamgpu_opts& o = C.opts;
   if (o.nrk_wrtv != 2 && o.nrk_wrtv != 3) { set_error("acoust_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  if (C.halo.on && (!C.halo.dyn || o.ithil_monot > 0 || o.iwind_monot > 0)) {
+    set_error("prog_wrtv_rk on a rank with a halo needs the V and M plans and no flux-corrected faces");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
   cudaStream_t s = C.stream;
   OG_CHECK(ensure_dyn_buffers(C));
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL || !C.dy.uploaded) {
@@ -962,8 +973,8 @@ int dyn_prog_wrtv_rk(int istp) {
   const unsigned nbw = cdiv((size_t)d.nw_prog * mza, 256), nbv = cdiv((size_t)d.nv_prog * mza, 256),
                  nbva = cdiv((size_t)d.nv_wadj * mza, 256);
   OG_PROF("prog_wrtv_rk", s);
-  if (!o.divh_damp_short && istp == 1) { OG_PROF("divh_damp", s); divh_damp(C, y.vmt.p, o.dtlm, s); }
-  if (!o.vort_damp_short && istp == 1) { OG_PROF("vort_damp", s); vort_damp(C, y.vmt.p, o.dtlm, s); }
+  if (!o.divh_damp_short && istp == 1) { OG_PROF("divh_damp", s); OG_CHECK(divh_damp(C, y.vmt.p, o.dtlm, s)); }
+  if (!o.vort_damp_short && istp == 1) { OG_PROF("vort_damp", s); OG_CHECK(vort_damp(C, y.vmt.p, o.dtlm, s)); }
   SetupW sw{tp.rho.p, y.thil.p, y.wmc.p, y.thilt.p, y.vmxet.p, y.vmyet.p, y.vmzet.p, y.volt.p, y.rho0.p,
             y.rth0.p, y.wmc0.p, y.sh_th.p, y.sh_vx.p, y.sh_vy.p, y.sh_vz.p, y.rayf_cof.p, y.dn01d.p, y.th01d.p,
             o.krayf_bot};
@@ -982,8 +993,8 @@ int dyn_prog_wrtv_rk(int istp) {
     OG_PROF("eddy_columns", s);
     OG_CHECK(dyn_eddy_columns(C, rayleigh_th, s));
   }
-  if (o.divh_damp_short) { OG_PROF("divh_damp", s); divh_damp(C, y.sh_vmt.p, o.dtsm, s); }
-  if (o.vort_damp_short) { OG_PROF("vort_damp", s); vort_damp(C, y.sh_vmt.p, o.dtsm, s); }
+  if (o.divh_damp_short) { OG_PROF("divh_damp", s); OG_CHECK(divh_damp(C, y.sh_vmt.p, o.dtsm, s)); }
+  if (o.vort_damp_short) { OG_PROF("vort_damp", s); OG_CHECK(vort_damp(C, y.sh_vmt.p, o.dtsm, s)); }
   // start values of the fields fluxes_wrtv_monot limits (prog_wrtv_rk.f90:186-198)
   const bool thil_monot = o.ithil_monot > 0, wind_monot = o.iwind_monot > 0;
   const size_t wzb = (size_t)mza * d.mwa * sizeof(float);
@@ -1024,8 +1035,20 @@ int dyn_prog_wrtv_rk(int istp) {
     for (int q = 0; q < 4; ++q) { if (ordf[q] == 2) m2 |= 1u << q; if (ordf[q] >= 3) m3 |= 1u << q; }
     {
       OG_PROF("grad4", s);
-      if (m2) { k_grad4<2><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m2, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
-      if (m3) { k_grad4<3><<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, m3, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
+      // on a rank with a halo the gradients of ring 1 are computed here (the
+      // reference exchanges them): over jtw_wadj, the owned columns and ring 1
+      DynK gg = g;
+      const int* gt = d.jtw_prog.p;
+      int gn = d.nw_prog;
+      unsigned nbg = nbw;
+      if (C.halo.on) {
+        gg.off_w = d.off_wwadj;
+        gt = d.jtw_wadj.p;
+        gn = d.nw_wadj;
+        nbg = cdiv((size_t)gn * mza, 256);
+      }
+      if (m2) { k_grad4<2><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m2, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
+      if (m3) { k_grad4<3><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m3, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
     }
     { OG_PROF("upw4", s); k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p); OG_LAUNCHED(); }
     {
@@ -1066,17 +1089,33 @@ int dyn_prog_wrtv_rk(int istp) {
     A.zwgt_bot8 = y.zwgt_bot8.p; A.zwgt_top8 = y.zwgt_top8.p; A.b20 = y.b20.p;
     const size_t smem = (size_t)WRT_WARPS * mza * 13 * sizeof(double);
     { OG_PROF("wrt_begs", s); k_wrt_begs<<<cdiv(d.nw_prog, WRT_WARPS), WRT_WARPS * 32, smem, s>>>(g, A); OG_LAUNCHED(); }
+    if (C.halo.on) {
+      // prog_wrtv_rk.f90:418-429: what prog_v_begs reads at border V points
+      OG_PROF("halo_exchange", s);
+      HField f5[5] = {{y.press.p, 8}, {tp.rho.p, 8}, {y.rk_vx.p, 4}, {y.rk_vy.p, 4}, {y.rk_vz.p, 4}};
+      OG_CHECK(halo_exchange_fields(C, HALO_W, f5, 5, s));
+    }
     {
       OG_PROF("prog_v", s);
       k_prog_v<<<nbv, 256, 0, s>>>(g, d.jtv_prog.p, d.nv_prog, dts, y.vmc0.p, y.sh_vmt.p, y.press.p, y.pvfac.p,
                                    y.vn.p, y.rk_vx.p, y.rk_vy.p, y.rk_vz.p, y.volvi.p, tp.rho.p, y.vmc.p, y.vc.p);
       OG_LAUNCHED();
     }
+    if (C.halo.on) {   // prog_wrtv_rk.f90:442-447
+      OG_PROF("halo_exchange", s);
+      HField f2[2] = {{y.vmc.p, 4}, {y.vc.p, 4}};
+      OG_CHECK(halo_exchange_fields(C, HALO_V, f2, 2, s));
+    }
     {
       OG_PROF("vel_t3d", s);
       k_vel_t3d<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, tp.wc.p, y.vc.p, y.wno2.p, y.ecv.p, y.vxe.p,
                                     y.vye.p, y.vze.p);
       OG_LAUNCHED();
+    }
+    if (C.halo.on) {   // prog_wrtv_rk.f90:464-472
+      OG_PROF("halo_exchange", s);
+      HField f6[6] = {{y.vxe.p, 4}, {y.vye.p, 4}, {y.vze.p, 4}, {y.wmc.p, 4}, {tp.wc.p, 4}, {y.thil.p, 4}};
+      OG_CHECK(halo_exchange_fields(C, HALO_W, f6, 6, s));
     }
   }
   (void)wz;

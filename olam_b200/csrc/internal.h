@@ -115,7 +115,7 @@ struct DevGrid {
   int mza = 0, mwa = 0, mva = 0, mma = 0;
   int nw_prog = 0, nv_wadj = 0, nv_prog = 0, nw_wadj = 0, nm_prog = 0;
   DevBuf<int> jtw_prog, jtv_wadj, jtv_prog, jtw_wadj, jtm_prog;  // 0-based
-  int off_wprog = -1, off_vwadj = -1, off_vprog = -1;   // contiguous tables: first entry (0-based), else -1
+  int off_wprog = -1, off_vwadj = -1, off_vprog = -1, off_wwadj = -1;   // contiguous tables: first entry (0-based), else -1
   DevBuf<int> npoly;     // (mwa)
   DevBuf<int> w_nb;      // (mwa, 8) 0-based W neighbours, padded with self
   DevBuf<int> w_ev;      // (mwa, 8) 0-based V neighbours, padded with 0
@@ -294,11 +294,20 @@ struct Glue {
 };
 
 // halo exchange of the tracer step (halo.cu)
+// a point kind's exchange lists (W columns, V or M points)
+struct HaloList {
+  std::vector<int> nsend, nrecv;     // per neighbour
+  size_t ns = 0, nr = 0;
+  DevBuf<int> send, recv;            // 0-based indices, neighbour after neighbour
+};
+
 struct Halo {
-  bool on = false, host_staged = false;
+  bool on = false, host_staged = false, dyn = false;
   std::vector<int> rank, nsend, nrecv;
   size_t ns = 0, nr = 0;             // columns sent / received in all
   DevBuf<int> send_cols, recv_cols;  // 0-based W indices, neighbour after neighbour
+  HaloList lv, lm;                   // V and M points (the acoustic step)
+  DevBuf<int> wsend, wrecv;          // copies of the column lists for field exchanges
   DevBuf<float> sendbuf, recvbuf;    // packed columns (all levels and tracers)
   float* hsend = nullptr;            // pinned host copies (host-staged hook)
   float* hrecv = nullptr;
@@ -373,6 +382,10 @@ void transport_release_pipeline();
 // halo exchange (halo.cu)
 int halo_set(const olamgpu_halo* h);
 int halo_exchange(Context& C, float* Q, int ntp, cudaStream_t s);
+// fields of mza elements per point (4 or 8 bytes each) of one point kind
+enum { HALO_W = 0, HALO_V = 1, HALO_M = 2 };
+struct HField { void* p; int esize; };
+int halo_exchange_fields(Context& C, int kind, const HField* f, int nf, cudaStream_t s);
 void halo_release();
 // long-step glue and the recorded step (timestep.cu)
 int glue_set_scalars_bottom();

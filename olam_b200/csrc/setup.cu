@@ -67,6 +67,7 @@ int upload_grid(const olamgpu_grid* g, DevGrid& d, cudaStream_t s) {
   d.off_wprog = run_start(g->jtw_prog, g->nw_prog);
   d.off_vwadj = run_start(g->jtv_wadj, g->nv_wadj);
   d.off_vprog = run_start(g->jtv_prog, g->nv_prog);
+  d.off_wwadj = run_start(g->jtw_wadj, g->nw_wadj);
   if (g->jtm_prog && g->nm_prog > 0)
     OG_CHECK(upload_list(d.jtm_prog, g->jtm_prog, g->nm_prog, mma, "jtm_prog", s));
 

@@ -297,6 +297,13 @@ static int run_sequence(Context& C, unsigned flags, int nmass, const int* ids) {
   OG_CHECK(transport_run(nullptr, nullptr));
   if (flags & OLAMGPU_TS_MAXMIN) OG_CHECK(launch_maxmin(C, s));
   launch_bottom_fill(C, s);
+  if (C.halo.on) {
+    // the border columns of the tracers and thil for the next step
+    // (timestep.f90:310-314)
+    if (C.tr.n > 0 && C.tr.q_valid) OG_CHECK(halo_exchange(C, C.tr.q[C.tr.qcur].p, C.tr.ntp, s));
+    HField f[1] = {{C.dy.thil.p, 4}};
+    OG_CHECK(halo_exchange_fields(C, HALO_W, f, 1, s));
+  }
   if (flags & OLAMGPU_TS_MASS) OG_CHECK(launch_mass(C, nmass, ids, s));
   OG_CUDA(cudaGetLastError());
   return OLAMGPU_OK;

@@ -88,6 +88,8 @@ class Local:
         self.grid, self.wmap, self.vmap, self.mmap = grid, wmap, vmap, mmap
         self.nown = nown
         self.send, self.recv = send, recv
+        # V- and M-point plans of the acoustic step (filled by local_grid)
+        self.send_v, self.recv_v, self.send_m, self.recv_m = {}, {}, {}, {}
 
     def w(self, a):
         """A global W-point array restricted to this rank's points."""
@@ -174,7 +176,63 @@ def local_grid(g, owner, rank):
         theirs = theirs[owner[theirs] == rank]
         if theirs.size:
             send[r] = winv[np.sort(theirs)]
-    return Local(lg, wmap, vmap, mmap, owned.size, send, recv)
+    loc = Local(lg, wmap, vmap, mmap, owned.size, send, recv)
+    # V and M points: owned by the rank of a W point (para_decomp.F90: a V
+    # point by its W neighbour iw(mod(iv,2)+1), here an M point by its first
+    # W corner); the rank that owns one holds it (an edge, or a corner set,
+    # of its own columns), so every point held but not owned is received
+    # from its owner, in global order on both sides
+    vown, mown_all = v_owner(g, owner), m_owner(g, owner)
+    for r in range(nranks):
+        if r == rank:
+            continue
+        mine_v = vmap[1:][vown[vmap[1:]] == r]
+        if mine_v.size:
+            loc.recv_v[r] = vinv[np.sort(mine_v)]
+        mine_m = mmap[1:][mown_all[mmap[1:]] == r]
+        if mine_m.size:
+            loc.recv_m[r] = minv[np.sort(mine_m)]
+        ov, om = _held_vm(g, owner, r)
+        theirs_v = ov[vown[ov] == rank]
+        if theirs_v.size:
+            loc.send_v[r] = vinv[np.sort(theirs_v)]
+        theirs_m = om[mown_all[om] == rank]
+        if theirs_m.size:
+            loc.send_m[r] = minv[np.sort(theirs_m)]
+    return loc
+
+
+def v_owner(g, owner):
+    """Rank owning each V point (the rank of its W neighbour iw(mod(iv,2)+1),
+    iv the 1-based index); -1 for the dummy point."""
+    vg = np.arange(g.mva)
+    side = (vg + 1) % 2
+    o = owner[g.itab_v_iw[vg, side]].astype(np.int32)
+    o[0] = -1
+    return o
+
+
+def m_owner(g, owner):
+    """Rank owning each M point (the rank of its first W corner)."""
+    o = owner[g.itab_m_iw[:, 0]].astype(np.int32)
+    o[0] = -1
+    return o
+
+
+def _held_vm(g, owner, r):
+    """The V and M points (global indices) that rank r holds."""
+    owned = np.nonzero(owner == r)[0].astype(np.int64)
+    r1, r2 = _rings(g, owned)
+    core = np.concatenate([owned, r1])
+    ev = g.itab_w_iv[core]
+    valid = np.arange(ev.shape[1])[None, :] < g.npoly[core][:, None]
+    vset = np.unique(ev[valid])
+    held = np.zeros(g.mwa, bool)
+    held[np.concatenate([owned, r1, r2])] = True
+    cand = np.unique(g.itab_w_im[np.concatenate([owned, r1, r2])])
+    cand = cand[cand > 0]
+    mset = cand[np.all(held[g.itab_m_iw[cand]], axis=1)]
+    return vset, mset
 
 
 def exchange(a, loc, dist):

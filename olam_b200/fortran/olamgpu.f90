@@ -77,6 +77,7 @@ module olamgpu_c
      integer(c_int) :: host_staged
      type(c_funptr) :: exchange     ! int f(user, nnb, rank, sendbuf, sendcount, recvbuf, recvcount, stream)
      type(c_ptr)    :: user
+     type(c_ptr)    :: nsend_v, send_v, nrecv_v, recv_v, nsend_m, send_m, nrecv_m, recv_m
   end type olamgpu_halo
 
   type, bind(C) :: olamgpu_eddy

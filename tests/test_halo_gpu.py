@@ -187,3 +187,121 @@ def test_two_processes_over_gloo():
             assert e < 1e-5, (rank, t, e)
         covered[cols] = True
     assert covered[1:].all()
+
+
+def _gloo_hook(dist, torch):
+    def hook(ranks, sbuf, rbuf):
+        ops, got = [], []
+        for r, sv, rv in zip(ranks, sbuf, rbuf):
+            if sv.size:
+                ops.append(dist.P2POp(dist.isend, torch.from_numpy(sv.copy()), r))
+            if rv.size:
+                t = torch.empty(rv.size, dtype=torch.float32)
+                got.append((rv, t))
+                ops.append(dist.P2POp(dist.irecv, t, r))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for rv, t in got:
+            rv[:] = t.numpy()
+        return 0
+    return hook
+
+
+W_OUT = ("rho", "press", "thil", "wc", "wmc", "vxe", "vye", "vze", "wmasc")
+V_OUT = ("vmc", "vc", "vmasc")
+
+
+def _long_case():
+    from olam_b200.synth.state import fast_lognormal_tracers
+    from test_dynamics_gpu import dyn_case
+    g, ds = dyn_case(nxp=8, nlev=12, seed=4)
+    arrays = oracle_lib.dyn_arrays(g, ds)
+    tr = fast_lognormal_tracers(g, 6, seed=8, as_list=True)
+    return g, arrays, tr
+
+
+def _long_steps(g, arrays, tr, halo=None, nsteps=2):
+    opts = abi.make_opts(600.0, nacoust=4)
+    hs = HostState(**{k: np.array(v, copy=True) for k, v in arrays.items()})
+    dev = OlamGpu(abi.FortranGrid(g), opts, hs)
+    p = [q.copy() for q in tr]
+    t = [np.zeros_like(q) for q in tr]
+    try:
+        dev.register_scalars(p, t)
+        dev.set_coherence(abi.RESIDENT)
+        if halo is not None:
+            dev.set_halo(halo)
+        for _ in range(nsteps):
+            dev.timestep(0)
+        dev.sync_to_host(abi.F_ALL)
+    finally:
+        dev.close()
+    return {n: hs[n] for n in W_OUT + V_OUT}, np.stack(p)
+
+
+def _long_proc(rank, world, port, q):
+    try:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                                timeout=timedelta(seconds=120))
+        g, arrays, tr = _long_case()
+        loc = decomp.local_grid(g, decomp.bisect(g, world), rank)
+        la = {k: (loc.w(v) if v.shape[0] == g.mwa else loc.v(v)) for k, v in arrays.items()}
+        lt = [loc.w(x) for x in tr]
+        halo = abi.make_halo(loc.send, loc.recv, _gloo_hook(dist, torch),
+                             vm=(loc.send_v, loc.recv_v, loc.send_m, loc.recv_m))
+        out, scp = _long_steps(loc.grid, la, lt, halo)
+        own = loc.owned
+        vown = loc.grid.jtv_prog - 1
+        res = {"w": loc.wmap[own], "v": loc.vmap[vown], "scp": scp[:, own]}
+        for n in W_OUT:
+            res[n] = out[n][own]
+        for n in V_OUT:
+            res[n] = out[n][vown]
+        q.put((rank, res))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:   # report to the parent instead of hanging it
+        import traceback
+        q.put((rank, repr(e) + traceback.format_exc()[-1500:]))
+
+
+def test_long_step_two_processes_over_gloo():
+    # two long steps of the whole dynamical core (olamgpu_timestep: the
+    # acoustic steps with their damping and the tracer step) on a two-way
+    # split, as two processes on the one GPU exchanging over gloo, against
+    # the one-domain run
+    import socket
+    import torch.multiprocessing as mp
+    g, arrays, tr = _long_case()
+    ref, rscp = _long_steps(g, arrays, tr)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_long_proc, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=600) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    covw = np.zeros(g.mwa, bool)
+    covv = np.zeros(g.mva, bool)
+    for rank, r in res:
+        assert not isinstance(r, str), r
+        for n in W_OUT:
+            e = relerr(r[n][:, 1:], ref[n][r["w"]][:, 1:])
+            assert e < 1e-6, (rank, n, e)
+        for n in V_OUT:
+            e = relerr(r[n][:, 1:], ref[n][r["v"]][:, 1:])
+            assert e < 1e-6, (rank, n, e)
+        e = relerr(r["scp"], rscp[:, r["w"]])
+        assert e < 1e-6, (rank, "scp", e)
+        covw[r["w"]] = True
+        covv[r["v"]] = True
+    assert covw[1:].all() and covv[1:].all()
