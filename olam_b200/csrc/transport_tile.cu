@@ -88,7 +88,7 @@ struct TileArgs {
 // Four tile columns per block of 256 threads, a thread per level.
 __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
   __shared__ int wall[4][TILE_TCW];
-  __shared__ float amall[4][TILE_AW];
+  __shared__ __align__(16) float amall[4][TILE_AW];
   const int sub = threadIdx.x >> 6, lt = threadIdx.x & 63;
   const size_t r = (size_t)blockIdx.x * 4 + sub;   // tile-column record
   const int t = (int)(r / A.T), i = (int)(r - (size_t)t * A.T);
@@ -118,15 +118,24 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
     const size_t x = (size_t)iw * mza + kd;
     float* o = A.wrec + x * TILE_WR;
     float sumw = 0.f;
-    float v4[4];
+    // four slots at a time (16-byte reads of the face rows of A)
+    const float4* am4 = reinterpret_cast<const float4*>(am);
 #pragma unroll
-    for (int j = 0; j < TILE_NS; ++j) {
-      float acc = 0.f;
+    for (int q = 0; q < TILE_NS / 4; ++q) {
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-      for (int f = 0; f < 6; ++f) acc = fmaf(dvvm[f], am[(f * 2 + up[f]) * TILE_NS + j], acc);
-      sumw += acc;
-      v4[j & 3] = acc;
-      if ((j & 3) == 3) reinterpret_cast<float4*>(o)[j >> 2] = make_float4(v4[0], v4[1], v4[2], v4[3]);
+      for (int f = 0; f < 6; ++f) {
+        const float4 a = am4[(f * 2 + up[f]) * (TILE_NS / 4) + q];
+        acc.x = fmaf(dvvm[f], a.x, acc.x);
+        acc.y = fmaf(dvvm[f], a.y, acc.y);
+        acc.z = fmaf(dvvm[f], a.z, acc.z);
+        acc.w = fmaf(dvvm[f], a.w, acc.w);
+      }
+      sumw += acc.x;
+      sumw += acc.y;
+      sumw += acc.z;
+      sumw += acc.w;
+      reinterpret_cast<float4*>(o)[q] = acc;
     }
     // vertical faces: grad_z_quadratic at level lev from (lev-1, lev, lev+1),
     // S(lev) + c1' (S(lev+1) - S(lev)) + c2' (S(lev) - S(lev-1)), the primes
