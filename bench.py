@@ -196,6 +196,12 @@ def dist_init(a):
     return 1, 0, 0, None
 
 
+def workload_name(g, a):
+    """The workload both arms report (the same string in both lines)."""
+    return (f"scalar_transport_rk NXP={a.nxp} ({g.mwa - 1} columns), {a.nlev} levels, {a.ntr} tracers, "
+            f"RK{a.nrk}, horiz order {a.order}, iscal_monot {a.monot}, dt {a.dt} s")
+
+
 def run_reference(a):
     ws, rank, local, dist = 1, int(os.environ.get("RANK", "0")), 0, None
     if rank != 0:
@@ -214,8 +220,8 @@ def run_reference(a):
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "impl": "reference",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"scalar_transport_rk NXP={a.nxp} {a.nlev} levels {a.ntr} "
-                                   f"tracers RK{a.nrk} order {a.order}"},
+            "config": {"workload": workload_name(g, a), "form": "the reference's loops (C++ restatement)",
+                       "parallelism": "host threads of one node"},
             "cpu_baseline": {"kind": res["kind"], "cores": res["cores"], "sample": res["sample"],
                              "value": v, "unit": "cell-updates/s"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
@@ -497,9 +503,7 @@ def main():
             "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"scalar_transport_rk NXP={a.nxp} ({g.mwa - 1} columns), "
-                                   f"{a.nlev} levels, {a.ntr} tracers, RK{a.nrk}, "
-                                   f"horiz order {a.order}, iscal_monot {a.monot}, dt {a.dt} s",
+            "config": {"workload": workload_name(g, a),
                        "form": "fused batched, tiled" if tiled else "fused batched",
                        "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (12.5 GB of tracers per array)"},
