@@ -152,11 +152,11 @@ static void release_all() {
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
                        &d.w_nb, &d.w_ev, &d.w_im, &d.v_iw, &d.v_im, &d.m_iv, &d.m_iw, &d.m_im,
                        &d.lpw, &d.lpv, &d.lpm, &d.iwglobe, &d.w_nonprog, &d.colrec,
-                       &d.tile_hdr, &d.tile_u, &d.tile_tc, &d.tile_rev};
+                       &d.tile_hdr, &d.tile_u, &d.tile_tc, &d.tile_rev, &d.tile_band_lev};
   for (auto* b : ib) b->release();
   DevBuf<float>* fb[] = {&d.w_dirv, &d.gxc, &d.gyc, &d.xy_h, &d.xy_hu, &d.dxps, &d.dyps, &d.xx0_v,
                          &d.xy0_v, &d.yy0_v, &d.xx0_vu, &d.xy0_vu, &d.yy0_vu, &d.a_w, &d.a_wu,
-                         &d.volti, &d.ew_b, &d.ew_u, &d.tile_a};
+                         &d.volti, &d.ew_b, &d.ew_u, &d.tile_a, &d.tile_band};
   for (auto* b : fb) b->release();
   d.ew_order = 0;
   d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
@@ -241,10 +241,8 @@ int olamgpu_init(const olamgpu_grid* grid, const olamgpu_opts* opts, const olamg
   if (order == 2 || order == 3) {
     rc = build_fused_weights(grid, C.g, order, C.stream);
     if (rc != OLAMGPU_OK) { release_all(); return rc; }
-    if (C.tp.flat) {
-      rc = build_tiles(grid, C.g, order, C.stream);
-      if (rc != OLAMGPU_OK) { release_all(); return rc; }
-    }
+    rc = build_tiles(grid, C.g, order, C.stream);
+    if (rc != OLAMGPU_OK) { release_all(); return rc; }
   }
   if (state) { C.hstate = *state; C.have_state = true; } else C.have_state = false;
   register_state_arrays(C);

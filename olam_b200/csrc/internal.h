@@ -143,7 +143,7 @@ struct DevGrid {
   DevBuf<float> ew_b, ew_u;      // (mva, 2, 8)
   int ew_order = 0;
   DevBuf<int> colrec;            // (nw_prog, COLREC_WORDS) fused-kernel column records
-  // Tile tables of the tiled fused kernel (flat grids).  Tile t owns tile_T
+  // Tile tables of the tiled fused kernel.  Tile t owns tile_T
   // consecutive prognostic columns; its neighbourhood U lists those columns,
   // then the rest of their neighbours, then the rest of those cells'
   // neighbours.  hdr[t] = {u_off, nU, 0, nT}.
@@ -152,6 +152,11 @@ struct DevGrid {
   DevBuf<int> tile_tc;           // (ntiles * tile_T, TILE_TCW) tile-cell records
   DevBuf<float> tile_a;          // (ntiles * tile_T, TILE_AW) slot weights
   DevBuf<int> tile_rev;          // (ntiles * tile_T, TILE_NS) transposed slots
+  // terrain: slot weights of the level bands of a column below which some
+  // term of its faces' reconstructions is under ground (TILE_AW floats per
+  // band) and the level at which each band ends
+  DevBuf<float> tile_band;
+  DevBuf<int> tile_band_lev;
   int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_order = 0;
   bool tile_closed = false;      // every neighbourhood column is prognosed
   std::vector<int> h_lpw;        // host copies used at set-up
@@ -162,7 +167,8 @@ struct DevGrid {
 // slots; the U-row byte offsets (U index * 256) of the TILE_NS slot columns
 // -- the cell's neighbours, then their other neighbours; unused slots point
 // at the cell itself; V index of each face; dirv of each face (pentagons:
-// the sixth face has dirv 0); pad.
+// the sixth face has dirv 0); the cell's first terrain band and its number
+// of bands (0 where every term is above ground at every level); pad.
 #define TILE_NS 20
 #define TILE_TC_IW 0
 #define TILE_TC_SIDE 1
@@ -171,12 +177,18 @@ struct DevGrid {
 #define TILE_TC_SLOT 4
 #define TILE_TC_EV 24
 #define TILE_TC_DV 30
+#define TILE_TC_BOFF 36
+#define TILE_TC_NB 37
 #define TILE_TCW 40
 // Slot weights (TILE_AW floats per tile cell): A[f][k][j] for face f < 6,
 // k = 0 when the cell is the upwind side of face f and 1 when the
 // neighbour across it is, slot j < TILE_NS: the weight of S(slot j) - S(cell)
 // in (upwind face value) - S(cell).  The order-2 or order-3 reconstruction
 // (gradient coefficients times face offsets) is folded into A at set-up.
+// With terrain the gradient of a cell leaves out, at level k, the
+// neighbours across its faces under ground (k < lpv of the face); a cell's
+// levels then fall into bands [lo, hi) with one A each, the last band (all
+// terms present) being the table above.
 #define TILE_AW (6 * 2 * TILE_NS)
 // Transposed slots (TILE_NS ints per tile cell), for the adjoint: for each
 // column c that has this cell as its slot j, c's U-row byte offset | j;
@@ -345,6 +357,8 @@ struct TileHost {
   int T = 0, ntiles = 0, nu_max = 0, order = 0;
   std::vector<int> hdr, ulist, tc, rev;
   std::vector<float> a;
+  std::vector<float> band;       // terrain bands (TILE_AW floats each)
+  std::vector<int> band_lev;     // the device level at which each band ends
 };
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th);
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);

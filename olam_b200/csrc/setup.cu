@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "internal.h"
@@ -425,7 +426,6 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       w[TILE_TC_NP] = np;
       w[TILE_TC_NS] = ns;
       for (int j = 0; j < TILE_NS; ++j) w[TILE_TC_SLOT + j] = (j < ns ? loc[slots[j]] : i) * 256;
-      std::fill(acc.begin(), acc.end(), 0.0);
       int side = 0;
       for (int f = 0; f < 6; ++f) {
         const bool v = f < np;
@@ -434,22 +434,55 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
         side |= sd << f;
         w[TILE_TC_EV + f] = iv;
         w[TILE_TC_DV + f] = fbits(v ? g->itab_w_dirv[(size_t)c * 7 + f] : 0.f);
-        if (!v) continue;
-        // the cell upwind: S(c) + sum_n w_n (S(nb_n(c)) - S(c))
-        for (int n = 0; n < np; ++n) acc[(f * 2 + 0) * TILE_NS + slot_of(nbr(c, n))] += face_weight(g, order, iv, sd, n);
-        // the neighbour u upwind: (1 - sum_n w_n)(S(u) - S(c)) + sum_n w_n (S(nb_n(u)) - S(c))
-        const int u = nbr(c, f), npu = g->npoly[u];
-        double sw = 0.0;
-        for (int n = 0; n < npu; ++n) {
-          const double wn = face_weight(g, order, iv, 1 - sd, n);
-          sw += wn;
-          const int x = nbr(u, n);
-          if (x != c) acc[(f * 2 + 1) * TILE_NS + slot_of(x)] += wn;
-        }
-        acc[(f * 2 + 1) * TILE_NS + slot_of(u)] += 1.0 - sw;
       }
       w[TILE_TC_SIDE] = side;
+      // device level of the lowest prognosed level of face iv
+      auto lpv_of = [&](int iv) { return g->lpv[iv] - 1; };
+      auto edge = [&](int x, int n) { return g->itab_w_iv[(size_t)x * 7 + n] - 1; };
+      // the slot weights at level lev: a gradient term counts where its
+      // face is above ground (grad_t2d skips k < lpv)
+      auto fold = [&](int lev) {
+        std::fill(acc.begin(), acc.end(), 0.0);
+        for (int f = 0; f < np; ++f) {
+          const int iv = w[TILE_TC_EV + f], sd = (side >> f) & 1;
+          // the cell upwind: S(c) + sum_n w_n (S(nb_n(c)) - S(c))
+          for (int n = 0; n < np; ++n)
+            if (lpv_of(edge(c, n)) <= lev)
+              acc[(f * 2 + 0) * TILE_NS + slot_of(nbr(c, n))] += face_weight(g, order, iv, sd, n);
+          // the neighbour u upwind: (1 - sum_n w_n)(S(u) - S(c)) + sum_n w_n (S(nb_n(u)) - S(c))
+          const int u = nbr(c, f), npu = g->npoly[u];
+          double sw = 0.0;
+          for (int n = 0; n < npu; ++n) {
+            if (lpv_of(edge(u, n)) > lev) continue;
+            const double wn = face_weight(g, order, iv, 1 - sd, n);
+            sw += wn;
+            const int x = nbr(u, n);
+            if (x != c) acc[(f * 2 + 1) * TILE_NS + slot_of(x)] += wn;
+          }
+          acc[(f * 2 + 1) * TILE_NS + slot_of(u)] += 1.0 - sw;
+        }
+      };
+      fold(std::numeric_limits<int>::max());
       for (int k = 0; k < TILE_AW; ++k) a[k] = (float)acc[k];
+      // terrain bands: the levels above the column's floor at which a term
+      // of its faces' reconstructions comes above ground
+      std::vector<int> ls;
+      const int kbc = g->lpw[c] - 1;
+      for (int f = 0; f < np; ++f) {
+        const int u = nbr(c, f);
+        for (int n = 0; n < np; ++n) ls.push_back(lpv_of(edge(c, n)));
+        for (int n = 0; n < g->npoly[u]; ++n) ls.push_back(lpv_of(edge(u, n)));
+      }
+      std::sort(ls.begin(), ls.end());
+      ls.erase(std::unique(ls.begin(), ls.end()), ls.end());
+      ls.erase(std::remove_if(ls.begin(), ls.end(), [&](int l) { return l <= kbc || l >= g->mza; }), ls.end());
+      w[TILE_TC_BOFF] = (int)(th.band_lev.size());
+      w[TILE_TC_NB] = (int)ls.size();
+      for (size_t b = 0; b < ls.size(); ++b) {
+        fold(b == 0 ? kbc : ls[b - 1]);
+        for (int k = 0; k < TILE_AW; ++k) th.band.push_back((float)acc[k]);
+        th.band_lev.push_back(ls[b]);
+      }
       // transposed slots: the cells that have c as a slot are c's own slot
       // cells (the relation "within two rings" is symmetric)
       int* r = &rv[((size_t)t * T + i) * TILE_NS];
@@ -484,6 +517,12 @@ int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
   OG_CHECK(upload(d.tile_a, th.a.data(), th.a.size(), s));
   OG_CHECK(upload(d.tile_rev, th.rev.data(), th.rev.size(), s));
   OG_CHECK(upload(d.tile_tc, th.tc.data(), th.tc.size(), s));
+  d.tile_band.release();
+  d.tile_band_lev.release();
+  if (!th.band_lev.empty()) {
+    OG_CHECK(upload(d.tile_band, th.band.data(), th.band.size(), s));
+    OG_CHECK(upload(d.tile_band_lev, th.band_lev.data(), th.band_lev.size(), s));
+  }
   OG_CUDA(cudaStreamSynchronize(s));
   // closed: every column of every neighbourhood is prognosed (a global
   // domain), so the transposed slots cover every column a stage reads

@@ -311,8 +311,8 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     set_error("a halo exchange needs the unlimited step (iscal_monot = 0) in a batched transport form");
     return OLAMGPU_E_UNSUPPORTED;
   }
-  if (batched && !tp.flat) {
-    set_error("the fused transport form needs lpw = lpv = 2 (no terrain); use the plain form");
+  if (batched && !tiled && !tp.flat) {
+    set_error("the per-column fused transport form needs lpw = lpv = 2 (no terrain); use the tiled or plain form");
     return OLAMGPU_E_UNSUPPORTED;
   }
   if (batched && !tiled && (double)mwa * mza * (double)((tr.ntp + 3) / 4 * 2) >= 4294967296.0) {

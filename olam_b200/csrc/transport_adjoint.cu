@@ -488,7 +488,7 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
     set_error("the adjoint does not cover horizontal diffusion of the tracers");
     return OLAMGPU_E_UNSUPPORTED;
   }
-  if (!tile_stage_available(d, tp, order)) {
+  if (!tp.flat || !tile_stage_available(d, tp, order)) {
     set_error("the adjoint needs the tiled transport tables (grids without terrain, lpw = lpv = 2)");
     return OLAMGPU_E_UNSUPPORTED;
   }

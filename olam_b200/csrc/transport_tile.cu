@@ -1,5 +1,4 @@
-// transport_tile.cu -- the fused RK stage of update_scalar in tiles, for
-// grids without terrain (lpw = lpv = 2 everywhere).
+// transport_tile.cu -- the fused RK stage of update_scalar in tiles.
 //
 // Restates, fused into one pass over the batched layout Q[iw][kd][ntp],
 // omodel/scalar_transport_rk.F90:
@@ -19,7 +18,11 @@
 // over the column's <= TILE_NS neighbours and second neighbours, with
 // W_j = sum_f dirv * vmasc * A[f][upwind][j].  The winds are fixed for the
 // long step, so k_weights forms these per-(column, level) records once per
-// step (both stages and the adjoint read them).
+// step (both stages and the adjoint read them).  With terrain a column's
+// faces, and the gradient terms across faces, below their lpv drop out (the
+// reference's loops start at lpv): k_weights leaves out the faces and takes
+// the slot weights of the level's terrain band; k_tile starts each column at
+// its own lpw.
 //
 // k_tile: a block owns a tile of T = 16 NC consecutive prognostic columns
 // and a group of 64 tracers and sweeps the levels bottom to top.  While it
@@ -40,6 +43,10 @@ namespace olamgpu {
 
 struct WeightArgs {
   int mza, T, kb, ntiles;
+  const int* __restrict__ lpw;      // lowest prognosed device level of each W column
+  const int* __restrict__ lpv;      // and of each V face
+  const float* __restrict__ band;   // terrain bands' slot weights (TILE_AW each)
+  const int* __restrict__ band_lev; // the level at which each band ends
   const int4* __restrict__ hdr;
   const int* __restrict__ tc;
   const float* __restrict__ amat;
@@ -53,6 +60,7 @@ struct WeightArgs {
 
 struct TileArgs {
   int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa;
+  const int* __restrict__ lpw;      // lowest prognosed device level of each W column
   int grp0, ngrp;                   // the tracer groups of 64 this launch runs
   float dtr;
   const int4* __restrict__ hdr;
@@ -102,14 +110,16 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
   __syncthreads();
   if (!live) return;
   const int iw = w[TILE_TC_IW], np = w[TILE_TC_NP], side = w[TILE_TC_SIDE];
-  const int mza = A.mza, kb = A.kb;
+  const int mza = A.mza, kb = max(A.kb, __ldg(A.lpw + iw));   // the column's own floor
+  const int nband = w[TILE_TC_NB], boff = w[TILE_TC_BOFF];
   for (int kd = kb + lt; kd < mza; kd += 64) {
     float dvvm[6];
     int up[6];
     float sw = 0.f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      const float vm = f < np ? __ldg(A.vmasc + (size_t)w[TILE_TC_EV + f] * mza + kd) : 0.f;
+      const int iv = w[TILE_TC_EV + f];
+      const float vm = (f < np && kd >= __ldg(A.lpv + iv)) ? __ldg(A.vmasc + (size_t)iv * mza + kd) : 0.f;
       dvvm[f] = __int_as_float(w[TILE_TC_DV + f]) * vm;
       // 1: the neighbour across face f is upwind
       up[f] = ((vm < 0.f ? 1 : 0) != ((side >> f) & 1)) ? 1 : 0;
@@ -119,24 +129,31 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
     float* o = A.wrec + x * TILE_WR;
     float sumw = 0.f;
     // four slots at a time (16-byte reads of the face rows of A)
-    const float4* am4 = reinterpret_cast<const float4*>(am);
+    auto slot_weights = [&](const float4* am4) {
 #pragma unroll
-    for (int q = 0; q < TILE_NS / 4; ++q) {
-      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int q = 0; q < TILE_NS / 4; ++q) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        const float4 a = am4[(f * 2 + up[f]) * (TILE_NS / 4) + q];
-        acc.x = fmaf(dvvm[f], a.x, acc.x);
-        acc.y = fmaf(dvvm[f], a.y, acc.y);
-        acc.z = fmaf(dvvm[f], a.z, acc.z);
-        acc.w = fmaf(dvvm[f], a.w, acc.w);
+        for (int f = 0; f < 6; ++f) {
+          const float4 a = am4[(f * 2 + up[f]) * (TILE_NS / 4) + q];
+          acc.x = fmaf(dvvm[f], a.x, acc.x);
+          acc.y = fmaf(dvvm[f], a.y, acc.y);
+          acc.z = fmaf(dvvm[f], a.z, acc.z);
+          acc.w = fmaf(dvvm[f], a.w, acc.w);
+        }
+        sumw += acc.x;
+        sumw += acc.y;
+        sumw += acc.z;
+        sumw += acc.w;
+        reinterpret_cast<float4*>(o)[q] = acc;
       }
-      sumw += acc.x;
-      sumw += acc.y;
-      sumw += acc.z;
-      sumw += acc.w;
-      reinterpret_cast<float4*>(o)[q] = acc;
-    }
+    };
+    // the terrain band of level kd (bands end at increasing levels; past
+    // the last one every term is above ground)
+    int b = 0;
+    while (b < nband && kd >= __ldg(A.band_lev + boff + b)) ++b;
+    if (b < nband) slot_weights(reinterpret_cast<const float4*>(A.band + (size_t)(boff + b) * TILE_AW));
+    else slot_weights(reinterpret_cast<const float4*>(am));
     // vertical faces: grad_z_quadratic at level lev from (lev-1, lev, lev+1),
     // S(lev) + c1' (S(lev+1) - S(lev)) + c2' (S(lev) - S(lev-1)), the primes
     // zeroing the differences across the column's ends
@@ -175,6 +192,8 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
   W.tc = d.tile_tc.p; W.amat = d.tile_a.p;
   W.vmasc = tp.vmasc.p; W.wmasc = tp.wmasc.p; W.volti = d.volti.p; W.rhos = rhos; W.a_w = d.a_w.p;
   W.wrec = tp.wrec.p;
+  W.lpw = d.lpw.p; W.lpv = d.lpv.p;
+  W.band = d.tile_band.p; W.band_lev = d.tile_band_lev.p;
   k_weights<<<cdiv((size_t)d.ntiles * d.tile_T, 4), 256, 0, s>>>(W);
   OG_LAUNCHED();
   return OLAMGPU_OK;
@@ -197,7 +216,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
   const int tile = blockIdx.x / ngrp, grp = A.grp0 + (blockIdx.x - tile * ngrp);
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
-  const int mza = A.mza, ntp = A.ntp, kb = A.kb;
+  const int mza = A.mza, ntp = A.ntp, kb = A.kb;   // kb: the lowest floor of any column
   const int nu4 = (nU + 3) & ~3;      // rows gathered four at a time
   auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
   const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * 256), rbuf = al((size_t)T * TILE_WR * 4);
@@ -278,12 +297,14 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
   const int cb = 2 * warp + half;
   F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], s00[NC], st[NC];
   OFF cbase[NC];
+  int kbc[NC];   // each column's own floor (lpw): levels below it are not prognosed
   stage(kb, 0);
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
     const int c = cb + 16 * n;
     m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = s00[n] = st[n] = zero4();
     cbase[n] = 0;
+    kbc[n] = c < nT ? max(kb, __ldg(A.lpw + IWT[c])) : mza;
     if (c < nT && act) {
       cbase[n] = (OFF)IWT[c] * (OFF)mza * (OFF)ntp + (OFF)(t0 + 4 * hl);
       if (kb + 1 < mza) p1[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 1) * (OFF)ntp));
@@ -307,6 +328,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
     for (int n = 0; n < NC; ++n) {
       const int c = cb + 16 * n;
       if (c >= nT) continue;
+      // the column's window holds no level below its floor
+      if (kd == kbc[n]) m2[n] = m1[n] = zero4();
       const float* rc = Rc + c * TILE_WR;
       const float4 r5 = reinterpret_cast<const float4*>(rc)[5];   // SW, volti/rhos, 1/rhos, D
       const float4 r6 = reinterpret_cast<const float4*>(rc)[6];   // beta0 .. beta3
@@ -337,9 +360,10 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
       // scp = scp0 + dtr * (sct + volti * (fluxdiv + fexpl * vflux)) / rhos
       const F4 o = fma4s(A.dtr * r5.y, fd, fma4s(A.dtr * r5.z, st[n], s00[n]));
       if (act) {
-        stg4(A.OUT + (cbase[n] + (OFF)kd * (OFF)ntp), o);
-        if (kd == kb)
-          for (int k2 = 0; k2 < kb; ++k2) stg4(A.OUT + (cbase[n] + (OFF)k2 * (OFF)ntp), o);
+        if (kd >= kbc[n]) stg4(A.OUT + (cbase[n] + (OFF)kd * (OFF)ntp), o);
+        // levels below the floor take the floor's value (scalar_w_column)
+        if (kd == kbc[n])
+          for (int k2 = 0; k2 < kd; ++k2) stg4(A.OUT + (cbase[n] + (OFF)k2 * (OFF)ntp), o);
         // slide the column's window up one level and read ahead
         m2[n] = m1[n]; m1[n] = s0; p1[n] = p2[n]; p2[n] = p3[n];
         if (kd + 4 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(kd + 4) * (OFF)ntp));
@@ -389,7 +413,8 @@ static int row_map(CUtensorMap* m, const float* base, int width, size_t nrows, i
 }
 
 bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
-  return tp.flat && (d.tile_T == 16 || d.tile_T == 32) && d.tile_order == order;
+  (void)tp;
+  return (d.tile_T == 16 || d.tile_T == 32) && d.tile_order == order;
 }
 
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
@@ -402,7 +427,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   TileArgs A;
   A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1;
   A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.mwa = d.mwa;
-  A.dtr = dtr;
+  A.dtr = dtr; A.lpw = d.lpw.p;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   A.ulist = d.tile_u.p; A.tc = d.tile_tc.p;
   A.ff = tp.ff.p; A.wrec = tp.wrec.p;

@@ -1,0 +1,120 @@
+"""scalar_transport_rk on a grid with terrain through the C-ABI: a mountain
+raises the lowest prognosed level lpw of the columns under it (up to 4
+levels) and every face takes the higher floor of its two cells (lpv), so
+the reconstruction and the flux divergence drop faces and gradient terms
+level by level (the reference's loops start at lpv and lpw).  The tiled
+and plain forms are checked against the oracle, and against themselves
+with NaN below every floor (values the reference never reads)."""
+import copy
+
+import numpy as np
+import pytest
+
+import oracle_lib
+from conftest import relerr, small_case
+from olam_b200 import abi
+from olam_b200.lib import HostState, OlamGpu, OlamGpuError
+from test_transport_gpu import TOL32, TOL64
+
+pytestmark = pytest.mark.gpu
+
+
+def terrain_case(nxp=6, nlev=12, ntr=6, hmax=4, **kw):
+    g0, st0 = small_case(nxp=nxp, nlev=nlev, ntr=ntr, **kw)
+    g = copy.copy(g0)
+    xyz = np.asarray(g.xew, dtype=np.float64).T
+    rad = np.linalg.norm(xyz, axis=1)
+    rad[rad == 0] = 1.0
+    top = xyz[1] / rad[1]
+    ang = np.arccos(np.clip(xyz @ top / rad, -1.0, 1.0))
+    lpw = 2 + np.floor(hmax * np.clip(1.0 - ang / 0.9, 0.0, 1.0) ** 0.6).astype(np.int32)
+    lpw = np.minimum(lpw, g.mza - 2)
+    lpw[0] = 2
+    g.lpw = lpw.astype(np.int32)
+    g.lpv = np.maximum(lpw[g.itab_v_iw[:, 0]], lpw[g.itab_v_iw[:, 1]]).astype(np.int32)
+    g.lpv[0] = 2
+    return g, st0
+
+
+def run(g, st, opts, form, tracers=None, prof=False):
+    hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)
+    dev = OlamGpu(abi.FortranGrid(g), opts, hs)
+    try:
+        dev.set_transport_form(form)
+        var_p = [np.ascontiguousarray(t.copy()) for t in (tracers if tracers is not None else st.tracers)]
+        var_t = [np.ascontiguousarray(t.copy()) for t in st.sct]
+        dev.register_scalars(var_p, var_t)
+        if prof:
+            dev.profile(True, reset=True)
+        dev.scalar_transport_rk(st.rho_old)
+        p = dev.profile_read() if prof else None
+        return np.stack(var_p), p
+    finally:
+        dev.close()
+
+
+def test_terrain_case_has_terrain():
+    g, _ = terrain_case()
+    assert (g.lpw[1:] > 2).sum() > 20 and (g.lpw[1:] == 2).sum() > 20
+    assert g.lpw.max() >= 5
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(nrk_scal=3), dict(scal_order=3),
+                                dict(nrk_scal=3, scal_order=3), dict(iscal_monot=1), dict(iscal_monot=2)])
+def test_terrain_parity(kw):
+    g, st = terrain_case()
+    opts = abi.make_opts(1800.0, **kw)
+    fg = abi.FortranGrid(g)
+    ref32 = oracle_lib.scalar_transport(fg, opts, st.tracers, st.sct, st)
+    ref64 = oracle_lib.scalar_transport(fg, opts, st.tracers, st.sct, st, fp64=True)
+    tiled, prof = run(g, st, opts, abi.TRANSPORT_FUSED, prof=True)
+    assert "tile_stage1" in prof, prof
+    plain, _ = run(g, st, opts, abi.TRANSPORT_PLAIN)
+    for out in (tiled, plain):
+        for n in range(st.ntr):
+            assert relerr(out[n], ref64[n]) < TOL64, (kw, n, relerr(out[n], ref64[n]))
+            assert relerr(out[n], ref32[n]) < TOL32, (kw, n, relerr(out[n], ref32[n]))
+
+
+def test_terrain_parity_implicit():
+    # vertical CFL > 1: implicit columns, their solves starting at lpw
+    g, st = terrain_case(nxp=5, nlev=12, ntr=4, dtlm=3600.0, seed=7, w_amp=3.0)
+    for kw in (dict(), dict(nrk_scal=3)):
+        opts = abi.make_opts(3600.0, **kw)
+        fg = abi.FortranGrid(g)
+        ref64, ff, _ = oracle_lib.scalar_transport(fg, opts, st.tracers, st.sct, st, fp64=True, want_ff=True)
+        assert (ff > 0).any()
+        out, _ = run(g, st, opts, abi.TRANSPORT_FUSED)
+        for n in range(st.ntr):
+            assert relerr(out[n], ref64[n]) < TOL64, (kw, n, relerr(out[n], ref64[n]))
+
+
+@pytest.mark.parametrize("form", [abi.TRANSPORT_FUSED, abi.TRANSPORT_PLAIN])
+def test_terrain_never_reads_below_the_floor(form):
+    g, st = terrain_case()
+    opts = abi.make_opts(1800.0, nrk_scal=3, scal_order=3)
+    base, _ = run(g, st, opts, form)
+    tr = [t.copy() for t in st.tracers]
+    below = np.arange(g.mza)[None, :] < (g.lpw[:, None] - 1)
+    below[0] = False
+    for t in tr:
+        t[below] = np.nan
+    out, _ = run(g, st, opts, form, tracers=tr)
+    assert np.isfinite(out[:, 1:]).all()
+    # the levels below a floor take the floor's value, as with finite inputs
+    assert np.array_equal(out[:, 1:], base[:, 1:])
+
+
+def test_terrain_column_form_and_adjoint_rejected():
+    g, st = terrain_case()
+    opts = abi.make_opts(1800.0)
+    with pytest.raises(OlamGpuError):
+        run(g, st, opts, abi.TRANSPORT_FUSED_COLUMN)
+    hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)
+    dev = OlamGpu(abi.FortranGrid(g), opts, hs)
+    try:
+        dev.register_scalars([t.copy() for t in st.tracers], [t.copy() for t in st.sct])
+        with pytest.raises(OlamGpuError):
+            dev.scalar_transport_rk_adjoint([t.copy() for t in st.tracers], st.rho_old)
+    finally:
+        dev.close()
