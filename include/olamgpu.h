@@ -249,11 +249,11 @@ int olamgpu_sync_to_host(unsigned fieldmask);
  * OLAMGPU_TRANSPORT_FUSED (default): all tracers of an RK stage in one
  *   launch over the batched layout, in tiles of neighbouring columns whose
  *   neighbourhood is staged in shared memory (one column per block where
- *   the tile tables do not fit).
+ *   the tile tables do not fit).  Runs any lpw / lpv (terrain).
  * OLAMGPU_TRANSPORT_PLAIN: one set of kernels per tracer mirroring the
  *   reference's passes (kept for comparison).
  * OLAMGPU_TRANSPORT_FUSED_COLUMN: the batched form with one column per
- *   block (kept for comparison). */
+ *   block (kept for comparison; grids without terrain only). */
 enum { OLAMGPU_TRANSPORT_FUSED = 0, OLAMGPU_TRANSPORT_PLAIN = 1, OLAMGPU_TRANSPORT_FUSED_COLUMN = 2 };
 int olamgpu_set_transport_form(int form);
 
