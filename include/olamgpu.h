@@ -270,8 +270,9 @@ int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag);
  * applies its transpose.  lam[n] (mza,mwa) holds dJ/d(new scp) of tracer n
  * on entry and dJ/d(old scp) on return; lam_sct[n] receives dJ/d(sct).
  * rho_old and the registered vmasc / wmasc / rho are those of the forward
- * step.  No counterpart in the reference (OLAM has no adjoint); grids with
- * terrain, iscal_monot > 0 and tracer diffusion get OLAMGPU_E_UNSUPPORTED. */
+ * step.  No counterpart in the reference (OLAM has no adjoint); any lpw /
+ * lpv (terrain); iscal_monot > 0 and tracer diffusion get
+ * OLAMGPU_E_UNSUPPORTED. */
 int olamgpu_scalar_transport_rk_adjoint(const float* rho_old, float* const* lam, float* const* lam_sct);
 
 /* Replaces prog_wrtv_rk() (prog_wrtv_rk.f90:58-488); istp is mem_ijtabs%istp. */

@@ -135,6 +135,7 @@ __global__ void k_adj_implicit(GridK g, const int* __restrict__ list, const int*
 
 struct AdjRecArgs {
   int mza, T, kb, mwa;
+  const int* __restrict__ lpw;      // each W column's floor (device level)
   const int4* __restrict__ hdr;
   const int* __restrict__ ulist;
   const int* __restrict__ tc;
@@ -148,7 +149,7 @@ struct AdjRecArgs {
 
 // one block per tile column, a thread per level
 __global__ void k_adj_records(AdjRecArgs A) {
-  __shared__ int cols[TILE_NS], js[TILE_NS];
+  __shared__ int cols[TILE_NS], js[TILE_NS], kbs[TILE_NS];
   __shared__ int xs;
   const int t = blockIdx.x / A.T, i = blockIdx.x - t * A.T;
   const int4 h = A.hdr[t];
@@ -164,14 +165,16 @@ __global__ void k_adj_records(AdjRecArgs A) {
     if (c < 1 || c >= A.mwa) { c = 1; j = TILE_NS; }
     cols[threadIdx.x] = c;
     js[threadIdx.x] = j;
+    kbs[threadIdx.x] = max(A.kb, __ldg(A.lpw + c));   // c is prognosed from this level up
   }
   if (threadIdx.x == 0) {
     int x = __ldg(A.tc + (size_t)blockIdx.x * TILE_TCW + TILE_TC_IW);
     xs = (x >= 1 && x < A.mwa) ? x : 0;
   }
   __syncthreads();
-  const int x = xs, mza = A.mza, kb = A.kb;
+  const int x = xs, mza = A.mza;
   if (x == 0) return;
+  const int kb = max(A.kb, __ldg(A.lpw + x));   // x's own floor
   const float* wm = A.wmasc + (size_t)x * mza;
   auto rec = [&](int col, int k) { return A.wrec + ((size_t)col * mza + k) * TILE_WR; };
   for (int kd = kb + threadIdx.x; kd < mza; kd += blockDim.x) {
@@ -181,7 +184,7 @@ __global__ void k_adj_records(AdjRecArgs A) {
     for (int e = 0; e < TILE_NS; ++e) {
       const int j = js[e];
       const float* rc = rec(cols[e], kd);
-      v4[e & 3] = j < TILE_NS ? __ldg(rc + j) * __ldg(rc + TILE_NS + 1) : 0.f;
+      v4[e & 3] = (j < TILE_NS && kd >= kbs[e]) ? __ldg(rc + j) * __ldg(rc + TILE_NS + 1) : 0.f;
       if ((e & 3) == 3) reinterpret_cast<float4*>(o)[e >> 2] = make_float4(v4[0], v4[1], v4[2], v4[3]);
     }
     // faces f = kd-2 .. kd+1 (the ones whose upwind stencil can hold level
@@ -221,6 +224,7 @@ __global__ void k_adj_records(AdjRecArgs A) {
 // ---- transpose of update_scalar over a tile -----------------------------------
 struct TileAdjArgs {
   int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa;
+  const int* __restrict__ lpw;      // each W column's floor (device level)
   float dtr;
   int first, last;                  // first / last reverse stage of the step
   const int4* __restrict__ hdr;
@@ -321,6 +325,7 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], l0[NC], ls[NC];
   long long cbase[NC];
   bool need0[NC];
+  int kbc[NC];   // each column's own floor: levels below it are not prognosed
   stage(kb, 0);
   __syncthreads();   // FEX
 #pragma unroll
@@ -329,6 +334,7 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
     m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = l0[n] = ls[n] = zero4();
     cbase[n] = 0;
     need0[n] = false;
+    kbc[n] = c < nT ? max(kb, __ldg(A.lpw + IWT[c])) : mza;
     if (c < nT && act) {
       need0[n] = !first || FEX[c] < 1.0f;
       cbase[n] = (long long)IWT[c] * mza * ntp + t0 + 4 * hl;
@@ -352,6 +358,7 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
     for (int n = 0; n < NC; ++n) {
       const int c = cb + 16 * n;
       if (c >= nT) continue;
+      if (kd == kbc[n]) m2[n] = m1[n] = zero4();
       const float* rc = Rc + c * TADJ_RW;
       const F4 lx = lds4(Ul, c * 256);
       F4 acc = zero4();
@@ -381,15 +388,18 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
       const F4 lsn = fma4s(dtr * ri, lx, ls[n]);
       if (act) {
         const long long row = cbase[n] + (long long)kd * ntp;
-        if (last) {
-          stg4(A.LIN + row, add4(lin, l0n));
-        } else {
-          stg4(A.LIN + row, lin);
-          stg4(A.L0 + row, l0n);
+        if (kd >= kbc[n]) {
+          if (last) {
+            stg4(A.LIN + row, add4(lin, l0n));
+          } else {
+            stg4(A.LIN + row, lin);
+            stg4(A.L0 + row, l0n);
+          }
+          stg4(A.LS + row, lsn);
         }
-        stg4(A.LS + row, lsn);
-        if (kd == kb)
-          for (int k2 = 0; k2 < kb; ++k2) {
+        // the stage reads no level below the column's floor
+        if (kd == kbc[n])
+          for (int k2 = 0; k2 < kd; ++k2) {
             const long long r2 = cbase[n] + (long long)k2 * ntp;
             stg4(A.LIN + r2, zero4());
             if (first) { stg4(A.L0 + r2, zero4()); stg4(A.LS + r2, zero4()); }
@@ -412,7 +422,7 @@ static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L
                            int ntp, int istage, int nrk, float dtr, int first, int last, int* status,
                            cudaStream_t s) {
   TileAdjArgs A;
-  A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1;
+  A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1; A.lpw = d.lpw.p;
   A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.mwa = d.mwa;
   A.dtr = dtr; A.first = first; A.last = last;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
@@ -440,7 +450,7 @@ static int launch_adj_records(const DevGrid& d, Transport& tp, int* status, cuda
     OG_CUDA(cudaMemsetAsync(tp.adj_trec.p, 0, tp.adj_trec.bytes(), s));
   }
   AdjRecArgs R;
-  R.mza = d.mza; R.T = d.tile_T; R.kb = 1; R.mwa = d.mwa;
+  R.mza = d.mza; R.T = d.tile_T; R.kb = 1; R.mwa = d.mwa; R.lpw = d.lpw.p;
   R.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   R.ulist = d.tile_u.p; R.tc = d.tile_tc.p; R.rev = d.tile_rev.p;
   R.wrec = tp.wrec.p; R.wmasc = tp.wmasc.p; R.a_w = d.a_w.p; R.trec = tp.adj_trec.p;
@@ -488,8 +498,8 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
     set_error("the adjoint does not cover horizontal diffusion of the tracers");
     return OLAMGPU_E_UNSUPPORTED;
   }
-  if (!tp.flat || !tile_stage_available(d, tp, order)) {
-    set_error("the adjoint needs the tiled transport tables (grids without terrain, lpw = lpv = 2)");
+  if (!tile_stage_available(d, tp, order)) {
+    set_error("the adjoint needs the tiled transport tables");
     return OLAMGPU_E_UNSUPPORTED;
   }
   if (!d.tile_closed) {

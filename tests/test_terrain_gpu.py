@@ -4,7 +4,8 @@ levels) and every face takes the higher floor of its two cells (lpv), so
 the reconstruction and the flux divergence drop faces and gradient terms
 level by level (the reference's loops start at lpv and lpw).  The tiled
 and plain forms are checked against the oracle, and against themselves
-with NaN below every floor (values the reference never reads)."""
+with NaN below every floor (values the reference never reads); the tiled
+adjoint against the oracle's adjoint."""
 import copy
 
 import numpy as np
@@ -105,16 +106,20 @@ def test_terrain_never_reads_below_the_floor(form):
     assert np.array_equal(out[:, 1:], base[:, 1:])
 
 
-def test_terrain_column_form_and_adjoint_rejected():
+def test_terrain_column_form_rejected():
     g, st = terrain_case()
-    opts = abi.make_opts(1800.0)
     with pytest.raises(OlamGpuError):
-        run(g, st, opts, abi.TRANSPORT_FUSED_COLUMN)
-    hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)
-    dev = OlamGpu(abi.FortranGrid(g), opts, hs)
-    try:
-        dev.register_scalars([t.copy() for t in st.tracers], [t.copy() for t in st.sct])
-        with pytest.raises(OlamGpuError):
-            dev.scalar_transport_rk_adjoint([t.copy() for t in st.tracers], st.rho_old)
-    finally:
-        dev.close()
+        run(g, st, abi.make_opts(1800.0), abi.TRANSPORT_FUSED_COLUMN)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(nrk_scal=3, scal_order=3)])
+def test_terrain_adjoint_matches_oracle(kw):
+    from test_adjoint_gpu import _adjoint_vs_oracle
+    g, st = terrain_case(ntr=3)
+    _adjoint_vs_oracle(g, st, abi.make_opts(1800.0, **kw), 3)
+
+
+def test_terrain_adjoint_implicit_columns():
+    from test_adjoint_gpu import _adjoint_vs_oracle
+    g, st = terrain_case(nxp=5, nlev=12, ntr=4, dtlm=3600.0, seed=7, w_amp=3.0)
+    _adjoint_vs_oracle(g, st, abi.make_opts(3600.0, nrk_scal=3), 4)
