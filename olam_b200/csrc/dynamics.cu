@@ -695,8 +695,7 @@ int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s) {
     return OLAMGPU_E_ARG;
   }
   for (int i = 1; i < mma; ++i)
-    if (g->lpm[i] != 2) { set_error("prog_wrtv_rk on this build needs flat terrain (lpm = 2)"); return OLAMGPU_E_UNSUPPORTED; }
-  if (!C.tp.flat) { set_error("prog_wrtv_rk on this build needs flat terrain (lpw = lpv = 2)"); return OLAMGPU_E_UNSUPPORTED; }
+    if (g->lpm[i] < 2 || g->lpm[i] > mza) { set_error("lpm out of range [2,mza] at M point " + std::to_string(i + 1)); return OLAMGPU_E_ARG; }
   for (int i = 1; i < mwa; ++i)
     if (g->lve2 && g->lve2[i] != 0) { set_error("shaved cells (lve2 > 0) are not supported"); return OLAMGPU_E_UNSUPPORTED; }
   if (mza > 128) { set_error("prog_wrtv_rk supports mza <= 128"); return OLAMGPU_E_UNSUPPORTED; }

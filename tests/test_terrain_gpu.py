@@ -5,7 +5,8 @@ the reconstruction and the flux divergence drop faces and gradient terms
 level by level (the reference's loops start at lpv and lpw).  The tiled
 and plain forms are checked against the oracle, and against themselves
 with NaN below every floor (values the reference never reads); the tiled
-adjoint against the oracle's adjoint."""
+adjoint against the oracle's adjoint; prog_wrtv_rk's long step against
+the oracle and olamgpu_timestep against the single calls."""
 import copy
 
 import numpy as np
@@ -20,8 +21,10 @@ from test_transport_gpu import TOL32, TOL64
 pytestmark = pytest.mark.gpu
 
 
-def terrain_case(nxp=6, nlev=12, ntr=6, hmax=4, **kw):
-    g0, st0 = small_case(nxp=nxp, nlev=nlev, ntr=ntr, **kw)
+def terrain_grid(g0, hmax=4):
+    """A copy of grid g0 with a mountain: lpw rises to 2 + hmax under it,
+    a face's lpv is the higher floor of its two cells, an M point's lpm the
+    highest lpv of its three faces (omodel/hex_grid.f90:1446)."""
     g = copy.copy(g0)
     xyz = np.asarray(g.xew, dtype=np.float64).T
     rad = np.linalg.norm(xyz, axis=1)
@@ -34,7 +37,14 @@ def terrain_case(nxp=6, nlev=12, ntr=6, hmax=4, **kw):
     g.lpw = lpw.astype(np.int32)
     g.lpv = np.maximum(lpw[g.itab_v_iw[:, 0]], lpw[g.itab_v_iw[:, 1]]).astype(np.int32)
     g.lpv[0] = 2
-    return g, st0
+    g.lpm = np.max(g.lpv[g.itab_m_iv], axis=1).astype(np.int32)
+    g.lpm[0] = 2
+    return g
+
+
+def terrain_case(nxp=6, nlev=12, ntr=6, hmax=4, **kw):
+    g0, st0 = small_case(nxp=nxp, nlev=nlev, ntr=ntr, **kw)
+    return terrain_grid(g0, hmax), st0
 
 
 def run(g, st, opts, form, tracers=None, prof=False):
@@ -123,3 +133,52 @@ def test_terrain_adjoint_implicit_columns():
     from test_adjoint_gpu import _adjoint_vs_oracle
     g, st = terrain_case(nxp=5, nlev=12, ntr=4, dtlm=3600.0, seed=7, w_amp=3.0)
     _adjoint_vs_oracle(g, st, abi.make_opts(3600.0, nrk_scal=3), 4)
+
+
+DYN_CASES = [dict(), dict(nrk_wrtv=2), dict(thil_order=3, wind_order=3),
+             dict(ithil_monot=1, iwind_monot=1), dict(divh_damp_fact=0.0, vort_damp_fact=0.0)]
+
+
+@pytest.mark.parametrize("kw", DYN_CASES)
+def test_terrain_long_step_parity(kw):
+    from test_dynamics_gpu import check_fields, dyn_case, gpu_long_steps, oracle_long_steps
+    g0, ds = dyn_case()
+    g = terrain_grid(g0)
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(600.0, nacoust=4, **kw)
+    arrays = oracle_lib.dyn_arrays(g, ds)
+    o64, _ = oracle_long_steps(fg, opts, arrays, 1, True)
+    o32, _ = oracle_long_steps(fg, opts, arrays, 1, False)
+    hs, _ = gpu_long_steps(fg, opts, arrays, 1, abi.SYNC_EACH_CALL)
+    check_fields(hs, o32, o64)
+
+
+def test_terrain_timestep_matches_single_calls():
+    from test_timestep_gpu import Dev, _case, _same
+    g0, _, arrays, tr = _case()
+    g = terrain_grid(g0)
+    opts = abi.make_opts(600.0, nacoust=4)
+    out = []
+    for one_call in (False, True):
+        d = Dev(g, arrays, tr, opts)
+        try:
+            for _ in range(2):
+                if one_call:
+                    d.dev.timestep(0)
+                else:
+                    d.dev.tend0(None)
+                    for j in range(1, opts.nacoust + 1):
+                        d.dev.prog_wrtv_rk(j)
+                    d.dev.timeavg_momsc()
+                    d.dev.scalar_transport_rk(None)
+                    d.dev.set_scalars_bottom()
+            out.append(d.host())
+        finally:
+            d.close()
+    _same(out[0], out[1])
+    scp = out[1]["scp"]
+    assert np.isfinite(scp[:, 1:]).all()
+    # the levels below each column's floor took the floor's value
+    for iw in range(1, g.mwa):
+        kb = g.lpw[iw] - 1
+        assert np.array_equal(scp[:, iw, :kb], np.repeat(scp[:, iw, kb:kb + 1], kb, axis=1))
