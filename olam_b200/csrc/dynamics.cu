@@ -607,17 +607,73 @@ __global__ void k_prog_v(DynK g, const int* __restrict__ vprog, int nv, float dt
   vc[x] = 2.0f * v / (float)(rho[x1] + rho[x2]);
 }
 
-// vel_t3d_hex (vel_t3d.f90:39-108), no shaved cells
+// Prognostic shaved-cell method (prog_wrtv_rk.f90:202-211): the momentum of
+// the lve2 lowest levels of a column with closed V faces at the step's start.
+// A thread per (column, shaved level).
+__global__ void k_shaved_save(DynK g, const int* __restrict__ prog, int nprog, const int* __restrict__ lve2,
+                              int nve2, const float* __restrict__ vxe, const float* __restrict__ vye,
+                              const float* __restrict__ vze, const double* __restrict__ rho, float* __restrict__ vm0) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nprog * nve2) return;
+  const int j = (int)(i / nve2), ks = (int)(i % nve2);
+  const int iw = prog[j];
+  if (ks >= lve2[iw]) return;
+  const size_t x = (size_t)iw * g.mza + LPW(iw) + ks;
+  const float rs = (float)rho[x];
+  float* o = vm0 + ((size_t)iw * nve2 + ks) * 3;
+  o[0] = vxe[x] * rs; o[1] = vye[x] * rs; o[2] = vze[x] * rs;
+}
+
+// the shaved-cell inputs of k_vel_t3d: lve2 == nullptr on grids without
+// closed faces; prog != 0 in a stage of prog_wrtv_rk (the velocities of the
+// shaved levels are prognosed first, update_vxe_undrgnd), 0 in diagvel_t3d
+// (the cell's current velocities)
+struct Shaved {
+  const int* lve2;
+  const float* vm0;
+  const float *rkx, *rky, *rkz;
+  const double* rho;
+  const float* vn;
+  int nve2, prog;
+  float dts;
+};
+
+static Shaved shaved_args(const Dyn& y, const Transport& tp, int prog, float dts) {
+  Shaved a{};
+  if (y.nve2_max > 0) { a.lve2 = y.lve2.p; a.vm0 = y.vm0.p; a.nve2 = y.nve2_max; }
+  a.rkx = y.rk_vx.p; a.rky = y.rk_vy.p; a.rkz = y.rk_vz.p;
+  a.rho = tp.rho.p; a.vn = y.vn.p; a.prog = prog; a.dts = dts;
+  return a;
+}
+
+// update_vxe_undrgnd (prog_wrtv_rk.f90:1558-1595) and vel_t3d_hex
+// (vel_t3d.f90:39-108): a closed face (below its lpv) contributes the normal
+// component of the cell's prognosed velocity at that level
 __global__ void k_vel_t3d(DynK g, const int* __restrict__ prog, int nprog, const float* __restrict__ wc,
                           const float* __restrict__ vc, const float* __restrict__ wno2,
                           const float* __restrict__ ecv, float* __restrict__ vxe, float* __restrict__ vye,
-                          float* __restrict__ vze) {
+                          float* __restrict__ vze, Shaved sh) {
   PK(j, kd, nprog);
   const int iw = WTAB(j);
   const int kb = LPW(iw);
   if (kd < kb) return;
   const int mza = g.mza;
   const size_t cb = (size_t)iw * mza;
+  const int ks = kd - kb;
+  const bool shaved = sh.lve2 && ks < sh.lve2[iw];
+  float p1x = 0.f, p1y = 0.f, p1z = 0.f;
+  if (shaved) {
+    if (sh.prog) {
+      const float rsi = 1.0f / (float)sh.rho[cb + kd];
+      const float vt = g.volti[cb + kd];
+      const float* m = sh.vm0 + ((size_t)iw * sh.nve2 + ks) * 3;
+      p1x = (m[0] + sh.dts * (sh.rkx[cb + kd] * vt)) * rsi;
+      p1y = (m[1] + sh.dts * (sh.rky[cb + kd] * vt)) * rsi;
+      p1z = (m[2] + sh.dts * (sh.rkz[cb + kd] * vt)) * rsi;
+    } else {
+      p1x = vxe[cb + kd]; p1y = vye[cb + kd]; p1z = vze[cb + kd];
+    }
+  }
   const float wst = wc[cb + kd - 1] + wc[cb + kd];
   float x = wst * wno2[iw * 3], y = wst * wno2[iw * 3 + 1], z = wst * wno2[iw * 3 + 2];
   const int np = g.npoly[iw];
@@ -625,8 +681,10 @@ __global__ void k_vel_t3d(DynK g, const int* __restrict__ prog, int nprog, const
   for (int n = 0; n < 7; ++n) {
     if (n >= np) break;
     const int iv = g.w_ev[iw * 8 + n];
-    if (kd < LPV(iv)) continue;
-    const float v = vc[(size_t)iv * mza + kd];
+    float v;
+    if (kd >= LPV(iv)) v = vc[(size_t)iv * mza + kd];
+    else if (shaved) v = sh.vn[iv * 3] * p1x + sh.vn[iv * 3 + 1] * p1y + sh.vn[iv * 3 + 2] * p1z;
+    else continue;
     x = x + ecv[(iw * 7 + n) * 3] * v;
     y = y + ecv[(iw * 7 + n) * 3 + 1] * v;
     z = z + ecv[(iw * 7 + n) * 3 + 2] * v;
@@ -696,8 +754,30 @@ int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s) {
   }
   for (int i = 1; i < mma; ++i)
     if (g->lpm[i] < 2 || g->lpm[i] > mza) { set_error("lpm out of range [2,mza] at M point " + std::to_string(i + 1)); return OLAMGPU_E_ARG; }
-  for (int i = 1; i < mwa; ++i)
-    if (g->lve2 && g->lve2[i] != 0) { set_error("shaved cells (lve2 > 0) are not supported"); return OLAMGPU_E_UNSUPPORTED; }
+  // shaved cells: lve2(iw) levels from lpw up have closed V faces; every
+  // closed face must lie within them (hex_grid.f90 sets lve2 to the largest
+  // lpv - lpw of the column's faces)
+  int nve2 = 0;
+  std::vector<int> lve2(mwa, 0);
+  for (int i = 1; i < mwa; ++i) {
+    const int l = g->lve2 ? g->lve2[i] : 0;
+    if (l < 0 || l > mza) { set_error("lve2 out of range [0,mza] at W point " + std::to_string(i + 1)); return OLAMGPU_E_ARG; }
+    for (int n = 0; n < g->npoly[i]; ++n) {
+      const int iv = g->itab_w_iv[(size_t)i * 7 + n] - 1;
+      if (iv >= 1 && iv < mva && g->lpv[iv] - g->lpw[i] > l) {
+        set_error("lve2 at W point " + std::to_string(i + 1) + " does not cover its closed V faces (lpv - lpw)");
+        return OLAMGPU_E_ARG;
+      }
+    }
+    lve2[i] = l;
+    nve2 = std::max(nve2, l);
+  }
+  y.nve2_max = nve2;
+  if (nve2 > 0) {
+    OG_CHECK(upload(y.lve2, lve2.data(), lve2.size(), s));
+    OG_CHECK(y.vm0.alloc((size_t)mwa * nve2 * 3));
+    OG_CUDA(cudaMemsetAsync(y.vm0.p, 0, y.vm0.bytes(), s));
+  }
   if (mza > 128) { set_error("prog_wrtv_rk supports mza <= 128"); return OLAMGPU_E_UNSUPPORTED; }
   if ((size_t)std::max(std::max(mwa, mva), mma) * mza >= (1ull << 31)) {
     set_error("prog_wrtv_rk supports grids with max(mwa, mva, mma) * mza < 2^31");
@@ -980,6 +1060,12 @@ int dyn_prog_wrtv_rk(int istp) {
   const bool rayleigh_th = o.rayf_cof && o.initial == 1;
   // with eddy diffusion the Rayleigh term on thil follows the eddy terms
   if (!rayleigh_th || y.eddy_on) sw.rayf_cof = nullptr;
+  if (y.nve2_max > 0 && d.nw_prog > 0) {
+    k_shaved_save<<<cdiv((size_t)d.nw_prog * y.nve2_max, 256), 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, y.lve2.p,
+                                                                             y.nve2_max, y.vxe.p, y.vye.p, y.vze.p,
+                                                                             tp.rho.p, y.vm0.p);
+    OG_LAUNCHED();
+  }
   { OG_PROF("setup_w", s); k_setup_w<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, sw); OG_LAUNCHED(); }
   {
     OG_PROF("setup_v", s);
@@ -1108,7 +1194,7 @@ int dyn_prog_wrtv_rk(int istp) {
     {
       OG_PROF("vel_t3d", s);
       k_vel_t3d<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, tp.wc.p, y.vc.p, y.wno2.p, y.ecv.p, y.vxe.p,
-                                    y.vye.p, y.vze.p);
+                                    y.vye.p, y.vze.p, shaved_args(y, tp, 1, dts));
       OG_LAUNCHED();
     }
     if (C.halo.on) {   // prog_wrtv_rk.f90:464-472
@@ -1192,7 +1278,8 @@ int dyn_diagvel_t3d() {
   Dyn& y = C.dy;
   if (d.nw_prog > 0) {
     k_vel_t3d<<<cdiv((size_t)d.nw_prog * d.mza, 256), 256, 0, s>>>(dynk(d), d.jtw_prog.p, d.nw_prog, C.tp.wc.p, y.vc.p,
-                                                                    y.wno2.p, y.ecv.p, y.vxe.p, y.vye.p, y.vze.p);
+                                                                    y.wno2.p, y.ecv.p, y.vxe.p, y.vye.p, y.vze.p,
+                                                                    shaved_args(y, C.tp, 0, 0.f));
     OG_LAUNCHED();
   }
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
@@ -1218,6 +1305,8 @@ void dyn_release() {
                         &y.m_sfv, &y.m_sin, &y.m_sout};
   for (auto* b : f) b->release();
   y.lpmmin.release();
+  y.lve2.release();
+  y.vm0.release();
   dyn_eddy_release();
   y = Dyn();
 }

@@ -264,6 +264,12 @@ struct Dyn {
   DevBuf<float> gx;              // gradient planes of the 4 fields
   DevBuf<float> div2d, fdivh, vort2d, fvorth, fvortl, vfact;
   DevBuf<int> lpmmin;
+  // prognostic shaved-cell method: lve2 of every W column and the start
+  // momentum of its lve2 lowest levels, (mwa, nve2_max, 3); none on grids
+  // where no column has a closed face (nve2_max = 0)
+  DevBuf<int> lve2;
+  DevBuf<float> vm0;
+  int nve2_max = 0;
   bool div_first = true, vort_first = true;
   // grid metrics of the dynamics
   DevBuf<float> arv, arw, volwi, volvi, wn, wno2, vn, ecv, gdz_wgtm, gdz_wgtp;

@@ -18,6 +18,8 @@
  *                          scalar_monot_limiter; centered_monot = .false.,
  *                          iorderv = 3)
  *   vel_t3d_hex            omodel/vel_t3d.f90:39-108
+ *   update_vxe_undrgnd     omodel/prog_wrtv_rk.f90:1558-1595 (shaved cells,
+ *                          with the start values of :202-211)
  *   divh_damp, vort_damp   omodel/vort_div_damp.f90:1-445
  *   laplacian2d/_m         omodel/grad_lib.f90:494-559
  *   tridiffo               outils/tridiag_lib.f90:10-36
@@ -28,7 +30,7 @@
  * Real literals that OLAM writes in default precision (e.g. fr = .70) keep
  * their single-precision value when promoted to real(8).
  * Not restated (off in every configuration this build runs): nudging,
- * shaved cells (lve2 > 0), the supercell test's thil_init offset, Lagrangian
+ * the supercell test's thil_init offset, Lagrangian
  * particle sums, the shallow-water test cases.
  */
 #include <algorithm>
@@ -776,6 +778,30 @@ static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
   std::vector<T> thl0, vxe0, vye0, vze0;   // start values of the limited fields (186-198)
   if (thil_monot) thl0.assign(s.thil, s.thil + wz);
   if (wind_monot) { vxe0.assign(s.vxe, s.vxe + wz); vye0.assign(s.vye, s.vye + wz); vze0.assign(s.vze, s.vze + wz); }
+  // prognostic shaved-cell method (202-211): the momentum of the levels of a
+  // column with closed V faces (lve2 of them from lpw up) at the step's start
+  const int* lve2 = X.g->lve2;
+  int nve2 = 0;
+  if (lve2)
+    for (int iw = 2; iw <= mwa; ++iw) {
+      nve2 = std::max(nve2, lve2[iw - 1]);
+      for (int jv = 1; jv <= G.npoly(iw); ++jv)
+        if (G.lpv(G.w_iv(iw, jv)) - G.lpw(iw) > lve2[iw - 1]) return OLAMGPU_E_ARG;   // a closed face not covered
+    }
+  const size_t nv2 = (size_t)std::max(nve2, 1);
+  std::vector<T> vm0(3 * nv2 * (size_t)mwa);
+  auto M0 = [&](int c, int ks, int iw) -> T& { return vm0[(((size_t)(iw - 1) * nv2) + ks - 1) * 3 + c]; };
+  if (nve2)
+    for (int j = 0; j < X.g->nw_prog; ++j) {
+      const int iw = X.g->jtw_prog[j];
+      for (int ks = 1; ks <= lve2[iw - 1]; ++ks) {
+        const int k = ks + G.lpw(iw) - 1;
+        const T rs = (T)F2(s.rho, k, iw);
+        M0(0, ks, iw) = F2(s.vxe, k, iw) * rs;
+        M0(1, ks, iw) = F2(s.vye, k, iw) * rs;
+        M0(2, ks, iw) = F2(s.vze, k, iw) * rs;
+      }
+    }
   // column setup (166-253)
   for (int j = 0; j < X.g->nw_prog; ++j) {
     int iw = X.g->jtw_prog[j];
@@ -1028,10 +1054,22 @@ static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
         F2(s.vc, k, iv) = (T)2.0 * v / (T)(F2(s.rho, k, iw1) + F2(s.rho, k, iw2));
       }
     }
-    // vel_t3d_hex (vel_t3d.f90:39-108), no shaved cells
+    // update_vxe_undrgnd (1558-1595): the prognosed velocities of the levels
+    // with closed faces, then vel_t3d_hex (vel_t3d.f90:39-108), whose closed
+    // faces take the normal component of those
     for (int j = 0; j < X.g->nw_prog; ++j) {
       int iw = X.g->jtw_prog[j];
       int ka = G.lpw(iw);
+      const int nsh = lve2 ? lve2[iw - 1] : 0;
+      std::vector<T> p1(3 * (size_t)std::max(nsh, 1));
+      for (int ks = 1; ks <= nsh; ++ks) {
+        const int k = ks + ka - 1;
+        const T rsi = (T)1 / (T)F2(s.rho, k, iw);
+        const T vt = (T)F2(X.g->volti, k, iw);
+        p1[(ks - 1) * 3 + 0] = (M0(0, ks, iw) + dts * (F2(vmxet_rk.data(), k, iw) * vt)) * rsi;
+        p1[(ks - 1) * 3 + 1] = (M0(1, ks, iw) + dts * (F2(vmyet_rk.data(), k, iw) * vt)) * rsi;
+        p1[(ks - 1) * 3 + 2] = (M0(2, ks, iw) + dts * (F2(vmzet_rk.data(), k, iw) * vt)) * rsi;
+      }
       for (int k = ka; k <= mza; ++k) {
         T wst = F2(s.wc, k - 1, iw) + F2(s.wc, k, iw);
         F2(s.vxe, k, iw) = wst * X.wnxo2[iw - 1];
@@ -1046,6 +1084,14 @@ static int prog_wrtv_rk(DynCtx<T>& X, const DynState<T>& s, int istp) {
           F2(s.vxe, k, iw) = F2(s.vxe, k, iw) + ex * F2(s.vc, k, iv);
           F2(s.vye, k, iw) = F2(s.vye, k, iw) + ey * F2(s.vc, k, iv);
           F2(s.vze, k, iw) = F2(s.vze, k, iw) + ez * F2(s.vc, k, iv);
+        }
+        for (int k = ka; k <= G.lpv(iv) - 1; ++k) {
+          const int ksw = k - ka + 1;
+          const T vcwall = X.vnx[iv - 1] * p1[(ksw - 1) * 3] + X.vny[iv - 1] * p1[(ksw - 1) * 3 + 1] +
+                           X.vnz[iv - 1] * p1[(ksw - 1) * 3 + 2];
+          F2(s.vxe, k, iw) = F2(s.vxe, k, iw) + ex * vcwall;
+          F2(s.vye, k, iw) = F2(s.vye, k, iw) + ey * vcwall;
+          F2(s.vze, k, iw) = F2(s.vze, k, iw) + ez * vcwall;
         }
       }
       for (int k = 1; k <= ka - 1; ++k) {

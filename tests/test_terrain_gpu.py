@@ -5,7 +5,8 @@ the reconstruction and the flux divergence drop faces and gradient terms
 level by level (the reference's loops start at lpv and lpw).  The tiled
 and plain forms are checked against the oracle, and against themselves
 with NaN below every floor (values the reference never reads); the tiled
-adjoint against the oracle's adjoint; prog_wrtv_rk's long step against
+adjoint against the oracle's adjoint; prog_wrtv_rk's long step (with the
+prognostic shaved-cell method of the columns beside higher ones) against
 the oracle and olamgpu_timestep against the single calls."""
 import copy
 
@@ -24,7 +25,8 @@ pytestmark = pytest.mark.gpu
 def terrain_grid(g0, hmax=4):
     """A copy of grid g0 with a mountain: lpw rises to 2 + hmax under it,
     a face's lpv is the higher floor of its two cells, an M point's lpm the
-    highest lpv of its three faces (omodel/hex_grid.f90:1446)."""
+    highest lpv of its three faces (omodel/hex_grid.f90:1446), a column's
+    lve2 the largest lpv - lpw of its faces (its shaved levels)."""
     g = copy.copy(g0)
     xyz = np.asarray(g.xew, dtype=np.float64).T
     rad = np.linalg.norm(xyz, axis=1)
@@ -39,6 +41,10 @@ def terrain_grid(g0, hmax=4):
     g.lpv[0] = 2
     g.lpm = np.max(g.lpv[g.itab_m_iv], axis=1).astype(np.int32)
     g.lpm[0] = 2
+    # shaved cells: the levels of a column with closed faces (hex_grid.f90:1927)
+    faces = np.arange(g.itab_w_iv.shape[1])[None, :] < g.npoly[:, None]
+    g.lve2 = np.where(faces, g.lpv[g.itab_w_iv] - lpw[:, None], 0).max(axis=1).clip(0).astype(np.int32)
+    g.lve2[0] = 0
     return g
 
 
@@ -68,6 +74,7 @@ def test_terrain_case_has_terrain():
     g, _ = terrain_case()
     assert (g.lpw[1:] > 2).sum() > 20 and (g.lpw[1:] == 2).sum() > 20
     assert g.lpw.max() >= 5
+    assert (g.lve2 > 0).sum() > 20
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(nrk_scal=3), dict(scal_order=3),
