@@ -80,7 +80,10 @@ typedef struct olamgpu_grid {
   const int*   itab_m_iw;
   const int*   itab_m_im;
 
-  /* lowest prognosed levels (mem_grid.f90:20-24) */
+  /* lowest prognosed levels (mem_grid.f90:20-24); lve2(iw), the number of
+   * levels from lpw(iw) up with closed V faces (the prognostic shaved-cell
+   * method of prog_wrtv_rk), must be at least lpv - lpw of every face of
+   * the column (OLAM's grid sets it to the largest); NULL reads as 0 */
   const int* lpw;  const int* lpv;  const int* lpm;  const int* lve2;
 
   /* 1-D vertical arrays (mza) */
