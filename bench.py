@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-long-step", action="store_true")
+    p.add_argument("--terrain", type=int, default=0,
+                   help="a step-topography mountain raising lpw by up to this many levels (0: flat)")
     p.add_argument("--long-step-only", action="store_true",
                    help="time only the long step (olamgpu_timestep) and print its object")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -128,13 +130,20 @@ def make_case(a):
     from olam_b200.synth.state import fast_lognormal_tracers, transport_state
     g = build_grid(a.nxp, stretched_levels(a.nlev, 100.0, 30000.0), seed=2)
     st = transport_state(g, a.dt, 0, seed=2)
+    if a.terrain > 0:
+        from olam_b200.synth.grid import with_terrain
+        g = with_terrain(g, a.terrain)
     tr = fast_lognormal_tracers(g, a.ntr, seed=2024, as_list=True)
     return g, st, tr
 
 
+def prognostic_cells(g):
+    """Cells the step updates: levels lpw..mza of every W column."""
+    return int((g.mza + 1 - g.lpw[1:].astype(np.int64)).sum())
+
+
 def cell_updates(g, ntr):
-    # prognostic cells: levels lpw..mza of every W column (lpw = 2 here)
-    return ntr * (g.mwa - 1) * (g.mza - 1)
+    return ntr * prognostic_cells(g)
 
 
 def bytes_per_launch(g, ntr, stage):
@@ -142,7 +151,7 @@ def bytes_per_launch(g, ntr, stage):
     12 B on stage 1 (read scp0 and sct, write) and 16 B on later stages (read
     scp, scp0, sct, write), plus 32 B per cell of shared winds, densities and
     volumes (vmasc 3 faces x 4, wmasc 4, rho 8, rho_old 4, volti 4)."""
-    cells = (g.mwa - 1) * (g.mza - 1)
+    cells = prognostic_cells(g)
     per_tr = 12 if stage == 1 else 16
     return cells * (ntr * per_tr + 32)
 
@@ -199,7 +208,8 @@ def dist_init(a):
 def workload_name(g, a):
     """The workload both arms report (the same string in both lines)."""
     return (f"scalar_transport_rk NXP={a.nxp} ({g.mwa - 1} columns), {a.nlev} levels, {a.ntr} tracers, "
-            f"RK{a.nrk}, horiz order {a.order}, iscal_monot {a.monot}, dt {a.dt} s")
+            f"RK{a.nrk}, horiz order {a.order}, iscal_monot {a.monot}, dt {a.dt} s"
+            + (f", terrain up to {a.terrain} levels" if a.terrain > 0 else ""))
 
 
 def run_reference(a):
@@ -291,7 +301,8 @@ def bench_long_step(g, tr, a, max_over_ranks):
     except (OSError, ValueError):
         pass
     peak = float(peaks.get("hbm_gbs") or 6650.0)
-    cw, cv = (g.mwa - 1) * (g.mza - 1), (g.mva - 1) * (g.mza - 1)   # above-ground W and V cells
+    cw = prognostic_cells(g)                                            # above-ground W and V cells
+    cv = int((g.mza + 1 - g.lpv[1:].astype(np.int64)).sum())
     # bytes each launch must move at least (every array element it reads or
     # writes once; stage-averaged for wrt_begs over the 3 RK stages)
     algo = {
@@ -461,7 +472,7 @@ def main():
         dev.profile(False, reset=True)
         adj_ms = max_over_ranks(aprof["adjoint"][0] / aprof["adjoint"][1])
         st_ms, st_n = aprof.get("adj_stage", (0.0, 0))
-        stage_bytes = (a.ntr * 24 + 128) * (g.mwa - 1) * (g.mza - 1)
+        stage_bytes = (a.ntr * 24 + 128) * prognostic_cells(g)
         adjoint = {
             "ms_per_step": adj_ms, "forward_ms_per_step": ms_step,
             "adjoint_over_forward": adj_ms / ms_step,

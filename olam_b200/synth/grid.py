@@ -709,3 +709,31 @@ def _adv_coefficients(g):
     g.yy0_vu = np.stack([dy1 * dy1, dy2 * dy2], axis=1).astype(F32)
     for arr in (g.xx0_v, g.xy0_v, g.yy0_v, g.xx0_vu, g.xy0_vu, g.yy0_vu):
         arr[0] = 0.0
+
+
+def with_terrain(g0, hmax=4, width=0.9):
+    """A copy of grid g0 with a step-topography mountain centred on W point
+    1: lpw rises to 2 + hmax (Fortran levels) within ``width`` radians of
+    it; a face's lpv is the higher floor of its two cells, an M point's lpm
+    the highest lpv of its three faces (omodel/hex_grid.f90:1446) and a
+    column's lve2 the largest lpv - lpw of its faces (hex_grid.f90:1927,
+    the shaved-cell levels).  The metric arrays stay those of g0."""
+    import copy
+    g = copy.copy(g0)
+    xyz = np.asarray(g.xew, dtype=np.float64).T
+    rad = np.linalg.norm(xyz, axis=1)
+    rad[rad == 0] = 1.0
+    top = xyz[1] / rad[1]
+    ang = np.arccos(np.clip(xyz @ top / rad, -1.0, 1.0))
+    lpw = 2 + np.floor(hmax * np.clip(1.0 - ang / width, 0.0, 1.0) ** 0.6).astype(np.int32)
+    lpw = np.minimum(lpw, g.mza - 2)
+    lpw[0] = 2
+    g.lpw = lpw.astype(np.int32)
+    g.lpv = np.maximum(lpw[g.itab_v_iw[:, 0]], lpw[g.itab_v_iw[:, 1]]).astype(np.int32)
+    g.lpv[0] = 2
+    g.lpm = np.max(g.lpv[g.itab_m_iv], axis=1).astype(np.int32)
+    g.lpm[0] = 2
+    faces = np.arange(g.itab_w_iv.shape[1])[None, :] < g.npoly[:, None]
+    g.lve2 = np.where(faces, g.lpv[g.itab_w_iv] - lpw[:, None], 0).max(axis=1).clip(0).astype(np.int32)
+    g.lve2[0] = 0
+    return g

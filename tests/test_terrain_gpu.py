@@ -8,8 +8,6 @@ with NaN below every floor (values the reference never reads); the tiled
 adjoint against the oracle's adjoint; prog_wrtv_rk's long step (with the
 prognostic shaved-cell method of the columns beside higher ones) against
 the oracle and olamgpu_timestep against the single calls."""
-import copy
-
 import numpy as np
 import pytest
 
@@ -23,29 +21,8 @@ pytestmark = pytest.mark.gpu
 
 
 def terrain_grid(g0, hmax=4):
-    """A copy of grid g0 with a mountain: lpw rises to 2 + hmax under it,
-    a face's lpv is the higher floor of its two cells, an M point's lpm the
-    highest lpv of its three faces (omodel/hex_grid.f90:1446), a column's
-    lve2 the largest lpv - lpw of its faces (its shaved levels)."""
-    g = copy.copy(g0)
-    xyz = np.asarray(g.xew, dtype=np.float64).T
-    rad = np.linalg.norm(xyz, axis=1)
-    rad[rad == 0] = 1.0
-    top = xyz[1] / rad[1]
-    ang = np.arccos(np.clip(xyz @ top / rad, -1.0, 1.0))
-    lpw = 2 + np.floor(hmax * np.clip(1.0 - ang / 0.9, 0.0, 1.0) ** 0.6).astype(np.int32)
-    lpw = np.minimum(lpw, g.mza - 2)
-    lpw[0] = 2
-    g.lpw = lpw.astype(np.int32)
-    g.lpv = np.maximum(lpw[g.itab_v_iw[:, 0]], lpw[g.itab_v_iw[:, 1]]).astype(np.int32)
-    g.lpv[0] = 2
-    g.lpm = np.max(g.lpv[g.itab_m_iv], axis=1).astype(np.int32)
-    g.lpm[0] = 2
-    # shaved cells: the levels of a column with closed faces (hex_grid.f90:1927)
-    faces = np.arange(g.itab_w_iv.shape[1])[None, :] < g.npoly[:, None]
-    g.lve2 = np.where(faces, g.lpv[g.itab_w_iv] - lpw[:, None], 0).max(axis=1).clip(0).astype(np.int32)
-    g.lve2[0] = 0
-    return g
+    from olam_b200.synth.grid import with_terrain
+    return with_terrain(g0, hmax)
 
 
 def terrain_case(nxp=6, nlev=12, ntr=6, hmax=4, **kw):
