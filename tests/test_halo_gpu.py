@@ -106,7 +106,7 @@ def test_halo_needs_the_unlimited_batched_step():
         _rank(g, st, opts, loc, _stages(g, st, 1800.0, 2), abi.TRANSPORT_PLAIN, 2)
 
 
-def _proc_main(rank, world, port, q):
+def _proc_main(rank, world, port, q, terrain=0):
     """One rank of a decomposed tracer step as its own process: its part of
     the grid through the library, the exchange hook moving the packed border
     columns over gloo (host-staged)."""
@@ -117,6 +117,9 @@ def _proc_main(rank, world, port, q):
         dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
                                 timeout=timedelta(seconds=120))
         g, st = small_case(nxp=8, nlev=12, ntr=6)
+        if terrain:
+            from olam_b200.synth.grid import with_terrain
+            g = with_terrain(g, terrain, width=2.0)
         opts = abi.make_opts(1800.0, nrk_scal=3)
         loc = decomp.local_grid(g, decomp.bisect(g, world), rank)
         calls = {"n": 0}
@@ -156,14 +159,20 @@ def _proc_main(rank, world, port, q):
         q.put((rank, repr(e), None, None))
 
 
-def test_two_processes_over_gloo():
+@pytest.mark.parametrize("terrain", [0, 4])
+def test_two_processes_over_gloo(terrain):
     # two ranks as two processes sharing the GPU: no kernel waits on the
     # other rank (each hook call follows a finished stage on the host), the
     # border columns move over gloo; together the ranks reproduce the
-    # one-domain step
+    # one-domain step (flat, and with a mountain across the ranks' border)
     import socket
     import torch.multiprocessing as mp
     g, st = small_case(nxp=8, nlev=12, ntr=6)
+    if terrain:
+        from olam_b200.synth.grid import with_terrain
+        g = with_terrain(g, terrain, width=2.0)
+        owner = decomp.bisect(g, 2)
+        assert all((g.lpw[1:][owner[1:] == r] > 2).sum() > 50 for r in range(2))
     opts = abi.make_opts(1800.0, nrk_scal=3)
     ref, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED)
     with socket.socket() as sk:
@@ -171,7 +180,7 @@ def test_two_processes_over_gloo():
         port = sk.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_proc_main, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_proc_main, args=(r, 2, port, q, terrain)) for r in range(2)]
     for p in procs:
         p.start()
     res = [q.get(timeout=600) for _ in range(2)]
