@@ -21,8 +21,8 @@
 // step (both stages and the adjoint read them).  With terrain a column's
 // faces, and the gradient terms across faces, below their lpv drop out (the
 // reference's loops start at lpv): k_weights leaves out the faces and takes
-// the slot weights of the level's terrain band; k_tile starts each column at
-// its own lpw.
+// the slot weights of the level's terrain band; k_tile sweeps a tile from
+// its lowest floor and stores each column from its own lpw up.
 //
 // k_tile: a block owns a tile of T = 16 NC consecutive prognostic columns
 // and a group of 64 tracers and sweeps the levels bottom to top.  While it
