@@ -156,13 +156,23 @@ def bytes_per_launch(g, ntr, stage):
     return cells * (ntr * per_tr + 32)
 
 
-def cpu_sample(g, st, tr, a, target_s, ntr_fixed=None):
-    """Time the oracle on a bounded tracer sample of the same workload.
-
-    The sample is the first n tracers for one long step, n chosen from a
-    one-tracer calibration so the timed run takes about ``target_s``."""
+def oracle_module():
+    """The CPU oracle (the checker and the CPU baseline), its -march=native
+    build made on this machine when the compiler allows."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
+    oracle_lib.use_native()
+    return oracle_lib
+
+
+def cpu_sample(g, st, tr, a, target_s, ntr_fixed=None, keep=False):
+    """Time the oracle on a bounded tracer sample of the same workload.
+
+    The sample is the first n tracers of ``tr`` (at most len(tr)) for one
+    long step, n chosen from a one-tracer calibration so the timed run takes
+    about ``target_s``.  With ``keep`` the result holds the oracle's output
+    (n, mwa, mza) under "out" (not printed)."""
+    oracle_lib = oracle_module()
     from olam_b200 import abi
     fg = abi.FortranGrid(g)
     opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
@@ -171,24 +181,99 @@ def cpu_sample(g, st, tr, a, target_s, ntr_fixed=None):
         pass
     s = S()
     s.__dict__.update(st.__dict__)
+    res = {}
 
     def run(n):
         sct = [np.zeros_like(tr[0]) for _ in range(n)]
         t0 = time.perf_counter()
-        oracle_lib.scalar_transport(fg, opts, tr[:n], sct, s)
-        return time.perf_counter() - t0
+        out = oracle_lib.scalar_transport(fg, opts, tr[:n], sct, s)
+        dt = time.perf_counter() - t0
+        if keep:
+            res["out"] = out
+        return dt
 
     if ntr_fixed is None:
         t1 = run(1)
-        n = int(max(1, min(a.ntr, round(target_s / max(t1, 1e-3)))))
+        n = int(max(1, min(len(tr), round(target_s / max(t1, 1e-3)))))
         t = run(n) if n > 1 else t1
     else:
-        n = ntr_fixed
+        n = min(ntr_fixed, len(tr))
         t = run(n)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": cell_updates(g, n) / t, "unit": "cell-updates/s", "cores": cores,
-            "kind": "port", "seconds": t, "ntr": n,
-            "sample": f"{n} of {a.ntr} tracers, one long step, NXP={a.nxp}, {a.nlev} levels"}
+    res.update({"value": cell_updates(g, n) / t, "unit": "cell-updates/s", "cores": cores,
+                "kind": "port", "seconds": t, "ntr": n, "library": oracle_lib._NAME,
+                "sample": f"{n} of {a.ntr} tracers, one long step, NXP={a.nxp}, {a.nlev} levels"})
+    return res
+
+
+def prognostic_mask(g):
+    """(mwa, mza) bool: the cells a step updates (levels lpw..mza of every
+    column but the dummy point)."""
+    k = np.arange(g.mza)[None, :]
+    m = k >= (g.lpw.astype(np.int64)[:, None] - 1)
+    m[0] = False
+    return m
+
+
+def field_errors(out, ref, mask):
+    """Normwise max relative error max|a - b| / max|b| and RMS relative
+    error sqrt(sum (a - b)^2 / sum b^2) over the masked cells."""
+    a = np.asarray(out, np.float64)[mask]
+    b = np.asarray(ref, np.float64)[mask]
+    d = a - b
+    den_max, den_rms = np.abs(b).max(), np.sqrt((b * b).sum())
+    return (float(np.abs(d).max() / den_max) if den_max > 0 else float(np.abs(d).max()),
+            float(np.sqrt((d * d).sum()) / den_rms) if den_rms > 0 else float(np.sqrt((d * d).sum())))
+
+
+def tracer_masses(g, rho, tracers):
+    """sum over the prognostic cells of rho * volt * scp per tracer, in
+    float64 on the GPU (the masses before a step, with rho_old)."""
+    import torch
+    w = np.where(prognostic_mask(g), np.asarray(rho, np.float64) * g.volt, 0.0)
+    wd = torch.from_numpy(w).cuda()
+    out = []
+    for t in tracers:
+        out.append(float((torch.from_numpy(t).cuda().double() * wd).sum().item()))
+    del wd
+    return np.array(out)
+
+
+def error_report(g, a, gpu_first, init_sample, st, cpu, mass_before, mass_after):
+    """The GPU's first step against the oracle on the sampled tracers (the
+    FP32 run of the CPU baseline, and an FP64 run on up to 4 of them), and
+    the global tracer mass drift of the GPU step for every tracer."""
+    oracle_lib = oracle_module()
+    from olam_b200 import abi
+    mask = prognostic_mask(g)
+    n32 = cpu["ntr"]
+    n64 = min(n32, 4)
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
+    ref64 = oracle_lib.scalar_transport(fg, opts, init_sample[:n64], [np.zeros_like(init_sample[0])] * n64,
+                                        st, fp64=True)
+    e32 = [field_errors(gpu_first[i], cpu["out"][i], mask) for i in range(n32)]
+    e64 = [field_errors(gpu_first[i], ref64[i], mask) for i in range(n64)]
+    s64 = [field_errors(cpu["out"][i], ref64[i], mask) for i in range(n64)]
+    w = np.where(mask, np.asarray(st.rho, np.float64) * g.volt, 0.0)
+    m64 = np.array([(ref64[i] * w).sum() for i in range(n64)])
+    live = mass_before > 0
+    drift = np.abs(mass_after[live] - mass_before[live]) / mass_before[live]
+    d64 = np.abs(m64 - mass_before[:n64]) / mass_before[:n64]
+    agg = lambda e: {"max_rel": max(x[0] for x in e), "rms_rel": max(x[1] for x in e)}  # noqa: E731
+    return {
+        "fields": "tracer scp after one step (prognostic cells), worst tracer of the sample",
+        "tracers_vs_fp32_oracle": dict(agg(e32), ntr=n32),
+        "tracers_vs_fp64_oracle": dict(agg(e64), ntr=n64),
+        "fp32_oracle_vs_fp64_oracle": dict(agg(s64), ntr=n64),
+        "mass_drift": {"definition": "|sum rho volt scp after - sum rho_old volt scp before| / before, "
+                                     "per tracer, over all tracers with mass",
+                       "gpu_max": float(drift.max()) if drift.size else None,
+                       "gpu_median": float(np.median(drift)) if drift.size else None,
+                       "fp64_oracle_max": float(d64.max()) if d64.size else None,
+                       "ntr": int(live.sum())},
+        "tolerance": 1e-5,
+    }
 
 
 def dist_init(a):
@@ -340,6 +425,11 @@ def main():
         return 0
     fg = abi.FortranGrid(g)
     opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
+    # the first tracers' initial values (the oracle's sample) and every
+    # tracer's mass, for the error report
+    report = rank == 0 and not a.no_cpu
+    init_sample = [t.copy() for t in tr[:min(a.ntr, 16)]] if report else []
+    mass_before = tracer_masses(g, st.rho_old, tr) if report else None
     hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)
     dev = OlamGpu(fg, opts, hs)
     var_p = tr                     # separately allocated, as OLAM's var_p
@@ -364,6 +454,15 @@ def main():
     dev.set_coherence(abi.RESIDENT)
     dev.sync_to_device(abi.F_ALL)
     dev.scalar_transport_rk(st.rho_old)          # uploads rho_old once
+    gpu_first, mass_after = None, None
+    if report:
+        # the first step's result for the error report (outside the timed region)
+        dev.sync_to_host(abi.F_SCALARS)
+        gpu_first = [t.copy() for t in var_p[:len(init_sample)]]
+        mass_after = np.zeros(a.ntr)
+        for i0 in range(0, a.ntr, 8):
+            ids = list(range(i0 + 1, min(a.ntr, i0 + 8) + 1))
+            mass_after[i0:i0 + len(ids)] = dev.mass_sums(ids)[1:]
     for _ in range(a.warmup):
         dev.scalar_transport_rk(None)
     torch.cuda.synchronize()
@@ -504,9 +603,11 @@ def main():
     if not a.no_long_step:
         long_step = bench_long_step(g, tr, a, max_over_ranks)
 
-    cpu = None
-    if rank == 0 and not a.no_cpu:
-        cpu = cpu_sample(g, st, tr, a, a.cpu_seconds)
+    cpu, errors = None, None
+    if report:
+        cpu = cpu_sample(g, st, init_sample, a, a.cpu_seconds, keep=True)
+        errors = error_report(g, a, gpu_first, init_sample, st, cpu, mass_before, mass_after)
+        cpu.pop("out")
 
     if rank == 0:
         line = {
@@ -531,6 +632,7 @@ def main():
             "adjoint": adjoint,
             "long_step": long_step,
             "cpu_baseline": cpu,
+            "errors": errors,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -27,7 +27,8 @@
 // k_tile: a block owns a tile of T = 16 NC consecutive prognostic columns
 // and a group of 64 tracers and sweeps the levels bottom to top.  While it
 // computes level kd from one shared-memory buffer it copies level kd+1 into
-// the other (16-byte cp.async): the tracer rows of the tile's two-ring
+// the other (TMA four-row gathers, cp.async.bulk.tensor tile::gather4, on
+// one mbarrier per buffer): the tracer rows of the tile's two-ring
 // neighbourhood U and the tile columns' weight records.  A half warp owns NC
 // columns, four tracers per lane (packed FFMA2); the column's own values at
 // kd-2 .. kd+3 and its scp0 / sct rows stay in registers across levels (one

@@ -22,10 +22,26 @@ def build():
     subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
 
 
+def use_native():
+    """Switch to the -march=native build of the oracle (same bits, faster),
+    built on this machine; keeps the portable build if that fails.  Call it
+    before the first oracle call.  Returns the library file in use."""
+    global _NAME
+    if _LIB is not None:
+        return _NAME
+    r = subprocess.run(["make", "-s", "-C", ORACLE_DIR, "native"], capture_output=True)
+    if r.returncode == 0 and os.path.exists(os.path.join(ORACLE_DIR, "liboracle_native.so")):
+        _NAME = "liboracle_native.so"
+    return _NAME
+
+
+_NAME = "liboracle.so"
+
+
 def lib():
     global _LIB
     if _LIB is None:
-        path = os.path.join(ORACLE_DIR, "liboracle.so")
+        path = os.path.join(ORACLE_DIR, _NAME)
         if not os.path.exists(path):
             build()
         _LIB = C.CDLL(path)
