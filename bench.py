@@ -228,7 +228,7 @@ def field_errors(out, ref, mask):
 
 def tracer_masses(g, rho, tracers):
     """sum over the prognostic cells of rho * volt * scp per tracer, in
-    float64 on the GPU (the masses before a step, with rho_old)."""
+    float64 on the GPU (before a step with rho_old, after it with rho)."""
     import torch
     w = np.where(prognostic_mask(g), np.asarray(rho, np.float64) * g.volt, 0.0)
     wd = torch.from_numpy(w).cuda()
@@ -459,10 +459,7 @@ def main():
         # the first step's result for the error report (outside the timed region)
         dev.sync_to_host(abi.F_SCALARS)
         gpu_first = [t.copy() for t in var_p[:len(init_sample)]]
-        mass_after = np.zeros(a.ntr)
-        for i0 in range(0, a.ntr, 8):
-            ids = list(range(i0 + 1, min(a.ntr, i0 + 8) + 1))
-            mass_after[i0:i0 + len(ids)] = dev.mass_sums(ids)[1:]
+        mass_after = tracer_masses(g, st.rho, var_p)
     for _ in range(a.warmup):
         dev.scalar_transport_rk(None)
     torch.cuda.synchronize()

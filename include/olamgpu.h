@@ -388,11 +388,14 @@ int olamgpu_timestep_diag(float* smax, double* sums);
  * during the call (a caller whose memory is fixed up front, or that records
  * its work into a CUDA graph).  The call allocates nothing: its scratch is
  * a fixed 64 MiB device array (gradient planes, V-face values, a zeroed
- * implicit fraction), so grids needing more (about NXP > 66 at 61 levels,
- * order 2) get OLAMGPU_E_ARG.  The first call on a device looks the scratch
- * up (make it before any stream capture); calls that overlap in time share
- * the scratch and race, so serialise them.  stream: a cudaStream_t, or NULL
- * for the library's stream. */
+ * implicit fraction): i2d * mwa * mza + mva * mza + mwa floats must fit in
+ * 16 Mi (i2d = 2 for order 2, 5 for order 3), i.e. up to NXP = 74 at order 2
+ * and NXP = 58 at order 3 with mza = 61; larger grids get OLAMGPU_E_ARG.
+ * The call must be made with the device of olamgpu_init current (else
+ * OLAMGPU_E_STATE).  The first call on a device looks the scratch up (make
+ * it before any stream capture; olamgpu_finalize forgets it); calls that
+ * overlap in time share the scratch and race, so serialise them.  stream: a
+ * cudaStream_t, or NULL for the library's stream. */
 int olamgpu_update_scalar_noalloc(const float* scp, const float* scp0, const float* sct,
                                   const float* rhos, const float* vmasc, const float* wmasc,
                                   float dtr, float* out, void* stream);

@@ -330,6 +330,7 @@ int olamgpu_finalize(void) {
   Context& C = ctx();
   if (C.stream) cudaStreamSynchronize(C.stream);
   release_all();
+  noalloc_forget();
   C.initialised = false;
   C.have_state = false;
   if (C.stream) { cudaStreamDestroy(C.stream); C.stream = nullptr; }

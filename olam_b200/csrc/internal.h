@@ -420,6 +420,8 @@ int dyn_diagvel_t3d();
 void prof_suspend(bool on);
 // adjoint of one unlimited step (transport_adjoint.cu)
 int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* const* lam_sct);
+// forgets the scratch address of olamgpu_update_scalar_noalloc (finalize)
+void noalloc_forget();
 int tracers_to_device(cudaStream_t s);   // host -> per-tracer mirrors (-> Q)
 int tracers_to_host(cudaStream_t s);     // (Q ->) per-tracer mirrors -> host
 int ensure_q(cudaStream_t s);            // per-tracer mirrors -> Q if needed

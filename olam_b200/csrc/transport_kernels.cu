@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "transport_kernels.cuh"
@@ -922,27 +923,38 @@ void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t 
 // per column -- lives in a fixed device array, so the call itself never
 // allocates device memory.
 // ---------------------------------------------------------------------------
-#define NOALLOC_SCRATCH_FLOATS (16u << 20)   // 64 MiB: about NXP <= 66 at 61 levels, order 2
+// Scratch need in floats: i2d * mwa * mza (gradient planes, i2d = 2 for
+// order 2 and 5 for order 3) + mva * mza (V-face values) + mwa (implicit
+// fraction).  On the icosahedral grid (mwa = 10 NXP^2 + 3, mva = 30 NXP^2 + 1)
+// with mza = 61 that fits up to NXP = 74 at order 2 and NXP = 58 at order 3.
+#define NOALLOC_SCRATCH_FLOATS (16u << 20)   // 64 MiB
 static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_SCRATCH_FLOATS];
 
-// address of g_noalloc_scratch on the current device, looked up on the first
-// call made with that device current
-static int noalloc_scratch(float** out) {
-  static float* ptrs[64] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) { set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e)); return OLAMGPU_E_CUDA; }
+// Address of g_noalloc_scratch per device, looked up by the first call made
+// with that device current and kept until olamgpu_finalize (after which an
+// application may reset the device).  Guarded by a mutex: calls may come
+// from several host threads.
+static std::mutex g_noalloc_mu;
+static float* g_noalloc_ptr[64] = {};
+
+void noalloc_forget() {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  for (float*& p : g_noalloc_ptr) p = nullptr;
+}
+
+static int noalloc_scratch(int dev, float** out) {
   if (dev < 0 || dev >= 64) { set_error("device ordinal above 63"); return OLAMGPU_E_UNSUPPORTED; }
-  if (!ptrs[dev]) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
     float* p = nullptr;
-    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_scratch);
+    const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       return OLAMGPU_E_CUDA;
     }
-    ptrs[dev] = p;
+    g_noalloc_ptr[dev] = p;
   }
-  *out = ptrs[dev];
+  *out = g_noalloc_ptr[dev];
   return OLAMGPU_OK;
 }
 
@@ -965,8 +977,17 @@ static int update_scalar_noalloc(const float* scp, const float* scp0, const floa
               " floats of scratch; the fixed scratch holds " + std::to_string(NOALLOC_SCRATCH_FLOATS));
     return OLAMGPU_E_ARG;
   }
+  // the grid tables live on the device olamgpu_init ran on: the call must
+  // be made with that device current
+  int dev = -1;
+  OG_CUDA(cudaGetDevice(&dev));
+  if (dev != C.device) {
+    set_error("update_scalar_noalloc: device " + std::to_string(dev) + " is current, the library was initialised on " +
+              std::to_string(C.device));
+    return OLAMGPU_E_STATE;
+  }
   float* scr = nullptr;
-  OG_CHECK(noalloc_scratch(&scr));
+  OG_CHECK(noalloc_scratch(dev, &scr));
   float* gx = scr;
   float* upv = scr + n_gx;
   float* ff = upv + n_upv;

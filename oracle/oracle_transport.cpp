@@ -20,6 +20,7 @@
 #include <cstring>
 
 #include "oracle_common.h"
+#include "oracle_dual.h"
 
 namespace oracle {
 
@@ -372,7 +373,7 @@ static void update_scalar_monot(const TransportCtx<T>& C, T* scp, const T* scp0,
       T rscp_low = s0c[k - 1] * F2(rhos, k, iw) + dtr * vt * fl[k];
       T flux_in = fmax_(dtrp * vt * fin[k], eps0);
       T flux_out = fmin_(dtrp * vt * fout[k], -eps0);
-      T epsr = eps1 * std::fabs(rscp_low);
+      T epsr = eps1 * abs_(rscp_low);
       T sc_in = fmax_(smax[k] - (rscp_low + epsr) - eps0, (T)0);
       T sc_out = fmin_(smin[k] - (rscp_low - epsr) + eps0, (T)0);
       scale_inout[(size_t)(iw - 1) * mza + k - 1] =
@@ -735,6 +736,35 @@ static int prepare_step(const GridT<T>& G, const olamgpu_grid* g, const olamgpu_
   return OLAMGPU_OK;
 }
 
+/* implicit vertical transport of one stage (scalar_transport_rk.F90:347-375) */
+template <class T>
+static void implicit_step(const GridT<T>& G, const StepCoef<T>& SC, int istage, T dtr, T* scp, const T* scp0) {
+  const int mza = G.mza, nrk = SC.nrk;
+  const size_t plane = (size_t)mza * G.mwa;
+  const auto& I = SC.imp[istage - 1];
+  const int nn = (int)I.iw.size();
+#pragma omp parallel for schedule(static)
+  for (int jj = 0; jj < nn; ++jj) {
+    int iw = I.iw[jj];
+    int kb = G.lpw(iw);
+    std::vector<T> dscp0(mza + 1, 0), delex(mza + 1, 0), del(mza + 1, 0);
+    dscp0[mza] = 0;
+    dscp0[kb - 1] = 0;
+    for (int k = kb; k <= mza - 1; ++k) dscp0[k] = F2(scp0, k + 1, iw) - F2(scp0, k, iw);
+    T ffv = SC.ff_implic[(size_t)(iw - 1) * nrk + istage - 1];
+    for (int k = kb; k <= mza; ++k) {
+      T c1 = ffv * dtr * G.volti_(k, iw) / SC.rhos[(size_t)(istage - 1) * plane + (size_t)(iw - 1) * mza + k - 1];
+      delex[k] = F2(scp, k, iw) - F2(scp0, k, iw) -
+                 c1 * (fmin_(F2(SC.wmasc.data(), k, iw), (T)0.) * dscp0[k] +
+                       fmax_(F2(SC.wmasc.data(), k - 1, iw), (T)0.) * dscp0[k - 1]);
+    }
+    tridif_fini(kb, mza, &I.b1[(size_t)jj * (mza + 1)], &I.b2[(size_t)jj * (mza + 1)],
+                &I.b3[(size_t)jj * (mza + 1)], delex.data(), del.data());
+    for (int k = kb; k <= mza; ++k) F2(scp, k, iw) = F2(scp0, k, iw) + del[k];
+    for (int k = 2; k <= kb - 1; ++k) F2(scp, k, iw) = F2(scp, kb, iw);
+  }
+}
+
 /* scalar_transport_rk (scalar_transport_rk.F90:30-385) */
 template <class T>
 static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
@@ -758,7 +788,6 @@ static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int
   const std::vector<T>& ff_implic = SC.ff_implic;
   const std::vector<T>& rhos = SC.rhos;
   const std::vector<int>& kwtop = SC.kwtop;
-  auto& imp = SC.imp;
   const size_t plane = (size_t)mza * mwa;
   if (ff_out)
     for (size_t i = 0; i < ff_implic.size(); ++i) ff_out[i] = (float)ff_implic[i];
@@ -809,33 +838,292 @@ static int scalar_transport_rk(const olamgpu_grid* g, const olamgpu_opts* o, int
       } else {
         update_scalar(C, scp, scp0.data(), sct, rhos_nrk, dtr, iorder, istage);
       }
-      // implicit vertical transport (347-375)
-      auto& I = imp[istage - 1];
-      const int nn = (int)I.iw.size();
-#pragma omp parallel for schedule(static)
-      for (int jj = 0; jj < nn; ++jj) {
-        int iw = I.iw[jj];
-        int kb = G.lpw(iw);
-        std::vector<T> dscp0(mza + 1, 0), delex(mza + 1, 0), del(mza + 1, 0);
-        dscp0[mza] = 0;
-        dscp0[kb - 1] = 0;
-        for (int k = kb; k <= mza - 1; ++k) dscp0[k] = F2(scp0.data(), k + 1, iw) - F2(scp0.data(), k, iw);
-        T ffv = ff_implic[(size_t)(iw - 1) * nrk + istage - 1];
-        for (int k = kb; k <= mza; ++k) {
-          T c1 = ffv * dtr * G.volti_(k, iw) /
-                 rhos[(size_t)(istage - 1) * plane + (size_t)(iw - 1) * mza + k - 1];
-          delex[k] = F2(scp, k, iw) - F2(scp0.data(), k, iw) -
-                     c1 * (fmin_(F2(wmasc.data(), k, iw), (T)0.) * dscp0[k] +
-                           fmax_(F2(wmasc.data(), k - 1, iw), (T)0.) * dscp0[k - 1]);
-        }
-        tridif_fini(kb, mza, &I.b1[(size_t)jj * (mza + 1)], &I.b2[(size_t)jj * (mza + 1)],
-                    &I.b3[(size_t)jj * (mza + 1)], delex.data(), del.data());
-        for (int k = kb; k <= mza; ++k) F2(scp, k, iw) = F2(scp0.data(), k, iw) + del[k];
-        for (int k = 2; k <= kb - 1; ++k) F2(scp, k, iw) = F2(scp, kb, iw);
-      }
+      implicit_step(G, SC, istage, dtr, scp, scp0.data());
     }
   }
   return OLAMGPU_OK;
+}
+
+/* The positive-definite last stage (update_scalar_pd,
+ * scalar_transport_rk.F90:1085-1472) with every intermediate kept, for its
+ * adjoint: the same arithmetic as update_scalar_pd above, in the same
+ * order, on the stage input S and the pre-updated scp0' (S0). */
+template <class T>
+struct PdRecord {
+  std::vector<T> gx, upv_low, hiv, sfv;             // faces: (mza, mva); gx: gradient planes
+  std::vector<T> upw_low, hiw, sfw;                  // columns: (mza + 1) per W point, index k
+  std::vector<T> rscp, fo_raw, fo, sc_raw, sc, den, scale;   // cells (mza, mwa)
+};
+
+template <class T>
+static void pd_record(const TransportCtx<T>& C, const T* S, const T* S0, const T* rhos, T dtr, int iorderh,
+                      int istage, PdRecord<T>& R) {
+  const GridT<T>& G = C.G;
+  const int mza = G.mza, mwa = G.mwa, mva = G.mva;
+  const int i2d = iorderh == 2 ? 2 : (iorderh == 3 ? 5 : 0);
+  const size_t plane = (size_t)mza * mwa, cols = (size_t)(mza + 1) * (mwa + 1);
+  R.gx.assign(plane * (i2d > 0 ? i2d : 1), (T)0);
+  R.upv_low.assign((size_t)mza * mva, (T)0); R.hiv = R.upv_low; R.sfv = R.upv_low;
+  R.upw_low.assign(cols, (T)0); R.hiw = R.upw_low; R.sfw = R.upw_low;
+  R.rscp.assign(plane, (T)0); R.fo_raw = R.rscp; R.fo = R.rscp; R.sc_raw = R.rscp; R.sc = R.rscp;
+  R.den = R.rscp; R.scale = R.rscp;
+  const T* vmasc = C.vmasc.data();
+  const T* wmasc = C.wmasc.data();
+  const T eps0 = (T)kEps0, onep = (T)1.0 + (T)kEps1, onem = (T)1.0 - (T)kEps1;
+  if (iorderh > 1) gradients(G, S, iorderh, true, R.gx);
+  vflux_hilo(C, S, S0, R.gx, iorderh, false, true, R.upv_low, R.hiv, R.sfv);
+  for (int j = 0; j < G.g->nw_prog; ++j) {
+    const int iw = G.g->jtw_prog[j];
+    const T fimpl = C.ff(istage, iw);
+    const T mdtrp = -onep * dtr;
+    const int kb = G.lpw(iw);
+    const T fexpl = (T)1. - fimpl;
+    T* upw = &R.upw_low[(size_t)iw * (mza + 1)];   // upw[k], k = kb-1 .. mza
+    T* hiw = &R.hiw[(size_t)iw * (mza + 1)];
+    T* sfw = &R.sfw[(size_t)iw * (mza + 1)];
+    std::vector<T> scpb(mza), scpt(mza), fl(mza + 1, (T)0), fout(mza + 1, (T)0);
+    const T* s0c = S0 + (size_t)(iw - 1) * mza;
+    const T* col = S + (size_t)(iw - 1) * mza;
+    upw[kb - 1] = col[kb - 1];
+    upw[mza] = col[mza - 1];
+    for (int k = kb; k <= mza - 1; ++k) {
+      upw[k] = s0c[k - 1];
+      if (F2(wmasc, k, iw) < (T)0) upw[k] = s0c[k];
+    }
+    grad_z_quadratic(G, iw, col, scpb.data(), scpt.data(), 0, 0, true);
+    sfw[kb - 1] = 0;
+    sfw[mza] = 0;
+    for (int k = kb; k <= mza - 1; ++k) {
+      hiw[k] = scpt[k - 1];
+      if (F2(wmasc, k, iw) < (T)0) hiw[k] = scpb[k];
+      hiw[k] = hiw[k] - upw[k];
+      sfw[k] = fexpl * F2(wmasc, k, iw) * hiw[k];
+    }
+    for (int jv = 1; jv <= G.npoly(iw); ++jv) {
+      const int iv = G.w_iv(iw, jv);
+      const T d = G.w_dirv(iw, jv);
+      for (int k = G.lpv(iv); k <= mza; ++k) {
+        fl[k] = fl[k] + d * F2(vmasc, k, iv) * (F2(R.upv_low.data(), k, iv) - s0c[k - 1]);
+        fout[k] = fout[k] + fmin_(d * F2(R.sfv.data(), k, iv), (T)0);
+      }
+    }
+    for (int k = kb; k <= mza; ++k) {
+      if (fimpl > (T).001)
+        fl[k] = fl[k] + fexpl * (F2(wmasc, k - 1, iw) * (upw[k - 1] - s0c[k - 1])
+                                 - F2(wmasc, k, iw) * (upw[k] - s0c[k - 1]))
+                + fimpl * s0c[k - 1] * (F2(wmasc, k, iw) - F2(wmasc, k - 1, iw));
+      else
+        fl[k] = fl[k] + F2(wmasc, k - 1, iw) * (upw[k - 1] - s0c[k - 1])
+                - F2(wmasc, k, iw) * (upw[k] - s0c[k - 1]);
+      fout[k] = fout[k] + fmin_(sfw[k - 1], (T)0) - fmax_(sfw[k], (T)0);
+      const size_t x = (size_t)(iw - 1) * mza + k - 1;
+      R.rscp[x] = s0c[k - 1] * F2(rhos, k, iw) + dtr * G.volti_(k, iw) * fl[k];
+      R.fo_raw[x] = mdtrp * G.volti_(k, iw) * fout[k];
+      R.fo[x] = fmax_(R.fo_raw[x], eps0);
+      R.sc_raw[x] = onem * R.rscp[x] - eps0;
+      R.sc[x] = fmax_(R.sc_raw[x], (T)0);
+      R.den[x] = fmax_(R.fo[x], (T)0.01 * R.sc[x]);
+      R.scale[x] = fmin_((T)1., R.sc[x] / R.den[x]);
+    }
+  }
+}
+
+/* Transpose of the positive-definite last stage at the recorded forward
+ * state, branch by branch: every min / max / sign test takes the side the
+ * forward took (the limiter's active masks), so this is the transpose of
+ * the stage's Jacobian there.  L: adjoint of the stage output (below-ground
+ * levels already folded); adds the adjoint of the stage input S to Lin and
+ * of S0 (scp0') to L0p. */
+template <class T>
+static void pd_stage_adjoint(const TransportCtx<T>& C, const PdRecord<T>& R, const T* S0, const T* rhos, T dtr,
+                             int iorderh, int istage, const T* L, T* Lin, T* L0p) {
+  const GridT<T>& G = C.G;
+  const int mza = G.mza, mwa = G.mwa, mva = G.mva;
+  const size_t plane = (size_t)mza * mwa;
+  const int np2d = iorderh == 2 ? 2 : 5;
+  const T* vm = C.vmasc.data();
+  const T* wm = C.wmasc.data();
+  const T onep = (T)1.0 + (T)kEps1, onem = (T)1.0 - (T)kEps1, eps0 = (T)kEps0;
+  std::vector<T> Lupv((size_t)mza * mva, (T)0), Lupv_low((size_t)mza * mva, (T)0), Lhiv((size_t)mza * mva, (T)0),
+      Lsfv((size_t)mza * mva, (T)0), Lscale(plane, (T)0), Lg(plane * np2d, (T)0);
+  const size_t cw = (size_t)(mza + 1);
+  std::vector<T> Lupw(cw * (mwa + 1), (T)0), Lupw_low(cw * (mwa + 1), (T)0), Lhiw(cw * (mwa + 1), (T)0),
+      Lsfw(cw * (mwa + 1), (T)0);
+  auto scale_at = [&](int k, int iw) { return R.scale[(size_t)(iw - 1) * mza + k - 1]; };
+  // scalar_tend_pd: out = s0 + dtr volti fluxdiv / rhos
+  for (int j = 0; j < G.g->nw_prog; ++j) {
+    const int iw = G.g->jtw_prog[j], kb = G.lpw(iw);
+    const T fimpl = C.ff(istage, iw);
+    const T fe = fimpl > (T).001 ? (T)1. - fimpl : (T)1.;
+    T* lupw = &Lupw[(size_t)iw * cw];
+    for (int k = kb; k <= mza; ++k) {
+      const T lk = F2(L, k, iw);
+      const T mu = lk * dtr * G.volti_(k, iw) / F2(rhos, k, iw);
+      F2(L0p, k, iw) += lk;
+      for (int jv = 1; jv <= G.npoly(iw); ++jv) {
+        const int iv = G.w_iv(iw, jv);
+        if (k < G.lpv(iv)) continue;
+        const T a = mu * G.w_dirv(iw, jv) * F2(vm, k, iv);
+        F2(Lupv.data(), k, iv) += a;
+        F2(L0p, k, iw) -= a;
+      }
+      lupw[k - 1] += mu * fe * F2(wm, k - 1, iw);
+      lupw[k] -= mu * fe * F2(wm, k, iw);
+      F2(L0p, k, iw) -= mu * fe * (F2(wm, k - 1, iw) - F2(wm, k, iw));
+    }
+  }
+  // vertical faces: upw = upw_low + hiw * scale(k or k+1)
+  for (int j = 0; j < G.g->nw_prog; ++j) {
+    const int iw = G.g->jtw_prog[j], kb = G.lpw(iw);
+    const T* lupw = &Lupw[(size_t)iw * cw];
+    T* lul = &Lupw_low[(size_t)iw * cw];
+    T* lhw = &Lhiw[(size_t)iw * cw];
+    const T* hiw = &R.hiw[(size_t)iw * cw];
+    const T* sfw = &R.sfw[(size_t)iw * cw];
+    lul[kb - 1] += lupw[kb - 1];   // the boundary faces carry scp(kb), scp(mza) unscaled
+    lul[mza] += lupw[mza];
+    for (int k = kb; k <= mza - 1; ++k) {
+      const int ks = sfw[k] < (T)0 ? k + 1 : k;
+      lul[k] += lupw[k];
+      lhw[k] += lupw[k] * scale_at(ks, iw);
+      Lscale[(size_t)(iw - 1) * mza + ks - 1] += lupw[k] * hiw[k];
+    }
+  }
+  // horizontal faces: upv = upv_low + hiv * scale(iw1, or iw2 where sfluxvh < 0)
+  for (int j = 0; j < G.g->nv_wadj; ++j) {
+    const int iv = G.g->jtv_wadj[j];
+    const int iw1 = G.v_iw(iv, 1), iw2 = G.v_iw(iv, 2);
+    for (int k = G.lpv(iv); k <= mza; ++k) {
+      const T a = F2(Lupv.data(), k, iv);
+      const int ws = F2(R.sfv.data(), k, iv) < (T)0 ? iw2 : iw1;
+      F2(Lupv_low.data(), k, iv) += a;
+      F2(Lhiv.data(), k, iv) += a * scale_at(k, ws);
+      Lscale[(size_t)(ws - 1) * mza + k - 1] += a * F2(R.hiv.data(), k, iv);
+    }
+  }
+  // the scale factors: scale = min(1, sc / max(fo, 0.01 sc)), sc = max(onem rscp - eps0, 0),
+  // fo = max(mdtrp volti fout, eps0), rscp = s0 rhos + dtr volti fl
+  std::vector<T> Lfl(plane, (T)0), Lfout(plane, (T)0);
+  for (int j = 0; j < G.g->nw_prog; ++j) {
+    const int iw = G.g->jtw_prog[j], kb = G.lpw(iw);
+    for (int k = kb; k <= mza; ++k) {
+      const size_t x = (size_t)(iw - 1) * mza + k - 1;
+      const T ls = Lscale[x];
+      const T ratio = R.sc[x] / R.den[x];
+      if (ls == (T)0 || (T)1. < ratio) continue;   // min took 1: no dependence
+      T lsc = ls / R.den[x];
+      const T lden = -ls * R.sc[x] / (R.den[x] * R.den[x]);
+      T lfo = 0;
+      if (R.fo[x] > (T)0.01 * R.sc[x]) lfo = lden;
+      else lsc += (T)0.01 * lden;
+      if (R.fo_raw[x] > eps0) Lfout[x] += lfo * (-onep * dtr) * G.volti_(k, iw);
+      if (R.sc_raw[x] > (T)0) {
+        const T lr = onem * lsc;
+        F2(L0p, k, iw) += lr * F2(rhos, k, iw);
+        Lfl[x] += lr * dtr * G.volti_(k, iw);
+      }
+    }
+  }
+  // fout = sum_f min(dirv sfluxvh, 0) + min(sfw(k-1), 0) - max(sfw(k), 0);
+  // fl = sum_f dirv vm (upv_low - s0) + the low-order vertical flux
+  for (int j = 0; j < G.g->nw_prog; ++j) {
+    const int iw = G.g->jtw_prog[j], kb = G.lpw(iw);
+    const T fimpl = C.ff(istage, iw);
+    const T fexpl = (T)1. - fimpl;
+    const bool imp = fimpl > (T).001;
+    const T fe = imp ? fexpl : (T)1.;
+    const T* sfw = &R.sfw[(size_t)iw * cw];
+    T* lsw = &Lsfw[(size_t)iw * cw];
+    T* lul = &Lupw_low[(size_t)iw * cw];
+    for (int k = kb; k <= mza; ++k) {
+      const size_t x = (size_t)(iw - 1) * mza + k - 1;
+      const T lo = Lfout[x], lf = Lfl[x];
+      for (int jv = 1; jv <= G.npoly(iw); ++jv) {
+        const int iv = G.w_iv(iw, jv);
+        if (k < G.lpv(iv)) continue;
+        const T d = G.w_dirv(iw, jv);
+        if (d * F2(R.sfv.data(), k, iv) < (T)0) F2(Lsfv.data(), k, iv) += d * lo;
+        const T a = lf * d * F2(vm, k, iv);
+        F2(Lupv_low.data(), k, iv) += a;
+        F2(L0p, k, iw) -= a;
+      }
+      if (sfw[k - 1] < (T)0) lsw[k - 1] += lo;
+      if (sfw[k] > (T)0) lsw[k] -= lo;
+      lul[k - 1] += lf * fe * F2(wm, k - 1, iw);
+      lul[k] -= lf * fe * F2(wm, k, iw);
+      F2(L0p, k, iw) -= lf * fe * (F2(wm, k - 1, iw) - F2(wm, k, iw));
+      if (imp) F2(L0p, k, iw) += lf * fimpl * (F2(wm, k, iw) - F2(wm, k - 1, iw));
+    }
+  }
+  // sfw = fexpl wm hiw; hiw = (scpb(k+1) or scpt(k)) - upw_low; upw_low from s0
+  // (interior faces) or S (the boundary faces); scpb / scpt of grad_z_quadratic(S)
+  for (int j = 0; j < G.g->nw_prog; ++j) {
+    const int iw = G.g->jtw_prog[j], kb = G.lpw(iw);
+    const T fexpl = (T)1. - C.ff(istage, iw);
+    T* lsw = &Lsfw[(size_t)iw * cw];
+    T* lhw = &Lhiw[(size_t)iw * cw];
+    T* lul = &Lupw_low[(size_t)iw * cw];
+    std::vector<T> Lb(mza + 1, (T)0), Lt(mza + 1, (T)0), Lds(mza + 1, (T)0);
+    for (int k = kb; k <= mza - 1; ++k) {
+      lhw[k] += fexpl * F2(wm, k, iw) * lsw[k];
+      if (F2(wm, k, iw) < (T)0) Lb[k + 1] += lhw[k];
+      else Lt[k] += lhw[k];
+      lul[k] -= lhw[k];
+      if (F2(wm, k, iw) < (T)0) F2(L0p, k + 1, iw) += lul[k];
+      else F2(L0p, k, iw) += lul[k];
+    }
+    F2(Lin, kb, iw) += lul[kb - 1];
+    F2(Lin, mza, iw) += lul[mza];
+    for (int k = kb; k <= mza; ++k) {
+      F2(Lin, k, iw) += Lb[k] + Lt[k];
+      Lds[k] += Lb[k] * G.aw(G.a_w, k, 1, 1) + Lt[k] * G.aw(G.a_w, k, 1, 2);
+      Lds[k - 1] += Lb[k] * G.aw(G.a_w, k, 2, 1) + Lt[k] * G.aw(G.a_w, k, 2, 2);
+    }
+    for (int k = kb; k <= mza - 1; ++k) {
+      F2(Lin, k + 1, iw) += Lds[k];
+      F2(Lin, k, iw) -= Lds[k];
+    }
+  }
+  // faces: sfluxvh = vm hiv; hiv = side value(upwind side) - s0(upwind cell); upv_low = s0(upwind cell)
+  for (int j = 0; j < G.g->nv_wadj; ++j) {
+    const int iv = G.g->jtv_wadj[j];
+    for (int k = G.lpv(iv); k <= mza; ++k) {
+      const T vmk = F2(vm, k, iv);
+      const int s = vmk < (T)0 ? 2 : 1;
+      const int iws = G.v_iw(iv, s);
+      const T lh = F2(Lhiv.data(), k, iv) + vmk * F2(Lsfv.data(), k, iv);
+      F2(L0p, k, iws) += F2(Lupv_low.data(), k, iv) - lh;
+      if (lh == (T)0) continue;
+      const size_t x = (size_t)(iws - 1) * mza + k - 1;
+      Lin[x] += lh;
+      if (iorderh == 1) continue;
+      Lg[x] += G.v2(G.dxps, s, iv) * lh;
+      Lg[plane + x] += G.v2(G.dyps, s, iv) * lh;
+      if (iorderh == 3) {
+        Lg[2 * plane + x] += G.v2(G.xx0_v, s, iv) * lh;
+        Lg[3 * plane + x] += G.v2(G.xy0_v, s, iv) * lh;
+        Lg[4 * plane + x] += G.v2(G.yy0_v, s, iv) * lh;
+      }
+    }
+  }
+  // grad_t2d[_quadratic] of S
+  if (iorderh > 1)
+    for (int j = 0; j < G.g->nw_prog; ++j) {
+      const int iw = G.g->jtw_prog[j];
+      for (int nn = 1; nn <= G.npoly(iw); ++nn) {
+        const int iwn = G.w_iw(iw, nn), ivn = G.w_iv(iw, nn);
+        T c[5];
+        if (iorderh == 2) { c[0] = G.gxps_coef(nn, iw); c[1] = G.gyps_coef(nn, iw); }
+        else for (int m = 0; m < 5; ++m) c[m] = G.xyh(G.xy_h, m + 1, nn, iw);
+        for (int k = G.lpv(ivn); k <= mza; ++k) {
+          const size_t x = (size_t)(iw - 1) * mza + k - 1;
+          T t = 0;
+          for (int m = 0; m < np2d; ++m) t += c[m] * Lg[m * plane + x];
+          F2(Lin, k, iwn) += t;
+          Lin[x] -= t;
+        }
+      }
+    }
 }
 
 /* Adjoint of scalar_transport_rk for one long step with the winds and
@@ -849,8 +1137,12 @@ template <class T>
 static int scalar_transport_rk_adjoint(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
                                        T* const* lam_list, T* const* lsct_list, const float* vmasc_f,
                                        const float* wmasc_f, const double* rho, const float* rho_old_f,
-                                       const float* wc) {
-  if (o->iscal_monot != 0) return OLAMGPU_E_UNSUPPORTED;
+                                       const float* wc, const T* const* scp_fwd = nullptr,
+                                       const T* const* sct_fwd = nullptr, const int* pdef = nullptr) {
+  if (o->iscal_monot == 1) return OLAMGPU_E_UNSUPPORTED;
+  if (o->iscal_monot == 2 && pdef && (!scp_fwd || !sct_fwd))
+    for (int n = 0; n < nscal; ++n)
+      if (pdef[n]) return OLAMGPU_E_ARG;   // the limited stage needs the forward's inputs
   GridT<T> G(g);
   const int mza = g->mza, mwa = g->mwa, mva = g->mva;
   const int iorder = o->scal_horiz_adv_order;
@@ -866,11 +1158,34 @@ static int scalar_transport_rk_adjoint(const olamgpu_grid* g, const olamgpu_opts
   const T* rhos_nrk = SC.rhos.data() + (size_t)(nrk - 1) * plane;
   std::vector<char> prog(mwa + 1, 0);
   for (int j = 0; j < g->nw_prog; ++j) prog[g->jtw_prog[j]] = 1;
+  TransportCtx<T> C{G, mza, mwa, mva, SC.vmasc, SC.wmasc, SC.ff_implic, nrk};
 
   for (int n = 0; n < nscal; ++n) {
     T* lam = lam_list[n];
     T* ls = lsct_list[n];
     std::fill(ls, ls + plane, (T)0);
+    // positive-definite last stage: recompute the forward to it and record
+    // the stage's intermediates (its input, scp0' and the limiter's branches)
+    const bool pdn = o->iscal_monot == 2 && pdef && pdef[n];
+    PdRecord<T> R;
+    std::vector<T> S0p, Lp;
+    if (pdn) {
+      std::vector<T> sf(scp_fwd[n], scp_fwd[n] + plane), s0(sf), st(sct_fwd[n], sct_fwd[n] + plane);
+      for (int istage = 1; istage < nrk; ++istage) {
+        update_scalar(C, sf.data(), s0.data(), st.data(), rhos_nrk, SC.dtlr[istage - 1], iorder, istage);
+        implicit_step(G, SC, istage, SC.dtlr[istage - 1], sf.data(), s0.data());
+      }
+      S0p = s0;
+      const T dtr = SC.dtlr[nrk - 1];
+      for (int j = 0; j < g->nw_wadj; ++j) {
+        const int iw = g->jtw_wadj[j], kb = G.lpw(iw);
+        for (int k = kb; k <= mza; ++k)
+          F2(S0p.data(), k, iw) = F2(S0p.data(), k, iw) + dtr * F2(st.data(), k, iw) / F2(SC.rho_old.data(), k, iw);
+        for (int k = 2; k <= kb - 1; ++k) F2(S0p.data(), k, iw) = F2(S0p.data(), kb, iw);
+      }
+      pd_record(C, sf.data(), S0p.data(), rhos_nrk, dtr, iorder, nrk, R);
+      Lp.assign(plane, (T)0);
+    }
     std::vector<T> L(lam, lam + plane), L0(plane, (T)0), Lin(plane), Lupv((size_t)mza * mva),
         Lg(plane * np2d);
     // columns outside jtw_prog keep their values through the step
@@ -880,6 +1195,9 @@ static int scalar_transport_rk_adjoint(const olamgpu_grid* g, const olamgpu_opts
 
     for (int istage = nrk; istage >= 1; --istage) {
       const T dtr = SC.dtlr[istage - 1];
+      const bool pd_stage = pdn && istage == nrk;
+      // the stage's s0: scp0, or scp0' on the positive-definite stage
+      T* L0s = pd_stage ? Lp.data() : L0.data();
       // ---- implicit columns: out' = s0 + T^-1 (out - s0 - G s0)
       auto& I = SC.imp[istage - 1];
       for (size_t jj = 0; jj < I.iw.size(); ++jj) {
@@ -895,16 +1213,16 @@ static int scalar_transport_rk_adjoint(const olamgpu_grid* g, const olamgpu_opts
         for (int k = mza; k >= kb; --k) nu[k] = cji[k] * (z[k] - (k < mza ? cim1[k + 1] * nu[k + 1] : (T)0));
         const T ffv = SC.ff_implic[(size_t)(iw - 1) * nrk + istage - 1];
         for (int k = kb; k <= mza; ++k) {
-          F2(L0.data(), k, iw) += F2(L.data(), k, iw) - nu[k];
+          F2(L0s, k, iw) += F2(L.data(), k, iw) - nu[k];
           const T c1 = ffv * dtr * G.volti_(k, iw) / SC.rhos[(size_t)(istage - 1) * plane + (size_t)(iw - 1) * mza + k - 1];
           const T gk = -c1 * nu[k];
           if (k <= mza - 1) {   // min(wmasc(k),0) * (s0(k+1) - s0(k))
             const T a = fmin_(F2(wm, k, iw), (T)0.) * gk;
-            F2(L0.data(), k + 1, iw) += a; F2(L0.data(), k, iw) -= a;
+            F2(L0s, k + 1, iw) += a; F2(L0s, k, iw) -= a;
           }
           if (k - 1 >= kb) {    // max(wmasc(k-1),0) * (s0(k) - s0(k-1))
             const T a = fmax_(F2(wm, k - 1, iw), (T)0.) * gk;
-            F2(L0.data(), k, iw) += a; F2(L0.data(), k - 1, iw) -= a;
+            F2(L0s, k, iw) += a; F2(L0s, k - 1, iw) -= a;
           }
           F2(L.data(), k, iw) = nu[k];
         }
@@ -913,6 +1231,23 @@ static int scalar_transport_rk_adjoint(const olamgpu_grid* g, const olamgpu_opts
       std::fill(Lin.begin(), Lin.end(), (T)0);
       std::fill(Lupv.begin(), Lupv.end(), (T)0);
       std::fill(Lg.begin(), Lg.end(), (T)0);
+      if (pd_stage) {
+        for (int j = 0; j < g->nw_prog; ++j) {
+          const int iw = g->jtw_prog[j], kb = G.lpw(iw);
+          for (int k = 1; k <= kb - 1; ++k) { F2(L.data(), kb, iw) += F2(L.data(), k, iw); F2(L.data(), k, iw) = 0; }
+        }
+        pd_stage_adjoint(C, R, S0p.data(), rhos_nrk, dtr, iorder, nrk, L.data(), Lin.data(), Lp.data());
+        // scp0' = scp0 + dtr sct / rho_old from lpw up
+        for (int j = 0; j < g->nw_prog; ++j) {
+          const int iw = g->jtw_prog[j], kb = G.lpw(iw);
+          for (int k = kb; k <= mza; ++k) {
+            F2(L0.data(), k, iw) += F2(Lp.data(), k, iw);
+            F2(ls, k, iw) += F2(Lp.data(), k, iw) * dtr / F2(SC.rho_old.data(), k, iw);
+          }
+        }
+        L.swap(Lin);
+        continue;
+      }
       for (int j = 0; j < g->nw_prog; ++j) {
         const int iw = g->jtw_prog[j], kb = G.lpw(iw);
         const T fexpl = (T)1.0 - SC.ff_implic[(size_t)(iw - 1) * nrk + istage - 1];
@@ -1043,6 +1378,65 @@ int oracle_scalar_transport_rk_adjoint_f64(const olamgpu_grid* g, const olamgpu_
                                            const float* wmasc, const double* rho, const float* rho_old,
                                            const float* wc) {
   return oracle::scalar_transport_rk_adjoint<double>(g, o, nscal, lam, lsct, vmasc, wmasc, rho, rho_old, wc);
+}
+
+/* The adjoint with the positive-definite limiter (iscal_monot = 2): the
+ * forward step's inputs scp_fwd / sct_fwd and the pdef flags select and
+ * reconstruct the limited last stage of every pdef tracer. */
+int oracle_scalar_transport_rk_adjoint_pd_f32(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
+                                              const float* const* scp_fwd, const float* const* sct_fwd,
+                                              const int* pdef, float* const* lam, float* const* lsct,
+                                              const float* vmasc, const float* wmasc, const double* rho,
+                                              const float* rho_old, const float* wc) {
+  return oracle::scalar_transport_rk_adjoint<float>(g, o, nscal, lam, lsct, vmasc, wmasc, rho, rho_old, wc, scp_fwd,
+                                                    sct_fwd, pdef);
+}
+
+int oracle_scalar_transport_rk_adjoint_pd_f64(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
+                                              const double* const* scp_fwd, const double* const* sct_fwd,
+                                              const int* pdef, double* const* lam, double* const* lsct,
+                                              const float* vmasc, const float* wmasc, const double* rho,
+                                              const float* rho_old, const float* wc) {
+  return oracle::scalar_transport_rk_adjoint<double>(g, o, nscal, lam, lsct, vmasc, wmasc, rho, rho_old, wc,
+                                                     scp_fwd, sct_fwd, pdef);
+}
+
+}
+
+extern "C" {
+
+/* Tangent-linear of one scalar_transport_rk step in FP64: the step of
+ * oracle_scalar_transport_rk_f64 on scp / sct (new scp returned in scp), and
+ * in dscp its exact directional derivative along (dscp, dsct) -- the
+ * Jacobian-vector product of the step, limiters included, with the winds
+ * and densities fixed.  No horizontal diffusion. */
+int oracle_scalar_transport_rk_tl_f64(const olamgpu_grid* g, const olamgpu_opts* o, int nscal,
+                                      double* const* scp, double* const* dscp, double* const* sct,
+                                      double* const* dsct, const int* pdef, const float* vmasc,
+                                      const float* wmasc, const double* rho, const float* rho_old,
+                                      const float* wc) {
+  const size_t plane = (size_t)g->mza * g->mwa;
+  std::vector<std::vector<oracle::Dual>> s(nscal), t(nscal);
+  std::vector<oracle::Dual*> sp(nscal), tp(nscal);
+  for (int n = 0; n < nscal; ++n) {
+    s[n].resize(plane);
+    t[n].resize(plane);
+    for (size_t i = 0; i < plane; ++i) {
+      s[n][i] = oracle::Dual(scp[n][i], dscp[n][i]);
+      t[n][i] = oracle::Dual(sct[n][i], dsct[n][i]);
+    }
+    sp[n] = s[n].data();
+    tp[n] = t[n].data();
+  }
+  const int rc = oracle::scalar_transport_rk<oracle::Dual>(g, o, nscal, sp.data(), tp.data(), pdef, nullptr, vmasc,
+                                                          wmasc, rho, rho_old, wc, nullptr, nullptr, nullptr,
+                                                          nullptr);
+  for (int n = 0; n < nscal; ++n)
+    for (size_t i = 0; i < plane; ++i) {
+      scp[n][i] = s[n][i].v;
+      dscp[n][i] = s[n][i].d;
+    }
+  return rc;
 }
 
 }

@@ -235,3 +235,54 @@ def scalar_transport_adjoint(fg, opts, lam, st, fp64=False):
            abi.ptr(np.ascontiguousarray(st.wc, np.float32), C.c_float))
     assert rc == 0, f"oracle adjoint returned {rc}"
     return np.stack(la), np.stack(ls)
+
+
+def _winds(st):
+    return (abi.ptr(np.ascontiguousarray(st.vmasc, np.float32), C.c_float),
+            abi.ptr(np.ascontiguousarray(st.wmasc, np.float32), C.c_float),
+            abi.ptr(np.ascontiguousarray(st.rho, np.float64), C.c_double),
+            abi.ptr(np.ascontiguousarray(st.rho_old, np.float32), C.c_float),
+            abi.ptr(np.ascontiguousarray(st.wc, np.float32), C.c_float))
+
+
+def scalar_transport_tl(fg, opts, tracers, sct, dtracers, dsct, st, pdef=None):
+    """The oracle's step in FP64 and its exact tangent-linear: returns
+    (new tracers, the directional derivative of the new tracers along
+    (dtracers, dsct)), each (ntr, mwa, mza) float64."""
+    L = lib()
+    f = L.oracle_scalar_transport_rk_tl_f64
+    f.restype = C.c_int
+    dp = C.POINTER(C.c_double)
+    f.argtypes = [C.POINTER(abi.Grid), C.POINTER(abi.Opts), C.c_int, C.POINTER(dp), C.POINTER(dp),
+                  C.POINTER(dp), C.POINTER(dp), abi.c_int_p] + [abi.c_float_p, abi.c_float_p, abi.c_double_p,
+                                                                  abi.c_float_p, abi.c_float_p]
+    cp = lambda xs: [np.ascontiguousarray(x, np.float64).copy() for x in xs]  # noqa: E731
+    s, ds, t, dt = cp(tracers), cp(dtracers), cp(sct), cp(dsct)
+    pd = np.ascontiguousarray(pdef if pdef is not None else np.ones(len(s)), dtype=np.int32)
+    rc = f(C.byref(fg.struct), C.byref(opts), len(s), abi.ptr_array(s, C.c_double), abi.ptr_array(ds, C.c_double),
+           abi.ptr_array(t, C.c_double), abi.ptr_array(dt, C.c_double), abi.ptr(pd, C.c_int), *_winds(st))
+    assert rc == 0, f"oracle tangent-linear returned {rc}"
+    return np.stack(s), np.stack(ds)
+
+
+def scalar_transport_adjoint_pd(fg, opts, lam, st, tracers, sct, pdef=None, fp64=False):
+    """The oracle's adjoint of one step with the positive-definite limiter
+    (iscal_monot = 2) on the forward step from (tracers, sct).  Returns
+    (adjoint of the old tracers, adjoint of sct)."""
+    dt = np.float64 if fp64 else np.float32
+    ct = C.c_double if fp64 else C.c_float
+    L = lib()
+    f = L.oracle_scalar_transport_rk_adjoint_pd_f64 if fp64 else L.oracle_scalar_transport_rk_adjoint_pd_f32
+    f.restype = C.c_int
+    tp = C.POINTER(ct)
+    f.argtypes = [C.POINTER(abi.Grid), C.POINTER(abi.Opts), C.c_int, C.POINTER(tp), C.POINTER(tp), abi.c_int_p,
+                  C.POINTER(tp), C.POINTER(tp)] + [abi.c_float_p, abi.c_float_p, abi.c_double_p, abi.c_float_p,
+                                                   abi.c_float_p]
+    cp = lambda xs: [np.ascontiguousarray(x, dt).copy() for x in xs]  # noqa: E731
+    sf, tf, la = cp(tracers), cp(sct), cp(lam)
+    ls = [np.zeros_like(x) for x in la]
+    pd = np.ascontiguousarray(pdef if pdef is not None else np.ones(len(la)), dtype=np.int32)
+    rc = f(C.byref(fg.struct), C.byref(opts), len(la), abi.ptr_array(sf, ct), abi.ptr_array(tf, ct),
+           abi.ptr(pd, C.c_int), abi.ptr_array(la, ct), abi.ptr_array(ls, ct), *_winds(st))
+    assert rc == 0, f"oracle adjoint returned {rc}"
+    return np.stack(la), np.stack(ls)

@@ -15,10 +15,14 @@ from olam_b200.lib import HostState, OlamGpu, check
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_two_stages_match_transport():
+@pytest.mark.parametrize("order,terrain", [(2, 0), (3, 0), (2, 3)])
+def test_noalloc_two_stages_match_transport(order, terrain):
     import torch
     g, st = small_case(nxp=6, nlev=12, ntr=1, seed=31)
-    opts = abi.make_opts(1800.0)                      # RK2, order 2, no limiter
+    if terrain:
+        from olam_b200.synth.grid import with_terrain
+        g = with_terrain(g, terrain)                   # lpw / lpv floors of a mountain
+    opts = abi.make_opts(1800.0, scal_order=order)    # RK2, no limiter
     fg = abi.FortranGrid(g)
     hs = HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc)
     dev = OlamGpu(fg, opts, hs)
@@ -70,5 +74,26 @@ def test_noalloc_rejects_null_arrays():
         rc = dev.lib.olamgpu_update_scalar_noalloc(None, None, None, None, None, None, C.c_float(1.0),
                                                    None, None)
         assert rc == abi.E_ARG
+    finally:
+        dev.close()
+
+
+def test_noalloc_rejects_a_grid_beyond_the_scratch():
+    # NXP = 75 with 60 levels at order 2 needs 50 NXP^2 mza + ... > 16 Mi floats
+    from olam_b200.synth.grid import build_grid, stretched_levels
+    from olam_b200.synth.state import transport_state
+    g = build_grid(75, stretched_levels(60, 100.0, 30000.0), seed=5)
+    st = transport_state(g, 600.0, 0, seed=5)
+    fg = abi.FortranGrid(g)
+    dev = OlamGpu(fg, abi.make_opts(600.0), HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho))
+    try:
+        import torch
+        a = torch.zeros(g.mwa * g.mza, dtype=torch.float32, device="cuda")
+        v = torch.zeros(g.mva * g.mza, dtype=torch.float32, device="cuda")
+        p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        rc = dev.lib.olamgpu_update_scalar_noalloc(p(a), p(a), p(a), p(a), p(v), p(a), C.c_float(1.0),
+                                                   p(a), None)
+        assert rc == abi.E_ARG
+        assert b"scratch" in dev.lib.olamgpu_strerror(rc)
     finally:
         dev.close()
