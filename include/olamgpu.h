@@ -377,6 +377,39 @@ int olamgpu_timestep(unsigned flags, int nmass, const int* mass_ids);
  * status the device recorded during the step, if any. */
 int olamgpu_timestep_diag(float* smax, double* sums);
 
+/* ---- surface emission and the checkpointed window adjoint -------------------
+ * Surface emission: OLAM's physics adds surface sources to the tracer
+ * tendencies between tend0 and scalar_transport_rk (omodel/timestep.f90:
+ * 76-254); a long step on the device (olamgpu_timestep) has no host physics
+ * in between, so emis[n] (mwa), per registered scalar n (NULL entries: none;
+ * a NULL array: off), is added to var_t(lpw(iw), iw) of scalar n right
+ * after tend0 of every device long step.  Registering scalars drops it. */
+int olamgpu_set_surface_emission(const float* const* emis);
+
+/* A window of nsteps device long steps (olamgpu_timestep's sequence, with
+ * `flags` as there: OLAMGPU_TS_GRAPH replays the recorded step) that keeps a
+ * checkpoint of the state carried from step to step (rho, press, thil, wc,
+ * wmc, vxe/vye/vze, vmc, vc and the damping's saved planes) at the start of
+ * every segment of nchk steps, and the state after the last step.  RESIDENT
+ * mode, one domain, the tiled transport form, and the options the adjoint
+ * runs (see olamgpu_scalar_transport_rk_adjoint).  No counterpart in OLAM:
+ * the forward half of the window adjoint. */
+int olamgpu_window_forward(int nsteps, int nchk, unsigned flags);
+
+/* Adjoint of the window's tracer transport, with the winds and densities of
+ * every step those of the forward: lam[n] (mza, mwa) holds dJ/d(scalar n
+ * after the window) on entry and dJ/d(scalar n before it) on return;
+ * lam_sct[n] receives dJ/d(var_t of scalar n), the tendency held for every
+ * step of the window (so dJ/d(emis[n](iw)) is lam_sct[n](lpw(iw), iw)).
+ * Segment by segment from the last, the segment's checkpoint is restored,
+ * its steps' dynamics are run again to regenerate the winds and densities
+ * each step's transport read (vmasc, wmasc, rho, rho_old), and the one-step
+ * adjoint is applied to those steps in reverse order, all on the device.
+ * The state after the window is restored at the end.  Device memory: one
+ * checkpoint per segment plus nchk steps' transport inputs.  No counterpart
+ * in OLAM. */
+int olamgpu_window_adjoint(float* const* lam, float* const* lam_sct);
+
 /* One explicit RK stage of update_scalar (scalar_transport_rk.F90:389-615:
  * grad_t2d[_quadratic], scalar_v_column, scalar_w_column; every column
  * explicit, no limiter) for ONE tracer, on device arrays the caller owns, in

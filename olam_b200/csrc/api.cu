@@ -147,6 +147,7 @@ static void unregister_state_arrays() {
 
 static void release_all() {
   unregister_state_arrays();
+  window_release();
   Context& C = ctx();
   DevGrid& d = C.g;
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
@@ -176,7 +177,7 @@ static void release_all() {
   Transport& tp = C.tp;
   DevBuf<float>* tb[] = {&tp.vmasc, &tp.wmasc, &tp.rho_old, &tp.wc, &tp.rhos, &tp.ff, &tp.imp_b,
                          &tp.cfl_red, &tp.gx, &tp.upv, &tp.hiv, &tp.sfv, &tp.scale, &tp.upw,
-                         &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx,
+                         &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx, &tp.emis,
                          &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec, &tp.adj_trec,
                          &tp.adj_planes};
   for (auto* b : tb) b->release();
@@ -190,6 +191,7 @@ static void release_all() {
   tp.adj_ptab.release();
   tp.adj_ptab2.release();
   tp.have_turb = false;
+  tp.have_emis = false;
   transport_release_pipeline();
   halo_release();
   glue_release();
@@ -268,6 +270,8 @@ int olamgpu_register_scalars(int num_scalar, float* const* var_p, float* const* 
   for (int n = 0; n < num_scalar; ++n)
     if (!var_p[n] || !var_t[n]) { set_error("NULL var_p/var_t for scalar " + std::to_string(n + 1)); return OLAMGPU_E_ARG; }
   glue_drop_graphs();
+  window_release();
+  C.tp.have_emis = false;   // the emission table is per registered scalar
   Tracers& tr = C.tr;
   // drop a previous registration
   for (size_t i = 0; i < tr.p.size(); ++i) {
@@ -463,6 +467,12 @@ int olamgpu_timestep(unsigned flags, int nmass, const int* mass_ids) {
 }
 
 int olamgpu_timestep_diag(float* smax, double* sums) { return glue_timestep_diag(smax, sums); }
+
+int olamgpu_set_surface_emission(const float* const* emis) { return emission_set(emis); }
+
+int olamgpu_window_forward(int nsteps, int nchk, unsigned flags) { return window_forward(nsteps, nchk, flags); }
+
+int olamgpu_window_adjoint(float* const* lam, float* const* lam_sct) { return window_adjoint(lam, lam_sct); }
 
 void* olamgpu_stream(void) { return (void*)ctx().stream; }
 

@@ -246,6 +246,10 @@ struct Transport {
   DevBuf<float> akhodx;
   DevBuf<int> khtopv;
   bool have_turb = false;
+  // surface emission (olamgpu_set_surface_emission): (mwa, ntp), added to
+  // the tendencies at lpw after tend0 of each long step
+  DevBuf<float> emis;
+  bool have_emis = false;
 };
 
 // Device state and scratch of prog_wrtv_rk (omodel/prog_wrtv_rk.f90).  The
@@ -334,6 +338,26 @@ struct Halo {
   void* user = nullptr;
 };
 
+// checkpointed window of long steps (window.cu): the state at the start of
+// every segment of nchk steps, the state after the window, and the step
+// inputs of the segment being reversed
+struct Window {
+  bool valid = false;
+  bool tracers = false;              // checkpoints hold the tracers (limited transport)
+  int nsteps = 0, nchk = 0;
+  unsigned flags = 0;
+  std::vector<DevBuf<char>> chk;
+  std::vector<int> chk_qcur;
+  std::vector<char> chk_div_first, chk_vort_first;
+  DevBuf<char> fin;
+  int fin_qcur = 0;
+  bool fin_div_first = false, fin_vort_first = false;
+  DevBuf<char> seg;                  // (nchk) x the inputs of one step
+  DevBuf<float> lsacc;               // adjoint of the tendencies, summed over the steps
+  DevBuf<float*> ptab;
+  DevBuf<float> planes;
+};
+
 struct Context {
   bool initialised = false;
   int device = -1;
@@ -350,6 +374,7 @@ struct Context {
   Dyn dy;
   Glue glue;
   Halo halo;
+  Window win;
   DevBuf<int> status;        // device status word (bounds/NaN flags)
 };
 
@@ -420,6 +445,23 @@ int dyn_diagvel_t3d();
 void prof_suspend(bool on);
 // adjoint of one unlimited step (transport_adjoint.cu)
 int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* const* lam_sct);
+// the options and tables the adjoint needs (OLAMGPU_OK when it can run)
+int adjoint_ready(Context& C);
+// the reverse step on the device, at the step inputs held in tp (winds,
+// densities, rho_old): tp.adj_l[0] holds the adjoint of the step's output
+// in the batched layout; on return tp.adj_l[nrk & 1] holds the adjoint of
+// its input and tp.adj_ls that of the tendencies
+int adjoint_core(Context& C, const float* rho_old_host);
+// the long step's device sequence (timestep.cu); without the transport:
+// the dynamics and the glue of thil only
+int glue_run_sequence(Context& C, unsigned flags, bool with_transport);
+// checkpointed window of long steps (window.cu)
+int window_forward(int nsteps, int nchk, unsigned flags);
+int window_adjoint(float* const* lam, float* const* lam_sct);
+void window_release();
+// surface emission of the registered tracers (timestep.cu)
+int emission_set(const float* const* emis);
+void launch_emission(Context& C, cudaStream_t s);
 // forgets the scratch address of olamgpu_update_scalar_noalloc (finalize)
 void noalloc_forget();
 int tracers_to_device(cudaStream_t s);   // host -> per-tracer mirrors (-> Q)

@@ -287,13 +287,78 @@ int glue_mass_sums(int nsel, const int* ids, double* sums) {
   return check_device_status();
 }
 
-// the long step's device sequence (timestep.f90:66-319)
-static int run_sequence(Context& C, unsigned flags, int nmass, const int* ids) {
+// ---- surface emission ----------------------------------------------------------
+// OLAM's physics adds surface sources to the tracer tendencies between tend0
+// and scalar_transport_rk; the long step on the device has no host physics in
+// between, so a registered emission field E(iw) per tracer is added to
+// var_t(lpw, iw) right after tend0.
+__global__ void k_emission(const int* __restrict__ prog, int nprog, const int* __restrict__ lpw, int mza,
+                           const float* __restrict__ emis, int ntp, int n, float* __restrict__ q,
+                           float* const* __restrict__ planes) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nprog * n) return;
+  const int j = (int)(i / n), t = (int)(i % n);
+  const int iw = prog[j];
+  const size_t cell = (size_t)iw * mza + lpw[iw];
+  const float e = emis[(size_t)iw * ntp + t];
+  if (q) q[cell * ntp + t] += e;
+  else planes[t][cell] += e;
+}
+
+static DevBuf<float*> g_emis_ptab;
+
+void launch_emission(Context& C, cudaStream_t s) {
+  Tracers& tr = C.tr;
+  if (!C.tp.have_emis || tr.n <= 0 || C.g.nw_prog <= 0) return;
+  float* q = nullptr;
+  float* const* planes = nullptr;
+  if (tr.q_valid && tr.qt.p) q = tr.qt.p;
+  else planes = g_emis_ptab.p;
+  k_emission<<<cdiv((size_t)C.g.nw_prog * tr.n, 256), 256, 0, s>>>(C.g.jtw_prog.p, C.g.nw_prog, C.g.lpw.p, C.g.mza,
+                                                                  C.tp.emis.p, tr.ntp, tr.n, q, planes);
+  OG_LAUNCHED();
+}
+
+int emission_set(const float* const* emis) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  glue_drop_graphs();
+  Tracers& tr = C.tr;
+  if (!emis) { C.tp.have_emis = false; return OLAMGPU_OK; }
+  if (tr.n <= 0) { set_error("surface emission: register the scalars first"); return OLAMGPU_E_STATE; }
+  const int mwa = C.g.mwa, ntp = tr.ntp;
+  std::vector<float> h((size_t)mwa * ntp, 0.f);
+  for (int n = 0; n < tr.n; ++n)
+    if (emis[n])
+      for (int iw = 0; iw < mwa; ++iw) h[(size_t)iw * ntp + n] = emis[n][iw];
+  cudaStream_t s = C.stream;
+  OG_CHECK(upload(C.tp.emis, h.data(), h.size(), s));
+  std::vector<float*> pt(tr.n);
+  for (int n = 0; n < tr.n; ++n) pt[n] = tr.t[n].p;
+  OG_CHECK(upload(g_emis_ptab, pt.data(), pt.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));   // the host vectors die here
+  C.tp.have_emis = true;
+  return OLAMGPU_OK;
+}
+
+// the long step's device sequence (timestep.f90:66-319); without the
+// transport (with_transport false) the dynamics and the glue of thil only
+static int run_sequence(Context& C, unsigned flags, int nmass, const int* ids, bool with_transport = true) {
   cudaStream_t s = C.stream;
   OG_CHECK(dyn_tend0(nullptr));
+  if (with_transport) launch_emission(C, s);
   if (flags & OLAMGPU_TS_HORIZ_K) OG_CHECK(dyn_comp_horiz_k());
   for (int j = 1; j <= C.opts.nacoust; ++j) OG_CHECK(dyn_prog_wrtv_rk(j));
   OG_CHECK(dyn_timeavg_momsc());
+  if (!with_transport) {
+    if (C.dy.thil.p && C.g.nw_prog > 0) {
+      k_bottom_fill<<<cdiv(C.g.nw_prog, 256), 256, 0, s>>>(C.g.jtw_prog.p, C.g.nw_prog, C.g.lpw.p, C.g.mza,
+                                                           C.dy.thil.p, 1, 1);
+      OG_LAUNCHED();
+    }
+    OG_CUDA(cudaGetLastError());
+    return OLAMGPU_OK;
+  }
   OG_CHECK(transport_run(nullptr, nullptr));
   if (flags & OLAMGPU_TS_MAXMIN) OG_CHECK(launch_maxmin(C, s));
   launch_bottom_fill(C, s);
@@ -307,6 +372,10 @@ static int run_sequence(Context& C, unsigned flags, int nmass, const int* ids) {
   if (flags & OLAMGPU_TS_MASS) OG_CHECK(launch_mass(C, nmass, ids, s));
   OG_CUDA(cudaGetLastError());
   return OLAMGPU_OK;
+}
+
+int glue_run_sequence(Context& C, unsigned flags, bool with_transport) {
+  return run_sequence(C, flags & ~(unsigned)(OLAMGPU_TS_MAXMIN | OLAMGPU_TS_MASS), 0, nullptr, with_transport);
 }
 
 static bool same_step(const StepGraph& g, unsigned flags, int nmass, const int* ids) {

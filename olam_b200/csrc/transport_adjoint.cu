@@ -470,13 +470,96 @@ static int planes_table(DevBuf<float*>& tab, float* base, int n, size_t plane, c
   return OLAMGPU_OK;
 }
 
-int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* const* lam_sct) {
-  Context& C = ctx();
+// the options and tables the adjoint needs
+static int adjoint_checks(Context& C) {
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
   if (!C.have_state || !C.hstate.vmasc || !C.hstate.wmasc || !C.hstate.rho) {
     set_error("state arrays vmasc/wmasc/rho were not registered at init");
     return OLAMGPU_E_STATE;
   }
+  const DevGrid& d = C.g;
+  const int nrk = C.opts.nrk_scal;
+  const int order = C.opts.scal_horiz_adv_order;
+  if (nrk != 2 && nrk != 3) { set_error("scalar_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
+  if (C.opts.iscal_monot != 0) {
+    set_error("the adjoint covers the unlimited transport (iscal_monot = 0) only");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  if (C.tp.have_turb) {
+    set_error("the adjoint does not cover horizontal diffusion of the tracers");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  if (!tile_stage_available(d, C.tp, order)) {
+    set_error("the adjoint needs the tiled transport tables");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  if (!d.tile_closed) {
+    set_error("the adjoint needs every neighbour of a prognosed column to be prognosed (a global domain)");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  return OLAMGPU_OK;
+}
+
+int adjoint_core(Context& C, const float* rho_old_host) {
+  const DevGrid& d = C.g;
+  Transport& tp = C.tp;
+  cudaStream_t s = C.stream;
+  const int mza = d.mza, mwa = d.mwa;
+  const int nrk = C.opts.nrk_scal;
+  const int ntp = C.tr.ntp;
+  const size_t plane = (size_t)mza * mwa, qn = plane * ntp;
+  OG_CHECK(tp.adj_l[0].alloc(qn));
+  OG_CHECK(tp.adj_l[1].alloc(qn));
+  if (tp.adj_l0.n < qn) OG_CHECK(tp.adj_l0.alloc(qn));
+  OG_CHECK(tp.adj_ls.alloc(qn));
+  float dtlr[3];
+  OG_CHECK(transport_prepare(C, rho_old_host, false, dtlr));
+  const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * plane;
+  {
+    OG_PROF("adj_records", s);
+    OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s));
+    OG_CHECK(launch_adj_records(d, tp, C.status.p, s));
+  }
+  // the reverse stages alternate between the two lam buffers; the last
+  // one writes into adj_l[fin]
+  const int fin = nrk & 1;
+  float* L = tp.adj_l[0].p;
+  float* LIN = tp.adj_l[1].p;
+  const size_t colsize = (size_t)mza * ntp;
+  if (d.n_nonprog > 0) {
+    k_adj_nonprog<<<cdiv((size_t)d.n_nonprog * colsize, 256), 256, 0, s>>>(d.w_nonprog.p, d.n_nonprog, colsize, L,
+                                                                          LIN, tp.adj_ls.p, fin);
+    OG_LAUNCHED();
+  }
+  for (int istage = nrk; istage >= 1; --istage) {
+    const float dtr = dtlr[istage - 1];
+    const int first = istage == nrk, last = istage == 1;
+    {
+      OG_PROF("adj_implicit", s);
+      k_adj_implicit<<<cdiv((size_t)d.nw_prog * ntp, 128), 128, 0, s>>>(
+          gridk(d), tp.imp_list.p + (size_t)(istage - 1) * mwa, tp.imp_count.p + (istage - 1),
+          tp.imp_b.p + (size_t)(istage - 1) * mwa * 3 * mza, tp.ff.p, tp.wmasc.p,
+          tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage, dtr, ntp, first, L, tp.adj_l0.p);
+      OG_LAUNCHED();
+      if (d.nw_prog > 0)
+        k_adj_fold0<<<cdiv((size_t)d.nw_prog * (ntp / 4), 256), 256, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p,
+                                                                             mza, ntp, L);
+      OG_LAUNCHED();
+    }
+    {
+      OG_PROF("adj_stage", s);
+      OG_CHECK(launch_tile_adj(d, tp, L, LIN, tp.adj_l0.p, tp.adj_ls.p, ntp, istage, nrk, dtr, first, last,
+                               C.status.p, s));
+    }
+    std::swap(L, LIN);
+  }
+  return OLAMGPU_OK;
+}
+
+int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* const* lam_sct) {
+  Context& C = ctx();
+  OG_CHECK(adjoint_checks(C));
   const int n = C.tr.n;
   if (n <= 0) return OLAMGPU_OK;
   if (!lam || !lam_sct) { set_error("lam and lam_sct must be arrays of num_scalar pointers"); return OLAMGPU_E_ARG; }
@@ -487,25 +570,6 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   cudaStream_t s = C.stream;
   const int mza = d.mza, mwa = d.mwa;
   const int nrk = C.opts.nrk_scal;
-  const int order = C.opts.scal_horiz_adv_order;
-  if (nrk != 2 && nrk != 3) { set_error("scalar_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
-  if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
-  if (C.opts.iscal_monot != 0) {
-    set_error("the adjoint covers the unlimited transport (iscal_monot = 0) only");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
-  if (tp.have_turb) {
-    set_error("the adjoint does not cover horizontal diffusion of the tracers");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
-  if (!tile_stage_available(d, tp, order)) {
-    set_error("the adjoint needs the tiled transport tables");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
-  if (!d.tile_closed) {
-    set_error("the adjoint needs every neighbour of a prognosed column to be prognosed (a global domain)");
-    return OLAMGPU_E_UNSUPPORTED;
-  }
   const int ntp = C.tr.ntp;
   const size_t plane = (size_t)mza * mwa, qn = plane * ntp;
   // per-tracer planes on the device start on 16-byte boundaries (the layout
@@ -513,9 +577,7 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   const size_t pstride = (plane + 3) & ~(size_t)3;
 
   OG_CHECK(tp.adj_l[0].alloc(qn));
-  OG_CHECK(tp.adj_l[1].alloc(qn));
   OG_CHECK(tp.adj_l0.alloc(std::max(qn, pstride * n)));
-  OG_CHECK(tp.adj_ls.alloc(qn));
   OG_CHECK(tp.adj_planes.alloc(pstride * n));
   OG_CHECK(planes_table(tp.adj_ptab, tp.adj_planes.p, n, pstride, s));
   // lams leaves through lam0's memory, which is free after the last stage
@@ -523,55 +585,14 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   for (int i = 0; i < n; ++i)
     OG_CUDA(cudaMemcpyAsync(tp.adj_planes.p + (size_t)i * pstride, lam[i], plane * sizeof(float),
                             cudaMemcpyHostToDevice, s));
-
   {
     // device work of the step (in RESIDENT mode the preparation uploads nothing)
     OG_PROF("adjoint", s);
-    float dtlr[3];
-    OG_CHECK(transport_prepare(C, rho_old_host, false, dtlr));
-    const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * plane;
     { OG_PROF("adj_gather", s); launch_gather_q(tp.adj_l[0].p, (const float* const*)tp.adj_ptab.p, n, ntp, plane, s); }
-    {
-      OG_PROF("adj_records", s);
-      OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s));
-      OG_CHECK(launch_adj_records(d, tp, C.status.p, s));
-    }
-    // the reverse stages alternate between the two lam buffers; the last
-    // one writes into adj_l[fin]
-    const int fin = nrk & 1;
-    float* L = tp.adj_l[0].p;
-    float* LIN = tp.adj_l[1].p;
-    const size_t colsize = (size_t)mza * ntp;
-    if (d.n_nonprog > 0) {
-      k_adj_nonprog<<<cdiv((size_t)d.n_nonprog * colsize, 256), 256, 0, s>>>(d.w_nonprog.p, d.n_nonprog, colsize, L,
-                                                                            LIN, tp.adj_ls.p, fin);
-      OG_LAUNCHED();
-    }
-    for (int istage = nrk; istage >= 1; --istage) {
-      const float dtr = dtlr[istage - 1];
-      const int first = istage == nrk, last = istage == 1;
-      {
-        OG_PROF("adj_implicit", s);
-        k_adj_implicit<<<cdiv((size_t)d.nw_prog * ntp, 128), 128, 0, s>>>(
-            gridk(d), tp.imp_list.p + (size_t)(istage - 1) * mwa, tp.imp_count.p + (istage - 1),
-            tp.imp_b.p + (size_t)(istage - 1) * mwa * 3 * mza, tp.ff.p, tp.wmasc.p,
-            tp.rhos.p + (size_t)(istage - 1) * plane, nrk, istage, dtr, ntp, first, L, tp.adj_l0.p);
-        OG_LAUNCHED();
-        if (d.nw_prog > 0)
-          k_adj_fold0<<<cdiv((size_t)d.nw_prog * (ntp / 4), 256), 256, 0, s>>>(d.jtw_prog.p, d.nw_prog, d.lpw.p,
-                                                                               mza, ntp, L);
-        OG_LAUNCHED();
-      }
-      {
-        OG_PROF("adj_stage", s);
-        OG_CHECK(launch_tile_adj(d, tp, L, LIN, tp.adj_l0.p, tp.adj_ls.p, ntp, istage, nrk, dtr, first, last,
-                                 C.status.p, s));
-      }
-      std::swap(L, LIN);
-    }
+    OG_CHECK(adjoint_core(C, rho_old_host));
     {
       OG_PROF("adj_scatter", s);
-      launch_scatter_q(tp.adj_l[fin].p, tp.adj_ptab.p, n, ntp, plane, s);
+      launch_scatter_q(tp.adj_l[nrk & 1].p, tp.adj_ptab.p, n, ntp, plane, s);
       launch_scatter_q(tp.adj_ls.p, tp.adj_ptab2.p, n, ntp, plane, s);
     }
   }
@@ -585,5 +606,7 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   OG_CUDA(cudaStreamSynchronize(s));
   return check_device_status();
 }
+
+int adjoint_ready(Context& C) { return adjoint_checks(C); }
 
 }  // namespace olamgpu

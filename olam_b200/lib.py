@@ -29,6 +29,7 @@ EXPORTS = [
     "olamgpu_scalar_transport_rk_adjoint", "olamgpu_set_eddy", "olamgpu_comp_horiz_k",
     "olamgpu_set_scalars_bottom", "olamgpu_diagvel_t3d", "olamgpu_tracer_maxmin", "olamgpu_mass_sums",
     "olamgpu_timestep", "olamgpu_timestep_diag", "olamgpu_set_halo",
+    "olamgpu_set_surface_emission", "olamgpu_window_forward", "olamgpu_window_adjoint",
 ]
 
 
@@ -79,6 +80,9 @@ def load():
     lib.olamgpu_mass_sums.argtypes = [C.c_int, abi.c_int_p, abi.c_double_p]
     lib.olamgpu_timestep.argtypes = [C.c_uint, C.c_int, abi.c_int_p]
     lib.olamgpu_timestep_diag.argtypes = [abi.c_float_p, abi.c_double_p]
+    lib.olamgpu_set_surface_emission.argtypes = [C.POINTER(abi.c_float_p)]
+    lib.olamgpu_window_forward.argtypes = [C.c_int, C.c_int, C.c_uint]
+    lib.olamgpu_window_adjoint.argtypes = [C.POINTER(abi.c_float_p), C.POINTER(abi.c_float_p)]
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
             getattr(lib, name).restype = C.c_int
@@ -207,6 +211,28 @@ class OlamGpu:
         ids = np.ascontiguousarray(mass_ids, dtype=np.int32)
         self._mass_ids = ids
         check(self.lib.olamgpu_timestep(int(flags), int(ids.size), abi.ptr(ids, C.c_int) if ids.size else None))
+
+    def set_surface_emission(self, emis):
+        """emis: list (one per registered scalar) of (mwa,) float32 arrays or
+        None entries, or None to switch the emission off."""
+        if emis is None:
+            self._emis = None
+            check(self.lib.olamgpu_set_surface_emission(None))
+            return
+        self._emis = [None if e is None else np.ascontiguousarray(e, dtype=np.float32) for e in emis]
+        arr = (abi.c_float_p * len(self._emis))(*[abi.ptr(e, C.c_float) for e in self._emis])
+        check(self.lib.olamgpu_set_surface_emission(arr))
+
+    def window_forward(self, nsteps, nchk, flags=0):
+        check(self.lib.olamgpu_window_forward(int(nsteps), int(nchk), int(flags)))
+
+    def window_adjoint(self, lam):
+        """lam: list of (mwa, mza) float32 arrays of dJ/d(scalars after the
+        window); returns (dJ/d(scalars before it), dJ/d(tendencies))."""
+        lam_io = [np.array(x, dtype=np.float32, order="C", copy=True) for x in lam]
+        lsct = [np.zeros_like(x) for x in lam_io]
+        check(self.lib.olamgpu_window_adjoint(abi.ptr_array(lam_io, C.c_float), abi.ptr_array(lsct, C.c_float)))
+        return lam_io, lsct
 
     def timestep_diag(self, ntr, nmass=0):
         smax = np.zeros((ntr, 2), np.float32)
