@@ -148,6 +148,7 @@ static void unregister_state_arrays() {
 static void release_all() {
   unregister_state_arrays();
   window_release();
+  pd_adjoint_release();
   Context& C = ctx();
   DevGrid& d = C.g;
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,

@@ -328,11 +328,66 @@ static double face_weight(const olamgpu_grid* g, int order, int iv, int sd, int 
   return dx * x[0] + dy * x[1] + (double)g->xx0_v[e] * x[2] + (double)g->xy0_v[e] * x[3] + (double)g->yy0_v[e] * x[4];
 }
 
+// Distance along a Hilbert curve filling a 2^b x 2^b grid (the published
+// iterative construction: at each scale take the quadrant's index along the
+// curve, then reflect and transpose the point into that quadrant's frame).
+static unsigned long long hilbert_index(unsigned b, unsigned x, unsigned y) {
+  unsigned long long d = 0;
+  for (unsigned s = 1u << (b - 1); s > 0; s >>= 1) {
+    const unsigned rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
+    d += (unsigned long long)s * s * ((3u * rx) ^ ry);
+    if (ry == 0) {
+      if (rx == 1) { x = s - 1 - (x & (s - 1)); y = s - 1 - (y & (s - 1)); }
+      std::swap(x, y);
+    }
+    x &= s - 1;
+    y &= s - 1;
+  }
+  return d;
+}
+
+// The prognosed columns in an order of the library's own that keeps nearby
+// columns together, whatever the caller's numbering: each column's unit
+// normal (its position on the sphere) is projected onto the face of the
+// circumscribing cube it points at, and the faces' points are ordered along
+// a Hilbert curve.  Without the normals, jtw_prog's order.
+std::vector<int> locality_order(const olamgpu_grid* g) {
+  const int nprog = g->nw_prog;
+  std::vector<int> cols(nprog);
+  for (int j = 0; j < nprog; ++j) cols[j] = g->jtw_prog[j] - 1;
+  if (!g->wnx || !g->wny || !g->wnz) return cols;
+  const unsigned bits = 16;
+  const double q = (double)(1u << bits);
+  std::vector<std::pair<unsigned long long, int>> key(nprog);
+  for (int j = 0; j < nprog; ++j) {
+    const int c = cols[j];
+    const double p[3] = {g->wnx[c], g->wny[c], g->wnz[c]};
+    int ax = 0;
+    for (int a = 1; a < 3; ++a) if (std::fabs(p[a]) > std::fabs(p[ax])) ax = a;
+    const double m = std::fabs(p[ax]) > 0 ? std::fabs(p[ax]) : 1.0;
+    const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+    auto cell = [&](double v) {
+      const double t = (v / m + 1.0) * 0.5 * q;
+      return (unsigned)std::min(std::max(t, 0.0), q - 1.0);
+    };
+    const unsigned face = (unsigned)(2 * ax + (p[ax] > 0 ? 1 : 0));
+    key[j] = {((unsigned long long)face << 40) | hilbert_index(bits, cell(p[o1]), cell(p[o2])), c};
+  }
+  std::stable_sort(key.begin(), key.end(),
+                   [](const std::pair<unsigned long long, int>& a, const std::pair<unsigned long long, int>& b) {
+                     return a.first < b.first;
+                   });
+  for (int j = 0; j < nprog; ++j) cols[j] = key[j].second;
+  return cols;
+}
+
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
   th = TileHost();
   if (order != 2 && order != 3) return;
   const int nprog = g->nw_prog, mwa = g->mwa;
   if (nprog <= 0) return;
+  // tiles are runs of this order's columns
+  const std::vector<int> cols = locality_order(g);
   for (int j = 0; j < nprog; ++j) {
     const int c = g->jtw_prog[j] - 1;
     if (g->npoly[c] < 3 || g->npoly[c] > 6) return;  // left to the column kernel
@@ -365,7 +420,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
     auto add = [&](int x) {
       if (stamp[x] != t) { stamp[x] = t; loc[x] = (int)U.size(); U.push_back(x); }
     };
-    for (int j = j0; j < j1; ++j) add(g->jtw_prog[j] - 1);
+    for (int j = j0; j < j1; ++j) add(cols[j]);
     const int nt = (int)U.size();
     for (int i = 0; i < nt; ++i)
       for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));

@@ -24,6 +24,35 @@ static int mode_for(const Context& C, int n) {
   return MODE_PLAIN;
 }
 
+// The last RK stage's mode of every tracer (d_mode[0, n)) and the flags of
+// the tracers whose scp0 takes the low-order pre-update (d_mode[n, 2n)),
+// uploaded when they change only (the upload reads pageable host memory,
+// which a recorded step could not repeat).
+int tracer_modes(Context& C, std::vector<int>& modes, std::vector<int>& pdm, bool& anylim, bool& any_pdm) {
+  Tracers& tr = C.tr;
+  Transport& tp = C.tp;
+  modes.assign(tr.n, MODE_PLAIN);
+  pdm.assign(tr.n, 0);
+  anylim = any_pdm = false;
+  for (int n = 0; n < tr.n; ++n) {
+    modes[n] = mode_for(C, n);
+    anylim |= modes[n] != MODE_PLAIN;
+    pdm[n] = (C.opts.iscal_monot > 0 && tr.pdef[n]) ? 1 : 0;
+    any_pdm |= pdm[n] != 0;
+  }
+  std::vector<int> hm(modes);
+  hm.insert(hm.end(), pdm.begin(), pdm.end());
+  if (hm != tp.h_mode || !tp.d_mode.p) {
+    OG_CHECK(tp.d_mode.alloc((size_t)std::max(tr.n, 1) * 2));
+    if (tr.n > 0) {
+      OG_CUDA(cudaMemcpyAsync(tp.d_mode.p, hm.data(), hm.size() * sizeof(int), cudaMemcpyHostToDevice, C.stream));
+      OG_CUDA(cudaStreamSynchronize(C.stream));
+    }
+    tp.h_mode = hm;
+  }
+  return OLAMGPU_OK;
+}
+
 int tracers_to_device(cudaStream_t s) {
   Context& C = ctx();
   Tracers& tr = C.tr;
@@ -332,26 +361,9 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * wz;
 
   // last-stage mode per tracer
-  std::vector<int> modes(tr.n);
-  bool anylim = false;
-  for (int n = 0; n < tr.n; ++n) { modes[n] = mode_for(C, n); anylim |= modes[n] != MODE_PLAIN; }
-  std::vector<int> pdm(tr.n);
-  for (int n = 0; n < tr.n; ++n) pdm[n] = (C.opts.iscal_monot > 0 && tr.pdef[n]) ? 1 : 0;
-  {
-    // uploaded when they change only (the upload reads pageable host memory,
-    // which a recorded step could not repeat)
-    std::vector<int> hm(modes);
-    hm.insert(hm.end(), pdm.begin(), pdm.end());
-    if (hm != tp.h_mode || !tp.d_mode.p) {
-      OG_CHECK(tp.d_mode.alloc((size_t)std::max(tr.n, 1) * 2));
-      if (tr.n > 0) {
-        OG_CUDA(cudaMemcpyAsync(tp.d_mode.p, hm.data(), hm.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-        OG_CUDA(cudaStreamSynchronize(s));
-      }
-      tp.h_mode = hm;
-    }
-  }
-  const bool any_pdm = std::any_of(pdm.begin(), pdm.end(), [](int v) { return v != 0; });
+  std::vector<int> modes, pdm;
+  bool anylim = false, any_pdm = false;
+  OG_CHECK(tracer_modes(C, modes, pdm, anylim, any_pdm));
 
   if (pipelined) {
     OG_CHECK(pipelined_step(C, dtlr, rhos_nrk));

@@ -237,10 +237,22 @@ struct TileAdjArgs {
   float* __restrict__ LIN;          // adjoint of the stage input (last stage: of the old scp)
   float* __restrict__ L0;           // adjoint of scp0
   float* __restrict__ LS;           // adjoint of sct
+  const int* skip;                  // (ntr) or NULL: tracers whose results this launch leaves alone
+  int ntr;                          // registered tracers (skip's length)
   int* err;
 };
 
 #define TADJ_THREADS 256
+
+// a row of four tracers, leaving the ones flagged in mask (bit j: tracer j) alone
+__device__ __forceinline__ void stg4m(float* p, F4 v, int mask) {
+  if (mask == 0) { stg4(p, v); return; }
+  if (mask == 15) return;
+  if (!(mask & 1)) p[0] = v.a.x;
+  if (!(mask & 2)) p[1] = v.a.y;
+  if (!(mask & 4)) p[2] = v.b.x;
+  if (!(mask & 8)) p[3] = v.b.y;
+}
 
 size_t tile_adj_smem_bytes(int T, int nu) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
@@ -321,6 +333,12 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   const bool act = 4 * hl < seg;
   const int cb = 2 * warp + half;
   const bool first = A.first != 0, last = A.last != 0;
+  int skm = 0;   // this lane's tracers whose results are written elsewhere
+  if (A.skip)
+    for (int j = 0; j < 4; ++j) {
+      const int tr = t0 + 4 * hl + j;
+      if (tr < A.ntr && A.skip[tr]) skm |= 1 << j;
+    }
   const float dtr = A.dtr;
   F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], l0[NC], ls[NC];
   long long cbase[NC];
@@ -390,19 +408,19 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
         const long long row = cbase[n] + (long long)kd * ntp;
         if (kd >= kbc[n]) {
           if (last) {
-            stg4(A.LIN + row, add4(lin, l0n));
+            stg4m(A.LIN + row, add4(lin, l0n), skm);
           } else {
-            stg4(A.LIN + row, lin);
-            stg4(A.L0 + row, l0n);
+            stg4m(A.LIN + row, lin, skm);
+            stg4m(A.L0 + row, l0n, skm);
           }
-          stg4(A.LS + row, lsn);
+          stg4m(A.LS + row, lsn, skm);
         }
         // the stage reads no level below the column's floor
         if (kd == kbc[n])
           for (int k2 = 0; k2 < kd; ++k2) {
             const long long r2 = cbase[n] + (long long)k2 * ntp;
-            stg4(A.LIN + r2, zero4());
-            if (first) { stg4(A.L0 + r2, zero4()); stg4(A.LS + r2, zero4()); }
+            stg4m(A.LIN + r2, zero4(), skm);
+            if (first) { stg4m(A.L0 + r2, zero4(), skm); stg4m(A.LS + r2, zero4(), skm); }
           }
         // slide the column's window up one level and read ahead
         m2[n] = m1[n]; m1[n] = lx; p1[n] = p2[n]; p2[n] = p3[n];
@@ -420,8 +438,9 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
 
 static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L, float* LIN, float* L0, float* LS,
                            int ntp, int istage, int nrk, float dtr, int first, int last, int* status,
-                           cudaStream_t s) {
+                           cudaStream_t s, const int* skip = nullptr, int ntr = 0) {
   TileAdjArgs A;
+  A.skip = skip; A.ntr = ntr;
   A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1; A.lpw = d.lpw.p;
   A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.mwa = d.mwa;
   A.dtr = dtr; A.first = first; A.last = last;
@@ -482,8 +501,8 @@ static int adjoint_checks(Context& C) {
   const int order = C.opts.scal_horiz_adv_order;
   if (nrk != 2 && nrk != 3) { set_error("scalar_timestep_level must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
   if (order != 2 && order != 3) { set_error("scal_horiz_adv_order must be 2 or 3"); return OLAMGPU_E_UNSUPPORTED; }
-  if (C.opts.iscal_monot != 0) {
-    set_error("the adjoint covers the unlimited transport (iscal_monot = 0) only");
+  if (C.opts.iscal_monot == 1) {
+    set_error("the adjoint covers the unlimited and the positive-definite transport (iscal_monot = 0 or 2)");
     return OLAMGPU_E_UNSUPPORTED;
   }
   if (C.tp.have_turb) {
@@ -516,10 +535,39 @@ int adjoint_core(Context& C, const float* rho_old_host) {
   float dtlr[3];
   OG_CHECK(transport_prepare(C, rho_old_host, false, dtlr));
   const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * plane;
+  std::vector<int> modes, pdm;
+  bool anylim = false, any_pdm = false;
+  OG_CHECK(tracer_modes(C, modes, pdm, anylim, any_pdm));
+  const bool pd = C.opts.iscal_monot == 2 && anylim;
   {
     OG_PROF("adj_records", s);
     OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s));
     OG_CHECK(launch_adj_records(d, tp, C.status.p, s));
+  }
+  // the positive-definite last stage is taken at the forward state: the
+  // step again from its input tracers (Q[qcur]) and tendencies (qt) to the
+  // last stage's input, and scp0' = scp0 + dtr sct / rho_old
+  const float* S_in = nullptr;
+  float* S0p = nullptr;
+  if (pd) {
+    OG_PROF("adj_pd_recompute", s);
+    Tracers& tr = C.tr;
+    const float* F = tr.q[tr.qcur].p;
+    float* B1 = tr.q[(tr.qcur + 1) % 3].p;
+    float* B2 = tr.q[(tr.qcur + 2) % 3].p;
+    const float* in = F;
+    float* outs[2] = {B1, B2};
+    for (int istage = 1; istage < nrk; ++istage) {
+      float* out = outs[(istage - 1) & 1];
+      OG_CHECK(launch_tile_stage(d, tp, in, F, tr.qt.p, out, ntp, istage, nrk, dtlr[istage - 1], C.status.p, s));
+      launch_implicit_solve(d, tp, nrk, istage, dtlr[istage - 1], CTView{F, ntp, 0}, TView{out, ntp, 0}, ntp, s);
+      in = out;
+    }
+    S_in = in;
+    S0p = in == B1 ? B2 : B1;
+    OG_CUDA(cudaMemcpyAsync(S0p, F, qn * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    launch_scp0_pd_update(d, tp, TView{S0p, ntp, 0}, CTView{tr.qt.p, ntp, 0}, tp.d_mode.p + tr.n, tr.n,
+                          dtlr[nrk - 1], s);
   }
   // the reverse stages alternate between the two lam buffers; the last
   // one writes into adj_l[fin]
@@ -547,10 +595,15 @@ int adjoint_core(Context& C, const float* rho_old_host) {
                                                                              mza, ntp, L);
       OG_LAUNCHED();
     }
+    const bool pd_stage = pd && first;
+    if (pd_stage) {
+      // the limited tracers' transpose; the batched kernel below leaves them alone
+      OG_CHECK(pd_adjoint_stage(C, S_in, S0p, L, LIN, tp.adj_l0.p, tp.adj_ls.p, dtr, 0, C.tr.n, s));
+    }
     {
       OG_PROF("adj_stage", s);
       OG_CHECK(launch_tile_adj(d, tp, L, LIN, tp.adj_l0.p, tp.adj_ls.p, ntp, istage, nrk, dtr, first, last,
-                               C.status.p, s));
+                               C.status.p, s, pd_stage ? tp.d_mode.p + C.tr.n : nullptr, C.tr.n));
     }
     std::swap(L, LIN);
   }
@@ -579,6 +632,12 @@ int transport_adjoint_run(const float* rho_old_host, float* const* lam, float* c
   OG_CHECK(tp.adj_l[0].alloc(qn));
   OG_CHECK(tp.adj_l0.alloc(std::max(qn, pstride * n)));
   OG_CHECK(tp.adj_planes.alloc(pstride * n));
+  if (C.opts.iscal_monot == 2) {
+    // the limited stage's adjoint is taken at the forward state: the
+    // registered tracers and tendencies are the step's inputs
+    if (C.coherence == OLAMGPU_SYNC_EACH_CALL) OG_CHECK(tracers_to_device(s));
+    OG_CHECK(ensure_q(s));
+  }
   OG_CHECK(planes_table(tp.adj_ptab, tp.adj_planes.p, n, pstride, s));
   // lams leaves through lam0's memory, which is free after the last stage
   OG_CHECK(planes_table(tp.adj_ptab2, tp.adj_l0.p, n, pstride, s));

@@ -25,8 +25,6 @@
 
 namespace olamgpu {
 
-static const float kEps0 = 1.e-32f;
-static const float kEps1 = 3.e-07f;
 
 GridK gridk(const DevGrid& d) {
   GridK g;
@@ -35,25 +33,6 @@ GridK gridk(const DevGrid& d) {
   g.v_iw = d.v_iw.p; g.lpw = d.lpw.p; g.lpv = d.lpv.p; g.volti = d.volti.p;
   g.a_w = d.a_w.p; g.a_wu = d.a_wu.p;
   return g;
-}
-
-__device__ __forceinline__ float AW(const float* a, int mza, int kd, int i, int j) {
-  return __ldg(a + kd + mza * ((i - 1) + 2 * (j - 1)));
-}
-
-// grad_z_quadratic (grad_lib.f90:166-229) at device level kd, from the three
-// column values around it.  Boundary flags as itopbc/ibotbc.
-__device__ __forceinline__ void zrec(const float* a, int mza, int kd, int kb, float sm1, float s0,
-                                     float sp1, float sp2_unused, bool ibot, bool itop,
-                                     float& sb, float& st) {
-  (void)sp2_unused;
-  float ds_k, ds_km1;
-  if (kd <= mza - 2) ds_k = sp1 - s0;
-  else ds_k = itop ? (s0 - sm1) : 0.f;
-  if (kd >= kb + 1) ds_km1 = s0 - sm1;
-  else ds_km1 = ibot ? ((kb <= mza - 2) ? sp1 - s0 : 0.f) : 0.f;
-  sb = s0 + ds_k * AW(a, mza, kd, 1, 1) + ds_km1 * AW(a, mza, kd, 2, 1);
-  st = s0 + ds_k * AW(a, mza, kd, 1, 2) + ds_km1 * AW(a, mza, kd, 2, 2);
 }
 
 // ---------------------------------------------------------------------------

@@ -38,6 +38,31 @@ struct GridK {
 
 GridK gridk(const DevGrid& d);
 
+// the positive-definite / monotonic limiters' constants (scalar_transport_rk.F90:14-17)
+static const float kEps0 = 1.e-32f;
+static const float kEps1 = 3.e-07f;
+
+// a_w(k, i, j) of a Fortran (mza, 2, 2) array at device level kd
+__device__ __forceinline__ float AW(const float* a, int mza, int kd, int i, int j) {
+  return __ldg(a + kd + mza * ((i - 1) + 2 * (j - 1)));
+}
+
+// grad_z_quadratic (grad_lib.f90:166-229) at device level kd, from the three
+// column values around it.  Boundary flags as itopbc/ibotbc.
+__device__ __forceinline__ void zrec(const float* a, int mza, int kd, int kb, float sm1, float s0,
+                                     float sp1, float sp2_unused, bool ibot, bool itop,
+                                     float& sb, float& st) {
+  (void)sp2_unused;
+  float ds_k, ds_km1;
+  if (kd <= mza - 2) ds_k = sp1 - s0;
+  else ds_k = itop ? (s0 - sm1) : 0.f;
+  if (kd >= kb + 1) ds_km1 = s0 - sm1;
+  else ds_km1 = ibot ? ((kb <= mza - 2) ? sp1 - s0 : 0.f) : 0.f;
+  sb = s0 + ds_k * AW(a, mza, kd, 1, 1) + ds_km1 * AW(a, mza, kd, 2, 1);
+  st = s0 + ds_k * AW(a, mza, kd, 1, 2) + ds_km1 * AW(a, mza, kd, 2, 2);
+}
+
+
 // Per-tracer update mode on the last RK stage.
 enum { MODE_PLAIN = 0, MODE_MONOT = 1, MODE_PD = 2 };
 
@@ -94,6 +119,19 @@ void launch_gather_q(float* q, const float* const* src, int n, int ntp, size_t n
                      cudaStream_t s);
 void launch_scatter_q(const float* q, float* const* dst, int n, int ntp, size_t npts_k,
                       cudaStream_t s);
+
+// the tracers' last-stage modes on the device (tp.d_mode: modes, then the
+// flags of the low-order scp0 pre-update), uploaded when they change
+int tracer_modes(Context& C, std::vector<int>& modes, std::vector<int>& pdm, bool& anylim, bool& any_pdm);
+
+// adjoint of the positive-definite last stage (transport_adjoint_pd.cu) for
+// the tracers [t0, t0 + nt) of the batched layout whose mode is MODE_PD: S
+// the stage input, S0p scp0', L the adjoint of the stage output (below-ground
+// levels folded), L0 the implicit solve's adjoint of scp0'; writes their
+// LIN (adjoint of S), L0 (of scp0) and LS (of sct)
+int pd_adjoint_stage(Context& C, const float* S, const float* S0p, const float* L, float* LIN, float* L0,
+                     float* LS, float dtr, int t0, int nt, cudaStream_t s);
+void pd_adjoint_release();
 
 // inputs and per-step coefficients shared by the transport and its adjoint
 // (transport.cu): uploads, check_cfls, rhos, implicit factors; dtlr per stage

@@ -119,7 +119,9 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
   W.nsteps = nsteps;
   W.nchk = nchk;
   W.flags = flags & ~(unsigned)(OLAMGPU_TS_MAXMIN | OLAMGPU_TS_MASS);
-  W.tracers = false;
+  // the limiter's adjoint is taken at the forward state: checkpoints and
+  // the recomputed segments keep the tracers too
+  W.tracers = C.opts.iscal_monot == 2;
   const int nseg = (nsteps + nchk - 1) / nchk;
   W.chk.resize(nseg);
   W.chk_qcur.assign(nseg, 0);
@@ -166,7 +168,9 @@ int window_adjoint(float* const* lam, float* const* lam_sct) {
   const int ntp = C.tr.ntp, nrk = C.opts.nrk_scal;
   const size_t plane = (size_t)d.mza * d.mwa, qn = plane * ntp;
   const size_t pstride = (plane + 3) & ~(size_t)3;
-  const size_t sb = step_bytes(C);
+  // per step: the transport inputs, and with the limiter the tracers at the step's start
+  const size_t qbytes = (qn * sizeof(float) + 255) & ~(size_t)255;
+  const size_t sb = step_bytes(C) + (W.tracers ? qbytes : 0);
   OG_CHECK(W.seg.alloc(sb * (size_t)W.nchk));
   OG_CHECK(W.lsacc.alloc(qn));
   OG_CHECK(W.planes.alloc(pstride * n));
@@ -196,12 +200,20 @@ int window_adjoint(float* const* lam, float* const* lam_sct) {
         C.dy.div_first = W.chk_div_first[g];
         C.dy.vort_first = W.chk_vort_first[g];
         for (int step = s0; step < s1; ++step) {
+          char* slot = W.seg.p + sb * (size_t)(step - s0);
+          if (W.tracers)
+            OG_CUDA(cudaMemcpyAsync(slot + step_bytes(C), C.tr.q[C.tr.qcur].p, qn * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, s));
           OG_CHECK(glue_run_sequence(C, W.flags, W.tracers));
-          OG_CHECK(copy_step(C, W.seg.p + sb * (size_t)(step - s0), true));
+          OG_CHECK(copy_step(C, slot, true));
         }
       }
       for (int step = s1 - 1; step >= s0; --step) {
-        OG_CHECK(copy_step(C, W.seg.p + sb * (size_t)(step - s0), false));
+        char* slot = W.seg.p + sb * (size_t)(step - s0);
+        OG_CHECK(copy_step(C, slot, false));
+        if (W.tracers)
+          OG_CUDA(cudaMemcpyAsync(C.tr.q[C.tr.qcur].p, slot + step_bytes(C), qn * sizeof(float),
+                                  cudaMemcpyDeviceToDevice, s));
         OG_CHECK(adjoint_core(C, nullptr));
         if (nrk & 1) std::swap(tp.adj_l[0], tp.adj_l[1]);   // the step's result back into adj_l[0]
         k_accumulate<<<cdiv(qn, 256), 256, 0, s>>>(W.lsacc.p, tp.adj_ls.p, qn, first ? 1 : 0);

@@ -267,17 +267,29 @@ class Grid:
                 f"mva={self.mva}, mma={self.mma})")
 
 
-def build_grid(nxp, zz, seed=0):
+def build_grid(nxp, zz, seed=0, numbering="local"):
     """Build a global hex grid with NXP divisions and explicit levels ``zz``.
 
     ``zz`` has mza entries (zz[0] = ground).  Edge orientation (which W is
     ``itab_v%iw(1)``) is drawn from ``seed`` so both signs of ``dirv`` occur.
+    ``numbering`` orders the W points: "local" (cube-face Z-order, nearby
+    cells get nearby ids), "generation" (the order the icosahedral
+    subdivision makes them: the icosahedron's triangles one after another,
+    row by row inside each, as a mesh generator numbers them) or "random"
+    (a seeded random permutation).
     """
     rng = np.random.default_rng(seed)
     g = Grid()
     g.nxp = nxp
     posu, tris = _subdivide(nxp)
-    order = _locality_order(posu)
+    if numbering == "local":
+        order = _locality_order(posu)
+    elif numbering == "generation":
+        order = np.arange(posu.shape[0])
+    elif numbering == "random":
+        order = np.random.default_rng(seed + 99).permutation(posu.shape[0])
+    else:
+        raise ValueError(f"unknown numbering {numbering!r}")
     inv = np.empty_like(order)
     inv[order] = np.arange(order.size)
     posu = posu[order]
