@@ -471,6 +471,45 @@ int olamgpu_timestep_diag(float* smax, double* sums) { return glue_timestep_diag
 
 int olamgpu_set_surface_emission(const float* const* emis) { return emission_set(emis); }
 
+int olamgpu_set_tile_shape(int T, int G, int KS) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  glue_drop_graphs();
+  Transport& tp = C.tp;
+  if (T == 0 && G == 0 && KS == 0) {   // back to the autotuner
+    tp.autotune = true;
+    tp.tuned_ntp = -1;
+    return OLAMGPU_OK;
+  }
+  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8) {
+    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8");
+    return OLAMGPU_E_ARG;
+  }
+  const int order = C.opts.scal_horiz_adv_order;
+  if (C.g.tile_T != T) OG_CHECK(build_tiles(&C.hgrid, C.g, order, C.stream, T));
+  if (C.g.tile_T != T || !tile_shape_fits(C.g, G)) {
+    set_error("tile shape: this grid has no " + std::to_string(T) + "-column tiles of " + std::to_string(G) +
+              " tracers within the shared memory");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
+  C.g.tile_G = G;
+  C.g.tile_KS = KS;
+  tp.autotune = false;
+  return OLAMGPU_OK;
+}
+
+int olamgpu_tile_shape(int* shape, int max, int* cand, float* ms) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return -OLAMGPU_E_STATE; }
+  if (shape) { shape[0] = C.g.tile_T; shape[1] = C.g.tile_G; shape[2] = C.g.tile_KS; }
+  const auto& L = C.tp.tune_log;
+  for (int i = 0; i < (int)L.size() && i < max; ++i) {
+    if (cand) { cand[4 * i] = L[i].T; cand[4 * i + 1] = L[i].G; cand[4 * i + 2] = L[i].KS; cand[4 * i + 3] = L[i].chosen; }
+    if (ms) ms[i] = L[i].ms;
+  }
+  return (int)L.size();
+}
+
 int olamgpu_window_forward(int nsteps, int nchk, unsigned flags) { return window_forward(nsteps, nchk, flags); }
 
 int olamgpu_window_adjoint(float* const* lam, float* const* lam_sct) { return window_adjoint(lam, lam_sct); }

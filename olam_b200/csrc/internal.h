@@ -158,6 +158,7 @@ struct DevGrid {
   DevBuf<float> tile_band;
   DevBuf<int> tile_band_lev;
   int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_order = 0;
+  int tile_G = 64, tile_KS = 1;  // the stage kernel's tracers per block and level chunks
   bool tile_closed = false;      // every neighbourhood column is prognosed
   std::vector<int> h_lpw;        // host copies used at set-up
 };
@@ -198,6 +199,12 @@ struct DevGrid {
 // W[0..TILE_NS), SW, volti / rhos, 1 / rhos, SW - sum W, the vertical flux's
 // coefficients on S(kd-2 .. kd+2) and on S0, wmasc(kd-1), wmasc(kd).
 #define TILE_WR 32
+
+// a shape of the tiled stage kernel: columns per tile, tracers per block,
+// level chunks per tile
+struct TileShape { int T, G, KS; };
+// one candidate the autotuner timed (ms per stage launch)
+struct TuneRec { int T, G, KS, chosen; float ms; };
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)
@@ -250,6 +257,11 @@ struct Transport {
   // the tendencies at lpw after tend0 of each long step
   DevBuf<float> emis;
   bool have_emis = false;
+  // tile-shape autotuner (transport_tile.cu): on while no shape is forced;
+  // tuned_ntp is the tracer count the current shape was chosen for
+  bool autotune = true;
+  int tuned_ntp = -1;
+  std::vector<TuneRec> tune_log;
 };
 
 // Device state and scratch of prog_wrtv_rk (omodel/prog_wrtv_rk.f90).  The
@@ -391,9 +403,11 @@ struct TileHost {
   std::vector<float> band;       // terrain bands (TILE_AW floats each)
   std::vector<int> band_lev;     // the device level at which each band ends
 };
-void make_tiles(const olamgpu_grid* g, int order, TileHost& th);
-int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
-size_t tile_smem_bytes(int T, int nu_max, int mza);
+// T: tile width (0: the widest whose neighbourhoods fit two blocks per SM)
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0);
+int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T = 0);
+// dynamic shared memory of the stage kernel: T columns, nu_max rows of rb bytes
+size_t tile_smem_bytes(int T, int nu_max, int rb);
 
 // dynamics entry points (dynamics.cu)
 int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s);

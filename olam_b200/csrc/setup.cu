@@ -300,15 +300,14 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 
 // ---- tiles of the tiled fused kernel ------------------------------------------
 
-size_t tile_smem_bytes(int T, int nu, int mza) {
+size_t tile_smem_bytes(int T, int nu, int rb) {
   auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
   // k_tile's layout (128-byte aligned parts after aligning the base): two
   // level barriers, two level buffers of U rows (rows in fours) and of the
   // tile columns' weight records, the U rows' global row indices, slot
   // offsets, tile columns, explicit fractions
-  (void)mza;
   const size_t nu4 = (size_t)((nu + 3) & ~3);
-  return 127 + 128 + 2 * al(nu4 * 256) + 2 * al((size_t)T * TILE_WR * 4) + al((size_t)(nu + 3) * 4) +
+  return 127 + 128 + 2 * al(nu4 * rb) + 2 * al((size_t)T * TILE_WR * 4) + al((size_t)(nu + 3) * 4) +
          al((size_t)T * TILE_NS * 4) + al((size_t)T * 4) + (size_t)T * 4;
 }
 
@@ -381,7 +380,7 @@ std::vector<int> locality_order(const olamgpu_grid* g) {
   return cols;
 }
 
-void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req) {
   th = TileHost();
   if (order != 2 && order != 3) return;
   const int nprog = g->nw_prog, mwa = g->mwa;
@@ -429,9 +428,11 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
   };
   int T = 0, numax = 0;
-  // one or two columns for each of the 16 half-warps of a block
+  // one or two columns for each of the 16 half-warps of a block (64 tracers
+  // per block: 256-byte rows), or the width asked for
   const int cand[] = {32, 16};
   for (int Tc : cand) {
+    if (T_req > 0 && Tc != T_req) continue;
     std::fill(stamp.begin(), stamp.end(), -1);
     const int nt = (nprog + Tc - 1) / Tc;
     int nu = 0;
@@ -439,7 +440,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
       gather(t, Tc);
       nu = std::max(nu, (int)U.size());
     }
-    if (nu <= 65535 && tile_smem_bytes(Tc, nu, g->mza) <= TILE_SMEM_MAX) {
+    if (nu <= 65535 && (T_req > 0 || tile_smem_bytes(Tc, nu, 256) <= TILE_SMEM_MAX)) {
       T = Tc; numax = nu;
       break;
     }
@@ -560,12 +561,12 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th) {
   th.order = order;
 }
 
-int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
+int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T) {
   d.tile_T = d.ntiles = d.tile_nu_max = 0;
   d.tile_order = 0;
   d.tile_closed = false;
   TileHost th;
-  make_tiles(g, order, th);
+  make_tiles(g, order, th, T);
   if (!th.T) return OLAMGPU_OK;
   OG_CHECK(upload(d.tile_hdr, th.hdr.data(), th.hdr.size(), s));
   OG_CHECK(upload(d.tile_u, th.ulist.data(), th.ulist.size(), s));

@@ -261,6 +261,13 @@ static int pipelined_step(Context& C, const float* dtlr, const float* rhos_nrk) 
     OG_CUDA(cudaStreamSynchronize(s));   // the host vectors die here
   }
   { OG_PROF("tile_weights", s); OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s)); }
+  if (tp.autotune && tp.tuned_ntp != ntp) {
+    // the shape on this step's inputs: the tracers' device copies and the
+    // step's records (a rotation buffer as the scratch output)
+    OG_CHECK(ensure_q(s));
+    OG_CHECK(tile_autotune(C, tr.q[tr.qcur].p, tr.q[tr.qcur].p, tr.qt.p, tr.q[(tr.qcur + 1) % 3].p, dtlr[nrk - 1]));
+    tr.q_valid = false;   // the per-tracer arrays are what the pipelined step reads
+  }
   // the RK buffer sequence of the batched step
   const int a = tr.qcur;
   int bin[3], bout[3];
@@ -294,7 +301,7 @@ static int pipelined_step(Context& C, const float* dtlr, const float* rhos_nrk) 
       float* OUT = tr.q[bout[istage - 1]].p;
       {
         OG_PROF(istage == 1 ? "tile_stage1" : "tile_stage", s);
-        OG_CHECK(launch_tile_stage(d, tp, IN, A, tr.qt.p, OUT, ntp, istage, nrk, dtr, C.status.p, s, g, 1));
+        OG_CHECK(launch_tile_stage(d, tp, IN, A, tr.qt.p, OUT, ntp, istage, nrk, dtr, C.status.p, s, g, 1, 64));
       }
       {
         OG_PROF("implicit_solve", s);
@@ -377,7 +384,14 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
     if (tp.have_turb)
       for (int n = 0; n < tr.n; ++n)
         if (tr.sgsmix[n]) launch_diffusion(d, tp, CTView{A, ntp, n}, TView{T, ntp, n}, 1, s);
-    if (tiled) { OG_PROF("tile_weights", s); OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s)); }
+    if (tiled) {
+      OG_PROF("tile_weights", s);
+      OG_CHECK(launch_tile_weights(d, tp, rhos_nrk, s));
+      // the stage kernel's shape for this grid and tracer count, chosen on
+      // this step's inputs (the next rotation buffer is scratch)
+      if (tp.autotune && tp.tuned_ntp != ntp)
+        OG_CHECK(tile_autotune(C, A, A, T, tr.q[(a + 1) % 3].p, dtlr[nrk - 1]));
+    }
     int in_b = a, out_b = (a + 1) % 3;
     for (int istage = 1; istage <= nrk; ++istage) {
       const float dtr = dtlr[istage - 1];

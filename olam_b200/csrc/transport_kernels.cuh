@@ -100,9 +100,17 @@ void launch_fused_stage(const DevGrid& d, const Transport& tp, const float* S, c
 // the step's per-(column, level) weight records (into tp.wrec), then a stage
 bool tile_stage_available(const DevGrid& d, const Transport& tp, int order);
 int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cudaStream_t s);
+// grp0 / ngrp_run: the tracer groups of G tracers this launch runs (0, 0:
+// all); G_force: tracers per block (0: the tuned shape's)
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
                       const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr, int* status,
-                      cudaStream_t s, int grp0 = 0, int ngrp_run = 0);
+                      cudaStream_t s, int grp0 = 0, int ngrp_run = 0, int G_force = 0);
+// does the current tile width have a stage kernel of G tracers per block
+// within the shared memory
+bool tile_shape_fits(const DevGrid& d, int G);
+// choose the stage kernel's shape on the step's inputs (S, S0, SCT; OUT is
+// scratch); rebuilds the tile tables when the width changes
+int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT, float* OUT, float dtr);
 
 // copy the columns outside jtw_prog (colsize floats each) from src to dst
 void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, size_t colsize,

@@ -37,6 +37,9 @@
 // staging.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+#include <map>
+
 #include "transport_kernels.cuh"
 #include "tile_common.cuh"
 
@@ -61,6 +64,7 @@ struct WeightArgs {
 
 struct TileArgs {
   int mza, ntp, nrk, istage, kb, ntiles, T, nu_max, mwa;
+  int ks;                           // level chunks per tile (blocks per tile and group)
   const int* __restrict__ lpw;      // lowest prognosed device level of each W column
   int grp0, ngrp;                   // the tracer groups of 64 this launch runs
   float dtr;
@@ -202,25 +206,40 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
 
 // ---- the stage kernel -------------------------------------------------------------
 // Shared memory (in this order; tile_smem_bytes in setup.cu sizes it the
-// same way): two level buffers of U rows (256 B each), two of the tile
+// same way): two level buffers of U rows (4 G bytes each), two of the tile
 // columns' records, the U rows' global row offsets, the slot byte offsets,
 // the tile columns, their explicit fractions.
+// Shape: LPC lanes per column, four tracers per lane, so a block's tracer
+// group is G = 4 LPC tracers (32, 64 or 128) and a warp serves 32 / LPC
+// columns at a time; NC columns per lane group, T = 8 warps x (32 / LPC) x
+// NC columns per tile.  A launch may split the level sweep of a tile into
+// KS chunks run by different blocks (A.ks).
 // OFF: the type of element offsets into the batched arrays -- unsigned when
 // they all fit in 32 bits (fewer address instructions), else long long.
-template <int NC, typename OFF>
-__global__ void __launch_bounds__(TILE_THREADS, 2)
+template <int NC, int LPC, typename OFF>
+__global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
     k_tile(TileArgs A, const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int T = 16 * NC;
-  // the tracer groups of a tile run side by side (its records are read once from HBM)
-  const int ngrp = A.ngrp;
-  const int tile = blockIdx.x / ngrp, grp = A.grp0 + (blockIdx.x - tile * ngrp);
+  constexpr int CPW = 32 / LPC;              // columns a warp serves at once
+  constexpr int TW = TILE_NW * CPW;          // columns a block serves at once
+  constexpr int T = TW * NC;
+  constexpr int G = 4 * LPC;                 // tracers of the block's group
+  constexpr int RB = 4 * G;                  // bytes of a staged row
+  // block order: tile, then level chunk, then tracer group (the groups of a
+  // tile run side by side, so its records are read once from HBM)
+  const int ngrp = A.ngrp, nks = A.ks;
+  const int tile = blockIdx.x / (ngrp * nks);
+  const int rem = blockIdx.x - tile * ngrp * nks;
+  const int ks = rem / ngrp, grp = A.grp0 + (rem - ks * ngrp);
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;   // kb: the lowest floor of any column
+  // this block's levels [klo, khi)
+  const int chunk = (mza - kb + nks - 1) / nks;
+  const int klo = kb + ks * chunk, khi = min(mza, klo + chunk);
   const int nu4 = (nU + 3) & ~3;      // rows gathered four at a time
   auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
-  const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * 256), rbuf = al((size_t)T * TILE_WR * 4);
+  const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * RB), rbuf = al((size_t)T * TILE_WR * 4);
   // 128-byte aligned start (pointer arithmetic on the shared array keeps the
   // accesses shared-memory instructions)
   unsigned char* p = smraw + ((128u - (smem_addr(smraw) & 127u)) & 127u);
@@ -232,7 +251,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
   int* IWT = reinterpret_cast<int*>(p);               p += al((size_t)T * 4);
   float* FEX = reinterpret_cast<float*>(p);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int t0 = grp * 64;
+  const int t0 = grp * G;
+  if (klo >= khi) return;   // an empty chunk (more chunks than levels): uniform per block
 
   // tables of this tile, checked once: every index must address the arrays
   // it is used on (a failure is recorded and the block does nothing)
@@ -242,7 +262,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
       const int c = i / TILE_NS, j = i - c * TILE_NS;
       const int v = __ldg(A.tc + ((size_t)tile * T + c) * TILE_TCW + TILE_TC_SLOT + j);
       if ((unsigned)v >= (unsigned)nU * 256u || (v & 255)) bad = 6;
-      SLOT[i] = v;
+      SLOT[i] = (v >> 8) * RB;
     }
     for (int i = tid; i < nT; i += TILE_THREADS) {
       const int v = __ldg(A.tc + ((size_t)tile * T + i) * TILE_TCW + TILE_TC_IW);
@@ -266,68 +286,71 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
   }
   for (int i = tid; i < nT; i += TILE_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
-  const int seg = min(64, ntp - t0);  // tracers of this group (a multiple of 4)
+  const int seg = min(G, ntp - t0);  // tracers of this group (a multiple of 4)
   // level k into buffer b, completing on barrier b: warp w's lane 0 gathers
-  // the U-row quadruples w, w + 8, ... (TMA, 256 B per row) and the records
-  // of tile columns 4w .. 4w+3
+  // the U-row quadruples w, w + 8, ... (TMA, RB bytes per row) and the
+  // records of tile-column quadruples w, w + 8, ...
   auto stage = [&](int k, int b) {
     if (lane != 0) return;
     const int ng = nu4 >> 2, nr = (nT + 3) >> 2;
     const int myg = warp < ng ? (ng - warp + TILE_NW - 1) / TILE_NW : 0;
-    const int myr = warp < nr ? 1 : 0;
+    const int myr = warp < nr ? (nr - warp + TILE_NW - 1) / TILE_NW : 0;
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * 256 + myr * 4 * TILE_WR * 4));
+    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * RB + myr * 4 * TILE_WR * 4));
     char* Ub = UB + b * ubuf;
     for (int g = warp; g < ng; g += TILE_NW) {
       const int* r = RIDX + 4 * g;
-      tma_gather4(Ub + 4 * g * 256, &tmS, t0, r[0] + k, r[1] + k, r[2] + k, r[3] + k, &BAR[b]);
+      tma_gather4(Ub + 4 * g * RB, &tmS, t0, r[0] + k, r[1] + k, r[2] + k, r[3] + k, &BAR[b]);
     }
-    if (myr) {
-      const int c0 = 4 * warp;
+    for (int q = warp; q < nr; q += TILE_NW) {
+      const int c0 = 4 * q;
       const int y0 = IWT[c0] * mza, y1 = IWT[min(c0 + 1, nT - 1)] * mza;
       const int y2 = IWT[min(c0 + 2, nT - 1)] * mza, y3 = IWT[min(c0 + 3, nT - 1)] * mza;
       tma_gather4(RBB + b * rbuf + c0 * TILE_WR * 4, &tmR, 0, y0 + k, y1 + k, y2 + k, y3 + k, &BAR[b]);
     }
   };
 
-  // a half warp per column (columns cb, cb + 16, ...): lane hl holds tracers
-  // t0 + 4 hl .. + 3; the column's rows kd-2, kd-1, kd+1, kd+2, kd+3 (read
-  // ahead) and its scp0 / sct rows at kd stay in registers
-  const int half = lane >> 4, hl = lane & 15;
+  // LPC lanes per column (columns cb, cb + TW, ...): lane hl of the group
+  // holds tracers t0 + 4 hl .. + 3; the column's rows kd-2, kd-1, kd+1,
+  // kd+2, kd+3 (read ahead) and its scp0 / sct rows at kd stay in registers
+  const int sub = lane / LPC, hl = lane - sub * LPC;
   const bool act = 4 * hl < seg;
-  const int cb = 2 * warp + half;
+  const int cb = CPW * warp + sub;
   F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], s00[NC], st[NC];
   OFF cbase[NC];
   int kbc[NC];   // each column's own floor (lpw): levels below it are not prognosed
-  stage(kb, 0);
+  stage(klo, 0);
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
-    const int c = cb + 16 * n;
+    const int c = cb + TW * n;
     m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = s00[n] = st[n] = zero4();
     cbase[n] = 0;
     kbc[n] = c < nT ? max(kb, __ldg(A.lpw + IWT[c])) : mza;
     if (c < nT && act) {
       cbase[n] = (OFF)IWT[c] * (OFF)mza * (OFF)ntp + (OFF)(t0 + 4 * hl);
-      if (kb + 1 < mza) p1[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 1) * (OFF)ntp));
-      if (kb + 2 < mza) p2[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 2) * (OFF)ntp));
-      if (kb + 3 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 3) * (OFF)ntp));
-      s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)kb * (OFF)ntp));
-      st[n] = ldg4(A.SCT + (cbase[n] + (OFF)kb * (OFF)ntp));
+      // a chunk above the column's floor starts with the rows below it
+      if (klo - 2 >= kbc[n]) m2[n] = ldg4(A.S + (cbase[n] + (OFF)(klo - 2) * (OFF)ntp));
+      if (klo - 1 >= kbc[n]) m1[n] = ldg4(A.S + (cbase[n] + (OFF)(klo - 1) * (OFF)ntp));
+      if (klo + 1 < mza) p1[n] = ldg4(A.S + (cbase[n] + (OFF)(klo + 1) * (OFF)ntp));
+      if (klo + 2 < mza) p2[n] = ldg4(A.S + (cbase[n] + (OFF)(klo + 2) * (OFF)ntp));
+      if (klo + 3 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(klo + 3) * (OFF)ntp));
+      s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)klo * (OFF)ntp));
+      st[n] = ldg4(A.SCT + (cbase[n] + (OFF)klo * (OFF)ntp));
     }
   }
   __syncthreads();   // the explicit fractions
   // a level's copies are waited for at most TILE_WAIT_POLLS polls; a block
   // whose copies never complete records it and stops at the level's end
   int failed = 0;
-  for (int kd = kb; kd < mza; ++kd) {
-    const int lv = kd - kb, cur = lv & 1;
+  for (int kd = klo; kd < khi; ++kd) {
+    const int lv = kd - klo, cur = lv & 1;
     if (!mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS)) failed = 1;
-    if (kd + 1 < mza) stage(kd + 1, cur ^ 1);
+    if (kd + 1 < khi) stage(kd + 1, cur ^ 1);
     const char* Ul = UB + cur * ubuf + hl * 16;
     const float* Rc = reinterpret_cast<const float*>(RBB + cur * rbuf);
 #pragma unroll
     for (int n = 0; n < NC; ++n) {
-      const int c = cb + 16 * n;
+      const int c = cb + TW * n;
       if (c >= nT) continue;
       // the column's window holds no level below its floor
       if (kd == kbc[n]) m2[n] = m1[n] = zero4();
@@ -336,7 +359,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
       const float4 r6 = reinterpret_cast<const float4*>(rc)[6];   // beta0 .. beta3
       const float2 r7 = reinterpret_cast<const float2*>(rc)[14];  // beta4, omega
       const float fx = FEX[c];
-      const F4 s0 = lds4(Ul, c * 256);
+      const F4 s0 = lds4(Ul, c * RB);
       // horizontal: sum_j W_j S(slot j) + D S - SW S0
       F4 fd = zero4();
       const int* sl = SLOT + c * TILE_NS;
@@ -418,15 +441,34 @@ bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
   return (d.tile_T == 16 || d.tile_T == 32) && d.tile_order == order;
 }
 
+// the stage kernel of a tile shape (T columns, G tracers per block)
+using TileKern = void (*)(TileArgs, const CUtensorMap, const CUtensorMap);
+static TileKern tile_kernel(int T, int G, bool off32) {
+  if (T == 32 && G == 64) return off32 ? k_tile<2, 16, unsigned> : k_tile<2, 16, long long>;
+  if (T == 32 && G == 32) return off32 ? k_tile<1, 8, unsigned> : k_tile<1, 8, long long>;
+  if (T == 16 && G == 64) return off32 ? k_tile<1, 16, unsigned> : k_tile<1, 16, long long>;
+  if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned> : k_tile<2, 32, long long>;
+  return nullptr;
+}
+
+// the largest dynamic shared memory a block may use
+#define TILE_SMEM_LIMIT (227 * 1024)
+
+bool tile_shape_fits(const DevGrid& d, int G) {
+  return tile_kernel(d.tile_T, G, true) && tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G) <= TILE_SMEM_LIMIT;
+}
+
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
                       const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr, int* status,
-                      cudaStream_t s, int grp0, int ngrp_run) {
+                      cudaStream_t s, int grp0, int ngrp_run, int G_force) {
   if (tp.wrec.n != (size_t)d.mza * d.mwa * TILE_WR) {
     set_error("tile stage: the weight records of the step were not formed");
     return OLAMGPU_E_STATE;
   }
+  const int G = G_force > 0 ? G_force : d.tile_G;
+  const int KS = std::max(1, d.tile_KS);
   TileArgs A;
-  A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1;
+  A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1; A.ks = KS;
   A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.mwa = d.mwa;
   A.dtr = dtr; A.lpw = d.lpw.p;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
@@ -434,26 +476,119 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   A.ff = tp.ff.p; A.wrec = tp.wrec.p;
   A.S = S; A.S0 = S0; A.SCT = SCT; A.OUT = OUT;
   A.err = status;
-  const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, d.mza);
-  const int ngrp_all = (ntp + 63) / 64;
+  const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G);
+  const int ngrp_all = (ntp + G - 1) / G;
   if (ngrp_run <= 0) { grp0 = 0; ngrp_run = ngrp_all; }
   if (grp0 < 0 || grp0 + ngrp_run > ngrp_all) { set_error("tile stage: tracer groups out of range"); return OLAMGPU_E_ARG; }
   A.grp0 = grp0; A.ngrp = ngrp_run;
-  const unsigned nblk = (unsigned)d.ntiles * (unsigned)ngrp_run;
+  const unsigned nblk = (unsigned)d.ntiles * (unsigned)ngrp_run * (unsigned)KS;
   // element offsets in 32 bits when every array of the batched layout fits
   const bool off32 = (double)d.mwa * d.mza * ntp < 4294967296.0;
+  const TileKern kern = tile_kernel(d.tile_T, G, off32);
+  if (!kern || smem > TILE_SMEM_LIMIT) {
+    set_error("tile stage: no kernel for " + std::to_string(d.tile_T) + "-column tiles of " + std::to_string(G) +
+              " tracers within the shared memory");
+    return OLAMGPU_E_UNSUPPORTED;
+  }
   alignas(64) CUtensorMap tmS, tmR;
-  OG_CHECK(row_map(&tmS, S, ntp, (size_t)d.mwa * d.mza, 64));
+  OG_CHECK(row_map(&tmS, S, ntp, (size_t)d.mwa * d.mza, G));
   OG_CHECK(row_map(&tmR, tp.wrec.p, TILE_WR, (size_t)d.mwa * d.mza, TILE_WR));
-  auto go = [&](auto kern) -> int {
-    OG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<nblk, TILE_THREADS, smem, s>>>(A, tmS, tmR);
-    return OLAMGPU_OK;
-  };
-  if (d.tile_T == 32) OG_CHECK(off32 ? go(k_tile<2, unsigned>) : go(k_tile<2, long long>));
-  else OG_CHECK(off32 ? go(k_tile<1, unsigned>) : go(k_tile<1, long long>));
+  OG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<nblk, TILE_THREADS, smem, s>>>(A, tmS, tmR);
   OG_LAUNCHED();
   return OLAMGPU_OK;
+}
+
+// ---- tile-shape autotuner --------------------------------------------------------
+// The stage kernel's shape -- columns per tile (T), tracers per block (G:
+// LPC lanes per column) and level chunks per tile (KS, the levels a block's
+// threads sweep) -- is chosen on the actual grid, tracer count and
+// reconstruction order: each candidate the shared memory admits runs the
+// stage on the step's own inputs a few times, and the fastest is kept.  The
+// choice is cached per (grid, tracer count, order) for the process.
+struct ShapeKey {
+  unsigned long long h;
+  bool operator<(const ShapeKey& o) const { return h < o.h; }
+};
+static std::map<ShapeKey, TileShape> g_shape_cache;
+
+static unsigned long long shape_key(const olamgpu_grid* g, int ntp, int order) {
+  unsigned long long h = 1469598103934665603ull;   // FNV-1a over the values that shape the tiles
+  auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ull; };
+  mix((unsigned)g->mza); mix((unsigned)g->mwa); mix((unsigned)g->nw_prog); mix((unsigned)ntp); mix((unsigned)order);
+  for (int j = 0; j < g->nw_prog; ++j) mix((unsigned)g->jtw_prog[j]);
+  for (int i = 0; i < g->mwa; ++i) mix((unsigned)g->lpw[i]);
+  return h;
+}
+
+int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT, float* OUT, float dtr) {
+  DevGrid& d = C.g;
+  Transport& tp = C.tp;
+  cudaStream_t s = C.stream;
+  const int ntp = C.tr.ntp, nrk = C.opts.nrk_scal, order = C.opts.scal_horiz_adv_order;
+  tp.tune_log.clear();
+  const ShapeKey key{shape_key(&C.hgrid, ntp, order)};
+  auto use = [&](const TileShape& sh) -> int {
+    if (d.tile_T != sh.T) OG_CHECK(build_tiles(&C.hgrid, d, order, s, sh.T));
+    d.tile_G = sh.G;
+    d.tile_KS = sh.KS;
+    return OLAMGPU_OK;
+  };
+  auto it = g_shape_cache.find(key);
+  if (it != g_shape_cache.end()) {
+    OG_CHECK(use(it->second));
+    tp.tuned_ntp = ntp;
+    return OLAMGPU_OK;
+  }
+  cudaEvent_t e0, e1;
+  OG_CUDA(cudaEventCreate(&e0));
+  OG_CUDA(cudaEventCreate(&e1));
+  TileShape best{0, 0, 0};
+  float best_ms = 0.f;
+  prof_suspend(true);
+  int rc = OLAMGPU_OK;
+  const int Ts[2] = {32, 16};
+  for (int T : Ts) {
+    if (d.tile_T != T) {
+      rc = build_tiles(&C.hgrid, d, order, s, T);
+      if (rc != OLAMGPU_OK || d.tile_T != T) { rc = OLAMGPU_OK; continue; }   // no tables of this width
+    }
+    const int Gs[2] = {T == 32 ? 64 : 64, T == 32 ? 32 : 128};
+    for (int G : Gs) {
+      if (!tile_shape_fits(d, G)) continue;
+      for (int KS = 1; KS <= 2; ++KS) {
+        d.tile_G = G;
+        d.tile_KS = KS;
+        float ms = 1e30f;
+        for (int r = 0; r < 4 && rc == OLAMGPU_OK; ++r) {
+          cudaEventRecord(e0, s);
+          rc = launch_tile_stage(d, tp, S, S0, SCT, OUT, ntp, nrk, nrk, dtr, C.status.p, s, 0, 0, 0);
+          cudaEventRecord(e1, s);
+          if (rc != OLAMGPU_OK) break;
+          cudaEventSynchronize(e1);
+          float t = 0.f;
+          cudaEventElapsedTime(&t, e0, e1);
+          if (r > 0) ms = std::min(ms, t);   // the first run warms up
+        }
+        if (rc != OLAMGPU_OK) break;
+        tp.tune_log.push_back({T, G, KS, 0, ms});
+        if (!best.T || ms < best_ms) { best = TileShape{T, G, KS}; best_ms = ms; }
+      }
+      if (rc != OLAMGPU_OK) break;
+    }
+    if (rc != OLAMGPU_OK) break;
+  }
+  prof_suspend(false);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  OG_CHECK(rc);
+  if (!best.T) { set_error("tile autotune: no shape runs on this grid"); return OLAMGPU_E_UNSUPPORTED; }
+  for (auto& r : tp.tune_log)
+    if (r.T == best.T && r.G == best.G && r.KS == best.KS) r.chosen = 1;
+  OG_CHECK(use(best));
+  g_shape_cache[key] = best;
+  tp.tuned_ntp = ntp;
+  return check_device_status();
 }
 
 }  // namespace olamgpu

@@ -30,6 +30,7 @@ EXPORTS = [
     "olamgpu_set_scalars_bottom", "olamgpu_diagvel_t3d", "olamgpu_tracer_maxmin", "olamgpu_mass_sums",
     "olamgpu_timestep", "olamgpu_timestep_diag", "olamgpu_set_halo",
     "olamgpu_set_surface_emission", "olamgpu_window_forward", "olamgpu_window_adjoint",
+    "olamgpu_set_tile_shape", "olamgpu_tile_shape",
 ]
 
 
@@ -83,6 +84,8 @@ def load():
     lib.olamgpu_set_surface_emission.argtypes = [C.POINTER(abi.c_float_p)]
     lib.olamgpu_window_forward.argtypes = [C.c_int, C.c_int, C.c_uint]
     lib.olamgpu_window_adjoint.argtypes = [C.POINTER(abi.c_float_p), C.POINTER(abi.c_float_p)]
+    lib.olamgpu_set_tile_shape.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.olamgpu_tile_shape.argtypes = [abi.c_int_p, C.c_int, abi.c_int_p, abi.c_float_p]
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
             getattr(lib, name).restype = C.c_int
@@ -222,6 +225,21 @@ class OlamGpu:
         self._emis = [None if e is None else np.ascontiguousarray(e, dtype=np.float32) for e in emis]
         arr = (abi.c_float_p * len(self._emis))(*[abi.ptr(e, C.c_float) for e in self._emis])
         check(self.lib.olamgpu_set_surface_emission(arr))
+
+    def set_tile_shape(self, T=0, G=0, KS=0):
+        check(self.lib.olamgpu_set_tile_shape(int(T), int(G), int(KS)))
+
+    def tile_shape(self, maxn=32):
+        """((T, G, KS) in use, [(T, G, KS, chosen, ms) of the last tuning])."""
+        shape = np.zeros(3, np.int32)
+        cand = np.zeros(4 * maxn, np.int32)
+        ms = np.zeros(maxn, np.float32)
+        n = self.lib.olamgpu_tile_shape(abi.ptr(shape, C.c_int), maxn, abi.ptr(cand, C.c_int), abi.ptr(ms, C.c_float))
+        if n < 0:
+            check(-n)
+        log = [(int(cand[4 * i]), int(cand[4 * i + 1]), int(cand[4 * i + 2]), int(cand[4 * i + 3]), float(ms[i]))
+               for i in range(min(n, maxn))]
+        return tuple(int(x) for x in shape), log
 
     def window_forward(self, nsteps, nchk, flags=0):
         check(self.lib.olamgpu_window_forward(int(nsteps), int(nchk), int(flags)))
