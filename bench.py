@@ -69,6 +69,16 @@ def parse():
     p.add_argument("--long-step-only", action="store_true",
                    help="time only the long step (olamgpu_timestep) and print its object")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--numbering", default="local", choices=["local", "generation", "random"],
+                   help="W-point numbering of the grid (the library orders its tiles itself)")
+    p.add_argument("--no-window", action="store_true")
+    p.add_argument("--window-only", action="store_true",
+                   help="time only the checkpointed window adjoint and print its object")
+    p.add_argument("--win-nxp", type=int, default=100)
+    p.add_argument("--win-ntr", type=int, default=32)
+    p.add_argument("--win-steps", type=int, default=24)
+    p.add_argument("--win-chk", type=int, default=6)
+    p.add_argument("--win-monot", type=int, default=0)
     return p.parse_args()
 
 
@@ -128,7 +138,7 @@ class Clocks:
 def make_case(a):
     from olam_b200.synth.grid import build_grid, stretched_levels
     from olam_b200.synth.state import fast_lognormal_tracers, transport_state
-    g = build_grid(a.nxp, stretched_levels(a.nlev, 100.0, 30000.0), seed=2)
+    g = build_grid(a.nxp, stretched_levels(a.nlev, 100.0, 30000.0), seed=2, numbering=a.numbering)
     st = transport_state(g, a.dt, 0, seed=2)
     if a.terrain > 0:
         from olam_b200.synth.grid import with_terrain
@@ -407,6 +417,96 @@ def bench_long_step(g, tr, a, max_over_ranks):
     return out
 
 
+def bench_window(a, max_over_ranks):
+    """The adjoint of tracer transport over a window of long steps: NXP=100
+    (100,002 columns), 60 levels, 32 FP32 tracers with a seeded surface
+    emission each, 24 long steps of 120 s of the whole core (balanced jet,
+    4 acoustic RK3 steps) with checkpoints every 6 steps; the loss is a
+    seeded weighted sum of the tracers after the window at 200 receptor
+    cells in the lowest 3 levels.  Device time of olamgpu_window_forward
+    (the 24 steps and their checkpoints) and of olamgpu_window_adjoint
+    (per segment: the checkpoint restored, the dynamics run again, the
+    one-step adjoints in reverse).  The unlimited step is linear in the
+    tracers and emissions for fixed winds, so J = <dJ/dx0, x0> + <dJ/dE, E>
+    exactly: a size-independent check of the gradient at full size."""
+    import torch
+    from olam_b200 import abi
+    from olam_b200.lib import HostState, OlamGpu
+    from olam_b200.synth.grid import build_grid, stretched_levels
+    from olam_b200.synth.state import dynamics_state, fast_lognormal_tracers
+    g = build_grid(a.win_nxp, stretched_levels(a.nlev, 100.0, 30000.0), seed=4)
+    ds = dynamics_state(g, seed=4)
+    tr = fast_lognormal_tracers(g, a.win_ntr, seed=31, as_list=True)
+    rng = np.random.default_rng(41)
+    emis = [(1e-13 * rng.random(g.mwa)).astype(np.float32) for _ in range(a.win_ntr)]
+    for e in emis:
+        e[0] = 0.0
+    wz = lambda: np.zeros((g.mwa, g.mza), np.float32)   # noqa: E731
+    hs = HostState(rho=ds.rho, press=ds.press, thil=ds.thil, wc=ds.wc, wmc=ds.wmc, vxe=ds.vxe, vye=ds.vye,
+                   vze=ds.vze, vmc=ds.vmc, vc=ds.vc, vmasc=np.zeros((g.mva, g.mza), np.float32), wmasc=wz(),
+                   alpha_press=ds.alpha_press, pwfac=ds.pwfac, pvfac=ds.pvfac, thilt=wz(), vmxet=wz(),
+                   vmyet=wz(), vmzet=wz(), vmt=np.zeros((g.mva, g.mza), np.float32))
+    opts = abi.make_opts(120.0, nacoust=4, nrk_scal=3, iscal_monot=a.win_monot)
+    dev = OlamGpu(abi.FortranGrid(g), opts, hs)
+    out = {"workload": f"window adjoint: NXP={a.win_nxp} ({g.mwa - 1} columns), {a.nlev} levels, "
+                       f"{a.win_ntr} tracers with surface emission, {a.win_steps} long steps of 120 s "
+                       f"(nacoust 4, acoustic RK3, tracer RK3, iscal_monot {a.win_monot}), "
+                       f"checkpoints every {a.win_chk} steps; loss: 200 receptor cells in the lowest 3 levels"}
+    try:
+        var_p = [t.copy() for t in tr]
+        var_t = [np.zeros_like(t) for t in tr]
+        dev.register_scalars(var_p, var_t)
+        dev.set_surface_emission(emis)
+        dev.set_coherence(abi.RESIDENT)
+        dev.timestep(abi.TS_GRAPH)           # buffers, tile shape, graphs: then back to the start
+        dev.sync_to_device(abi.F_ALL)
+        for t, t0 in zip(var_p, tr):
+            t[...] = t0
+        dev.sync_to_device(abi.F_SCALARS)
+        torch.cuda.synchronize()
+        stream = torch.cuda.ExternalStream(dev.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dev.window_forward(a.win_steps, a.win_chk, abi.TS_GRAPH)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms = max_over_ranks(e0.elapsed_time(e1))
+        dev.sync_to_host(abi.F_SCALARS)
+        # receptors: 200 cells in the lowest three levels, a seeded weight per tracer
+        rr = np.random.default_rng(43)
+        iw = rr.integers(1, g.mwa, 200)
+        kk = g.lpw[iw] - 1 + rr.integers(0, 3, 200)
+        w = rr.standard_normal((a.win_ntr, 200))
+        lam = [np.zeros((g.mwa, g.mza), np.float32) for _ in range(a.win_ntr)]
+        J = 0.0
+        for n in range(a.win_ntr):
+            np.add.at(lam[n], (iw, kk), w[n].astype(np.float32))
+            J += float((lam[n].astype(np.float64) * var_p[n]).sum())
+        dev.profile(True, reset=True)
+        g0, gs = dev.window_adjoint(lam)
+        prof = dev.profile_read()
+        dev.profile(False, reset=True)
+        adj_ms = max_over_ranks(prof["window_adjoint"][0])
+        lin = 0.0
+        lpw0 = g.lpw - 1
+        for n in range(a.win_ntr):
+            lin += float((g0[n].astype(np.float64) * np.asarray(tr[n], np.float64)).sum())
+            lin += float((gs[n][np.arange(g.mwa), lpw0].astype(np.float64) * emis[n]).sum())
+        out.update({
+            "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+            "recompute_ms": prof.get("window_recompute", (0.0, 0))[0],
+            "adjoint_steps_ms": prof.get("adj_stage", (0.0, 0))[0] + prof.get("adj_records", (0.0, 0))[0]
+            + prof.get("adj_implicit", (0.0, 0))[0],
+            "loss": J, "loss_from_gradient": lin,
+            "euler_relerr": abs(lin - J) / abs(J) if J else None,
+            "check": "J(x0, E) = <dJ/dx0, x0> + <dJ/dE, E> for the unlimited (linear) step"
+                     if a.win_monot == 0 else "limited step: no linear identity",
+        })
+    finally:
+        dev.close()
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -422,6 +522,11 @@ def main():
         out = bench_long_step(g, tr, a, lambda x: x)
         if rank == 0:
             print(json.dumps({"long_step": out}), flush=True)
+        return 0
+    if a.window_only:
+        out = bench_window(a, lambda x: x)
+        if rank == 0:
+            print(json.dumps({"window_adjoint": out}), flush=True)
         return 0
     fg = abi.FortranGrid(g)
     opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
@@ -479,6 +584,11 @@ def main():
     ms = e0.elapsed_time(e1)
     launches = dev.launch_count()
     prof = dev.profile_read()
+    used, tlog = dev.tile_shape()
+    tile_shape = {"T": used[0], "G": used[1], "KS": used[2],
+                  "candidates_ms_per_stage": [{"T": r[0], "G": r[1], "KS": r[2], "ms": r[4]} for r in tlog],
+                  "note": "columns per tile, tracers per block, level chunks per tile; chosen by the "
+                          "library's autotuner on the first step"}
     dev.profile(False, reset=True)
     clk = clocks.stop()
     barrier()
@@ -519,7 +629,7 @@ def main():
             traffic = None
 
     # ---- plain one-kernel-per-tracer form on the same device data
-    plain = None
+    plain, plain_passes = None, None
     if not a.no_plain:
         dev.set_transport_form(abi.TRANSPORT_PLAIN)
         dev.scalar_transport_rk(None)
@@ -534,6 +644,26 @@ def main():
         torch.cuda.synchronize()
         pms = max_over_ranks(p0.elapsed_time(p1) / ksteps)
         plain = ws * nupd / (pms * 1e-3)
+        # each pass's time (CUDA events around every launch, one more step)
+        # against the bytes it moves at least: every array it reads or writes
+        # once (cells: prognostic cells; faces: V-face levels)
+        dev.profile(True, reset=True)
+        dev.scalar_transport_rk(None)
+        pprof = dev.profile_read()
+        dev.profile(False, reset=True)
+        cells = prognostic_cells(g)
+        faces = int((g.mza + 1 - g.lpv[1:].astype(np.int64)).sum())
+        i2d = 5 if a.order == 3 else 2
+        pbytes = {"pass_grad": (4 + 4 * i2d) * cells,
+                  "pass_vflux": (4 + 4 * i2d) * cells + 8 * faces,
+                  "pass_wcol": 28 * cells + 8 * faces}
+        plain_passes = {}
+        for nm, b in pbytes.items():
+            if nm in pprof and pprof[nm][1]:
+                pm = pprof[nm][0] / pprof[nm][1]
+                plain_passes[nm] = {"ms_per_launch": pm, "launches_per_step": pprof[nm][1],
+                                    "bytes_per_launch": b, "achieved_gbs": b / (pm * 1e-3) / 1e9,
+                                    "frac": b / (pm * 1e-3) / 1e9 / peak}
         dev.set_transport_form(abi.TRANSPORT_FUSED)
 
     # ---- the batched form with one column per block, for comparison
@@ -600,6 +730,10 @@ def main():
     if not a.no_long_step:
         long_step = bench_long_step(g, tr, a, max_over_ranks)
 
+    window = None
+    if not a.no_window:
+        window = bench_window(a, max_over_ranks)
+
     cpu, errors = None, None
     if report:
         cpu = cpu_sample(g, st, init_sample, a, a.cpu_seconds, keep=True)
@@ -622,11 +756,14 @@ def main():
                          "peak_source": peak_src, "kernel": f"{kname} ({pre})",
                          "kernel_ms_per_launch": (tot_ms / nl) if nl else None},
             "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+            "tile_shape": tile_shape,
             "plain_gpu_value": plain,
+            "plain_passes": plain_passes,
             "fused_over_plain": (value / plain) if plain else None,
             "fused_column_value": column,
             "e2e": e2e,
             "adjoint": adjoint,
+            "window_adjoint": window,
             "long_step": long_step,
             "cpu_baseline": cpu,
             "errors": errors,

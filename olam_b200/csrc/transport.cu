@@ -147,7 +147,14 @@ static void passes_stage(Context& C, CTView in, CTView scp0, CTView sct, TView o
   const bool monot = limited_stage && C.opts.iscal_monot == 1;
   { OG_PROF("pass_grad", s); launch_grad(d, in, C.tp.gx.p, nt, order, !monot, s); }
   { OG_PROF("pass_vflux", s); launch_vflux(d, C.tp, in, scp0, C.tp.gx.p, nt, order, monot, mode, limited_stage, s); }
-  { OG_PROF("pass_wcol", s); launch_wcol(d, C.tp, in, scp0, sct, rhos, out, nt, istage, nrk, dtr, mode, limited_stage, s); }
+  if (limited_stage) {
+    // the limiters' scale factors run down each column (a thread per column)
+    OG_PROF("pass_wcol", s);
+    launch_wcol(d, C.tp, in, scp0, sct, rhos, out, nt, istage, nrk, dtr, mode, limited_stage, s);
+  } else {
+    OG_PROF("pass_wcol", s);
+    launch_wcell(d, C.tp, in, scp0, sct, rhos, out, nt, istage, nrk, dtr, s);
+  }
   if (limited_stage) {
     { OG_PROF("pass_vapply", s); launch_vapply(d, C.tp, nt, mode, s); }
     { OG_PROF("pass_tend", s); launch_tend(d, C.tp, in, scp0, rhos, out, nt, istage, nrk, dtr, mode, s); }

@@ -664,6 +664,72 @@ __global__ void k_wcol(WcolArgs A) {
   }
 }
 
+// pass 3 of an unlimited stage, one thread per (level, column, tracer) with
+// the level fastest for one tracer (nt = 1: a column's levels are adjacent,
+// so every load of a warp is coalesced).  scalar_w_column
+// (scalar_transport_rk.F90:537-612) has no recurrence in k: the face values
+// scp_upw(k-1), scp_upw(k) come from grad_z_quadratic of the upwind level,
+// i.e. from scp(k-2 .. k+2), and each cell's update is independent.
+__global__ void k_wcell(WcolArgs A) {
+  const GridK& g = A.g;
+  const int mza = g.mza;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)A.nprog * mza * A.nt) return;
+  int t, kd, j;
+  if (A.nt == 1) { t = 0; kd = (int)(i % mza); j = (int)(i / mza); }
+  else { t = (int)(i % A.nt); const size_t r = i / A.nt; kd = (int)(r % mza); j = (int)(r / mza); }
+  const int iw = A.prog[j];
+  const int kb = g.lpw[iw];
+  if (kd < kb) return;   // written by the thread of level kb
+  const int np = g.npoly[iw];
+  const float fimpl = A.ff[(size_t)iw * A.nrk + A.istage - 1];
+  const float fexpl = 1.0f - fimpl;
+  const float* wm = A.wmasc + (size_t)iw * mza;
+  auto S = [&](int k) { return A.scp.base[((size_t)iw * mza + k) * A.scp.ld + A.scp.t0 + t]; };
+  // scp_upw at the top face of level f (f = kb-1 .. mza-1)
+  auto upw = [&](int f) -> float {
+    if (f == kb - 1) return S(kb);        // scp_upw(kb-1) = scp(kb)
+    if (f == mza - 1) return S(mza - 1);  // scp_upw(mza) = scp(mza)
+    float sb, st;
+    if (wm[f] < 0.f) {                    // scpb(f+1) from (f, f+1, f+2)
+      zrec(g.a_w, mza, f + 1, kb, S(f), S(f + 1), (f + 2 < mza) ? S(f + 2) : 0.f, 0.f, false, false, sb, st);
+      return sb;
+    }
+    zrec(g.a_w, mza, f, kb, (f - 1 >= kb) ? S(f - 1) : 0.f, S(f), S(f + 1), 0.f, false, false, sb, st);
+    return st;
+  };
+  const size_t ntz = (size_t)A.nt;
+  const float s00 = A.scp0.base[((size_t)iw * mza + kd) * A.scp0.ld + A.scp0.t0 + t];
+  float fd = 0.f;
+  for (int n = 0; n < np; ++n) {
+    const int iv = g.w_ev[iw * 8 + n];
+    if (kd < g.lpv[iv]) continue;
+    fd = fd + g.w_dirv[iw * 8 + n] * A.vmasc[(size_t)iv * mza + kd] * (A.upv[((size_t)iv * mza + kd) * ntz + t] - s00);
+  }
+  fd = fd + fexpl * (wm[kd - 1] * (upw(kd - 1) - s00) - wm[kd] * (upw(kd) - s00));
+  const float sctv = A.sct.base[((size_t)iw * mza + kd) * A.sct.ld + A.sct.t0 + t];
+  const float o = s00 + A.dtr * (sctv + g.volti[(size_t)iw * mza + kd] * fd) / A.rhos[(size_t)iw * mza + kd];
+  float* out = A.out.base + (size_t)iw * mza * A.out.ld + A.out.t0 + t;
+  out[(size_t)kd * A.out.ld] = o;
+  if (kd == kb)
+    for (int k = 0; k < kb; ++k) out[(size_t)k * A.out.ld] = o;
+}
+
+void launch_wcell(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct, const float* rhos,
+                  TView out, int nt, int istage, int nrk, float dtr, cudaStream_t s) {
+  WcolArgs A;
+  A.g = gridk(d);
+  A.prog = d.jtw_prog.p; A.nprog = d.nw_prog;
+  A.scp = scp; A.scp0 = scp0; A.sct = sct; A.rhos = rhos;
+  A.vmasc = tp.vmasc.p; A.wmasc = tp.wmasc.p; A.ff = tp.ff.p;
+  A.upv = tp.upv.p; A.sfv = nullptr; A.scale = nullptr; A.upw = nullptr;
+  A.out = out; A.nt = nt; A.istage = istage; A.nrk = nrk; A.dtr = dtr;
+  A.mode = nullptr;
+  const size_t n = (size_t)d.nw_prog * d.mza * nt;
+  k_wcell<<<cdiv(n, 256), 256, 0, s>>>(A);
+  OG_LAUNCHED();
+}
+
 void launch_wcol(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct,
                  const float* rhos, TView out, int nt, int istage, int nrk, float dtr,
                  const int* mode, bool anylim, cudaStream_t s) {

@@ -87,6 +87,9 @@ void launch_vflux(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0
 void launch_wcol(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct,
                  const float* rhos, TView out, int nt, int istage, int nrk, float dtr,
                  const int* mode, bool anylim, cudaStream_t s);
+// pass 3 of an unlimited stage, a thread per cell (coalesced in k)
+void launch_wcell(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct, const float* rhos,
+                  TView out, int nt, int istage, int nrk, float dtr, cudaStream_t s);
 void launch_vapply(const DevGrid& d, const Transport& tp, int nt, const int* mode, cudaStream_t s);
 void launch_tend(const DevGrid& d, const Transport& tp, CTView scp_in, CTView scp0, const float* rhos,
                  TView out, int nt, int istage, int nrk, float dtr, const int* mode, cudaStream_t s);
