@@ -162,6 +162,8 @@ static void release_all() {
   for (auto* b : fb) b->release();
   d.ew_order = 0;
   d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
+  d.tile_G = 64;
+  d.tile_KS = 1;
   Tracers& tr = C.tr;
   for (size_t i = 0; i < tr.p.size(); ++i) {
     tr.p[i].release();
@@ -193,6 +195,9 @@ static void release_all() {
   tp.adj_ptab2.release();
   tp.have_turb = false;
   tp.have_emis = false;
+  tp.autotune = true;
+  tp.tuned_ntp = -1;
+  tp.tune_log.clear();
   transport_release_pipeline();
   halo_release();
   glue_release();
