@@ -126,6 +126,36 @@ def make_halo(send, recv, fn, host_staged=True, vm=None):
         except Exception:   # an exception must not cross the C frame
             return 1
 
+    return _halo_struct(ranks, rk, ns, nr, sc, rc, hook, host_staged, vm)
+
+
+def make_halo_device(send, recv, fn, vm=None):
+    """A Halo whose hook gets the library's DEVICE buffers and stream:
+    fn(ranks, sendbufs, recvbufs, stream) -> int, each buffer a pair
+    (device pointer as int, float count), stream a cudaStream_t as int.
+    The hook orders its transfers on that stream (CUDA-aware MPI, NCCL
+    send/recv); the library unpacks after it returns, on the same stream."""
+    ranks = sorted(set(send) | set(recv) | (set().union(*[set(d) for d in vm]) if vm else set()))
+    rk = np.array(ranks, np.int32)
+    ns = np.array([len(send.get(r, ())) for r in ranks], np.int32)
+    nr = np.array([len(recv.get(r, ())) for r in ranks], np.int32)
+    sc = np.ascontiguousarray(np.concatenate([np.asarray(send.get(r, []), np.int64) for r in ranks]
+                                             + [np.zeros(0, np.int64)]) + 1, np.int32)
+    rc = np.ascontiguousarray(np.concatenate([np.asarray(recv.get(r, []), np.int64) for r in ranks]
+                                             + [np.zeros(0, np.int64)]) + 1, np.int32)
+
+    def hook(user, nnb, rank, sbuf, scount, rbuf, rcount, stream):
+        try:
+            sb = [(C.cast(sbuf[i], C.c_void_p).value or 0, int(scount[i])) for i in range(nnb)]
+            rb = [(C.cast(rbuf[i], C.c_void_p).value or 0, int(rcount[i])) for i in range(nnb)]
+            return int(fn([rank[i] for i in range(nnb)], sb, rb, stream or 0))
+        except Exception:   # an exception must not cross the C frame
+            return 1
+
+    return _halo_struct(ranks, rk, ns, nr, sc, rc, hook, False, vm)
+
+
+def _halo_struct(ranks, rk, ns, nr, sc, rc, hook, host_staged, vm):
     h = Halo()
     h.nnb = len(ranks)
     h.rank, h.nsend, h.nrecv = ptr(rk, C.c_int), ptr(ns, C.c_int), ptr(nr, C.c_int)

@@ -431,6 +431,75 @@ struct WrtSmem {
   float *b15, *rkx, *rky, *rkz, *b31, *b32, *b33, *dwm, *wmf;
 };
 
+// The W system of prog_wrt_begs, b31(k) x(k-1) + b32(k) x(k) + b33(k) x(k+1)
+// = dwm(k) for k = k0 .. k1, which the reference solves with the Thomas
+// algorithm (tridiffo, outils/tridiag_lib.f90:10-36), solved here by
+// parallel cyclic reduction over a warp: row i = k - k0 lives in lane
+// i % 32 (R rows per lane, i = lane + 32 r); in a step of stride s every row
+// eliminates its couplings to rows i - s and i + s with those rows' current
+// equations (rows outside the system act as identity rows), so after
+// ceil(log2(n)) steps each row holds x(k) = d / b.
+template <int R>
+__device__ __forceinline__ void warp_tridiag(WrtSmem& m, int k0, int k1, int lane) {
+  const int n = k1 - k0 + 1;
+  float a[R], b[R], c[R], d[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = lane + 32 * r;
+    const bool in = i < n;
+    a[r] = in && i > 0 ? m.b31[k0 + i] : 0.f;
+    b[r] = in ? m.b32[k0 + i] : 1.f;
+    c[r] = in && i < n - 1 ? m.b33[k0 + i] : 0.f;
+    d[r] = in ? m.dwm[k0 + i] : 0.f;
+  }
+  for (int s = 1; s < n; s <<= 1) {
+    float am[R], bm[R], cm[R], dm[R], ap[R], bp[R], cp[R], dp[R];
+    if (s < 32) {
+      const int src_m = (lane - s) & 31, src_p = (lane + s) & 31;
+      const bool wrap_m = lane < s, wrap_p = lane + s >= 32;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        // the equations of rows i - s and i + s: rows of lane (lane -+ s) & 31,
+        // one row lower / higher in that lane where the stride wraps
+        const float ta = __shfl_sync(0xffffffffu, a[r], src_m), tb = __shfl_sync(0xffffffffu, b[r], src_m);
+        const float tc = __shfl_sync(0xffffffffu, c[r], src_m), td = __shfl_sync(0xffffffffu, d[r], src_m);
+        const float ua = __shfl_sync(0xffffffffu, a[r], src_p), ub = __shfl_sync(0xffffffffu, b[r], src_p);
+        const float uc = __shfl_sync(0xffffffffu, c[r], src_p), ud = __shfl_sync(0xffffffffu, d[r], src_p);
+        // row r of the source lane serves this lane's row r (no wrap) or r + 1 (wrap, minus side)
+        if (!wrap_m) { am[r] = ta; bm[r] = tb; cm[r] = tc; dm[r] = td; }
+        else if (r + 1 < R) { am[r + 1] = ta; bm[r + 1] = tb; cm[r + 1] = tc; dm[r + 1] = td; }
+        if (!wrap_p) { ap[r] = ua; bp[r] = ub; cp[r] = uc; dp[r] = ud; }
+        else if (r >= 1) { ap[r - 1] = ua; bp[r - 1] = ub; cp[r - 1] = uc; dp[r - 1] = ud; }
+      }
+      if (wrap_m) { am[0] = 0.f; bm[0] = 1.f; cm[0] = 0.f; dm[0] = 0.f; }          // row i - s < 0
+      if (wrap_p) { ap[R - 1] = 0.f; bp[R - 1] = 1.f; cp[R - 1] = 0.f; dp[R - 1] = 0.f; }   // beyond the rows
+    } else {
+      // strides of whole lanes' rows: the same lane, r -+ s / 32
+      const int q = s >> 5;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (r - q >= 0) { am[r] = a[r - q]; bm[r] = b[r - q]; cm[r] = c[r - q]; dm[r] = d[r - q]; }
+        else { am[r] = 0.f; bm[r] = 1.f; cm[r] = 0.f; dm[r] = 0.f; }
+        if (r + q < R) { ap[r] = a[r + q]; bp[r] = b[r + q]; cp[r] = c[r + q]; dp[r] = d[r + q]; }
+        else { ap[r] = 0.f; bp[r] = 1.f; cp[r] = 0.f; dp[r] = 0.f; }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float al = -a[r] / bm[r], ga = -c[r] / bp[r];
+      const float na = al * am[r], nc = ga * cp[r];
+      const float nb = b[r] + al * cm[r] + ga * ap[r];
+      const float nd = d[r] + al * dm[r] + ga * dp[r];
+      a[r] = na; b[r] = nb; c[r] = nc; d[r] = nd;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n) m.wmf[k0 + i] = d[r] / b[r];
+  }
+}
+
 __global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs A) {
   extern __shared__ double wsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -533,17 +602,11 @@ __global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs 
     m.b33[kd] = A.arw[x + 1] * (b22 + b26 - b24 * thil_upw[x + 1]);
   }
   __syncwarp();
-  // phase 3: tridiffo (ka..mza-1) on one lane
-  if (lane == 0 && kb <= mza - 2) {
-    float cji = 1.0f / m.b32[kb];
-    m.wmf[kb] = m.dwm[kb] * cji;
-    for (int kd = kb + 1; kd <= mza - 2; ++kd) {
-      const float scr = cji * m.b33[kd - 1];
-      m.b33[kd - 1] = scr;  // keep scr1(k) for the back substitution
-      cji = 1.0f / (m.b32[kd] - m.b31[kd] * scr);
-      m.wmf[kd] = cji * (m.dwm[kd] - m.b31[kd] * m.wmf[kd - 1]);
-    }
-    for (int kd = mza - 3; kd >= kb; --kd) m.wmf[kd] = m.wmf[kd] - m.b33[kd] * m.wmf[kd + 1];
+  // phase 3: tridiffo's system (faces kb..mza-2) by cyclic reduction across
+  // the warp's lanes
+  if (kb <= mza - 2) {
+    if (mza - 1 - kb <= 64) warp_tridiag<2>(m, kb, mza - 2, lane);
+    else warp_tridiag<4>(m, kb, mza - 2, lane);
   }
   __syncwarp();
   // phase 4: implicit fluxes and the updates of rho, press, thil and vm*et_rk

@@ -231,7 +231,7 @@ def dynamics_state(g, jet_amp=35.0, kind="jet", t_sfc=300.0, lapse=6.5e-3,
 
 def fast_lognormal_tracers(g, ntr, seed=2024, median=1.0e-8, sigma_ln=1.5,
                            clip=(1.0e-12, 1.0e-6), zero_frac=0.1, zero_above=15000.0,
-                           dtype=np.float32, as_list=False):
+                           dtype=np.float32, as_list=False, cols=None):
     """Large-case tracer fields: seeded lognormal mixing ratios, separable in
     horizontal and vertical so that 100+ full-size fields generate quickly.
 
@@ -244,8 +244,11 @@ def fast_lognormal_tracers(g, ntr, seed=2024, median=1.0e-8, sigma_ln=1.5,
     rng = np.random.default_rng(seed)
     lat, lon = _latlon(g)
     zt = g.zt.astype(np.float64)
-    out = ([np.empty((g.mwa, g.mza), dtype=dtype) for _ in range(ntr)] if as_list
-           else np.empty((ntr, g.mwa, g.mza), dtype=dtype))
+    # cols: only these W points (a rank's part of the grid), in this order;
+    # the values are those of the whole-grid fields at those points
+    nw = g.mwa if cols is None else len(cols)
+    out = ([np.empty((nw, g.mza), dtype=dtype) for _ in range(ntr)] if as_list
+           else np.empty((ntr, nw, g.mza), dtype=dtype))
     nz = int(round(zero_frac * ntr))
     zsel = set(rng.choice(ntr, nz, replace=False).tolist()) if nz else set()
     above = zt > zero_above
@@ -254,6 +257,8 @@ def fast_lognormal_tracers(g, ntr, seed=2024, median=1.0e-8, sigma_ln=1.5,
         m1, m2 = rng.integers(1, 6, 2)
         h = np.sin(m1 * lon + a[0]) * np.cos(m2 * lat + a[1]) + 0.3 * rng.standard_normal(g.mwa)
         v = 0.5 * np.sin(2 * np.pi * zt / rng.uniform(5e3, 3e4) + a[2])
+        if cols is not None:
+            h = h[cols]
         eh = (median * np.exp(sigma_ln * h / 1.2)).astype(np.float32)
         ev = np.exp(sigma_ln * v / 1.2).astype(np.float32)
         q = out[n]

@@ -98,6 +98,61 @@ def test_two_ranks_match_one_domain(form, nrk):
     assert covered[1:].all()
 
 
+@pytest.mark.parametrize("nrk", [2, 3])
+def test_device_buffer_hook_matches_one_domain(nrk):
+    # the hook gets the library's device buffers and stream (as an NCCL or
+    # CUDA-aware MPI exchange would); it checks the packed send columns and
+    # writes the neighbour's stage values into the receive buffers with
+    # copies ordered on that stream (olam_b200/nccl_halo.py's device views)
+    import torch
+    from olam_b200.nccl_halo import device_view
+    g, st = small_case(nxp=8, nlev=12, ntr=6)
+    opts = abi.make_opts(1800.0, nrk_scal=nrk)
+    ref, _ = run_gpu(g, st, opts, abi.TRANSPORT_FUSED)
+    stages = _stages(g, st, 1800.0, nrk)
+    owner = decomp.bisect(g, 2)
+    ntr, mza = len(st.tracers), g.mza
+    ntp = (ntr + 3) // 4 * 4
+    for rank in range(2):
+        loc = decomp.local_grid(g, owner, rank)
+        calls = {"n": 0, "send_err": 0.0}
+
+        def hook(ranks, sbufs, rbufs, stream):
+            k = calls["n"]
+            calls["n"] += 1
+            with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                for r, (sp, sn), (rp, rn) in zip(ranks, sbufs, rbufs):
+                    if sn:
+                        got = device_view(sp, sn).cpu().numpy().reshape(len(loc.send[r]), mza, ntp)[:, :, :ntr]
+                        want = stages[k][:, loc.wmap[loc.send[r]], :].transpose(1, 2, 0)
+                        calls["send_err"] = max(calls["send_err"], relerr(got, want))
+                    if rn:
+                        cols = loc.wmap[loc.recv[r]]
+                        blk = np.zeros((len(cols), mza, ntp), np.float32)
+                        blk[:, :, :ntr] = stages[k][:, cols, :].transpose(1, 2, 0)
+                        device_view(rp, rn).copy_(torch.from_numpy(blk.ravel()).cuda())
+            return 0
+
+        fg = abi.FortranGrid(loc.grid)
+        hs = HostState(vmasc=loc.v(st.vmasc), wmasc=loc.w(st.wmasc), rho=loc.w(st.rho), wc=loc.w(st.wc))
+        dev = OlamGpu(fg, opts, hs)
+        try:
+            var_p = [loc.w(t).copy() for t in st.tracers]
+            var_t = [loc.w(t).copy() for t in st.sct]
+            dev.register_scalars(var_p, var_t)
+            dev.set_halo(abi.make_halo_device(loc.send, loc.recv, hook))
+            dev.set_coherence(abi.RESIDENT)
+            dev.scalar_transport_rk(loc.w(st.rho_old))
+            dev.sync_to_host(abi.F_SCALARS)
+        finally:
+            dev.close()
+        assert calls["n"] == nrk - 1
+        assert calls["send_err"] < 1e-5, calls
+        own = loc.owned
+        for n in range(ntr):
+            assert relerr(var_p[n][own], ref[n][loc.wmap[own]]) < 1e-5, (rank, n)
+
+
 def test_halo_needs_the_unlimited_batched_step():
     g, st = small_case(nxp=6, nlev=8, ntr=2)
     loc = decomp.local_grid(g, decomp.bisect(g, 2), 0)
