@@ -434,69 +434,67 @@ struct WrtSmem {
 // The W system of prog_wrt_begs, b31(k) x(k-1) + b32(k) x(k) + b33(k) x(k+1)
 // = dwm(k) for k = k0 .. k1, which the reference solves with the Thomas
 // algorithm (tridiffo, outils/tridiag_lib.f90:10-36), solved here by
-// parallel cyclic reduction over a warp: row i = k - k0 lives in lane
+// parallel cyclic reduction over a warp: row i = k - k0 is updated by lane
 // i % 32 (R rows per lane, i = lane + 32 r); in a step of stride s every row
 // eliminates its couplings to rows i - s and i + s with those rows' current
 // equations (rows outside the system act as identity rows), so after
-// ceil(log2(n)) steps each row holds x(k) = d / b.
+// ceil(log2(n)) steps each row holds x(k) = d / b.  The equations live in
+// the column's shared memory as FP64 (the inputs and the result are the
+// reference's real(4)): w is a small residual of large terms, and FP64 keeps
+// it nearer the exact solve than a real(4) sweep.  The four FP64 arrays
+// reuse pex and rex (not read after phase 2) and the float coefficient
+// arrays themselves (read into registers first).
 template <int R>
 __device__ __forceinline__ void warp_tridiag(WrtSmem& m, int k0, int k1, int lane) {
   const int n = k1 - k0 + 1;
-  float a[R], b[R], c[R], d[R];
+  double* A = m.pex;
+  double* B = m.rex;
+  double* Cc = reinterpret_cast<double*>(m.b31);   // b31 and b32: 2 mza floats
+  double* D = reinterpret_cast<double*>(m.b33);    // b33 and dwm
+  float ra[R], rb[R], rc[R], rd[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = lane + 32 * r;
-    const bool in = i < n;
-    a[r] = in && i > 0 ? m.b31[k0 + i] : 0.f;
-    b[r] = in ? m.b32[k0 + i] : 1.f;
-    c[r] = in && i < n - 1 ? m.b33[k0 + i] : 0.f;
-    d[r] = in ? m.dwm[k0 + i] : 0.f;
+    ra[r] = i < n && i > 0 ? m.b31[k0 + i] : 0.f;
+    rb[r] = i < n ? m.b32[k0 + i] : 1.f;
+    rc[r] = i < n - 1 ? m.b33[k0 + i] : 0.f;
+    rd[r] = i < n ? m.dwm[k0 + i] : 0.f;
   }
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n) { A[i] = ra[r]; B[i] = rb[r]; Cc[i] = rc[r]; D[i] = rd[r]; }
+  }
+  __syncwarp();
   for (int s = 1; s < n; s <<= 1) {
-    float am[R], bm[R], cm[R], dm[R], ap[R], bp[R], cp[R], dp[R];
-    if (s < 32) {
-      const int src_m = (lane - s) & 31, src_p = (lane + s) & 31;
-      const bool wrap_m = lane < s, wrap_p = lane + s >= 32;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        // the equations of rows i - s and i + s: rows of lane (lane -+ s) & 31,
-        // one row lower / higher in that lane where the stride wraps
-        const float ta = __shfl_sync(0xffffffffu, a[r], src_m), tb = __shfl_sync(0xffffffffu, b[r], src_m);
-        const float tc = __shfl_sync(0xffffffffu, c[r], src_m), td = __shfl_sync(0xffffffffu, d[r], src_m);
-        const float ua = __shfl_sync(0xffffffffu, a[r], src_p), ub = __shfl_sync(0xffffffffu, b[r], src_p);
-        const float uc = __shfl_sync(0xffffffffu, c[r], src_p), ud = __shfl_sync(0xffffffffu, d[r], src_p);
-        // row r of the source lane serves this lane's row r (no wrap) or r + 1 (wrap, minus side)
-        if (!wrap_m) { am[r] = ta; bm[r] = tb; cm[r] = tc; dm[r] = td; }
-        else if (r + 1 < R) { am[r + 1] = ta; bm[r + 1] = tb; cm[r + 1] = tc; dm[r + 1] = td; }
-        if (!wrap_p) { ap[r] = ua; bp[r] = ub; cp[r] = uc; dp[r] = ud; }
-        else if (r >= 1) { ap[r - 1] = ua; bp[r - 1] = ub; cp[r - 1] = uc; dp[r - 1] = ud; }
-      }
-      if (wrap_m) { am[0] = 0.f; bm[0] = 1.f; cm[0] = 0.f; dm[0] = 0.f; }          // row i - s < 0
-      if (wrap_p) { ap[R - 1] = 0.f; bp[R - 1] = 1.f; cp[R - 1] = 0.f; dp[R - 1] = 0.f; }   // beyond the rows
-    } else {
-      // strides of whole lanes' rows: the same lane, r -+ s / 32
-      const int q = s >> 5;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (r - q >= 0) { am[r] = a[r - q]; bm[r] = b[r - q]; cm[r] = c[r - q]; dm[r] = d[r - q]; }
-        else { am[r] = 0.f; bm[r] = 1.f; cm[r] = 0.f; dm[r] = 0.f; }
-        if (r + q < R) { ap[r] = a[r + q]; bp[r] = b[r + q]; cp[r] = c[r + q]; dp[r] = d[r + q]; }
-        else { ap[r] = 0.f; bp[r] = 1.f; cp[r] = 0.f; dp[r] = 0.f; }
-      }
-    }
+    double na[R], nb[R], nc[R], nd[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const float al = -a[r] / bm[r], ga = -c[r] / bp[r];
-      const float na = al * am[r], nc = ga * cp[r];
-      const float nb = b[r] + al * cm[r] + ga * ap[r];
-      const float nd = d[r] + al * dm[r] + ga * dp[r];
-      a[r] = na; b[r] = nb; c[r] = nc; d[r] = nd;
+      const int i = lane + 32 * r;
+      if (i >= n) continue;
+      const int im = i - s, ip = i + s;
+      const double ai = A[i], bi = B[i], ci = Cc[i], di = D[i];
+      double al = 0.0, ga = 0.0, am = 0.0, cm = 0.0, dm = 0.0, ap = 0.0, cp = 0.0, dp = 0.0;
+      if (im >= 0) { al = -ai / B[im]; am = A[im]; cm = Cc[im]; dm = D[im]; }
+      if (ip < n) { ga = -ci / B[ip]; ap = A[ip]; cp = Cc[ip]; dp = D[ip]; }
+      na[r] = al * am;
+      nc[r] = ga * cp;
+      nb[r] = bi + al * cm + ga * ap;
+      nd[r] = di + al * dm + ga * dp;
     }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n) { A[i] = na[r]; B[i] = nb[r]; Cc[i] = nc[r]; D[i] = nd[r]; }
+    }
+    __syncwarp();
   }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = lane + 32 * r;
-    if (i < n) m.wmf[k0 + i] = d[r] / b[r];
+    if (i < n) m.wmf[k0 + i] = (float)(D[i] / B[i]);
   }
 }
 
@@ -606,7 +604,7 @@ __global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs 
   // the warp's lanes
   if (kb <= mza - 2) {
     if (mza - 1 - kb <= 64) warp_tridiag<2>(m, kb, mza - 2, lane);
-    else warp_tridiag<4>(m, kb, mza - 2, lane);
+    else warp_tridiag<4>(m, kb, mza - 2, lane);   // mza <= 128
   }
   __syncwarp();
   // phase 4: implicit fluxes and the updates of rho, press, thil and vm*et_rk

@@ -404,7 +404,9 @@ struct TileHost {
   std::vector<int> band_lev;     // the device level at which each band ends
 };
 // T: tile width (0: the widest whose neighbourhoods fit two blocks per SM)
-void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0);
+// nu_cap: the largest neighbourhood of a tile (0: where two blocks of 64
+// tracers fit an SM)
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0, int nu_cap = 0);
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T = 0);
 // dynamic shared memory of the stage kernel: T columns, nu_max rows of rb bytes
 size_t tile_smem_bytes(int T, int nu_max, int rb);

@@ -380,7 +380,7 @@ std::vector<int> locality_order(const olamgpu_grid* g) {
   return cols;
 }
 
-void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req) {
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int nu_cap) {
   th = TileHost();
   if (order != 2 && order != 3) return;
   const int nprog = g->nw_prog, mwa = g->mwa;
@@ -412,10 +412,16 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req) {
   }
   std::vector<int> stamp(mwa, -1), loc(mwa, 0);
   std::vector<int> U;
-  // neighbourhood of tile t in U (local index of column x: loc[x] while stamp[x] == t)
-  auto gather = [&](int t, int T) {
+  // Tiles are runs of at most T columns of the order above; a run closes
+  // early where one more column would take its two-ring neighbourhood
+  // beyond the cap (where the curve jumps between faces of the cube), so
+  // that no outlier sets every block's shared memory.  tstart[t] is the
+  // first column of tile t.
+  std::vector<int> tstart;
+  // the neighbourhood of columns [j0, j1) in U (local index of column x:
+  // loc[x] while stamp[x] == t)
+  auto gather_cols = [&](int t, int j0, int j1) {
     U.clear();
-    const int j0 = t * T, j1 = std::min(nprog, j0 + T);
     auto add = [&](int x) {
       if (stamp[x] != t) { stamp[x] = t; loc[x] = (int)U.size(); U.push_back(x); }
     };
@@ -427,26 +433,69 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req) {
     for (int i = nt; i < nr1; ++i)
       for (int n = 0; n < g->npoly[U[i]]; ++n) add(nbr(U[i], n));
   };
+  auto gather = [&](int t, int T) {
+    gather_cols(t, tstart[t], std::min(nprog, std::min(tstart[t + 1], tstart[t] + T)));
+  };
+  // the runs for width Tc and cap (0: no cap); returns the largest neighbourhood
+  std::vector<int> mark(mwa, 0), trial;
+  auto form = [&](int Tc, int cap) -> int {
+    tstart.clear();
+    std::fill(mark.begin(), mark.end(), 0);
+    int nu_max = 0, j = 0, epoch = 0;
+    while (j < nprog) {
+      tstart.push_back(j);
+      ++epoch;   // mark[x] == epoch: x is in the run's neighbourhood
+      int nu = 0, len = 0;
+      while (j + len < nprog && len < Tc) {
+        const int c = cols[j + len];
+        // the cells of the candidate's two rings not yet in the neighbourhood
+        trial.clear();
+        auto count = [&](int x) {
+          if (mark[x] != epoch) { mark[x] = epoch; trial.push_back(x); }
+        };
+        count(c);
+        for (int n = 0; n < g->npoly[c]; ++n) count(nbr(c, n));
+        for (int n = 0; n < g->npoly[c]; ++n) {
+          const int x = nbr(c, n);
+          for (int m = 0; m < g->npoly[x]; ++m) count(nbr(x, m));
+        }
+        if (cap > 0 && len > 0 && nu + (int)trial.size() > cap) {
+          for (int x : trial) mark[x] = 0;   // the run ends before this column
+          break;
+        }
+        nu += (int)trial.size();
+        ++len;
+      }
+      nu_max = std::max(nu_max, nu);
+      j += len;
+    }
+    tstart.push_back(nprog);
+    return nu_max;
+  };
   int T = 0, numax = 0;
   // one or two columns for each of the 16 half-warps of a block (64 tracers
-  // per block: 256-byte rows), or the width asked for
+  // per block: 256-byte rows), or the width asked for.  Neighbourhoods are
+  // capped where two blocks of the widest rows the stage kernel runs on
+  // tiles of this width fit an SM (32 columns: 64 tracers, 256-byte rows;
+  // 16 columns: 128 tracers, 512-byte rows), or at nu_cap when given.
   const int cand[] = {32, 16};
   for (int Tc : cand) {
     if (T_req > 0 && Tc != T_req) continue;
-    std::fill(stamp.begin(), stamp.end(), -1);
-    const int nt = (nprog + Tc - 1) / Tc;
-    int nu = 0;
-    for (int t = 0; t < nt; ++t) {
-      gather(t, Tc);
-      nu = std::max(nu, (int)U.size());
+    int cap = nu_cap;
+    if (cap <= 0) {
+      const int rb = Tc == 16 ? 512 : 256;
+      cap = 4;
+      while (tile_smem_bytes(Tc, cap + 4, rb) <= TILE_SMEM_MAX) cap += 4;
     }
+    const int nu = form(Tc, cap);
+    std::fill(stamp.begin(), stamp.end(), -1);
     if (nu <= 65535 && (T_req > 0 || tile_smem_bytes(Tc, nu, 256) <= TILE_SMEM_MAX)) {
       T = Tc; numax = nu;
       break;
     }
   }
   if (!T) return;  // neighbourhoods too large: the column kernel runs
-  const int ntiles = (nprog + T - 1) / T;
+  const int ntiles = (int)tstart.size() - 1;
   std::vector<int>& hdr = th.hdr;
   std::vector<int>& ulist = th.ulist;
   std::vector<int>& tc = th.tc;
@@ -462,7 +511,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req) {
   for (int t = 0; t < ntiles; ++t) {
     gather(t, T);
     const int u_off = (int)ulist.size();
-    const int nT = std::min(T, nprog - t * T);
+    const int nT = tstart[t + 1] - tstart[t];
     hdr[(size_t)t * 4 + 0] = u_off;
     hdr[(size_t)t * 4 + 1] = (int)U.size();
     hdr[(size_t)t * 4 + 3] = nT;
