@@ -395,8 +395,59 @@ __global__ void k_grad(GridK g, const int* __restrict__ prog, int nprog, CTView 
   }
 }
 
+// One tracer in OLAM's own layout (the plain form): a warp per column, lanes
+// over the levels, the column's neighbours, face floors and coefficients
+// held in registers (read once per column instead of once per element).
+__global__ void k_grad1(GridK g, const int* __restrict__ prog, int nprog, const float* __restrict__ S,
+                        float* __restrict__ gx, int order, const float* __restrict__ cx,
+                        const float* __restrict__ cy, const float* __restrict__ xy) {
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= nprog) return;
+  const int mza = g.mza, iw = prog[w], np = g.npoly[iw];
+  const size_t plane = (size_t)g.mwa * mza;
+  int nb[7], lp[7];
+  float c[7][5];
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    nb[n] = iw; lp[n] = mza;
+    for (int m = 0; m < 5; ++m) c[n][m] = 0.f;
+    if (n < np) {
+      nb[n] = __ldg(g.w_nb + iw * 8 + n);
+      lp[n] = __ldg(g.lpv + __ldg(g.w_ev + iw * 8 + n));
+      if (order == 2) { c[n][0] = __ldg(cx + iw * 7 + n); c[n][1] = __ldg(cy + iw * 7 + n); }
+      else for (int m = 0; m < 5; ++m) c[n][m] = __ldg(xy + ((size_t)iw * 7 + n) * 5 + m);
+    }
+  }
+  for (int kd = lane; kd < mza; kd += 32) {
+    const float s0 = S[(size_t)iw * mza + kd];
+    float a[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int n = 0; n < 7; ++n) {
+      if (n >= np || kd < lp[n]) continue;
+      const float d = S[(size_t)nb[n] * mza + kd] - s0;
+      if (order == 2) {
+        a[0] = a[0] + c[n][0] * d;
+        a[1] = a[1] + c[n][1] * d;
+      } else {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) a[m] = a[m] + d * c[n][m];
+      }
+    }
+    const size_t o = (size_t)iw * mza + kd;
+    gx[o] = a[0];
+    gx[plane + o] = a[1];
+    if (order == 3) { gx[2 * plane + o] = a[2]; gx[3 * plane + o] = a[3]; gx[4 * plane + o] = a[4]; }
+  }
+}
+
 void launch_grad(const DevGrid& d, CTView scp, float* gx, int nt, int order, bool bounded,
                  cudaStream_t s) {
+  if (nt == 1 && scp.ld == 1 && scp.t0 == 0) {
+    k_grad1<<<cdiv((size_t)d.nw_prog * 32, 256), 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp.base, gx, order,
+                                                             d.gxc.p, d.gyc.p, bounded ? d.xy_h.p : d.xy_hu.p);
+    OG_LAUNCHED();
+    return;
+  }
   size_t n = (size_t)d.nw_prog * d.mza * nt;
   k_grad<<<cdiv(n, 256), 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp, gx, nt, order, d.gxc.p,
                                       d.gyc.p, bounded ? d.xy_h.p : d.xy_hu.p);
@@ -461,10 +512,49 @@ __global__ void k_vflux(GridK g, const int* __restrict__ vlist, int nv, CTView s
   }
 }
 
+// the upwind V-face values of one tracer (plain mode, OLAM's layout): a warp
+// per face, lanes over the levels, the face's cells and coefficients in
+// registers; only the upwind side's reconstruction is read
+__global__ void k_vflux1(GridK g, const int* __restrict__ vlist, int nv, const float* __restrict__ S,
+                         const float* __restrict__ gx, const float* __restrict__ vmasc, int order, VCoef vc,
+                         float* __restrict__ upv) {
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= nv) return;
+  const int mza = g.mza, iv = vlist[w], kv = g.lpv[iv];
+  const size_t plane = (size_t)g.mwa * mza;
+  // side 1 (itab_v%iw(1)) and side 2 coefficients, selected per level by the
+  // sign of the flux (no runtime-indexed arrays: they would live in local memory)
+  const int w1 = g.v_iw[iv * 2], w2 = g.v_iw[iv * 2 + 1];
+  const int e1 = iv * 2, e2 = iv * 2 + 1;
+  const float dx1 = __ldg(vc.dxps + e1), dy1 = __ldg(vc.dyps + e1), dx2 = __ldg(vc.dxps + e2), dy2 = __ldg(vc.dyps + e2);
+  float xx1 = 0.f, xy1 = 0.f, yy1 = 0.f, xx2 = 0.f, xy2 = 0.f, yy2 = 0.f;
+  if (order == 3) {
+    xx1 = __ldg(vc.xx + e1); xy1 = __ldg(vc.xy + e1); yy1 = __ldg(vc.yy + e1);
+    xx2 = __ldg(vc.xx + e2); xy2 = __ldg(vc.xy + e2); yy2 = __ldg(vc.yy + e2);
+  }
+  for (int kd = kv + lane; kd < mza; kd += 32) {
+    const float vm = vmasc[(size_t)iv * mza + kd];
+    const bool two = vm < 0.f;
+    const size_t o = (size_t)(two ? w2 : w1) * mza + kd;
+    float v = S[o];
+    v = v + (two ? dx2 : dx1) * gx[o] + (two ? dy2 : dy1) * gx[plane + o];
+    if (order == 3)
+      v = v + (two ? xx2 : xx1) * gx[2 * plane + o] + (two ? xy2 : xy1) * gx[3 * plane + o] +
+          (two ? yy2 : yy1) * gx[4 * plane + o];
+    upv[(size_t)iv * mza + kd] = v;
+  }
+}
+
 void launch_vflux(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, const float* gx,
                   int nt, int order, bool unbounded, const int* mode, bool anylim, cudaStream_t s) {
   VCoef vc{d.dxps.p, d.dyps.p, unbounded ? d.xx0_vu.p : d.xx0_v.p, unbounded ? d.xy0_vu.p : d.xy0_v.p,
            unbounded ? d.yy0_vu.p : d.yy0_v.p};
+  if (nt == 1 && scp.ld == 1 && scp.t0 == 0 && !anylim) {
+    k_vflux1<<<cdiv((size_t)d.nv_wadj * 32, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp.base, gx,
+                                                              tp.vmasc.p, order, vc, tp.upv.p);
+    OG_LAUNCHED();
+    return;
+  }
   size_t n = (size_t)d.nv_wadj * d.mza * nt;
   k_vflux<<<cdiv(n, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp, scp0, gx, tp.vmasc.p, nt,
                                        order, vc, anylim ? mode : nullptr, tp.upv.p, tp.hiv.p, tp.sfv.p);
@@ -715,6 +805,56 @@ __global__ void k_wcell(WcolArgs A) {
     for (int k = 0; k < kb; ++k) out[(size_t)k * A.out.ld] = o;
 }
 
+// the same for one tracer in OLAM's layout: a warp per column, lanes over
+// the levels, the column's faces (V point, dirv, floor) in registers
+__global__ void k_wcell1(WcolArgs A) {
+  const GridK& g = A.g;
+  const int mza = g.mza;
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= A.nprog) return;
+  const int iw = A.prog[w], kb = g.lpw[iw], np = g.npoly[iw];
+  int ev[7], lp[7];
+  float dv[7];
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    ev[n] = 0; lp[n] = mza; dv[n] = 0.f;
+    if (n < np) { ev[n] = g.w_ev[iw * 8 + n]; lp[n] = g.lpv[ev[n]]; dv[n] = g.w_dirv[iw * 8 + n]; }
+  }
+  const float fimpl = A.ff[(size_t)iw * A.nrk + A.istage - 1];
+  const float fexpl = 1.0f - fimpl;
+  const float* wm = A.wmasc + (size_t)iw * mza;
+  const float* Sc = A.scp.base + (size_t)iw * mza;
+  auto S = [&](int k) { return Sc[k]; };
+  auto upw = [&](int f) -> float {
+    if (f == kb - 1) return S(kb);
+    if (f == mza - 1) return S(mza - 1);
+    float sb, st;
+    if (wm[f] < 0.f) {
+      zrec(g.a_w, mza, f + 1, kb, S(f), S(f + 1), (f + 2 < mza) ? S(f + 2) : 0.f, 0.f, false, false, sb, st);
+      return sb;
+    }
+    zrec(g.a_w, mza, f, kb, (f - 1 >= kb) ? S(f - 1) : 0.f, S(f), S(f + 1), 0.f, false, false, sb, st);
+    return st;
+  };
+  float* out = A.out.base + (size_t)iw * mza;
+  for (int kd = kb + lane; kd < mza; kd += 32) {
+    const size_t x = (size_t)iw * mza + kd;
+    const float s00 = A.scp0.base[x];
+    float fd = 0.f;
+#pragma unroll
+    for (int n = 0; n < 7; ++n) {
+      if (n >= np || kd < lp[n]) continue;
+      const size_t xv = (size_t)ev[n] * mza + kd;
+      fd = fd + dv[n] * A.vmasc[xv] * (A.upv[xv] - s00);
+    }
+    fd = fd + fexpl * (wm[kd - 1] * (upw(kd - 1) - s00) - wm[kd] * (upw(kd) - s00));
+    const float o = s00 + A.dtr * (A.sct.base[x] + g.volti[x] * fd) / A.rhos[x];
+    out[kd] = o;
+    if (kd == kb)
+      for (int k = 0; k < kb; ++k) out[k] = o;
+  }
+}
+
 void launch_wcell(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0, CTView sct, const float* rhos,
                   TView out, int nt, int istage, int nrk, float dtr, cudaStream_t s) {
   WcolArgs A;
@@ -725,6 +865,12 @@ void launch_wcell(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0
   A.upv = tp.upv.p; A.sfv = nullptr; A.scale = nullptr; A.upw = nullptr;
   A.out = out; A.nt = nt; A.istage = istage; A.nrk = nrk; A.dtr = dtr;
   A.mode = nullptr;
+  if (nt == 1 && scp.ld == 1 && scp.t0 == 0 && scp0.ld == 1 && scp0.t0 == 0 && sct.ld == 1 && sct.t0 == 0 &&
+      out.ld == 1 && out.t0 == 0) {
+    k_wcell1<<<cdiv((size_t)d.nw_prog * 32, 256), 256, 0, s>>>(A);
+    OG_LAUNCHED();
+    return;
+  }
   const size_t n = (size_t)d.nw_prog * d.mza * nt;
   k_wcell<<<cdiv(n, 256), 256, 0, s>>>(A);
   OG_LAUNCHED();
