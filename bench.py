@@ -79,6 +79,8 @@ def parse():
     p.add_argument("--win-steps", type=int, default=24)
     p.add_argument("--win-chk", type=int, default=6)
     p.add_argument("--win-monot", type=int, default=0)
+    p.add_argument("--shape-sweep", action="store_true",
+                   help="time every tile shape in steady state (forced, after warm steps) and print them")
     return p.parse_args()
 
 
@@ -425,6 +427,45 @@ def bench_long_step(g, tr, a, max_over_ranks):
     return out
 
 
+def shape_sweep(g, st, tr, a):
+    """Every shape of the tiled stage kernel forced in turn on the workload,
+    timed in steady state: two warm steps, then the stage launches of
+    a.steps steps (CUDA events around each launch)."""
+    import torch
+    from olam_b200 import abi
+    from olam_b200.lib import HostState, OlamGpu
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)
+    dev = OlamGpu(fg, opts, HostState(vmasc=st.vmasc, wmasc=st.wmasc, rho=st.rho, wc=st.wc))
+    out = []
+    try:
+        dev.register_scalars(tr, [np.zeros_like(t) for t in tr])
+        dev.set_coherence(abi.RESIDENT)
+        dev.sync_to_device(abi.F_ALL)
+        dev.scalar_transport_rk(st.rho_old)
+        for T, G, KS in ((32, 64, 1), (32, 64, 2), (32, 32, 1), (32, 32, 2), (16, 64, 1), (16, 64, 2),
+                         (16, 128, 1), (16, 128, 2)):
+            try:
+                dev.set_tile_shape(T, G, KS)
+            except Exception as e:   # a shape this grid cannot run
+                out.append({"T": T, "G": G, "KS": KS, "error": str(e)})
+                continue
+            for _ in range(2):
+                dev.scalar_transport_rk(None)
+            torch.cuda.synchronize()
+            dev.profile(True, reset=True)
+            for _ in range(a.steps):
+                dev.scalar_transport_rk(None)
+            prof = dev.profile_read()
+            dev.profile(False, reset=True)
+            ms = [prof[k][0] / prof[k][1] for k in ("tile_stage1", "tile_stage") if k in prof]
+            out.append({"T": T, "G": G, "KS": KS, "ms_per_stage": ms})
+        used, tlog = dev.tile_shape()
+    finally:
+        dev.close()
+    return out
+
+
 def bench_window(a, max_over_ranks):
     """The adjoint of tracer transport over a window of long steps: NXP=100
     (100,002 columns), 60 levels, 32 FP32 tracers with a seeded surface
@@ -664,6 +705,9 @@ def main():
         out = bench_window(a, lambda x: x)
         if rank == 0:
             print(json.dumps({"window_adjoint": out}), flush=True)
+        return 0
+    if a.shape_sweep:
+        print(json.dumps({"shape_sweep": shape_sweep(g, st, tr, a)}), flush=True)
         return 0
     fg = abi.FortranGrid(g)
     opts = abi.make_opts(a.dt, nrk_scal=a.nrk, scal_order=a.order, iscal_monot=a.monot)

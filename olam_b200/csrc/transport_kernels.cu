@@ -398,53 +398,59 @@ __global__ void k_grad(GridK g, const int* __restrict__ prog, int nprog, CTView 
 // One tracer in OLAM's own layout (the plain form): a warp per column, lanes
 // over the levels, the column's neighbours, face floors and coefficients
 // held in registers (read once per column instead of once per element).
-__global__ void k_grad1(GridK g, const int* __restrict__ prog, int nprog, const float* __restrict__ S,
-                        float* __restrict__ gx, int order, const float* __restrict__ cx,
-                        const float* __restrict__ cy, const float* __restrict__ xy) {
+template <int ORDER>
+__global__ void __launch_bounds__(256)
+    k_grad1(GridK g, const int* __restrict__ prog, int nprog, const float* __restrict__ S, float* __restrict__ gx,
+            const float* __restrict__ cx, const float* __restrict__ cy, const float* __restrict__ xy) {
+  constexpr int M = ORDER == 2 ? 2 : 5;   // gradient planes
   const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (w >= nprog) return;
   const int mza = g.mza, iw = prog[w], np = g.npoly[iw];
   const size_t plane = (size_t)g.mwa * mza;
   int nb[7], lp[7];
-  float c[7][5];
+  float c[7][M];
 #pragma unroll
   for (int n = 0; n < 7; ++n) {
     nb[n] = iw; lp[n] = mza;
-    for (int m = 0; m < 5; ++m) c[n][m] = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) c[n][m] = 0.f;
     if (n < np) {
       nb[n] = __ldg(g.w_nb + iw * 8 + n);
       lp[n] = __ldg(g.lpv + __ldg(g.w_ev + iw * 8 + n));
-      if (order == 2) { c[n][0] = __ldg(cx + iw * 7 + n); c[n][1] = __ldg(cy + iw * 7 + n); }
-      else for (int m = 0; m < 5; ++m) c[n][m] = __ldg(xy + ((size_t)iw * 7 + n) * 5 + m);
+      if (ORDER == 2) { c[n][0] = __ldg(cx + iw * 7 + n); c[n][M - 1] = __ldg(cy + iw * 7 + n); }
+      else {
+#pragma unroll
+        for (int m = 0; m < M; ++m) c[n][m] = __ldg(xy + ((size_t)iw * 7 + n) * 5 + m);
+      }
     }
   }
   for (int kd = lane; kd < mza; kd += 32) {
     const float s0 = S[(size_t)iw * mza + kd];
-    float a[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    float a[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) a[m] = 0.f;
 #pragma unroll
     for (int n = 0; n < 7; ++n) {
       if (n >= np || kd < lp[n]) continue;
       const float d = S[(size_t)nb[n] * mza + kd] - s0;
-      if (order == 2) {
-        a[0] = a[0] + c[n][0] * d;
-        a[1] = a[1] + c[n][1] * d;
-      } else {
 #pragma unroll
-        for (int m = 0; m < 5; ++m) a[m] = a[m] + d * c[n][m];
-      }
+      for (int m = 0; m < M; ++m) a[m] = a[m] + c[n][m] * d;
     }
     const size_t o = (size_t)iw * mza + kd;
-    gx[o] = a[0];
-    gx[plane + o] = a[1];
-    if (order == 3) { gx[2 * plane + o] = a[2]; gx[3 * plane + o] = a[3]; gx[4 * plane + o] = a[4]; }
+#pragma unroll
+    for (int m = 0; m < M; ++m) gx[m * plane + o] = a[m];
   }
 }
 
 void launch_grad(const DevGrid& d, CTView scp, float* gx, int nt, int order, bool bounded,
                  cudaStream_t s) {
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0) {
-    k_grad1<<<cdiv((size_t)d.nw_prog * 32, 256), 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp.base, gx, order,
-                                                             d.gxc.p, d.gyc.p, bounded ? d.xy_h.p : d.xy_hu.p);
+    const unsigned nb = cdiv((size_t)d.nw_prog * 32, 256);
+    if (order == 2)
+      k_grad1<2><<<nb, 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp.base, gx, d.gxc.p, d.gyc.p, nullptr);
+    else
+      k_grad1<3><<<nb, 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp.base, gx, nullptr, nullptr,
+                                    bounded ? d.xy_h.p : d.xy_hu.p);
     OG_LAUNCHED();
     return;
   }
@@ -807,7 +813,7 @@ __global__ void k_wcell(WcolArgs A) {
 
 // the same for one tracer in OLAM's layout: a warp per column, lanes over
 // the levels, the column's faces (V point, dirv, floor) in registers
-__global__ void k_wcell1(WcolArgs A) {
+__global__ void __launch_bounds__(256, 4) k_wcell1(WcolArgs A) {
   const GridK& g = A.g;
   const int mza = g.mza;
   const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
