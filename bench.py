@@ -79,6 +79,8 @@ def parse():
     p.add_argument("--win-steps", type=int, default=24)
     p.add_argument("--win-chk", type=int, default=6)
     p.add_argument("--win-monot", type=int, default=0)
+    p.add_argument("--tile-shape", default="",
+                   help="T,G,KS: force this shape of the tiled stage kernel (default: the autotuner's)")
     p.add_argument("--shape-sweep", action="store_true",
                    help="time every tile shape in steady state (forced, after warm steps) and print them")
     return p.parse_args()
@@ -737,6 +739,8 @@ def main():
 
     # ---- device-resident fused form
     dev.set_transport_form(abi.TRANSPORT_FUSED)
+    if a.tile_shape:
+        dev.set_tile_shape(*[int(x) for x in a.tile_shape.split(",")])
     dev.set_coherence(abi.RESIDENT)
     dev.sync_to_device(abi.F_ALL)
     dev.scalar_transport_rk(st.rho_old)          # uploads rho_old once
