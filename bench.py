@@ -445,12 +445,12 @@ def shape_sweep(g, st, tr, a):
         dev.set_coherence(abi.RESIDENT)
         dev.sync_to_device(abi.F_ALL)
         dev.scalar_transport_rk(st.rho_old)
-        for T, G, KS in ((32, 64, 1), (32, 64, 2), (32, 32, 1), (32, 32, 2), (16, 64, 1), (16, 64, 2),
-                         (16, 128, 1), (16, 128, 2)):
+        for ordr in (0, 1):
+          for T, G, KS in ((32, 64, 1), (32, 32, 1), (16, 64, 1), (16, 128, 1), (16, 128, 2)):
             try:
-                dev.set_tile_shape(T, G, KS)
+                dev.set_tile_shape(T, G, KS, ordr)
             except Exception as e:   # a shape this grid cannot run
-                out.append({"T": T, "G": G, "KS": KS, "error": str(e)})
+                out.append({"T": T, "G": G, "KS": KS, "order": ordr, "error": str(e)})
                 continue
             for _ in range(2):
                 dev.scalar_transport_rk(None)
@@ -461,7 +461,7 @@ def shape_sweep(g, st, tr, a):
             prof = dev.profile_read()
             dev.profile(False, reset=True)
             ms = [prof[k][0] / prof[k][1] for k in ("tile_stage1", "tile_stage") if k in prof]
-            out.append({"T": T, "G": G, "KS": KS, "ms_per_stage": ms})
+            out.append({"T": T, "G": G, "KS": KS, "order": ordr, "ms_per_stage": ms})
         used, tlog = dev.tile_shape()
     finally:
         dev.close()
@@ -770,10 +770,12 @@ def main():
     launches = dev.launch_count()
     prof = dev.profile_read()
     used, tlog = dev.tile_shape()
-    tile_shape = {"T": used[0], "G": used[1], "KS": used[2],
-                  "candidates_ms_per_stage": [{"T": r[0], "G": r[1], "KS": r[2], "ms": r[4]} for r in tlog],
-                  "note": "columns per tile, tracers per block, level chunks per tile; chosen by the "
-                          "library's autotuner on the first step"}
+    tile_shape = {"T": used[0], "G": used[1], "KS": used[2], "order": used[3],
+                  "candidates_ms_per_stage": [{"T": r[0], "G": r[1], "KS": r[2], "order": r[3], "ms": r[5]}
+                                              for r in tlog],
+                  "note": "columns per tile, tracers per block, level chunks per tile, tile order (0: the "
+                          "library's curve, 1: the caller's numbering); chosen by the library's autotuner "
+                          "on the first step"}
     dev.profile(False, reset=True)
     clk = clocks.stop()
     barrier()

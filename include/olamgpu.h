@@ -378,19 +378,21 @@ int olamgpu_timestep(unsigned flags, int nmass, const int* mass_ids);
 int olamgpu_timestep_diag(float* smax, double* sums);
 
 /* ---- shape of the tiled stage kernel -------------------------------------------
- * The tiled transport kernel runs tiles of T neighbouring columns (16 or
- * 32) with G tracers per block (32, 64 or 128) and the levels of a tile
- * swept by KS blocks.  By default an autotuner picks the shape on the first
- * step for a grid and tracer count: every shape the shared memory admits
- * runs the stage on that step's inputs and the fastest is kept (cached per
- * grid, tracer count and order for the process).  olamgpu_set_tile_shape
- * forces a shape (0, 0, 0: back to the autotuner).  olamgpu_tile_shape
- * returns the shape in use (shape[3]: T, G, KS) and, for up to max
- * candidates of the last tuning, cand[4 i ..] = T, G, KS, chosen and ms[i]
- * the stage time in milliseconds; it returns the number of candidates (or
- * minus a status).  The batching replaces the reference's serial loop over
- * tracers (omodel/scalar_transport_rk.F90:223). */
-int olamgpu_set_tile_shape(int T, int G, int KS);
+ * The tiled transport kernel runs tiles of up to T neighbouring columns (16
+ * or 32) with G tracers per block (32, 64 or 128), the levels of a tile
+ * swept by KS blocks, the tiles running along the library's own curve over
+ * the columns' positions (ord 0) or along the caller's jtw_prog (ord 1).  By
+ * default an autotuner picks the shape on the first step for a grid and
+ * tracer count: every shape the shared memory admits runs the stage on that
+ * step's inputs and the fastest is kept (cached per grid, tracer count and
+ * order for the process).  olamgpu_set_tile_shape forces a shape (all zero:
+ * back to the autotuner).  olamgpu_tile_shape returns the shape in use
+ * (shape[4]: T, G, KS, ord) and, for up to max candidates of the last
+ * tuning, cand[5 i ..] = T, G, KS, ord, chosen and ms[i] the stage time in
+ * milliseconds; it returns the number of candidates (or minus a status).
+ * The batching replaces the reference's serial loop over tracers
+ * (omodel/scalar_transport_rk.F90:223). */
+int olamgpu_set_tile_shape(int T, int G, int KS, int ord);
 int olamgpu_tile_shape(int* shape, int max, int* cand, float* ms);
 
 /* ---- surface emission and the checkpointed window adjoint -------------------

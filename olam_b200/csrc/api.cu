@@ -164,6 +164,7 @@ static void release_all() {
   d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
   d.tile_G = 64;
   d.tile_KS = 1;
+  d.tile_ord = 0;
   Tracers& tr = C.tr;
   for (size_t i = 0; i < tr.p.size(); ++i) {
     tr.p[i].release();
@@ -476,7 +477,7 @@ int olamgpu_timestep_diag(float* smax, double* sums) { return glue_timestep_diag
 
 int olamgpu_set_surface_emission(const float* const* emis) { return emission_set(emis); }
 
-int olamgpu_set_tile_shape(int T, int G, int KS) {
+int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
   Context& C = ctx();
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
   glue_drop_graphs();
@@ -486,12 +487,12 @@ int olamgpu_set_tile_shape(int T, int G, int KS) {
     tp.tuned_ntp = -1;
     return OLAMGPU_OK;
   }
-  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8) {
-    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8");
+  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || (ord != 0 && ord != 1)) {
+    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0 or 1");
     return OLAMGPU_E_ARG;
   }
   const int order = C.opts.scal_horiz_adv_order;
-  if (C.g.tile_T != T) OG_CHECK(build_tiles(&C.hgrid, C.g, order, C.stream, T));
+  if (C.g.tile_T != T || C.g.tile_ord != ord) OG_CHECK(build_tiles(&C.hgrid, C.g, order, C.stream, T, ord));
   if (C.g.tile_T != T || !tile_shape_fits(C.g, G)) {
     set_error("tile shape: this grid has no " + std::to_string(T) + "-column tiles of " + std::to_string(G) +
               " tracers within the shared memory");
@@ -506,10 +507,13 @@ int olamgpu_set_tile_shape(int T, int G, int KS) {
 int olamgpu_tile_shape(int* shape, int max, int* cand, float* ms) {
   Context& C = ctx();
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return -OLAMGPU_E_STATE; }
-  if (shape) { shape[0] = C.g.tile_T; shape[1] = C.g.tile_G; shape[2] = C.g.tile_KS; }
+  if (shape) { shape[0] = C.g.tile_T; shape[1] = C.g.tile_G; shape[2] = C.g.tile_KS; shape[3] = C.g.tile_ord; }
   const auto& L = C.tp.tune_log;
   for (int i = 0; i < (int)L.size() && i < max; ++i) {
-    if (cand) { cand[4 * i] = L[i].T; cand[4 * i + 1] = L[i].G; cand[4 * i + 2] = L[i].KS; cand[4 * i + 3] = L[i].chosen; }
+    if (cand) {
+      int* c = cand + 5 * i;
+      c[0] = L[i].T; c[1] = L[i].G; c[2] = L[i].KS; c[3] = L[i].ord; c[4] = L[i].chosen;
+    }
     if (ms) ms[i] = L[i].ms;
   }
   return (int)L.size();

@@ -159,6 +159,7 @@ struct DevGrid {
   DevBuf<int> tile_band_lev;
   int tile_T = 0, ntiles = 0, tile_nu_max = 0, tile_order = 0;
   int tile_G = 64, tile_KS = 1;  // the stage kernel's tracers per block and level chunks
+  int tile_ord = 0;              // the order the tiles run along (make_tiles)
   bool tile_closed = false;      // every neighbourhood column is prognosed
   std::vector<int> h_lpw;        // host copies used at set-up
 };
@@ -202,9 +203,9 @@ struct DevGrid {
 
 // a shape of the tiled stage kernel: columns per tile, tracers per block,
 // level chunks per tile
-struct TileShape { int T, G, KS; };
+struct TileShape { int T, G, KS, ord; };
 // one candidate the autotuner timed (ms per stage launch)
-struct TuneRec { int T, G, KS, chosen; float ms; };
+struct TuneRec { int T, G, KS, ord, chosen; float ms; };
 
 struct Tracers {
   int n = 0, ntp = 0;            // count and padded count (multiple of 4)
@@ -406,8 +407,10 @@ struct TileHost {
 // T: tile width (0: the widest whose neighbourhoods fit two blocks per SM)
 // nu_cap: the largest neighbourhood of a tile (0: where two blocks of 64
 // tracers fit an SM)
-void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0, int nu_cap = 0);
-int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T = 0);
+// ord: the order tiles run along -- 0 the library's own curve over the
+// columns' positions, 1 the caller's jtw_prog
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0, int nu_cap = 0, int ord = 0);
+int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T = 0, int ord = 0);
 // dynamic shared memory of the stage kernel: T columns, nu_max rows of rb bytes
 size_t tile_smem_bytes(int T, int nu_max, int rb);
 

@@ -380,13 +380,20 @@ std::vector<int> locality_order(const olamgpu_grid* g) {
   return cols;
 }
 
-void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int nu_cap) {
+void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int nu_cap, int ord) {
   th = TileHost();
   if (order != 2 && order != 3) return;
   const int nprog = g->nw_prog, mwa = g->mwa;
   if (nprog <= 0) return;
-  // tiles are runs of this order's columns
-  const std::vector<int> cols = locality_order(g);
+  // tiles are runs of this order's columns: the library's curve (ord 0) or
+  // the caller's jtw_prog (ord 1)
+  std::vector<int> cols;
+  if (ord == 1) {
+    cols.resize(nprog);
+    for (int j = 0; j < nprog; ++j) cols[j] = g->jtw_prog[j] - 1;
+  } else {
+    cols = locality_order(g);
+  }
   for (int j = 0; j < nprog; ++j) {
     const int c = g->jtw_prog[j] - 1;
     if (g->npoly[c] < 3 || g->npoly[c] > 6) return;  // left to the column kernel
@@ -610,12 +617,13 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int n
   th.order = order;
 }
 
-int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T) {
+int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T, int ord) {
   d.tile_T = d.ntiles = d.tile_nu_max = 0;
   d.tile_order = 0;
   d.tile_closed = false;
+  d.tile_ord = ord;
   TileHost th;
-  make_tiles(g, order, th, T);
+  make_tiles(g, order, th, T, 0, ord);
   if (!th.T) return OLAMGPU_OK;
   OG_CHECK(upload(d.tile_hdr, th.hdr.data(), th.hdr.size(), s));
   OG_CHECK(upload(d.tile_u, th.ulist.data(), th.ulist.size(), s));

@@ -529,7 +529,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   tp.tune_log.clear();
   const ShapeKey key{shape_key(&C.hgrid, ntp, order)};
   auto use = [&](const TileShape& sh) -> int {
-    if (d.tile_T != sh.T) OG_CHECK(build_tiles(&C.hgrid, d, order, s, sh.T));
+    if (d.tile_T != sh.T || d.tile_ord != sh.ord) OG_CHECK(build_tiles(&C.hgrid, d, order, s, sh.T, sh.ord));
     d.tile_G = sh.G;
     d.tile_KS = sh.KS;
     return OLAMGPU_OK;
@@ -543,20 +543,23 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   cudaEvent_t e0, e1;
   OG_CUDA(cudaEventCreate(&e0));
   OG_CUDA(cudaEventCreate(&e1));
-  TileShape best{0, 0, 0};
+  TileShape best{0, 0, 0, 0};
   float best_ms = 0.f;
   prof_suspend(true);
   int rc = OLAMGPU_OK;
+  // split level sweeps only help where the tiles do not fill the GPU
+  const int ks_max = (size_t)d.ntiles * (size_t)((ntp + 63) / 64) < 4 * 148 ? 2 : 1;
   const int Ts[2] = {32, 16};
+  for (int ord = 0; ord <= 1 && rc == OLAMGPU_OK; ++ord)
   for (int T : Ts) {
-    if (d.tile_T != T) {
-      rc = build_tiles(&C.hgrid, d, order, s, T);
+    if (d.tile_T != T || d.tile_ord != ord) {
+      rc = build_tiles(&C.hgrid, d, order, s, T, ord);
       if (rc != OLAMGPU_OK || d.tile_T != T) { rc = OLAMGPU_OK; continue; }   // no tables of this width
     }
     const int Gs[2] = {T == 32 ? 64 : 64, T == 32 ? 32 : 128};
     for (int G : Gs) {
       if (!tile_shape_fits(d, G)) continue;
-      for (int KS = 1; KS <= 2; ++KS) {
+      for (int KS = 1; KS <= ks_max; ++KS) {
         d.tile_G = G;
         d.tile_KS = KS;
         float ms = 1e30f;
@@ -571,8 +574,8 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
           if (r > 0) ms = std::min(ms, t);   // the first run warms up
         }
         if (rc != OLAMGPU_OK) break;
-        tp.tune_log.push_back({T, G, KS, 0, ms});
-        if (!best.T || ms < best_ms) { best = TileShape{T, G, KS}; best_ms = ms; }
+        tp.tune_log.push_back({T, G, KS, ord, 0, ms});
+        if (!best.T || ms < best_ms) { best = TileShape{T, G, KS, ord}; best_ms = ms; }
       }
       if (rc != OLAMGPU_OK) break;
     }
@@ -584,7 +587,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   OG_CHECK(rc);
   if (!best.T) { set_error("tile autotune: no shape runs on this grid"); return OLAMGPU_E_UNSUPPORTED; }
   for (auto& r : tp.tune_log)
-    if (r.T == best.T && r.G == best.G && r.KS == best.KS) r.chosen = 1;
+    if (r.T == best.T && r.G == best.G && r.KS == best.KS && r.ord == best.ord) r.chosen = 1;
   OG_CHECK(use(best));
   g_shape_cache[key] = best;
   tp.tuned_ntp = ntp;

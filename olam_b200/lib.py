@@ -84,7 +84,7 @@ def load():
     lib.olamgpu_set_surface_emission.argtypes = [C.POINTER(abi.c_float_p)]
     lib.olamgpu_window_forward.argtypes = [C.c_int, C.c_int, C.c_uint]
     lib.olamgpu_window_adjoint.argtypes = [C.POINTER(abi.c_float_p), C.POINTER(abi.c_float_p)]
-    lib.olamgpu_set_tile_shape.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.olamgpu_set_tile_shape.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
     lib.olamgpu_tile_shape.argtypes = [abi.c_int_p, C.c_int, abi.c_int_p, abi.c_float_p]
     for name in EXPORTS:
         if name not in ("olamgpu_strerror", "olamgpu_stream", "olamgpu_launch_count"):
@@ -226,19 +226,18 @@ class OlamGpu:
         arr = (abi.c_float_p * len(self._emis))(*[abi.ptr(e, C.c_float) for e in self._emis])
         check(self.lib.olamgpu_set_surface_emission(arr))
 
-    def set_tile_shape(self, T=0, G=0, KS=0):
-        check(self.lib.olamgpu_set_tile_shape(int(T), int(G), int(KS)))
+    def set_tile_shape(self, T=0, G=0, KS=0, ord=0):
+        check(self.lib.olamgpu_set_tile_shape(int(T), int(G), int(KS), int(ord)))
 
     def tile_shape(self, maxn=32):
-        """((T, G, KS) in use, [(T, G, KS, chosen, ms) of the last tuning])."""
-        shape = np.zeros(3, np.int32)
-        cand = np.zeros(4 * maxn, np.int32)
+        """((T, G, KS, ord) in use, [(T, G, KS, ord, chosen, ms) of the last tuning])."""
+        shape = np.zeros(4, np.int32)
+        cand = np.zeros(5 * maxn, np.int32)
         ms = np.zeros(maxn, np.float32)
         n = self.lib.olamgpu_tile_shape(abi.ptr(shape, C.c_int), maxn, abi.ptr(cand, C.c_int), abi.ptr(ms, C.c_float))
         if n < 0:
             check(-n)
-        log = [(int(cand[4 * i]), int(cand[4 * i + 1]), int(cand[4 * i + 2]), int(cand[4 * i + 3]), float(ms[i]))
-               for i in range(min(n, maxn))]
+        log = [tuple(int(x) for x in cand[5 * i:5 * i + 5]) + (float(ms[i]),) for i in range(min(n, maxn))]
         return tuple(int(x) for x in shape), log
 
     def window_forward(self, nsteps, nchk, flags=0):

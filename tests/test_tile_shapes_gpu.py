@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-5
 
-SHAPES = [(32, 64, 1), (32, 32, 1), (16, 64, 1), (16, 128, 1), (32, 64, 2), (32, 32, 3), (16, 128, 2)]
+SHAPES = [(32, 64, 1, 0), (32, 32, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0), (32, 64, 2, 0), (32, 32, 3, 1),
+          (16, 128, 2, 1), (32, 64, 1, 1)]
 
 
 def tracers(g, ntr, seed):
@@ -63,9 +64,9 @@ def test_autotuner_picks_a_timed_shape_and_agrees_with_it():
     opts = abi.make_opts(1800.0)
     out, used, log = run(g, st, opts, tr, steps=2)
     assert len(log) >= 4
-    chosen = [r for r in log if r[3]]
-    assert len(chosen) == 1 and chosen[0][:3] == used
-    assert chosen[0][4] == min(r[4] for r in log)
+    chosen = [r for r in log if r[4]]
+    assert len(chosen) == 1 and chosen[0][:4] == used
+    assert chosen[0][5] == min(r[5] for r in log)
     forced, used2, _ = run(g, st, opts, tr, shape=used, steps=2)
     assert used2 == used
     assert np.array_equal(out, forced)
@@ -78,7 +79,7 @@ def test_per_call_mode_with_a_tuned_shape():
     tr = tracers(g, 72, seed=9)
     opts = abi.make_opts(1800.0)
     ref = oracle_lib.scalar_transport(abi.FortranGrid(g), opts, tr, [np.zeros_like(t) for t in tr], st, fp64=True)
-    for shape in ((16, 128, 2), (32, 32, 1)):
+    for shape in ((16, 128, 2, 0), (32, 32, 1, 1)):
         out, used, _ = run(g, st, opts, tr, shape, coherence=abi.SYNC_EACH_CALL)
         for n in range(len(tr)):
             assert relerr(out[n][1:], ref[n][1:]) < TOL64, (shape, n)
