@@ -216,7 +216,7 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
 // KS chunks run by different blocks (A.ks).
 // OFF: the type of element offsets into the batched arrays -- unsigned when
 // they all fit in 32 bits (fewer address instructions), else long long.
-template <int NC, int LPC, typename OFF>
+template <int NC, int LPC, typename OFF, bool SPLIT>
 __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
     k_tile(TileArgs A, const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -227,16 +227,16 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
   constexpr int RB = 4 * G;                  // bytes of a staged row
   // block order: tile, then level chunk, then tracer group (the groups of a
   // tile run side by side, so its records are read once from HBM)
-  const int ngrp = A.ngrp, nks = A.ks;
+  const int ngrp = A.ngrp, nks = SPLIT ? A.ks : 1;
   const int tile = blockIdx.x / (ngrp * nks);
   const int rem = blockIdx.x - tile * ngrp * nks;
-  const int ks = rem / ngrp, grp = A.grp0 + (rem - ks * ngrp);
+  const int ks = SPLIT ? rem / ngrp : 0, grp = A.grp0 + (rem - ks * ngrp);
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;   // kb: the lowest floor of any column
-  // this block's levels [klo, khi)
-  const int chunk = (mza - kb + nks - 1) / nks;
-  const int klo = kb + ks * chunk, khi = min(mza, klo + chunk);
+  // this block's levels [klo, khi) (the whole column without a split)
+  const int chunk = SPLIT ? (mza - kb + nks - 1) / nks : mza - kb;
+  const int klo = SPLIT ? kb + ks * chunk : kb, khi = SPLIT ? min(mza, klo + chunk) : mza;
   const int nu4 = (nU + 3) & ~3;      // rows gathered four at a time
   auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
   const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * RB), rbuf = al((size_t)T * TILE_WR * 4);
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
   float* FEX = reinterpret_cast<float*>(p);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int t0 = grp * G;
-  if (klo >= khi) return;   // an empty chunk (more chunks than levels): uniform per block
+  if (SPLIT && klo >= khi) return;   // an empty chunk (more chunks than levels): uniform per block
 
   // tables of this tile, checked once: every index must address the arrays
   // it is used on (a failure is recorded and the block does nothing)
@@ -329,8 +329,8 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
     if (c < nT && act) {
       cbase[n] = (OFF)IWT[c] * (OFF)mza * (OFF)ntp + (OFF)(t0 + 4 * hl);
       // a chunk above the column's floor starts with the rows below it
-      if (klo - 2 >= kbc[n]) m2[n] = ldg4(A.S + (cbase[n] + (OFF)(klo - 2) * (OFF)ntp));
-      if (klo - 1 >= kbc[n]) m1[n] = ldg4(A.S + (cbase[n] + (OFF)(klo - 1) * (OFF)ntp));
+      if (SPLIT && klo - 2 >= kbc[n]) m2[n] = ldg4(A.S + (cbase[n] + (OFF)(klo - 2) * (OFF)ntp));
+      if (SPLIT && klo - 1 >= kbc[n]) m1[n] = ldg4(A.S + (cbase[n] + (OFF)(klo - 1) * (OFF)ntp));
       if (klo + 1 < mza) p1[n] = ldg4(A.S + (cbase[n] + (OFF)(klo + 1) * (OFF)ntp));
       if (klo + 2 < mza) p2[n] = ldg4(A.S + (cbase[n] + (OFF)(klo + 2) * (OFF)ntp));
       if (klo + 3 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(klo + 3) * (OFF)ntp));
@@ -443,12 +443,17 @@ bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
 
 // the stage kernel of a tile shape (T columns, G tracers per block)
 using TileKern = void (*)(TileArgs, const CUtensorMap, const CUtensorMap);
-static TileKern tile_kernel(int T, int G, bool off32) {
-  if (T == 32 && G == 64) return off32 ? k_tile<2, 16, unsigned> : k_tile<2, 16, long long>;
-  if (T == 32 && G == 32) return off32 ? k_tile<1, 8, unsigned> : k_tile<1, 8, long long>;
-  if (T == 16 && G == 64) return off32 ? k_tile<1, 16, unsigned> : k_tile<1, 16, long long>;
-  if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned> : k_tile<2, 32, long long>;
+template <bool SPLIT>
+static TileKern tile_kernel_s(int T, int G, bool off32) {
+  if (T == 32 && G == 64) return off32 ? k_tile<2, 16, unsigned, SPLIT> : k_tile<2, 16, long long, SPLIT>;
+  if (T == 32 && G == 32) return off32 ? k_tile<1, 8, unsigned, SPLIT> : k_tile<1, 8, long long, SPLIT>;
+  if (T == 16 && G == 64) return off32 ? k_tile<1, 16, unsigned, SPLIT> : k_tile<1, 16, long long, SPLIT>;
+  if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned, SPLIT> : k_tile<2, 32, long long, SPLIT>;
   return nullptr;
+}
+// the kernel of a shape; the level sweep is split (KS > 1) only in its own instance
+static TileKern tile_kernel(int T, int G, bool off32, int KS = 1) {
+  return KS > 1 ? tile_kernel_s<true>(T, G, off32) : tile_kernel_s<false>(T, G, off32);
 }
 
 // the largest dynamic shared memory a block may use
@@ -484,7 +489,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   const unsigned nblk = (unsigned)d.ntiles * (unsigned)ngrp_run * (unsigned)KS;
   // element offsets in 32 bits when every array of the batched layout fits
   const bool off32 = (double)d.mwa * d.mza * ntp < 4294967296.0;
-  const TileKern kern = tile_kernel(d.tile_T, G, off32);
+  const TileKern kern = tile_kernel(d.tile_T, G, off32, KS);
   if (!kern || smem > TILE_SMEM_LIMIT) {
     set_error("tile stage: no kernel for " + std::to_string(d.tile_T) + "-column tiles of " + std::to_string(G) +
               " tracers within the shared memory");
