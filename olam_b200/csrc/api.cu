@@ -19,6 +19,13 @@ int check_device_status() {
   int h[4];
   OG_CUDA(cudaMemcpyAsync(h, C.status.p, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
   OG_CUDA(cudaStreamSynchronize(C.stream));
+  if (h[0] == 130 || h[0] == 131) {
+    // the tiled stage kernel's level copies did not complete within its poll limit
+    set_error(std::string("a level copy of the tiled transport kernel timed out (tile ") + std::to_string(h[1]) +
+              ", block " + std::to_string(h[2]) + ", level " + std::to_string(h[3]) +
+              (h[0] == 131 ? "; copies were still in flight at exit)" : ")"));
+    return OLAMGPU_E_NUMERIC;
+  }
   if (h[0]) {
     set_error("a device bounds check failed (code " + std::to_string(h[0]) + ", value " + std::to_string(h[1]) +
               ", block " + std::to_string(h[2]) + ", thread " + std::to_string(h[3]) + ")");

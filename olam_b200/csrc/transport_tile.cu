@@ -398,7 +398,13 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
       }
     }
     if (__syncthreads_or(failed)) {
-      if (tid == 0 && atomicCAS(A.err, 0, 130) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = kd; }
+      // the copies of this level and of the next one may still be in flight
+      // into this block's shared memory: wait for them (bounded again) before
+      // the block exits and its shared memory is handed to another block
+      const bool cur_done = mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS);
+      const bool nxt_done = kd + 1 >= khi || mbar_wait_bounded(&BAR[cur ^ 1], ((lv + 1) >> 1) & 1, TILE_WAIT_POLLS);
+      const int code = (cur_done && nxt_done) ? 130 : 131;
+      if (tid == 0 && atomicCAS(A.err, 0, code) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = kd; }
       return;
     }
   }
