@@ -273,9 +273,14 @@ int olamgpu_scalar_transport_rk(const float* rho_old, olamgpu_cfl_diag* diag);
  * applies its transpose.  lam[n] (mza,mwa) holds dJ/d(new scp) of tracer n
  * on entry and dJ/d(old scp) on return; lam_sct[n] receives dJ/d(sct).
  * rho_old and the registered vmasc / wmasc / rho are those of the forward
- * step.  No counterpart in the reference (OLAM has no adjoint); any lpw /
- * lpv (terrain); iscal_monot > 0 and tracer diffusion get
- * OLAMGPU_E_UNSUPPORTED. */
+ * step.  With the positive-definite limiter (iscal_monot = 2, tracers with
+ * pdef set; update_scalar_pd, scalar_transport_rk.F90:1085-1472) the
+ * registered var_p / var_t must hold the forward step's inputs: the step is
+ * run forward again on the device, the limiter's branches (which faces are
+ * scaled, which factor is the minimum) are recorded, and the transpose of
+ * the step's Jacobian at that state is applied.  No counterpart in the
+ * reference (OLAM has no adjoint); any lpw / lpv (terrain); iscal_monot = 1
+ * and tracer diffusion get OLAMGPU_E_UNSUPPORTED. */
 int olamgpu_scalar_transport_rk_adjoint(const float* rho_old, float* const* lam, float* const* lam_sct);
 
 /* Replaces prog_wrtv_rk() (prog_wrtv_rk.f90:58-488); istp is mem_ijtabs%istp. */

@@ -28,6 +28,8 @@ module olamgpu_c
                                OLAMGPU_F_FACS = 2048, OLAMGPU_F_SCALARS = 4096,            &
                                OLAMGPU_F_SCALAR_TEND = 8192, OLAMGPU_F_EDDY = 16384,       &
                                OLAMGPU_F_ALL = 65535
+  integer(c_int), parameter :: OLAMGPU_TS_GRAPH = 1, OLAMGPU_TS_HORIZ_K = 2, &
+                               OLAMGPU_TS_MAXMIN = 4, OLAMGPU_TS_MASS = 8
 
   type, bind(C) :: olamgpu_grid
      integer(c_int) :: mza, mwa, mva, mma
@@ -154,6 +156,36 @@ module olamgpu_c
      integer(c_int) function olamgpu_set_halo(halo) bind(C, name="olamgpu_set_halo")
        import :: c_int, olamgpu_halo
        type(olamgpu_halo), intent(in) :: halo
+     end function
+     integer(c_int) function olamgpu_timestep(flags, nmass, mass_ids) bind(C, name="olamgpu_timestep")
+       import :: c_int
+       integer(c_int), value :: flags, nmass
+       integer(c_int), intent(in) :: mass_ids(*)
+     end function
+     ! emis(n): c_loc of scalar n's (mwa) surface source, or c_null_ptr
+     integer(c_int) function olamgpu_set_surface_emission(emis) bind(C, name="olamgpu_set_surface_emission")
+       import :: c_int, c_ptr
+       type(c_ptr), intent(in) :: emis(*)
+     end function
+     integer(c_int) function olamgpu_window_forward(nsteps, nchk, flags) bind(C, name="olamgpu_window_forward")
+       import :: c_int
+       integer(c_int), value :: nsteps, nchk, flags
+     end function
+     integer(c_int) function olamgpu_window_adjoint(lam, lam_sct) bind(C, name="olamgpu_window_adjoint")
+       import :: c_int, c_ptr
+       type(c_ptr), intent(in) :: lam(*)
+       type(c_ptr), intent(in) :: lam_sct(*)
+     end function
+     integer(c_int) function olamgpu_set_tile_shape(t, g, ks, ord) bind(C, name="olamgpu_set_tile_shape")
+       import :: c_int
+       integer(c_int), value :: t, g, ks, ord
+     end function
+     integer(c_int) function olamgpu_tile_shape(shape, nmax, cand, ms) bind(C, name="olamgpu_tile_shape")
+       import :: c_int, c_float
+       integer(c_int), intent(out) :: shape(4)
+       integer(c_int), value :: nmax
+       integer(c_int), intent(out) :: cand(*)
+       real(c_float), intent(out) :: ms(*)
      end function
      integer(c_int) function olamgpu_finalize() bind(C, name="olamgpu_finalize")
        import :: c_int

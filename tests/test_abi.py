@@ -26,6 +26,15 @@ def test_library_exports_header_symbols():
     assert set(names) == set(lib.EXPORTS)
 
 
+def test_fortran_interfaces_name_header_symbols():
+    # every bind(C) interface of the Fortran module binds an entry point the
+    # header declares
+    src = open(os.path.join(ROOT, "olam_b200", "fortran", "olamgpu.f90")).read()
+    bound = set(re.findall(r'bind\(C,\s*name="(olamgpu_[a-z0-9_]+)"\)', src))
+    assert len(bound) >= 20
+    assert not bound - set(_declared()), sorted(bound - set(_declared()))
+
+
 def test_struct_sizes_match_header():
     # field counts of the ctypes mirror follow the header's declarations
     txt = open(os.path.join(ROOT, "include", "olamgpu.h")).read()
@@ -55,6 +64,9 @@ def test_strerror_and_state_errors():
     assert L.olamgpu_timestep(0, 0, None) == abi.E_STATE
     assert L.olamgpu_timestep_diag(None, None) == abi.E_STATE
     assert L.olamgpu_set_halo(None) == abi.E_STATE
+    assert L.olamgpu_set_surface_emission(None) == abi.E_STATE
+    assert L.olamgpu_window_forward(2, 1, 0) == abi.E_STATE
+    assert L.olamgpu_window_adjoint(None, None) == abi.E_STATE
 
 
 def test_null_arguments_rejected():
