@@ -515,6 +515,12 @@ def bench_window(a, max_over_ranks):
             t[...] = t0
         dev.sync_to_device(abi.F_SCALARS)
         torch.cuda.synchronize()
+
+        def used_gb():
+            free, total = torch.cuda.mem_get_info()
+            return (total - free) / 1e9
+
+        mem = {"after_first_step": used_gb()}
         stream = torch.cuda.ExternalStream(dev.stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -534,7 +540,9 @@ def bench_window(a, max_over_ranks):
             np.add.at(lam[n], (iw, kk), w[n].astype(np.float32))
             J += float((lam[n].astype(np.float64) * var_p[n]).sum())
         dev.profile(True, reset=True)
+        mem["after_forward"] = used_gb()
         g0, gs = dev.window_adjoint(lam)
+        mem["after_adjoint"] = used_gb()
         prof = dev.profile_read()
         dev.profile(False, reset=True)
         adj_ms = max_over_ranks(prof["window_adjoint"][0])
@@ -550,6 +558,7 @@ def bench_window(a, max_over_ranks):
             + prof.get("adj_implicit", (0.0, 0))[0],
             "loss": J, "loss_from_gradient": lin,
             "euler_relerr": abs(lin - J) / abs(J) if J else None,
+            "device_gb_in_use": mem,
             "check": "J(x0, E) = <dJ/dx0, x0> + <dJ/dE, E> for the unlimited (linear) step"
                      if a.win_monot == 0 else "limited step: no linear identity",
         })
@@ -774,8 +783,9 @@ def main():
                   "candidates_ms_per_stage": [{"T": r[0], "G": r[1], "KS": r[2], "order": r[3], "ms": r[5]}
                                               for r in tlog],
                   "note": "columns per tile, tracers per block, level chunks per tile, tile order (0: the "
-                          "library's curve, 1: the caller's numbering); chosen by the library's autotuner "
-                          "on the first step"}
+                          "library's curve, 1: the caller's numbering); "
+                          + ("forced by --tile-shape" if a.tile_shape else
+                             "chosen by the library's autotuner on the first step")}
     dev.profile(False, reset=True)
     clk = clocks.stop()
     barrier()

@@ -168,6 +168,11 @@ static void release_all() {
                          &d.volti, &d.ew_b, &d.ew_u, &d.tile_a, &d.tile_band};
   for (auto* b : fb) b->release();
   d.ew_order = 0;
+  {
+    auto& a = d.adj_tiles;
+    a.hdr.release(); a.u.release(); a.tc.release(); a.rev.release();
+    a.T = a.ntiles = a.nu_max = a.order = 0;
+  }
   d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
   d.tile_G = 64;
   d.tile_KS = 1;

@@ -161,6 +161,14 @@ struct DevGrid {
   int tile_G = 64, tile_KS = 1;  // the stage kernel's tracers per block and level chunks
   int tile_ord = 0;              // the order the tiles run along (make_tiles)
   bool tile_closed = false;      // every neighbourhood column is prognosed
+  // The adjoint's own tiles when the stage kernel runs another width: the
+  // reverse stage moves half as many bytes again per row as the forward and
+  // is fastest on 32-column tiles (fewer halo rows per column); the same
+  // tables as above, built on first use (T = 0: not built).
+  struct {
+    DevBuf<int> hdr, u, tc, rev;
+    int T = 0, ntiles = 0, nu_max = 0, order = 0;
+  } adj_tiles;
   std::vector<int> h_lpw;        // host copies used at set-up
 };
 
@@ -411,6 +419,7 @@ struct TileHost {
 // columns' positions, 1 the caller's jtw_prog
 void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0, int nu_cap = 0, int ord = 0);
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T = 0, int ord = 0);
+int build_adj_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
 // dynamic shared memory of the stage kernel: T columns, nu_max rows of rb bytes
 size_t tile_smem_bytes(int T, int nu_max, int rb);
 

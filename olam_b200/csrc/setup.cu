@@ -649,4 +649,25 @@ int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, in
   return OLAMGPU_OK;
 }
 
+// 32-column tiles along the library's curve for the adjoint's reverse stage
+// (hdr, U list, tile-cell records, transposed slots); none if they do not
+// fit in shared memory
+int build_adj_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s) {
+  auto& a = d.adj_tiles;
+  a.T = a.ntiles = a.nu_max = 0;
+  TileHost th;
+  make_tiles(g, order, th, 32, 0, 0);
+  if (th.T != 32) return OLAMGPU_OK;
+  OG_CHECK(upload(a.hdr, th.hdr.data(), th.hdr.size(), s));
+  OG_CHECK(upload(a.u, th.ulist.data(), th.ulist.size(), s));
+  OG_CHECK(upload(a.tc, th.tc.data(), th.tc.size(), s));
+  OG_CHECK(upload(a.rev, th.rev.data(), th.rev.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));
+  a.T = th.T;
+  a.ntiles = th.ntiles;
+  a.nu_max = th.nu_max;
+  a.order = order;
+  return OLAMGPU_OK;
+}
+
 }  // namespace olamgpu

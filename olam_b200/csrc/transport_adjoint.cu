@@ -436,22 +436,39 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   }
 }
 
+// the tiles the reverse stage runs: the adjoint's own 32-column tiles when
+// they are built and fit in shared memory, else the stage kernel's
+struct AdjTiles {
+  const int4* hdr;
+  const int *u, *tc, *rev;
+  int T, ntiles, nu_max;
+};
+
+static AdjTiles adj_tiles_of(const DevGrid& d) {
+  const auto& a = d.adj_tiles;
+  if (a.T == 32 && a.order == d.tile_order && tile_adj_smem_bytes(a.T, a.nu_max) <= 227 * 1024)
+    return {reinterpret_cast<const int4*>(a.hdr.p), a.u.p, a.tc.p, a.rev.p, a.T, a.ntiles, a.nu_max};
+  return {reinterpret_cast<const int4*>(d.tile_hdr.p), d.tile_u.p, d.tile_tc.p, d.tile_rev.p,
+          d.tile_T, d.ntiles, d.tile_nu_max};
+}
+
 static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L, float* LIN, float* L0, float* LS,
                            int ntp, int istage, int nrk, float dtr, int first, int last, int* status,
                            cudaStream_t s, const int* skip = nullptr, int ntr = 0) {
+  const AdjTiles t = adj_tiles_of(d);
   TileAdjArgs A;
   A.skip = skip; A.ntr = ntr;
   A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1; A.lpw = d.lpw.p;
-  A.ntiles = d.ntiles; A.T = d.tile_T; A.nu_max = d.tile_nu_max; A.mwa = d.mwa;
+  A.ntiles = t.ntiles; A.T = t.T; A.nu_max = t.nu_max; A.mwa = d.mwa;
   A.dtr = dtr; A.first = first; A.last = last;
-  A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
-  A.ulist = d.tile_u.p; A.tc = d.tile_tc.p; A.rev = d.tile_rev.p;
+  A.hdr = t.hdr;
+  A.ulist = t.u; A.tc = t.tc; A.rev = t.rev;
   A.ff = tp.ff.p; A.trec = tp.adj_trec.p;
   A.L = L; A.LIN = LIN; A.L0 = L0; A.LS = LS;
   A.err = status;
-  const size_t smem = tile_adj_smem_bytes(d.tile_T, d.tile_nu_max);
-  const unsigned nblk = (unsigned)d.ntiles * (unsigned)((ntp + 63) / 64);
-  if (d.tile_T == 32) {
+  const size_t smem = tile_adj_smem_bytes(t.T, t.nu_max);
+  const unsigned nblk = (unsigned)t.ntiles * (unsigned)((ntp + 63) / 64);
+  if (t.T == 32) {
     OG_CUDA(cudaFuncSetAttribute(k_tile_adj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_tile_adj<2><<<nblk, TADJ_THREADS, smem, s>>>(A);
   } else {
@@ -468,13 +485,14 @@ static int launch_adj_records(const DevGrid& d, Transport& tp, int* status, cuda
     OG_CHECK(tp.adj_trec.alloc(n));
     OG_CUDA(cudaMemsetAsync(tp.adj_trec.p, 0, tp.adj_trec.bytes(), s));
   }
+  const AdjTiles t = adj_tiles_of(d);
   AdjRecArgs R;
-  R.mza = d.mza; R.T = d.tile_T; R.kb = 1; R.mwa = d.mwa; R.lpw = d.lpw.p;
-  R.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
-  R.ulist = d.tile_u.p; R.tc = d.tile_tc.p; R.rev = d.tile_rev.p;
+  R.mza = d.mza; R.T = t.T; R.kb = 1; R.mwa = d.mwa; R.lpw = d.lpw.p;
+  R.hdr = t.hdr;
+  R.ulist = t.u; R.tc = t.tc; R.rev = t.rev;
   R.wrec = tp.wrec.p; R.wmasc = tp.wmasc.p; R.a_w = d.a_w.p; R.trec = tp.adj_trec.p;
   R.err = status;
-  k_adj_records<<<(unsigned)d.ntiles * d.tile_T, 64, 0, s>>>(R);
+  k_adj_records<<<(unsigned)t.ntiles * t.T, 64, 0, s>>>(R);
   OG_LAUNCHED();
   return OLAMGPU_OK;
 }
@@ -521,9 +539,12 @@ static int adjoint_checks(Context& C) {
 }
 
 int adjoint_core(Context& C, const float* rho_old_host) {
-  const DevGrid& d = C.g;
   Transport& tp = C.tp;
   cudaStream_t s = C.stream;
+  // the adjoint's 32-column tiles, once per grid, when the stage kernel runs narrower ones
+  if (C.g.tile_T != 32 && (C.g.adj_tiles.T == 0 || C.g.adj_tiles.order != C.g.tile_order))
+    OG_CHECK(build_adj_tiles(&C.hgrid, C.g, C.g.tile_order, s));
+  const DevGrid& d = C.g;
   const int mza = d.mza, mwa = d.mwa;
   const int nrk = C.opts.nrk_scal;
   const int ntp = C.tr.ntp;
