@@ -413,8 +413,8 @@ def bench_long_step(g, tr, a, max_over_ranks):
     # bytes each launch must move at least (every array element it reads or
     # writes once; stage-averaged for wrt_begs over the 3 RK stages)
     algo = {
-        "setup_w": 76 * cw, "setup_v": 16 * cv, "vmca": 20 * cv, "grad4": 48 * cw, "upw4": 36 * cw,
-        "upv4": 20 * cv + 48 * cw, "wrt_begs": (136 + 16 / 3) * cw + 24 * cv, "prog_v": 24 * cv + 28 * cw,
+        "setup_w": 76 * cw, "setup_v": 16 * cv, "vmca": 20 * cv, "upw4": 36 * cw,
+        "grad_upv4": 16 * cw + 20 * cv, "wrt_begs": (136 + 16 / 3) * cw + 24 * cv, "prog_v": 24 * cv + 28 * cw,
         "vel_t3d": 16 * cw + 4 * cv,
     }
     kern = {}

@@ -8,13 +8,16 @@
 //   k_vmca                  vmca and vmasc on the last stage   (prog_wrtv_rk.f90:320-368); the
 //                           stage copies *_rk = *_short and vmca of the other stages are
 //                           formed inside k_wrt_begs
-//   k_grad4, k_upw4, k_upv4 fluxes_wrtv for thil, vxe, vye, vze (:950-1129), the four
-//                           fields of one stage in one launch each; on the
-//                           last stage the fields with ithil_monot /
-//                           iwind_monot > 0 take dynamics_monot.cu's values
+//   k_upw4, k_grad_upv4     fluxes_wrtv for thil, vxe, vye, vze (:950-1129), the four
+//                           fields of one stage in one launch each (the
+//                           gradients and the V-face values in one pass over
+//                           the W cells); on the last stage the fields with
+//                           ithil_monot / iwind_monot > 0 take
+//                           dynamics_monot.cu's values
 //   k_wrt_begs              prog_wrt_begs (:494-884): one warp per column, lanes over
-//                           levels for the explicit terms, one lane for the serial
-//                           tridiagonal solve (tridiffo, tridiag_lib.f90:10-36)
+//                           levels for the explicit terms and for the
+//                           tridiagonal solve (tridiffo, tridiag_lib.f90:10-36,
+//                           by parallel cyclic reduction)
 //   k_prog_v                prog_v_begs (:888-946)
 //   k_vel_t3d               vel_t3d_hex (vel_t3d.f90:39-108)
 // With eddy diffusion registered, dynamics_eddy.cu's k_eddy_w follows
@@ -281,26 +284,34 @@ __global__ void k_vmca(DynK g, const int* __restrict__ vadj, int nv, const float
 
 struct Four { const float* f[4]; };
 
-// gradient planes of the fields in fmask (grad_t2d for ORD 2, or
-// grad_t2d_quadratic with bounded=.false. for ORD 3, as fluxes_wrtv calls
-// them).  gx layout: [field][plane][iw][kd].  The neighbour loop is outside
-// the field loop: each neighbour's table entries and coefficients are read
-// once for the four fields, and the four gathers are independent.
+struct VSide { const float* dxps; const float* dyps; const float* xx0_v; const float* xy0_v; const float* yy0_v; };
+
+// The horizontal face values of fluxes_wrtv (prog_wrtv_rk.f90:973-1075) in
+// one pass over the W cells: grad_t2d (ORD 2) or grad_t2d_quadratic with
+// bounded=.false. (ORD 3) of the fields in gmask, kept in registers, then
+// scalar_v_column for the faces this cell is upwind of -- side 1 of the
+// face unless vmc < 0 -- each face being written by exactly one of its two
+// cells: S(k,iw) + dxps dS/dx + dyps dS/dy (+ the quadratic terms at ORD 3)
+// for the fields in gmask, S(k,iw) alone for those in pmask.  No gradient
+// planes go through memory.  Thread per (column, level); the neighbour loop
+// is outside the field loop, so each neighbour's table entries and
+// coefficients are read once for the four fields.
 template <int ORD>
-__global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s, unsigned fmask,
-                        const float* __restrict__ cx, const float* __restrict__ cy,
-                        const float* __restrict__ xy_hu, float* __restrict__ gx) {
+__global__ void k_grad_upv4(DynK g, const int* __restrict__ prog, int nprog, Four s, unsigned gmask,
+                            unsigned pmask, const float* __restrict__ cx, const float* __restrict__ cy,
+                            const float* __restrict__ xy_hu, VSide c, const float* __restrict__ vmc,
+                            float* __restrict__ upv) {
   PK(j, kd, nprog);
   constexpr int NPL = ORD == 2 ? 2 : 5;
   const int iw = WTAB(j);
   const unsigned mza = g.mza;
-  const size_t plane = (size_t)g.mwa * mza;
+  const size_t vplane = (size_t)g.mva * mza;
   const unsigned x = (unsigned)iw * mza + kd;
   const int np = g.npoly[iw];
   float c0[4], a[4][NPL];
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
-    c0[f] = ((fmask >> f) & 1u) ? s.f[f][x] : 0.f;
+    c0[f] = (((gmask | pmask) >> f) & 1u) ? s.f[f][x] : 0.f;
 #pragma unroll
     for (int m = 0; m < NPL; ++m) a[f][m] = 0.f;
   }
@@ -320,18 +331,33 @@ __global__ void k_grad4(DynK g, const int* __restrict__ prog, int nprog, Four s,
     const unsigned xn = (unsigned)iwn * mza + kd;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-      if (!((fmask >> f) & 1u)) continue;
+      if (!((gmask >> f) & 1u)) continue;
       const float d = s.f[f][xn] - c0[f];
 #pragma unroll
       for (int m = 0; m < NPL; ++m) a[f][m] = a[f][m] + w[m] * d;
     }
   }
 #pragma unroll
-  for (int f = 0; f < 4; ++f) {
-    if (!((fmask >> f) & 1u)) continue;
-    float* G = gx + (size_t)f * 5 * plane;
+  for (int n = 0; n < 7; ++n) {
+    if (n >= np) break;
+    const int iv = g.w_ev[iw * 8 + n];
+    if (kd < LPV(iv)) continue;
+    const unsigned xv = (unsigned)iv * mza + kd;
+    const int side = g.v_iw[iv * 2] == iw ? 0 : 1;
+    if ((vmc[xv] < 0.f) != (side == 1)) continue;   // the other cell is upwind
+    const float dx = c.dxps[iv * 2 + side], dy = c.dyps[iv * 2 + side];
+    float xx = 0.f, xy = 0.f, yy = 0.f;
+    if (ORD == 3) { xx = c.xx0_v[iv * 2 + side]; xy = c.xy0_v[iv * 2 + side]; yy = c.yy0_v[iv * 2 + side]; }
 #pragma unroll
-    for (int m = 0; m < NPL; ++m) G[m * plane + x] = a[f][m];
+    for (int f = 0; f < 4; ++f) {
+      if (!(((gmask | pmask) >> f) & 1u)) continue;
+      float v = c0[f];
+      if ((gmask >> f) & 1u) {
+        v = v + dx * a[f][0] + dy * a[f][1];
+        if (ORD == 3) v = v + xx * a[f][2] + xy * a[f][3] + yy * a[f][4];
+      }
+      upv[(size_t)f * vplane + xv] = v;
+    }
   }
 }
 
@@ -363,44 +389,6 @@ __global__ void k_upw4(DynK g, const int* __restrict__ prog, int nprog, Four s, 
       v = b + dsk * c1 + dskm1 * c2;
     }
     upw[(size_t)f * plane + cb + kd] = v;
-  }
-}
-
-struct VSide { const float* dxps; const float* dyps; const float* xx0_v; const float* xy0_v; const float* yy0_v; };
-
-// V-face values of the four fields, from the upwind cell only (the side the
-// sign of vmc selects): fields in gmask add the linear gradient terms,
-// fields in qmask also the quadratic ones (order 3)
-__global__ void k_upv4(DynK g, const int* __restrict__ vadj, int nv, Four s, unsigned gmask, unsigned qmask,
-                       const float* __restrict__ gx, VSide c, const float* __restrict__ vmc,
-                       float* __restrict__ upv) {
-  PK(j, kd, nv);
-  const int iv = VATAB(j);
-  if (kd < LPV(iv)) return;
-  const unsigned mza = g.mza;
-  const size_t plane = (size_t)g.mwa * mza, vplane = (size_t)g.mva * mza;
-  const unsigned xv = (unsigned)iv * mza + kd;
-  // both sides' table entries load alongside vmc; the sign picks one
-  const float vm = vmc[xv];
-  const int2 iwp = *reinterpret_cast<const int2*>(g.v_iw + iv * 2);
-  const float2 dxp = *reinterpret_cast<const float2*>(c.dxps + iv * 2);
-  const float2 dyp = *reinterpret_cast<const float2*>(c.dyps + iv * 2);
-  const bool neg = vm < 0.f;
-  const int side = neg ? 1 : 0;
-  const int iw = neg ? iwp.y : iwp.x;
-  const unsigned xw = (unsigned)iw * mza + kd;
-  const float dx = neg ? dxp.y : dxp.x, dy = neg ? dyp.y : dyp.x;
-  float xx = 0.f, xy = 0.f, yy = 0.f;
-  if (qmask) { xx = c.xx0_v[iv * 2 + side]; xy = c.xy0_v[iv * 2 + side]; yy = c.yy0_v[iv * 2 + side]; }
-#pragma unroll
-  for (int f = 0; f < 4; ++f) {
-    float v = s.f[f][xw];
-    if ((gmask >> f) & 1u) {
-      const float* G = gx + (size_t)f * 5 * plane;
-      v = v + dx * G[xw] + dy * G[plane + xw];
-      if ((qmask >> f) & 1u) v = v + xx * G[2 * plane + xw] + xy * G[3 * plane + xw] + yy * G[4 * plane + xw];
-    }
-    upv[(size_t)f * vplane + xv] = v;
   }
 }
 
@@ -919,7 +907,6 @@ static int ensure_dyn_buffers(Context& C) {
   for (auto* b : v) OG_CHECK(A(*b, vz));
   OG_CHECK(A(y.upw, 4 * wz));
   OG_CHECK(A(y.upv, 4 * vz));
-  OG_CHECK(A(y.gx, 20 * wz));
   OG_CHECK(A(y.div2d, 2 * wz));
   OG_CHECK(A(y.vort2d, 2 * mz));
   OG_CHECK(A(y.fvorth, C.g.mva)); OG_CHECK(A(y.fvortl, C.g.mva));
@@ -1180,9 +1167,15 @@ int dyn_prog_wrtv_rk(int istp) {
     unsigned m2 = 0, m3 = 0;
     for (int q = 0; q < 4; ++q) { if (ordf[q] == 2) m2 |= 1u << q; if (ordf[q] >= 3) m3 |= 1u << q; }
     {
-      OG_PROF("grad4", s);
-      // on a rank with a halo the gradients of ring 1 are computed here (the
-      // reference exchanges them): over jtw_wadj, the owned columns and ring 1
+      OG_PROF("upw4", s);
+      k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p);
+      OG_LAUNCHED();
+    }
+    {
+      OG_PROF("grad_upv4", s);
+      // every face of jtv_wadj is written by its upwind cell: the columns
+      // (and on a rank with a halo, ring 1, whose gradients the reference
+      // exchanges) hold the gradients of their own faces' upwind sides
       DynK gg = g;
       const int* gt = d.jtw_prog.p;
       int gn = d.nw_prog;
@@ -1193,15 +1186,18 @@ int dyn_prog_wrtv_rk(int istp) {
         gn = d.nw_wadj;
         nbg = cdiv((size_t)gn * mza, 256);
       }
-      if (m2) { k_grad4<2><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m2, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
-      if (m3) { k_grad4<3><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m3, d.gxc.p, d.gyc.p, d.xy_hu.p, y.gx.p); OG_LAUNCHED(); }
-    }
-    { OG_PROF("upw4", s); k_upw4<<<nbw, 256, 0, s>>>(g, d.jtw_prog.p, d.nw_prog, f, y.wmc.p, y.upw.p); OG_LAUNCHED(); }
-    {
-      OG_PROF("upv4", s);
       VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
-      k_upv4<<<nbva, 256, 0, s>>>(g, d.jtv_wadj.p, d.nv_wadj, f, m2 | m3, m3, y.gx.p, vs, y.vmc.p, y.upv.p);
-      OG_LAUNCHED();
+      const unsigned plain = 0xFu & ~(m2 | m3);
+      if (m2 || plain) {
+        k_grad_upv4<2><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m2, plain, d.gxc.p, d.gyc.p, d.xy_hu.p, vs, y.vmc.p,
+                                           y.upv.p);
+        OG_LAUNCHED();
+      }
+      if (m3) {
+        k_grad_upv4<3><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m3, 0u, d.gxc.p, d.gyc.p, d.xy_hu.p, vs, y.vmc.p,
+                                           y.upv.p);
+        OG_LAUNCHED();
+      }
     }
     // last stage: flux-corrected face values replace those of the limited fields (370-399)
     if (last && thil_monot) {
@@ -1358,7 +1354,7 @@ void dyn_release() {
   DevBuf<float>* f[] = {&y.thil, &y.wmc, &y.vxe, &y.vye, &y.vze, &y.vmc, &y.vc, &y.alpha_press, &y.pwfac,
                         &y.pvfac, &y.thilt, &y.vmxet, &y.vmyet, &y.vmzet, &y.vmt, &y.wmc0, &y.vmc0, &y.vmca,
                         &y.sh_th, &y.sh_vx, &y.sh_vy, &y.sh_vz, &y.sh_vmt, &y.rk_vx, &y.rk_vy,
-                        &y.rk_vz, &y.upw, &y.upv, &y.gx, &y.div2d, &y.fdivh, &y.vort2d, &y.fvorth, &y.fvortl,
+                        &y.rk_vz, &y.upw, &y.upv, &y.div2d, &y.fdivh, &y.vort2d, &y.fvorth, &y.fvortl,
                         &y.vfact, &y.arv, &y.arw, &y.volwi, &y.volvi, &y.wn, &y.wno2, &y.vn, &y.ecv,
                         &y.gdz_wgtm, &y.gdz_wgtp, &y.dniv, &y.dniu, &y.dnv, &y.arw0, &y.arm0, &y.zfacit,
                         &y.dzit, &y.xx_yy, &y.xx_yy_m, &y.b20, &y.rayf_cof, &y.dn01d, &y.th01d, &y.vc03d,

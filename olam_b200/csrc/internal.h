@@ -286,7 +286,6 @@ struct Dyn {
   DevBuf<float> sh_th, sh_vx, sh_vy, sh_vz, sh_vmt;    // *_short
   DevBuf<float> rk_vx, rk_vy, rk_vz;                   // *_rk (thilt_rk stays in registers)
   DevBuf<float> upw, upv;        // 4 fields: thil, vxe, vye, vze
-  DevBuf<float> gx;              // gradient planes of the 4 fields
   DevBuf<float> div2d, fdivh, vort2d, fvorth, fvortl, vfact;
   DevBuf<int> lpmmin;
   // prognostic shaved-cell method: lve2 of every W column and the start

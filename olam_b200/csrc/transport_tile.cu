@@ -275,50 +275,40 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
       RIDX[i] = v * mza;
     }
   }
-  // the barrier region: a full barrier per level buffer, a count of the
-  // warps done with each buffer's level, an error flag, the last level issued
-  int* CNT = reinterpret_cast<int*>(BAR + 2);
-  volatile int* FLAG = CNT + 2;
-  volatile int* ISSUED = CNT + 3;
   if (tid == 0) {
-    mbar_init(&BAR[0], 1);
-    mbar_init(&BAR[1], 1);
-    CNT[0] = CNT[1] = 0;
-    *FLAG = 0;
-    *ISSUED = -1;
+    mbar_init(&BAR[0], TILE_NW);
+    mbar_init(&BAR[1], TILE_NW);
     mbar_init_fence();
   }
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
     return;
   }
+  for (int i = tid; i < nT; i += TILE_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
   const int seg = min(G, ntp - t0);  // tracers of this group (a multiple of 4)
-  // level k (lv = k - klo) into buffer b, completing on barrier b, issued by
-  // one thread: the U-row quadruples (TMA, RB bytes per row) and the records
-  // of the tile-column quadruples
+  // level k into buffer b, completing on barrier b: warp w's lane 0 gathers
+  // the U-row quadruples w, w + 8, ... (TMA, RB bytes per row) and the
+  // records of tile-column quadruples w, w + 8, ...
   auto stage = [&](int k, int b) {
+    if (lane != 0) return;
     const int ng = nu4 >> 2, nr = (nT + 3) >> 2;
-    *ISSUED = k - klo;
+    const int myg = warp < ng ? (ng - warp + TILE_NW - 1) / TILE_NW : 0;
+    const int myr = warp < nr ? (nr - warp + TILE_NW - 1) / TILE_NW : 0;
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&BAR[b], (unsigned)(ng * 4 * RB + nr * 4 * TILE_WR * 4));
+    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * RB + myr * 4 * TILE_WR * 4));
     char* Ub = UB + b * ubuf;
-    for (int g = 0; g < ng; ++g) {
+    for (int g = warp; g < ng; g += TILE_NW) {
       const int* r = RIDX + 4 * g;
       tma_gather4(Ub + 4 * g * RB, &tmS, t0, r[0] + k, r[1] + k, r[2] + k, r[3] + k, &BAR[b]);
     }
-    for (int q = 0; q < nr; ++q) {
+    for (int q = warp; q < nr; q += TILE_NW) {
       const int c0 = 4 * q;
       const int y0 = IWT[c0] * mza, y1 = IWT[min(c0 + 1, nT - 1)] * mza;
       const int y2 = IWT[min(c0 + 2, nT - 1)] * mza, y3 = IWT[min(c0 + 3, nT - 1)] * mza;
       tma_gather4(RBB + b * rbuf + c0 * TILE_WR * 4, &tmR, 0, y0 + k, y1 + k, y2 + k, y3 + k, &BAR[b]);
     }
   };
-  if (tid == 0) {
-    stage(klo, 0);
-    if (klo + 1 < khi) stage(klo + 1, 1);
-  }
-  for (int i = tid; i < nT; i += TILE_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
   // LPC lanes per column (columns cb, cb + TW, ...): lane hl of the group
   // holds tracers t0 + 4 hl .. + 3; the column's rows kd-2, kd-1, kd+1,
@@ -329,6 +319,7 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
   F4 m2[NC], m1[NC], p1[NC], p2[NC], p3[NC], s00[NC], st[NC];
   OFF cbase[NC];
   int kbc[NC];   // each column's own floor (lpw): levels below it are not prognosed
+  stage(klo, 0);
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
     const int c = cb + TW * n;
@@ -348,27 +339,13 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
     }
   }
   __syncthreads();   // the explicit fractions
-  // No block-wide barrier per level: a warp waits only for its level's
-  // copies, and the last warp to finish a level refills that level's buffer
-  // with the level two above (so warps may drift apart by up to two
-  // levels).  Every wait is bounded; a warp whose copies never complete
-  // raises the block's flag, and every warp that sees it waits (bounded
-  // again) for the copies issued and not yet consumed, and leaves.
+  // a level's copies are waited for at most TILE_WAIT_POLLS polls; a block
+  // whose copies never complete records it and stops at the level's end
+  int failed = 0;
   for (int kd = klo; kd < khi; ++kd) {
     const int lv = kd - klo, cur = lv & 1;
-    int failed = mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS) ? 0 : 1;
-    if (failed) *FLAG = 1;
-    if (__any_sync(0xffffffffu, failed | *FLAG)) {
-      // the levels lv .. ISSUED are in flight or complete: wait for them
-      bool drained = true;
-      const int last = min(*ISSUED, lv + 1);
-      for (int l = lv; l <= last; ++l)
-        if (!mbar_wait_bounded(&BAR[l & 1], (l >> 1) & 1, TILE_WAIT_POLLS)) drained = false;
-      if (lane == 0 && atomicCAS(A.err, 0, drained ? 130 : 131) == 0) {
-        A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = kd;
-      }
-      return;
-    }
+    if (!mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS)) failed = 1;
+    if (kd + 1 < khi) stage(kd + 1, cur ^ 1);
     const char* Ul = UB + cur * ubuf + hl * 16;
     const float* Rc = reinterpret_cast<const float*>(RBB + cur * rbuf);
 #pragma unroll
@@ -420,17 +397,15 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
         }
       }
     }
-    // this warp is done with buffer cur; the last warp to finish the level
-    // refills it with level kd + 2 (its reads are ordered before the copies
-    // by the fences around the count)
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence_block();
-      if (atomicAdd(&CNT[cur], 1) == TILE_NW - 1) {
-        __threadfence_block();
-        CNT[cur] = 0;
-        if (kd + 2 < khi) stage(kd + 2, cur);
-      }
+    if (__syncthreads_or(failed)) {
+      // the copies of this level and of the next one may still be in flight
+      // into this block's shared memory: wait for them (bounded again) before
+      // the block exits and its shared memory is handed to another block
+      const bool cur_done = mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS);
+      const bool nxt_done = kd + 1 >= khi || mbar_wait_bounded(&BAR[cur ^ 1], ((lv + 1) >> 1) & 1, TILE_WAIT_POLLS);
+      const int code = (cur_done && nxt_done) ? 130 : 131;
+      if (tid == 0 && atomicCAS(A.err, 0, code) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = kd; }
+      return;
     }
   }
 }
