@@ -395,15 +395,16 @@ __global__ void k_grad(GridK g, const int* __restrict__ prog, int nprog, CTView 
   }
 }
 
-// One tracer in OLAM's own layout (the plain form): a warp per column, lanes
-// over the levels, the column's neighbours, face floors and coefficients
-// held in registers (read once per column instead of once per element).
+// One tracer in OLAM's own layout (the plain form): a half warp per column
+// (two columns per warp), lanes over the levels, two levels per lane in
+// flight at a time; the column's neighbours, face floors and coefficients
+// are held in registers (read once per column instead of once per element).
 template <int ORDER>
 __global__ void __launch_bounds__(256)
     k_grad1(GridK g, const int* __restrict__ prog, int nprog, const float* __restrict__ S, float* __restrict__ gx,
             const float* __restrict__ cx, const float* __restrict__ cy, const float* __restrict__ xy) {
   constexpr int M = ORDER == 2 ? 2 : 5;   // gradient planes
-  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), hl = threadIdx.x & 15;
   if (w >= nprog) return;
   const int mza = g.mza, iw = prog[w], np = g.npoly[iw];
   const size_t plane = (size_t)g.mwa * mza;
@@ -424,28 +425,40 @@ __global__ void __launch_bounds__(256)
       }
     }
   }
-  for (int kd = lane; kd < mza; kd += 32) {
-    const float s0 = S[(size_t)iw * mza + kd];
-    float a[M];
+  for (int k0 = hl; k0 < mza; k0 += 32) {
+    const int k1 = k0 + 16;
+    const bool v1 = k1 < mza;
+    const float s0 = S[(size_t)iw * mza + k0], s1 = v1 ? S[(size_t)iw * mza + k1] : 0.f;
+    float a[M], b[M];
 #pragma unroll
-    for (int m = 0; m < M; ++m) a[m] = 0.f;
+    for (int m = 0; m < M; ++m) a[m] = b[m] = 0.f;
 #pragma unroll
     for (int n = 0; n < 7; ++n) {
-      if (n >= np || kd < lp[n]) continue;
-      const float d = S[(size_t)nb[n] * mza + kd] - s0;
+      if (n >= np) continue;
+      if (k0 >= lp[n]) {
+        const float d = S[(size_t)nb[n] * mza + k0] - s0;
 #pragma unroll
-      for (int m = 0; m < M; ++m) a[m] = a[m] + c[n][m] * d;
+        for (int m = 0; m < M; ++m) a[m] = a[m] + c[n][m] * d;
+      }
+      if (v1 && k1 >= lp[n]) {
+        const float d = S[(size_t)nb[n] * mza + k1] - s1;
+#pragma unroll
+        for (int m = 0; m < M; ++m) b[m] = b[m] + c[n][m] * d;
+      }
     }
-    const size_t o = (size_t)iw * mza + kd;
+    const size_t o = (size_t)iw * mza + k0;
 #pragma unroll
-    for (int m = 0; m < M; ++m) gx[m * plane + o] = a[m];
+    for (int m = 0; m < M; ++m) {
+      gx[m * plane + o] = a[m];
+      if (v1) gx[m * plane + o + 16] = b[m];
+    }
   }
 }
 
 void launch_grad(const DevGrid& d, CTView scp, float* gx, int nt, int order, bool bounded,
                  cudaStream_t s) {
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0) {
-    const unsigned nb = cdiv((size_t)d.nw_prog * 32, 256);
+    const unsigned nb = cdiv((size_t)d.nw_prog * 16, 256);
     if (order == 2)
       k_grad1<2><<<nb, 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp.base, gx, d.gxc.p, d.gyc.p, nullptr);
     else
@@ -518,13 +531,23 @@ __global__ void k_vflux(GridK g, const int* __restrict__ vlist, int nv, CTView s
   }
 }
 
-// the upwind V-face values of one tracer (plain mode, OLAM's layout): a warp
-// per face, lanes over the levels, the face's cells and coefficients in
-// registers; only the upwind side's reconstruction is read
-__global__ void k_vflux1(GridK g, const int* __restrict__ vlist, int nv, const float* __restrict__ S,
-                         const float* __restrict__ gx, const float* __restrict__ vmasc, int order, VCoef vc,
-                         float* __restrict__ upv) {
-  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+// the upwind V-face values of one tracer (plain mode, OLAM's layout): a half
+// warp per face (two faces per warp), lanes over the levels with two levels
+// per lane in flight, the face's cells and coefficients in registers; only
+// the upwind side's reconstruction is read
+__device__ __forceinline__ float vface1(const float* __restrict__ S, const float* __restrict__ gx, size_t plane,
+                                        int order, size_t o, float dx, float dy, float xx, float xy, float yy) {
+  float v = S[o];
+  v = v + dx * gx[o] + dy * gx[plane + o];
+  if (order == 3) v = v + xx * gx[2 * plane + o] + xy * gx[3 * plane + o] + yy * gx[4 * plane + o];
+  return v;
+}
+
+__global__ void __launch_bounds__(256)
+    k_vflux1(GridK g, const int* __restrict__ vlist, int nv, const float* __restrict__ S,
+             const float* __restrict__ gx, const float* __restrict__ vmasc, int order, VCoef vc,
+             float* __restrict__ upv) {
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), hl = threadIdx.x & 15;
   if (w >= nv) return;
   const int mza = g.mza, iv = vlist[w], kv = g.lpv[iv];
   const size_t plane = (size_t)g.mwa * mza;
@@ -538,16 +561,19 @@ __global__ void k_vflux1(GridK g, const int* __restrict__ vlist, int nv, const f
     xx1 = __ldg(vc.xx + e1); xy1 = __ldg(vc.xy + e1); yy1 = __ldg(vc.yy + e1);
     xx2 = __ldg(vc.xx + e2); xy2 = __ldg(vc.xy + e2); yy2 = __ldg(vc.yy + e2);
   }
-  for (int kd = kv + lane; kd < mza; kd += 32) {
-    const float vm = vmasc[(size_t)iv * mza + kd];
-    const bool two = vm < 0.f;
-    const size_t o = (size_t)(two ? w2 : w1) * mza + kd;
-    float v = S[o];
-    v = v + (two ? dx2 : dx1) * gx[o] + (two ? dy2 : dy1) * gx[plane + o];
-    if (order == 3)
-      v = v + (two ? xx2 : xx1) * gx[2 * plane + o] + (two ? xy2 : xy1) * gx[3 * plane + o] +
-          (two ? yy2 : yy1) * gx[4 * plane + o];
-    upv[(size_t)iv * mza + kd] = v;
+  for (int k0 = kv + hl; k0 < mza; k0 += 32) {
+    const int k1 = k0 + 16;
+    const bool v1 = k1 < mza;
+    const bool two0 = vmasc[(size_t)iv * mza + k0] < 0.f;
+    const bool two1 = v1 && vmasc[(size_t)iv * mza + k1] < 0.f;
+    const float u0 = vface1(S, gx, plane, order, (size_t)(two0 ? w2 : w1) * mza + k0, two0 ? dx2 : dx1,
+                            two0 ? dy2 : dy1, two0 ? xx2 : xx1, two0 ? xy2 : xy1, two0 ? yy2 : yy1);
+    float u1 = 0.f;
+    if (v1)
+      u1 = vface1(S, gx, plane, order, (size_t)(two1 ? w2 : w1) * mza + k1, two1 ? dx2 : dx1, two1 ? dy2 : dy1,
+                  two1 ? xx2 : xx1, two1 ? xy2 : xy1, two1 ? yy2 : yy1);
+    upv[(size_t)iv * mza + k0] = u0;
+    if (v1) upv[(size_t)iv * mza + k1] = u1;
   }
 }
 
@@ -556,7 +582,7 @@ void launch_vflux(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0
   VCoef vc{d.dxps.p, d.dyps.p, unbounded ? d.xx0_vu.p : d.xx0_v.p, unbounded ? d.xy0_vu.p : d.xy0_v.p,
            unbounded ? d.yy0_vu.p : d.yy0_v.p};
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0 && !anylim) {
-    k_vflux1<<<cdiv((size_t)d.nv_wadj * 32, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp.base, gx,
+    k_vflux1<<<cdiv((size_t)d.nv_wadj * 16, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp.base, gx,
                                                               tp.vmasc.p, order, vc, tp.upv.p);
     OG_LAUNCHED();
     return;
@@ -811,12 +837,13 @@ __global__ void k_wcell(WcolArgs A) {
     for (int k = 0; k < kb; ++k) out[(size_t)k * A.out.ld] = o;
 }
 
-// the same for one tracer in OLAM's layout: a warp per column, lanes over
-// the levels, the column's faces (V point, dirv, floor) in registers
-__global__ void __launch_bounds__(256, 4) k_wcell1(WcolArgs A) {
+// the same for one tracer in OLAM's layout: a half warp per column (two
+// columns per warp), lanes over the levels with two levels per lane in
+// flight, the column's faces (V point, dirv, floor) in registers
+__global__ void __launch_bounds__(256, 3) k_wcell1(WcolArgs A) {
   const GridK& g = A.g;
   const int mza = g.mza;
-  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), hl = threadIdx.x & 15;
   if (w >= A.nprog) return;
   const int iw = A.prog[w], kb = g.lpw[iw], np = g.npoly[iw];
   int ev[7], lp[7];
@@ -828,8 +855,8 @@ __global__ void __launch_bounds__(256, 4) k_wcell1(WcolArgs A) {
   }
   const float fimpl = A.ff[(size_t)iw * A.nrk + A.istage - 1];
   const float fexpl = 1.0f - fimpl;
-  const float* wm = A.wmasc + (size_t)iw * mza;
-  const float* Sc = A.scp.base + (size_t)iw * mza;
+  const float* __restrict__ wm = A.wmasc + (size_t)iw * mza;
+  const float* __restrict__ Sc = A.scp.base + (size_t)iw * mza;
   auto S = [&](int k) { return Sc[k]; };
   auto upw = [&](int f) -> float {
     if (f == kb - 1) return S(kb);
@@ -842,8 +869,8 @@ __global__ void __launch_bounds__(256, 4) k_wcell1(WcolArgs A) {
     zrec(g.a_w, mza, f, kb, (f - 1 >= kb) ? S(f - 1) : 0.f, S(f), S(f + 1), 0.f, false, false, sb, st);
     return st;
   };
-  float* out = A.out.base + (size_t)iw * mza;
-  for (int kd = kb + lane; kd < mza; kd += 32) {
+  // the update of level kd, from loads only (no store in between)
+  auto cell = [&](int kd) -> float {
     const size_t x = (size_t)iw * mza + kd;
     const float s00 = A.scp0.base[x];
     float fd = 0.f;
@@ -854,10 +881,17 @@ __global__ void __launch_bounds__(256, 4) k_wcell1(WcolArgs A) {
       fd = fd + dv[n] * A.vmasc[xv] * (A.upv[xv] - s00);
     }
     fd = fd + fexpl * (wm[kd - 1] * (upw(kd - 1) - s00) - wm[kd] * (upw(kd) - s00));
-    const float o = s00 + A.dtr * (A.sct.base[x] + g.volti[x] * fd) / A.rhos[x];
-    out[kd] = o;
-    if (kd == kb)
-      for (int k = 0; k < kb; ++k) out[k] = o;
+    return s00 + A.dtr * (A.sct.base[x] + g.volti[x] * fd) / A.rhos[x];
+  };
+  float* out = A.out.base + (size_t)iw * mza;
+  for (int k0 = kb + hl; k0 < mza; k0 += 32) {
+    const int k1 = k0 + 16;
+    const float o0 = cell(k0);
+    const float o1 = k1 < mza ? cell(k1) : 0.f;
+    out[k0] = o0;
+    if (k1 < mza) out[k1] = o1;
+    if (k0 == kb)
+      for (int k = 0; k < kb; ++k) out[k] = o0;
   }
 }
 
@@ -873,7 +907,7 @@ void launch_wcell(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0
   A.mode = nullptr;
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0 && scp0.ld == 1 && scp0.t0 == 0 && sct.ld == 1 && sct.t0 == 0 &&
       out.ld == 1 && out.t0 == 0) {
-    k_wcell1<<<cdiv((size_t)d.nw_prog * 32, 256), 256, 0, s>>>(A);
+    k_wcell1<<<cdiv((size_t)d.nw_prog * 16, 256), 256, 0, s>>>(A);
     OG_LAUNCHED();
     return;
   }
