@@ -79,6 +79,9 @@ def parse():
     p.add_argument("--win-steps", type=int, default=24)
     p.add_argument("--win-chk", type=int, default=6)
     p.add_argument("--win-monot", type=int, default=0)
+    p.add_argument("--large", action="store_true",
+                   help="only the large combined run (NXP=400, 80 levels, 32 tracers, 24 long steps of 60 s)")
+    p.add_argument("--large-nxp", type=int, default=400)
     p.add_argument("--tile-shape", default="",
                    help="T,G,KS: force this shape of the tiled stage kernel (default: the autotuner's)")
     p.add_argument("--shape-sweep", action="store_true",
@@ -149,6 +152,19 @@ def make_case(a):
         g = with_terrain(g, a.terrain)
     tr = fast_lognormal_tracers(g, a.ntr, seed=2024, as_list=True)
     return g, st, tr
+
+
+def acoustic_bytes(g):
+    """Bytes each acoustic-step launch must move at least (every array
+    element it reads or writes once; stage-averaged for wrt_begs over the 3
+    RK stages), per kernel scope."""
+    cw = prognostic_cells(g)                                            # above-ground W and V cells
+    cv = int((g.mza + 1 - g.lpv[1:].astype(np.int64)).sum())
+    return {
+        "setup_w": 76 * cw, "setup_v": 16 * cv, "vmca": 20 * cv, "upw4": 36 * cw,
+        "grad_upv4": 16 * cw + 20 * cv, "wrt_begs": (136 + 16 / 3) * cw + 24 * cv, "prog_v": 24 * cv + 28 * cw,
+        "vel_t3d": 16 * cw + 4 * cv,
+    }
 
 
 def prognostic_cells(g):
@@ -408,15 +424,7 @@ def bench_long_step(g, tr, a, max_over_ranks):
     except (OSError, ValueError):
         pass
     peak = float(peaks.get("hbm_gbs") or 6650.0)
-    cw = prognostic_cells(g)                                            # above-ground W and V cells
-    cv = int((g.mza + 1 - g.lpv[1:].astype(np.int64)).sum())
-    # bytes each launch must move at least (every array element it reads or
-    # writes once; stage-averaged for wrt_begs over the 3 RK stages)
-    algo = {
-        "setup_w": 76 * cw, "setup_v": 16 * cv, "vmca": 20 * cv, "upw4": 36 * cw,
-        "grad_upv4": 16 * cw + 20 * cv, "wrt_begs": (136 + 16 / 3) * cw + 24 * cv, "prog_v": 24 * cv + 28 * cw,
-        "vel_t3d": 16 * cw + 4 * cv,
-    }
+    algo = acoustic_bytes(g)
     kern = {}
     for name, b in algo.items():
         if name in prof and prof[name][1]:
@@ -567,6 +575,132 @@ def bench_window(a, max_over_ranks):
     return out
 
 
+def bench_large(a):
+    """The large combined run: NXP=400 (1,600,002 columns), 80 levels to
+    40 km, the balanced jet, 32 FP32 tracers with a surface emission each,
+    through the whole device long step (4 acoustic RK3 steps, RK3 tracer
+    transport, damping) for 24 steps of 60 s, replayed as a CUDA graph
+    (device time of the 24 steps); then the window adjoint over the same 24
+    steps with a checkpoint every a.win_chk steps, if the device memory
+    holds it (an allocation failure is reported, not hidden).  Throughput:
+    tracer cell-updates/s; the HBM fraction counts the bytes of the kernels
+    with an algorithmic byte count (acoustic kernels, the tracer stages and
+    records) over the whole step's device time."""
+    import torch
+    from olam_b200 import abi
+    from olam_b200.lib import HostState, OlamGpu
+    from olam_b200.synth.grid import build_grid, stretched_levels
+    from olam_b200.synth.state import dynamics_state, fast_lognormal_tracers
+    nxp, nlev, ntr, nsteps, dt = a.large_nxp, 80, 32, 24, 60.0
+    g = build_grid(nxp, stretched_levels(nlev, 100.0, 40000.0), seed=4)
+    ds = dynamics_state(g, seed=4)
+    tr = fast_lognormal_tracers(g, ntr, seed=31, as_list=True)
+    rng = np.random.default_rng(41)
+    emis = [(1e-13 * rng.random(g.mwa)).astype(np.float32) for _ in range(ntr)]
+    for e in emis:
+        e[0] = 0.0
+    wz = lambda: np.zeros((g.mwa, g.mza), np.float32)   # noqa: E731
+    hs = HostState(rho=ds.rho, press=ds.press, thil=ds.thil, wc=ds.wc, wmc=ds.wmc, vxe=ds.vxe, vye=ds.vye,
+                   vze=ds.vze, vmc=ds.vmc, vc=ds.vc, vmasc=np.zeros((g.mva, g.mza), np.float32), wmasc=wz(),
+                   alpha_press=ds.alpha_press, pwfac=ds.pwfac, pvfac=ds.pvfac, thilt=wz(), vmxet=wz(),
+                   vmyet=wz(), vmzet=wz(), vmt=np.zeros((g.mva, g.mza), np.float32))
+    opts = abi.make_opts(dt, nacoust=4, nrk_scal=3)
+    cells = prognostic_cells(g)
+    out = {"workload": f"NXP={nxp} ({g.mwa - 1} columns), {nlev} levels to 40 km, balanced jet, {ntr} tracers "
+                       f"with surface emission, {nsteps} long steps of {dt:.0f} s (nacoust 4, acoustic RK3, "
+                       f"tracer RK3, damping), the long step replayed as a CUDA graph"}
+    dev = OlamGpu(abi.FortranGrid(g), opts, hs)
+
+    def used_gb():
+        free, total = torch.cuda.mem_get_info()
+        return (total - free) / 1e9
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs") or 6650.0)
+    try:
+        var_p = [t.copy() for t in tr]
+        var_t = [np.zeros_like(t) for t in tr]
+        dev.register_scalars(var_p, var_t)
+        dev.set_surface_emission(emis)
+        dev.set_coherence(abi.RESIDENT)
+        dev.timestep(abi.TS_GRAPH)            # buffers, tile shape, graph: then back to the start
+        dev.sync_to_device(abi.F_ALL)
+        torch.cuda.synchronize()
+        mem = {"after_first_step": used_gb()}
+        stream = torch.cuda.ExternalStream(dev.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dev.profile(True, reset=True)
+        e0.record(stream)
+        for _ in range(nsteps):
+            dev.timestep(abi.TS_GRAPH)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        prof = dev.profile_read()
+        dev.profile(False, reset=True)
+        fwd_ms = e0.elapsed_time(e1)
+        mem["after_forward"] = used_gb()
+        # algorithmic bytes of one long step: the acoustic kernels, the tracer
+        # stages (12 | 16 B per tracer-cell + 32 B per cell) and the step records
+        per_launch = acoustic_bytes(g)
+        per_launch["tile_stage1"] = (ntr * 12 + 32) * cells
+        per_launch["tile_stage"] = (ntr * 16 + 32) * cells
+        per_launch["tile_weights"] = 128 * cells
+        step_bytes, counted_ms = 0.0, 0.0
+        for name, b in per_launch.items():
+            if name in prof and prof[name][1]:
+                step_bytes += b * prof[name][1] / nsteps
+                counted_ms += prof[name][0] / nsteps
+        ms_step = fwd_ms / nsteps
+        out["forward"] = {
+            "ms_per_step": ms_step, "cell_updates_per_s": ntr * cells / (ms_step * 1e-3),
+            "algorithmic_gb_per_step": step_bytes / 1e9,
+            "hbm_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak,
+            "hbm_frac_of_counted_kernels": step_bytes / (counted_ms * 1e-3) / 1e9 / peak if counted_ms else None,
+            "counted_ms_per_step": counted_ms,
+            "tile_stage_ms": (prof["tile_stage"][0] / prof["tile_stage"][1]) if "tile_stage" in prof else None,
+            "peak_gbs": peak,
+        }
+        out["device_gb_in_use"] = mem
+        # the window and its adjoint from the same start
+        dev.sync_to_device(abi.F_ALL)
+        for t, t0 in zip(var_p, tr):
+            t[...] = t0
+        dev.sync_to_device(abi.F_SCALARS)
+        torch.cuda.synchronize()
+        try:
+            e0.record(stream)
+            dev.window_forward(nsteps, a.win_chk, abi.TS_GRAPH)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            wf_ms = e0.elapsed_time(e1)
+            mem["after_window_forward"] = used_gb()
+            lam = [np.zeros((g.mwa, g.mza), np.float32) for _ in range(ntr)]
+            rr = np.random.default_rng(43)
+            iw = rr.integers(1, g.mwa, 200)
+            kk = g.lpw[iw] - 1 + rr.integers(0, 3, 200)
+            for n in range(ntr):
+                np.add.at(lam[n], (iw, kk), rr.standard_normal(200).astype(np.float32))
+            dev.profile(True, reset=True)
+            dev.window_adjoint(lam)
+            aprof = dev.profile_read()
+            dev.profile(False, reset=True)
+            adj_ms = aprof["window_adjoint"][0]
+            mem["after_adjoint"] = used_gb()
+            out["adjoint"] = {"window_forward_ms": wf_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / wf_ms,
+                              "cell_updates_per_s": ntr * cells * nsteps / (adj_ms * 1e-3),
+                              "checkpoint_every": a.win_chk}
+        except Exception as e:   # the library's allocation failure, reported as such
+            out["adjoint"] = {"unavailable": str(e)[:300], "checkpoint_every": a.win_chk,
+                              "device_gb_in_use_at_failure": used_gb()}
+    finally:
+        dev.close()
+    return out
+
+
 def run_decomposed(a, ws, rank, dist):
     """--gpus N > 1: the same global grid and tracers split over the N
     ranks by recursive coordinate bisection (olam_b200/decomp.py, in the
@@ -706,6 +840,9 @@ def main():
     torch.cuda.set_device(local)
     if ws > 1:
         return run_decomposed(a, ws, rank, dist)
+    if a.large:
+        print(json.dumps({"large": bench_large(a)}), flush=True)
+        return 0
     g, st, tr = make_case(a)
     if a.long_step_only:
         out = bench_long_step(g, tr, a, lambda x: x)
