@@ -26,23 +26,43 @@ def device_view(ptr: int, n: int):
     return torch.as_tensor(_DeviceArray(ptr, n), device="cuda")
 
 
-def nccl_exchange(dist):
-    """The exchange hook for abi.make_halo_device: sends each neighbour its
-    packed columns and receives its own, as one batch of NCCL point-to-point
-    operations on the library's stream."""
+def host_view(ptr: int, n: int):
+    """A torch tensor viewing n float32 values of host memory at ptr (no copy)."""
+    import ctypes
+
+    import numpy as np
     import torch
+    if n == 0:
+        return torch.zeros(0, dtype=torch.float32)
+    return torch.from_numpy(np.ctypeslib.as_array((ctypes.c_float * n).from_address(ptr)))
+
+
+def nccl_exchange(dist, view=None, on_stream=None):
+    """The exchange hook for abi.make_halo_device: sends each neighbour its
+    packed columns and receives its own, as one batch of point-to-point
+    operations on the library's stream.  view(ptr, n) wraps a buffer and
+    on_stream(stream) orders the operations; both default to device
+    memory and the library's CUDA stream (with host views and no stream
+    the same hook runs over gloo, which is how the pairing is tested
+    without a GPU)."""
+    import torch
+    if view is None:
+        view = device_view
+    if on_stream is None:
+        def on_stream(stream):
+            return torch.cuda.stream(torch.cuda.ExternalStream(stream))
 
     def fn(ranks, sbufs, rbufs, stream):
-        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+        with on_stream(stream):
             ops = []
             for r, (sp, sn), (rp, rn) in zip(ranks, sbufs, rbufs):
                 if sn:
-                    ops.append(dist.P2POp(dist.isend, device_view(sp, sn), r))
+                    ops.append(dist.P2POp(dist.isend, view(sp, sn), r))
                 if rn:
-                    ops.append(dist.P2POp(dist.irecv, device_view(rp, rn), r))
+                    ops.append(dist.P2POp(dist.irecv, view(rp, rn), r))
             if ops:
                 for req in dist.batch_isend_irecv(ops):
-                    req.wait()   # the library stream waits; the host does not
+                    req.wait()   # with a CUDA stream: the stream waits, the host does not
         return 0
 
     return fn
