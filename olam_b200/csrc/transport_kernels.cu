@@ -395,16 +395,22 @@ __global__ void k_grad(GridK g, const int* __restrict__ prog, int nprog, CTView 
   }
 }
 
-// One tracer in OLAM's own layout (the plain form): a half warp per column
-// (two columns per warp), lanes over the levels, two levels per lane in
-// flight at a time; the column's neighbours, face floors and coefficients
-// are held in registers (read once per column instead of once per element).
+// The one-tracer passes of the plain form (OLAM's own layout) give PLC
+// lanes to a column or face (32 / PLC of them per warp) and keep PLU levels
+// per lane in flight: the levels of a column are PLC apart per lane, PLC *
+// PLU per round.
+#define PLC 16
+#define PLU 2
+
+// grad_t2d / grad_t2d_quadratic of one tracer: the column's neighbours, face
+// floors and coefficients held in registers (read once per column instead
+// of once per element)
 template <int ORDER>
 __global__ void __launch_bounds__(256)
     k_grad1(GridK g, const int* __restrict__ prog, int nprog, const float* __restrict__ S, float* __restrict__ gx,
             const float* __restrict__ cx, const float* __restrict__ cy, const float* __restrict__ xy) {
   constexpr int M = ORDER == 2 ? 2 : 5;   // gradient planes
-  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), hl = threadIdx.x & 15;
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / PLC), hl = threadIdx.x % PLC;
   if (w >= nprog) return;
   const int mza = g.mza, iw = prog[w], np = g.npoly[iw];
   const size_t plane = (size_t)g.mwa * mza;
@@ -425,32 +431,35 @@ __global__ void __launch_bounds__(256)
       }
     }
   }
-  for (int k0 = hl; k0 < mza; k0 += 32) {
-    const int k1 = k0 + 16;
-    const bool v1 = k1 < mza;
-    const float s0 = S[(size_t)iw * mza + k0], s1 = v1 ? S[(size_t)iw * mza + k1] : 0.f;
-    float a[M], b[M];
+  for (int k0 = hl; k0 < mza; k0 += PLC * PLU) {
+    float a[PLU][M], s0[PLU];
 #pragma unroll
-    for (int m = 0; m < M; ++m) a[m] = b[m] = 0.f;
+    for (int u = 0; u < PLU; ++u) {
+      const int k = k0 + PLC * u;
+      s0[u] = k < mza ? S[(size_t)iw * mza + k] : 0.f;
+#pragma unroll
+      for (int m = 0; m < M; ++m) a[u][m] = 0.f;
+    }
 #pragma unroll
     for (int n = 0; n < 7; ++n) {
       if (n >= np) continue;
-      if (k0 >= lp[n]) {
-        const float d = S[(size_t)nb[n] * mza + k0] - s0;
 #pragma unroll
-        for (int m = 0; m < M; ++m) a[m] = a[m] + c[n][m] * d;
-      }
-      if (v1 && k1 >= lp[n]) {
-        const float d = S[(size_t)nb[n] * mza + k1] - s1;
+      for (int u = 0; u < PLU; ++u) {
+        const int k = k0 + PLC * u;
+        if (k < mza && k >= lp[n]) {
+          const float d = S[(size_t)nb[n] * mza + k] - s0[u];
 #pragma unroll
-        for (int m = 0; m < M; ++m) b[m] = b[m] + c[n][m] * d;
+          for (int m = 0; m < M; ++m) a[u][m] = a[u][m] + c[n][m] * d;
+        }
       }
     }
-    const size_t o = (size_t)iw * mza + k0;
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      gx[m * plane + o] = a[m];
-      if (v1) gx[m * plane + o + 16] = b[m];
+    for (int u = 0; u < PLU; ++u) {
+      const int k = k0 + PLC * u;
+      if (k >= mza) continue;
+      const size_t o = (size_t)iw * mza + k;
+#pragma unroll
+      for (int m = 0; m < M; ++m) gx[m * plane + o] = a[u][m];
     }
   }
 }
@@ -458,7 +467,7 @@ __global__ void __launch_bounds__(256)
 void launch_grad(const DevGrid& d, CTView scp, float* gx, int nt, int order, bool bounded,
                  cudaStream_t s) {
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0) {
-    const unsigned nb = cdiv((size_t)d.nw_prog * 16, 256);
+    const unsigned nb = cdiv((size_t)d.nw_prog * PLC, 256);
     if (order == 2)
       k_grad1<2><<<nb, 256, 0, s>>>(gridk(d), d.jtw_prog.p, d.nw_prog, scp.base, gx, d.gxc.p, d.gyc.p, nullptr);
     else
@@ -531,10 +540,9 @@ __global__ void k_vflux(GridK g, const int* __restrict__ vlist, int nv, CTView s
   }
 }
 
-// the upwind V-face values of one tracer (plain mode, OLAM's layout): a half
-// warp per face (two faces per warp), lanes over the levels with two levels
-// per lane in flight, the face's cells and coefficients in registers; only
-// the upwind side's reconstruction is read
+// the upwind V-face values of one tracer (plain mode, OLAM's layout): PLC
+// lanes per face, PLU levels per lane in flight, the face's cells and
+// coefficients in registers; only the upwind side's reconstruction is read
 __device__ __forceinline__ float vface1(const float* __restrict__ S, const float* __restrict__ gx, size_t plane,
                                         int order, size_t o, float dx, float dy, float xx, float xy, float yy) {
   float v = S[o];
@@ -547,7 +555,7 @@ __global__ void __launch_bounds__(256)
     k_vflux1(GridK g, const int* __restrict__ vlist, int nv, const float* __restrict__ S,
              const float* __restrict__ gx, const float* __restrict__ vmasc, int order, VCoef vc,
              float* __restrict__ upv) {
-  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), hl = threadIdx.x & 15;
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / PLC), hl = threadIdx.x % PLC;
   if (w >= nv) return;
   const int mza = g.mza, iv = vlist[w], kv = g.lpv[iv];
   const size_t plane = (size_t)g.mwa * mza;
@@ -561,19 +569,23 @@ __global__ void __launch_bounds__(256)
     xx1 = __ldg(vc.xx + e1); xy1 = __ldg(vc.xy + e1); yy1 = __ldg(vc.yy + e1);
     xx2 = __ldg(vc.xx + e2); xy2 = __ldg(vc.xy + e2); yy2 = __ldg(vc.yy + e2);
   }
-  for (int k0 = kv + hl; k0 < mza; k0 += 32) {
-    const int k1 = k0 + 16;
-    const bool v1 = k1 < mza;
-    const bool two0 = vmasc[(size_t)iv * mza + k0] < 0.f;
-    const bool two1 = v1 && vmasc[(size_t)iv * mza + k1] < 0.f;
-    const float u0 = vface1(S, gx, plane, order, (size_t)(two0 ? w2 : w1) * mza + k0, two0 ? dx2 : dx1,
-                            two0 ? dy2 : dy1, two0 ? xx2 : xx1, two0 ? xy2 : xy1, two0 ? yy2 : yy1);
-    float u1 = 0.f;
-    if (v1)
-      u1 = vface1(S, gx, plane, order, (size_t)(two1 ? w2 : w1) * mza + k1, two1 ? dx2 : dx1, two1 ? dy2 : dy1,
-                  two1 ? xx2 : xx1, two1 ? xy2 : xy1, two1 ? yy2 : yy1);
-    upv[(size_t)iv * mza + k0] = u0;
-    if (v1) upv[(size_t)iv * mza + k1] = u1;
+  for (int k0 = kv + hl; k0 < mza; k0 += PLC * PLU) {
+    float u[PLU];
+#pragma unroll
+    for (int q = 0; q < PLU; ++q) {
+      const int k = k0 + PLC * q;
+      u[q] = 0.f;
+      if (k < mza) {
+        const bool two = vmasc[(size_t)iv * mza + k] < 0.f;
+        u[q] = vface1(S, gx, plane, order, (size_t)(two ? w2 : w1) * mza + k, two ? dx2 : dx1, two ? dy2 : dy1,
+                      two ? xx2 : xx1, two ? xy2 : xy1, two ? yy2 : yy1);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < PLU; ++q) {
+      const int k = k0 + PLC * q;
+      if (k < mza) upv[(size_t)iv * mza + k] = u[q];
+    }
   }
 }
 
@@ -582,7 +594,7 @@ void launch_vflux(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0
   VCoef vc{d.dxps.p, d.dyps.p, unbounded ? d.xx0_vu.p : d.xx0_v.p, unbounded ? d.xy0_vu.p : d.xy0_v.p,
            unbounded ? d.yy0_vu.p : d.yy0_v.p};
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0 && !anylim) {
-    k_vflux1<<<cdiv((size_t)d.nv_wadj * 16, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp.base, gx,
+    k_vflux1<<<cdiv((size_t)d.nv_wadj * PLC, 256), 256, 0, s>>>(gridk(d), d.jtv_wadj.p, d.nv_wadj, scp.base, gx,
                                                               tp.vmasc.p, order, vc, tp.upv.p);
     OG_LAUNCHED();
     return;
@@ -837,13 +849,13 @@ __global__ void k_wcell(WcolArgs A) {
     for (int k = 0; k < kb; ++k) out[(size_t)k * A.out.ld] = o;
 }
 
-// the same for one tracer in OLAM's layout: a half warp per column (two
-// columns per warp), lanes over the levels with two levels per lane in
-// flight, the column's faces (V point, dirv, floor) in registers
+// the same for one tracer in OLAM's layout: PLC lanes per column, PLU
+// levels per lane in flight, the column's faces (V point, dirv, floor) in
+// registers
 __global__ void __launch_bounds__(256, 3) k_wcell1(WcolArgs A) {
   const GridK& g = A.g;
   const int mza = g.mza;
-  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4), hl = threadIdx.x & 15;
+  const int w = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / PLC), hl = threadIdx.x % PLC;
   if (w >= A.nprog) return;
   const int iw = A.prog[w], kb = g.lpw[iw], np = g.npoly[iw];
   int ev[7], lp[7];
@@ -884,14 +896,15 @@ __global__ void __launch_bounds__(256, 3) k_wcell1(WcolArgs A) {
     return s00 + A.dtr * (A.sct.base[x] + g.volti[x] * fd) / A.rhos[x];
   };
   float* out = A.out.base + (size_t)iw * mza;
-  for (int k0 = kb + hl; k0 < mza; k0 += 32) {
-    const int k1 = k0 + 16;
-    const float o0 = cell(k0);
-    const float o1 = k1 < mza ? cell(k1) : 0.f;
-    out[k0] = o0;
-    if (k1 < mza) out[k1] = o1;
+  for (int k0 = kb + hl; k0 < mza; k0 += PLC * PLU) {
+    float o[PLU];
+#pragma unroll
+    for (int q = 0; q < PLU; ++q) o[q] = k0 + PLC * q < mza ? cell(k0 + PLC * q) : 0.f;
+#pragma unroll
+    for (int q = 0; q < PLU; ++q)
+      if (k0 + PLC * q < mza) out[k0 + PLC * q] = o[q];
     if (k0 == kb)
-      for (int k = 0; k < kb; ++k) out[k] = o0;
+      for (int k = 0; k < kb; ++k) out[k] = o[0];
   }
 }
 
@@ -907,7 +920,7 @@ void launch_wcell(const DevGrid& d, const Transport& tp, CTView scp, CTView scp0
   A.mode = nullptr;
   if (nt == 1 && scp.ld == 1 && scp.t0 == 0 && scp0.ld == 1 && scp0.t0 == 0 && sct.ld == 1 && sct.t0 == 0 &&
       out.ld == 1 && out.t0 == 0) {
-    k_wcell1<<<cdiv((size_t)d.nw_prog * 16, 256), 256, 0, s>>>(A);
+    k_wcell1<<<cdiv((size_t)d.nw_prog * PLC, 256), 256, 0, s>>>(A);
     OG_LAUNCHED();
     return;
   }
