@@ -454,7 +454,7 @@ def shape_sweep(g, st, tr, a):
         dev.sync_to_device(abi.F_ALL)
         dev.scalar_transport_rk(st.rho_old)
         for ordr in (0, 1):
-          for T, G, KS in ((32, 64, 1), (32, 32, 1), (16, 64, 1), (16, 128, 1), (16, 128, 2)):
+          for T, G, KS in ((32, 64, 1), (32, 32, 1), (32, 128, 1), (16, 64, 1), (16, 128, 1), (16, 128, 2)):
             try:
                 dev.set_tile_shape(T, G, KS, ordr)
             except Exception as e:   # a shape this grid cannot run

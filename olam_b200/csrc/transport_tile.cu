@@ -216,12 +216,13 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
 // KS chunks run by different blocks (A.ks).
 // OFF: the type of element offsets into the batched arrays -- unsigned when
 // they all fit in 32 bits (fewer address instructions), else long long.
-template <int NC, int LPC, typename OFF, bool SPLIT>
-__global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
+template <int NC, int LPC, typename OFF, bool SPLIT, int NW = TILE_NW>
+__global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
     k_tile(TileArgs A, const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int NT = NW * 32;                // threads of the block
   constexpr int CPW = 32 / LPC;              // columns a warp serves at once
-  constexpr int TW = TILE_NW * CPW;          // columns a block serves at once
+  constexpr int TW = NW * CPW;               // columns a block serves at once
   constexpr int T = TW * NC;
   constexpr int G = 4 * LPC;                 // tracers of the block's group
   constexpr int RB = 4 * G;                  // bytes of a staged row
@@ -258,33 +259,33 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
   // it is used on (a failure is recorded and the block does nothing)
   int bad = (nU > A.nu_max || nT > T || nT > nU || A.T != T) ? 1 : 0;
   if (!bad) {
-    for (int i = tid; i < nT * TILE_NS; i += TILE_THREADS) {
+    for (int i = tid; i < nT * TILE_NS; i += NT) {
       const int c = i / TILE_NS, j = i - c * TILE_NS;
       const int v = __ldg(A.tc + ((size_t)tile * T + c) * TILE_TCW + TILE_TC_SLOT + j);
       if ((unsigned)v >= (unsigned)nU * 256u || (v & 255)) bad = 6;
       SLOT[i] = (v >> 8) * RB;
     }
-    for (int i = tid; i < nT; i += TILE_THREADS) {
+    for (int i = tid; i < nT; i += NT) {
       const int v = __ldg(A.tc + ((size_t)tile * T + i) * TILE_TCW + TILE_TC_IW);
       if (v < 1 || v >= A.mwa) bad = 4;
       IWT[i] = v;
     }
-    for (int i = tid; i < nu4; i += TILE_THREADS) {
+    for (int i = tid; i < nu4; i += NT) {
       const int v = __ldg(A.ulist + u_off + (i < nU ? i : 0));   // padding rows repeat row 0
       if (v < 1 || v >= A.mwa) bad = 8;
       RIDX[i] = v * mza;
     }
   }
   if (tid == 0) {
-    mbar_init(&BAR[0], TILE_NW);
-    mbar_init(&BAR[1], TILE_NW);
+    mbar_init(&BAR[0], NW);
+    mbar_init(&BAR[1], NW);
     mbar_init_fence();
   }
   if (__syncthreads_or(bad)) {
     if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
     return;
   }
-  for (int i = tid; i < nT; i += TILE_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
+  for (int i = tid; i < nT; i += NT) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
   const int seg = min(G, ntp - t0);  // tracers of this group (a multiple of 4)
   // level k into buffer b, completing on barrier b: warp w's lane 0 gathers
@@ -293,16 +294,16 @@ __global__ void __launch_bounds__(TILE_THREADS, NC == 1 ? 3 : 2)
   auto stage = [&](int k, int b) {
     if (lane != 0) return;
     const int ng = nu4 >> 2, nr = (nT + 3) >> 2;
-    const int myg = warp < ng ? (ng - warp + TILE_NW - 1) / TILE_NW : 0;
-    const int myr = warp < nr ? (nr - warp + TILE_NW - 1) / TILE_NW : 0;
+    const int myg = warp < ng ? (ng - warp + NW - 1) / NW : 0;
+    const int myr = warp < nr ? (nr - warp + NW - 1) / NW : 0;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * RB + myr * 4 * TILE_WR * 4));
     char* Ub = UB + b * ubuf;
-    for (int g = warp; g < ng; g += TILE_NW) {
+    for (int g = warp; g < ng; g += NW) {
       const int* r = RIDX + 4 * g;
       tma_gather4(Ub + 4 * g * RB, &tmS, t0, r[0] + k, r[1] + k, r[2] + k, r[3] + k, &BAR[b]);
     }
-    for (int q = warp; q < nr; q += TILE_NW) {
+    for (int q = warp; q < nr; q += NW) {
       const int c0 = 4 * q;
       const int y0 = IWT[c0] * mza, y1 = IWT[min(c0 + 1, nT - 1)] * mza;
       const int y2 = IWT[min(c0 + 2, nT - 1)] * mza, y3 = IWT[min(c0 + 3, nT - 1)] * mza;
@@ -451,12 +452,16 @@ bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
 using TileKern = void (*)(TileArgs, const CUtensorMap, const CUtensorMap);
 template <bool SPLIT>
 static TileKern tile_kernel_s(int T, int G, bool off32) {
+  // 32-column tiles of 128 tracers: a block of 16 warps, one per SM
+  if (T == 32 && G == 128) return off32 ? k_tile<2, 32, unsigned, SPLIT, 16> : k_tile<2, 32, long long, SPLIT, 16>;
   if (T == 32 && G == 64) return off32 ? k_tile<2, 16, unsigned, SPLIT> : k_tile<2, 16, long long, SPLIT>;
   if (T == 32 && G == 32) return off32 ? k_tile<1, 8, unsigned, SPLIT> : k_tile<1, 8, long long, SPLIT>;
   if (T == 16 && G == 64) return off32 ? k_tile<1, 16, unsigned, SPLIT> : k_tile<1, 16, long long, SPLIT>;
   if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned, SPLIT> : k_tile<2, 32, long long, SPLIT>;
   return nullptr;
 }
+// threads of a shape's block
+static unsigned tile_threads(int T, int G) { return (T == 32 && G == 128) ? 512u : (unsigned)TILE_THREADS; }
 // the kernel of a shape; the level sweep is split (KS > 1) only in its own instance
 static TileKern tile_kernel(int T, int G, bool off32, int KS = 1) {
   return KS > 1 ? tile_kernel_s<true>(T, G, off32) : tile_kernel_s<false>(T, G, off32);
@@ -505,7 +510,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   OG_CHECK(row_map(&tmS, S, ntp, (size_t)d.mwa * d.mza, G));
   OG_CHECK(row_map(&tmR, tp.wrec.p, TILE_WR, (size_t)d.mwa * d.mza, TILE_WR));
   OG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<nblk, TILE_THREADS, smem, s>>>(A, tmS, tmR);
+  kern<<<nblk, tile_threads(d.tile_T, G), smem, s>>>(A, tmS, tmR);
   OG_LAUNCHED();
   return OLAMGPU_OK;
 }
@@ -567,8 +572,9 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
       rc = build_tiles(&C.hgrid, d, order, s, T, ord);
       if (rc != OLAMGPU_OK || d.tile_T != T) { rc = OLAMGPU_OK; continue; }   // no tables of this width
     }
-    const int Gs[2] = {T == 32 ? 64 : 64, T == 32 ? 32 : 128};
+    const int Gs[3] = {64, T == 32 ? 32 : 128, T == 32 ? 128 : 0};
     for (int G : Gs) {
+      if (!G) continue;
       if (!tile_shape_fits(d, G)) continue;
       for (int KS = 1; KS <= ks_max; ++KS) {
         d.tile_G = G;

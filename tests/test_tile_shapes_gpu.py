@@ -1,5 +1,5 @@
 """GPU parity of every shape of the tiled transport kernel (columns per tile
-T, tracers per block G, level chunks per tile KS) against the FP64 oracle,
+T, tracers per block G, level chunks per tile KS, tile order) against the FP64 oracle,
 with and without terrain, and the autotuner that picks among them."""
 import numpy as np
 import pytest
@@ -13,8 +13,8 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-5
 
-SHAPES = [(32, 64, 1, 0), (32, 32, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0), (32, 64, 2, 0), (32, 32, 3, 1),
-          (16, 128, 2, 1), (32, 64, 1, 1)]
+SHAPES = [(32, 64, 1, 0), (32, 32, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0), (32, 128, 1, 0), (32, 64, 2, 0),
+          (32, 32, 3, 1), (16, 128, 2, 1), (32, 128, 2, 1), (32, 64, 1, 1)]
 
 
 def tracers(g, ntr, seed):
