@@ -486,7 +486,7 @@ __device__ __forceinline__ void warp_tridiag(WrtSmem& m, int k0, int k1, int lan
   }
 }
 
-__global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs A) {
+__global__ void __launch_bounds__(WRT_WARPS * 32, 6) k_wrt_begs(DynK g, WrtArgs A) {
   extern __shared__ double wsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j = blockIdx.x * WRT_WARPS + warp;

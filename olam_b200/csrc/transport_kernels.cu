@@ -399,8 +399,8 @@ __global__ void k_grad(GridK g, const int* __restrict__ prog, int nprog, CTView 
 // lanes to a column or face (32 / PLC of them per warp) and keep PLU levels
 // per lane in flight: the levels of a column are PLC apart per lane, PLC *
 // PLU per round.
-#define PLC 16
-#define PLU 2
+#define PLC 8
+#define PLU 4
 
 // grad_t2d / grad_t2d_quadratic of one tracer: the column's neighbours, face
 // floors and coefficients held in registers (read once per column instead
