@@ -454,11 +454,12 @@ def shape_sweep(g, st, tr, a):
         dev.sync_to_device(abi.F_ALL)
         dev.scalar_transport_rk(st.rho_old)
         for ordr in (0, 1):
-          for T, G, KS in ((32, 64, 1), (32, 32, 1), (32, 128, 1), (16, 64, 1), (16, 128, 1), (16, 128, 2)):
+          for T, G, KS, pk in ((32, 64, 1, 0), (32, 32, 1, 0), (32, 128, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0),
+                               (16, 128, 2, 0), (16, 128, 1, 2)):
             try:
-                dev.set_tile_shape(T, G, KS, ordr)
+                dev.set_tile_shape(T, G, KS, ordr | pk)
             except Exception as e:   # a shape this grid cannot run
-                out.append({"T": T, "G": G, "KS": KS, "order": ordr, "error": str(e)})
+                out.append({"T": T, "G": G, "KS": KS, "order": ordr | pk, "error": str(e)})
                 continue
             for _ in range(2):
                 dev.scalar_transport_rk(None)
@@ -469,7 +470,7 @@ def shape_sweep(g, st, tr, a):
             prof = dev.profile_read()
             dev.profile(False, reset=True)
             ms = [prof[k][0] / prof[k][1] for k in ("tile_stage1", "tile_stage") if k in prof]
-            out.append({"T": T, "G": G, "KS": KS, "order": ordr, "ms_per_stage": ms})
+            out.append({"T": T, "G": G, "KS": KS, "order": ordr | pk, "ms_per_stage": ms})
         used, tlog = dev.tile_shape()
     finally:
         dev.close()
@@ -920,7 +921,8 @@ def main():
                   "candidates_ms_per_stage": [{"T": r[0], "G": r[1], "KS": r[2], "order": r[3], "ms": r[5]}
                                               for r in tlog],
                   "note": "columns per tile, tracers per block, level chunks per tile, tile order (0: the "
-                          "library's curve, 1: the caller's numbering); "
+                          "library's curve, 1: the caller's numbering; +2: the paired kernel, a warp per "
+                          "column pair reading each U row once for both); "
                           + ("forced by --tile-shape" if a.tile_shape else
                              "chosen by the library's autotuner on the first step")}
     dev.profile(False, reset=True)

@@ -386,7 +386,10 @@ int olamgpu_timestep_diag(float* smax, double* sums);
  * The tiled transport kernel runs tiles of up to T neighbouring columns (16
  * or 32) with G tracers per block (32, 64 or 128), the levels of a tile
  * swept by KS blocks, the tiles running along the library's own curve over
- * the columns' positions (ord 0) or along the caller's jtw_prog (ord 1).  By
+ * the columns' positions (ord bit 0 clear) or along the caller's jtw_prog
+ * (bit 0 set); ord bit 1 selects the paired form (T = 16, G = 128, KS = 1:
+ * a warp serves two neighbouring columns and reads each tracer row either
+ * of them needs once).  By
  * default an autotuner picks the shape on the first step for a grid and
  * tracer count: every shape the shared memory admits runs the stage on that
  * step's inputs and the fastest is kept (cached per grid, tracer count and

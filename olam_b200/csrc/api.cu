@@ -161,7 +161,7 @@ static void release_all() {
   DevBuf<int>* ib[] = {&d.jtw_prog, &d.jtv_wadj, &d.jtv_prog, &d.jtw_wadj, &d.jtm_prog, &d.npoly,
                        &d.w_nb, &d.w_ev, &d.w_im, &d.v_iw, &d.v_im, &d.m_iv, &d.m_iw, &d.m_im,
                        &d.lpw, &d.lpv, &d.lpm, &d.iwglobe, &d.w_nonprog, &d.colrec,
-                       &d.tile_hdr, &d.tile_u, &d.tile_tc, &d.tile_rev, &d.tile_band_lev};
+                       &d.tile_hdr, &d.tile_u, &d.tile_tc, &d.tile_rev, &d.tile_band_lev, &d.tile_pair};
   for (auto* b : ib) b->release();
   DevBuf<float>* fb[] = {&d.w_dirv, &d.gxc, &d.gyc, &d.xy_h, &d.xy_hu, &d.dxps, &d.dyps, &d.xx0_v,
                          &d.xy0_v, &d.yy0_v, &d.xx0_vu, &d.xy0_vu, &d.yy0_vu, &d.a_w, &d.a_wu,
@@ -174,6 +174,8 @@ static void release_all() {
     a.T = a.ntiles = a.nu_max = a.order = 0;
   }
   d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
+  d.tile_paired = false;
+  d.tile_pairk = false;
   d.tile_G = 64;
   d.tile_KS = 1;
   d.tile_ord = 0;
@@ -194,7 +196,7 @@ static void release_all() {
   DevBuf<float>* tb[] = {&tp.vmasc, &tp.wmasc, &tp.rho_old, &tp.wc, &tp.rhos, &tp.ff, &tp.imp_b,
                          &tp.cfl_red, &tp.gx, &tp.upv, &tp.hiv, &tp.sfv, &tp.scale, &tp.upw,
                          &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx, &tp.emis,
-                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec, &tp.adj_trec,
+                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec, &tp.adj_trec, &tp.prec,
                          &tp.adj_planes};
   for (auto* b : tb) b->release();
   tp.rho.release();
@@ -499,19 +501,25 @@ int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
     tp.tuned_ntp = -1;
     return OLAMGPU_OK;
   }
-  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || (ord != 0 && ord != 1)) {
-    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0 or 1");
+  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || ord < 0 || ord > 3) {
+    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0..3");
+    return OLAMGPU_E_ARG;
+  }
+  const bool paired = (ord & 2) != 0;
+  if (paired && (T != 16 || G != 128 || KS != 1)) {
+    set_error("tile shape: the paired kernel runs 16-column tiles of 128 tracers, KS = 1");
     return OLAMGPU_E_ARG;
   }
   const int order = C.opts.scal_horiz_adv_order;
-  if (C.g.tile_T != T || C.g.tile_ord != ord) OG_CHECK(build_tiles(&C.hgrid, C.g, order, C.stream, T, ord));
-  if (C.g.tile_T != T || !tile_shape_fits(C.g, G)) {
+  if (C.g.tile_T != T || C.g.tile_ord != (ord & 1)) OG_CHECK(build_tiles(&C.hgrid, C.g, order, C.stream, T, ord & 1));
+  if (C.g.tile_T != T || !tile_shape_fits(C.g, G) || (paired && !C.g.tile_paired)) {
     set_error("tile shape: this grid has no " + std::to_string(T) + "-column tiles of " + std::to_string(G) +
-              " tracers within the shared memory");
+              " tracers within the shared memory" + (paired ? " with column pairs" : ""));
     return OLAMGPU_E_UNSUPPORTED;
   }
   C.g.tile_G = G;
   C.g.tile_KS = KS;
+  C.g.tile_pairk = paired;
   tp.autotune = false;
   return OLAMGPU_OK;
 }
@@ -519,7 +527,10 @@ int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
 int olamgpu_tile_shape(int* shape, int max, int* cand, float* ms) {
   Context& C = ctx();
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return -OLAMGPU_E_STATE; }
-  if (shape) { shape[0] = C.g.tile_T; shape[1] = C.g.tile_G; shape[2] = C.g.tile_KS; shape[3] = C.g.tile_ord; }
+  if (shape) {
+    shape[0] = C.g.tile_T; shape[1] = C.g.tile_G; shape[2] = C.g.tile_KS;
+    shape[3] = C.g.tile_ord | (C.g.tile_pairk ? 2 : 0);
+  }
   const auto& L = C.tp.tune_log;
   for (int i = 0; i < (int)L.size() && i < max; ++i) {
     if (cand) {

@@ -161,6 +161,10 @@ struct DevGrid {
   int tile_G = 64, tile_KS = 1;  // the stage kernel's tracers per block and level chunks
   int tile_ord = 0;              // the order the tiles run along (make_tiles)
   bool tile_closed = false;      // every neighbourhood column is prognosed
+  DevBuf<int> tile_pair;         // (ntiles * 8, TILE_PT): 16-column tiles as 8 column pairs
+  bool tile_paired = false;      // tile_pair holds the tables of the current tiles
+  bool tile_pairk = false;       // the stage runs the paired kernel (16 columns, 128 tracers)
+  int tile_gen = 0;              // counts the tile builds (records of other tiles are stale)
   // The adjoint's own tiles when the stage kernel runs another width: the
   // reverse stage moves half as many bytes again per row as the forward and
   // is fastest on 32-column tiles (fewer halo rows per column); the same
@@ -208,6 +212,26 @@ struct DevGrid {
 // W[0..TILE_NS), SW, volti / rhos, 1 / rhos, SW - sum W, the vertical flux's
 // coefficients on S(kd-2 .. kd+2) and on S0, wmasc(kd-1), wmasc(kd).
 #define TILE_WR 32
+// Column pairs of a 16-column tile (the paired stage kernel): columns 2p and
+// 2p+1 of tile order form pair p, and a warp serves both from one read of
+// each U row either of them needs.  Pair table (TILE_PT words): the number
+// of union rows ne (the rows of either column's slots other than the two
+// columns' own rows), the slot of column B in column A's slots (-1: none),
+// the slot of A in B's, 0, then per union row r | (ja + 1) << 8 | (jb + 1)
+// << 16 with ja, jb the row's slot in A's and B's slots (-1: not a slot).
+#define TILE_PU 40
+#define TILE_PT (4 + TILE_PU)
+// Pair record of a level (TILE_PR words, written per step from the two
+// columns' weight records): [0] the number of union rows with a non-zero
+// weight at this level; per column (A at 4, B at 16, 12 words each): SW,
+// volti/rhos, 1/rhos, D, beta_0..4, omega, the weight of the other column's
+// own row, 0; from word 28 the rows' U indices as bytes (TILE_PU of them),
+// from word 40 their weights (wA, wB) in the same order.
+#define TILE_PR 120
+#define TILE_PR_A 4
+#define TILE_PR_B 16
+#define TILE_PR_IDX 28
+#define TILE_PR_W 40
 
 // a shape of the tiled stage kernel: columns per tile, tracers per block,
 // level chunks per tile
@@ -253,6 +277,8 @@ struct Transport {
   DevBuf<int> d_mode;            // per-tracer last-stage mode
   std::vector<int> h_mode;       // what d_mode holds (uploaded when it changes)
   DevBuf<float> wrec;            // (mwa, mza, TILE_WR) weight records of the step
+  DevBuf<float> prec;            // (ntiles * 8, mza, TILE_PR) pair records of the step (paired kernel)
+  int prec_gen = -1;             // the tile build prec was formed for
   // adjoint (transport_adjoint.cu): lam rotation, lam0, lams in the batched
   // layout, per-tracer planes
   DevBuf<float> adj_l[2], adj_l0, adj_ls, adj_planes;
@@ -410,6 +436,7 @@ struct TileHost {
   std::vector<float> a;
   std::vector<float> band;       // terrain bands (TILE_AW floats each)
   std::vector<int> band_lev;     // the device level at which each band ends
+  std::vector<int> pair;         // 16-column tiles: the column pairs' union tables (TILE_PT words each)
 };
 // T: tile width (0: the widest whose neighbourhoods fit two blocks per SM)
 // nu_cap: the largest neighbourhood of a tile (0: where two blocks of 64

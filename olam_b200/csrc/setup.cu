@@ -515,6 +515,9 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int n
   auto fbits = [](float f) { int i; std::memcpy(&i, &f, 4); return i; };
   std::fill(stamp.begin(), stamp.end(), -1);
   std::vector<double> acc(TILE_AW);
+  // pair tables index U rows with bytes
+  auto nU_fits_bytes = [](size_t n) { return n <= 256; };
+  bool break_pairs = false;
   for (int t = 0; t < ntiles; ++t) {
     gather(t, T);
     const int u_off = (int)ulist.size();
@@ -610,7 +613,43 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int n
       }
       slots = mine;
     }
+    // 16-column tiles: the union tables of the column pairs (2p, 2p+1)
+    if (T == 16 && th.pair.size() != (size_t)ntiles * 8 * TILE_PT) th.pair.assign((size_t)ntiles * 8 * TILE_PT, 0);
+    if (T == 16 && nU_fits_bytes(U.size())) {
+      for (int pp = 0; pp < 8; ++pp) {
+        int* pt = &th.pair[((size_t)t * 8 + pp) * TILE_PT];
+        const int ia = 2 * pp, ib = 2 * pp + 1;
+        if (ia >= nT) { pt[1] = pt[2] = -1; continue; }
+        const bool hasb = ib < nT;
+        const int* wa = &tc[((size_t)t * T + ia) * TILE_TCW];
+        const int* wb = hasb ? &tc[((size_t)t * T + ib) * TILE_TCW] : nullptr;
+        const int nsa = wa[TILE_TC_NS], nsb = hasb ? wb[TILE_TC_NS] : 0;
+        std::vector<int> rows;
+        auto slot_row = [](const int* w, int j) { return w[TILE_TC_SLOT + j] / 256; };
+        for (int j = 0; j < nsa; ++j) rows.push_back(slot_row(wa, j));
+        for (int j = 0; j < nsb; ++j) rows.push_back(slot_row(wb, j));
+        std::sort(rows.begin(), rows.end());
+        rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+        rows.erase(std::remove_if(rows.begin(), rows.end(), [&](int r) { return r == ia || r == ib; }), rows.end());
+        if ((int)rows.size() > TILE_PU) { th.pair.clear(); break; }
+        auto find = [&](const int* w, int ns, int r) {
+          for (int j = 0; j < ns; ++j) if (slot_row(w, j) == r) return j;
+          return -1;
+        };
+        pt[0] = (int)rows.size();
+        pt[1] = hasb ? find(wa, nsa, ib) : -1;
+        pt[2] = hasb ? find(wb, nsb, ia) : -1;
+        for (size_t e = 0; e < rows.size(); ++e) {
+          const int ja = find(wa, nsa, rows[e]), jb = hasb ? find(wb, nsb, rows[e]) : -1;
+          pt[4 + e] = rows[e] | ((ja + 1) << 8) | ((jb + 1) << 16);
+        }
+      }
+    } else if (T == 16) {
+      th.pair.clear();
+    }
+    if (T == 16 && th.pair.empty()) break_pairs = true;
   }
+  if (break_pairs) th.pair.clear();
   th.T = T;
   th.ntiles = ntiles;
   th.nu_max = numax;
@@ -621,6 +660,8 @@ int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, in
   d.tile_T = d.ntiles = d.tile_nu_max = 0;
   d.tile_order = 0;
   d.tile_closed = false;
+  d.tile_paired = false;
+  ++d.tile_gen;
   d.tile_ord = ord;
   TileHost th;
   make_tiles(g, order, th, T, 0, ord);
@@ -630,6 +671,12 @@ int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, in
   OG_CHECK(upload(d.tile_a, th.a.data(), th.a.size(), s));
   OG_CHECK(upload(d.tile_rev, th.rev.data(), th.rev.size(), s));
   OG_CHECK(upload(d.tile_tc, th.tc.data(), th.tc.size(), s));
+  d.tile_paired = false;
+  d.tile_pair.release();
+  if (!th.pair.empty()) {
+    OG_CHECK(upload(d.tile_pair, th.pair.data(), th.pair.size(), s));
+    d.tile_paired = true;
+  }
   d.tile_band.release();
   d.tile_band_lev.release();
   if (!th.band_lev.empty()) {

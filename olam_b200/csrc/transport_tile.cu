@@ -184,6 +184,8 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
   }
 }
 
+int launch_pair_records(const DevGrid& d, Transport& tp, cudaStream_t s);
+
 int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cudaStream_t s) {
   const size_t n = (size_t)d.mza * d.mwa * TILE_WR;
   if (tp.wrec.n != n) {
@@ -201,6 +203,8 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
   W.band = d.tile_band.p; W.band_lev = d.tile_band_lev.p;
   k_weights<<<cdiv((size_t)d.ntiles * d.tile_T, 4), 256, 0, s>>>(W);
   OG_LAUNCHED();
+  // the paired kernel reads the pairs' records, formed from these
+  if (d.tile_pairk && d.tile_paired && d.tile_T == 16) OG_CHECK(launch_pair_records(d, tp, s));
   return OLAMGPU_OK;
 }
 
@@ -411,6 +415,283 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
   }
 }
 
+// ---- the paired stage kernel ------------------------------------------------------
+// 16-column tiles as 8 column pairs (2p, 2p+1), a warp per pair, 128
+// tracers per block: each U row either column of a pair needs is read once
+// and applied to both, with the pair's weights of the level gathered into
+// one record per step (k_pair_records) -- the union rows with a non-zero
+// weight for either column, their U indices and the two weights.
+struct PairArgs {
+  int mza, ntiles;
+  const int4* __restrict__ hdr;
+  const int* __restrict__ tc;
+  const int* __restrict__ pair;     // (ntiles * 8, TILE_PT)
+  const float* __restrict__ wrec;   // (mwa, mza, TILE_WR)
+  float* __restrict__ prec;         // (ntiles * 8, mza, TILE_PR)
+};
+
+// a warp per (tile, pair, level): the two columns' records in two registers
+// per lane (word = lane), the union rows' weights picked by shuffles, the
+// non-zero ones compacted in order by a ballot
+__global__ void __launch_bounds__(256) k_pair_records(PairArgs A) {
+  const size_t wid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int mza = A.mza;
+  if (wid >= (size_t)A.ntiles * 8 * mza) return;   // uniform per warp
+  const size_t tp = wid / mza;
+  const int kd = (int)(wid - tp * mza);
+  const int t = (int)(tp >> 3), pp = (int)(tp & 7);
+  const int nT = A.hdr[t].w;
+  float* o = A.prec + wid * TILE_PR;
+  const int ia = 2 * pp, ib = 2 * pp + 1;
+  const bool hasa = ia < nT, hasb = ib < nT;
+  const int iwa = hasa ? A.tc[((size_t)t * 16 + ia) * TILE_TCW + TILE_TC_IW] : 0;
+  const int iwb = hasb ? A.tc[((size_t)t * 16 + ib) * TILE_TCW + TILE_TC_IW] : 0;
+  const float va = hasa ? A.wrec[((size_t)iwa * mza + kd) * TILE_WR + lane] : 0.f;
+  const float vb = hasb ? A.wrec[((size_t)iwb * mza + kd) * TILE_WR + lane] : 0.f;
+  const int* pt = A.pair + tp * TILE_PT;
+  const int ne = hasa ? pt[0] : 0, jab = pt[1], jba = pt[2];
+  unsigned char* ob = reinterpret_cast<unsigned char*>(o + TILE_PR_IDX);
+  float* ow = o + TILE_PR_W;
+  int cnt = 0;
+#pragma unroll
+  for (int base = 0; base < TILE_PU; base += 32) {
+    const int e = base + lane;
+    const int code = (e < ne) ? pt[4 + e] : 0;
+    const int ja = ((code >> 8) & 255) - 1, jb = ((code >> 16) & 255) - 1;
+    const float xa = __shfl_sync(0xffffffffu, va, ja < 0 ? 0 : ja);
+    const float xb = __shfl_sync(0xffffffffu, vb, jb < 0 ? 0 : jb);
+    const float wa = (e < ne && ja >= 0) ? xa : 0.f, wb = (e < ne && jb >= 0) ? xb : 0.f;
+    const bool nz = (wa != 0.f) || (wb != 0.f);
+    const unsigned m = __ballot_sync(0xffffffffu, nz);
+    const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+    if (nz) {
+      ob[pos] = (unsigned char)(code & 255);
+      ow[2 * pos] = wa;
+      ow[2 * pos + 1] = wb;
+    }
+    cnt += __popc(m);
+  }
+  // the entries past the count: row 0, zero weights (the kernel may read a
+  // group of four whole)
+  for (int i = cnt + lane; i < TILE_PU; i += 32) {
+    ob[i] = 0;
+    ow[2 * i] = 0.f;
+    ow[2 * i + 1] = 0.f;
+  }
+  // per column: SW, volti/rhos, 1/rhos, D, beta_0..4, omega (record words
+  // 20..29), the other column's own-row weight, 0
+  const int src = lane < 10 ? 20 + lane : 0;
+  const float sa = __shfl_sync(0xffffffffu, va, lane == 10 ? (jab < 0 ? 0 : jab) : src);
+  const float sb = __shfl_sync(0xffffffffu, vb, lane == 10 ? (jba < 0 ? 0 : jba) : src);
+  if (lane < 12) {
+    o[TILE_PR_A + lane] = lane < 10 ? sa : (lane == 10 && jab >= 0 ? sa : 0.f);
+    o[TILE_PR_B + lane] = lane < 10 ? sb : (lane == 10 && jba >= 0 ? sb : 0.f);
+  }
+  if (lane < 4) o[lane] = lane == 0 ? __int_as_float(cnt) : 0.f;
+}
+
+int launch_pair_records(const DevGrid& d, Transport& tp, cudaStream_t s) {
+  if (!d.tile_paired || d.tile_T != 16) { set_error("pair records: no paired tiles"); return OLAMGPU_E_STATE; }
+  const size_t n = (size_t)d.ntiles * 8 * d.mza * TILE_PR;
+  if (tp.prec.n != n) OG_CHECK(tp.prec.alloc(n));
+  PairArgs A;
+  A.mza = d.mza; A.ntiles = d.ntiles;
+  A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
+  A.tc = d.tile_tc.p; A.pair = d.tile_pair.p; A.wrec = tp.wrec.p; A.prec = tp.prec.p;
+  const size_t warps = (size_t)d.ntiles * 8 * d.mza;
+  k_pair_records<<<(unsigned)cdiv(warps * 32, 256), 256, 0, s>>>(A);
+  OG_LAUNCHED();
+  tp.prec_gen = d.tile_gen;
+  return OLAMGPU_OK;
+}
+
+// the stage over paired tiles: a warp per pair, 32 lanes over 128 tracers
+template <typename OFF>
+__global__ void __launch_bounds__(TILE_THREADS, 2)
+    k_tile_pair(TileArgs A, const int* __restrict__ pair, const __grid_constant__ CUtensorMap tmS,
+                const __grid_constant__ CUtensorMap tmP) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int T = 16, G = 128, RB = 4 * G;
+  const int ngrp = A.ngrp;
+  const int tile = blockIdx.x / ngrp;
+  const int grp = A.grp0 + (blockIdx.x - tile * ngrp);
+  const int4 h = A.hdr[tile];
+  const int u_off = h.x, nU = h.y, nT = h.w;
+  const int mza = A.mza, ntp = A.ntp, kb = A.kb;
+  const int nu4 = (nU + 3) & ~3;
+  auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
+  const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * RB), rbuf = al((size_t)8 * TILE_PR * 4);
+  unsigned char* p = smraw + ((128u - (smem_addr(smraw) & 127u)) & 127u);
+  unsigned long long* BAR = reinterpret_cast<unsigned long long*>(p); p += 128;
+  char* UB = reinterpret_cast<char*>(p);              p += 2 * ubuf;
+  unsigned char* RBB = p;                             p += 2 * rbuf;
+  int* RIDX = reinterpret_cast<int*>(p);              p += al((size_t)(A.nu_max + 3) * 4);
+  int* IWT = reinterpret_cast<int*>(p);               p += al((size_t)T * 4);
+  float* FEX = reinterpret_cast<float*>(p);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int t0 = grp * G;
+
+  int bad = (nU > A.nu_max || nT > T || nT > nU || A.T != T || nU > 256) ? 1 : 0;
+  if (!bad) {
+    for (int i = tid; i < nT; i += TILE_THREADS) {
+      const int v = __ldg(A.tc + ((size_t)tile * T + i) * TILE_TCW + TILE_TC_IW);
+      if (v < 1 || v >= A.mwa) bad = 4;
+      IWT[i] = v;
+    }
+    for (int i = tid; i < nu4; i += TILE_THREADS) {
+      const int v = __ldg(A.ulist + u_off + (i < nU ? i : 0));   // padding rows repeat row 0
+      if (v < 1 || v >= A.mwa) bad = 8;
+      RIDX[i] = v * mza;
+    }
+    // the pairs' union rows (the per-level records copy their indices)
+    for (int i = tid; i < 8 * TILE_PU; i += TILE_THREADS) {
+      const int* pt = pair + ((size_t)tile * 8 + i / TILE_PU) * TILE_PT;
+      const int e = i % TILE_PU;
+      if (e < pt[0] && (pt[4 + e] & 255) >= nU) bad = 10;
+      if (e == 0 && pt[0] > TILE_PU) bad = 11;
+    }
+  }
+  if (tid == 0) {
+    mbar_init(&BAR[0], TILE_NW);
+    mbar_init(&BAR[1], TILE_NW);
+    mbar_init_fence();
+  }
+  if (__syncthreads_or(bad)) {
+    if (bad && atomicCAS(A.err, 0, 100 + bad) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = tid; }
+    return;
+  }
+  for (int i = tid; i < nT; i += TILE_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
+
+  const int seg = min(G, ntp - t0);
+  // level k into buffer b: warp w's lane 0 gathers the U-row quadruples w,
+  // w + 8, ...; warps 0 and 1 the records of pairs 0..3 and 4..7
+  auto stage = [&](int k, int b) {
+    if (lane != 0) return;
+    const int ng = nu4 >> 2;
+    const int myg = warp < ng ? (ng - warp + TILE_NW - 1) / TILE_NW : 0;
+    const int myr = warp < 2 ? 1 : 0;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * RB + myr * 4 * TILE_PR * 4));
+    char* Ub = UB + b * ubuf;
+    for (int g = warp; g < ng; g += TILE_NW) {
+      const int* r = RIDX + 4 * g;
+      tma_gather4(Ub + 4 * g * RB, &tmS, t0, r[0] + k, r[1] + k, r[2] + k, r[3] + k, &BAR[b]);
+    }
+    if (myr) {
+      const int y = (tile * 8 + 4 * warp) * mza + k;
+      tma_gather4(RBB + b * rbuf + 4 * warp * TILE_PR * 4, &tmP, 0, y, y + mza, y + 2 * mza, y + 3 * mza, &BAR[b]);
+    }
+  };
+
+  // the pair of this warp: columns 2 warp (A) and 2 warp + 1 (B); lane l
+  // holds tracers t0 + 4 l .. + 3 of both
+  const bool act = 4 * lane < seg;
+  F4 m2[2], m1[2], p1[2], p2[2], p3[2], s00[2], st[2];
+  OFF cbase[2];
+  int kbc[2];
+  stage(kb, 0);
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+    const int c = 2 * warp + n;
+    m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = s00[n] = st[n] = zero4();
+    cbase[n] = 0;
+    kbc[n] = c < nT ? max(kb, __ldg(A.lpw + IWT[c])) : mza;
+    if (c < nT && act) {
+      cbase[n] = (OFF)IWT[c] * (OFF)mza * (OFF)ntp + (OFF)(t0 + 4 * lane);
+      if (kb + 1 < mza) p1[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 1) * (OFF)ntp));
+      if (kb + 2 < mza) p2[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 2) * (OFF)ntp));
+      if (kb + 3 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(kb + 3) * (OFF)ntp));
+      s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)kb * (OFF)ntp));
+      st[n] = ldg4(A.SCT + (cbase[n] + (OFF)kb * (OFF)ntp));
+    }
+  }
+  __syncthreads();   // the explicit fractions
+  const bool hasa = 2 * warp < nT, hasb = 2 * warp + 1 < nT;
+  int failed = 0;
+  for (int kd = kb; kd < mza; ++kd) {
+    const int lv = kd - kb, cur = lv & 1;
+    if (!mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS)) failed = 1;
+    if (kd + 1 < mza) stage(kd + 1, cur ^ 1);
+    const char* Ul = UB + cur * ubuf + lane * 16;
+    const float* rp = reinterpret_cast<const float*>(RBB + cur * rbuf) + warp * TILE_PR;
+    if (hasa) {
+      // the union rows: four per step, one word of byte indices and two
+      // (wA, wB) pairs of weights per half
+      const int cnt = min(__float_as_int(rp[0]), TILE_PU);
+      const unsigned* ix4 = reinterpret_cast<const unsigned*>(rp + TILE_PR_IDX);
+      const float4* w4 = reinterpret_cast<const float4*>(rp + TILE_PR_W);
+      F4 fa = zero4(), fb = zero4();
+      for (int e = 0; e < cnt; e += 4) {
+        const unsigned ix = ix4[e >> 2];
+        const float4 wl = w4[e >> 1], wh = w4[(e >> 1) + 1];
+        {
+          const F4 r = lds4(Ul, (int)(ix & 255u) * RB);
+          fa = fma4s(wl.x, r, fa);
+          fb = fma4s(wl.y, r, fb);
+        }
+        if (e + 1 < cnt) {
+          const F4 r = lds4(Ul, (int)((ix >> 8) & 255u) * RB);
+          fa = fma4s(wl.z, r, fa);
+          fb = fma4s(wl.w, r, fb);
+        }
+        if (e + 2 < cnt) {
+          const F4 r = lds4(Ul, (int)((ix >> 16) & 255u) * RB);
+          fa = fma4s(wh.x, r, fa);
+          fb = fma4s(wh.y, r, fb);
+        }
+        if (e + 3 < cnt) {
+          const F4 r = lds4(Ul, (int)(ix >> 24) * RB);
+          fa = fma4s(wh.z, r, fa);
+          fb = fma4s(wh.w, r, fb);
+        }
+      }
+      // the two columns' own rows at kd
+      const F4 sa = lds4(Ul, (2 * warp) * RB);
+      const F4 sb = hasb ? lds4(Ul, (2 * warp + 1) * RB) : zero4();
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        if (n == 1 && !hasb) continue;
+        const int c = 2 * warp + n;
+        if (kd == kbc[n]) m2[n] = m1[n] = zero4();
+        const float* sc = rp + (n == 0 ? TILE_PR_A : TILE_PR_B);
+        const float4 q0 = reinterpret_cast<const float4*>(sc)[0];   // SW, volti/rhos, 1/rhos, D
+        const float4 q1 = reinterpret_cast<const float4*>(sc)[1];   // beta0 .. beta3
+        const float4 q2 = reinterpret_cast<const float4*>(sc)[2];   // beta4, omega, other's own row, 0
+        const float fx = FEX[c];
+        const F4 own = n == 0 ? sa : sb, other = n == 0 ? sb : sa;
+        F4 fd = n == 0 ? fa : fb;
+        fd = fma4s(q2.z, other, fd);
+        fd = fma4s(fx * q1.x, m2[n], fd);
+        fd = fma4s(fx * q1.y, m1[n], fd);
+        fd = fma4s(fmaf(fx, q1.z, q0.w), own, fd);
+        fd = fma4s(fx * q1.w, p1[n], fd);
+        fd = fma4s(fx * q2.x, p2[n], fd);
+        fd = fma4s(fmaf(fx, q2.y, -q0.x), s00[n], fd);
+        const F4 o = fma4s(A.dtr * q0.y, fd, fma4s(A.dtr * q0.z, st[n], s00[n]));
+        if (act) {
+          if (kd >= kbc[n]) stg4(A.OUT + (cbase[n] + (OFF)kd * (OFF)ntp), o);
+          if (kd == kbc[n])
+            for (int k2 = 0; k2 < kd; ++k2) stg4(A.OUT + (cbase[n] + (OFF)k2 * (OFF)ntp), o);
+          m2[n] = m1[n]; m1[n] = own; p1[n] = p2[n]; p2[n] = p3[n];
+          if (kd + 4 < mza) p3[n] = ldg4(A.S + (cbase[n] + (OFF)(kd + 4) * (OFF)ntp));
+          if (kd + 1 < mza) {
+            s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
+            st[n] = ldg4(A.SCT + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
+          }
+        }
+      }
+    }
+    if (__syncthreads_or(failed)) {
+      const bool cur_done = mbar_wait_bounded(&BAR[cur], (lv >> 1) & 1, TILE_WAIT_POLLS);
+      const bool nxt_done = kd + 1 >= mza || mbar_wait_bounded(&BAR[cur ^ 1], ((lv + 1) >> 1) & 1, TILE_WAIT_POLLS);
+      const int code = (cur_done && nxt_done) ? 130 : 131;
+      if (tid == 0 && atomicCAS(A.err, 0, code) == 0) { A.err[1] = tile; A.err[2] = blockIdx.x; A.err[3] = kd; }
+      return;
+    }
+  }
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no
 // link-time dependency on the driver library)
 static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
@@ -470,6 +751,16 @@ static TileKern tile_kernel(int T, int G, bool off32, int KS = 1) {
 // the largest dynamic shared memory a block may use
 #define TILE_SMEM_LIMIT (227 * 1024)
 
+// the paired kernel's layout: two level barriers, two level buffers of U
+// rows of 128 tracers and of the 8 pairs' records, the U rows' global row
+// indices, the tile columns, their explicit fractions
+static size_t tile_pair_smem_bytes(int nu) {
+  auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
+  const size_t nu4 = (size_t)((nu + 3) & ~3);
+  return 127 + 128 + 2 * al(nu4 * 512) + 2 * al((size_t)8 * TILE_PR * 4) + al((size_t)(nu + 3) * 4) + al(16 * 4) +
+         16 * 4;
+}
+
 bool tile_shape_fits(const DevGrid& d, int G) {
   return tile_kernel(d.tile_T, G, true) && tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G) <= TILE_SMEM_LIMIT;
 }
@@ -500,6 +791,26 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   const unsigned nblk = (unsigned)d.ntiles * (unsigned)ngrp_run * (unsigned)KS;
   // element offsets in 32 bits when every array of the batched layout fits
   const bool off32 = (double)d.mwa * d.mza * ntp < 4294967296.0;
+  if (d.tile_pairk && d.tile_T == 16 && G == 128 && KS == 1) {
+    if (!d.tile_paired || !tp.prec.p || tp.prec_gen != d.tile_gen) {
+      set_error("tile stage: the pair records of the step were not formed");
+      return OLAMGPU_E_STATE;
+    }
+    const size_t psmem = tile_pair_smem_bytes(d.tile_nu_max);
+    if (psmem > TILE_SMEM_LIMIT || d.tile_nu_max > 256) {
+      set_error("tile stage: the paired tiles do not fit in shared memory");
+      return OLAMGPU_E_UNSUPPORTED;
+    }
+    alignas(64) CUtensorMap tmS, tmP;
+    OG_CHECK(row_map(&tmS, S, ntp, (size_t)d.mwa * d.mza, G));
+    OG_CHECK(row_map(&tmP, tp.prec.p, TILE_PR, (size_t)d.ntiles * 8 * d.mza, TILE_PR));
+    auto pk = off32 ? k_tile_pair<unsigned> : k_tile_pair<long long>;
+    OG_CUDA(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
+    A.ks = 1;
+    pk<<<(unsigned)d.ntiles * (unsigned)ngrp_run, TILE_THREADS, psmem, s>>>(A, d.tile_pair.p, tmS, tmP);
+    OG_LAUNCHED();
+    return OLAMGPU_OK;
+  }
   const TileKern kern = tile_kernel(d.tile_T, G, off32, KS);
   if (!kern || smem > TILE_SMEM_LIMIT) {
     set_error("tile stage: no kernel for " + std::to_string(d.tile_T) + "-column tiles of " + std::to_string(G) +
@@ -544,10 +855,13 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   const int ntp = C.tr.ntp, nrk = C.opts.nrk_scal, order = C.opts.scal_horiz_adv_order;
   tp.tune_log.clear();
   const ShapeKey key{shape_key(&C.hgrid, ntp, order)};
+  // ord: bit 0 the caller's order, bit 1 the paired kernel
   auto use = [&](const TileShape& sh) -> int {
-    if (d.tile_T != sh.T || d.tile_ord != sh.ord) OG_CHECK(build_tiles(&C.hgrid, d, order, s, sh.T, sh.ord));
+    if (d.tile_T != sh.T || d.tile_ord != (sh.ord & 1)) OG_CHECK(build_tiles(&C.hgrid, d, order, s, sh.T, sh.ord & 1));
     d.tile_G = sh.G;
     d.tile_KS = sh.KS;
+    d.tile_pairk = (sh.ord & 2) != 0 && d.tile_paired;
+    if (d.tile_pairk) OG_CHECK(launch_pair_records(d, tp, s));
     return OLAMGPU_OK;
   };
   auto it = g_shape_cache.find(key);
@@ -566,6 +880,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   // split level sweeps only help where the tiles do not fill the GPU
   const int ks_max = (size_t)d.ntiles * (size_t)((ntp + 63) / 64) < 4 * 148 ? 2 : 1;
   const int Ts[2] = {32, 16};
+  d.tile_pairk = false;
   for (int ord = 0; ord <= 1 && rc == OLAMGPU_OK; ++ord)
   for (int T : Ts) {
     if (d.tile_T != T || d.tile_ord != ord) {
@@ -593,6 +908,27 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
         if (rc != OLAMGPU_OK) break;
         tp.tune_log.push_back({T, G, KS, ord, 0, ms});
         if (!best.T || ms < best_ms) { best = TileShape{T, G, KS, ord}; best_ms = ms; }
+        // the paired kernel on the same tiles
+        if (T == 16 && G == 128 && KS == 1 && d.tile_paired && d.tile_nu_max <= 256 &&
+            tile_pair_smem_bytes(d.tile_nu_max) <= TILE_SMEM_LIMIT) {
+          d.tile_pairk = true;
+          rc = launch_pair_records(d, tp, s);
+          float pm = 1e30f;
+          for (int r = 0; r < 4 && rc == OLAMGPU_OK; ++r) {
+            cudaEventRecord(e0, s);
+            rc = launch_tile_stage(d, tp, S, S0, SCT, OUT, ntp, nrk, nrk, dtr, C.status.p, s, 0, 0, 0);
+            cudaEventRecord(e1, s);
+            if (rc != OLAMGPU_OK) break;
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r > 0) pm = std::min(pm, t);
+          }
+          d.tile_pairk = false;
+          if (rc != OLAMGPU_OK) break;
+          tp.tune_log.push_back({T, G, KS, ord | 2, 0, pm});
+          if (pm < best_ms) { best = TileShape{T, G, KS, ord | 2}; best_ms = pm; }
+        }
       }
       if (rc != OLAMGPU_OK) break;
     }
