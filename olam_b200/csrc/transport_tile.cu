@@ -432,17 +432,19 @@ struct PairArgs {
 
 // a warp per (tile, pair, level): the two columns' records in two registers
 // per lane (word = lane), the union rows' weights picked by shuffles, the
-// non-zero ones compacted in order by a ballot
+// non-zero ones compacted in order by a ballot; the record is assembled in
+// shared memory and stored whole (coalesced)
 __global__ void __launch_bounds__(256) k_pair_records(PairArgs A) {
+  __shared__ __align__(16) float rec[8][TILE_PR];
   const size_t wid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int mza = A.mza;
   if (wid >= (size_t)A.ntiles * 8 * mza) return;   // uniform per warp
   const size_t tp = wid / mza;
   const int kd = (int)(wid - tp * mza);
   const int t = (int)(tp >> 3), pp = (int)(tp & 7);
   const int nT = A.hdr[t].w;
-  float* o = A.prec + wid * TILE_PR;
+  float* r = rec[wl];
   const int ia = 2 * pp, ib = 2 * pp + 1;
   const bool hasa = ia < nT, hasb = ib < nT;
   const int iwa = hasa ? A.tc[((size_t)t * 16 + ia) * TILE_TCW + TILE_TC_IW] : 0;
@@ -451,8 +453,11 @@ __global__ void __launch_bounds__(256) k_pair_records(PairArgs A) {
   const float vb = hasb ? A.wrec[((size_t)iwb * mza + kd) * TILE_WR + lane] : 0.f;
   const int* pt = A.pair + tp * TILE_PT;
   const int ne = hasa ? pt[0] : 0, jab = pt[1], jba = pt[2];
-  unsigned char* ob = reinterpret_cast<unsigned char*>(o + TILE_PR_IDX);
-  float* ow = o + TILE_PR_W;
+  // the entries past the count stay row 0 with zero weights
+  for (int i = lane; i < TILE_PR; i += 32) r[i] = 0.f;
+  __syncwarp();
+  unsigned char* rb = reinterpret_cast<unsigned char*>(r + TILE_PR_IDX);
+  float2* rw = reinterpret_cast<float2*>(r + TILE_PR_W);
   int cnt = 0;
 #pragma unroll
   for (int base = 0; base < TILE_PU; base += 32) {
@@ -466,29 +471,25 @@ __global__ void __launch_bounds__(256) k_pair_records(PairArgs A) {
     const unsigned m = __ballot_sync(0xffffffffu, nz);
     const int pos = cnt + __popc(m & ((1u << lane) - 1u));
     if (nz) {
-      ob[pos] = (unsigned char)(code & 255);
-      ow[2 * pos] = wa;
-      ow[2 * pos + 1] = wb;
+      rb[pos] = (unsigned char)(code & 255);
+      rw[pos] = make_float2(wa, wb);
     }
     cnt += __popc(m);
-  }
-  // the entries past the count: row 0, zero weights (the kernel may read a
-  // group of four whole)
-  for (int i = cnt + lane; i < TILE_PU; i += 32) {
-    ob[i] = 0;
-    ow[2 * i] = 0.f;
-    ow[2 * i + 1] = 0.f;
   }
   // per column: SW, volti/rhos, 1/rhos, D, beta_0..4, omega (record words
   // 20..29), the other column's own-row weight, 0
   const int src = lane < 10 ? 20 + lane : 0;
   const float sa = __shfl_sync(0xffffffffu, va, lane == 10 ? (jab < 0 ? 0 : jab) : src);
   const float sb = __shfl_sync(0xffffffffu, vb, lane == 10 ? (jba < 0 ? 0 : jba) : src);
-  if (lane < 12) {
-    o[TILE_PR_A + lane] = lane < 10 ? sa : (lane == 10 && jab >= 0 ? sa : 0.f);
-    o[TILE_PR_B + lane] = lane < 10 ? sb : (lane == 10 && jba >= 0 ? sb : 0.f);
+  if (lane < 11) {
+    r[TILE_PR_A + lane] = lane < 10 ? sa : (jab >= 0 ? sa : 0.f);
+    r[TILE_PR_B + lane] = lane < 10 ? sb : (jba >= 0 ? sb : 0.f);
   }
-  if (lane < 4) o[lane] = lane == 0 ? __int_as_float(cnt) : 0.f;
+  if (lane == 0) r[0] = __int_as_float(cnt);
+  __syncwarp();
+  float4* o4 = reinterpret_cast<float4*>(A.prec + wid * TILE_PR);
+  const float4* r4 = reinterpret_cast<const float4*>(r);
+  if (lane < TILE_PR / 4) o4[lane] = r4[lane];
 }
 
 int launch_pair_records(const DevGrid& d, Transport& tp, cudaStream_t s) {
@@ -608,6 +609,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
   }
   __syncthreads();   // the explicit fractions
   const bool hasa = 2 * warp < nT, hasb = 2 * warp + 1 < nT;
+  const float fxa = hasa ? FEX[2 * warp] : 0.f, fxb = hasb ? FEX[2 * warp + 1] : 0.f;
   int failed = 0;
   for (int kd = kb; kd < mza; ++kd) {
     const int lv = kd - kb, cur = lv & 1;
@@ -622,29 +624,27 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
       const unsigned* ix4 = reinterpret_cast<const unsigned*>(rp + TILE_PR_IDX);
       const float4* w4 = reinterpret_cast<const float4*>(rp + TILE_PR_W);
       F4 fa = zero4(), fb = zero4();
-      for (int e = 0; e < cnt; e += 4) {
-        const unsigned ix = ix4[e >> 2];
-        const float4 wl = w4[e >> 1], wh = w4[(e >> 1) + 1];
-        {
-          const F4 r = lds4(Ul, (int)(ix & 255u) * RB);
-          fa = fma4s(wl.x, r, fa);
-          fb = fma4s(wl.y, r, fb);
-        }
-        if (e + 1 < cnt) {
-          const F4 r = lds4(Ul, (int)((ix >> 8) & 255u) * RB);
-          fa = fma4s(wl.z, r, fa);
-          fb = fma4s(wl.w, r, fb);
-        }
-        if (e + 2 < cnt) {
-          const F4 r = lds4(Ul, (int)((ix >> 16) & 255u) * RB);
-          fa = fma4s(wh.x, r, fa);
-          fb = fma4s(wh.y, r, fb);
-        }
-        if (e + 3 < cnt) {
-          const F4 r = lds4(Ul, (int)(ix >> 24) * RB);
-          fa = fma4s(wh.z, r, fa);
-          fb = fma4s(wh.w, r, fb);
-        }
+      // eight rows per step (the entries past the count are row 0 with zero
+      // weights), their loads issued together
+      for (int e = 0; e < cnt; e += 8) {
+        const uint2 ix2 = *reinterpret_cast<const uint2*>(ix4 + (e >> 2));
+        const float4 w0 = w4[e >> 1], w1 = w4[(e >> 1) + 1], w2 = w4[(e >> 1) + 2], w3 = w4[(e >> 1) + 3];
+        const F4 r0 = lds4(Ul, (int)(ix2.x & 255u) * RB);
+        const F4 r1 = lds4(Ul, (int)((ix2.x >> 8) & 255u) * RB);
+        const F4 r2 = lds4(Ul, (int)((ix2.x >> 16) & 255u) * RB);
+        const F4 r3 = lds4(Ul, (int)(ix2.x >> 24) * RB);
+        const F4 r4 = lds4(Ul, (int)(ix2.y & 255u) * RB);
+        const F4 r5 = lds4(Ul, (int)((ix2.y >> 8) & 255u) * RB);
+        const F4 r6 = lds4(Ul, (int)((ix2.y >> 16) & 255u) * RB);
+        const F4 r7 = lds4(Ul, (int)(ix2.y >> 24) * RB);
+        fa = fma4s(w0.x, r0, fa); fb = fma4s(w0.y, r0, fb);
+        fa = fma4s(w0.z, r1, fa); fb = fma4s(w0.w, r1, fb);
+        fa = fma4s(w1.x, r2, fa); fb = fma4s(w1.y, r2, fb);
+        fa = fma4s(w1.z, r3, fa); fb = fma4s(w1.w, r3, fb);
+        fa = fma4s(w2.x, r4, fa); fb = fma4s(w2.y, r4, fb);
+        fa = fma4s(w2.z, r5, fa); fb = fma4s(w2.w, r5, fb);
+        fa = fma4s(w3.x, r6, fa); fb = fma4s(w3.y, r6, fb);
+        fa = fma4s(w3.z, r7, fa); fb = fma4s(w3.w, r7, fb);
       }
       // the two columns' own rows at kd
       const F4 sa = lds4(Ul, (2 * warp) * RB);
@@ -652,13 +652,12 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
         if (n == 1 && !hasb) continue;
-        const int c = 2 * warp + n;
         if (kd == kbc[n]) m2[n] = m1[n] = zero4();
         const float* sc = rp + (n == 0 ? TILE_PR_A : TILE_PR_B);
         const float4 q0 = reinterpret_cast<const float4*>(sc)[0];   // SW, volti/rhos, 1/rhos, D
         const float4 q1 = reinterpret_cast<const float4*>(sc)[1];   // beta0 .. beta3
         const float4 q2 = reinterpret_cast<const float4*>(sc)[2];   // beta4, omega, other's own row, 0
-        const float fx = FEX[c];
+        const float fx = n == 0 ? fxa : fxb;
         const F4 own = n == 0 ? sa : sb, other = n == 0 ? sb : sa;
         F4 fd = n == 0 ? fa : fb;
         fd = fma4s(q2.z, other, fd);
