@@ -219,7 +219,9 @@ struct DevGrid {
 // D; 8..11 beta_0..3; 12..15 beta_4, omega, 0, 0; from word 16 the U rows
 // of the non-zero slots as bytes (TILE_NS of them, in slot order), from
 // word 24 their weights; entries past the count are row 0 with weight 0.
-#define TILE_CR 44
+// 48 words: four records (one four-row gather) span a multiple of 128
+// bytes, the alignment of a bulk tensor copy's shared-memory destination.
+#define TILE_CR 48
 #define TILE_CR_IDX 16
 #define TILE_CR_W 24
 // Column pairs of a 16-column tile (the paired stage kernel): columns 2p and

@@ -82,6 +82,7 @@ struct TileArgs {
 };
 
 #define TILE_THREADS 256
+#define G_OF(LPC) (4 * (LPC))   // tracers of a block with LPC lanes per column
 #define TILE_NW (TILE_THREADS / 32)
 // polls of a level barrier before a block gives up (seconds at the slowest)
 #define TILE_WAIT_POLLS (1u << 26)
@@ -261,6 +262,8 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
     k_tile(TileArgs A, const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int RW = CMP ? TILE_CR : TILE_WR;   // words of a staged record
+  // every four-row gather's shared-memory destination on a 128-byte boundary
+  static_assert((4 * RW * 4) % 128 == 0 && (4 * 4 * G_OF(LPC)) % 128 == 0, "gather destinations");
   constexpr int NT = NW * 32;                // threads of the block
   constexpr int CPW = 32 / LPC;              // columns a warp serves at once
   constexpr int TW = NW * CPW;               // columns a block serves at once
@@ -566,6 +569,7 @@ int launch_pair_records(const DevGrid& d, Transport& tp, cudaStream_t s) {
 }
 
 // the stage over paired tiles: a warp per pair, 32 lanes over 128 tracers
+static_assert((4 * TILE_PR * 4) % 128 == 0, "pair-record gather destinations on 128-byte boundaries");
 template <typename OFF>
 __global__ void __launch_bounds__(TILE_THREADS, 2)
     k_tile_pair(TileArgs A, const int* __restrict__ pair, const __grid_constant__ CUtensorMap tmS,
