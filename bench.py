@@ -455,7 +455,7 @@ def shape_sweep(g, st, tr, a):
         dev.scalar_transport_rk(st.rho_old)
         for ordr in (0, 1):
           for T, G, KS, pk in ((32, 64, 1, 0), (32, 32, 1, 0), (32, 128, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0),
-                               (16, 128, 2, 0), (16, 128, 1, 2), (16, 128, 1, 4), (32, 64, 1, 4)):
+                               (16, 128, 2, 0), (16, 128, 1, 2)):
             try:
                 dev.set_tile_shape(T, G, KS, ordr | pk)
             except Exception as e:   # a shape this grid cannot run
@@ -928,8 +928,7 @@ def main():
                                               for r in tlog],
                   "note": "columns per tile, tracers per block, level chunks per tile, tile order (0: the "
                           "library's curve, 1: the caller's numbering; +2: the paired kernel, a warp per "
-                          "column pair reading each U row once for both; +4: the compact records, the "
-                          "level's non-zero slots only); "
+                          "column pair reading each U row once for both); "
                           + ("forced by --tile-shape" if a.tile_shape else
                              "chosen by the library's autotuner on the first step")}
     dev.profile(False, reset=True)

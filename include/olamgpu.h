@@ -389,8 +389,7 @@ int olamgpu_timestep_diag(float* smax, double* sums);
  * the columns' positions (ord bit 0 clear) or along the caller's jtw_prog
  * (bit 0 set); ord bit 1 selects the paired form (T = 16, G = 128, KS = 1:
  * a warp serves two neighbouring columns and reads each tracer row either
- * of them needs once), bit 2 the compact records (KS = 1: per level the
- * list of a column's non-zero slot weights instead of all of them).  By
+ * of them needs once).  By
  * default an autotuner picks the shape on the first step for a grid and
  * tracer count: every shape the shared memory admits runs the stage on that
  * step's inputs and the fastest is kept (cached per grid, tracer count and

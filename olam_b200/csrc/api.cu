@@ -176,7 +176,6 @@ static void release_all() {
   d.tile_T = d.ntiles = d.tile_nu_max = d.tile_order = 0;
   d.tile_paired = false;
   d.tile_pairk = false;
-  d.tile_cmp = false;
   d.tile_G = 64;
   d.tile_KS = 1;
   d.tile_ord = 0;
@@ -197,7 +196,7 @@ static void release_all() {
   DevBuf<float>* tb[] = {&tp.vmasc, &tp.wmasc, &tp.rho_old, &tp.wc, &tp.rhos, &tp.ff, &tp.imp_b,
                          &tp.cfl_red, &tp.gx, &tp.upv, &tp.hiv, &tp.sfv, &tp.scale, &tp.upw,
                          &tp.plain_out[0], &tp.plain_out[1], &tp.akhodx, &tp.emis,
-                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec, &tp.adj_trec, &tp.prec, &tp.crec,
+                         &tp.adj_l[0], &tp.adj_l[1], &tp.adj_l0, &tp.adj_ls, &tp.wrec, &tp.adj_trec, &tp.prec,
                          &tp.adj_planes};
   for (auto* b : tb) b->release();
   tp.rho.release();
@@ -502,23 +501,18 @@ int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
     tp.tuned_ntp = -1;
     return OLAMGPU_OK;
   }
-  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || ord < 0 || ord > 5) {
-    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0..5");
+  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || ord < 0 || ord > 3) {
+    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0..3");
     return OLAMGPU_E_ARG;
   }
-  const bool paired = (ord & 2) != 0, cmp = (ord & 4) != 0;
+  const bool paired = (ord & 2) != 0;
   if (paired && (T != 16 || G != 128 || KS != 1)) {
     set_error("tile shape: the paired kernel runs 16-column tiles of 128 tracers, KS = 1");
     return OLAMGPU_E_ARG;
   }
-  if (cmp && KS != 1) {
-    set_error("tile shape: the compact records run whole level sweeps, KS = 1");
-    return OLAMGPU_E_ARG;
-  }
   const int order = C.opts.scal_horiz_adv_order;
   if (C.g.tile_T != T || C.g.tile_ord != (ord & 1)) OG_CHECK(build_tiles(&C.hgrid, C.g, order, C.stream, T, ord & 1));
-  if (C.g.tile_T != T || !tile_shape_fits(C.g, G) || (paired && !C.g.tile_paired) ||
-      (cmp && !tile_shape_fits_cmp(C.g, G))) {
+  if (C.g.tile_T != T || !tile_shape_fits(C.g, G) || (paired && !C.g.tile_paired)) {
     set_error("tile shape: this grid has no " + std::to_string(T) + "-column tiles of " + std::to_string(G) +
               " tracers within the shared memory" + (paired ? " with column pairs" : ""));
     return OLAMGPU_E_UNSUPPORTED;
@@ -526,7 +520,6 @@ int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
   C.g.tile_G = G;
   C.g.tile_KS = KS;
   C.g.tile_pairk = paired;
-  C.g.tile_cmp = cmp;
   tp.autotune = false;
   return OLAMGPU_OK;
 }
@@ -536,7 +529,7 @@ int olamgpu_tile_shape(int* shape, int max, int* cand, float* ms) {
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return -OLAMGPU_E_STATE; }
   if (shape) {
     shape[0] = C.g.tile_T; shape[1] = C.g.tile_G; shape[2] = C.g.tile_KS;
-    shape[3] = C.g.tile_ord | (C.g.tile_pairk ? 2 : 0) | (C.g.tile_cmp ? 4 : 0);
+    shape[3] = C.g.tile_ord | (C.g.tile_pairk ? 2 : 0);
   }
   const auto& L = C.tp.tune_log;
   for (int i = 0; i < (int)L.size() && i < max; ++i) {

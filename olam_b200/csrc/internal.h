@@ -164,7 +164,6 @@ struct DevGrid {
   DevBuf<int> tile_pair;         // (ntiles * 8, TILE_PT): 16-column tiles as 8 column pairs
   bool tile_paired = false;      // tile_pair holds the tables of the current tiles
   bool tile_pairk = false;       // the stage runs the paired kernel (16 columns, 128 tracers)
-  bool tile_cmp = false;         // the stage reads compact records (the non-zero slots only)
   int tile_gen = 0;              // counts the tile builds (records of other tiles are stale)
   // The adjoint's own tiles when the stage kernel runs another width: the
   // reverse stage moves half as many bytes again per row as the forward and
@@ -213,17 +212,6 @@ struct DevGrid {
 // W[0..TILE_NS), SW, volti / rhos, 1 / rhos, SW - sum W, the vertical flux's
 // coefficients on S(kd-2 .. kd+2) and on S0, wmasc(kd-1), wmasc(kd).
 #define TILE_WR 32
-// Compact record of a tile column's level (TILE_CR words, written with the
-// weight record when the stage runs the compact form): [0] the number of
-// slots with a non-zero weight at the level; 4..7 SW, volti/rhos, 1/rhos,
-// D; 8..11 beta_0..3; 12..15 beta_4, omega, 0, 0; from word 16 the U rows
-// of the non-zero slots as bytes (TILE_NS of them, in slot order), from
-// word 24 their weights; entries past the count are row 0 with weight 0.
-// 48 words: four records (one four-row gather) span a multiple of 128
-// bytes, the alignment of a bulk tensor copy's shared-memory destination.
-#define TILE_CR 48
-#define TILE_CR_IDX 16
-#define TILE_CR_W 24
 // Column pairs of a 16-column tile (the paired stage kernel): columns 2p and
 // 2p+1 of tile order form pair p, and a warp serves both from one read of
 // each U row either of them needs.  Pair table (TILE_PT words): the number
@@ -291,8 +279,6 @@ struct Transport {
   DevBuf<float> wrec;            // (mwa, mza, TILE_WR) weight records of the step
   DevBuf<float> prec;            // (ntiles * 8, mza, TILE_PR) pair records of the step (paired kernel)
   int prec_gen = -1;             // the tile build prec was formed for
-  DevBuf<float> crec;            // (mwa, mza, TILE_CR) compact records of the step (compact form)
-  int crec_gen = -1;             // the tile build crec was formed for
   // adjoint (transport_adjoint.cu): lam rotation, lam0, lams in the batched
   // layout, per-tracer planes
   DevBuf<float> adj_l[2], adj_l0, adj_ls, adj_planes;
@@ -461,7 +447,7 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T = 0, int n
 int build_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s, int T = 0, int ord = 0);
 int build_adj_tiles(const olamgpu_grid* g, DevGrid& d, int order, cudaStream_t s);
 // dynamic shared memory of the stage kernel: T columns, nu_max rows of rb bytes
-size_t tile_smem_bytes(int T, int nu_max, int rb, int rw = TILE_WR);
+size_t tile_smem_bytes(int T, int nu_max, int rb);
 
 // dynamics entry points (dynamics.cu)
 int dyn_setup(const olamgpu_grid* g, const olamgpu_opts* o, cudaStream_t s);

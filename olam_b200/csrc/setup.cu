@@ -300,14 +300,14 @@ int build_fused_weights(const olamgpu_grid* g, DevGrid& d, int order, cudaStream
 
 // ---- tiles of the tiled fused kernel ------------------------------------------
 
-size_t tile_smem_bytes(int T, int nu, int rb, int rw) {
+size_t tile_smem_bytes(int T, int nu, int rb) {
   auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
   // k_tile's layout (128-byte aligned parts after aligning the base): two
   // level barriers, two level buffers of U rows (rows in fours) and of the
   // tile columns' weight records, the U rows' global row indices, slot
   // offsets, tile columns, explicit fractions
   const size_t nu4 = (size_t)((nu + 3) & ~3);
-  return 127 + 128 + 2 * al(nu4 * rb) + 2 * al((size_t)T * rw * 4) + al((size_t)(nu + 3) * 4) +
+  return 127 + 128 + 2 * al(nu4 * rb) + 2 * al((size_t)T * TILE_WR * 4) + al((size_t)(nu + 3) * 4) +
          al((size_t)T * TILE_NS * 4) + al((size_t)T * 4) + (size_t)T * 4;
 }
 

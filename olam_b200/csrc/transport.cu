@@ -272,8 +272,7 @@ static int pipelined_step(Context& C, const float* dtlr, const float* rhos_nrk) 
     // the shape on this step's inputs: the tracers' device copies and the
     // step's records (a rotation buffer as the scratch output)
     OG_CHECK(ensure_q(s));
-    OG_CHECK(tile_autotune(C, tr.q[tr.qcur].p, tr.q[tr.qcur].p, tr.qt.p, tr.q[(tr.qcur + 1) % 3].p, dtlr[nrk - 1],
-                           rhos_nrk));
+    OG_CHECK(tile_autotune(C, tr.q[tr.qcur].p, tr.q[tr.qcur].p, tr.qt.p, tr.q[(tr.qcur + 1) % 3].p, dtlr[nrk - 1]));
     tr.q_valid = false;   // the per-tracer arrays are what the pipelined step reads
   }
   // the RK buffer sequence of the batched step
@@ -398,7 +397,7 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
       // the stage kernel's shape for this grid and tracer count, chosen on
       // this step's inputs (the next rotation buffer is scratch)
       if (tp.autotune && tp.tuned_ntp != ntp)
-        OG_CHECK(tile_autotune(C, A, A, T, tr.q[(a + 1) % 3].p, dtlr[nrk - 1], rhos_nrk));
+        OG_CHECK(tile_autotune(C, A, A, T, tr.q[(a + 1) % 3].p, dtlr[nrk - 1]));
     }
     int in_b = a, out_b = (a + 1) % 3;
     for (int istage = 1; istage <= nrk; ++istage) {

@@ -111,11 +111,9 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
 // does the current tile width have a stage kernel of G tracers per block
 // within the shared memory
 bool tile_shape_fits(const DevGrid& d, int G);
-bool tile_shape_fits_cmp(const DevGrid& d, int G);
 // choose the stage kernel's shape on the step's inputs (S, S0, SCT; OUT is
 // scratch); rebuilds the tile tables when the width changes
-int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT, float* OUT, float dtr,
-                  const float* rhos);
+int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT, float* OUT, float dtr);
 
 // copy the columns outside jtw_prog (colsize floats each) from src to dst
 void launch_copy_cols(const int* cols, int ncol, const float* src, float* dst, size_t colsize,

@@ -60,7 +60,6 @@ struct WeightArgs {
   const float* __restrict__ rhos;   // rhos(:,:,nrk)
   const float* __restrict__ a_w;    // Fortran (mza, 2, 2)
   float* __restrict__ wrec;         // (mwa, mza, TILE_WR)
-  float* __restrict__ crec;         // (mwa, mza, TILE_CR) compact records, or NULL
 };
 
 struct TileArgs {
@@ -82,7 +81,6 @@ struct TileArgs {
 };
 
 #define TILE_THREADS 256
-#define G_OF(LPC) (4 * (LPC))   // tracers of a block with LPC lanes per column
 #define TILE_NW (TILE_THREADS / 32)
 // polls of a level barrier before a block gives up (seconds at the slowest)
 #define TILE_WAIT_POLLS (1u << 26)
@@ -135,7 +133,6 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
     const size_t x = (size_t)iw * mza + kd;
     float* o = A.wrec + x * TILE_WR;
     float sumw = 0.f;
-    float wj[TILE_NS];   // the slot weights, for the compact record
     // four slots at a time (16-byte reads of the face rows of A)
     auto slot_weights = [&](const float4* am4) {
 #pragma unroll
@@ -154,7 +151,6 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
         sumw += acc.z;
         sumw += acc.w;
         reinterpret_cast<float4*>(o)[q] = acc;
-        wj[4 * q] = acc.x; wj[4 * q + 1] = acc.y; wj[4 * q + 2] = acc.z; wj[4 * q + 3] = acc.w;
       }
     };
     // the terrain band of level kd (bands end at increasing levels; past
@@ -182,30 +178,9 @@ __global__ void __launch_bounds__(256) k_weights(WeightArgs A) {
     else if (wk0 < 0.f) face(-wk0, kd + 1, true, 2); // scpb(kd+1) from (kd, kd+1, kd+2)
     else face(-wk0, kd, false, 1);                   // scpt(kd) from (kd-1, kd, kd+1)
     const float rh = __ldg(A.rhos + x);
-    const float4 r5 = make_float4(sw, __ldg(A.volti + x) / rh, 1.0f / rh, sw - sumw);
-    const float4 r6 = make_float4(beta[0], beta[1], beta[2], beta[3]);
-    reinterpret_cast<float4*>(o)[5] = r5;
-    reinterpret_cast<float4*>(o)[6] = r6;
+    reinterpret_cast<float4*>(o)[5] = make_float4(sw, __ldg(A.volti + x) / rh, 1.0f / rh, sw - sumw);
+    reinterpret_cast<float4*>(o)[6] = make_float4(beta[0], beta[1], beta[2], beta[3]);
     reinterpret_cast<float4*>(o)[7] = make_float4(beta[4], wk0 - wkm1, wkm1, wk0);
-    if (A.crec) {
-      // the non-zero slots in slot order: their U rows (bytes) and weights
-      float* cr = A.crec + x * TILE_CR;
-      unsigned char* ci = reinterpret_cast<unsigned char*>(cr + TILE_CR_IDX);
-      float* cw = cr + TILE_CR_W;
-      int cnt = 0;
-#pragma unroll
-      for (int j = 0; j < TILE_NS; ++j)
-        if (wj[j] != 0.f) {
-          ci[cnt] = (unsigned char)(w[TILE_TC_SLOT + j] >> 8);
-          cw[cnt] = wj[j];
-          ++cnt;
-        }
-      for (int j = cnt; j < TILE_NS; ++j) { ci[j] = 0; cw[j] = 0.f; }
-      reinterpret_cast<float4*>(cr)[0] = make_float4(__int_as_float(cnt), 0.f, 0.f, 0.f);
-      reinterpret_cast<float4*>(cr)[1] = r5;
-      reinterpret_cast<float4*>(cr)[2] = r6;
-      reinterpret_cast<float4*>(cr)[3] = make_float4(beta[4], wk0 - wkm1, 0.f, 0.f);
-    }
   }
 }
 
@@ -224,16 +199,6 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
   W.tc = d.tile_tc.p; W.amat = d.tile_a.p;
   W.vmasc = tp.vmasc.p; W.wmasc = tp.wmasc.p; W.volti = d.volti.p; W.rhos = rhos; W.a_w = d.a_w.p;
   W.wrec = tp.wrec.p;
-  W.crec = nullptr;
-  if (d.tile_cmp) {
-    const size_t nc = (size_t)d.mza * d.mwa * TILE_CR;
-    if (tp.crec.n != nc) {
-      OG_CHECK(tp.crec.alloc(nc));
-      OG_CUDA(cudaMemsetAsync(tp.crec.p, 0, tp.crec.bytes(), s));
-    }
-    W.crec = tp.crec.p;
-    tp.crec_gen = d.tile_gen;
-  }
   W.lpw = d.lpw.p; W.lpv = d.lpv.p;
   W.band = d.tile_band.p; W.band_lev = d.tile_band_lev.p;
   k_weights<<<cdiv((size_t)d.ntiles * d.tile_T, 4), 256, 0, s>>>(W);
@@ -255,15 +220,12 @@ int launch_tile_weights(const DevGrid& d, Transport& tp, const float* rhos, cuda
 // KS chunks run by different blocks (A.ks).
 // OFF: the type of element offsets into the batched arrays -- unsigned when
 // they all fit in 32 bits (fewer address instructions), else long long.
-// CMP: the records are the compact ones (the non-zero slots of the level,
-// their U rows and weights in a list: no per-slot test, and no slot table)
-template <int NC, int LPC, typename OFF, bool SPLIT, int NW = TILE_NW, bool CMP = false>
+template <int NC, int LPC, typename OFF, bool SPLIT, int NW = TILE_NW>
 __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
     k_tile(TileArgs A, const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmR) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int RW = CMP ? TILE_CR : TILE_WR;   // words of a staged record
   // every four-row gather's shared-memory destination on a 128-byte boundary
-  static_assert((4 * RW * 4) % 128 == 0 && (4 * 4 * G_OF(LPC)) % 128 == 0, "gather destinations");
+  static_assert((4 * TILE_WR * 4) % 128 == 0 && (4 * 4 * 4 * LPC) % 128 == 0, "gather destinations");
   constexpr int NT = NW * 32;                // threads of the block
   constexpr int CPW = 32 / LPC;              // columns a warp serves at once
   constexpr int TW = NW * CPW;               // columns a block serves at once
@@ -284,7 +246,7 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
   const int klo = SPLIT ? kb + ks * chunk : kb, khi = SPLIT ? min(mza, klo + chunk) : mza;
   const int nu4 = (nU + 3) & ~3;      // rows gathered four at a time
   auto al = [](size_t b) { return (b + 127) & ~size_t(127); };
-  const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * RB), rbuf = al((size_t)T * RW * 4);
+  const size_t ubuf = al((size_t)((A.nu_max + 3) & ~3) * RB), rbuf = al((size_t)T * TILE_WR * 4);
   // 128-byte aligned start (pointer arithmetic on the shared array keeps the
   // accesses shared-memory instructions)
   unsigned char* p = smraw + ((128u - (smem_addr(smraw) & 127u)) & 127u);
@@ -341,7 +303,7 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
     const int myg = warp < ng ? (ng - warp + NW - 1) / NW : 0;
     const int myr = warp < nr ? (nr - warp + NW - 1) / NW : 0;
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * RB + myr * 4 * RW * 4));
+    mbar_arrive_expect_tx(&BAR[b], (unsigned)(myg * 4 * RB + myr * 4 * TILE_WR * 4));
     char* Ub = UB + b * ubuf;
     for (int g = warp; g < ng; g += NW) {
       const int* r = RIDX + 4 * g;
@@ -351,7 +313,7 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
       const int c0 = 4 * q;
       const int y0 = IWT[c0] * mza, y1 = IWT[min(c0 + 1, nT - 1)] * mza;
       const int y2 = IWT[min(c0 + 2, nT - 1)] * mza, y3 = IWT[min(c0 + 3, nT - 1)] * mza;
-      tma_gather4(RBB + b * rbuf + c0 * RW * 4, &tmR, 0, y0 + k, y1 + k, y2 + k, y3 + k, &BAR[b]);
+      tma_gather4(RBB + b * rbuf + c0 * TILE_WR * 4, &tmR, 0, y0 + k, y1 + k, y2 + k, y3 + k, &BAR[b]);
     }
   };
 
@@ -399,46 +361,25 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
       if (c >= nT) continue;
       // the column's window holds no level below its floor
       if (kd == kbc[n]) m2[n] = m1[n] = zero4();
-      const float* rc = Rc + c * RW;
-      const float4 r5 = reinterpret_cast<const float4*>(rc)[CMP ? 1 : 5];   // SW, volti/rhos, 1/rhos, D
-      const float4 r6 = reinterpret_cast<const float4*>(rc)[CMP ? 2 : 6];   // beta0 .. beta3
-      const float2 r7 = reinterpret_cast<const float2*>(rc)[CMP ? 6 : 14];  // beta4, omega
+      const float* rc = Rc + c * TILE_WR;
+      const float4 r5 = reinterpret_cast<const float4*>(rc)[5];   // SW, volti/rhos, 1/rhos, D
+      const float4 r6 = reinterpret_cast<const float4*>(rc)[6];   // beta0 .. beta3
+      const float2 r7 = reinterpret_cast<const float2*>(rc)[14];  // beta4, omega
       const float fx = FEX[c];
       const F4 s0 = lds4(Ul, c * RB);
       // horizontal: sum_j W_j S(slot j) + D S - SW S0
       F4 fd = zero4();
-      if (CMP) {
-        // the level's non-zero slots, four per step (entries past the count
-        // are row 0 with weight 0); none below the column's floor, where
-        // the records are not formed
-        const int cnt = kd >= kbc[n] ? min(__float_as_int(rc[0]), TILE_NS) : 0;
-        const unsigned* ix = reinterpret_cast<const unsigned*>(rc + TILE_CR_IDX);
-        const float4* wv = reinterpret_cast<const float4*>(rc + TILE_CR_W);
-        for (int e = 0; e < cnt; e += 4) {
-          const unsigned i4 = ix[e >> 2];
-          const float4 w = wv[e >> 2];
-          const F4 x0 = lds4(Ul, (int)(i4 & 255u) * RB);
-          const F4 x1 = lds4(Ul, (int)((i4 >> 8) & 255u) * RB);
-          const F4 x2 = lds4(Ul, (int)((i4 >> 16) & 255u) * RB);
-          const F4 x3 = lds4(Ul, (int)(i4 >> 24) * RB);
-          fd = fma4s(w.x, x0, fd);
-          fd = fma4s(w.y, x1, fd);
-          fd = fma4s(w.z, x2, fd);
-          fd = fma4s(w.w, x3, fd);
-        }
-      } else {
-        const int* sl = SLOT + c * TILE_NS;
+      const int* sl = SLOT + c * TILE_NS;
 #pragma unroll
-        for (int q = 0; q < TILE_NS / 4; ++q) {
-          const int4 so = reinterpret_cast<const int4*>(sl)[q];
-          const float4 w4 = reinterpret_cast<const float4*>(rc)[q];
-          // a slot whose weight is zero at this level (a face whose upwind
-          // side does not reach it) is not read
-          if (w4.x != 0.f) fd = fma4s(w4.x, lds4(Ul, so.x), fd);
-          if (w4.y != 0.f) fd = fma4s(w4.y, lds4(Ul, so.y), fd);
-          if (w4.z != 0.f) fd = fma4s(w4.z, lds4(Ul, so.z), fd);
-          if (w4.w != 0.f) fd = fma4s(w4.w, lds4(Ul, so.w), fd);
-        }
+      for (int q = 0; q < TILE_NS / 4; ++q) {
+        const int4 so = reinterpret_cast<const int4*>(sl)[q];
+        const float4 w4 = reinterpret_cast<const float4*>(rc)[q];
+        // a slot whose weight is zero at this level (a face whose upwind
+        // side does not reach it) is not read
+        if (w4.x != 0.f) fd = fma4s(w4.x, lds4(Ul, so.x), fd);
+        if (w4.y != 0.f) fd = fma4s(w4.y, lds4(Ul, so.y), fd);
+        if (w4.z != 0.f) fd = fma4s(w4.z, lds4(Ul, so.z), fd);
+        if (w4.w != 0.f) fd = fma4s(w4.w, lds4(Ul, so.w), fd);
       }
       // vertical quadratic upwind faces, fexpl times sum_q beta_q S(kd-2+q) + omega S0
       fd = fma4s(fx * r6.x, m2[n], fd);
@@ -802,19 +743,10 @@ static TileKern tile_kernel_s(int T, int G, bool off32) {
   if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned, SPLIT> : k_tile<2, 32, long long, SPLIT>;
   return nullptr;
 }
-// the compact-record instances (whole level sweeps)
-static TileKern tile_kernel_c(int T, int G, bool off32) {
-  if (T == 32 && G == 64) return off32 ? k_tile<2, 16, unsigned, false, TILE_NW, true>
-                                       : k_tile<2, 16, long long, false, TILE_NW, true>;
-  if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned, false, TILE_NW, true>
-                                        : k_tile<2, 32, long long, false, TILE_NW, true>;
-  return nullptr;
-}
 // threads of a shape's block
 static unsigned tile_threads(int T, int G) { return (T == 32 && G == 128) ? 512u : (unsigned)TILE_THREADS; }
 // the kernel of a shape; the level sweep is split (KS > 1) only in its own instance
-static TileKern tile_kernel(int T, int G, bool off32, int KS = 1, bool cmp = false) {
-  if (cmp) return KS > 1 ? nullptr : tile_kernel_c(T, G, off32);
+static TileKern tile_kernel(int T, int G, bool off32, int KS = 1) {
   return KS > 1 ? tile_kernel_s<true>(T, G, off32) : tile_kernel_s<false>(T, G, off32);
 }
 
@@ -835,11 +767,6 @@ bool tile_shape_fits(const DevGrid& d, int G) {
   return tile_kernel(d.tile_T, G, true) && tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G) <= TILE_SMEM_LIMIT;
 }
 
-bool tile_shape_fits_cmp(const DevGrid& d, int G) {
-  return tile_kernel(d.tile_T, G, true, 1, true) && d.tile_nu_max <= 256 &&
-         tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G, TILE_CR) <= TILE_SMEM_LIMIT;
-}
-
 int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, const float* S0,
                       const float* SCT, float* OUT, int ntp, int istage, int nrk, float dtr, int* status,
                       cudaStream_t s, int grp0, int ngrp_run, int G_force) {
@@ -858,11 +785,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   A.ff = tp.ff.p; A.wrec = tp.wrec.p;
   A.S = S; A.S0 = S0; A.SCT = SCT; A.OUT = OUT;
   A.err = status;
-  // the compact form where it has an instance (a forced tracer group of
-  // another width, as the per-call step's, runs the slot-record form)
-  const bool cmp = d.tile_cmp && KS == 1 && !(d.tile_pairk && d.tile_T == 16 && G == 128) &&
-                   tile_kernel_c(d.tile_T, G, true) != nullptr;
-  const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G, cmp ? TILE_CR : TILE_WR);
+  const size_t smem = tile_smem_bytes(d.tile_T, d.tile_nu_max, 4 * G);
   const int ngrp_all = (ntp + G - 1) / G;
   if (ngrp_run <= 0) { grp0 = 0; ngrp_run = ngrp_all; }
   if (grp0 < 0 || grp0 + ngrp_run > ngrp_all) { set_error("tile stage: tracer groups out of range"); return OLAMGPU_E_ARG; }
@@ -890,11 +813,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
     OG_LAUNCHED();
     return OLAMGPU_OK;
   }
-  if (cmp && (!tp.crec.p || tp.crec_gen != d.tile_gen)) {
-    set_error("tile stage: the compact records of the step were not formed");
-    return OLAMGPU_E_STATE;
-  }
-  const TileKern kern = tile_kernel(d.tile_T, G, off32, KS, cmp);
+  const TileKern kern = tile_kernel(d.tile_T, G, off32, KS);
   if (!kern || smem > TILE_SMEM_LIMIT) {
     set_error("tile stage: no kernel for " + std::to_string(d.tile_T) + "-column tiles of " + std::to_string(G) +
               " tracers within the shared memory");
@@ -902,8 +821,7 @@ int launch_tile_stage(const DevGrid& d, const Transport& tp, const float* S, con
   }
   alignas(64) CUtensorMap tmS, tmR;
   OG_CHECK(row_map(&tmS, S, ntp, (size_t)d.mwa * d.mza, G));
-  if (cmp) OG_CHECK(row_map(&tmR, tp.crec.p, TILE_CR, (size_t)d.mwa * d.mza, TILE_CR));
-  else OG_CHECK(row_map(&tmR, tp.wrec.p, TILE_WR, (size_t)d.mwa * d.mza, TILE_WR));
+  OG_CHECK(row_map(&tmR, tp.wrec.p, TILE_WR, (size_t)d.mwa * d.mza, TILE_WR));
   OG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<nblk, tile_threads(d.tile_T, G), smem, s>>>(A, tmS, tmR);
   OG_LAUNCHED();
@@ -932,23 +850,20 @@ static unsigned long long shape_key(const olamgpu_grid* g, int ntp, int order) {
   return h;
 }
 
-int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT, float* OUT, float dtr,
-                  const float* rhos) {
+int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT, float* OUT, float dtr) {
   DevGrid& d = C.g;
   Transport& tp = C.tp;
   cudaStream_t s = C.stream;
   const int ntp = C.tr.ntp, nrk = C.opts.nrk_scal, order = C.opts.scal_horiz_adv_order;
   tp.tune_log.clear();
   const ShapeKey key{shape_key(&C.hgrid, ntp, order)};
-  // ord: bit 0 the caller's order, bit 1 the paired kernel, bit 2 the compact records
+  // ord: bit 0 the caller's order, bit 1 the paired kernel
   auto use = [&](const TileShape& sh) -> int {
     if (d.tile_T != sh.T || d.tile_ord != (sh.ord & 1)) OG_CHECK(build_tiles(&C.hgrid, d, order, s, sh.T, sh.ord & 1));
     d.tile_G = sh.G;
     d.tile_KS = sh.KS;
     d.tile_pairk = (sh.ord & 2) != 0 && d.tile_paired;
-    d.tile_cmp = (sh.ord & 4) != 0;
-    // the step's records for these tiles (and their pair or compact forms)
-    OG_CHECK(launch_tile_weights(d, tp, rhos, s));
+    if (d.tile_pairk) OG_CHECK(launch_pair_records(d, tp, s));
     return OLAMGPU_OK;
   };
   auto it = g_shape_cache.find(key);
@@ -968,7 +883,6 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   const int ks_max = (size_t)d.ntiles * (size_t)((ntp + 63) / 64) < 4 * 148 ? 2 : 1;
   const int Ts[2] = {32, 16};
   d.tile_pairk = false;
-  d.tile_cmp = false;
   for (int ord = 0; ord <= 1 && rc == OLAMGPU_OK; ++ord)
   for (int T : Ts) {
     if (d.tile_T != T || d.tile_ord != ord) {
@@ -1016,26 +930,6 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
           if (rc != OLAMGPU_OK) break;
           tp.tune_log.push_back({T, G, KS, ord | 2, 0, pm});
           if (pm < best_ms) { best = TileShape{T, G, KS, ord | 2}; best_ms = pm; }
-        }
-        // the compact records on the same tiles
-        if (KS == 1 && tile_shape_fits_cmp(d, G)) {
-          d.tile_cmp = true;
-          rc = launch_tile_weights(d, tp, rhos, s);
-          float cm = 1e30f;
-          for (int r = 0; r < 4 && rc == OLAMGPU_OK; ++r) {
-            cudaEventRecord(e0, s);
-            rc = launch_tile_stage(d, tp, S, S0, SCT, OUT, ntp, nrk, nrk, dtr, C.status.p, s, 0, 0, 0);
-            cudaEventRecord(e1, s);
-            if (rc != OLAMGPU_OK) break;
-            cudaEventSynchronize(e1);
-            float t = 0.f;
-            cudaEventElapsedTime(&t, e0, e1);
-            if (r > 0) cm = std::min(cm, t);
-          }
-          d.tile_cmp = false;
-          if (rc != OLAMGPU_OK) break;
-          tp.tune_log.push_back({T, G, KS, ord | 4, 0, cm});
-          if (cm < best_ms) { best = TileShape{T, G, KS, ord | 4}; best_ms = cm; }
         }
       }
       if (rc != OLAMGPU_OK) break;
