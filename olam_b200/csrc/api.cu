@@ -520,6 +520,7 @@ int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
   C.g.tile_G = G;
   C.g.tile_KS = KS;
   C.g.tile_pairk = paired;
+  if (!paired) tp.prec.release();   // no pair records without the paired kernel
   tp.autotune = false;
   return OLAMGPU_OK;
 }

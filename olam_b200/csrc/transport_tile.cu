@@ -910,9 +910,14 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
         if (rc != OLAMGPU_OK) break;
         tp.tune_log.push_back({T, G, KS, ord, 0, ms});
         if (!best.T || ms < best_ms) { best = TileShape{T, G, KS, ord}; best_ms = ms; }
-        // the paired kernel on the same tiles
+        // the paired kernel on the same tiles, where its per-step pair
+        // records fit in the free device memory
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t prec_b = (size_t)d.ntiles * 8 * d.mza * TILE_PR * sizeof(float);
         if (T == 16 && G == 128 && KS == 1 && d.tile_paired && d.tile_nu_max <= 256 &&
-            tile_pair_smem_bytes(d.tile_nu_max) <= TILE_SMEM_LIMIT) {
+            tile_pair_smem_bytes(d.tile_nu_max) <= TILE_SMEM_LIMIT &&
+            (tp.prec.n * sizeof(float) >= prec_b || free_b > prec_b + ((size_t)2 << 30))) {
           d.tile_pairk = true;
           rc = launch_pair_records(d, tp, s);
           float pm = 1e30f;
@@ -943,6 +948,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   if (!best.T) { set_error("tile autotune: no shape runs on this grid"); return OLAMGPU_E_UNSUPPORTED; }
   for (auto& r : tp.tune_log)
     if (r.T == best.T && r.G == best.G && r.KS == best.KS && r.ord == best.ord) r.chosen = 1;
+  if (!(best.ord & 2)) tp.prec.release();   // the pair records of the tuning runs
   OG_CHECK(use(best));
   g_shape_cache[key] = best;
   tp.tuned_ntp = ntp;
