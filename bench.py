@@ -348,7 +348,7 @@ def run_reference(a):
     v = full["value"]
     line = {"metric": "tracer cell-updates/s", "value": v, "unit": "cell-updates/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "impl": "reference",
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": workload_name(g, a), "form": "the reference's loops (C++ restatement)",
                        "parallelism": "host threads of one node"},
