@@ -361,88 +361,6 @@ __global__ void k_grad_upv4(DynK g, const int* __restrict__ prog, int nprog, Fou
   }
 }
 
-// The same pass for the common case of second-order reconstruction of all
-// four fields: AC_PLC lanes per column (32 / AC_PLC columns per warp), each
-// lane AC_PLU levels in flight, the column's neighbours, face floors,
-// gradient coefficients, upwind sides and face offsets read once per column
-// into registers (instead of once per level); the arithmetic is that of
-// k_grad_upv4<2>, term for term.
-#define AC_PLC 8
-#define AC_PLU 2
-__global__ void __launch_bounds__(256)
-    k_grad_upv4c(DynK g, const int* __restrict__ prog, int nprog, Four s, const float* __restrict__ cx,
-                 const float* __restrict__ cy, VSide c, const float* __restrict__ vmc, float* __restrict__ upv) {
-  const int j = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) / AC_PLC), hl = threadIdx.x % AC_PLC;
-  if (j >= nprog) return;
-  const int iw = WTAB(j);
-  const int mza = g.mza;
-  const size_t vplane = (size_t)g.mva * mza;
-  const int np = g.npoly[iw];
-  int nb[7], ev[7], lp[7];
-  float wx[7], wy[7], dx[7], dy[7];
-  unsigned side = 0;
-#pragma unroll
-  for (int n = 0; n < 7; ++n) {
-    nb[n] = iw; ev[n] = 0; lp[n] = mza; wx[n] = wy[n] = dx[n] = dy[n] = 0.f;
-    if (n < np) {
-      nb[n] = g.w_nb[iw * 8 + n];
-      ev[n] = g.w_ev[iw * 8 + n];
-      lp[n] = LPV(ev[n]);
-      wx[n] = cx[iw * 7 + n];
-      wy[n] = cy[iw * 7 + n];
-      const int sd = g.v_iw[ev[n] * 2] == iw ? 0 : 1;
-      side |= (unsigned)sd << n;
-      dx[n] = c.dxps[ev[n] * 2 + sd];
-      dy[n] = c.dyps[ev[n] * 2 + sd];
-    }
-  }
-  for (int k0 = hl; k0 < mza; k0 += AC_PLC * AC_PLU) {
-    float c0[AC_PLU][4], a[AC_PLU][4][2];
-#pragma unroll
-    for (int u = 0; u < AC_PLU; ++u) {
-      const int k = k0 + AC_PLC * u;
-#pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        c0[u][f] = k < mza ? s.f[f][(size_t)iw * mza + k] : 0.f;
-        a[u][f][0] = a[u][f][1] = 0.f;
-      }
-    }
-#pragma unroll
-    for (int n = 0; n < 7; ++n) {
-      if (n >= np) break;
-#pragma unroll
-      for (int u = 0; u < AC_PLU; ++u) {
-        const int k = k0 + AC_PLC * u;
-        if (k >= mza || k < lp[n]) continue;
-        const size_t xn = (size_t)nb[n] * mza + k;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          const float d = s.f[f][xn] - c0[u][f];
-          a[u][f][0] = a[u][f][0] + wx[n] * d;
-          a[u][f][1] = a[u][f][1] + wy[n] * d;
-        }
-      }
-    }
-#pragma unroll
-    for (int n = 0; n < 7; ++n) {
-      if (n >= np) break;
-#pragma unroll
-      for (int u = 0; u < AC_PLU; ++u) {
-        const int k = k0 + AC_PLC * u;
-        if (k >= mza || k < lp[n]) continue;
-        const size_t xv = (size_t)ev[n] * mza + k;
-        if ((vmc[xv] < 0.f) != (((side >> n) & 1u) != 0)) continue;   // the other cell is upwind
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          float v = c0[u][f];
-          v = v + dx[n] * a[u][f][0] + dy[n] * a[u][f][1];
-          upv[(size_t)f * vplane + xv] = v;
-        }
-      }
-    }
-  }
-}
-
 // vertical upwind face values of the four fields (scalar_w_column of
 // fluxes_wrtv, prog_wrtv_rk.f90:1085-1126): thread per (column, face kd)
 __global__ void k_upw4(DynK g, const int* __restrict__ prog, int nprog, Four s, const float* __restrict__ wmc,
@@ -1270,11 +1188,7 @@ int dyn_prog_wrtv_rk(int istp) {
       }
       VSide vs{d.dxps.p, d.dyps.p, d.xx0_v.p, d.xy0_v.p, d.yy0_v.p};
       const unsigned plain = 0xFu & ~(m2 | m3);
-      if (m2 == 0xFu) {   // all four fields of second order: the column form
-        k_grad_upv4c<<<cdiv((size_t)gn * AC_PLC, 256), 256, 0, s>>>(gg, gt, gn, f, d.gxc.p, d.gyc.p, vs, y.vmc.p,
-                                                                     y.upv.p);
-        OG_LAUNCHED();
-      } else if (m2 || plain) {
+      if (m2 || plain) {
         k_grad_upv4<2><<<nbg, 256, 0, s>>>(gg, gt, gn, f, m2, plain, d.gxc.p, d.gyc.p, d.xy_hu.p, vs, y.vmc.p,
                                            y.upv.p);
         OG_LAUNCHED();
