@@ -1,0 +1,51 @@
+"""CPU checks of the measurement helpers of bench.py: the cells a step
+updates, the algorithmic bytes of a stage launch, and the error measures of
+the report (normwise max and RMS relative error over the prognostic cells)."""
+import importlib.util
+import os
+
+import numpy as np
+
+from conftest import small_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def bench():
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def test_prognostic_cells_and_mask_agree():
+    b = bench()
+    g, _ = small_case(nxp=4, nlev=8, ntr=1)
+    mask = b.prognostic_mask(g)
+    assert not mask[0].any()                       # the dummy point
+    assert int(mask.sum()) == b.prognostic_cells(g)
+    assert b.cell_updates(g, 7) == 7 * b.prognostic_cells(g)
+
+
+def test_stage_bytes():
+    b = bench()
+    g, _ = small_case(nxp=4, nlev=8, ntr=1)
+    c = b.prognostic_cells(g)
+    assert b.bytes_per_launch(g, 128, 1) == c * (128 * 12 + 32)
+    assert b.bytes_per_launch(g, 128, 2) == c * (128 * 16 + 32)
+
+
+def test_field_errors():
+    b = bench()
+    rng = np.random.default_rng(3)
+    ref = rng.random((5, 6)) + 1.0
+    mask = np.ones_like(ref, bool)
+    mask[0] = False
+    assert b.field_errors(ref, ref, mask) == (0.0, 0.0)
+    out = ref.copy()
+    out[2, 3] += 1e-3                              # one cell off
+    mx, rms = b.field_errors(out, ref, mask)
+    assert abs(mx - 1e-3 / ref[mask].max()) < 1e-15
+    assert abs(rms - 1e-3 / np.sqrt((ref[mask] ** 2).sum())) < 1e-15
+    out[0, 0] += 5.0                               # outside the mask: ignored
+    assert b.field_errors(out, ref, mask)[0] == mx
