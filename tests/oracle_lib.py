@@ -29,9 +29,20 @@ def use_native():
     global _NAME
     if _LIB is not None:
         return _NAME
-    r = subprocess.run(["make", "-s", "-C", ORACLE_DIR, "native"], capture_output=True)
-    if r.returncode == 0 and os.path.exists(os.path.join(ORACLE_DIR, "liboracle_native.so")):
-        _NAME = "liboracle_native.so"
+    # named for this host's CPU features: a build from another machine is not reused
+    import hashlib
+    flags = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("flags", "model name")):
+                    flags += line
+    except OSError:
+        pass
+    name = "liboracle_native_%s.so" % hashlib.sha1(flags.encode()).hexdigest()[:12]
+    r = subprocess.run(["make", "-s", "-C", ORACLE_DIR, "native", "NATIVE_SO=" + name], capture_output=True)
+    if r.returncode == 0 and os.path.exists(os.path.join(ORACLE_DIR, name)):
+        _NAME = name
     return _NAME
 
 
