@@ -29,6 +29,10 @@ __device__ __forceinline__ F4 ldg4(const float* p) {
   const float4 v = __ldg(reinterpret_cast<const float4*>(p));
   return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
 }
+// bring the line at p into L2 ahead of a later load (no register held)
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
 __device__ __forceinline__ void stg4(float* p, F4 v) {
   *reinterpret_cast<float4*>(p) = make_float4(v.a.x, v.a.y, v.b.x, v.b.y);
 }

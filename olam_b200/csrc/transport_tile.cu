@@ -402,6 +402,13 @@ __global__ void __launch_bounds__(NW * 32, NW > TILE_NW ? 1 : (NC == 1 ? 3 : 2))
           s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
           st[n] = ldg4(A.SCT + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
         }
+        // the rows these loads take two levels on, into L2 now (one level
+        // of lead leaves the loads waiting on HBM)
+        if (kd + 6 < mza) prefetch_l2(A.S + (cbase[n] + (OFF)(kd + 6) * (OFF)ntp));
+        if (kd + 3 < mza) {
+          prefetch_l2(A.S0 + (cbase[n] + (OFF)(kd + 3) * (OFF)ntp));
+          prefetch_l2(A.SCT + (cbase[n] + (OFF)(kd + 3) * (OFF)ntp));
+        }
       }
     }
     if (__syncthreads_or(failed)) {
@@ -432,18 +439,17 @@ struct PairArgs {
   float* __restrict__ prec;         // (ntiles * 8, mza, TILE_PR)
 };
 
-// a warp per (tile, pair, level): the two columns' records in two registers
-// per lane (word = lane), the union rows' weights picked by shuffles, the
-// non-zero ones compacted in order by a ballot; the record is assembled in
-// shared memory and stored whole (coalesced)
+// a warp per (tile, pair), looping over the levels: the pair's table decoded
+// once into registers (two union rows per lane); per level the two columns'
+// records in two registers per lane (word = lane), the union rows' weights
+// picked by shuffles, the non-zero ones compacted in order by a ballot, the
+// record assembled in shared memory and stored whole (coalesced)
 __global__ void __launch_bounds__(256) k_pair_records(PairArgs A) {
   __shared__ __align__(16) float rec[8][TILE_PR];
-  const size_t wid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const size_t tp = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int mza = A.mza;
-  if (wid >= (size_t)A.ntiles * 8 * mza) return;   // uniform per warp
-  const size_t tp = wid / mza;
-  const int kd = (int)(wid - tp * mza);
+  if (tp >= (size_t)A.ntiles * 8) return;   // uniform per warp
   const int t = (int)(tp >> 3), pp = (int)(tp & 7);
   const int nT = A.hdr[t].w;
   float* r = rec[wl];
@@ -451,47 +457,61 @@ __global__ void __launch_bounds__(256) k_pair_records(PairArgs A) {
   const bool hasa = ia < nT, hasb = ib < nT;
   const int iwa = hasa ? A.tc[((size_t)t * 16 + ia) * TILE_TCW + TILE_TC_IW] : 0;
   const int iwb = hasb ? A.tc[((size_t)t * 16 + ib) * TILE_TCW + TILE_TC_IW] : 0;
-  const float va = hasa ? A.wrec[((size_t)iwa * mza + kd) * TILE_WR + lane] : 0.f;
-  const float vb = hasb ? A.wrec[((size_t)iwb * mza + kd) * TILE_WR + lane] : 0.f;
   const int* pt = A.pair + tp * TILE_PT;
   const int ne = hasa ? pt[0] : 0, jab = pt[1], jba = pt[2];
-  // the entries past the count stay row 0 with zero weights
-  for (int i = lane; i < TILE_PR; i += 32) r[i] = 0.f;
-  __syncwarp();
-  unsigned char* rb = reinterpret_cast<unsigned char*>(r + TILE_PR_IDX);
-  float2* rw = reinterpret_cast<float2*>(r + TILE_PR_W);
-  int cnt = 0;
+  // this lane's union rows e = lane and lane + 32: the row and its slots in A and B
+  int code[2], ja[2], jb[2];
 #pragma unroll
-  for (int base = 0; base < TILE_PU; base += 32) {
-    const int e = base + lane;
-    const int code = (e < ne) ? pt[4 + e] : 0;
-    const int ja = ((code >> 8) & 255) - 1, jb = ((code >> 16) & 255) - 1;
-    const float xa = __shfl_sync(0xffffffffu, va, ja < 0 ? 0 : ja);
-    const float xb = __shfl_sync(0xffffffffu, vb, jb < 0 ? 0 : jb);
-    const float wa = (e < ne && ja >= 0) ? xa : 0.f, wb = (e < ne && jb >= 0) ? xb : 0.f;
-    const bool nz = (wa != 0.f) || (wb != 0.f);
-    const unsigned m = __ballot_sync(0xffffffffu, nz);
-    const int pos = cnt + __popc(m & ((1u << lane) - 1u));
-    if (nz) {
-      rb[pos] = (unsigned char)(code & 255);
-      rw[pos] = make_float2(wa, wb);
-    }
-    cnt += __popc(m);
+  for (int h = 0; h < 2; ++h) {
+    const int e = lane + 32 * h;
+    code[h] = (e < ne && e < TILE_PU) ? pt[4 + e] : 0;
+    ja[h] = (e < ne) ? ((code[h] >> 8) & 255) - 1 : -1;
+    jb[h] = (e < ne) ? ((code[h] >> 16) & 255) - 1 : -1;
   }
-  // per column: SW, volti/rhos, 1/rhos, D, beta_0..4, omega (record words
-  // 20..29), the other column's own-row weight, 0
   const int src = lane < 10 ? 20 + lane : 0;
-  const float sa = __shfl_sync(0xffffffffu, va, lane == 10 ? (jab < 0 ? 0 : jab) : src);
-  const float sb = __shfl_sync(0xffffffffu, vb, lane == 10 ? (jba < 0 ? 0 : jba) : src);
-  if (lane < 11) {
-    r[TILE_PR_A + lane] = lane < 10 ? sa : (jab >= 0 ? sa : 0.f);
-    r[TILE_PR_B + lane] = lane < 10 ? sb : (jba >= 0 ? sb : 0.f);
+  const float* ra = A.wrec + (size_t)iwa * mza * TILE_WR + lane;
+  const float* rb = A.wrec + (size_t)iwb * mza * TILE_WR + lane;
+  float va = hasa ? ra[0] : 0.f, vb = hasb ? rb[0] : 0.f;
+  for (int kd = 0; kd < mza; ++kd) {
+    // the next level's words, loaded while this one is assembled
+    const float na = (hasa && kd + 1 < mza) ? ra[(size_t)(kd + 1) * TILE_WR] : 0.f;
+    const float nb = (hasb && kd + 1 < mza) ? rb[(size_t)(kd + 1) * TILE_WR] : 0.f;
+    for (int i = lane; i < TILE_PR; i += 32) r[i] = 0.f;
+    __syncwarp();
+    unsigned char* rbt = reinterpret_cast<unsigned char*>(r + TILE_PR_IDX);
+    float2* rw = reinterpret_cast<float2*>(r + TILE_PR_W);
+    int cnt = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float xa = __shfl_sync(0xffffffffu, va, ja[h] < 0 ? 0 : ja[h]);
+      const float xb = __shfl_sync(0xffffffffu, vb, jb[h] < 0 ? 0 : jb[h]);
+      const float wa = ja[h] >= 0 ? xa : 0.f, wb = jb[h] >= 0 ? xb : 0.f;
+      const bool nz = (wa != 0.f) || (wb != 0.f);
+      const unsigned m = __ballot_sync(0xffffffffu, nz);
+      const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+      if (nz) {
+        rbt[pos] = (unsigned char)(code[h] & 255);
+        rw[pos] = make_float2(wa, wb);
+      }
+      cnt += __popc(m);
+    }
+    // per column: SW, volti/rhos, 1/rhos, D, beta_0..4, omega (record words
+    // 20..29), the other column's own-row weight, 0
+    const float sa = __shfl_sync(0xffffffffu, va, lane == 10 ? (jab < 0 ? 0 : jab) : src);
+    const float sb = __shfl_sync(0xffffffffu, vb, lane == 10 ? (jba < 0 ? 0 : jba) : src);
+    if (lane < 11) {
+      r[TILE_PR_A + lane] = lane < 10 ? sa : (jab >= 0 ? sa : 0.f);
+      r[TILE_PR_B + lane] = lane < 10 ? sb : (jba >= 0 ? sb : 0.f);
+    }
+    if (lane == 0) r[0] = __int_as_float(cnt);
+    __syncwarp();
+    float4* o4 = reinterpret_cast<float4*>(A.prec + (tp * mza + kd) * TILE_PR);
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    if (lane < TILE_PR / 4) o4[lane] = r4[lane];
+    __syncwarp();
+    va = na;
+    vb = nb;
   }
-  if (lane == 0) r[0] = __int_as_float(cnt);
-  __syncwarp();
-  float4* o4 = reinterpret_cast<float4*>(A.prec + wid * TILE_PR);
-  const float4* r4 = reinterpret_cast<const float4*>(r);
-  if (lane < TILE_PR / 4) o4[lane] = r4[lane];
 }
 
 int launch_pair_records(const DevGrid& d, Transport& tp, cudaStream_t s) {
@@ -502,7 +522,7 @@ int launch_pair_records(const DevGrid& d, Transport& tp, cudaStream_t s) {
   A.mza = d.mza; A.ntiles = d.ntiles;
   A.hdr = reinterpret_cast<const int4*>(d.tile_hdr.p);
   A.tc = d.tile_tc.p; A.pair = d.tile_pair.p; A.wrec = tp.wrec.p; A.prec = tp.prec.p;
-  const size_t warps = (size_t)d.ntiles * 8 * d.mza;
+  const size_t warps = (size_t)d.ntiles * 8;
   k_pair_records<<<(unsigned)cdiv(warps * 32, 256), 256, 0, s>>>(A);
   OG_LAUNCHED();
   tp.prec_gen = d.tile_gen;
@@ -680,6 +700,11 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
           if (kd + 1 < mza) {
             s00[n] = ldg4(A.S0 + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
             st[n] = ldg4(A.SCT + (cbase[n] + (OFF)(kd + 1) * (OFF)ntp));
+          }
+          if (kd + 6 < mza) prefetch_l2(A.S + (cbase[n] + (OFF)(kd + 6) * (OFF)ntp));
+          if (kd + 3 < mza) {
+            prefetch_l2(A.S0 + (cbase[n] + (OFF)(kd + 3) * (OFF)ntp));
+            prefetch_l2(A.SCT + (cbase[n] + (OFF)(kd + 3) * (OFF)ntp));
           }
         }
       }
