@@ -944,7 +944,18 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
             tile_pair_smem_bytes(d.tile_nu_max) <= TILE_SMEM_LIMIT &&
             (tp.prec.n * sizeof(float) >= prec_b || free_b > prec_b + ((size_t)2 << 30))) {
           d.tile_pairk = true;
-          rc = launch_pair_records(d, tp, s);
+          // its per-step pair records count against it, shared by the nrk stages
+          float rec_ms = 1e30f;
+          for (int r = 0; r < 2 && rc == OLAMGPU_OK; ++r) {
+            cudaEventRecord(e0, s);
+            rc = launch_pair_records(d, tp, s);
+            cudaEventRecord(e1, s);
+            if (rc != OLAMGPU_OK) break;
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r > 0) rec_ms = t;
+          }
           float pm = 1e30f;
           for (int r = 0; r < 4 && rc == OLAMGPU_OK; ++r) {
             cudaEventRecord(e0, s);
@@ -958,6 +969,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
           }
           d.tile_pairk = false;
           if (rc != OLAMGPU_OK) break;
+          pm += rec_ms / (float)nrk;
           tp.tune_log.push_back({T, G, KS, ord | 2, 0, pm});
           if (pm < best_ms) { best = TileShape{T, G, KS, ord | 2}; best_ms = pm; }
         }
