@@ -455,7 +455,7 @@ def shape_sweep(g, st, tr, a):
         dev.scalar_transport_rk(st.rho_old)
         for ordr in (0, 1):
           for T, G, KS, pk in ((32, 64, 1, 0), (32, 32, 1, 0), (32, 128, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0),
-                               (16, 128, 2, 0), (16, 128, 1, 2)):
+                               (16, 128, 2, 0), (16, 128, 1, 2), (8, 128, 1, 0)):
             try:
                 dev.set_tile_shape(T, G, KS, ordr | pk)
             except Exception as e:   # a shape this grid cannot run

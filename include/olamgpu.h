@@ -383,8 +383,8 @@ int olamgpu_timestep(unsigned flags, int nmass, const int* mass_ids);
 int olamgpu_timestep_diag(float* smax, double* sums);
 
 /* ---- shape of the tiled stage kernel -------------------------------------------
- * The tiled transport kernel runs tiles of up to T neighbouring columns (16
- * or 32) with G tracers per block (32, 64 or 128), the levels of a tile
+ * The tiled transport kernel runs tiles of up to T neighbouring columns (8,
+ * 16 or 32) with G tracers per block (32, 64 or 128; 8-column tiles 128), the levels of a tile
  * swept by KS blocks, the tiles running along the library's own curve over
  * the columns' positions (ord bit 0 clear) or along the caller's jtw_prog
  * (bit 0 set); ord bit 1 selects the paired form (T = 16, G = 128, KS = 1:

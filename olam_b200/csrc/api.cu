@@ -501,8 +501,9 @@ int olamgpu_set_tile_shape(int T, int G, int KS, int ord) {
     tp.tuned_ntp = -1;
     return OLAMGPU_OK;
   }
-  if ((T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || ord < 0 || ord > 3) {
-    set_error("tile shape: T 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0..3");
+  if ((T != 8 && T != 16 && T != 32) || (G != 32 && G != 64 && G != 128) || KS < 1 || KS > 8 || ord < 0 ||
+      ord > 3) {
+    set_error("tile shape: T 8, 16 or 32, G 32, 64 or 128, 1 <= KS <= 8, order 0..3");
     return OLAMGPU_E_ARG;
   }
   const bool paired = (ord & 2) != 0;

@@ -482,17 +482,21 @@ void make_tiles(const olamgpu_grid* g, int order, TileHost& th, int T_req, int n
   int T = 0, numax = 0;
   // one or two columns for each of the 16 half-warps of a block (64 tracers
   // per block: 256-byte rows), or the width asked for.  Neighbourhoods are
-  // capped where two blocks of the widest rows the stage kernel runs on
-  // tiles of this width fit an SM (32 columns: 64 tracers, 256-byte rows;
-  // 16 columns: 128 tracers, 512-byte rows), or at nu_cap when given.
-  const int cand[] = {32, 16};
+  // capped where the blocks of the widest rows the stage kernel runs on
+  // tiles of this width fit an SM: two for 32 columns (64 tracers,
+  // 256-byte rows) and 16 columns (128 tracers, 512-byte rows), three for
+  // 8 columns (128 tracers: a warp per column, one column each), or at
+  // nu_cap when given.  8-column tiles only when asked for.
+  const int cand[] = {32, 16, 8};
   for (int Tc : cand) {
     if (T_req > 0 && Tc != T_req) continue;
+    if (T_req <= 0 && Tc == 8) continue;
     int cap = nu_cap;
     if (cap <= 0) {
-      const int rb = Tc == 16 ? 512 : 256;
+      const int rb = Tc == 32 ? 256 : 512;
+      const size_t smax = Tc == 8 ? (size_t)(227 / 3 - 1) * 1024 : (size_t)TILE_SMEM_MAX;
       cap = 4;
-      while (tile_smem_bytes(Tc, cap + 4, rb) <= TILE_SMEM_MAX) cap += 4;
+      while (tile_smem_bytes(Tc, cap + 4, rb) <= smax) cap += 4;
     }
     const int nu = form(Tc, cap);
     std::fill(stamp.begin(), stamp.end(), -1);

@@ -369,7 +369,8 @@ int transport_run(const float* rho_old_host, olamgpu_cfl_diag* diag) {
   // domain: the tracers go through in groups of 64 so that the copies in,
   // the step and the copies out of different groups overlap
   const bool pipelined = C.coherence == OLAMGPU_SYNC_EACH_CALL && tiled && C.opts.iscal_monot == 0 &&
-                         !tp.have_turb && !C.halo.on && d.n_nonprog == 0 && tr.n > 64;
+                         !tp.have_turb && !C.halo.on && d.n_nonprog == 0 && tr.n > 64 &&
+                         tile_shape_fits(d, 64);   // its groups are 64 tracers wide
   float dtlr[3];
   OG_CHECK(transport_prepare(C, rho_old_host, !pipelined, dtlr));
   const float* rhos_nrk = tp.rhos.p + (size_t)(nrk - 1) * wz;

@@ -545,6 +545,13 @@ int adjoint_core(Context& C, const float* rho_old_host) {
   if (C.g.tile_T != 32 && (C.g.adj_tiles.T == 0 || C.g.adj_tiles.order != C.g.tile_order))
     OG_CHECK(build_adj_tiles(&C.hgrid, C.g, C.g.tile_order, s));
   const DevGrid& d = C.g;
+  {
+    const int at = adj_tiles_of(d).T;
+    if (at != 16 && at != 32) {
+      set_error("the adjoint runs on 16- or 32-column tiles; none could be built for this grid");
+      return OLAMGPU_E_UNSUPPORTED;
+    }
+  }
   const int mza = d.mza, mwa = d.mwa;
   const int nrk = C.opts.nrk_scal;
   const int ntp = C.tr.ntp;

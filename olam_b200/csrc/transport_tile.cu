@@ -753,7 +753,7 @@ static int row_map(CUtensorMap* m, const float* base, int width, size_t nrows, i
 
 bool tile_stage_available(const DevGrid& d, const Transport& tp, int order) {
   (void)tp;
-  return (d.tile_T == 16 || d.tile_T == 32) && d.tile_order == order;
+  return (d.tile_T == 8 || d.tile_T == 16 || d.tile_T == 32) && d.tile_order == order;
 }
 
 // the stage kernel of a tile shape (T columns, G tracers per block)
@@ -766,6 +766,8 @@ static TileKern tile_kernel_s(int T, int G, bool off32) {
   if (T == 32 && G == 32) return off32 ? k_tile<1, 8, unsigned, SPLIT> : k_tile<1, 8, long long, SPLIT>;
   if (T == 16 && G == 64) return off32 ? k_tile<1, 16, unsigned, SPLIT> : k_tile<1, 16, long long, SPLIT>;
   if (T == 16 && G == 128) return off32 ? k_tile<2, 32, unsigned, SPLIT> : k_tile<2, 32, long long, SPLIT>;
+  // 8-column tiles of 128 tracers: a warp per column, three blocks per SM
+  if (T == 8 && G == 128) return off32 ? k_tile<1, 32, unsigned, SPLIT> : k_tile<1, 32, long long, SPLIT>;
   return nullptr;
 }
 // threads of a shape's block
@@ -906,7 +908,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
   int rc = OLAMGPU_OK;
   // split level sweeps only help where the tiles do not fill the GPU
   const int ks_max = (size_t)d.ntiles * (size_t)((ntp + 63) / 64) < 4 * 148 ? 2 : 1;
-  const int Ts[2] = {32, 16};
+  const int Ts[3] = {32, 16, 8};
   d.tile_pairk = false;
   for (int ord = 0; ord <= 1 && rc == OLAMGPU_OK; ++ord)
   for (int T : Ts) {
@@ -914,7 +916,7 @@ int tile_autotune(Context& C, const float* S, const float* S0, const float* SCT,
       rc = build_tiles(&C.hgrid, d, order, s, T, ord);
       if (rc != OLAMGPU_OK || d.tile_T != T) { rc = OLAMGPU_OK; continue; }   // no tables of this width
     }
-    const int Gs[3] = {64, T == 32 ? 32 : 128, T == 32 ? 128 : 0};
+    const int Gs[3] = {T == 8 ? 0 : 64, T == 32 ? 32 : 128, T == 32 ? 128 : 0};
     for (int G : Gs) {
       if (!G) continue;
       if (!tile_shape_fits(d, G)) continue;

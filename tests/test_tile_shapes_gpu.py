@@ -1,5 +1,6 @@
 """GPU parity of every shape of the tiled transport kernel (columns per tile
-T, tracers per block G, level chunks per tile KS, tile order) against the FP64 oracle,
+T = 8, 16 or 32, tracers per block G, level chunks per tile KS, tile order)
+against the FP64 oracle,
 with and without terrain, and the autotuner that picks among them."""
 import numpy as np
 import pytest
@@ -16,7 +17,8 @@ TOL64 = 1e-5
 # order: bit 0 the caller's column order, bit 1 the paired kernel (column
 # pairs of 16-column tiles reading each U row once for both)
 SHAPES = [(32, 64, 1, 0), (32, 32, 1, 0), (16, 64, 1, 0), (16, 128, 1, 0), (32, 128, 1, 0), (32, 64, 2, 0),
-          (32, 32, 3, 1), (16, 128, 2, 1), (32, 128, 2, 1), (32, 64, 1, 1), (16, 128, 1, 2), (16, 128, 1, 3)]
+          (32, 32, 3, 1), (16, 128, 2, 1), (32, 128, 2, 1), (32, 64, 1, 1), (16, 128, 1, 2), (16, 128, 1, 3),
+          (8, 128, 1, 0), (8, 128, 2, 1)]
 
 
 def tracers(g, ntr, seed):
