@@ -82,6 +82,10 @@ def parse():
     p.add_argument("--large", action="store_true",
                    help="only the large combined run (NXP=400, 80 levels, 32 tracers, 24 long steps of 60 s)")
     p.add_argument("--large-nxp", type=int, default=400)
+    p.add_argument("--large-chk", type=int, default=12,
+                   help="large run: a checkpoint every this many steps (kept in page-locked host memory)")
+    p.add_argument("--large-seg", type=int, default=4,
+                   help="large run: the adjoint holds this many steps' transport inputs at once")
     p.add_argument("--tile-shape", default="",
                    help="T,G,KS: force this shape of the tiled stage kernel (default: the autotuner's)")
     p.add_argument("--shape-sweep", action="store_true",
@@ -576,17 +580,35 @@ def bench_window(a, max_over_ranks):
     return out
 
 
+def recomputed_steps(nsteps, nchk, part):
+    """Long steps the window adjoint runs again: each part [a, b) of a
+    segment [s0, s1) (parts of `part` steps from s0, reversed from the last;
+    part 0 or above nchk: the whole segment) runs the steps s0 .. b-1 from
+    the segment's checkpoint."""
+    part = nchk if part <= 0 else min(part, nchk)
+    n = 0
+    for s0 in range(0, nsteps, nchk):
+        s1 = min(nsteps, s0 + nchk)
+        b = s1
+        while b > s0:
+            n += b - s0
+            b = s0 + (b - 1 - s0) // part * part
+    return n
+
+
 def bench_large(a):
     """The large combined run: NXP=400 (1,600,002 columns), 80 levels to
     40 km, the balanced jet, 32 FP32 tracers with a surface emission each,
     through the whole device long step (4 acoustic RK3 steps, RK3 tracer
     transport, damping) for 24 steps of 60 s, replayed as a CUDA graph
     (device time of the 24 steps); then the window adjoint over the same 24
-    steps with a checkpoint every a.win_chk steps, if the device memory
-    holds it (an allocation failure is reported, not hidden).  Throughput:
-    tracer cell-updates/s; the HBM fraction counts the bytes of the kernels
+    steps with a checkpoint every a.large_chk steps kept in page-locked host
+    memory, the adjoint reversing a.large_seg steps at a time (an allocation
+    failure is reported, not hidden).  Throughput: tracer cell-updates/s,
+    forward and backward; the HBM fraction counts the bytes of the kernels
     with an algorithmic byte count (acoustic kernels, the tracer stages and
-    records) over the whole step's device time."""
+    records, the reverse stages) over the device time.  Device memory in use
+    is sampled during the window's two halves (the peak of the samples)."""
     import torch
     from olam_b200 import abi
     from olam_b200.lib import HostState, OlamGpu
@@ -616,6 +638,23 @@ def bench_large(a):
         free, total = torch.cuda.mem_get_info()
         return (total - free) / 1e9
 
+    class PeakSampler:
+        """Device memory in use, sampled every 20 ms while a call runs."""
+        def __enter__(self):
+            self.peak, self.stop = used_gb(), threading.Event()
+
+            def run():
+                while not self.stop.wait(0.02):
+                    self.peak = max(self.peak, used_gb())
+            self.th = threading.Thread(target=run, daemon=True)
+            self.th.start()
+            return self
+
+        def __exit__(self, *exc):
+            self.stop.set()
+            self.th.join()
+            self.peak = max(self.peak, used_gb())
+
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -623,7 +662,9 @@ def bench_large(a):
         pass
     peak = float(peaks.get("hbm_gbs") or 6650.0)
     try:
-        var_p = [t.copy() for t in tr]
+        # the tracers as registered are the start of both runs (the device
+        # steps never write the host arrays back)
+        var_p = tr
         var_t = [np.zeros_like(t) for t in tr]
         dev.register_scalars(var_p, var_t)
         dev.set_surface_emission(emis)
@@ -655,11 +696,15 @@ def bench_large(a):
         per_launch["tile_stage1"] = (ntr * 12 + 32) * cells
         per_launch["tile_stage"] = (ntr * 16 + 32) * cells
         per_launch["tile_weights"] = 128 * cells
-        step_bytes, counted_ms = 0.0, 0.0
-        for name, b in per_launch.items():
-            if name in prof and prof[name][1]:
-                step_bytes += b * prof[name][1] / nprof
-                counted_ms += prof[name][0] / nprof
+
+        def counted(pr, n):
+            b, ms = 0.0, 0.0
+            for name, x in per_launch.items():
+                if name in pr and pr[name][1]:
+                    b += x * pr[name][1] / n
+                    ms += pr[name][0] / n
+            return b, ms
+        step_bytes, counted_ms = counted(prof, nprof)
         ms_step = fwd_ms / nsteps
         out["forward"] = {
             "ms_per_step": ms_step, "cell_updates_per_s": ntr * cells / (ms_step * 1e-3),
@@ -674,35 +719,64 @@ def bench_large(a):
         out["device_gb_in_use"] = mem
         # the window and its adjoint from the same start
         dev.sync_to_device(abi.F_ALL)
-        for t, t0 in zip(var_p, tr):
-            t[...] = t0
-        dev.sync_to_device(abi.F_SCALARS)
         torch.cuda.synchronize()
+        wa = {"checkpoint_every": a.large_chk, "steps_reversed_at_once": a.large_seg,
+              "checkpoints": "page-locked host memory"}
         try:
-            e0.record(stream)
-            dev.window_forward(nsteps, a.win_chk, abi.TS_GRAPH)
-            e1.record(stream)
-            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dev.window_memory(True, a.large_seg, nsteps, a.large_chk)
+            wa["host_page_lock_s"] = time.perf_counter() - t0
+            with PeakSampler() as ps:
+                e0.record(stream)
+                dev.window_forward(nsteps, a.large_chk, abi.TS_GRAPH)
+                e1.record(stream)
+                torch.cuda.synchronize()
             wf_ms = e0.elapsed_time(e1)
-            mem["after_window_forward"] = used_gb()
-            lam = [np.zeros((g.mwa, g.mza), np.float32) for _ in range(ntr)]
+            mem["window_forward_peak"] = ps.peak
+            # dJ/d(tracers after the window) at 200 receptor cells per tracer,
+            # in the registered arrays themselves (not read again)
+            lam = var_p
             rr = np.random.default_rng(43)
-            iw = rr.integers(1, g.mwa, 200)
-            kk = g.lpw[iw] - 1 + rr.integers(0, 3, 200)
             for n in range(ntr):
+                lam[n][...] = 0.0
+                iw = rr.integers(1, g.mwa, 200)
+                kk = g.lpw[iw] - 1 + rr.integers(0, 3, 200)
                 np.add.at(lam[n], (iw, kk), rr.standard_normal(200).astype(np.float32))
             dev.profile(True, reset=True)
-            dev.window_adjoint(lam)
+            with PeakSampler() as ps:
+                e0.record(stream)
+                dev.window_adjoint(lam, lam_sct=var_t, in_place=True)
+                e1.record(stream)
+                torch.cuda.synchronize()
+            adj_ms = e0.elapsed_time(e1)
             aprof = dev.profile_read()
             dev.profile(False, reset=True)
-            adj_ms = aprof["window_adjoint"][0]
+            mem["window_adjoint_peak"] = ps.peak
             mem["after_adjoint"] = used_gb()
-            out["adjoint"] = {"window_forward_ms": wf_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / wf_ms,
-                              "cell_updates_per_s": ntr * cells * nsteps / (adj_ms * 1e-3),
-                              "checkpoint_every": a.win_chk}
+            # algorithmic bytes of the backward: the recomputed dynamics (the
+            # acoustic kernels' counts) and the reverse stages (24 B per
+            # tracer-cell: read lam, write lam_in, read-modify-write lam(scp0)
+            # and lam(sct); 128 B of records per cell)
+            per_launch["adj_stage"] = (ntr * 24 + 128) * cells
+            bwd_bytes, bwd_counted_ms = counted(aprof, 1)
+            wa.update({
+                "window_forward_ms": wf_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / wf_ms,
+                "forward_cell_updates_per_s": ntr * cells * nsteps / (wf_ms * 1e-3),
+                "cell_updates_per_s": ntr * cells * nsteps / (adj_ms * 1e-3),
+                "algorithmic_gb": bwd_bytes / 1e9,
+                "hbm_frac": bwd_bytes / (adj_ms * 1e-3) / 1e9 / peak,
+                "hbm_frac_of_counted_kernels": (bwd_bytes / (bwd_counted_ms * 1e-3) / 1e9 / peak
+                                                if bwd_counted_ms else None),
+                "recompute_ms": aprof.get("window_recompute", (None,))[0],
+                "reverse_stage_ms": aprof.get("adj_stage", (None,))[0],
+                "records_ms": aprof.get("adj_records", (None,))[0],
+                "recomputed_steps": recomputed_steps(nsteps, a.large_chk, a.large_seg),
+                "kernels_ms": {k: v[0] for k, v in aprof.items()},
+            })
+            out["adjoint"] = wa
         except Exception as e:   # the library's allocation failure, reported as such
-            out["adjoint"] = {"unavailable": str(e)[:300], "checkpoint_every": a.win_chk,
-                              "device_gb_in_use_at_failure": used_gb()}
+            wa.update({"unavailable": str(e)[:300], "device_gb_in_use_at_failure": used_gb()})
+            out["adjoint"] = wa
     finally:
         dev.close()
     return out

@@ -155,6 +155,7 @@ static void unregister_state_arrays() {
 static void release_all() {
   unregister_state_arrays();
   window_release();
+  window_memory_release();
   pd_adjoint_release();
   Context& C = ctx();
   DevGrid& d = C.g;
@@ -547,6 +548,10 @@ int olamgpu_tile_shape(int* shape, int max, int* cand, float* ms) {
 int olamgpu_window_forward(int nsteps, int nchk, unsigned flags) { return window_forward(nsteps, nchk, flags); }
 
 int olamgpu_window_adjoint(float* const* lam, float* const* lam_sct) { return window_adjoint(lam, lam_sct); }
+
+int olamgpu_window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk) {
+  return window_memory(host_checkpoints, segment_steps, nsteps, nchk);
+}
 
 void* olamgpu_stream(void) { return (void*)ctx().stream; }
 

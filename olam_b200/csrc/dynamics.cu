@@ -1290,7 +1290,10 @@ int dyn_tend0(float* rho_old_host) {
   k_tend0_v<<<cdiv((size_t)(C.g.mva - 1) * C.g.mza, 256), 256, 0, s>>>(g, y.vmt.p, tp.vmasc.p);
   OG_LAUNCHED(); OG_LAUNCHED();
   // scalar tendencies var_t = 0 for k >= lpw (the device copies)
-  for (int n = 0; n < C.tr.n; ++n) OG_CUDA(cudaMemsetAsync(C.tr.t[n].p, 0, (size_t)C.g.mza * C.g.mwa * 4, s));
+  // (a window's adjoint lends the per-tracer arrays' memory out while it
+  // runs the dynamics again: there are none to clear then)
+  for (int n = 0; n < C.tr.n; ++n)
+    if (C.tr.t[n].p) OG_CUDA(cudaMemsetAsync(C.tr.t[n].p, 0, (size_t)C.g.mza * C.g.mwa * 4, s));
   if (C.tr.q_valid && C.tr.qt.p) OG_CUDA(cudaMemsetAsync(C.tr.qt.p, 0, C.tr.qt.bytes(), s));
   if (C.coherence == OLAMGPU_SYNC_EACH_CALL) {
     OG_CHECK(dyn_state_to_host(OLAMGPU_F_TEND | OLAMGPU_F_VMASC | OLAMGPU_F_WMASC, s));

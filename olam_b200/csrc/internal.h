@@ -84,10 +84,13 @@ struct ProfScope {
 };
 #define OG_PROF(name, s) ::olamgpu::ProfScope og_prof_scope_(name, s)
 
+// a device array; a borrowed one is a view of memory another buffer owns
+// (release forgets it without freeing)
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool owned = true;
   int alloc(size_t count) {
     if (p && n == count) return OLAMGPU_OK;
     release();
@@ -101,12 +104,43 @@ struct DevBuf {
     n = count;
     return OLAMGPU_OK;
   }
+  void borrow(T* q, size_t count) {
+    release();
+    p = q;
+    n = count;
+    owned = false;
+  }
   void release() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    owned = true;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// page-locked host memory (device copies to and from it run asynchronously)
+struct HostBuf {
+  char* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (p && n == count) return OLAMGPU_OK;
+    release();
+    if (count == 0) return OLAMGPU_OK;
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&p), count, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error(std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+      return OLAMGPU_E_NOMEM;
+    }
+    n = count;
+    return OLAMGPU_OK;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
   }
-  size_t bytes() const { return n * sizeof(T); }
 };
 
 // ---- device grid ------------------------------------------------------------
@@ -386,22 +420,36 @@ struct Halo {
 
 // checkpointed window of long steps (window.cu): the state at the start of
 // every segment of nchk steps, the state after the window, and the step
-// inputs of the segment being reversed
+// inputs of the part of a segment being reversed
+struct StateBlob {                   // one saved state, on the device or in page-locked host memory
+  DevBuf<char> dev;
+  int slot = -1;                     // its entry of WindowMem::pool when on the host
+};
+
 struct Window {
   bool valid = false;
   bool tracers = false;              // checkpoints hold the tracers (limited transport)
+  bool lean = false;                 // the adjoint borrows the tracer buffers (unlimited transport)
   int nsteps = 0, nchk = 0;
   unsigned flags = 0;
-  std::vector<DevBuf<char>> chk;
+  std::vector<StateBlob> chk;
   std::vector<int> chk_qcur;
   std::vector<char> chk_div_first, chk_vort_first;
-  DevBuf<char> fin;
+  StateBlob fin;
   int fin_qcur = 0;
   bool fin_div_first = false, fin_vort_first = false;
-  DevBuf<char> seg;                  // (nchk) x the inputs of one step
+  DevBuf<char> seg;                  // (steps held at once) x the inputs of one step
   DevBuf<float> lsacc;               // adjoint of the tendencies, summed over the steps
   DevBuf<float*> ptab;
   DevBuf<float> planes;
+};
+
+// where the next window keeps its states (olamgpu_window_memory); kept
+// across windows so that the host memory is page-locked once
+struct WindowMem {
+  bool host = false;                 // checkpoints and the final state in page-locked host memory
+  int seg_steps = 0;                 // steps whose transport inputs the adjoint holds at once (0: nchk)
+  std::vector<HostBuf> pool;         // the final state, then checkpoints 0 .. nseg-1
 };
 
 struct Context {
@@ -421,6 +469,7 @@ struct Context {
   Glue glue;
   Halo halo;
   Window win;
+  WindowMem winmem;
   DevBuf<int> status;        // device status word (bounds/NaN flags)
 };
 
@@ -505,7 +554,9 @@ int adjoint_ready(Context& C);
 // densities, rho_old): tp.adj_l[0] holds the adjoint of the step's output
 // in the batched layout; on return tp.adj_l[nrk & 1] holds the adjoint of
 // its input and tp.adj_ls that of the tendencies
-int adjoint_core(Context& C, const float* rho_old_host);
+// ls_acc: the adjoint of the tendencies accumulates into adj_ls (a window
+// sums it over its steps) instead of starting from zero
+int adjoint_core(Context& C, const float* rho_old_host, bool ls_acc = false);
 // the long step's device sequence (timestep.cu); without the transport:
 // the dynamics and the glue of thil only
 int glue_run_sequence(Context& C, unsigned flags, bool with_transport);
@@ -513,9 +564,13 @@ int glue_run_sequence(Context& C, unsigned flags, bool with_transport);
 int window_forward(int nsteps, int nchk, unsigned flags);
 int window_adjoint(float* const* lam, float* const* lam_sct);
 void window_release();
+int window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk);
+void window_memory_release();
 // surface emission of the registered tracers (timestep.cu)
 int emission_set(const float* const* emis);
 void launch_emission(Context& C, cudaStream_t s);
+// the emission's table of per-tracer tendency arrays, after those moved
+int emission_repoint(Context& C, cudaStream_t s);
 // forgets the scratch address of olamgpu_update_scalar_noalloc (finalize)
 void noalloc_forget();
 int tracers_to_device(cudaStream_t s);   // host -> per-tracer mirrors (-> Q)

@@ -341,6 +341,16 @@ int emission_set(const float* const* emis) {
   return OLAMGPU_OK;
 }
 
+int emission_repoint(Context& C, cudaStream_t s) {
+  Tracers& tr = C.tr;
+  if (!C.tp.have_emis || tr.n <= 0) return OLAMGPU_OK;
+  std::vector<float*> pt(tr.n);
+  for (int n = 0; n < tr.n; ++n) pt[n] = tr.t[n].p;
+  OG_CHECK(upload(g_emis_ptab, pt.data(), pt.size(), s));
+  OG_CUDA(cudaStreamSynchronize(s));   // the host vector dies here
+  return OLAMGPU_OK;
+}
+
 // the long step's device sequence (timestep.f90:66-319); without the
 // transport (with_transport false) the dynamics and the glue of thil only
 static int run_sequence(Context& C, unsigned flags, int nmass, const int* ids, bool with_transport = true) {

@@ -67,7 +67,10 @@ int tracers_to_device(cudaStream_t s) {
 
 static int pointer_table(std::vector<DevBuf<float>>& bufs, DevBuf<float*>& dst, cudaStream_t s) {
   std::vector<float*> h(bufs.size());
-  for (size_t i = 0; i < bufs.size(); ++i) h[i] = bufs[i].p;
+  for (size_t i = 0; i < bufs.size(); ++i) {
+    h[i] = bufs[i].p;
+    if (!h[i]) { set_error("a per-tracer device array is missing"); return OLAMGPU_E_STATE; }
+  }
   OG_CHECK(dst.alloc(std::max<size_t>(h.size(), 1)));
   if (!h.empty())
     OG_CUDA(cudaMemcpyAsync(dst.p, h.data(), h.size() * sizeof(float*), cudaMemcpyHostToDevice, s));

@@ -35,7 +35,7 @@ __global__ void k_adj_nonprog(const int* __restrict__ cols, int ncol, size_t col
   if (i >= (size_t)ncol * colsize) return;
   const size_t x = (size_t)cols[i / colsize] * colsize + i % colsize;
   const float v = lam[x];
-  lams[x] = 0.f;
+  if (lams) lams[x] = 0.f;   // (a window's sum keeps its zero there)
   if (final_is_other) { other[x] = v; lam[x] = 0.f; }
   else other[x] = 0.f;
 }
@@ -227,6 +227,7 @@ struct TileAdjArgs {
   const int* __restrict__ lpw;      // each W column's floor (device level)
   float dtr;
   int first, last;                  // first / last reverse stage of the step
+  int ls_first;                     // LS is written, not accumulated (the first stage, unless a window sums it)
   const int4* __restrict__ hdr;
   const int* __restrict__ ulist;
   const int* __restrict__ tc;
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   const int half = lane >> 4, hl = lane & 15;
   const bool act = 4 * hl < seg;
   const int cb = 2 * warp + half;
-  const bool first = A.first != 0, last = A.last != 0;
+  const bool first = A.first != 0, last = A.last != 0, lsfirst = A.ls_first != 0;
   int skm = 0;   // this lane's tracers whose results are written elsewhere
   if (A.skip)
     for (int j = 0; j < 4; ++j) {
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
       if (kb + 2 < mza) p2[n] = ldg4(q + (long long)(kb + 2) * ntp);
       if (kb + 3 < mza) p3[n] = ldg4(q + (long long)(kb + 3) * ntp);
       if (need0[n]) l0[n] = ldg4(A.L0 + cbase[n] + (long long)kb * ntp);
-      if (!first) ls[n] = ldg4(A.LS + cbase[n] + (long long)kb * ntp);
+      if (!lsfirst) ls[n] = ldg4(A.LS + cbase[n] + (long long)kb * ntp);
     }
   }
   cp_async_wait_all();
@@ -420,14 +421,15 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
           for (int k2 = 0; k2 < kd; ++k2) {
             const long long r2 = cbase[n] + (long long)k2 * ntp;
             stg4m(A.LIN + r2, zero4(), skm);
-            if (first) { stg4m(A.L0 + r2, zero4(), skm); stg4m(A.LS + r2, zero4(), skm); }
+            if (first) stg4m(A.L0 + r2, zero4(), skm);
+            if (lsfirst) stg4m(A.LS + r2, zero4(), skm);
           }
         // slide the column's window up one level and read ahead
         m2[n] = m1[n]; m1[n] = lx; p1[n] = p2[n]; p2[n] = p3[n];
         if (kd + 4 < mza) p3[n] = ldg4(A.L + cbase[n] + (long long)(kd + 4) * ntp);
         if (kd + 1 < mza) {
           if (need0[n]) l0[n] = ldg4(A.L0 + cbase[n] + (long long)(kd + 1) * ntp);
-          if (!first) ls[n] = ldg4(A.LS + cbase[n] + (long long)(kd + 1) * ntp);
+          if (!lsfirst) ls[n] = ldg4(A.LS + cbase[n] + (long long)(kd + 1) * ntp);
         }
       }
     }
@@ -453,14 +455,14 @@ static AdjTiles adj_tiles_of(const DevGrid& d) {
 }
 
 static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L, float* LIN, float* L0, float* LS,
-                           int ntp, int istage, int nrk, float dtr, int first, int last, int* status,
-                           cudaStream_t s, const int* skip = nullptr, int ntr = 0) {
+                           int ntp, int istage, int nrk, float dtr, int first, int last, int ls_first,
+                           int* status, cudaStream_t s, const int* skip = nullptr, int ntr = 0) {
   const AdjTiles t = adj_tiles_of(d);
   TileAdjArgs A;
   A.skip = skip; A.ntr = ntr;
   A.mza = d.mza; A.ntp = ntp; A.nrk = nrk; A.istage = istage; A.kb = 1; A.lpw = d.lpw.p;
   A.ntiles = t.ntiles; A.T = t.T; A.nu_max = t.nu_max; A.mwa = d.mwa;
-  A.dtr = dtr; A.first = first; A.last = last;
+  A.dtr = dtr; A.first = first; A.last = last; A.ls_first = ls_first;
   A.hdr = t.hdr;
   A.ulist = t.u; A.tc = t.tc; A.rev = t.rev;
   A.ff = tp.ff.p; A.trec = tp.adj_trec.p;
@@ -538,7 +540,7 @@ static int adjoint_checks(Context& C) {
   return OLAMGPU_OK;
 }
 
-int adjoint_core(Context& C, const float* rho_old_host) {
+int adjoint_core(Context& C, const float* rho_old_host, bool ls_acc) {
   Transport& tp = C.tp;
   cudaStream_t s = C.stream;
   // the adjoint's 32-column tiles, once per grid, when the stage kernel runs narrower ones
@@ -605,7 +607,7 @@ int adjoint_core(Context& C, const float* rho_old_host) {
   const size_t colsize = (size_t)mza * ntp;
   if (d.n_nonprog > 0) {
     k_adj_nonprog<<<cdiv((size_t)d.n_nonprog * colsize, 256), 256, 0, s>>>(d.w_nonprog.p, d.n_nonprog, colsize, L,
-                                                                          LIN, tp.adj_ls.p, fin);
+                                                                          LIN, ls_acc ? nullptr : tp.adj_ls.p, fin);
     OG_LAUNCHED();
   }
   for (int istage = nrk; istage >= 1; --istage) {
@@ -631,7 +633,7 @@ int adjoint_core(Context& C, const float* rho_old_host) {
     {
       OG_PROF("adj_stage", s);
       OG_CHECK(launch_tile_adj(d, tp, L, LIN, tp.adj_l0.p, tp.adj_ls.p, ntp, istage, nrk, dtr, first, last,
-                               C.status.p, s, pd_stage ? tp.d_mode.p + C.tr.n : nullptr, C.tr.n));
+                               first && !ls_acc, C.status.p, s, pd_stage ? tp.d_mode.p + C.tr.n : nullptr, C.tr.n));
     }
     std::swap(L, LIN);
   }

@@ -14,10 +14,20 @@
 // step's transport inputs (vmasc, wmasc, rho, rho_old: the winds and
 // densities scalar_transport_rk reads), then applies the one-step adjoint
 // (transport_adjoint.cu) to those steps in reverse order on the device.
+// A segment is reversed in parts of at most seg_steps steps when fewer
+// steps' inputs fit (each part runs the segment again from its checkpoint).
 // The adjoint of the tendencies is summed over the steps (the tendencies of
 // the window are one field: the registered tendencies, or the surface
 // emission, held for every step).  Afterwards the state after the window is
 // put back, so the model continues from where the forward ended.
+//
+// Memory.  The checkpoints and the state after the window live on the
+// device, or in page-locked host memory (olamgpu_window_memory).  With
+// unlimited transport the adjoint is lean: the tracers are in the state
+// after the window, so it borrows the three tracer rotation buffers and the
+// tendencies' buffer for its four lam buffers, and frees the per-tracer
+// device arrays (not read while the batched layout holds the tracers) for
+// its records and the steps' inputs, allocating them again at the end.
 #include <algorithm>
 
 #include "transport_kernels.cuh"
@@ -25,7 +35,7 @@
 namespace olamgpu {
 
 // the device buffers one long step hands to the next
-static std::vector<std::pair<void*, size_t>> carried_state(Context& C, bool tracers) {
+static std::vector<std::pair<void*, size_t>> carried_state(Context& C, bool tracers, bool qt = false) {
   Dyn& y = C.dy;
   Transport& tp = C.tp;
   std::vector<std::pair<void*, size_t>> v;
@@ -43,23 +53,79 @@ static std::vector<std::pair<void*, size_t>> carried_state(Context& C, bool trac
   add(y.div2d.p, y.div2d.bytes());
   add(y.vort2d.p, y.vort2d.bytes());
   if (tracers) add(C.tr.q[C.tr.qcur].p, C.tr.q[C.tr.qcur].bytes());
+  // the lean adjoint lends the tendencies' buffer out: the state after the
+  // window keeps it (it holds the last step's emission and diffusion)
+  if (qt) add(C.tr.qt.p, C.tr.qt.bytes());
   return v;
 }
 
-static size_t state_bytes(Context& C, bool tracers) {
+static size_t state_bytes(Context& C, bool tracers, bool qt = false) {
   size_t b = 0;
-  for (auto& f : carried_state(C, tracers)) b += (f.second + 255) & ~(size_t)255;
+  for (auto& f : carried_state(C, tracers, qt)) b += (f.second + 255) & ~(size_t)255;
   return b;
 }
 
-static int copy_state(Context& C, DevBuf<char>& blob, bool tracers, bool save) {
-  const size_t need = state_bytes(C, tracers);
-  if (save && blob.n != need) OG_CHECK(blob.alloc(need));
-  if (blob.n != need) { set_error("window: a checkpoint does not match the state"); return OLAMGPU_E_STATE; }
+static char* blob_ptr(Context& C, const StateBlob& b) {
+  return b.slot >= 0 ? C.winmem.pool[b.slot].p : b.dev.p;
+}
+static size_t blob_size(Context& C, const StateBlob& b) {
+  return b.slot >= 0 ? C.winmem.pool[b.slot].n : b.dev.n;
+}
+
+// MemAvailable of /proc/meminfo in bytes (0 when it cannot be read)
+static size_t host_available() {
+  FILE* f = fopen("/proc/meminfo", "r");
+  if (!f) return 0;
+  char line[256];
+  size_t kb = 0;
+  while (fgets(line, sizeof line, f))
+    if (sscanf(line, "MemAvailable: %zu kB", &kb) == 1) break;
+  fclose(f);
+  return kb * 1024;
+}
+
+// page-lock `add` more bytes of host memory only while they stay well inside
+// what the host has free
+static int host_guard(size_t add) {
+  const size_t avail = host_available();
+  if (avail && add > avail / 10 * 7) {
+    set_error("window: " + std::to_string(add >> 20) + " MiB of page-locked host memory asked for, " +
+              std::to_string(avail >> 20) + " MiB available");
+    return OLAMGPU_E_NOMEM;
+  }
+  return OLAMGPU_OK;
+}
+
+// the storage of one saved state: pool entry `slot` on the host, else the device
+static int blob_take(Context& C, StateBlob& b, int slot, size_t need) {
+  WindowMem& M = C.winmem;
+  if (!M.host) {
+    b.slot = -1;
+    return b.dev.alloc(need);
+  }
+  b.dev.release();
+  if ((int)M.pool.size() <= slot) M.pool.resize(slot + 1);
+  if (M.pool[slot].n != need) {
+    const size_t had = M.pool[slot].n;
+    M.pool[slot].release();
+    OG_CHECK(host_guard(need > had ? need - had : 0));
+    OG_CHECK(M.pool[slot].alloc(need));
+  }
+  b.slot = slot;
+  return OLAMGPU_OK;
+}
+
+static int copy_state(Context& C, const StateBlob& blob, bool tracers, bool qt, bool save) {
+  const size_t need = state_bytes(C, tracers, qt);
+  char* base = blob_ptr(C, blob);
+  if (!base || blob_size(C, blob) != need) {
+    set_error("window: a checkpoint does not match the state");
+    return OLAMGPU_E_STATE;
+  }
   size_t off = 0;
-  for (auto& f : carried_state(C, tracers)) {
-    char* b = blob.p + off;
-    OG_CUDA(cudaMemcpyAsync(save ? b : f.first, save ? f.first : b, f.second, cudaMemcpyDeviceToDevice, C.stream));
+  for (auto& f : carried_state(C, tracers, qt)) {
+    char* b = base + off;
+    OG_CUDA(cudaMemcpyAsync(save ? b : f.first, save ? f.first : b, f.second, cudaMemcpyDefault, C.stream));
     off += (f.second + 255) & ~(size_t)255;
   }
   return OLAMGPU_OK;
@@ -93,13 +159,58 @@ __global__ void k_accumulate(float* __restrict__ acc, const float* __restrict__ 
 
 void window_release() {
   Window& W = ctx().win;
-  for (auto& b : W.chk) b.release();
-  W.fin.release();
+  for (auto& b : W.chk) b.dev.release();
+  W.fin.dev.release();
   W.seg.release();
   W.lsacc.release();
   W.ptab.release();
   W.planes.release();
   W = Window();
+}
+
+void window_memory_release() {
+  WindowMem& M = ctx().winmem;
+  for (auto& h : M.pool) h.release();
+  M = WindowMem();
+}
+
+int window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk) {
+  Context& C = ctx();
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (segment_steps < 0 || nsteps < 0 || nchk < 0) {
+    set_error("window memory: segment_steps, nsteps and nchk must not be negative");
+    return OLAMGPU_E_ARG;
+  }
+  // a window taken before keeps its states where they were: it is dropped
+  window_release();
+  WindowMem& M = C.winmem;
+  if (!host_checkpoints) {
+    for (auto& h : M.pool) h.release();
+    M.pool.clear();
+  }
+  M.host = host_checkpoints != 0;
+  M.seg_steps = segment_steps;
+  if (!M.host || nsteps == 0 || nchk == 0) return OLAMGPU_OK;
+  // page-lock now the states a window of nsteps with a checkpoint every nchk will keep
+  if (!C.dy.press.p || !C.dy.div2d.p || C.tr.n <= 0) {
+    set_error("window memory: the state's device buffers exist after the first long step; reserve after it");
+    return OLAMGPU_E_STATE;
+  }
+  OG_CHECK(ensure_q(C.stream));
+  const bool tracers = C.opts.iscal_monot == 2;
+  const int nseg = (nsteps + nchk - 1) / nchk;
+  std::vector<size_t> need(nseg + 1, state_bytes(C, tracers));
+  need[0] = state_bytes(C, true, !tracers);
+  size_t add = 0, had = 0;
+  for (int i = 0; i <= nseg; ++i) add += need[i];
+  for (size_t i = 0; i < M.pool.size(); ++i) had += M.pool[i].n;
+  for (size_t i = nseg + 1; i < M.pool.size(); ++i) M.pool[i].release();
+  M.pool.resize(nseg + 1);
+  for (int i = 0; i <= nseg; ++i)
+    if (M.pool[i].n != need[i]) M.pool[i].release();
+  OG_CHECK(host_guard(add > had ? add - had : 0));
+  for (int i = 0; i <= nseg; ++i) OG_CHECK(M.pool[i].alloc(need[i]));
+  return OLAMGPU_OK;
 }
 
 int window_forward(int nsteps, int nchk, unsigned flags) {
@@ -122,6 +233,7 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
   // the limiter's adjoint is taken at the forward state: checkpoints and
   // the recomputed segments keep the tracers too
   W.tracers = C.opts.iscal_monot == 2;
+  W.lean = !W.tracers;
   const int nseg = (nsteps + nchk - 1) / nchk;
   W.chk.resize(nseg);
   W.chk_qcur.assign(nseg, 0);
@@ -134,7 +246,8 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
       // taken once they exist (tend0 does not read what it overwrites)
       if (step == 0 && (!C.dy.press.p || !C.dy.div2d.p)) OG_CHECK(dyn_tend0(nullptr));
       OG_CHECK(ensure_q(s));
-      OG_CHECK(copy_state(C, W.chk[g], W.tracers, true));
+      OG_CHECK(blob_take(C, W.chk[g], g + 1, state_bytes(C, W.tracers)));
+      OG_CHECK(copy_state(C, W.chk[g], W.tracers, false, true));
       W.chk_qcur[g] = C.tr.qcur;
       W.chk_div_first[g] = C.dy.div_first;
       W.chk_vort_first[g] = C.dy.vort_first;
@@ -142,7 +255,8 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
     OG_CHECK(glue_timestep(W.flags, 0, nullptr));
   }
   OG_CHECK(ensure_q(s));
-  OG_CHECK(copy_state(C, W.fin, true, true));
+  OG_CHECK(blob_take(C, W.fin, 0, state_bytes(C, true, W.lean)));
+  OG_CHECK(copy_state(C, W.fin, true, W.lean, true));
   W.fin_qcur = C.tr.qcur;
   W.fin_div_first = C.dy.div_first;
   W.fin_vort_first = C.dy.vort_first;
@@ -151,6 +265,114 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
   W.valid = true;
   return check_device_status();
 }
+
+// the steps [a, b) of checkpoint g's segment again from the checkpoint,
+// keeping the transport inputs (and with the limiter the tracers at the
+// start) of each into its slot of the segment buffer
+static int recompute(Context& C, int g, int a, int b, size_t sb) {
+  Window& W = C.win;
+  cudaStream_t s = C.stream;
+  OG_PROF("window_recompute", s);
+  const size_t qn = (size_t)C.g.mza * C.g.mwa * C.tr.ntp;
+  C.tr.qcur = W.chk_qcur[g];
+  // in the lean form the tracer buffers hold the adjoint: tend0 must not
+  // clear the tendencies' buffer, which holds the tendencies' adjoint
+  C.tr.q_valid = !W.lean;
+  OG_CHECK(copy_state(C, W.chk[g], W.tracers, false, false));
+  C.dy.div_first = W.chk_div_first[g];
+  C.dy.vort_first = W.chk_vort_first[g];
+  for (int step = g * W.nchk; step < b; ++step) {
+    char* slot = step >= a ? W.seg.p + sb * (size_t)(step - a) : nullptr;
+    if (slot && W.tracers)
+      OG_CUDA(cudaMemcpyAsync(slot + step_bytes(C), C.tr.q[C.tr.qcur].p, qn * sizeof(float),
+                              cudaMemcpyDeviceToDevice, s));
+    OG_CHECK(glue_run_sequence(C, W.flags, W.tracers));
+    if (slot) OG_CHECK(copy_step(C, slot, true));
+  }
+  return OLAMGPU_OK;
+}
+
+// the one-step adjoint of the steps b-1 down to a, from their saved inputs
+static int reverse(Context& C, int a, int b, size_t sb, bool& first) {
+  Window& W = C.win;
+  Transport& tp = C.tp;
+  cudaStream_t s = C.stream;
+  const size_t qn = (size_t)C.g.mza * C.g.mwa * C.tr.ntp;
+  for (int step = b - 1; step >= a; --step) {
+    char* slot = W.seg.p + sb * (size_t)(step - a);
+    OG_CHECK(copy_step(C, slot, false));
+    if (W.tracers)
+      OG_CUDA(cudaMemcpyAsync(C.tr.q[C.tr.qcur].p, slot + step_bytes(C), qn * sizeof(float),
+                              cudaMemcpyDeviceToDevice, s));
+    // the lean form sums the tendencies' adjoint in adj_ls itself
+    OG_CHECK(adjoint_core(C, nullptr, W.lean && !first));
+    if (C.opts.nrk_scal & 1) std::swap(tp.adj_l[0], tp.adj_l[1]);   // the step's result back into adj_l[0]
+    if (!W.lean) {
+      k_accumulate<<<cdiv(qn, 256), 256, 0, s>>>(W.lsacc.p, tp.adj_ls.p, qn, first ? 1 : 0);
+      OG_LAUNCHED();
+    }
+    first = false;
+  }
+  return OLAMGPU_OK;
+}
+
+static int planes_table(Window& W, int n, size_t pstride, cudaStream_t s) {
+  std::vector<float*> h(n);
+  for (int i = 0; i < n; ++i) h[i] = W.planes.p + (size_t)i * pstride;
+  OG_CHECK(W.ptab.alloc(n));
+  OG_CUDA(cudaMemcpyAsync(W.ptab.p, h.data(), n * sizeof(float*), cudaMemcpyHostToDevice, s));
+  OG_CUDA(cudaStreamSynchronize(s));   // h dies here
+  return OLAMGPU_OK;
+}
+
+// The lean adjoint's borrowed and freed memory, given back however the call
+// ends: the buffers it allocated are freed, the state after the window is
+// put back (on an error too, so the model state stays that of the window's
+// end), the borrowed views are dropped and the per-tracer device arrays are
+// allocated again (zero: the batched layout holds the tracers, and the
+// tendencies were cleared by the last step's tend0).  Recorded long steps
+// cleared the old per-tracer arrays: they are recorded again.
+struct LeanScope {
+  Context& C;
+  bool on = false;
+  bool fin_restored = false;
+  explicit LeanScope(Context& c) : C(c) {}
+  int finish() {
+    if (!on) return OLAMGPU_OK;
+    on = false;
+    Window& W = C.win;
+    Transport& tp = C.tp;
+    Tracers& tr = C.tr;
+    cudaStream_t s = C.stream;
+    W.seg.release();
+    W.planes.release();
+    tp.adj_trec.release();
+    int rc = OLAMGPU_OK;
+    if (!fin_restored) {
+      tr.qcur = W.fin_qcur;
+      rc = copy_state(C, W.fin, true, true, false);
+      C.dy.div_first = W.fin_div_first;
+      C.dy.vort_first = W.fin_vort_first;
+    }
+    tr.q_valid = true;
+    for (int b = 0; b < 2; ++b) tp.adj_l[b].release();
+    tp.adj_l0.release();
+    tp.adj_ls.release();
+    const size_t plane = (size_t)C.g.mza * C.g.mwa;
+    for (int n = 0; n < tr.n; ++n) {
+      int r = tr.p[n].alloc(plane);
+      if (r == OLAMGPU_OK) r = tr.t[n].alloc(plane);
+      if (r == OLAMGPU_OK && cudaMemsetAsync(tr.p[n].p, 0, plane * sizeof(float), s) != cudaSuccess) r = OLAMGPU_E_CUDA;
+      if (r == OLAMGPU_OK && cudaMemsetAsync(tr.t[n].p, 0, plane * sizeof(float), s) != cudaSuccess) r = OLAMGPU_E_CUDA;
+      if (r != OLAMGPU_OK && rc == OLAMGPU_OK) rc = r;
+    }
+    const int re = emission_repoint(C, s);
+    if (rc == OLAMGPU_OK) rc = re;
+    glue_drop_graphs();
+    return rc;
+  }
+  ~LeanScope() { finish(); }
+};
 
 int window_adjoint(float* const* lam, float* const* lam_sct) {
   Context& C = ctx();
@@ -164,79 +386,87 @@ int window_adjoint(float* const* lam, float* const* lam_sct) {
     if (!lam[i] || !lam_sct[i]) { set_error("a lam or lam_sct entry is NULL"); return OLAMGPU_E_ARG; }
   cudaStream_t s = C.stream;
   Transport& tp = C.tp;
+  Tracers& tr = C.tr;
   const DevGrid& d = C.g;
-  const int ntp = C.tr.ntp, nrk = C.opts.nrk_scal;
+  const int ntp = tr.ntp;
   const size_t plane = (size_t)d.mza * d.mwa, qn = plane * ntp;
   const size_t pstride = (plane + 3) & ~(size_t)3;
   // per step: the transport inputs, and with the limiter the tracers at the step's start
   const size_t qbytes = (qn * sizeof(float) + 255) & ~(size_t)255;
   const size_t sb = step_bytes(C) + (W.tracers ? qbytes : 0);
-  OG_CHECK(W.seg.alloc(sb * (size_t)W.nchk));
-  OG_CHECK(W.lsacc.alloc(qn));
-  OG_CHECK(W.planes.alloc(pstride * n));
-  {
-    std::vector<float*> h(n);
-    for (int i = 0; i < n; ++i) h[i] = W.planes.p + (size_t)i * pstride;
-    OG_CHECK(W.ptab.alloc(n));
-    OG_CUDA(cudaMemcpyAsync(W.ptab.p, h.data(), n * sizeof(float*), cudaMemcpyHostToDevice, s));
-    OG_CUDA(cudaStreamSynchronize(s));   // h dies here
+  const int part = C.winmem.seg_steps > 0 ? std::min(C.winmem.seg_steps, W.nchk) : W.nchk;
+  LeanScope lean(C);
+  if (W.lean) {
+    // the tracers are in the state after the window: their buffers hold the
+    // four lam arrays; the per-tracer arrays' memory goes to the records and
+    // the steps' inputs (a one-step adjoint's own buffers are freed first)
+    for (int b = 0; b < 3; ++b)
+      if (tr.q[b].n != qn || tr.qt.n != qn) { set_error("window adjoint: the tracer buffers are missing"); return OLAMGPU_E_STATE; }
+    for (int b = 0; b < 2; ++b) tp.adj_l[b].release();
+    tp.adj_l0.release();
+    tp.adj_ls.release();
+    tp.adj_planes.release();
+    tp.adj_trec.release();
+    OG_CUDA(cudaStreamSynchronize(s));
+    lean.on = true;
+    for (int i = 0; i < n; ++i) { tr.p[i].release(); tr.t[i].release(); }
+    tp.adj_l[0].borrow(tr.q[0].p, qn);
+    tp.adj_l[1].borrow(tr.q[1].p, qn);
+    tp.adj_l0.borrow(tr.q[2].p, qn);
+    tp.adj_ls.borrow(tr.qt.p, qn);
+  } else {
+    OG_CHECK(W.lsacc.alloc(qn));
+    OG_CHECK(tp.adj_l[0].alloc(qn));
   }
-  OG_CHECK(tp.adj_l[0].alloc(qn));
+  OG_CHECK(W.planes.alloc(pstride * n));
+  OG_CHECK(planes_table(W, n, pstride, s));
   for (int i = 0; i < n; ++i)
     OG_CUDA(cudaMemcpyAsync(W.planes.p + (size_t)i * pstride, lam[i], plane * sizeof(float), cudaMemcpyHostToDevice, s));
   {
     OG_PROF("window_adjoint", s);
     launch_gather_q(tp.adj_l[0].p, (const float* const*)W.ptab.p, n, ntp, plane, s);
+    if (W.lean) {
+      OG_CUDA(cudaStreamSynchronize(s));   // the planes' memory goes to the steps' inputs
+      W.planes.release();
+    }
+    OG_CHECK(W.seg.alloc(sb * (size_t)part));
     const int nseg = (int)W.chk.size();
     bool first = true;
     for (int g = nseg - 1; g >= 0; --g) {
       const int s0 = g * W.nchk, s1 = std::min(W.nsteps, s0 + W.nchk);
-      {
-        // the segment's steps again from its checkpoint, keeping their transport inputs
-        OG_PROF("window_recompute", s);
-        C.tr.qcur = W.chk_qcur[g];
-        C.tr.q_valid = true;
-        OG_CHECK(copy_state(C, W.chk[g], W.tracers, false));
-        C.dy.div_first = W.chk_div_first[g];
-        C.dy.vort_first = W.chk_vort_first[g];
-        for (int step = s0; step < s1; ++step) {
-          char* slot = W.seg.p + sb * (size_t)(step - s0);
-          if (W.tracers)
-            OG_CUDA(cudaMemcpyAsync(slot + step_bytes(C), C.tr.q[C.tr.qcur].p, qn * sizeof(float),
-                                    cudaMemcpyDeviceToDevice, s));
-          OG_CHECK(glue_run_sequence(C, W.flags, W.tracers));
-          OG_CHECK(copy_step(C, slot, true));
-        }
-      }
-      for (int step = s1 - 1; step >= s0; --step) {
-        char* slot = W.seg.p + sb * (size_t)(step - s0);
-        OG_CHECK(copy_step(C, slot, false));
-        if (W.tracers)
-          OG_CUDA(cudaMemcpyAsync(C.tr.q[C.tr.qcur].p, slot + step_bytes(C), qn * sizeof(float),
-                                  cudaMemcpyDeviceToDevice, s));
-        OG_CHECK(adjoint_core(C, nullptr));
-        if (nrk & 1) std::swap(tp.adj_l[0], tp.adj_l[1]);   // the step's result back into adj_l[0]
-        k_accumulate<<<cdiv(qn, 256), 256, 0, s>>>(W.lsacc.p, tp.adj_ls.p, qn, first ? 1 : 0);
-        OG_LAUNCHED();
-        first = false;
+      // the segment's parts from the last: [a, b) with a = s0 + a multiple of part
+      for (int b = s1; b > s0;) {
+        const int a = s0 + (b - 1 - s0) / part * part;
+        OG_CHECK(recompute(C, g, a, b, sb));
+        OG_CHECK(reverse(C, a, b, sb, first));
+        b = a;
       }
     }
-    // the model continues from the state after the window
-    C.tr.qcur = W.fin_qcur;
-    C.tr.q_valid = true;
-    OG_CHECK(copy_state(C, W.fin, true, false));
-    C.dy.div_first = W.fin_div_first;
-    C.dy.vort_first = W.fin_vort_first;
+    if (!W.lean) {
+      // the model continues from the state after the window
+      tr.qcur = W.fin_qcur;
+      tr.q_valid = true;
+      OG_CHECK(copy_state(C, W.fin, true, false, false));
+      C.dy.div_first = W.fin_div_first;
+      C.dy.vort_first = W.fin_vort_first;
+    } else {
+      W.seg.release();
+      tp.adj_trec.release();
+      OG_CHECK(W.planes.alloc(pstride * n));
+      OG_CHECK(planes_table(W, n, pstride, s));
+    }
     launch_scatter_q(tp.adj_l[0].p, W.ptab.p, n, ntp, plane, s);
   }
   for (int i = 0; i < n; ++i)
     OG_CUDA(cudaMemcpyAsync(lam[i], W.planes.p + (size_t)i * pstride, plane * sizeof(float), cudaMemcpyDeviceToHost, s));
   OG_CUDA(cudaStreamSynchronize(s));   // the planes are reused for the tendencies' adjoint
-  launch_scatter_q(W.lsacc.p, W.ptab.p, n, ntp, plane, s);
+  launch_scatter_q(W.lean ? tp.adj_ls.p : W.lsacc.p, W.ptab.p, n, ntp, plane, s);
   for (int i = 0; i < n; ++i)
     OG_CUDA(cudaMemcpyAsync(lam_sct[i], W.planes.p + (size_t)i * pstride, plane * sizeof(float),
                             cudaMemcpyDeviceToHost, s));
   OG_CUDA(cudaGetLastError());
+  OG_CUDA(cudaStreamSynchronize(s));
+  OG_CHECK(lean.finish());
   OG_CUDA(cudaStreamSynchronize(s));
   return check_device_status();
 }

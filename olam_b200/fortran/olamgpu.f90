@@ -176,6 +176,11 @@ module olamgpu_c
        type(c_ptr), intent(in) :: lam(*)
        type(c_ptr), intent(in) :: lam_sct(*)
      end function
+     integer(c_int) function olamgpu_window_memory(host_checkpoints, segment_steps, nsteps, nchk) &
+         bind(C, name="olamgpu_window_memory")
+       import :: c_int
+       integer(c_int), value :: host_checkpoints, segment_steps, nsteps, nchk
+     end function
      integer(c_int) function olamgpu_set_tile_shape(t, g, ks, ord) bind(C, name="olamgpu_set_tile_shape")
        import :: c_int
        integer(c_int), value :: t, g, ks, ord

@@ -30,7 +30,7 @@ EXPORTS = [
     "olamgpu_set_scalars_bottom", "olamgpu_diagvel_t3d", "olamgpu_tracer_maxmin", "olamgpu_mass_sums",
     "olamgpu_timestep", "olamgpu_timestep_diag", "olamgpu_set_halo",
     "olamgpu_set_surface_emission", "olamgpu_window_forward", "olamgpu_window_adjoint",
-    "olamgpu_set_tile_shape", "olamgpu_tile_shape",
+    "olamgpu_window_memory", "olamgpu_set_tile_shape", "olamgpu_tile_shape",
 ]
 
 
@@ -84,6 +84,7 @@ def load():
     lib.olamgpu_set_surface_emission.argtypes = [C.POINTER(abi.c_float_p)]
     lib.olamgpu_window_forward.argtypes = [C.c_int, C.c_int, C.c_uint]
     lib.olamgpu_window_adjoint.argtypes = [C.POINTER(abi.c_float_p), C.POINTER(abi.c_float_p)]
+    lib.olamgpu_window_memory.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
     lib.olamgpu_set_tile_shape.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
     lib.olamgpu_tile_shape.argtypes = [abi.c_int_p, C.c_int, abi.c_int_p, abi.c_float_p]
     for name in EXPORTS:
@@ -243,13 +244,32 @@ class OlamGpu:
     def window_forward(self, nsteps, nchk, flags=0):
         check(self.lib.olamgpu_window_forward(int(nsteps), int(nchk), int(flags)))
 
-    def window_adjoint(self, lam):
+    def window_adjoint(self, lam, lam_sct=None, in_place=False):
         """lam: list of (mwa, mza) float32 arrays of dJ/d(scalars after the
-        window); returns (dJ/d(scalars before it), dJ/d(tendencies))."""
-        lam_io = [np.array(x, dtype=np.float32, order="C", copy=True) for x in lam]
-        lsct = [np.zeros_like(x) for x in lam_io]
+        window); returns (dJ/d(scalars before it), dJ/d(tendencies)).  With
+        in_place the first result is written into lam's own (C-contiguous
+        float32) arrays, and lam_sct, when given, receives the second."""
+        if in_place:
+            for x in lam:
+                if x.dtype != np.float32 or not x.flags.c_contiguous:
+                    raise ValueError("in_place needs C-contiguous float32 arrays")
+            lam_io = list(lam)
+        else:
+            lam_io = [np.array(x, dtype=np.float32, order="C", copy=True) for x in lam]
+        lsct = lam_sct if lam_sct is not None else [np.zeros_like(x) for x in lam_io]
+        for x, y in zip(lam_io, lsct):
+            if y.shape != x.shape or y.dtype != np.float32 or not y.flags.c_contiguous:
+                raise ValueError("lam_sct arrays must match lam (C-contiguous float32)")
         check(self.lib.olamgpu_window_adjoint(abi.ptr_array(lam_io, C.c_float), abi.ptr_array(lsct, C.c_float)))
         return lam_io, lsct
+
+    def window_memory(self, host_checkpoints=False, segment_steps=0, nsteps=0, nchk=0):
+        """Where the next window keeps its states: page-locked host memory for
+        the checkpoints and the final state (reserved now for nsteps / nchk
+        when both are given), and how many steps' transport inputs the
+        adjoint holds at once (0: a whole segment)."""
+        check(self.lib.olamgpu_window_memory(int(bool(host_checkpoints)), int(segment_steps), int(nsteps),
+                                             int(nchk)))
 
     def timestep_diag(self, ntr, nmass=0):
         smax = np.zeros((ntr, 2), np.float32)

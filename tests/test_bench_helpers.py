@@ -49,3 +49,15 @@ def test_field_errors():
     assert abs(rms - 1e-3 / np.sqrt((ref[mask] ** 2).sum())) < 1e-15
     out[0, 0] += 5.0                               # outside the mask: ignored
     assert b.field_errors(out, ref, mask)[0] == mx
+
+
+def test_recomputed_steps():
+    b = bench()
+    # whole segments: every step once
+    assert b.recomputed_steps(24, 6, 0) == 24
+    assert b.recomputed_steps(24, 6, 6) == 24
+    assert b.recomputed_steps(5, 2, 0) == 5
+    # a checkpoint every 12 steps, parts of 4: 12 + 8 + 4 per segment
+    assert b.recomputed_steps(24, 12, 4) == 2 * (12 + 8 + 4)
+    # a ragged last segment and part: segments [0, 3), [3, 5); parts of 1
+    assert b.recomputed_steps(5, 3, 1) == (3 + 2 + 1) + (2 + 1)

@@ -187,6 +187,49 @@ def test_window_gradient_against_fp64_oracle_and_differences(window_runs):
         assert abs(fd - dot32) <= 1e-5 * abs(fd), (fd, dot32)
 
 
+def test_window_host_checkpoints_and_parts(window_runs):
+    """The window with its checkpoints and final state in page-locked host
+    memory, a checkpoint every 3 steps and the adjoint holding one step's
+    inputs at a time (each step of a segment from its checkpoint again):
+    the same gradients, bit for bit, as device checkpoints every 2 steps
+    reversed a segment at a time.  Then the model goes on: one more long
+    step (recorded again, the per-tracer arrays allocated anew) equals the
+    window's own run continued by one step."""
+    r = window_runs
+    g, ds, tr, emis = case()
+    dev, hs, var_p = new_device(g, ds, tr, emis, r["opts"])
+    try:
+        with pytest.raises(Exception):
+            dev.window_memory(True, 1, NSTEPS, 3)      # no long step yet: sizes unknown
+        dev.window_memory(True, 1)                      # host memory taken by the window itself
+        dev.window_forward(NSTEPS, 3, abi.TS_GRAPH)
+        lam = [x.copy() for x in r["lam"]]
+        g0, gs = dev.window_adjoint(lam, in_place=True)
+        assert g0[0] is lam[0]
+        dev.sync_to_host(abi.F_SCALARS)
+        restored = [t.copy() for t in var_p]
+        dev.timestep(abi.TS_GRAPH)
+        dev.sync_to_host(abi.F_SCALARS)
+        next_step = [t.copy() for t in var_p]
+        dev.window_memory(True, 0, NSTEPS, 3)          # sizes known now: reserved at once
+    finally:
+        dev.close()
+    for n in range(NTR):
+        assert np.array_equal(g0[n], r["g0"][n]), n
+        assert np.array_equal(gs[n], r["gs"][n]), n
+        assert np.array_equal(restored[n], r["after"][n]), n
+    dev, hs, var_p = new_device(g, ds, tr, emis, r["opts"])
+    try:
+        for _ in range(NSTEPS + 1):
+            dev.timestep(0)
+        dev.sync_to_host(abi.F_SCALARS)
+        ref = [t.copy() for t in var_p]
+    finally:
+        dev.close()
+    for n in range(NTR):
+        assert np.array_equal(next_step[n], ref[n]), n
+
+
 def test_surface_emission_adds_mass():
     g, ds, tr, emis = case()
     opts = abi.make_opts(DT, nacoust=4, nrk_scal=2)
