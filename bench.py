@@ -82,7 +82,7 @@ def parse():
     p.add_argument("--large", action="store_true",
                    help="only the large combined run (NXP=400, 80 levels, 32 tracers, 24 long steps of 60 s)")
     p.add_argument("--large-nxp", type=int, default=400)
-    p.add_argument("--large-chk", type=int, default=12,
+    p.add_argument("--large-chk", type=int, default=8,
                    help="large run: a checkpoint every this many steps (kept in page-locked host memory)")
     p.add_argument("--large-seg", type=int, default=4,
                    help="large run: the adjoint holds this many steps' transport inputs at once")
