@@ -255,31 +255,39 @@ __device__ __forceinline__ void stg4m(float* p, F4 v, int mask) {
   if (!(mask & 8)) p[3] = v.b.y;
 }
 
-size_t tile_adj_smem_bytes(int T, int nu) {
+// G tracers per block: a U row of the tile's neighbourhood is 4 G bytes
+size_t tile_adj_smem_bytes(int T, int nu, int G = 64) {
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  return 2 * al((size_t)nu * 256) + 2 * al((size_t)T * TADJ_RW * 4) + al((size_t)nu * 8) +
+  return 2 * al((size_t)nu * 4 * G) + 2 * al((size_t)T * TADJ_RW * 4) + al((size_t)nu * 8) +
          al((size_t)T * TILE_NS * 4) + 2 * al((size_t)T * 4);
 }
 
 // The same sweep as k_tile: level kd+1 is copied into one buffer while kd is
-// computed from the other; a half warp owns NC columns with lam of the
-// column's levels kd-2 .. kd+3 and its lam0 / lams rows in registers.
+// computed from the other; G / 4 lanes own NC columns (four tracers a lane,
+// G tracers a block: 64, or 32 so that 32 tracers leave no lane idle) with
+// lam of the column's levels kd-2 .. kd+3 and its lam0 / lams rows in
+// registers.
 //   lam_in(x) = dtr (sum_e T_e lam(c_e) + sum_q (fexpl a_q + [q == 2] d) lam(kd-2+q))
 //   lam0 += lam (1 - dtr (b26 + fexpl b27)),  lams += lam dtr / rhos
 // On the first reverse stage lam0 is read only in implicit columns (the
 // implicit transpose wrote it there) and lams is not read; on the last the
 // result lam_in + lam0 is the adjoint of the old scp, written to LIN.
-template <int NC>
+template <int NC, int G>
 __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int T = 16 * NC;
-  const int ngrp = (A.ntp + 63) >> 6;   // the tracer groups of a tile side by side
+  constexpr int LPC = G / 4;                        // lanes per column
+  constexpr int CPW = 32 / LPC;                     // columns per warp
+  constexpr int NG = CPW * (TADJ_THREADS / 32);     // column groups of a block
+  constexpr int T = NG * NC;
+  constexpr int RB = 4 * G;                         // bytes of a staged U row
+  static_assert(G == 32 || G == 64, "32 or 64 tracers per block");
+  const int ngrp = (A.ntp + G - 1) / G;   // the tracer groups of a tile side by side
   const int tile = blockIdx.x / ngrp, grp = blockIdx.x - tile * ngrp;
   const int4 h = A.hdr[tile];
   const int u_off = h.x, nU = h.y, nT = h.w;
   const int mza = A.mza, ntp = A.ntp, kb = A.kb;
   auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
-  const size_t ubuf = al((size_t)A.nu_max * 256), rbuf = al((size_t)T * TADJ_RW * 4);
+  const size_t ubuf = al((size_t)A.nu_max * RB), rbuf = al((size_t)T * TADJ_RW * 4);
   unsigned char* p = smraw;
   char* UB = reinterpret_cast<char*>(p);              p += 2 * ubuf;
   unsigned char* RBB = p;                             p += 2 * rbuf;
@@ -288,14 +296,14 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   int* IWT = reinterpret_cast<int*>(p);               p += al((size_t)T * 4);
   float* FEX = reinterpret_cast<float*>(p);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int t0 = grp * 64;
+  const int t0 = grp * G;
 
   int bad = (nU > A.nu_max || nT > T || nT > nU || A.T != T) ? 1 : 0;
   if (!bad) {
     for (int i = tid; i < nT * TILE_NS; i += TADJ_THREADS) {
       const int v = __ldg(A.rev + (size_t)tile * T * TILE_NS + i);
       if ((unsigned)(v >> 8) >= (unsigned)nU || (v & 255) > TILE_NS) bad = 11;
-      REVO[i] = (v >> 8) * 256;
+      REVO[i] = (v >> 8) * RB;
     }
     for (int i = tid; i < nT; i += TADJ_THREADS) {
       const int v = __ldg(A.tc + ((size_t)tile * T + i) * TILE_TCW + TILE_TC_IW);
@@ -314,15 +322,15 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   }
   for (int i = tid; i < nT; i += TADJ_THREADS) FEX[i] = 1.0f - __ldg(A.ff + (size_t)IWT[i] * A.nrk + A.istage - 1);
 
-  const int seg = min(64, ntp - t0);
+  const int seg = min(G, ntp - t0);
   const int nch = seg >> 2;
-  const int ch = tid & 15;
+  const int ch = tid & (LPC - 1);
   auto stage = [&](int k, int b) {
     char* Ub = UB + b * ubuf;
     float* Rb = reinterpret_cast<float*>(RBB + b * rbuf);
     const long long koff = (long long)k * ntp + ch * 4;
     if (ch < nch)
-      for (int r = tid >> 4; r < nU; r += TADJ_THREADS / 16) cp_async16(Ub + r * 256 + ch * 16, A.L + ROW[r] + koff);
+      for (int r = tid / LPC; r < nU; r += TADJ_THREADS / LPC) cp_async16(Ub + r * RB + ch * 16, A.L + ROW[r] + koff);
     for (int i = tid; i < nT * (TADJ_RW / 4); i += TADJ_THREADS) {
       const int c = i / (TADJ_RW / 4), q = i - c * (TADJ_RW / 4);
       cp_async16(Rb + c * TADJ_RW + q * 4, A.trec + ((size_t)IWT[c] * mza + k) * TADJ_RW + q * 4);
@@ -330,9 +338,9 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
     cp_async_commit();
   };
 
-  const int half = lane >> 4, hl = lane & 15;
+  const int sub = lane / LPC, hl = lane % LPC;
   const bool act = 4 * hl < seg;
-  const int cb = 2 * warp + half;
+  const int cb = CPW * warp + sub;
   const bool first = A.first != 0, last = A.last != 0, lsfirst = A.ls_first != 0;
   int skm = 0;   // this lane's tracers whose results are written elsewhere
   if (A.skip)
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
   __syncthreads();   // FEX
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
-    const int c = cb + 16 * n;
+    const int c = cb + NG * n;
     m2[n] = m1[n] = p1[n] = p2[n] = p3[n] = l0[n] = ls[n] = zero4();
     cbase[n] = 0;
     need0[n] = false;
@@ -375,11 +383,11 @@ __global__ void __launch_bounds__(TADJ_THREADS, 2) k_tile_adj(TileAdjArgs A) {
     const float* Rc = reinterpret_cast<const float*>(RBB + cur * rbuf);
 #pragma unroll
     for (int n = 0; n < NC; ++n) {
-      const int c = cb + 16 * n;
+      const int c = cb + NG * n;
       if (c >= nT) continue;
       if (kd == kbc[n]) m2[n] = m1[n] = zero4();
       const float* rc = Rc + c * TADJ_RW;
-      const F4 lx = lds4(Ul, c * 256);
+      const F4 lx = lds4(Ul, c * RB);
       F4 acc = zero4();
       const int* ro = REVO + c * TILE_NS;
 #pragma unroll
@@ -468,14 +476,20 @@ static int launch_tile_adj(const DevGrid& d, const Transport& tp, const float* L
   A.ff = tp.ff.p; A.trec = tp.adj_trec.p;
   A.L = L; A.LIN = LIN; A.L0 = L0; A.LS = LS;
   A.err = status;
-  const size_t smem = tile_adj_smem_bytes(t.T, t.nu_max);
-  const unsigned nblk = (unsigned)t.ntiles * (unsigned)((ntp + 63) / 64);
-  if (t.T == 32) {
-    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile_adj<2><<<nblk, TADJ_THREADS, smem, s>>>(A);
+  // 32 tracers or fewer on 32-column tiles: 8 lanes a column, 32 tracers a
+  // block (a 64-tracer block would leave half its lanes idle)
+  const int G = (t.T == 32 && ntp <= 32) ? 32 : 64;
+  const size_t smem = tile_adj_smem_bytes(t.T, t.nu_max, G);
+  const unsigned nblk = (unsigned)t.ntiles * (unsigned)((ntp + G - 1) / G);
+  if (G == 32) {
+    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<1, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tile_adj<1, 32><<<nblk, TADJ_THREADS, smem, s>>>(A);
+  } else if (t.T == 32) {
+    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<2, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tile_adj<2, 64><<<nblk, TADJ_THREADS, smem, s>>>(A);
   } else {
-    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tile_adj<1><<<nblk, TADJ_THREADS, smem, s>>>(A);
+    OG_CUDA(cudaFuncSetAttribute(k_tile_adj<1, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tile_adj<1, 64><<<nblk, TADJ_THREADS, smem, s>>>(A);
   }
   OG_LAUNCHED();
   return OLAMGPU_OK;

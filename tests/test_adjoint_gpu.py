@@ -66,7 +66,7 @@ def test_adjoint_matches_oracle_implicit_columns():
         _adjoint_vs_oracle(g, st, opts, 4)
 
 
-@pytest.mark.parametrize("ntr", [5, 70])
+@pytest.mark.parametrize("ntr", [5, 32, 36, 70])
 def test_adjoint_matches_oracle_ragged_tracer_groups(ntr):
     # 5: one partial group of 64 tracers (ntp = 8); 70: a full and a ragged group
     g, st = small_case(nxp=5, nlev=10, ntr=ntr, seed=4)
