@@ -79,6 +79,9 @@ def parse():
     p.add_argument("--win-steps", type=int, default=24)
     p.add_argument("--win-chk", type=int, default=6)
     p.add_argument("--win-monot", type=int, default=0)
+    p.add_argument("--win-fd", type=int, default=0,
+                   help="window: check the gradient against central differences of the device forward "
+                        "along this many seeded directions of the initial tracers and the emission")
     p.add_argument("--large", action="store_true",
                    help="only the large combined run (NXP=400, 80 levels, 32 tracers, 24 long steps of 60 s)")
     p.add_argument("--large-nxp", type=int, default=400)
@@ -481,6 +484,48 @@ def shape_sweep(g, st, tr, a):
     return out
 
 
+def window_differences(a, g, dev, var_p, tr, emis, lam, g0, gs, h=0.5):
+    """Central differences of the loss along a.win_fd seeded directions
+    (dx: standard normal times each tracer, de: standard normal times each
+    emission): the window's long steps run again on the device from its
+    start (olamgpu_window_rewind: the same dynamics, so the same winds) at
+    x0 +- h dx, E +- h de, and (J+ - J-) / 2h is set against
+    <dJ/dx0, dx> + <dJ/dE, de> from the adjoint.  The unlimited step is
+    linear in (x0, E) for the fixed winds, so the difference has no
+    truncation error: what remains is FP32 rounding of the two runs."""
+    from olam_b200 import abi
+    rng = np.random.default_rng(47)
+    lpw0 = g.lpw - 1
+    cols = np.arange(g.mwa)
+
+    def loss(x, e):
+        dev.window_rewind()
+        for t, v in zip(var_p, x):
+            t[...] = v
+        dev.sync_to_device(abi.F_SCALARS)
+        dev.set_surface_emission(e)
+        for _ in range(a.win_steps):
+            dev.timestep(abi.TS_GRAPH)
+        dev.sync_to_host(abi.F_SCALARS)
+        return sum(float((lam[n].astype(np.float64) * var_p[n]).sum()) for n in range(len(var_p)))
+
+    errs = []
+    for _ in range(a.win_fd):
+        dx = [(rng.standard_normal(t.shape) * t).astype(np.float32) for t in tr]
+        de = [(rng.standard_normal(e.shape) * e).astype(np.float32) for e in emis]
+        for d in dx:
+            d[0] = 0.0
+        jp = loss([t + h * d for t, d in zip(tr, dx)], [e + h * d for e, d in zip(emis, de)])
+        jm = loss([t - h * d for t, d in zip(tr, dx)], [e - h * d for e, d in zip(emis, de)])
+        fd = (jp - jm) / (2 * h)
+        dot = sum(float((g0[n].astype(np.float64) * dx[n]).sum())
+                  + float((gs[n][cols, lpw0].astype(np.float64) * de[n]).sum()) for n in range(len(tr)))
+        errs.append(abs(fd - dot) / abs(fd) if fd else abs(dot))
+    dev.set_surface_emission(emis)
+    return {"directions": a.win_fd, "h": h, "max_relerr": max(errs), "median_relerr": float(np.median(errs)),
+            "forward": "the device's FP32 long steps (the same winds every run: the tracers are passive)"}
+
+
 def bench_window(a, max_over_ranks):
     """The adjoint of tracer transport over a window of long steps: NXP=100
     (100,002 columns), 60 levels, 32 FP32 tracers with a seeded surface
@@ -490,7 +535,8 @@ def bench_window(a, max_over_ranks):
     cells in the lowest 3 levels.  Device time of olamgpu_window_forward
     (the 24 steps and their checkpoints) and of olamgpu_window_adjoint
     (per segment: the checkpoint restored, the dynamics run again, the
-    one-step adjoints in reverse).  The unlimited step is linear in the
+    one-step adjoints in reverse), the second call on the same window (the
+    first also allocates the adjoint's buffers; its time is reported too).  The unlimited step is linear in the
     tracers and emissions for fixed winds, so J = <dJ/dx0, x0> + <dJ/dE, E>
     exactly: a size-independent check of the gradient at full size."""
     import torch
@@ -552,8 +598,13 @@ def bench_window(a, max_over_ranks):
         for n in range(a.win_ntr):
             np.add.at(lam[n], (iw, kk), w[n].astype(np.float32))
             J += float((lam[n].astype(np.float64) * var_p[n]).sum())
-        dev.profile(True, reset=True)
         mem["after_forward"] = used_gb()
+        # the first adjoint call also allocates its buffers; the second, of
+        # the same window, is the steady state an inversion's iterations see
+        dev.profile(True, reset=True)
+        dev.window_adjoint(lam)
+        first_ms = max_over_ranks(dev.profile_read()["window_adjoint"][0])
+        dev.profile(True, reset=True)
         g0, gs = dev.window_adjoint(lam)
         mem["after_adjoint"] = used_gb()
         prof = dev.profile_read()
@@ -564,8 +615,11 @@ def bench_window(a, max_over_ranks):
         for n in range(a.win_ntr):
             lin += float((g0[n].astype(np.float64) * np.asarray(tr[n], np.float64)).sum())
             lin += float((gs[n][np.arange(g.mwa), lpw0].astype(np.float64) * emis[n]).sum())
+        if a.win_fd > 0 and a.win_monot == 0:
+            out["central_differences"] = window_differences(a, g, dev, var_p, tr, emis, lam, g0, gs)
         out.update({
             "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+            "adjoint_first_call_ms": first_ms,
             "recompute_ms": prof.get("window_recompute", (0.0, 0))[0],
             "adjoint_steps_ms": prof.get("adj_stage", (0.0, 0))[0] + prof.get("adj_records", (0.0, 0))[0]
             + prof.get("adj_implicit", (0.0, 0))[0],

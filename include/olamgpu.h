@@ -434,26 +434,43 @@ int olamgpu_window_forward(int nsteps, int nchk, unsigned flags);
  * The state after the window is restored at the end.  Device memory: one
  * checkpoint per segment (unless olamgpu_window_memory puts them in host
  * memory) plus the transport inputs of the steps reversed at once (nchk, or
- * olamgpu_window_memory's segment_steps).  With unlimited transport the
- * adjoint's four lam arrays occupy the tracer buffers (the tracers are in
- * the state after the window) and the per-tracer device arrays are freed
- * during the call and allocated again at its end, so a recorded long step
- * is recorded again on the next olamgpu_timestep.  No counterpart in OLAM. */
+ * olamgpu_window_memory's segment_steps) and the adjoint's buffers (or,
+ * lean, none of its own: see olamgpu_window_memory).  No counterpart in
+ * OLAM. */
 int olamgpu_window_adjoint(float* const* lam, float* const* lam_sct);
 
-/* Where the next window keeps its states.  host_checkpoints != 0: the
- * checkpoints and the state after the window in page-locked host memory
- * (device copies over PCIe when they are taken and restored), so that the
- * device holds only the model and the adjoint's working set; with nsteps and
- * nchk > 0 the host memory for such a window is page-locked now (after the
- * first long step, whose buffers fix the sizes), else by
- * olamgpu_window_forward.  A request above 70 % of the host's available
- * memory fails with OLAMGPU_E_NOMEM.  segment_steps > 0: the adjoint holds
- * the transport inputs of at most that many steps at once, running a
- * segment again from its checkpoint for each part of it (more recomputation,
- * less device memory); 0: a whole segment.  Drops a window taken before.
- * No counterpart in OLAM. */
-int olamgpu_window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk);
+/* Where the next window keeps its states, and how its adjoint uses the
+ * device.  OLAMGPU_WIN_HOST in `flags`: the checkpoints and the state after
+ * the window in page-locked host memory (device copies over PCIe when they
+ * are taken and restored), so that the device holds only the model and the
+ * adjoint's working set; with nsteps and nchk > 0 the host memory for such
+ * a window is page-locked now (after the first long step, whose buffers fix
+ * the sizes), else by olamgpu_window_forward.  A request above 70 % of the
+ * host's available memory fails with OLAMGPU_E_NOMEM.  With unlimited
+ * transport the adjoint is lean when the device has no room for its own
+ * buffers: its four lam arrays occupy the tracer buffers (the tracers are in
+ * the state after the window) and the per-tracer device arrays are freed
+ * during the call and allocated again at its end, so a recorded long step is
+ * recorded again on the next olamgpu_timestep; OLAMGPU_WIN_LEAN makes it
+ * lean always.  segment_steps > 0: the adjoint holds the transport inputs of
+ * at most that many steps at once, running a segment again from its
+ * checkpoint for each part of it (more recomputation, less device memory);
+ * 0: a whole segment.  Drops a window taken before.  No counterpart in
+ * OLAM. */
+enum {
+  OLAMGPU_WIN_HOST = 1,           /* checkpoints in page-locked host memory          */
+  OLAMGPU_WIN_LEAN = 2            /* the lean adjoint even when the device has room  */
+};
+int olamgpu_window_memory(int flags, int segment_steps, int nsteps, int nchk);
+
+/* Put the state at the start of the last window back on the device (its
+ * first checkpoint: the dynamics and the damping's saved planes, and with
+ * the limiter the tracers), so that the same window can run again from the
+ * same start -- the next iteration of an inversion with new initial
+ * tracers or sources.  An unlimited window's checkpoints hold no tracers:
+ * send the new ones after the rewind (olamgpu_sync_to_device with
+ * OLAMGPU_F_SCALARS).  The window stays valid.  No counterpart in OLAM. */
+int olamgpu_window_rewind(void);
 
 /* One explicit RK stage of update_scalar (scalar_transport_rk.F90:389-615:
  * grad_t2d[_quadratic], scalar_v_column, scalar_w_column; every column

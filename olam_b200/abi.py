@@ -179,6 +179,7 @@ def _halo_struct(ranks, rk, ns, nr, sc, rc, hook, host_staged, vm):
 
 # olamgpu_timestep flags
 TS_GRAPH, TS_HORIZ_K, TS_MAXMIN, TS_MASS = 1, 2, 4, 8
+WIN_HOST, WIN_LEAN = 1, 2
 
 
 class Eddy(C.Structure):

@@ -549,9 +549,11 @@ int olamgpu_window_forward(int nsteps, int nchk, unsigned flags) { return window
 
 int olamgpu_window_adjoint(float* const* lam, float* const* lam_sct) { return window_adjoint(lam, lam_sct); }
 
-int olamgpu_window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk) {
-  return window_memory(host_checkpoints, segment_steps, nsteps, nchk);
+int olamgpu_window_memory(int flags, int segment_steps, int nsteps, int nchk) {
+  return window_memory(flags, segment_steps, nsteps, nchk);
 }
+
+int olamgpu_window_rewind(void) { return window_rewind(); }
 
 void* olamgpu_stream(void) { return (void*)ctx().stream; }
 

@@ -429,7 +429,8 @@ struct StateBlob {                   // one saved state, on the device or in pag
 struct Window {
   bool valid = false;
   bool tracers = false;              // checkpoints hold the tracers (limited transport)
-  bool lean = false;                 // the adjoint borrows the tracer buffers (unlimited transport)
+  bool lean_ok = false;              // unlimited transport: the adjoint may borrow the tracer buffers
+  bool lean = false;                 // this adjoint call does
   int nsteps = 0, nchk = 0;
   unsigned flags = 0;
   std::vector<StateBlob> chk;
@@ -448,6 +449,7 @@ struct Window {
 // across windows so that the host memory is page-locked once
 struct WindowMem {
   bool host = false;                 // checkpoints and the final state in page-locked host memory
+  bool lean_always = false;          // the lean adjoint even when the device has room for its own buffers
   int seg_steps = 0;                 // steps whose transport inputs the adjoint holds at once (0: nchk)
   std::vector<HostBuf> pool;         // the final state, then checkpoints 0 .. nseg-1
 };
@@ -564,7 +566,8 @@ int glue_run_sequence(Context& C, unsigned flags, bool with_transport);
 int window_forward(int nsteps, int nchk, unsigned flags);
 int window_adjoint(float* const* lam, float* const* lam_sct);
 void window_release();
-int window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk);
+int window_memory(int flags, int segment_steps, int nsteps, int nchk);
+int window_rewind();
 void window_memory_release();
 // surface emission of the registered tracers (timestep.cu)
 int emission_set(const float* const* emis);

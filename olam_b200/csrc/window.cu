@@ -23,11 +23,13 @@
 //
 // Memory.  The checkpoints and the state after the window live on the
 // device, or in page-locked host memory (olamgpu_window_memory).  With
-// unlimited transport the adjoint is lean: the tracers are in the state
-// after the window, so it borrows the three tracer rotation buffers and the
-// tendencies' buffer for its four lam buffers, and frees the per-tracer
-// device arrays (not read while the batched layout holds the tracers) for
-// its records and the steps' inputs, allocating them again at the end.
+// unlimited transport, when the device has no room for the adjoint's own
+// buffers (or when asked), the adjoint is lean: the tracers are in the
+// state after the window, so it borrows the three tracer rotation buffers
+// and the tendencies' buffer for its four lam buffers, and frees the
+// per-tracer device arrays (not read while the batched layout holds the
+// tracers) for its records and the steps' inputs, allocating them again at
+// the end.
 #include <algorithm>
 
 #include "transport_kernels.cuh"
@@ -174,7 +176,7 @@ void window_memory_release() {
   M = WindowMem();
 }
 
-int window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk) {
+int window_memory(int flags, int segment_steps, int nsteps, int nchk) {
   Context& C = ctx();
   if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
   if (segment_steps < 0 || nsteps < 0 || nchk < 0) {
@@ -184,11 +186,12 @@ int window_memory(int host_checkpoints, int segment_steps, int nsteps, int nchk)
   // a window taken before keeps its states where they were: it is dropped
   window_release();
   WindowMem& M = C.winmem;
-  if (!host_checkpoints) {
+  if (!(flags & OLAMGPU_WIN_HOST)) {
     for (auto& h : M.pool) h.release();
     M.pool.clear();
   }
-  M.host = host_checkpoints != 0;
+  M.host = (flags & OLAMGPU_WIN_HOST) != 0;
+  M.lean_always = (flags & OLAMGPU_WIN_LEAN) != 0;
   M.seg_steps = segment_steps;
   if (!M.host || nsteps == 0 || nchk == 0) return OLAMGPU_OK;
   // page-lock now the states a window of nsteps with a checkpoint every nchk will keep
@@ -233,7 +236,7 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
   // the limiter's adjoint is taken at the forward state: checkpoints and
   // the recomputed segments keep the tracers too
   W.tracers = C.opts.iscal_monot == 2;
-  W.lean = !W.tracers;
+  W.lean_ok = !W.tracers;
   const int nseg = (nsteps + nchk - 1) / nchk;
   W.chk.resize(nseg);
   W.chk_qcur.assign(nseg, 0);
@@ -255,14 +258,32 @@ int window_forward(int nsteps, int nchk, unsigned flags) {
     OG_CHECK(glue_timestep(W.flags, 0, nullptr));
   }
   OG_CHECK(ensure_q(s));
-  OG_CHECK(blob_take(C, W.fin, 0, state_bytes(C, true, W.lean)));
-  OG_CHECK(copy_state(C, W.fin, true, W.lean, true));
+  OG_CHECK(blob_take(C, W.fin, 0, state_bytes(C, true, W.lean_ok)));
+  OG_CHECK(copy_state(C, W.fin, true, W.lean_ok, true));
   W.fin_qcur = C.tr.qcur;
   W.fin_div_first = C.dy.div_first;
   W.fin_vort_first = C.dy.vort_first;
   OG_CUDA(cudaGetLastError());
   OG_CUDA(cudaStreamSynchronize(s));
   W.valid = true;
+  return check_device_status();
+}
+
+int window_rewind() {
+  Context& C = ctx();
+  Window& W = C.win;
+  if (!C.initialised) { set_error("olamgpu_init has not been called"); return OLAMGPU_E_STATE; }
+  if (!W.valid || W.chk.empty()) { set_error("window rewind: no window has run"); return OLAMGPU_E_STATE; }
+  // an unlimited window's checkpoints hold no tracers: those on the device
+  // stay until the caller sends the new ones
+  if (W.tracers) {
+    C.tr.qcur = W.chk_qcur[0];
+    C.tr.q_valid = true;
+  }
+  OG_CHECK(copy_state(C, W.chk[0], W.tracers, false, false));
+  C.dy.div_first = W.chk_div_first[0];
+  C.dy.vort_first = W.chk_vort_first[0];
+  OG_CUDA(cudaStreamSynchronize(C.stream));
   return check_device_status();
 }
 
@@ -395,6 +416,20 @@ int window_adjoint(float* const* lam, float* const* lam_sct) {
   const size_t qbytes = (qn * sizeof(float) + 255) & ~(size_t)255;
   const size_t sb = step_bytes(C) + (W.tracers ? qbytes : 0);
   const int part = C.winmem.seg_steps > 0 ? std::min(C.winmem.seg_steps, W.nchk) : W.nchk;
+  // lean when the device has no room for the adjoint's own buffers: four
+  // lam arrays, the tendencies' sum, the transposed records, the host
+  // transfer planes and the steps' inputs (with 2 GiB to spare)
+  W.lean = W.lean_ok && C.winmem.lean_always;
+  if (W.lean_ok && !W.lean) {
+    size_t fr = 0, tot = 0;
+    OG_CUDA(cudaMemGetInfo(&fr, &tot));
+    auto missing = [](const DevBuf<float>& b, size_t n) { return b.n == n ? (size_t)0 : n * sizeof(float); };
+    const size_t need = missing(tp.adj_l[0], qn) + missing(tp.adj_l[1], qn) + missing(tp.adj_ls, qn) +
+                        (tp.adj_l0.n >= qn ? 0 : qn * sizeof(float)) + qn * sizeof(float) +
+                        missing(tp.adj_trec, plane * 32 /* floats a cell */) + pstride * n * sizeof(float) + sb * (size_t)part +
+                        ((size_t)2 << 30);
+    W.lean = need > fr;
+  }
   LeanScope lean(C);
   if (W.lean) {
     // the tracers are in the state after the window: their buffers hold the
@@ -443,10 +478,11 @@ int window_adjoint(float* const* lam, float* const* lam_sct) {
       }
     }
     if (!W.lean) {
-      // the model continues from the state after the window
+      // the model continues from the state after the window (with the
+      // tendencies, which the dynamics run again cleared in tend0)
       tr.qcur = W.fin_qcur;
       tr.q_valid = true;
-      OG_CHECK(copy_state(C, W.fin, true, false, false));
+      OG_CHECK(copy_state(C, W.fin, true, W.lean_ok, false));
       C.dy.div_first = W.fin_div_first;
       C.dy.vort_first = W.fin_vort_first;
     } else {

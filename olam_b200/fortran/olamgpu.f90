@@ -30,6 +30,7 @@ module olamgpu_c
                                OLAMGPU_F_ALL = 65535
   integer(c_int), parameter :: OLAMGPU_TS_GRAPH = 1, OLAMGPU_TS_HORIZ_K = 2, &
                                OLAMGPU_TS_MAXMIN = 4, OLAMGPU_TS_MASS = 8
+  integer(c_int), parameter :: OLAMGPU_WIN_HOST = 1, OLAMGPU_WIN_LEAN = 2
 
   type, bind(C) :: olamgpu_grid
      integer(c_int) :: mza, mwa, mva, mma
@@ -176,10 +177,13 @@ module olamgpu_c
        type(c_ptr), intent(in) :: lam(*)
        type(c_ptr), intent(in) :: lam_sct(*)
      end function
-     integer(c_int) function olamgpu_window_memory(host_checkpoints, segment_steps, nsteps, nchk) &
+     integer(c_int) function olamgpu_window_memory(flags, segment_steps, nsteps, nchk) &
          bind(C, name="olamgpu_window_memory")
        import :: c_int
-       integer(c_int), value :: host_checkpoints, segment_steps, nsteps, nchk
+       integer(c_int), value :: flags, segment_steps, nsteps, nchk
+     end function
+     integer(c_int) function olamgpu_window_rewind() bind(C, name="olamgpu_window_rewind")
+       import :: c_int
      end function
      integer(c_int) function olamgpu_set_tile_shape(t, g, ks, ord) bind(C, name="olamgpu_set_tile_shape")
        import :: c_int

@@ -30,7 +30,7 @@ EXPORTS = [
     "olamgpu_set_scalars_bottom", "olamgpu_diagvel_t3d", "olamgpu_tracer_maxmin", "olamgpu_mass_sums",
     "olamgpu_timestep", "olamgpu_timestep_diag", "olamgpu_set_halo",
     "olamgpu_set_surface_emission", "olamgpu_window_forward", "olamgpu_window_adjoint",
-    "olamgpu_window_memory", "olamgpu_set_tile_shape", "olamgpu_tile_shape",
+    "olamgpu_window_memory", "olamgpu_window_rewind", "olamgpu_set_tile_shape", "olamgpu_tile_shape",
 ]
 
 
@@ -85,6 +85,7 @@ def load():
     lib.olamgpu_window_forward.argtypes = [C.c_int, C.c_int, C.c_uint]
     lib.olamgpu_window_adjoint.argtypes = [C.POINTER(abi.c_float_p), C.POINTER(abi.c_float_p)]
     lib.olamgpu_window_memory.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.olamgpu_window_rewind.argtypes = []
     lib.olamgpu_set_tile_shape.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
     lib.olamgpu_tile_shape.argtypes = [abi.c_int_p, C.c_int, abi.c_int_p, abi.c_float_p]
     for name in EXPORTS:
@@ -263,13 +264,19 @@ class OlamGpu:
         check(self.lib.olamgpu_window_adjoint(abi.ptr_array(lam_io, C.c_float), abi.ptr_array(lsct, C.c_float)))
         return lam_io, lsct
 
-    def window_memory(self, host_checkpoints=False, segment_steps=0, nsteps=0, nchk=0):
+    def window_rewind(self):
+        """The state at the start of the last window back on the device (an
+        unlimited window's tracers excepted: send the new ones after it)."""
+        check(self.lib.olamgpu_window_rewind())
+
+    def window_memory(self, host_checkpoints=False, segment_steps=0, nsteps=0, nchk=0, lean=False):
         """Where the next window keeps its states: page-locked host memory for
         the checkpoints and the final state (reserved now for nsteps / nchk
-        when both are given), and how many steps' transport inputs the
-        adjoint holds at once (0: a whole segment)."""
-        check(self.lib.olamgpu_window_memory(int(bool(host_checkpoints)), int(segment_steps), int(nsteps),
-                                             int(nchk)))
+        when both are given); how many steps' transport inputs the adjoint
+        holds at once (0: a whole segment); lean: the adjoint borrows the
+        tracer buffers even when the device has room for its own."""
+        flags = (abi.WIN_HOST if host_checkpoints else 0) | (abi.WIN_LEAN if lean else 0)
+        check(self.lib.olamgpu_window_memory(flags, int(segment_steps), int(nsteps), int(nchk)))
 
     def timestep_diag(self, ntr, nmass=0):
         smax = np.zeros((ntr, 2), np.float32)

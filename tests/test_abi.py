@@ -68,6 +68,7 @@ def test_strerror_and_state_errors():
     assert L.olamgpu_window_forward(2, 1, 0) == abi.E_STATE
     assert L.olamgpu_window_adjoint(None, None) == abi.E_STATE
     assert L.olamgpu_window_memory(1, 0, 4, 2) == abi.E_STATE
+    assert L.olamgpu_window_rewind() == abi.E_STATE
 
 
 def test_null_arguments_rejected():

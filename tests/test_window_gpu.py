@@ -11,7 +11,7 @@ the window and the surface emission rate of each tracer.  Checked against
     adjoint (olamgpu_scalar_transport_rk_adjoint) applied step by step in
     reverse -- the recomputation from checkpoints must give the same;
   * the FP64 oracle's one-step adjoints chained over the same winds, and
-    central finite differences of the FP64 oracle's forward chain along
+    central finite differences of the FP64 oracle's forward chain along 50
     seeded directions of the initial tracers and the emission."""
 import numpy as np
 import pytest
@@ -169,7 +169,7 @@ def test_window_gradient_against_fp64_oracle_and_differences(window_runs):
 
     def J(scp):
         return sum(float((scp[n] * r["lam"][n].astype(np.float64)).sum()) for n in range(NTR))
-    for _ in range(3):
+    for _ in range(50):
         dx = [rng.standard_normal((g.mwa, g.mza)) * t for t in r["tr"]]
         de = [rng.standard_normal(g.mwa) * e for e in r["emis"]]
         for a in dx:
@@ -189,10 +189,13 @@ def test_window_gradient_against_fp64_oracle_and_differences(window_runs):
 
 def test_window_host_checkpoints_and_parts(window_runs):
     """The window with its checkpoints and final state in page-locked host
-    memory, a checkpoint every 3 steps and the adjoint holding one step's
-    inputs at a time (each step of a segment from its checkpoint again):
-    the same gradients, bit for bit, as device checkpoints every 2 steps
-    reversed a segment at a time.  Then the model goes on: one more long
+    memory, a checkpoint every 3 steps, the adjoint holding one step's
+    inputs at a time (each step of a segment from its checkpoint again) and
+    lean (its lam arrays in the tracer buffers, the tendencies' adjoint
+    summed in place): the same gradient of the initial tracers bit for bit
+    as device checkpoints every 2 steps reversed a segment at a time with
+    the adjoint's own buffers, the emission's to 1e-6 (the sum over the
+    steps rounds in another order).  Then the model goes on: one more long
     step (recorded again, the per-tracer arrays allocated anew) equals the
     window's own run continued by one step."""
     r = window_runs
@@ -201,7 +204,7 @@ def test_window_host_checkpoints_and_parts(window_runs):
     try:
         with pytest.raises(Exception):
             dev.window_memory(True, 1, NSTEPS, 3)      # no long step yet: sizes unknown
-        dev.window_memory(True, 1)                      # host memory taken by the window itself
+        dev.window_memory(True, 1, lean=True)           # host memory taken by the window itself
         dev.window_forward(NSTEPS, 3, abi.TS_GRAPH)
         lam = [x.copy() for x in r["lam"]]
         g0, gs = dev.window_adjoint(lam, in_place=True)
@@ -216,7 +219,7 @@ def test_window_host_checkpoints_and_parts(window_runs):
         dev.close()
     for n in range(NTR):
         assert np.array_equal(g0[n], r["g0"][n]), n
-        assert np.array_equal(gs[n], r["gs"][n]), n
+        assert relerr(gs[n][1:], r["gs"][n][1:]) < 1e-6, n
         assert np.array_equal(restored[n], r["after"][n]), n
     dev, hs, var_p = new_device(g, ds, tr, emis, r["opts"])
     try:
@@ -228,6 +231,32 @@ def test_window_host_checkpoints_and_parts(window_runs):
         dev.close()
     for n in range(NTR):
         assert np.array_equal(next_step[n], ref[n]), n
+
+
+def test_window_rewind_runs_the_window_again(window_runs):
+    """After the window and its adjoint, olamgpu_window_rewind puts the
+    window's start back; with the initial tracers sent again the same long
+    steps give the window's own end state bit for bit (the next iteration
+    of an inversion runs on the same winds)."""
+    r = window_runs
+    g, ds, tr, emis = case()
+    dev, hs, var_p = new_device(g, ds, tr, emis, r["opts"])
+    try:
+        dev.window_memory(False, 0, lean=True)
+        dev.window_forward(NSTEPS, NCHK, abi.TS_GRAPH)
+        dev.window_adjoint(r["lam"])
+        dev.window_rewind()
+        for t, t0 in zip(var_p, tr):
+            t[...] = t0
+        dev.sync_to_device(abi.F_SCALARS)
+        for _ in range(NSTEPS):
+            dev.timestep(abi.TS_GRAPH)
+        dev.sync_to_host(abi.F_SCALARS)
+        again = [t.copy() for t in var_p]
+    finally:
+        dev.close()
+    for n in range(NTR):
+        assert np.array_equal(again[n], r["after"][n]), n
 
 
 def test_surface_emission_adds_mass():
