@@ -426,63 +426,57 @@ struct WrtSmem {
 // i % 32 (R rows per lane, i = lane + 32 r); in a step of stride s every row
 // eliminates its couplings to rows i - s and i + s with those rows' current
 // equations (rows outside the system act as identity rows), so after
-// ceil(log2(n)) steps each row holds x(k) = d / b.  The equations live in
-// the column's shared memory as FP64 (the inputs and the result are the
-// reference's real(4)): w is a small residual of large terms, and FP64 keeps
-// it nearer the exact solve than a real(4) sweep.  The four FP64 arrays
-// reuse pex and rex (not read after phase 2) and the float coefficient
-// arrays themselves (read into registers first).
+// ceil(log2(n)) steps each row holds x(k) = d / b.  A lane keeps its rows'
+// equations in registers and publishes, per step, a, c, d and 1 / b of each
+// in the column's shared memory for the rows that eliminate against it (one
+// division per row and step).  The equations are FP64 (the inputs and the
+// result are the reference's real(4)): w is a small residual of large
+// terms, and FP64 keeps it nearer the exact solve than a real(4) sweep.  The
+// four FP64 arrays reuse pex and rex (not read after phase 2) and the float
+// coefficient arrays themselves (read into registers first).
 template <int R>
 __device__ __forceinline__ void warp_tridiag(WrtSmem& m, int k0, int k1, int lane) {
   const int n = k1 - k0 + 1;
   double* A = m.pex;
-  double* B = m.rex;
+  double* RB = m.rex;                               // 1 / b
   double* Cc = reinterpret_cast<double*>(m.b31);   // b31 and b32: 2 mza floats
   double* D = reinterpret_cast<double*>(m.b33);    // b33 and dwm
-  float ra[R], rb[R], rc[R], rd[R];
+  double ra[R], rb[R], rc[R], rd[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = lane + 32 * r;
-    ra[r] = i < n && i > 0 ? m.b31[k0 + i] : 0.f;
-    rb[r] = i < n ? m.b32[k0 + i] : 1.f;
-    rc[r] = i < n - 1 ? m.b33[k0 + i] : 0.f;
-    rd[r] = i < n ? m.dwm[k0 + i] : 0.f;
-  }
-  __syncwarp();
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int i = lane + 32 * r;
-    if (i < n) { A[i] = ra[r]; B[i] = rb[r]; Cc[i] = rc[r]; D[i] = rd[r]; }
+    ra[r] = i < n && i > 0 ? (double)m.b31[k0 + i] : 0.0;
+    rb[r] = i < n ? (double)m.b32[k0 + i] : 1.0;
+    rc[r] = i < n - 1 ? (double)m.b33[k0 + i] : 0.0;
+    rd[r] = i < n ? (double)m.dwm[k0 + i] : 0.0;
   }
   __syncwarp();
   for (int s = 1; s < n; s <<= 1) {
-    double na[R], nb[R], nc[R], nd[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n) { A[i] = ra[r]; RB[i] = 1.0 / rb[r]; Cc[i] = rc[r]; D[i] = rd[r]; }
+    }
+    __syncwarp();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = lane + 32 * r;
       if (i >= n) continue;
       const int im = i - s, ip = i + s;
-      const double ai = A[i], bi = B[i], ci = Cc[i], di = D[i];
       double al = 0.0, ga = 0.0, am = 0.0, cm = 0.0, dm = 0.0, ap = 0.0, cp = 0.0, dp = 0.0;
-      if (im >= 0) { al = -ai / B[im]; am = A[im]; cm = Cc[im]; dm = D[im]; }
-      if (ip < n) { ga = -ci / B[ip]; ap = A[ip]; cp = Cc[ip]; dp = D[ip]; }
-      na[r] = al * am;
-      nc[r] = ga * cp;
-      nb[r] = bi + al * cm + ga * ap;
-      nd[r] = di + al * dm + ga * dp;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = lane + 32 * r;
-      if (i < n) { A[i] = na[r]; B[i] = nb[r]; Cc[i] = nc[r]; D[i] = nd[r]; }
+      if (im >= 0) { al = -ra[r] * RB[im]; am = A[im]; cm = Cc[im]; dm = D[im]; }
+      if (ip < n) { ga = -rc[r] * RB[ip]; ap = A[ip]; cp = Cc[ip]; dp = D[ip]; }
+      rb[r] = rb[r] + al * cm + ga * ap;
+      rd[r] = rd[r] + al * dm + ga * dp;
+      ra[r] = al * am;
+      rc[r] = ga * cp;
     }
     __syncwarp();
   }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = lane + 32 * r;
-    if (i < n) m.wmf[k0 + i] = (float)(D[i] / B[i]);
+    if (i < n) m.wmf[k0 + i] = (float)(rd[r] / rb[r]);
   }
 }
 
