@@ -480,7 +480,7 @@ __device__ __forceinline__ void warp_tridiag(WrtSmem& m, int k0, int k1, int lan
   }
 }
 
-__global__ void __launch_bounds__(WRT_WARPS * 32, 6) k_wrt_begs(DynK g, WrtArgs A) {
+__global__ void __launch_bounds__(WRT_WARPS * 32, 8) k_wrt_begs(DynK g, WrtArgs A) {
   extern __shared__ double wsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j = blockIdx.x * WRT_WARPS + warp;
@@ -1224,6 +1224,11 @@ int dyn_prog_wrtv_rk(int istp) {
     A.gdz_wgtm8 = y.gdz_wgtm8.p; A.gdz_wgtp8 = y.gdz_wgtp8.p; A.gdz_wgtm = y.gdz_wgtm.p; A.gdz_wgtp = y.gdz_wgtp.p;
     A.zwgt_bot8 = y.zwgt_bot8.p; A.zwgt_top8 = y.zwgt_top8.p; A.b20 = y.b20.p;
     const size_t smem = (size_t)WRT_WARPS * mza * 13 * sizeof(double);
+    // eight blocks of four column warps per SM: 64 registers a thread and
+    // the whole shared-memory carveout (8 x 25 KB at 61 levels; above 118
+    // levels a block needs more than the default 48 KB)
+    OG_CUDA(cudaFuncSetAttribute(k_wrt_begs, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    OG_CUDA(cudaFuncSetAttribute(k_wrt_begs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     { OG_PROF("wrt_begs", s); k_wrt_begs<<<cdiv(d.nw_prog, WRT_WARPS), WRT_WARPS * 32, smem, s>>>(g, A); OG_LAUNCHED(); }
     if (C.halo.on) {
       // prog_wrtv_rk.f90:418-429: what prog_v_begs reads at border V points

@@ -102,6 +102,21 @@ def test_long_step_parity_sync(kw):
         assert np.isfinite(hs[n]).all()
 
 
+@pytest.mark.parametrize("nlev", [70, 124])
+def test_long_step_parity_tall_columns(nlev):
+    """Columns of more than 65 levels (the column solve with four rows a
+    lane) and of more than 118 (a block of the column solve kernel above the
+    default 48 KB of shared memory)."""
+    g, ds = dyn_case(nxp=4, nlev=nlev, seed=6)
+    fg = abi.FortranGrid(g)
+    opts = abi.make_opts(300.0, nacoust=4)
+    arrays = oracle_lib.dyn_arrays(g, ds)
+    o64, _ = oracle_long_steps(fg, opts, arrays, 1, True)
+    o32, _ = oracle_long_steps(fg, opts, arrays, 1, False)
+    hs, _ = gpu_long_steps(fg, opts, arrays, 1, abi.SYNC_EACH_CALL)
+    check_fields(hs, o32, o64)
+
+
 def test_long_steps_parity_resident():
     g, ds = dyn_case(nxp=8, nlev=16, seed=5)
     fg = abi.FortranGrid(g)
