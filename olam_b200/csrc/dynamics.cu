@@ -297,7 +297,8 @@ struct VSide { const float* dxps; const float* dyps; const float* xx0_v; const f
 // is outside the field loop, so each neighbour's table entries and
 // coefficients are read once for the four fields.
 template <int ORD>
-__global__ void k_grad_upv4(DynK g, const int* __restrict__ prog, int nprog, Four s, unsigned gmask,
+__global__ void __launch_bounds__(256, ORD == 2 ? 6 : 1)   // order 2: 40 registers, six blocks per SM
+k_grad_upv4(DynK g, const int* __restrict__ prog, int nprog, Four s, unsigned gmask,
                             unsigned pmask, const float* __restrict__ cx, const float* __restrict__ cy,
                             const float* __restrict__ xy_hu, VSide c, const float* __restrict__ vmc,
                             float* __restrict__ upv) {
