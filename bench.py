@@ -32,6 +32,7 @@ reference itself is Fortran and cannot be built here).
 from __future__ import annotations
 
 import argparse
+import atexit
 import json
 import os
 import subprocess
@@ -97,7 +98,10 @@ def parse():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region: the sampler starts before
+    the warm-up (its first sample can take a second to come) and begin()
+    marks the start of the timed region; stop() keeps the samples that
+    arrived after the mark."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -107,25 +111,42 @@ class Clocks:
         self.index = index
         self.proc = None
         self.lines = []
+        self.t0 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            atexit.register(self._end)        # also when the run fails between start and stop
         except OSError:
             self.proc = None
 
+    def _end(self):
+        if self.proc is not None and self.proc.poll() is None:
+            self.proc.kill()
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self, wait_s=5.0):
+        """Mark the start of the timed region, once the sampler runs."""
+        end = time.monotonic() + wait_s
+        while self.proc is not None and not self.lines and time.monotonic() < end:
+            time.sleep(0.01)
+        self.t0 = time.monotonic()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t_end = time.monotonic()
+        # one more sample after the region ends, so that a short region has one
+        while len([1 for t, _ in self.lines if t >= (self.t0 or 0.0)]) == 0 and time.monotonic() < t_end + 0.5:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -133,7 +154,9 @@ class Clocks:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for t, ln in list(self.lines):
+            if self.t0 is not None and t < self.t0:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -880,14 +903,15 @@ def run_decomposed(a, ws, rank, dist):
 
     dev.set_coherence(abi.RESIDENT)
     dev.sync_to_device(abi.F_ALL)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
     dev.scalar_transport_rk(rho_old)
     for _ in range(a.warmup):
         dev.scalar_transport_rk(None)
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
-    clocks.start()
+    clocks.begin()
     dev.profile(True, reset=True)
     dev.launch_count(reset=True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1031,13 +1055,14 @@ def main():
         dev.sync_to_host(abi.F_SCALARS)
         gpu_first = [t.copy() for t in var_p[:len(init_sample)]]
         mass_after = tracer_masses(g, st.rho, var_p)
+    clocks = Clocks(local)
+    clocks.start()
     for _ in range(a.warmup):
         dev.scalar_transport_rk(None)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(local)
-    clocks.start()
+    clocks.begin()
     dev.profile(True, reset=True)
     dev.launch_count(reset=True)
     e0 = torch.cuda.Event(enable_timing=True)

@@ -61,3 +61,32 @@ def test_recomputed_steps():
     assert b.recomputed_steps(24, 12, 4) == 2 * (12 + 8 + 4)
     # a ragged last segment and part: segments [0, 3), [3, 5); parts of 1
     assert b.recomputed_steps(5, 3, 1) == (3 + 2 + 1) + (2 + 1)
+
+
+def test_clock_samples_of_the_timed_region():
+    """Only samples that arrive after begin() count; throttle reasons are
+    read from the active columns."""
+    b = bench()
+
+    class FakeProc:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+        def poll(self):
+            return 0
+
+    c = b.Clocks(0)
+    c.proc = FakeProc()
+    c.t0 = 10.0
+    row = "0, {sm}, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, {cap}"
+    c.lines = [(9.0, row.format(sm=900, cap="Not Active")),      # warm-up: left out
+               (10.1, row.format(sm=1900, cap="Not Active")),
+               (10.2, row.format(sm=1800, cap="Active")),
+               (10.3, "garbled")]
+    r = c.stop()
+    assert r["samples"] == 2
+    assert r["sm_mhz"] == 1850.0 and r["sm_max_mhz"] == 1965.0
+    assert r["reasons"] == ["sw_power_cap"]
