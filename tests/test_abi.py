@@ -74,3 +74,26 @@ def test_strerror_and_state_errors():
 def test_null_arguments_rejected():
     L = lib.load()
     assert L.olamgpu_init(None, None, None) == abi.E_ARG
+
+
+def _header_constants():
+    txt = open(os.path.join(ROOT, "include", "olamgpu.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for name, expr in re.findall(r"\b(OLAMGPU_(?:F|TS|WIN)_[A-Z0-9_]+)\s*=\s*([0-9xXa-fA-Fu<\s]+?)\s*[,}\n]", txt):
+        parts = [int(x.strip().rstrip("uU"), 0) for x in expr.split("<<")]   # N, 0xN or N << k
+        out[name] = parts[0] << parts[1] if len(parts) == 2 else parts[0]
+    return out
+
+
+def test_flag_constants_agree_across_bindings():
+    # the flag words of the header, the Python binding and the Fortran module
+    h = _header_constants()
+    assert {"OLAMGPU_F_ALL", "OLAMGPU_TS_GRAPH", "OLAMGPU_WIN_HOST", "OLAMGPU_WIN_LEAN"} <= set(h)
+    for name, v in h.items():
+        assert getattr(abi, name[len("OLAMGPU_"):]) == v, name
+    src = open(os.path.join(ROOT, "olam_b200", "fortran", "olamgpu.f90")).read()
+    fortran = {n: int(v) for n, v in re.findall(r"\b(OLAMGPU_(?:F|TS|WIN)_[A-Z0-9_]+)\s*=\s*(\d+)", src)}
+    assert fortran, "no Fortran parameters found"
+    for name, v in fortran.items():
+        assert h[name] == v, name
